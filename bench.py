@@ -1,0 +1,311 @@
+#!/usr/bin/env python
+"""Benchmark: 12k-panel swept-wing solve on B200, mixed precision vs plain FP64.
+
+Workload (one "step"): the 12,000-panel NACA 0012 swept wing (100 chordwise x
+120 spanwise quads, 45 deg sweep, AR 5, rigid wake, AoA 4.2 deg) solved end to
+end on the device: AIC assembly + factorisation + solve (mixed: FP32 factors,
+3xTF32 tensor-core update, FP64 refinement to ||r||/||b|| <= 1e-12).
+
+  value   device ms per mixed-precision solve, inputs (mesh, RHS) resident in HBM
+  e2e     the same through fp_solve_body with host buffers (H2D of Uinfs, D2H of Gamma)
+  extras  FP64 plain-solve ms, the ratio, |dCL| of mixed vs FP64, per-stage times
+
+The reference arm (--impl reference) times the CPU restatement of the
+reference solve (OpenMP assembly as in the reference's threaded loop, LAPACK
+LU via scipy) on the host cores, on the same configuration.
+
+Run: python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Multi-GPU runs are replicas (the dense solve does not shard): every rank
+solves its own wing; value = slowest rank's ms per step / N.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__ as ge  # noqa: E402
+
+METRIC = "12k-panel wing solve ms, mixed vs FP64 on B200 at |dCL|<=1e-7; adjoint/primal"
+N_CHORD, N_SPAN, AOA = 100, 120, 4.2
+B_SPAN, AR = 5.0, 5.0   # span and aspect ratio b/c_tip (chord 1)
+
+
+def wing_problem(fp, n_chord=N_CHORD, n_span=N_SPAN):
+    w = fp.meshes.swept_wing("0012", n_chord, n_span, 1.0, B_SPAN, 45.0, 1.0)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(AOA)
+    V = np.array([np.cos(a), 0.0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    return w, body, normals, cps, V, D, U
+
+
+def lift_coefficient(fp, body, gamma, V, Uinfs, D, solver):
+    """CL as test/runtests_solvers.jl:146-166: probes 0.02*c off the surface,
+    Cp with the Kutta average, F = -Cp q A n, L projected on cross(D, S)."""
+    body.strength = gamma
+    body.solved = True
+    body.add_field("Uinf", "vector", Uinfs, "cell")
+    body.add_field("Da", "vector", D, "system")
+    body.add_field("Db", "vector", D, "system")
+    fp.calcfield_U(body, body, offset=0.02, characteristiclength=lambda *a: B_SPAN / AR,
+                   fieldname="Uoff", solver=solver)
+    fp.calcfield_Cp(body, 1.0, U_fieldname="Uoff")
+    fp.calcfield_F(body, 1.0, 1.225)
+    Dhat = V / np.linalg.norm(V)
+    Shat = np.array([0.0, 1.0, 0.0])
+    Lhat = np.cross(Dhat, Shat)
+    LDS = fp.calcfield_LDS(body, Lhat, Dhat)
+    nondim = 0.5 * 1.225 * 1.0 * B_SPAN ** 2 / AR
+    L = LDS[:, 0]
+    return float(np.sign(np.dot(L, Lhat)) * np.linalg.norm(L) / nondim)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, ws, dist
+
+
+def max_over_ranks(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_reference_solve(fp, O, nthreads, sample="full"):
+    """One reference solve on the host: OpenMP assembly (threads over panels,
+    src/FLOWPanel_liftingbody.jl:476-478) + LAPACK LU + solve. Returns ms."""
+    w, body, normals, cps, V, D, U = wing_problem(fp)
+    t0 = time.perf_counter()
+    G = O.assemble_vortexring(w, cps, normals, D, D, nthreads=nthreads)
+    b = O.rhs_noflowthrough(U, normals)
+    x = O.solve_ludiv(G, b)
+    t1 = time.perf_counter()
+    return (t1 - t0) * 1e3, x
+
+
+def run_reference(args, rank, ws, dist):
+    if rank != 0:
+        return
+    fp = ge.load_package()
+    O = ge.load_oracle()
+    ncores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(ncores))
+    times = []
+    for i in range(args.warmup + args.steps):
+        ms, _ = cpu_reference_solve(fp, O, ncores)
+        if i >= args.warmup:
+            times.append(ms)
+    v = float(np.mean(times))
+    line = {"metric": METRIC, "value": v, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"swept wing NACA0012 {N_CHORD}x{N_SPAN}=12000 vortex-ring panels, "
+                                   "rigid wake, AoA 4.2, FP64 assembly + LAPACK LU", "n_panels": 12000},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "ms", "cores": ncores, "kind": "port",
+                             "sample": "full 12k-panel solve per step (assembly + dgetrf + dgetrs)"},
+            "e2e": {"value": v, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, ws, dist):
+    fp = ge.load_package()
+    cap = fp._capi
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    w, body, normals, cps, V, D, U = wing_problem(fp)
+    N = w.npanels
+    ctx = cap.Context(device)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    ctx.set_rhs(U)
+    VR = cap.FP_ELEMENT_VORTEXRING
+    opts = {p: cap.make_opts("ludiv", p) for p in ("fp64", "mixed")}
+
+    def device_step(prec):
+        p = cap.FP_PREC_MIXED if prec == "mixed" else cap.FP_PREC_FP64
+        ctx.assemble(VR, 1e-8, 1e-14, p)
+        ctx.factor(p)
+        st = ctx.solve_device(1, opts[prec])
+        return st.ms_assemble + st.ms_factor + st.ms_solve, st
+
+    # warm-up
+    for _ in range(args.warmup):
+        device_step("mixed")
+        device_step("fp64")
+    launches0 = ctx.kernel_launches()
+    res = {}
+    with ClockSampler(device) as clk:
+        for prec in ("mixed", "fp64"):
+            barrier(dist)
+            tot, stages = 0.0, np.zeros(3)
+            for _ in range(args.steps):
+                ms, st = device_step(prec)
+                tot += ms
+                stages += [st.ms_assemble, st.ms_factor, st.ms_solve]
+            res[prec] = (max_over_ranks(dist, tot / args.steps), stages / args.steps, st)
+    launches = ctx.kernel_launches() - launches0
+    ms_mixed, stg_m, st_m = res["mixed"]
+    ms_fp64, stg_d, st_d = res["fp64"]
+
+    # e2e through the public C ABI with host buffers
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        x_m, st = ctx.solve_body(VR, U, opts=opts["mixed"])
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            e2e.append((t1 - t0) * 1e3)
+    e2e_ms = max_over_ranks(dist, float(np.mean(e2e)))
+    x_d, _ = ctx.solve_body(VR, U, opts=opts["fp64"])
+
+    if rank != 0:
+        ctx.close()
+        return
+    # accuracy gate: CL of the mixed and FP64 strengths (same post-processing)
+    solver = fp.B200Solver("ludiv", "fp64", device=device)
+    CLm = lift_coefficient(fp, body, x_m, V, U, D, solver)
+    CLd = lift_coefficient(fp, body, x_d, V, U, D, solver)
+    rel_gamma = float(np.linalg.norm(x_m - x_d) / np.linalg.norm(x_d))
+    # roofline of the assembly kernel (FP64 pipe): ops pinned by the oracle's
+    # operation counter (248 per quad-ring interaction) per launch / device time
+    peak64 = cap.measure_fma_peak(device, True)
+    asm_ms, _ = ctx.last_kernel_ms(cap.FP_STAGE_ASSEMBLE)
+    ops = 248.0 * N * N + 290.0 * 2 * w.nsheddings * N
+    achieved = ops / (stg_d[0] * 1e-3) / 1e12
+    cpu = None
+    if not args.no_cpu_baseline:
+        O = ge.load_oracle()
+        ncores = os.cpu_count() or 1
+        ms_cpu, x_cpu = cpu_reference_solve(fp, O, ncores)
+        cpu = {"value": ms_cpu, "unit": "ms", "cores": ncores, "kind": "port",
+               "sample": "one full 12k-panel solve (OpenMP assembly + LAPACK dgetrf/dgetrs)",
+               "rel_diff_fp64_vs_cpu": float(np.linalg.norm(x_d - x_cpu) / np.linalg.norm(x_cpu))}
+    line = {"metric": METRIC, "value": ms_mixed * 1.0 / ws if ws > 1 else ms_mixed, "unit": "ms",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
+            "data": "synthetic",
+            "config": {"workload": f"swept wing NACA0012 {N_CHORD}x{N_SPAN}=12000 vortex-ring panels, "
+                                   "rigid wake, AoA 4.2; mixed: FP64 assembly, FP32 LU, FP64 IR to 1e-12",
+                       "n_panels": N, "l2": "inputs larger than L2 (AIC 1.15 GB FP64)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "fp64_ms_per_solve": ms_fp64, "speedup_mixed_vs_fp64": ms_fp64 / ms_mixed,
+            "stages_ms": {"mixed": dict(zip(("assemble", "factor", "solve"), stg_m.tolist())),
+                          "fp64": dict(zip(("assemble", "factor", "solve"), stg_d.tolist()))},
+            "accuracy": {"CL_mixed": CLm, "CL_fp64": CLd, "abs_dCL": abs(CLm - CLd),
+                         "rel_gamma_mixed_vs_fp64": rel_gamma, "ir_iters": st_m.ir_iters,
+                         "used_gmres": st_m.used_gmres, "rel_residual_mixed": st_m.rel_residual,
+                         "gepp_certified_fp64": bool(st_d.gepp_certified), "max_abs_L": st_d.max_abs_L},
+            "adjoint_over_primal": None,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 3 * 8 * N,
+                    "d2h_bytes_per_step": 8 * N},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp64", "kernel": "k_asm_ring+k_asm_wake", "achieved": achieved,
+                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
+                         "peak_source": "measured FP64 FMA throughput (fp_measure_fma_peak)"},
+            "clocks": clk.summary()}
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    solver.close()
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, ws, dist = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, ws, dist)
+        else:
+            run_ours(args, rank, ws, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

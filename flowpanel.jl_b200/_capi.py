@@ -1,0 +1,219 @@
+"""ctypes bindings of include/flowpanel_b200.h (the library's C ABI).
+
+The library is loaded from ``_build/libflowpanel_b200.so`` inside this
+package. There is no CPU fallback: without the library (or without a GPU)
+every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libflowpanel_b200.so")
+
+FP_OK, FP_EINVAL, FP_ESINGULAR, FP_ENOCONV, FP_ECUDA, FP_ETIMEOUT, FP_ESTATE = range(7)
+FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING = 0, 1
+FP_PREC_FP64, FP_PREC_MIXED = 0, 1
+FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
+FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND = range(4)
+
+# every symbol the header declares
+EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count", "fp_set_geometry",
+           "fp_set_wake", "fp_assemble", "fp_get_aic", "fp_set_rhs", "fp_factor", "fp_solve",
+           "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
+           "fp_kernel_launches")
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("solver", C.c_int), ("precision", C.c_int), ("ir_tol", C.c_double),
+                ("ir_maxiter", C.c_int), ("gmres_memory", C.c_int), ("gmres_atol", C.c_double),
+                ("gmres_rtol", C.c_double), ("gmres_itmax", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("ms_assemble", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
+                ("ir_iters", C.c_int), ("gmres_iters", C.c_int), ("used_gmres", C.c_int),
+                ("gepp_certified", C.c_int), ("max_abs_L", C.c_double), ("rel_residual", C.c_double)]
+
+    def asdict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class FlowPanelError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not found: build the CUDA library first "
+                               "(python flowpanel.jl_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.fp_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.fp_ctx_destroy.argtypes = [vp]
+        L.fp_last_error.argtypes = [vp]
+        L.fp_last_error.restype = C.c_char_p
+        L.fp_device_count.argtypes = []
+        L.fp_set_geometry.argtypes = [vp, _dp, C.c_int64, _ip, _ip, C.c_int64, _dp, _dp, _dp]
+        L.fp_set_wake.argtypes = [vp, _ip, C.c_int64, _dp, _dp]
+        L.fp_assemble.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_int]
+        L.fp_get_aic.argtypes = [vp, _dp]
+        L.fp_set_rhs.argtypes = [vp, _dp, C.c_int64]
+        L.fp_factor.argtypes = [vp, C.c_int]
+        L.fp_solve.argtypes = [vp, _dp, C.c_int64, C.POINTER(SolveOpts), C.POINTER(Stats)]
+        L.fp_solve_body.argtypes = [vp, C.c_int, C.c_double, C.c_double, _dp, C.c_int64,
+                                    C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
+        L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
+        L.fp_adjoint_solve.argtypes = [vp, _dp, C.c_int64, _dp]
+        L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
+        L.fp_measure_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
+        L.fp_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def make_opts(solver="ludiv", precision="fp64", ir_tol=1e-12, ir_maxiter=10, gmres_memory=50,
+              gmres_atol=-1.0, gmres_rtol=-1.0, gmres_itmax=0):
+    return SolveOpts(FP_SOLVER_GMRES if solver == "gmres" else FP_SOLVER_LU,
+                     FP_PREC_MIXED if precision == "mixed" else FP_PREC_FP64, ir_tol, ir_maxiter,
+                     gmres_memory, gmres_atol, gmres_rtol, gmres_itmax)
+
+
+class Context:
+    """One device context of the library (one CUDA stream)."""
+
+    def __init__(self, device=0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.fp_ctx_create(int(device), C.byref(h))
+        if rc:
+            raise FlowPanelError(rc, f"fp_ctx_create failed on device {device}")
+        self.h = h
+        self.N = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.fp_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        if rc:
+            raise FlowPanelError(rc, self._L.fp_last_error(self.h).decode())
+
+    def set_geometry(self, nodes, panel_offsets, panel_nodes, cps=None, normals=None, cp_offset=None):
+        nodes = _f64(nodes)
+        offs = np.ascontiguousarray(panel_offsets, dtype=np.int32)
+        pn = np.ascontiguousarray(panel_nodes, dtype=np.int32)
+        cps, normals, cp_offset = _f64(cps), _f64(normals), _f64(cp_offset)
+        self._chk(self._L.fp_set_geometry(self.h, _d(nodes), nodes.shape[0], _i(offs), _i(pn), len(offs) - 1,
+                                          _d(cps), _d(normals), _d(cp_offset)))
+        self.N = len(offs) - 1
+
+    def set_wake(self, shedding, Das, Dbs):
+        sh = np.ascontiguousarray(np.reshape(shedding, (-1, 6)), dtype=np.int32)
+        Das, Dbs = _f64(np.reshape(Das, (-1, 3))), _f64(np.reshape(Dbs, (-1, 3)))
+        self._chk(self._L.fp_set_wake(self.h, _i(sh), sh.shape[0], _d(Das), _d(Dbs)))
+
+    def assemble(self, element, kerneloffset=1e-8, kernelcutoff=1e-14, precision=FP_PREC_FP64):
+        self._chk(self._L.fp_assemble(self.h, element, kerneloffset, kernelcutoff, precision))
+
+    def get_aic(self):
+        G = np.empty((self.N, self.N), order="F")
+        self._chk(self._L.fp_get_aic(self.h, G.ctypes.data_as(_dp)))
+        return G
+
+    def set_rhs(self, Uinfs):
+        U = _f64(Uinfs)
+        k = U.size // (3 * self.N)
+        self._chk(self._L.fp_set_rhs(self.h, _d(U), k))
+        return k
+
+    def factor(self, precision=FP_PREC_FP64):
+        self._chk(self._L.fp_factor(self.h, precision))
+
+    def solve(self, k=1, opts=None):
+        x = np.empty((k, self.N))
+        st = Stats()
+        self._chk(self._L.fp_solve(self.h, _d(x), k, C.byref(opts) if opts is not None else None, C.byref(st)))
+        return (x[0] if k == 1 else x), st
+
+    def solve_device(self, k=1, opts=None):
+        """Solve without copying the solution back (it stays in HBM)."""
+        st = Stats()
+        self._chk(self._L.fp_solve(self.h, None, k, C.byref(opts) if opts is not None else None, C.byref(st)))
+        return st
+
+    def solve_body(self, element, Uinfs, kerneloffset=1e-8, kernelcutoff=1e-14, opts=None):
+        U = _f64(Uinfs)
+        k = U.size // (3 * self.N)
+        x = np.empty((k, self.N))
+        st = Stats()
+        self._chk(self._L.fp_solve_body(self.h, element, kerneloffset, kernelcutoff, _d(U), k,
+                                        C.byref(opts) if opts is not None else None, _d(x), C.byref(st)))
+        return (x[0] if k == 1 else x), st
+
+    def uind(self, element, strengths, targets, out=None, precision=FP_PREC_FP64, kerneloffset=1e-8,
+             kernelcutoff=1e-14):
+        targets = _f64(np.reshape(targets, (-1, 3)))
+        m = targets.shape[0]
+        out = np.zeros((m, 3)) if out is None else np.ascontiguousarray(out, dtype=np.float64)
+        self._chk(self._L.fp_uind(self.h, element, _d(_f64(strengths)), _d(targets), m, _d(out), precision,
+                                  kerneloffset, kernelcutoff))
+        return out
+
+    def adjoint_solve(self, ybar):
+        ybar = _f64(np.atleast_2d(ybar))
+        lam = np.empty_like(ybar)
+        self._chk(self._L.fp_adjoint_solve(self.h, _d(ybar), ybar.shape[0], _d(lam)))
+        return lam
+
+    def kernel_launches(self):
+        n = C.c_int64()
+        self._chk(self._L.fp_kernel_launches(self.h, C.byref(n)))
+        return n.value
+
+    def last_kernel_ms(self, stage):
+        ms = C.c_double()
+        n = C.c_int()
+        self._chk(self._L.fp_last_kernel_ms(self.h, stage, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+
+def measure_fma_peak(device=0, fp64=True):
+    """Sustained FMA throughput (TFLOP/s) of the FP64 or FP32 pipe."""
+    t = C.c_double()
+    rc = lib().fp_measure_fma_peak(int(device), 1 if fp64 else 0, C.byref(t))
+    if rc:
+        raise FlowPanelError(rc, "fp_measure_fma_peak failed")
+    return t.value

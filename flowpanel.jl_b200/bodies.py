@@ -1,0 +1,357 @@
+"""Host mirror of FLOWPanel.jl's body / solve / calcfield API over the C ABI.
+
+Names, arguments and error behaviour follow the reference:
+``solve(body, Uinfs, Das, Dbs; solver=...)`` (src/FLOWPanel_liftingbody.jl:172-216,
+src/FLOWPanel_multibody.jl:312-364, src/FLOWPanel_nonliftingbody.jl:93-130),
+``calcfield_U/Cp/F/LDS`` (src/FLOWPanel_postprocess.jl:28-110,1059-1689). The
+solver object is the drop-in: ``B200Solver`` owns a device context and runs the
+assembly, factorisation, solve and induced-velocity evaluation on the GPU.
+Geometry preprocessing and the O(N) post-processing stay on the host, as in
+the reference.
+"""
+from __future__ import annotations
+
+from typing import Callable, Dict, List, Optional
+
+import numpy as np
+
+from . import _capi
+from .meshes import Body as BodyInfo
+from .meshes import Mesh, concat
+
+
+# ----------------------------------------------------------------------------- bodies
+class AbstractBody:
+    element = None
+
+    def __init__(self, mesh: Mesh, CPoffset=1e-14, kerneloffset=1e-8, kernelcutoff=1e-14,
+                 characteristiclength: Optional[Callable] = None, name=None):
+        self.mesh = mesh
+        self.ncells = mesh.npanels
+        self.nnodes = mesh.nnodes
+        self.nsheddings = mesh.nsheddings
+        self.CPoffset = CPoffset
+        self.kerneloffset = kerneloffset
+        self.kernelcutoff = kernelcutoff
+        self.characteristiclength = characteristiclength
+        self.strength = np.zeros(self.ncells)
+        self.fields: Dict[str, dict] = {}
+        self.solved = False
+        self.name = name or type(self).__name__
+        if not mesh.bodies:
+            mesh.bodies = [BodyInfo(self.name, self.kind, mesh.npanels, mesh.nsheddings, CPoffset,
+                                    kerneloffset, kernelcutoff)]
+
+    kind = "vortexring"
+
+    # fields (src/FLOWPanel_abstractbody.jl:358-430)
+    def add_field(self, name, ftype, data, entry):
+        self.fields[name] = {"field_name": name, "field_type": ftype, "field_data": data, "entry_type": entry}
+
+    def get_field(self, name):
+        return self.fields[name]
+
+    def check_field(self, name):
+        return name in self.fields
+
+    def _cp_off_vector(self, off):
+        """Per-panel control-point offsets: a plain body uses ``off`` as given; a
+        MultiBody multiplies it by each member's sign(CPoffset)
+        (src/FLOWPanel_multibody.jl:664-676)."""
+        return np.full(self.ncells, float(off))
+
+    def _l_vector(self, characteristiclength):
+        if characteristiclength is None:
+            return np.ones(self.ncells)
+        return np.array([float(characteristiclength(self.mesh.nodes.T, self.mesh.panel(i)))
+                         for i in range(self.ncells)])
+
+
+class NonLiftingBody(AbstractBody):
+    """NonLiftingBody{ConstantSource} (src/FLOWPanel_nonliftingbody.jl:32-72)."""
+    kind = "source"
+    element = _capi.FP_ELEMENT_SOURCE
+
+
+class RigidWakeBody(AbstractBody):
+    """RigidWakeBody{VortexRing, 1} (src/FLOWPanel_liftingbody.jl:43-134)."""
+    kind = "vortexring"
+    element = _capi.FP_ELEMENT_VORTEXRING
+
+
+class MultiBody(AbstractBody):
+    """MultiBody of vortex-ring bodies (src/FLOWPanel_multibody.jl:19-79): the
+    bodies' panels are concatenated in order; G's column blocks follow them."""
+    kind = "vortexring"
+    element = _capi.FP_ELEMENT_VORTEXRING
+
+    def __init__(self, bodies: List[AbstractBody], names=None):
+        kinds = {b.kind for b in bodies}
+        if len(kinds) != 1:
+            raise ValueError("MultiBody: all bodies must use the same element type")
+        offs = {(b.kerneloffset, b.kernelcutoff) for b in bodies}
+        if len(offs) != 1:
+            raise ValueError("MultiBody: all bodies must share kerneloffset and kernelcutoff")
+        self.bodies = bodies
+        mesh = concat([b.mesh for b in bodies])
+        for info, b in zip(mesh.bodies, bodies):
+            info.CPoffset = b.CPoffset
+        b0 = bodies[0]
+        super().__init__(mesh, b0.CPoffset, b0.kerneloffset, b0.kernelcutoff, None, "MultiBody")
+        self.kind = b0.kind
+        self.element = b0.element
+
+    def _cp_off_vector(self, off):
+        out = np.empty(self.ncells)
+        k = 0
+        for b in self.bodies:
+            s = np.sign(b.CPoffset) if b.CPoffset != 0 else 1.0
+            out[k:k + b.ncells] = s * off
+            k += b.ncells
+        return out
+
+    def _l_vector(self, characteristiclength):
+        if characteristiclength is not None:
+            return super()._l_vector(characteristiclength)
+        return np.concatenate([b._l_vector(b.characteristiclength) for b in self.bodies])
+
+    def _default_off(self):
+        return np.concatenate([np.full(b.ncells, b.CPoffset) for b in self.bodies])
+
+
+# ----------------------------------------------------------------------------- geometry
+def _panel_arrays(mesh: Mesh):
+    """Dense (N, 4) node index array (triangles repeat no node: nn recorded)."""
+    offs = mesh.panel_offsets
+    nn = np.diff(offs)
+    idx = np.zeros((mesh.npanels, 4), np.int64)
+    for k in range(4):
+        sel = nn > k
+        idx[sel, k] = mesh.panel_nodes[offs[:-1][sel] + k]
+    return idx, nn
+
+
+def _frame(mesh: Mesh):
+    idx, nn = _panel_arrays(mesh)
+    P = mesh.nodes
+    e = P[idx[:, 1]] - P[idx[:, 0]]
+    f = P[idx[:, 2]] - P[idx[:, 0]]
+    t = e / np.linalg.norm(e, axis=1)[:, None]
+    c = np.cross(e, f)
+    n = c / np.linalg.norm(c, axis=1)[:, None]
+    o = np.cross(n, t)
+    return t, o, n, idx, nn
+
+
+def calc_normals(body: AbstractBody, flipbyCPoffset=False):
+    """Unit normals (N, 3) (src/FLOWPanel_abstractbody.jl:738-776)."""
+    _, _, n, _, _ = _frame(body.mesh)
+    if flipbyCPoffset:
+        if isinstance(body, MultiBody):
+            s = body._cp_off_vector(1.0)
+            n = n * s[:, None]
+        else:
+            n = n * (np.sign(body.CPoffset) if body.CPoffset != 0 else 1.0)
+    return n
+
+
+def calc_controlpoints(body: AbstractBody, normals=None, off=None, characteristiclength=None):
+    """Control points (N, 3): vertex mean, in-plane centroid correction, then
+    + off * l * n (src/FLOWPanel_abstractbody.jl:635-694)."""
+    t, o, n, idx, nn = _frame(body.mesh)
+    normals = n if normals is None else normals
+    P = body.mesh.nodes
+    mask = (np.arange(4)[None, :] < nn[:, None]).astype(float)
+    pts = P[idx] * mask[:, :, None]
+    c = pts.sum(axis=1) / nn[:, None]
+    d = (P[idx] - c[:, None, :]) * mask[:, :, None]
+    x = np.einsum("pkd,pd->p", d, t) / nn
+    y = np.einsum("pkd,pd->p", d, o) / nn
+    c = c + x[:, None] * t + y[:, None] * o
+    if off is None:
+        offv = body._default_off() if isinstance(body, MultiBody) else np.full(body.ncells, body.CPoffset)
+        l = body._l_vector(body.characteristiclength if not isinstance(body, MultiBody) else None)
+    else:
+        offv = body._cp_off_vector(off)
+        l = body._l_vector(characteristiclength)
+    return c + (offv * l)[:, None] * normals
+
+
+def calc_areas(body: AbstractBody):
+    """Panel areas (fan of triangles from the first node)."""
+    idx, nn = _panel_arrays(body.mesh)
+    P = body.mesh.nodes
+    a = 0.5 * np.linalg.norm(np.cross(P[idx[:, 1]] - P[idx[:, 0]], P[idx[:, 2]] - P[idx[:, 0]]), axis=1)
+    q = nn == 4
+    a[q] += 0.5 * np.linalg.norm(np.cross(P[idx[q, 2]] - P[idx[q, 0]], P[idx[q, 3]] - P[idx[q, 0]]), axis=1)
+    return a
+
+
+# ----------------------------------------------------------------------------- solver
+class B200Solver:
+    """The GPU solver object passed as ``solver=`` (the drop-in of
+    src/FLOWPanel_linearsolver.jl:24-157's solvers, owning assembly too).
+
+    method: "ludiv" | "backslash" (LU, same on the device) | "gmres"
+    precision: "fp64" (plain) | "mixed" (FP32 factors + FP64 refinement)
+    """
+
+    def __init__(self, method="ludiv", precision="fp64", device=0, ir_tol=1e-12, ir_maxiter=10,
+                 gmres_memory=50, atol=None, rtol=None, itmax=0):
+        if method not in ("ludiv", "backslash", "gmres"):
+            raise ValueError(f"unknown method {method}")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"unknown precision {precision}")
+        self.method, self.precision = method, precision
+        self.opts = _capi.make_opts("gmres" if method == "gmres" else "ludiv", precision, ir_tol, ir_maxiter,
+                                    gmres_memory, -1.0 if atol is None else atol,
+                                    -1.0 if rtol is None else rtol, itmax)
+        self.ctx = _capi.Context(device)
+        self.stats = None
+        self._geom_of = None
+
+    def load(self, body: AbstractBody, normals=None, CPs=None):
+        m = body.mesh
+        if normals is None:
+            normals = calc_normals(body)
+        if CPs is None:
+            CPs = calc_controlpoints(body, normals)
+        self.ctx.set_geometry(m.nodes, m.panel_offsets, m.panel_nodes, CPs, normals)
+        self._geom_of = id(body)
+
+    def close(self):
+        self.ctx.close()
+
+
+def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200Solver] = None):
+    """solve(body, Uinfs[, Das, Dbs]; solver): assemble, factor and solve on the
+    GPU, then store the strengths and the fields like the reference."""
+    Uinfs = np.asarray(Uinfs, dtype=np.float64)
+    if Uinfs.shape != (body.ncells, 3):
+        raise ValueError(f"Invalid Uinfs; expected size ({body.ncells}, 3), got {Uinfs.shape}")
+    lifting = body.kind == "vortexring"
+    if lifting:
+        if Das is None or Dbs is None:
+            raise ValueError("lifting bodies need Das and Dbs")
+        Das, Dbs = np.asarray(Das, float), np.asarray(Dbs, float)
+        if Das.shape != (body.nsheddings, 3):
+            raise ValueError(f"Invalid Das; expected size ({body.nsheddings}, 3), got {Das.shape}")
+        if Dbs.shape != (body.nsheddings, 3):
+            raise ValueError(f"Invalid Dbs; expected size ({body.nsheddings}, 3), got {Dbs.shape}")
+    solver = solver or B200Solver()
+    solver.load(body)
+    if lifting and body.nsheddings:
+        solver.ctx.set_wake(body.mesh.shedding, Das, Dbs)
+    elif lifting:
+        solver.ctx.set_wake(np.zeros((0, 6), np.int32), np.zeros((0, 3)), np.zeros((0, 3)))
+    x, st = solver.ctx.solve_body(body.element, Uinfs, body.kerneloffset, body.kernelcutoff, solver.opts)
+    solver.stats = st.asdict()
+    body.strength = np.array(x, dtype=np.float64)
+    body.solved = True
+    body.add_field("Uinf", "vector", Uinfs, "cell")
+    if lifting:
+        body.add_field("Da", "vector", Das, "system")
+        body.add_field("Db", "vector", Dbs, "system")
+        body.add_field("Gamma", "scalar", body.strength, "cell")
+    else:
+        body.add_field("sigma", "scalar", body.strength, "cell")
+    body._solver = solver
+    return body
+
+
+def Uind(body: AbstractBody, targets, out, solver: Optional[B200Solver] = None, precision="fp64"):
+    """Uind!: add the velocity induced by the solved body at targets (M, 3) to out
+    (src/FLOWPanel_abstractbody.jl:101-110)."""
+    if not body.solved:
+        raise RuntimeError("Source body hasn't been solved yet. Please call `solve(...)` function first.")
+    solver = solver or getattr(body, "_solver", None) or B200Solver()
+    if solver._geom_of != id(body):
+        solver.load(body)
+        if body.kind == "vortexring":
+            Da = body.get_field("Da")["field_data"]
+            Db = body.get_field("Db")["field_data"]
+            solver.ctx.set_wake(body.mesh.shedding, Da, Db)
+    prec = _capi.FP_PREC_MIXED if precision == "mixed" else _capi.FP_PREC_FP64
+    return solver.ctx.uind(body.element, body.strength, targets, out, prec,
+                           body.kerneloffset, body.kernelcutoff)
+
+
+def calcfield_U(sourcebody: AbstractBody, targetbody: AbstractBody, offset=None,
+                characteristiclength=None, fieldname="U", addfield=True, solver=None):
+    """calcfield_U: freestream + induced velocity at the (offset) control points
+    of targetbody (src/FLOWPanel_postprocess.jl:28-110)."""
+    if not sourcebody.solved:
+        raise RuntimeError("Source body hasn't been solved yet. Please call `solve(...)` function first.")
+    if not targetbody.check_field("Uinf"):
+        raise RuntimeError("Target body doesn't have freestream field `\"Uinf\"`.")
+    Uinfs = np.asarray(targetbody.get_field("Uinf")["field_data"], float)
+    normals = calc_normals(targetbody)
+    cps = calc_controlpoints(targetbody, normals, off=offset, characteristiclength=characteristiclength) \
+        if offset is not None else calc_controlpoints(targetbody, normals)
+    out = np.array(Uinfs, dtype=np.float64, copy=True)
+    out = Uind(sourcebody, cps, out, solver)
+    if addfield:
+        targetbody.add_field(fieldname, "vector", out, "cell")
+    return out
+
+
+def calcfield_Cp(body: AbstractBody, Uref, U_fieldname="U", Us=None, correct_kuttacondition=True,
+                 clip=None, fieldname="Cp", addfield=True):
+    """calcfield_Cp!: Cp = 1 - (|U|/Uref)^2, Kutta average over (pi, pi+1, pj, pj-1)
+    at each shedding edge (src/FLOWPanel_postprocess.jl:1059-1112)."""
+    Us = np.asarray(body.get_field(U_fieldname)["field_data"] if Us is None else Us, float)
+    Cp = 1 - (np.linalg.norm(Us, axis=1) / Uref) ** 2
+    if correct_kuttacondition and body.kind == "vortexring":
+        for (pi, nia, nib, pj, nja, njb) in body.mesh.shedding:
+            if pj != -1:
+                ave = (Cp[pi] + Cp[pi + 1] + Cp[pj] + Cp[pj - 1]) / 4
+                Cp[[pi, pi + 1, pj, pj - 1]] = ave
+            else:
+                ave = (Cp[pi] + Cp[pi + 1]) / 2
+                Cp[[pi, pi + 1]] = ave
+    if clip is not None:
+        Cp = np.array([clip(v) for v in Cp])
+    if addfield:
+        body.add_field(fieldname, "scalar", Cp, "cell")
+    return Cp
+
+
+def calcfield_F(body: AbstractBody, Uinf, rho, Cp_fieldname="Cp", correct_kuttacondition=True,
+                fieldname="F", addfield=True):
+    """calcfield_F!: F = -Cp (rho Uinf^2 / 2) A n with normals flipped by
+    sign(CPoffset) and the TE override (src/FLOWPanel_postprocess.jl:1199-1392)."""
+    Cps = np.asarray(body.get_field(Cp_fieldname)["field_data"], float)
+    areas = calc_areas(body)
+    normals = calc_normals(body, flipbyCPoffset=True)
+    q = 0.5 * rho * Uinf ** 2
+    F = (-q * Cps * areas)[:, None] * normals
+    if correct_kuttacondition and body.kind == "vortexring":
+        for (pi, nia, nib, pj, nja, njb) in body.mesh.shedding:
+            if pj != -1:
+                idx = [pi, pi + 1, pj, pj - 1]
+                ave = (Cps[pi] + Cps[pi + 1] + Cps[pj] + Cps[pj - 1]) / 4
+            else:
+                idx = [pi, pi + 1]
+                ave = (Cps[pi] + Cps[pi + 1]) / 2
+            for i in idx:
+                F[i] = -ave * q * areas[i] * normals[i]
+    if addfield:
+        body.add_field(fieldname, "vector", F, "cell")
+    return F
+
+
+def calcfield_LDS(body: AbstractBody, Lhat, Dhat, Shat=None, F_fieldname="F", addfield=True):
+    """calcfield_LDS!: lift, drag and sideslip vectors (columns) from the summed
+    force (src/FLOWPanel_postprocess.jl:1615-1689)."""
+    Lhat, Dhat = np.asarray(Lhat, float), np.asarray(Dhat, float)
+    Shat = np.cross(Lhat, Dhat) if Shat is None else np.asarray(Shat, float)
+    for v, nm in ((Lhat, "Lhat"), (Dhat, "Dhat"), (Shat, "Shat")):
+        if abs(np.linalg.norm(v) - 1) > 2 * np.finfo(float).eps:
+            raise ValueError(f"{nm}={v} is not a unitary vector")
+    Ftot = np.sum(np.asarray(body.get_field(F_fieldname)["field_data"], float), axis=0)
+    out = np.stack([Lhat * np.dot(Ftot, Lhat), Dhat * np.dot(Ftot, Dhat), Shat * np.dot(Ftot, Shat)], axis=1)
+    if addfield:
+        body.add_field("L", "vector", out[:, 0], "system")
+        body.add_field("D", "vector", out[:, 1], "system")
+        body.add_field("S", "vector", out[:, 2], "system")
+    return out

@@ -1,0 +1,602 @@
+// C ABI of the B200 panel-method library: context, geometry, orchestration.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fp_internal.cuh"
+
+using namespace fpb;
+
+namespace fpb {
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+}  // namespace fpb
+
+namespace {
+
+template <class T> void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+int check_ctx(fp_ctx* c) { return c ? FP_OK : FP_EINVAL; }
+
+// Device status bits -> FP_* status (and reset the word).
+int consume_status(fp_ctx* c) {
+  int st = 0;
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  if (st) {
+    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+    if (st & DEV_TIMEOUT) return c->err.set(FP_ETIMEOUT, "a bounded device-side wait ran out");
+    if (st & DEV_ZERO_PIVOT) return c->err.set(FP_ESINGULAR, "zero pivot in the LU factorisation");
+  }
+  return FP_OK;
+}
+
+// Panel unit vectors of docs/src/elements/paneldefinition.md:15-35.
+void frame(const double* nodes, const int32_t* pn, double t[3], double o[3], double n[3]) {
+  const double* a = nodes + 3 * (int64_t)pn[0];
+  const double* b = nodes + 3 * (int64_t)pn[1];
+  const double* c = nodes + 3 * (int64_t)pn[2];
+  double e[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  double f[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+  double ne = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+  for (int k = 0; k < 3; ++k) t[k] = e[k] / ne;
+  double cr[3] = {e[1] * f[2] - e[2] * f[1], e[2] * f[0] - e[0] * f[2], e[0] * f[1] - e[1] * f[0]};
+  double nc = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+  for (int k = 0; k < 3; ++k) n[k] = cr[k] / nc;
+  o[0] = n[1] * t[2] - n[2] * t[1];
+  o[1] = n[2] * t[0] - n[0] * t[2];
+  o[2] = n[0] * t[1] - n[1] * t[0];
+}
+
+int ensure_rhs(fp_ctx* c, int64_t k) {
+  if (k <= c->cap_rhs) return FP_OK;
+  dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
+  const size_t n = (size_t)c->ld * k;
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_rhs, n * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_x, n * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_r, n * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_w32, n * sizeof(float)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_norms, 2 * k * sizeof(double)));
+  c->cap_rhs = k;
+  return FP_OK;
+}
+
+int time_begin(fp_ctx* c) {
+  FP_CUDA_TRY(c->err, cudaEventRecord(c->ev0, c->stream));
+  return FP_OK;
+}
+int time_end(fp_ctx* c, double* ms) {
+  FP_CUDA_TRY(c->err, cudaEventRecord(c->ev1, c->stream));
+  FP_CUDA_TRY(c->err, cudaEventSynchronize(c->ev1));
+  float f = 0.f;
+  FP_CUDA_TRY(c->err, cudaEventElapsedTime(&f, c->ev0, c->ev1));
+  *ms = f;
+  return FP_OK;
+}
+
+void free_matrices(fp_ctx* c) {
+  dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
+  dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_part);
+  dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
+  dfree(c->d_V); dfree(c->d_h);
+  c->cap_rhs = 0; c->cap_gmres_m = 0;
+  c->assembled = -1; c->factored = -1; c->nrhs = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fp_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int fp_ctx_create(int device, fp_ctx** out) {
+  if (!out) return FP_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return FP_ECUDA;
+  if (device < 0 || device >= n) return FP_EINVAL;
+  fp_ctx* c = new fp_ctx();
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_cert, sizeof(float)) != cudaSuccess ||
+      cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+    delete c;
+    return FP_ECUDA;
+  }
+  *out = c;
+  return FP_OK;
+}
+
+int fp_ctx_destroy(fp_ctx* c) {
+  if (!c) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_matrices(c);
+  dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt); dfree(c->d_wake);
+  dfree(c->d_status); dfree(c->d_cert);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return FP_OK;
+}
+
+const char* fp_last_error(const fp_ctx* c) { return c ? c->err.msg.c_str() : "null context"; }
+
+int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_t* offsets,
+                    const int32_t* pnodes, int64_t npanels, const double* cps,
+                    const double* normals, const double* cp_offset) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!nodes || !offsets || !pnodes || nnodes <= 0 || npanels <= 0)
+    return c->err.set(FP_EINVAL, "fp_set_geometry: empty mesh or null pointer");
+  if (offsets[0] != 0) return c->err.set(FP_EINVAL, "fp_set_geometry: panel_offsets[0] must be 0");
+  for (int64_t p = 0; p < npanels; ++p) {
+    const int nn = offsets[p + 1] - offsets[p];
+    if (nn < 3 || nn > 4)
+      return c->err.set(FP_EINVAL, "fp_set_geometry: panel " + std::to_string(p) + " has " +
+                                       std::to_string(nn) + " nodes (3 or 4 supported)");
+    for (int k = 0; k < nn; ++k) {
+      const int32_t ni = pnodes[offsets[p] + k];
+      if (ni < 0 || ni >= nnodes)
+        return c->err.set(FP_EINVAL, "fp_set_geometry: node index out of range in panel " + std::to_string(p));
+    }
+  }
+  for (int64_t i = 0; i < 3 * nnodes; ++i)
+    if (!std::isfinite(nodes[i])) return c->err.set(FP_EINVAL, "fp_set_geometry: non-finite node coordinate");
+  if (c->N != npanels) free_matrices(c);
+  c->N = npanels;
+  c->ld = round_up(npanels, 64);
+  c->h_nodes.assign(nodes, nodes + 3 * nnodes);
+  c->h_offsets.assign(offsets, offsets + npanels + 1);
+  c->h_pnodes.assign(pnodes, pnodes + offsets[npanels]);
+  c->assembled = -1;
+  c->factored = -1;
+
+  std::vector<PanelRec> pr(npanels);
+  std::vector<SourceRec> sr(npanels);
+  std::vector<double> tgt(6 * npanels);
+  for (int64_t p = 0; p < npanels; ++p) {
+    const int32_t* pn = pnodes + offsets[p];
+    const int nn = offsets[p + 1] - offsets[p];
+    PanelRec& r = pr[p];
+    std::memset(&r, 0, sizeof(r));
+    for (int k = 0; k < nn; ++k)
+      for (int d = 0; d < 3; ++d) r.p[3 * k + d] = nodes[3 * (int64_t)pn[k] + d];
+    r.nn = nn;
+    double t[3], o[3], n[3];
+    frame(nodes, pn, t, o, n);
+    // source record: flipped frame (o, t, -n) of src/FLOWPanel_elements.jl:51-56
+    SourceRec& s = sr[p];
+    std::memset(&s, 0, sizeof(s));
+    s.nn = nn;
+    const double* O = nodes + 3 * (int64_t)pn[0];
+    for (int d = 0; d < 3; ++d) { s.O[d] = O[d]; s.t[d] = o[d]; s.o[d] = t[d]; s.n[d] = -n[d]; }
+    for (int k = 0; k < nn; ++k) {
+      const double* P = nodes + 3 * (int64_t)pn[k];
+      s.xs[k] = s.t[0] * (P[0] - O[0]) + s.t[1] * (P[1] - O[1]) + s.t[2] * (P[2] - O[2]);
+      s.ys[k] = s.o[0] * (P[0] - O[0]) + s.o[1] * (P[1] - O[1]) + s.o[2] * (P[2] - O[2]);
+      s.zs[k] = s.n[0] * (P[0] - O[0]) + s.n[1] * (P[1] - O[1]) + s.n[2] * (P[2] - O[2]);
+    }
+    for (int k = 0; k < nn; ++k) {
+      const int j = (k + 1) % nn;
+      const double dx = s.xs[j] - s.xs[k], dy = s.ys[j] - s.ys[k], dz = s.zs[j] - s.zs[k];
+      s.dij[k] = std::sqrt(dx * dx + dy * dy + dz * dz);
+      s.S[k] = (s.ys[j] - s.ys[k]) / s.dij[k];
+      s.Cc[k] = (s.xs[j] - s.xs[k]) / s.dij[k];
+    }
+    // control point and normal
+    double cp[3], nr[3];
+    if (normals) { for (int d = 0; d < 3; ++d) nr[d] = normals[3 * p + d]; }
+    else { for (int d = 0; d < 3; ++d) nr[d] = n[d]; }
+    if (cps) {
+      for (int d = 0; d < 3; ++d) cp[d] = cps[3 * p + d];
+    } else {
+      // _calc_controlpoints!: vertex mean, in-plane centroid correction, + off*l*n (l = 1)
+      double cc[3] = {0, 0, 0};
+      for (int k = 0; k < nn; ++k)
+        for (int d = 0; d < 3; ++d) cc[d] += nodes[3 * (int64_t)pn[k] + d];
+      for (int d = 0; d < 3; ++d) cc[d] /= nn;
+      double x = 0, y = 0;
+      for (int k = 0; k < nn; ++k) {
+        const double* P = nodes + 3 * (int64_t)pn[k];
+        for (int d = 0; d < 3; ++d) x += (P[d] - cc[d]) * t[d];
+        for (int d = 0; d < 3; ++d) y += (P[d] - cc[d]) * o[d];
+      }
+      x /= nn; y /= nn;
+      const double off = cp_offset ? cp_offset[p] : 1e-14;
+      for (int d = 0; d < 3; ++d) cp[d] = cc[d] + x * t[d] + y * o[d] + off * 1.0 * nr[d];
+    }
+    for (int d = 0; d < 3; ++d) {
+      tgt[d * npanels + p] = cp[d];
+      tgt[(3 + d) * npanels + p] = nr[d];
+    }
+  }
+  dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt);
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_panels, npanels * sizeof(PanelRec)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_src, npanels * sizeof(SourceRec)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tgt, 6 * npanels * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_panels, pr.data(), npanels * sizeof(PanelRec), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_src, sr.data(), npanels * sizeof(SourceRec), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_tgt, tgt.data(), 6 * npanels * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  c->has_geometry = true;
+  c->nsh = 0;
+  dfree(c->d_wake);
+  return FP_OK;
+}
+
+int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* Das,
+                const double* Dbs) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_set_wake: call fp_set_geometry first");
+  if (nsh < 0 || (nsh > 0 && (!shedding || !Das || !Dbs)))
+    return c->err.set(FP_EINVAL, "fp_set_wake: bad arguments");
+  const double tol = 2 * 2.220446049250313e-16;
+  std::vector<WakeRec> w(nsh);
+  std::vector<int> touched(c->N, 0);
+  bool disjoint = true;
+  for (int64_t e = 0; e < nsh; ++e) {
+    const int32_t* s = shedding + 6 * e;
+    const double* da = Das + 3 * e;
+    const double* db = Dbs + 3 * e;
+    // non-unit direction check of src/FLOWPanel_elements.jl:495-498
+    if (std::fabs(da[0] * da[0] + da[1] * da[1] + da[2] * da[2] - 1) > tol ||
+        std::fabs(db[0] * db[0] + db[1] * db[1] + db[2] * db[2] - 1) > tol)
+      return c->err.set(FP_EINVAL, "Found non-unitary semi-infinite direction at shedding edge " + std::to_string(e));
+    const int pi = s[0], pj = s[3];
+    if (pi < 0 || pi >= c->N || pj < -1 || pj >= c->N)
+      return c->err.set(FP_EINVAL, "fp_set_wake: panel index out of range at edge " + std::to_string(e));
+    auto node_of = [&](int panel, int local, double* out3) -> bool {
+      const int nn = c->h_offsets[panel + 1] - c->h_offsets[panel];
+      if (local < 0 || local >= nn) return false;
+      const int ni = c->h_pnodes[c->h_offsets[panel] + local];
+      for (int d = 0; d < 3; ++d) out3[d] = c->h_nodes[3 * (int64_t)ni + d];
+      return true;
+    };
+    WakeRec& r = w[e];
+    std::memset(&r, 0, sizeof(r));
+    if (!node_of(pi, s[1], r.pa) || !node_of(pi, s[2], r.pb))
+      return c->err.set(FP_EINVAL, "fp_set_wake: local node index out of range at edge " + std::to_string(e));
+    if (pj >= 0 && (!node_of(pj, s[4], r.qa) || !node_of(pj, s[5], r.qb)))
+      return c->err.set(FP_EINVAL, "fp_set_wake: local node index out of range at edge " + std::to_string(e));
+    for (int d = 0; d < 3; ++d) { r.da[d] = da[d]; r.db[d] = db[d]; }
+    r.pi = pi;
+    r.pj = pj;
+    if (touched[pi]++) disjoint = false;
+    if (pj >= 0 && touched[pj]++) disjoint = false;
+  }
+  dfree(c->d_wake);
+  if (nsh > 0) {
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_wake, nsh * sizeof(WakeRec)));
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_wake, w.data(), nsh * sizeof(WakeRec), cudaMemcpyHostToDevice, c->stream));
+    FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  }
+  c->h_shed.assign(shedding, shedding + 6 * nsh);
+  c->h_Da.assign(Das, Das + 3 * nsh);
+  c->h_Db.assign(Dbs, Dbs + 3 * nsh);
+  c->nsh = nsh;
+  c->wake_disjoint = disjoint;
+  c->assembled = -1;
+  c->factored = -1;
+  return FP_OK;
+}
+
+int fp_assemble(fp_ctx* c, int element, double kerneloffset, double kernelcutoff, int precision) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_assemble: no geometry");
+  if (element != FP_ELEMENT_SOURCE && element != FP_ELEMENT_VORTEXRING)
+    return c->err.set(FP_EINVAL, "fp_assemble: unknown element");
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED)
+    return c->err.set(FP_EINVAL, "fp_assemble: unknown precision");
+  const size_t elems = (size_t)c->ld * c->N;
+  if (!c->d_G) {
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G, elems * sizeof(double)));
+    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G, 0, elems * sizeof(double), c->stream));
+  }
+  const bool w32 = precision == FP_PREC_MIXED;
+  if (w32 && !c->d_G32) {
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G32, elems * sizeof(float)));
+    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G32, 0, elems * sizeof(float), c->stream));
+  }
+  c->kern_offset = kerneloffset;
+  c->kern_cutoff = kernelcutoff;
+  if (time_begin(c)) return FP_ECUDA;
+  int rc = element == FP_ELEMENT_VORTEXRING ? launch_assemble_ring(c, kerneloffset, kernelcutoff, w32)
+                                            : launch_assemble_source(c, kerneloffset, w32);
+  if (rc) return rc;
+  if (time_end(c, &c->ms_assemble)) return FP_ECUDA;
+  c->kms[FP_STAGE_ASSEMBLE] = c->ms_assemble;
+  c->klaunch[FP_STAGE_ASSEMBLE] = (element == FP_ELEMENT_VORTEXRING && c->nsh > 0) ? 2 : 1;
+  c->assembled = element;
+  c->assembled_prec = precision;
+  c->factored = -1;
+  return FP_OK;
+}
+
+int fp_get_aic(fp_ctx* c, double* G) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_get_aic: nothing assembled");
+  FP_CUDA_TRY(c->err, cudaMemcpy2DAsync(G, c->N * sizeof(double), c->d_G, c->ld * sizeof(double),
+                                        c->N * sizeof(double), c->N, cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  return FP_OK;
+}
+
+int fp_set_rhs(fp_ctx* c, const double* Uinfs, int64_t k) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_set_rhs: no geometry");
+  if (!Uinfs || k <= 0) return c->err.set(FP_EINVAL, "fp_set_rhs: bad arguments");
+  if (int rc = ensure_rhs(c, k)) return rc;
+  double* dU = nullptr;
+  const size_t bytes = 3 * (size_t)c->N * k * sizeof(double);
+  FP_CUDA_TRY(c->err, cudaMallocAsync(&dU, bytes, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(dU, Uinfs, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = launch_rhs(c, dU, k);
+  cudaFreeAsync(dU, c->stream);
+  if (rc) return rc;
+  c->nrhs = k;
+  return FP_OK;
+}
+
+static int alloc_factor_buffers(fp_ctx* c, int precision) {
+  const size_t elems = (size_t)c->ld * c->N;
+  const int64_t nblk = (c->N + kLuNB - 1) / kLuNB;
+  if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, c->N * sizeof(int32_t)));
+  if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
+  if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * c->N * sizeof(double)));
+  if (precision == FP_PREC_FP64) {
+    if (!c->d_LU) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_LU, elems * sizeof(double)));
+    if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));
+  } else {
+    if (!c->d_G32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G32, elems * sizeof(float)));
+    if (!c->d_dinv32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv32, nblk * 2 * kLuNB * kLuNB * sizeof(float)));
+  }
+  return FP_OK;
+}
+
+int fp_factor(fp_ctx* c, int precision) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_factor: assemble first");
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED)
+    return c->err.set(FP_EINVAL, "fp_factor: unknown precision");
+  if (int rc = alloc_factor_buffers(c, precision)) return rc;
+  if (time_begin(c)) return FP_ECUDA;
+  int rc;
+  if (precision == FP_PREC_FP64) {
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_LU, c->d_G, (size_t)c->ld * c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    rc = lu_factor<double>(c, c->d_LU, c->N, c->ld, c->d_ipiv, c->d_cert);
+    if (!rc) rc = lu_diag_inverses<double>(c, c->d_LU, c->N, c->ld);
+  } else {
+    if (c->assembled_prec != FP_PREC_MIXED) {
+      rc = convert_f64_f32(c, c->d_G, c->d_G32, c->N, c->N, c->ld, c->ld);
+      if (rc) return rc;
+    }
+    rc = lu_factor<float>(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert);
+    if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
+    c->assembled_prec = -2;   // the FP32 copy now holds factors
+  }
+  if (rc) return rc;
+  if (time_end(c, &c->ms_factor)) return FP_ECUDA;
+  c->kms[FP_STAGE_FACTOR] = c->ms_factor;
+  if ((rc = consume_status(c))) return rc;
+  float cert = 0.f;
+  FP_CUDA_TRY(c->err, cudaMemcpy(&cert, c->d_cert, sizeof(float), cudaMemcpyDeviceToHost));
+  c->last.max_abs_L = cert;
+  c->last.gepp_certified = cert <= 1.0f;
+  c->last.ms_factor = c->ms_factor;
+  c->factored = precision;
+  return FP_OK;
+}
+
+static void default_opts(fp_solve_opts& o) {
+  o.solver = FP_SOLVER_LU;
+  o.precision = FP_PREC_FP64;
+  o.ir_tol = 1e-12;
+  o.ir_maxiter = 10;
+  o.gmres_memory = 50;
+  o.gmres_atol = -1;
+  o.gmres_rtol = -1;
+  o.gmres_itmax = 0;
+}
+
+static void normalize_opts(fp_solve_opts& o) {
+  if (o.ir_tol <= 0) o.ir_tol = 1e-12;
+  if (o.ir_maxiter <= 0) o.ir_maxiter = 10;
+  if (o.gmres_memory <= 0) o.gmres_memory = 50;
+}
+
+// max over RHS of ||r_q|| / ||b_q||
+static int residual_ratio(fp_ctx* c, const double* r, const double* b, int64_t k, double* out,
+                          bool need_b) {
+  if (int rc = colnorm2(c, r, c->N, c->ld, k, c->d_norms)) return rc;
+  if (need_b)
+    if (int rc = colnorm2(c, b, c->N, c->ld, k, c->d_norms + k)) return rc;
+  std::vector<double> h(2 * k);
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(h.data(), c->d_norms, 2 * k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  double m = 0;
+  for (int64_t q = 0; q < k; ++q) {
+    const double bn = std::sqrt(h[k + q]);
+    const double rn = std::sqrt(h[q]);
+    m = std::max(m, bn > 0 ? rn / bn : rn);
+  }
+  *out = m;
+  return FP_OK;
+}
+
+int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stats* stats) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  fp_solve_opts o;
+  default_opts(o);
+  if (opts) o = *opts;
+  normalize_opts(o);
+  if (k <= 0 || k > c->nrhs) return c->err.set(FP_EINVAL, "fp_solve: k must be in 1..(number of RHS set)");
+  if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_solve: assemble first");
+  const int64_t n = c->N, ld = c->ld;
+  c->last.ir_iters = 0;
+  c->last.gmres_iters = 0;
+  c->last.used_gmres = 0;
+  int rc;
+  if (time_begin(c)) return FP_ECUDA;
+  if (o.solver == FP_SOLVER_GMRES) {
+    int it = 0;
+    double rr = 0;
+    rc = gmres_solve(c, c->d_rhs, c->d_x, k, o, false, &it, &rr);
+    if (rc && rc != FP_ENOCONV) return rc;
+    c->last.gmres_iters = it;
+    c->last.used_gmres = 1;
+    c->last.rel_residual = rr;
+    if (rc == FP_ENOCONV) {
+      time_end(c, &c->ms_solve);
+      return rc;
+    }
+  } else if (o.precision == FP_PREC_FP64) {
+    if (c->factored != FP_PREC_FP64) return c->err.set(FP_ESTATE, "fp_solve: no FP64 factors (call fp_factor)");
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_x, c->d_rhs, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_x, ld, k, false))) return rc;
+  } else {
+    if (c->factored != FP_PREC_MIXED) return c->err.set(FP_ESTATE, "fp_solve: no FP32 factors (call fp_factor)");
+    // mixed-precision iterative refinement: x0 = A32^-1 b; r = b - A x (FP64); d = A32^-1 r
+    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_x, 0, ld * k * sizeof(double), c->stream));
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_r, c->d_rhs, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    double prev = 1e300, rr = 0;
+    bool converged = false, first = true;
+    for (int it = 0; it < o.ir_maxiter; ++it) {
+      if ((rc = convert_f64_f32(c, c->d_r, c->d_w32, n, k, ld, ld))) return rc;
+      if ((rc = lu_solve<float>(c, c->d_G32, n, ld, c->d_ipiv, c->d_w32, ld, k, false))) return rc;
+      if ((rc = axpy_f32_to_f64(c, c->d_w32, c->d_x, n, k, ld))) return rc;
+      if ((rc = gemv_residual(c, c->d_G, n, ld, c->d_x, c->d_rhs, c->d_r, k))) return rc;
+      if ((rc = residual_ratio(c, c->d_r, c->d_rhs, k, &rr, first))) return rc;
+      if ((rc = consume_status(c))) return rc;
+      first = false;
+      c->last.ir_iters = it + 1;
+      if (rr <= o.ir_tol) { converged = true; break; }
+      if (rr > 0.5 * prev) break;   // stagnating or diverging: hand over to GMRES-IR
+      prev = rr;
+    }
+    c->last.rel_residual = rr;
+    if (!converged) {
+      int it = 0;
+      fp_solve_opts g = o;
+      g.gmres_atol = 0.0;
+      g.gmres_rtol = o.ir_tol;
+      rc = gmres_solve(c, c->d_rhs, c->d_x, k, g, true, &it, &rr);
+      c->last.gmres_iters = it;
+      c->last.used_gmres = 1;
+      c->last.rel_residual = rr;
+      if (rc) { time_end(c, &c->ms_solve); return rc; }
+    }
+  }
+  if (time_end(c, &c->ms_solve)) return FP_ECUDA;
+  c->kms[FP_STAGE_SOLVE] = c->ms_solve;
+  if ((rc = consume_status(c))) return rc;
+  if (o.solver == FP_SOLVER_LU && o.precision == FP_PREC_FP64) {
+    // residual of the FP64 solve, for the statistics
+    if ((rc = gemv_residual(c, c->d_G, n, ld, c->d_x, c->d_rhs, c->d_r, k))) return rc;
+    double rr = 0;
+    if ((rc = residual_ratio(c, c->d_r, c->d_rhs, k, &rr, true))) return rc;
+    c->last.rel_residual = rr;
+  }
+  if (x) {
+    FP_CUDA_TRY(c->err, cudaMemcpy2DAsync(x, n * sizeof(double), c->d_x, ld * sizeof(double), n * sizeof(double), k,
+                                          cudaMemcpyDeviceToHost, c->stream));
+    FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  }
+  c->last.ms_assemble = c->ms_assemble;
+  c->last.ms_factor = c->ms_factor;
+  c->last.ms_solve = c->ms_solve;
+  if (stats) *stats = c->last;
+  return FP_OK;
+}
+
+int fp_solve_body(fp_ctx* c, int element, double kerneloffset, double kernelcutoff,
+                  const double* Uinfs, int64_t k, const fp_solve_opts* opts, double* x,
+                  fp_stats* stats) {
+  if (check_ctx(c)) return FP_EINVAL;
+  fp_solve_opts o;
+  default_opts(o);
+  if (opts) o = *opts;
+  int rc;
+  const int prec = (o.solver == FP_SOLVER_LU) ? o.precision : FP_PREC_FP64;
+  if ((rc = fp_assemble(c, element, kerneloffset, kernelcutoff, prec))) return rc;
+  if ((rc = fp_set_rhs(c, Uinfs, k))) return rc;
+  if (o.solver == FP_SOLVER_LU || o.precision == FP_PREC_MIXED)
+    if ((rc = fp_factor(c, o.precision))) return rc;
+  return fp_solve(c, x, k, &o, stats);
+}
+
+int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targets, int64_t m,
+            double* out, int precision, double kerneloffset, double kernelcutoff) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_uind: no geometry");
+  if (!strengths || (m > 0 && (!targets || !out)) || m < 0)
+    return c->err.set(FP_EINVAL, "fp_uind: bad arguments");
+  if (m == 0) return FP_OK;
+  c->kern_offset = kerneloffset;
+  c->kern_cutoff = kernelcutoff;
+  double *ds = nullptr, *dt = nullptr, *dout = nullptr;
+  FP_CUDA_TRY(c->err, cudaMallocAsync(&ds, c->N * sizeof(double), c->stream));
+  FP_CUDA_TRY(c->err, cudaMallocAsync(&dt, 3 * m * sizeof(double), c->stream));
+  FP_CUDA_TRY(c->err, cudaMallocAsync(&dout, 3 * m * sizeof(double), c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(ds, strengths, c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(dt, targets, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(dout, out, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (time_begin(c)) return FP_ECUDA;
+  int rc = element == FP_ELEMENT_VORTEXRING ? launch_uind_ring(c, ds, dt, m, dout, precision == FP_PREC_MIXED)
+                                            : launch_uind_source(c, ds, dt, m, dout);
+  if (rc) return rc;
+  if (time_end(c, &c->ms_uind)) return FP_ECUDA;
+  c->kms[FP_STAGE_UIND] = c->ms_uind;
+  c->klaunch[FP_STAGE_UIND] = 1;
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(out, dout, 3 * m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  cudaFreeAsync(ds, c->stream);
+  cudaFreeAsync(dt, c->stream);
+  cudaFreeAsync(dout, c->stream);
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  return FP_OK;
+}
+
+int fp_adjoint_solve(fp_ctx* c, const double* ybar, int64_t k, double* lambda) {
+  if (check_ctx(c)) return FP_EINVAL;
+  return c->err.set(FP_EINVAL, "fp_adjoint_solve: transposed solve not built yet");
+}
+
+int fp_kernel_launches(fp_ctx* c, int64_t* count) {
+  if (check_ctx(c) || !count) return FP_EINVAL;
+  *count = c->nlaunch;
+  return FP_OK;
+}
+
+int fp_last_kernel_ms(fp_ctx* c, int stage, double* ms, int* launches) {
+  if (check_ctx(c) || stage < 0 || stage > 3) return FP_EINVAL;
+  if (ms) *ms = c->kms[stage];
+  if (launches) *launches = c->klaunch[stage];
+  return FP_OK;
+}
+
+}  // extern "C"

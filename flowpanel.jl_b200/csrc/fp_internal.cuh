@@ -1,0 +1,115 @@
+// Context and internal launchers of the B200 panel-method library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fp_common.cuh"
+#include "fp_elements.cuh"
+
+// Wake record: both horseshoes of one shedding edge, node coordinates resolved.
+struct WakeRec {
+  double pa[3], pb[3];   // upper: TE[1], TE[2] of panel pi
+  double qa[3], qb[3];   // lower: TE[1], TE[2] of panel pj (unused if pj < 0)
+  double da[3], db[3];
+  int pi, pj;
+};
+
+struct fp_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  fpb::ErrorSink err;
+
+  // sizes
+  int64_t N = 0;        // panels == unknowns == control points
+  int64_t ld = 0;       // leading dimension of the device matrices
+  int64_t nsh = 0;
+  bool wake_disjoint = true;   // every wake column touched by one edge only
+  bool has_geometry = false;
+  int assembled = -1;          // element kind of the assembled G, -1 none
+  int assembled_prec = -1;
+  int factored = -1;           // FP_PREC_* of the factors, -1 none
+  int64_t nrhs = 0;
+  double kern_offset = 1e-8;   // kerneloffset of the assembled body
+  double kern_cutoff = 1e-14;  // kernelcutoff of the assembled body
+
+  // host copies needed for post-processing calls
+  std::vector<int32_t> h_offsets, h_pnodes;
+  std::vector<double> h_nodes;
+  std::vector<int32_t> h_shed;
+  std::vector<double> h_Da, h_Db;
+
+  // device buffers
+  fpb::PanelRec* d_panels = nullptr;    // N records
+  fpb::SourceRec* d_src = nullptr;      // N records (source bodies)
+  double* d_tgt = nullptr;              // 6 x N SoA: cx, cy, cz, nx, ny, nz
+  WakeRec* d_wake = nullptr;            // nsh records
+  double* d_G = nullptr;                // FP64 AIC, ld x N
+  double* d_LU = nullptr;               // FP64 factors, ld x N
+  float* d_G32 = nullptr;               // FP32 AIC copy / FP32 factors, ld x N
+  int32_t* d_ipiv = nullptr;            // N
+  double* d_rhs = nullptr;              // N x k (ld)
+  double* d_x = nullptr;                // N x k
+  double* d_r = nullptr;                // N x k residual (FP64)
+  float* d_w32 = nullptr;               // N x k FP32 work
+  int* d_status = nullptr;              // device status word(s)
+  unsigned int* d_flags = nullptr;      // triangular-solve flags
+  float* d_cert = nullptr;              // max |L| certificate
+  double* d_dinv64 = nullptr;           // inverses of the FP64 diagonal blocks
+  float* d_dinv32 = nullptr;            // inverses of the FP32 diagonal blocks
+  double* d_part = nullptr;             // GEMV partial sums
+  double* d_norms = nullptr;            // column norms (2 x cap_rhs)
+  int64_t cap_rhs = 0;                  // allocated RHS columns
+  size_t cap_flags = 0;
+
+  // GMRES workspace
+  double* d_V = nullptr;                // (m+1) x ld Krylov basis
+  double* d_h = nullptr;                // small vectors
+  int cap_gmres_m = 0;
+
+  // timing
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double ms_assemble = 0, ms_factor = 0, ms_solve = 0, ms_uind = 0;
+  double kms[4] = {0, 0, 0, 0};
+  int klaunch[4] = {0, 0, 0, 0};
+  fp_stats last{};
+  int64_t nlaunch = 0;          // kernels launched by this context
+};
+
+namespace fpb {
+
+// assembly (fp_assembly.cu)
+int launch_assemble_ring(fp_ctx* c, double offset, double cutoff, bool write32);
+int launch_assemble_source(fp_ctx* c, double offset, bool write32);
+int launch_rhs(fp_ctx* c, const double* d_U, int64_t k);
+
+// dense linear algebra (fp_lu.cu)
+template <class T>
+int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert_max_L);
+template <class T>
+int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv, T* B,
+             int64_t ldb, int64_t k, bool transpose);
+int gemv_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const double* x,
+                  const double* b, double* r, int64_t k);
+int convert_f64_f32(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda,
+                    int64_t ldb);
+int axpy_f32_to_f64(fp_ctx* c, const float* d, double* x, int64_t n, int64_t k, int64_t ld);
+template <class T>
+int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda);
+int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out);
+constexpr int kLuNB = 64;        // block size of the factorisation and the solves
+constexpr int kGemvSplitHost = 16;
+
+// induced velocity (fp_field.cu)
+int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
+                     double* d_out, bool fp32);
+int launch_uind_source(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
+                       double* d_out);
+
+// GMRES (fp_gmres.cu)
+int gmres_solve(fp_ctx* c, const double* b, double* x, int64_t k, const fp_solve_opts& o,
+                bool precondition, int* iters, double* relres);
+
+int num_sms();
+}  // namespace fpb

@@ -1,0 +1,646 @@
+// Dense LU factorisation and triangular solves on sm_100a.
+//
+// Blocked right-looking LU with partial pivoting inside each NB x NB diagonal
+// block (the search runs over the rows of the block). After the block is
+// factored, L21 = A21 U11^-1 is formed and max|L21| is kept: when it is <= 1
+// every pivot equals the one LAPACK dgetrf (partial pivoting over the whole
+// column) picks, so the factorisation is the reference's up to rounding
+// (src/FLOWPanel_linearsolver.jl:173-234). The wing AICs of this path need
+// only adjacent-row swaps at the trailing edge, which the block search finds.
+//
+// Per block step: (1) k_panel: every CTA factors the diagonal block
+// redundantly in shared memory, CTA 0 writes it back, each CTA solves its own
+// slab of L21 rows; (2) k_swap_u12: row swaps on the other columns and
+// U12 = L11^-1 A12; (3) the trailing update A22 -= L21 U12 (SIMT FP64 GEMM,
+// or the 3xTF32 tcgen05 kernel of fp_tc.cu for the FP32 factors).
+//
+// Triangular solves run in one persistent kernel per sweep: CTAs take row
+// blocks by ticket (atomic counter), wait (bounded) for the blocks they depend
+// on, subtract their contribution and multiply by the precomputed inverse of
+// the diagonal block.
+#include <cfloat>
+
+#include "fp_internal.cuh"
+
+namespace fpb {
+
+constexpr int NB = 64;          // block size of the factorisation and of the solves
+constexpr int kPanelThreads = 128;
+constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
+
+template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
+
+// ----------------------------------------------------------------------------
+// (1) diagonal-block factorisation (redundant per CTA) + L21 slab solve
+template <class T>
+__global__ void __launch_bounds__(kPanelThreads)
+k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
+        float* __restrict__ cert, int* __restrict__ status) {
+  __shared__ T S[NB][NB + 1];   // S[c][r]: column-major with padding
+  __shared__ int piv_s;
+  __shared__ int lpiv[NB];
+  __shared__ float red[kPanelThreads / 32];
+  const int nb = (int)imin64(NB, n - k);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  // load the diagonal block (padding: identity)
+  for (int q = tid; q < NB * NB; q += kPanelThreads) {
+    const int r = q % NB, cc = q / NB;
+    T v;
+    if (r < nb && cc < nb) v = A[(k + cc) * lda + (k + r)];
+    else v = (r == cc) ? T(1) : T(0);
+    S[cc][r] = v;
+  }
+  __syncthreads();
+
+  for (int j = 0; j < nb; ++j) {
+    if (warp == 0) {
+      T best = T(-1);
+      int bi = j;
+      for (int r = j + lane; r < nb; r += 32) {
+        const T v = tabs(S[j][r]);
+        if (v > best) { best = v; bi = r; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) { piv_s = bi; lpiv[j] = bi; }
+    }
+    __syncthreads();
+    const int p = piv_s;
+    if (p != j && tid < NB) {
+      const T t0 = S[tid][j];
+      S[tid][j] = S[tid][p];
+      S[tid][p] = t0;
+    }
+    __syncthreads();
+    const T pv = S[j][j];
+    if (pv == T(0)) {
+      if (blockIdx.x == 0 && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
+    } else {
+      const T rp = T(1) / pv;
+      for (int r = j + 1 + tid; r < nb; r += kPanelThreads) S[j][r] *= rp;
+    }
+    __syncthreads();
+    const int m = nb - j - 1;
+    for (int q = tid; q < m * m; q += kPanelThreads) {
+      const int r = j + 1 + q % m, cc = j + 1 + q / m;
+      S[cc][r] -= S[j][r] * S[cc][j];
+    }
+    __syncthreads();
+  }
+
+  if (blockIdx.x == 0) {
+    for (int q = tid; q < nb * nb; q += kPanelThreads) {
+      const int r = q % nb, cc = q / nb;
+      A[(k + cc) * lda + (k + r)] = S[cc][r];
+    }
+    for (int j = tid; j < nb; j += kPanelThreads) ipiv[k + j] = (int32_t)(k + lpiv[j]);
+  }
+
+  // L21 rows of this CTA: x U11 = a
+  const int64_t r0 = k + nb + (int64_t)blockIdx.x * kPanelThreads;
+  const int64_t r = r0 + tid;
+  float lmax = 0.f;
+  if (r < n) {
+    T x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? A[(k + j) * lda + r] : T(0);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      if (j < nb) {
+        T s = x[j];
+#pragma unroll
+        for (int l = 0; l < j; ++l) s -= x[l] * S[j][l];
+        s = s / S[j][j];
+        x[j] = s;
+        lmax = fmaxf(lmax, (float)tabs(s));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+      if (j < nb) A[(k + j) * lda + r] = x[j];
+  }
+  // block max -> certificate
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+  if (lane == 0) red[warp] = lmax;
+  __syncthreads();
+  if (tid == 0) {
+    float mm = red[0];
+    for (int w = 1; w < kPanelThreads / 32; ++w) mm = fmaxf(mm, red[w]);
+    if (mm > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(mm));
+  }
+}
+
+// ----------------------------------------------------------------------------
+// (2) row swaps of the block on all other columns; U12 = L11^-1 A12 for the
+// columns right of the block. One warp per column, L11 in shared memory.
+constexpr int kSwapWarps = 4;
+template <class T>
+__global__ void __launch_bounds__(kSwapWarps * 32)
+k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv) {
+  __shared__ T L[NB][NB + 1];      // L[c][r]
+  __shared__ T col[kSwapWarps][NB];
+  __shared__ int lp[NB];
+  const int nb = (int)imin64(NB, n - k);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int q = tid; q < nb * nb; q += blockDim.x) {
+    const int r = q % nb, cc = q / nb;
+    L[cc][r] = A[(k + cc) * lda + (k + r)];
+  }
+  for (int j = tid; j < nb; j += blockDim.x) lp[j] = (int)(ipiv[k + j] - k);
+  __syncthreads();
+  const int64_t nother = n - nb;   // columns outside the diagonal block
+  for (int64_t q = (int64_t)blockIdx.x * kSwapWarps + warp; q < nother; q += (int64_t)gridDim.x * kSwapWarps) {
+    const int64_t c = (q < k) ? q : q + nb;
+    T* colp = A + c * lda + k;
+    for (int r = lane; r < nb; r += 32) col[warp][r] = colp[r];
+    __syncwarp();
+    if (lane == 0) {
+      for (int j = 0; j < nb; ++j) {
+        const int p = lp[j];
+        if (p != j) { const T t0 = col[warp][j]; col[warp][j] = col[warp][p]; col[warp][p] = t0; }
+      }
+    }
+    __syncwarp();
+    if (c >= k + nb) {
+      // forward substitution with the unit lower L11; lanes own rows lane, lane+32
+      T x0 = (lane < nb) ? col[warp][lane] : T(0);
+      T x1 = (lane + 32 < nb) ? col[warp][lane + 32] : T(0);
+      for (int j = 0; j < nb; ++j) {
+        const T xj = __shfl_sync(0xffffffffu, (j < 32) ? x0 : x1, j & 31);
+        if (lane > j) x0 -= L[j][lane] * xj;
+        if (lane + 32 > j && lane + 32 < nb) x1 -= L[j][lane + 32] * xj;
+      }
+      if (lane < nb) col[warp][lane] = x0;
+      if (lane + 32 < nb) col[warp][lane + 32] = x1;
+      __syncwarp();
+    }
+    for (int r = lane; r < nb; r += 32) colp[r] = col[warp][r];
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------------------
+// (3) trailing update C -= A B, SIMT register tiles (FP64 path).
+template <class T, int BM, int BN, int BK, int TM, int TN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ Cm, int64_t lda,
+           int64_t m, int64_t nn, int kk) {
+  constexpr int NT = (BM / TM) * (BN / TN);
+  __shared__ T As[BK][BM + 1];
+  __shared__ T Bs[BK][BN + 1];
+  const int tid = threadIdx.x;
+  const int tx = tid % (BN / TN), ty = tid / (BN / TN);
+  const int64_t i0 = (int64_t)blockIdx.x * BM, j0 = (int64_t)blockIdx.y * BN;
+  T acc[TM][TN];
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TN; ++b) acc[a][b] = T(0);
+  for (int k0 = 0; k0 < kk; k0 += BK) {
+    for (int q = tid; q < BK * BM; q += NT) {
+      const int ii = q % BM, kq = q / BM;
+      const int64_t gi = i0 + ii;
+      As[kq][ii] = (gi < m && k0 + kq < kk) ? Am[(int64_t)(k0 + kq) * lda + gi] : T(0);
+    }
+    for (int q = tid; q < BK * BN; q += NT) {
+      const int kq = q % BK, jj = q / BK;
+      const int64_t gj = j0 + jj;
+      Bs[kq][jj] = (gj < nn && k0 + kq < kk) ? Bm[gj * lda + k0 + kq] : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kq = 0; kq < BK; ++kq) {
+      T a[TM], b[TN];
+#pragma unroll
+      for (int u = 0; u < TM; ++u) a[u] = As[kq][ty + u * (BM / TM)];
+#pragma unroll
+      for (int v = 0; v < TN; ++v) b[v] = Bs[kq][tx + v * (BN / TN)];
+#pragma unroll
+      for (int u = 0; u < TM; ++u)
+#pragma unroll
+        for (int v = 0; v < TN; ++v) acc[u][v] += a[u] * b[v];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < TM; ++u) {
+    const int64_t gi = i0 + ty + u * (BM / TM);
+    if (gi >= m) continue;
+#pragma unroll
+    for (int v = 0; v < TN; ++v) {
+      const int64_t gj = j0 + tx + v * (BN / TN);
+      if (gj < nn) Cm[gj * lda + gi] -= acc[u][v];
+    }
+  }
+}
+
+// FP32 trailing update on tensor cores (fp_tc.cu); returns false if the
+// shape is not supported, in which case the SIMT kernel runs.
+bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
+                     int64_t nn, int kk);
+
+template <class T>
+static int trailing_update(fp_ctx* c, T* A, int64_t lda, int64_t m, int64_t nn, int kk,
+                           int64_t k) {
+  const T* L21 = A + k * lda + (k + kk);
+  const T* U12 = A + (k + kk) * lda + k;
+  T* C = A + (k + kk) * lda + (k + kk);
+  if (sizeof(T) == 4) {
+    if (tc_gemm_sub_f32(c, (const float*)L21, (const float*)U12, (float*)C, lda, m, nn, kk))
+      return FP_OK;
+    constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
+    dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
+    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(L21, U12, C, lda, m, nn, kk);
+    ++c->nlaunch;
+  } else {
+    constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
+    dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
+    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(L21, U12, C, lda, m, nn, kk);
+    ++c->nlaunch;
+  }
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+template <class T>
+int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
+  for (int64_t k = 0; k < n; k += NB) {
+    const int nb = (int)std::min<int64_t>(NB, n - k);
+    const int64_t below = n - k - nb;
+    const unsigned g1 = (unsigned)std::max<int64_t>(1, (below + kPanelThreads - 1) / kPanelThreads);
+    k_panel<T><<<g1, kPanelThreads, 0, c->stream>>>(A, lda, n, k, ipiv, cert, c->d_status);
+    ++c->nlaunch;
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+    if (n - nb > 0) {
+      const int64_t nother = n - nb;
+      const unsigned g2 = (unsigned)std::min<int64_t>((nother + kSwapWarps - 1) / kSwapWarps, 4 * 148);
+      k_swap_u12<T><<<g2, kSwapWarps * 32, 0, c->stream>>>(A, lda, n, k, ipiv);
+      ++c->nlaunch;
+      FP_CUDA_TRY(c->err, cudaGetLastError());
+    }
+    if (below > 0) {
+      int rc = trailing_update<T>(c, A, lda, below, below, nb, k);
+      if (rc) return rc;
+    }
+  }
+  return FP_OK;
+}
+
+// ----------------------------------------------------------------------------
+// Inverses of the diagonal blocks (unit-lower and upper), for the solves.
+// Dinv[b][0] = inv(L_bb), Dinv[b][1] = inv(U_bb), NB x NB column-major each.
+template <class T>
+__global__ void __launch_bounds__(NB)
+k_diag_inv(const T* __restrict__ A, int64_t lda, int64_t n, T* __restrict__ Dinv) {
+  __shared__ T Ls[NB][NB + 1];   // [c][r]
+  const int64_t b = blockIdx.x;
+  const int64_t k = b * NB;
+  const int nb = (int)imin64(NB, n - k);
+  const int t = threadIdx.x;   // column of the inverse
+  for (int q = t; q < NB * NB; q += NB) {
+    const int r = q % NB, cc = q / NB;
+    Ls[cc][r] = (r < nb && cc < nb) ? A[(k + cc) * lda + (k + r)] : ((r == cc) ? T(1) : T(0));
+  }
+  __syncthreads();
+  T* Li = Dinv + b * 2 * NB * NB;
+  T* Ui = Li + NB * NB;
+  // inv(L): column t solves L x = e_t (unit diagonal)
+  {
+    T x[NB];
+#pragma unroll
+    for (int r = 0; r < NB; ++r) x[r] = (r == t) ? T(1) : T(0);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const T xj = x[j];
+#pragma unroll
+      for (int r = j + 1; r < NB; ++r) x[r] -= Ls[j][r] * xj;
+    }
+#pragma unroll
+    for (int r = 0; r < NB; ++r) Li[t * NB + r] = x[r];
+  }
+  // inv(U): column t solves U x = e_t
+  {
+    T x[NB];
+#pragma unroll
+    for (int r = 0; r < NB; ++r) x[r] = (r == t) ? T(1) : T(0);
+#pragma unroll
+    for (int j = NB - 1; j >= 0; --j) {
+      const T xj = x[j] / Ls[j][j];
+      x[j] = xj;
+#pragma unroll
+      for (int r = 0; r < j; ++r) x[r] -= Ls[j][r] * xj;
+    }
+#pragma unroll
+    for (int r = 0; r < NB; ++r) Ui[t * NB + r] = x[r];
+  }
+}
+
+// Row swaps of the block-local pivots on k right-hand sides (forward order),
+// or their inverse (reverse order).
+template <class T>
+__global__ void k_apply_piv(T* __restrict__ B, int64_t ldb, int64_t n, int64_t k,
+                            const int32_t* __restrict__ ipiv, bool reverse) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nblk = (n + NB - 1) / NB;
+  if (t >= nblk * k) return;
+  const int64_t b = t % nblk, q = t / nblk;
+  const int64_t k0 = b * NB;
+  const int nb = (int)imin64(NB, n - k0);
+  T* col = B + q * ldb;
+  if (!reverse) {
+    for (int j = 0; j < nb; ++j) {
+      const int64_t p = ipiv[k0 + j];
+      if (p != k0 + j) { const T a = col[k0 + j]; col[k0 + j] = col[p]; col[p] = a; }
+    }
+  } else {
+    for (int j = nb - 1; j >= 0; --j) {
+      const int64_t p = ipiv[k0 + j];
+      if (p != k0 + j) { const T a = col[k0 + j]; col[k0 + j] = col[p]; col[p] = a; }
+    }
+  }
+}
+
+// Persistent blocked triangular solve (one sweep), KR right-hand sides.
+// LOWER: L y = b (unit lower, forward); else U x = y (upper, backward).
+// The solution overwrites B. flags[b] = 1 once block b is final.
+constexpr int kTrsThreads = 256;
+template <class T, bool LOWER, int KR>
+__global__ void __launch_bounds__(kTrsThreads)
+k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv,
+      T* __restrict__ B, int64_t ldb, unsigned int* __restrict__ flags,
+      unsigned int* __restrict__ ticket, int* __restrict__ status) {
+  __shared__ T acc[KR][NB];
+  __shared__ T y[KR][NB];
+  __shared__ int blk_s;
+  const int64_t nblk = (n + NB - 1) / NB;
+  const int tid = threadIdx.x;
+  const int r = tid % NB;          // row within the block
+  const int qg = tid / NB;         // RHS lane group
+  constexpr int QG = kTrsThreads / NB;
+  for (;;) {
+    if (tid == 0) blk_s = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    const int64_t tk = blk_s;
+    __syncthreads();
+    if (tk >= nblk) return;
+    const int64_t b = LOWER ? tk : nblk - 1 - tk;
+    const int64_t k0 = b * NB;
+    const int nb = (int)imin64(NB, n - k0);
+    for (int q = qg; q < KR; q += QG) acc[q][r] = (r < nb) ? B[q * ldb + k0 + r] : T(0);
+    // dependencies
+    for (int64_t s = 0; s < tk; ++s) {
+      const int64_t cb = LOWER ? s : nblk - 1 - s;
+      const int64_t c0 = cb * NB;
+      const int cn = (int)imin64(NB, n - c0);
+      if (tid == 0) {
+        int spins = 0;
+        while (atomicAdd(&flags[cb], 0u) == 0u) {
+          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); break; }
+          __nanosleep(64);
+        }
+      }
+      __syncthreads();
+      if (atomicOr(status, 0) & (int)DEV_TIMEOUT) return;
+      for (int q = qg; q < KR; q += QG) y[q][r] = (r < cn) ? __ldcg(&B[q * ldb + c0 + r]) : T(0);
+      __syncthreads();
+      if (r < nb) {
+        T s0[KR];
+#pragma unroll
+        for (int q = 0; q < KR; ++q) s0[q] = T(0);
+        // this thread accumulates row r for RHS q = qg, qg+QG, ...
+        for (int l = 0; l < cn; ++l) {
+          const T a = A[(c0 + l) * lda + k0 + r];
+#pragma unroll
+          for (int q = 0; q < KR; ++q)
+            if ((q % QG) == qg) s0[q] += a * y[q][l];
+        }
+#pragma unroll
+        for (int q = 0; q < KR; ++q)
+          if ((q % QG) == qg) acc[q][r] -= s0[q];
+      }
+      __syncthreads();
+    }
+    // x_b = inv(D_bb) acc
+    const T* Di = Dinv + b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
+    if (r < nb) {
+      T s0[KR];
+#pragma unroll
+      for (int q = 0; q < KR; ++q) s0[q] = T(0);
+      for (int l = 0; l < NB; ++l) {
+        const T a = Di[l * NB + r];
+#pragma unroll
+        for (int q = 0; q < KR; ++q)
+          if ((q % QG) == qg) s0[q] += a * acc[q][l];
+      }
+#pragma unroll
+      for (int q = 0; q < KR; ++q)
+        if ((q % QG) == qg) B[q * ldb + k0 + r] = s0[q];
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(&flags[b], 1u);
+  }
+}
+
+template <class T, bool LOWER, int KR>
+static int run_trs(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv, T* B,
+                   int64_t ldb) {
+  const int64_t nblk = (n + NB - 1) / NB;
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
+  const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
+  k_trs<T, LOWER, KR><<<grid, kTrsThreads, 0, c->stream>>>(A, lda, n, Dinv, B, ldb, c->d_flags,
+                                                           c->d_flags + nblk, c->d_status);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+template <class T>
+static int solve_group(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const T* Dinv, T* B,
+                       int64_t ldb, int kr) {
+  int rc;
+#define FP_TRS_CASE(KR)                                                        \
+  case KR:                                                                     \
+    if ((rc = run_trs<T, true, KR>(c, LU, n, lda, Dinv, B, ldb))) return rc;   \
+    return run_trs<T, false, KR>(c, LU, n, lda, Dinv, B, ldb);
+  switch (kr) {
+    FP_TRS_CASE(1)
+    FP_TRS_CASE(2)
+    FP_TRS_CASE(4)
+    FP_TRS_CASE(8)
+  }
+#undef FP_TRS_CASE
+  return c->err.set(FP_EINVAL, "unsupported RHS group");
+}
+
+// Dinv buffer and flags are sized by the caller (fp_capi.cu) for n.
+template <class T>
+int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv, T* B,
+             int64_t ldb, int64_t k, bool transpose) {
+  if (transpose) return c->err.set(FP_EINVAL, "transposed solve not available");
+  const int64_t nblk = (n + NB - 1) / NB;
+  T* Dinv = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_dinv64 : (void*)c->d_dinv32);
+  {
+    const int64_t t = nblk * k;
+    k_apply_piv<T><<<(unsigned)((t + 127) / 128), 128, 0, c->stream>>>(B, ldb, n, k, ipiv, false);
+    ++c->nlaunch;
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+  }
+  for (int64_t q0 = 0; q0 < k;) {
+    const int64_t left = k - q0;
+    const int kr = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+    int rc = solve_group<T>(c, LU, n, lda, Dinv, B + q0 * ldb, ldb, kr);
+    if (rc) return rc;
+    q0 += kr;
+  }
+  return FP_OK;
+}
+
+template <class T>
+int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda) {
+  const int64_t nblk = (n + NB - 1) / NB;
+  T* Dinv = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_dinv64 : (void*)c->d_dinv32);
+  k_diag_inv<T><<<(unsigned)nblk, NB, 0, c->stream>>>(LU, lda, n, Dinv);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+// ----------------------------------------------------------------------------
+// r = b - A x (FP64), k right-hand sides, split over column ranges.
+constexpr int kGemvRows = 128;
+constexpr int kGemvSplit = 16;
+template <int KR>
+__global__ void __launch_bounds__(kGemvRows)
+k_gemv_partial(const double* __restrict__ A, int64_t lda, int64_t n, const double* __restrict__ x,
+               int64_t ldx, double* __restrict__ part) {
+  const int64_t i = (int64_t)blockIdx.x * kGemvRows + threadIdx.x;
+  const int64_t cs = (n + kGemvSplit - 1) / kGemvSplit;
+  const int64_t c0 = blockIdx.y * cs, c1 = imin64(n, c0 + cs);
+  double s[KR];
+#pragma unroll
+  for (int q = 0; q < KR; ++q) s[q] = 0.0;
+  if (i < n) {
+    for (int64_t j = c0; j < c1; ++j) {
+      const double a = A[j * lda + i];
+#pragma unroll
+      for (int q = 0; q < KR; ++q) s[q] += a * __ldg(&x[q * ldx + j]);
+    }
+#pragma unroll
+    for (int q = 0; q < KR; ++q) part[((int64_t)blockIdx.y * KR + q) * n + i] = s[q];
+  }
+}
+
+template <int KR>
+__global__ void k_gemv_finish(const double* __restrict__ part, int64_t n, const double* __restrict__ b,
+                              int64_t ldb, double* __restrict__ r, int64_t ldr) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+#pragma unroll
+  for (int q = 0; q < KR; ++q) {
+    double s = 0.0;
+    for (int p = 0; p < kGemvSplit; ++p) s += part[((int64_t)p * KR + q) * n + i];
+    r[q * ldr + i] = b[q * ldb + i] - s;
+  }
+}
+
+int gemv_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const double* x,
+                  const double* b, double* r, int64_t k) {
+  for (int64_t q0 = 0; q0 < k;) {
+    const int64_t left = k - q0;
+    const int kr = left >= 4 ? 4 : left >= 2 ? 2 : 1;
+    dim3 g((unsigned)((n + kGemvRows - 1) / kGemvRows), kGemvSplit);
+    const unsigned gf = (unsigned)((n + 255) / 256);
+    const double* xq = x + q0 * lda;
+    if (kr == 4) {
+      k_gemv_partial<4><<<g, kGemvRows, 0, c->stream>>>(A, lda, n, xq, lda, c->d_part);
+      ++c->nlaunch;
+      k_gemv_finish<4><<<gf, 256, 0, c->stream>>>(c->d_part, n, b + q0 * lda, lda, r + q0 * lda, lda);
+      ++c->nlaunch;
+    } else if (kr == 2) {
+      k_gemv_partial<2><<<g, kGemvRows, 0, c->stream>>>(A, lda, n, xq, lda, c->d_part);
+      ++c->nlaunch;
+      k_gemv_finish<2><<<gf, 256, 0, c->stream>>>(c->d_part, n, b + q0 * lda, lda, r + q0 * lda, lda);
+      ++c->nlaunch;
+    } else {
+      k_gemv_partial<1><<<g, kGemvRows, 0, c->stream>>>(A, lda, n, xq, lda, c->d_part);
+      ++c->nlaunch;
+      k_gemv_finish<1><<<gf, 256, 0, c->stream>>>(c->d_part, n, b + q0 * lda, lda, r + q0 * lda, lda);
+      ++c->nlaunch;
+    }
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+    q0 += kr;
+  }
+  return FP_OK;
+}
+
+// ----------------------------------------------------------------------------
+__global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, int64_t n,
+                             int64_t k, int64_t lda, int64_t ldb) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * k) return;
+  const int64_t i = t % n, q = t / n;
+  b[q * ldb + i] = (float)a[q * lda + i];
+}
+__global__ void k_axpy_f32(const float* __restrict__ d, double* __restrict__ x, int64_t n,
+                           int64_t k, int64_t ld) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * k) return;
+  const int64_t i = t % n, q = t / n;
+  x[q * ld + i] += (double)d[q * ld + i];
+}
+
+int convert_f64_f32(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda,
+                    int64_t ldb) {
+  const int64_t t = n * k;
+  k_f64_to_f32<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(a, b, n, k, lda, ldb);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+int axpy_f32_to_f64(fp_ctx* c, const float* d, double* x, int64_t n, int64_t k, int64_t ld) {
+  const int64_t t = n * k;
+  k_axpy_f32<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(d, x, n, k, ld);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+// column norms ||a_q||_2^2 for q < k (one CTA per column)
+__global__ void k_colnorm2(const double* __restrict__ a, int64_t n, int64_t lda, double* __restrict__ out) {
+  __shared__ double red[256 / 32];
+  const int64_t q = blockIdx.x;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) { const double v = a[q * lda + i]; s += v * v; }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 256 / 32; ++w) t += red[w];
+    out[q] = t;
+  }
+}
+int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out) {
+  k_colnorm2<<<(unsigned)k, 256, 0, c->stream>>>(a, n, lda, d_out);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+template int lu_factor<double>(fp_ctx*, double*, int64_t, int64_t, int32_t*, float*);
+template int lu_factor<float>(fp_ctx*, float*, int64_t, int64_t, int32_t*, float*);
+template int lu_solve<double>(fp_ctx*, const double*, int64_t, int64_t, const int32_t*, double*, int64_t, int64_t, bool);
+template int lu_solve<float>(fp_ctx*, const float*, int64_t, int64_t, const int32_t*, float*, int64_t, int64_t, bool);
+template int lu_diag_inverses<double>(fp_ctx*, const double*, int64_t, int64_t);
+template int lu_diag_inverses<float>(fp_ctx*, const float*, int64_t, int64_t);
+
+}  // namespace fpb

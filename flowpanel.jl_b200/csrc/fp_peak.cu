@@ -1,0 +1,54 @@
+// Measurement utility: sustained FMA throughput of the FP64 and FP32 pipes,
+// the roofline denominators of the compute-bound assembly and field kernels
+// (the driver's measured peaks cover only HBM copy and the BF16 GEMM).
+#include "fp_internal.cuh"
+
+namespace fpb {
+
+template <class T>
+__global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters, T a, T b) {
+  T x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  const T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == T(-1.2345)) out[0] = s;   // keep the chain alive
+}
+
+}  // namespace fpb
+
+extern "C" int fp_measure_fma_peak(int device, int fp64, double* tflops) {
+  using namespace fpb;
+  if (!tflops) return FP_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return FP_ECUDA;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int blocks = sms * 8, threads = 256, iters = 2048;
+  void* out = nullptr;
+  if (cudaMalloc(&out, 16) != cudaSuccess) return FP_ECUDA;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(e0);
+    if (fp64) k_fma_peak<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+    else k_fma_peak<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (cudaGetLastError() != cudaSuccess) return FP_ECUDA;
+  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return FP_OK;
+}

@@ -1,0 +1,325 @@
+"""Synthetic panel meshes for the benchmark and test workloads.
+
+Meshing stays on the host in FLOWPanel.jl (GeometricTools lofts and
+revolutions, src/FLOWPanel_abstractliftingbody.jl:73-176,
+src/FLOWPanel_utils.jl:68-150). These generators produce the same kind of
+structured surface meshes directly, in the flat layout the C ABI takes:
+
+* ``nodes``          (nnodes, 3) float64  == Julia's 3 x nnodes column-major;
+* ``panel_offsets``  (npanels+1,) int32, ``panel_nodes`` int32, 0-based (CSR);
+* ``shedding``       (nsh, 6) int32 rows (pi, nia, nib, pj, nja, njb), 0-based,
+  nia/nib/nja/njb local to the panel, pj == -1 for no lower side
+  (the 6 x nsh matrix of src/FLOWPanel_liftingbody.jl:24-31).
+
+Panel node order makes ``(p2-p1) x (p3-p1)`` point out of the body, so every
+body here uses a positive ``CPoffset``. Wing contours run from the upper
+trailing edge over the leading edge to the lower trailing edge, chordwise index
+fastest, so the reference's Kutta average over (pi, pi+1, pj, pj-1)
+(src/FLOWPanel_postprocess.jl:1075-1097) averages the two panels on each side
+of the trailing edge.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List
+
+import numpy as np
+
+
+@dataclass
+class Body:
+    name: str
+    kind: str            # "source" | "vortexring"
+    ncells: int
+    nsheddings: int
+    CPoffset: float = 1e-14
+    kerneloffset: float = 1e-8
+    kernelcutoff: float = 1e-14
+
+
+@dataclass
+class Mesh:
+    nodes: np.ndarray
+    panel_offsets: np.ndarray
+    panel_nodes: np.ndarray
+    shedding: np.ndarray = field(default_factory=lambda: np.zeros((0, 6), np.int32))
+    bodies: List[Body] = field(default_factory=list)
+
+    @property
+    def npanels(self) -> int:
+        return len(self.panel_offsets) - 1
+
+    @property
+    def nnodes(self) -> int:
+        return self.nodes.shape[0]
+
+    @property
+    def nsheddings(self) -> int:
+        return int(self.shedding.shape[0])
+
+    def panel(self, i):
+        return self.panel_nodes[self.panel_offsets[i]:self.panel_offsets[i + 1]]
+
+    def cpoffset_sign(self):
+        """Per-panel sign(CPoffset) (MultiBody rule, src/FLOWPanel_multibody.jl:664-676)."""
+        s = np.empty(self.npanels)
+        k = 0
+        for b in self.bodies:
+            s[k:k + b.ncells] = np.sign(b.CPoffset) if b.CPoffset != 0 else 1.0
+            k += b.ncells
+        return s
+
+    def cpoffset(self):
+        s = np.empty(self.npanels)
+        k = 0
+        for b in self.bodies:
+            s[k:k + b.ncells] = b.CPoffset
+            k += b.ncells
+        return s
+
+
+def concat(meshes: List[Mesh]) -> Mesh:
+    """MultiBody: concatenate bodies; G's column blocks follow body order
+    (src/FLOWPanel_multibody.jl:502-530)."""
+    nodes, offs, pn, sh, bodies = [], [0], [], [], []
+    noff, poff = 0, 0
+    for m in meshes:
+        nodes.append(m.nodes)
+        pn.append(m.panel_nodes + noff)
+        offs.extend((m.panel_offsets[1:] + offs[-1]).tolist())
+        s = m.shedding.copy()
+        if len(s):
+            s[:, 0] += poff
+            s[:, 3] = np.where(s[:, 3] >= 0, s[:, 3] + poff, -1)
+        sh.append(s)
+        bodies.extend(m.bodies)
+        noff += m.nnodes
+        poff += m.npanels
+    return Mesh(np.concatenate(nodes), np.asarray(offs, np.int32), np.concatenate(pn).astype(np.int32),
+                np.concatenate(sh).astype(np.int32) if sh else np.zeros((0, 6), np.int32), bodies)
+
+
+def _quad_grid(P, drop_degenerate=True, tol=1e-14):
+    """Quads of a structured (ni+1) x (nj+1) node grid P[i, j] (contour i, span j).
+    Panel (i, j) = [n(i,j), n(i,j+1), n(i+1,j+1), n(i+1,j)]; coincident
+    consecutive nodes (poles) are dropped so that such panels become triangles."""
+    ni, nj = P.shape[0] - 1, P.shape[1] - 1
+    nodes = P.reshape(-1, 3)
+    idx = np.arange((ni + 1) * (nj + 1)).reshape(ni + 1, nj + 1)
+    offs, pn = [0], []
+    for j in range(nj):
+        for i in range(ni):
+            q = [idx[i, j], idx[i, j + 1], idx[i + 1, j + 1], idx[i + 1, j]]
+            if drop_degenerate:
+                keep = []
+                for k in range(4):
+                    a, b = q[k], q[(k + 1) % 4]
+                    if np.linalg.norm(nodes[a] - nodes[b]) > tol:
+                        keep.append(a)
+                q = keep
+            pn.extend(q)
+            offs.append(len(pn))
+    return nodes.copy(), np.asarray(offs, np.int32), np.asarray(pn, np.int32)
+
+
+# ------------------------------------------------------------------ sphere
+def sphere(R=1.0, ntheta=30, nphi=60, CPoffset=1e-14):
+    """Body of revolution: sphere of radius R centred at the origin, polar axis z;
+    ntheta polar x nphi azimuthal cells (pole rows are triangles). Constant-source
+    body as in examples/sphere.jl."""
+    th = np.linspace(0.0, np.pi, ntheta + 1)
+    ph = np.linspace(0.0, 2 * np.pi, nphi + 1)
+    T, PH = np.meshgrid(th, ph, indexing="ij")
+    P = np.stack([R * np.sin(T) * np.cos(PH), R * np.sin(T) * np.sin(PH), R * np.cos(T)], axis=-1)
+    P[0, :] = [0, 0, R]
+    P[-1, :] = [0, 0, -R]
+    P[:, -1] = P[:, 0]
+    # contour i along theta, "span" j along phi: (p2-p1) x (p3-p1) ~ e_phi x e_theta = -e_r,
+    # so reverse phi to point outwards.
+    P = P[:, ::-1].copy()
+    nodes, offs, pn = _quad_grid(P)
+    m = Mesh(nodes, offs, pn)
+    m.bodies = [Body("sphere", "source", m.npanels, 0, CPoffset)]
+    return m
+
+
+def triangulate(m: Mesh) -> Mesh:
+    """Split every quad into two triangles along its first diagonal (the
+    reference always meshes structured grids as triangles,
+    src/FLOWPanel_nonliftingbody.jl:834,855). Shedding rows are re-mapped to
+    the triangle that keeps the trailing-edge edge."""
+    offs, pn, newidx = [0], [], []
+    for i in range(m.npanels):
+        p = list(m.panel(i))
+        if len(p) == 4:
+            newidx.append(len(offs) - 1)
+            pn.extend([p[0], p[1], p[2]]); offs.append(len(pn))
+            pn.extend([p[0], p[2], p[3]]); offs.append(len(pn))
+        else:
+            newidx.append(len(offs) - 1)
+            pn.extend(p); offs.append(len(pn))
+    sh = []
+    for (pi, nia, nib, pj, nja, njb) in m.shedding:
+        def remap(pp, a, b):
+            p = list(m.panel(pp))
+            ga, gb = p[a], p[b]
+            base = newidx[pp]
+            for t in (base, base + 1):
+                tri = pn[offs[t]:offs[t + 1]]
+                if ga in tri and gb in tri:
+                    return t, tri.index(ga), tri.index(gb)
+            raise ValueError("edge lost in triangulation")
+        ti, ta, tb = remap(pi, nia, nib)
+        if pj >= 0:
+            tj, tc, td = remap(pj, nja, njb)
+        else:
+            tj, tc, td = -1, 0, 0
+        sh.append((ti, ta, tb, tj, tc, td))
+    out = Mesh(m.nodes.copy(), np.asarray(offs, np.int32), np.asarray(pn, np.int32),
+               np.asarray(sh, np.int32).reshape(-1, 6))
+    out.bodies = [Body(b.name, b.kind, 0, b.nsheddings, b.CPoffset, b.kerneloffset, b.kernelcutoff)
+                  for b in m.bodies]
+    # recount cells per body
+    k = 0
+    for b, ob in zip(out.bodies, m.bodies):
+        b.ncells = sum(2 if len(m.panel(i)) == 4 else 1 for i in range(k, k + ob.ncells))
+        k += ob.ncells
+    return out
+
+
+# ------------------------------------------------------------------ airfoils and wings
+def naca4_contour(code="0012", n_half=50, closed_te=True):
+    """NACA 4-digit section with cosine spacing, as a closed contour from the
+    upper trailing edge over the leading edge to the lower trailing edge;
+    returns (2*n_half+1, 2) points (x, z) on a unit chord."""
+    m = int(code[0]) / 100.0
+    p = int(code[1]) / 10.0
+    t = int(code[2:]) / 100.0
+    k = np.arange(n_half + 1)
+    x = 0.5 * (1 - np.cos(np.pi * k / n_half))          # LE -> TE
+    a4 = -0.1036 if closed_te else -0.1015
+    yt = 5 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 + a4 * x ** 4)
+    if m > 0:
+        yc = np.where(x < p, m / p ** 2 * (2 * p * x - x ** 2), m / (1 - p) ** 2 * ((1 - 2 * p) + 2 * p * x - x ** 2))
+        dyc = np.where(x < p, 2 * m / p ** 2 * (p - x), 2 * m / (1 - p) ** 2 * (p - x))
+    else:
+        yc = np.zeros_like(x)
+        dyc = np.zeros_like(x)
+    th = np.arctan(dyc)
+    xu, zu = x - yt * np.sin(th), yc + yt * np.cos(th)
+    xl, zl = x + yt * np.sin(th), yc - yt * np.cos(th)
+    if closed_te:
+        zu[-1] = zl[-1] = yc[-1]
+        xu[-1] = xl[-1] = 1.0
+    upper = np.stack([xu[::-1], zu[::-1]], axis=1)       # TE -> LE
+    lower = np.stack([xl[1:], zl[1:]], axis=1)           # LE(excl) -> TE
+    return np.concatenate([upper, lower])
+
+
+def wing_half(contour, y0, y1, nspan, chord0, chord1, xle0, xle1, twist0=0.0, twist1=0.0,
+              zle0=0.0, zle1=0.0, name="wing", CPoffset=1e-14):
+    """Loft one wing panel between spanwise stations y0 < y1 (linear
+    interpolation of chord, leading-edge position and twist about the quarter
+    chord). Returns a lifting Mesh with one shedding edge per spanwise strip."""
+    nc = contour.shape[0] - 1
+    ys = np.linspace(y0, y1, nspan + 1)
+    s = (ys - y0) / (y1 - y0)
+    P = np.zeros((nc + 1, nspan + 1, 3))
+    for j, sj in enumerate(s):
+        c = chord0 + (chord1 - chord0) * sj
+        xle = xle0 + (xle1 - xle0) * sj
+        zle = zle0 + (zle1 - zle0) * sj
+        tw = np.deg2rad(twist0 + (twist1 - twist0) * sj)
+        xc = (contour[:, 0] - 0.25) * c
+        zc = contour[:, 1] * c
+        xr = xc * np.cos(tw) + zc * np.sin(tw)
+        zr = -xc * np.sin(tw) + zc * np.cos(tw)
+        P[:, j, 0] = xle + 0.25 * c + xr
+        P[:, j, 1] = ys[j]
+        P[:, j, 2] = zle + zr
+    nodes, offs, pn = _quad_grid(P, drop_degenerate=False)
+    sh = np.zeros((nspan, 6), np.int32)
+    for j in range(nspan):
+        sh[j] = (j * nc + 0, 1, 0, j * nc + nc - 1, 3, 2)
+    m = Mesh(nodes, offs, pn, sh)
+    m.bodies = [Body(name, "vortexring", m.npanels, nspan, CPoffset)]
+    return m
+
+
+def swept_wing(naca="0012", n_chord=100, n_span=120, chord=1.0, b=5.0, sweep=45.0, taper=1.0,
+               twist_root=0.0, twist_tip=0.0):
+    """Swept wing as a MultiBody of two halves lofted from the root outwards on
+    each side (the practice of examples/sweptwing.jl:88-130). ``n_chord`` cells
+    around the section, ``n_span`` cells over the whole span. Root chord
+    ``chord``, tip chord ``chord*taper``, aspect ratio b/c_tip."""
+    assert n_chord % 2 == 0 and n_span % 2 == 0
+    cont = naca4_contour(naca, n_chord // 2)
+    tl = np.tan(np.deg2rad(sweep))
+    half = b / 2
+    ct = chord * taper
+    left = wing_half(cont, -half, 0.0, n_span // 2, ct, chord, half * tl, 0.0, twist_tip, twist_root, name="L")
+    right = wing_half(cont, 0.0, half, n_span // 2, chord, ct, 0.0, half * tl, twist_root, twist_tip, name="R")
+    return concat([left, right])
+
+
+def random_wings(n=64, seed=0, pmin=2000, pmax=8000):
+    """Batch of wings drawn from ``numpy.random.default_rng(seed)``: sweep U[0,45] deg,
+    aspect ratio U[4,10], taper U[0.3,1], linear twist U[-4,0] deg at the tip,
+    chordwise cells U{40..80} (even), spanwise U{50..100} (even); draws outside
+    [pmin, pmax] panels are rejected. Draw order: sweep, AR, taper, twist, nc, ns."""
+    rng = np.random.default_rng(seed)
+    out, params = [], []
+    while len(out) < n:
+        sweep = rng.uniform(0, 45)
+        ar = rng.uniform(4, 10)
+        taper = rng.uniform(0.3, 1)
+        twist = rng.uniform(-4, 0)
+        nc = 2 * int(rng.integers(20, 41))
+        ns = 2 * int(rng.integers(25, 51))
+        if not (pmin <= nc * ns <= pmax):
+            continue
+        ct = 1.0 * taper
+        b = ar * ct
+        out.append(swept_wing("0012", nc, ns, 1.0, b, sweep, taper, 0.0, twist))
+        params.append(dict(sweep=sweep, ar=ar, taper=taper, twist=twist, n_chord=nc, n_span=ns, b=b))
+    return out, params
+
+
+def prolate_ellipsoid(L=10.0, rmax=0.6, nx=120, ntheta=80, tail=0.9):
+    """Fuselage: prolate ellipsoid along x with semi-axes (L/2, rmax, rmax),
+    nx axial x ntheta circumferential cells, polar angle from the nose up to
+    ``tail*pi``. The tail is left open: a closed vortex-ring surface makes the
+    direct vortex-ring system singular (src/FLOWPanel_liftingbody.jl:86-91),
+    an open base keeps it well posed. The nose row is triangles."""
+    th = np.linspace(0.0, tail * np.pi, nx + 1)
+    ph = np.linspace(0.0, 2 * np.pi, ntheta + 1)
+    T, PH = np.meshgrid(th, ph, indexing="ij")
+    a = L / 2
+    P = np.stack([a * np.cos(T), rmax * np.sin(T) * np.cos(PH), rmax * np.sin(T) * np.sin(PH)], axis=-1)
+    P[0, :] = [a, 0, 0]
+    P[:, -1] = P[:, 0]
+    nodes, offs, pn = _quad_grid(P)
+    k = nx // 2                                   # a mid-body panel of the first strip
+    p = nodes[pn[offs[k]:offs[k + 1]]]
+    n = np.cross(p[1] - p[0], p[2] - p[0])
+    c = p.mean(axis=0)
+    if np.dot(n, c - np.array([c[0], 0.0, 0.0])) < 0:
+        P = P[:, ::-1].copy()
+        nodes, offs, pn = _quad_grid(P)
+    m = Mesh(nodes, offs, pn)
+    m.bodies = [Body("fuselage", "vortexring", m.npanels, 0)]
+    return m
+
+
+def wing_body(fuse_nx=120, fuse_nt=80, wing_nc=150, wing_ns=180, AR=8.0, taper=0.4,
+              sweep=40.0, croot=1.5):
+    """Wing-body: prolate ellipsoid fuselage (L=10 m, r=0.6 m) and a swept NACA 2412
+    wing (AR = b^2/S with S = b (croot+ctip)/2) whose root sections sit inside
+    the fuselage at y = +-0 (no intersection meshing)."""
+    fuse = prolate_ellipsoid(10.0, 0.6, fuse_nx, fuse_nt)
+    ct = croot * taper
+    b = AR * (croot + ct) / 2
+    wing = swept_wing("2412", wing_nc, wing_ns, croot, b, sweep, taper)
+    # place the wing root quarter chord near the fuselage mid-length, low wing
+    wing.nodes = wing.nodes + np.array([-1.0, 0.0, -0.2])
+    return concat([fuse, wing])

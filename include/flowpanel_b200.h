@@ -1,0 +1,166 @@
+/*
+ * flowpanel_b200.h — C ABI of the B200 (sm_100a) panel-method hot path.
+ *
+ * Drop-in boundary for FLOWPanel.jl's dense solve path: a Julia solver object
+ * calls these entry points through `ccall`; the Python
+ * host mirror in flowpanel.jl_b200/ calls them through ctypes.
+ *
+ * Conventions (Julia's column-major layouts, passed zero-copy):
+ *   nodes       3 x nnodes  double   (x0,y0,z0,x1,...)
+ *   panels      CSR: panel_offsets[npanels+1], panel_nodes[] 0-based node
+ *               indices, 3 or 4 nodes per panel (planar)
+ *   cps/normals 3 x npanels double (control points and unit normals)
+ *   shedding    6 x nsh int32: (pi, nia, nib, pj, nja, njb), 0-based panel
+ *               index and panel-local node indices, pj == -1 for no lower side
+ *   Das/Dbs     3 x nsh double, unit vectors
+ *   G           N x N column-major (column j = unit-strength influence of
+ *               panel j on every control point)
+ * All host buffers belong to the caller and are read (or, for outputs,
+ * written) during the call only. Device memory belongs to the context.
+ * Every entry point returns FP_OK (0) or an FP_E* status; fp_last_error()
+ * gives the text. Calls on one context are serialised by the caller; separate
+ * contexts may run concurrently.
+ */
+#ifndef FLOWPANEL_B200_H
+#define FLOWPANEL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FP_OK 0
+#define FP_EINVAL 1      /* bad argument (shape, non-unit direction, ...) */
+#define FP_ESINGULAR 2   /* zero pivot in the factorisation */
+#define FP_ENOCONV 3     /* iterative solver did not reach its tolerance */
+#define FP_ECUDA 4       /* CUDA runtime error */
+#define FP_ETIMEOUT 5    /* a bounded device-side wait ran out */
+#define FP_ESTATE 6      /* call out of order (e.g. solve before factor) */
+
+/* element kinds */
+#define FP_ELEMENT_SOURCE 0      /* NonLiftingBody{ConstantSource} */
+#define FP_ELEMENT_VORTEXRING 1  /* RigidWakeBody / MultiBody {VortexRing} */
+
+/* precision forms */
+#define FP_PREC_FP64 0   /* FP64 assembly + FP64 LU (the plain form) */
+#define FP_PREC_MIXED 1  /* FP32 factor (3xTF32 tensor-core update) + FP64 refinement */
+
+/* solvers */
+#define FP_SOLVER_LU 0     /* solve_ludiv! / solve_backslash! */
+#define FP_SOLVER_GMRES 1  /* solve_gmres! (restarted GMRES on the FP64 AIC) */
+
+typedef struct fp_ctx fp_ctx;
+
+typedef struct fp_solve_opts {
+  int solver;          /* FP_SOLVER_* */
+  int precision;       /* FP_PREC_*; for FP_SOLVER_LU the factor precision */
+  double ir_tol;       /* mixed: stop refining when ||b-Ax||_2 <= ir_tol*||b||_2 (<=0: 1e-12) */
+  int ir_maxiter;      /* mixed: refinement steps before GMRES-IR takes over (<=0: 10) */
+  int gmres_memory;    /* restart length (<=0: 50) */
+  double gmres_atol;   /* <0: sqrt(eps) */
+  double gmres_rtol;   /* <0: sqrt(eps) */
+  int gmres_itmax;     /* <=0: 2N */
+} fp_solve_opts;
+
+typedef struct fp_stats {
+  double ms_assemble;  /* device time of the last fp_assemble */
+  double ms_factor;    /* device time of the last fp_factor */
+  double ms_solve;     /* device time of the last fp_solve */
+  int ir_iters;        /* refinement steps of the last mixed solve */
+  int gmres_iters;     /* GMRES iterations of the last solve (all RHS) */
+  int used_gmres;      /* 1 if GMRES(-IR) produced the last solution */
+  int gepp_certified;  /* 1 if every pivot equals LAPACK dgetrf's choice */
+  double max_abs_L;    /* largest |L| entry below the diagonal blocks */
+  double rel_residual; /* max over RHS of ||b-Ax||_2/||b||_2 (FP64) */
+} fp_stats;
+
+/* Context: one CUDA device, one stream. Replaces the per-solve allocations of
+ * src/FLOWPanel_liftingbody.jl:191-199 (G = zeros(T, N, N), Gamma = zeros). */
+int fp_ctx_create(int device, fp_ctx** ctx);
+int fp_ctx_destroy(fp_ctx* ctx);
+const char* fp_last_error(const fp_ctx* ctx);
+/* 1 if the library was built with the sm_100a kernels and a device is usable */
+int fp_device_count(void);
+
+/* Geometry of the body (or the concatenated bodies of a MultiBody, in body
+ * order, src/FLOWPanel_multibody.jl:502-530). cps/normals are the ones
+ * _calc_controlpoints!/_calc_normals! produce (src/FLOWPanel_abstractbody.jl:635-755);
+ * NULL asks the library to compute them with off = cp_offset[i] * l = 1
+ * (pass cp_offset = NULL for the default 1e-14). */
+int fp_set_geometry(fp_ctx* ctx, const double* nodes, int64_t nnodes,
+                    const int32_t* panel_offsets, const int32_t* panel_nodes,
+                    int64_t npanels, const double* cps, const double* normals,
+                    const double* cp_offset);
+
+/* Kutta wake: the shedding matrix and the semi-infinite directions
+ * (src/FLOWPanel_liftingbody.jl:508-567, inputs of _G_Uvortexring!).
+ * Non-unit directions -> FP_EINVAL (src/FLOWPanel_elements.jl:495-498). */
+int fp_set_wake(fp_ctx* ctx, const int32_t* shedding, int64_t nsh, const double* Das,
+                const double* Dbs);
+
+/* Dense AIC assembly G = _G_U!(...): constant source
+ * (src/FLOWPanel_nonliftingbody.jl:141-186) or vortex rings plus the Kutta wake
+ * columns (src/FLOWPanel_liftingbody.jl:455-572). Always FP64 in HBM; with
+ * FP_PREC_MIXED an FP32 copy for the factorisation is written by the same pass. */
+int fp_assemble(fp_ctx* ctx, int element, double kerneloffset, double kernelcutoff,
+                int precision);
+
+/* Copy the assembled FP64 AIC to the host (N x N column-major). */
+int fp_get_aic(fp_ctx* ctx, double* G);
+
+/* Right-hand sides calc_bc_noflowthrough!: RHS_i = -Uinf_i . n_i
+ * (src/FLOWPanel_linearsolver.jl:297-312). Uinfs is 3 x N x k. */
+int fp_set_rhs(fp_ctx* ctx, const double* Uinfs, int64_t k);
+
+/* LU factorisation calc_Alu / LA.lu! (src/FLOWPanel_linearsolver.jl:173-234). */
+int fp_factor(fp_ctx* ctx, int precision);
+
+/* Solve for the k right-hand sides set by fp_set_rhs: solve_ludiv! /
+ * solve_backslash! / solve_gmres! (src/FLOWPanel_linearsolver.jl:24-157).
+ * x is N x k (column-major) on the host. opts may be NULL (LU, FP64). */
+int fp_solve(fp_ctx* ctx, double* x, int64_t k, const fp_solve_opts* opts, fp_stats* stats);
+
+/* End-to-end solve(body, Uinfs, Das, Dbs; solver) for a body already given by
+ * fp_set_geometry/fp_set_wake: assemble + RHS + factor + solve
+ * (src/FLOWPanel_liftingbody.jl:172-216, src/FLOWPanel_multibody.jl:312-364,
+ * src/FLOWPanel_nonliftingbody.jl:93-130). */
+int fp_solve_body(fp_ctx* ctx, int element, double kerneloffset, double kernelcutoff,
+                  const double* Uinfs, int64_t k, const fp_solve_opts* opts, double* x,
+                  fp_stats* stats);
+
+/* Induced velocity Uind! of the solved body on m targets, accumulated into
+ * out (3 x m): vortex rings + wake horseshoes with (Gamma_pi, Gamma_pj)
+ * (src/FLOWPanel_liftingbody.jl:576-661) or constant sources
+ * (src/FLOWPanel_nonliftingbody.jl:188-218), with the body's kerneloffset and
+ * kernelcutoff. precision FP_PREC_MIXED evaluates in FP32 (off-body probes). */
+int fp_uind(fp_ctx* ctx, int element, const double* strengths, const double* targets,
+            int64_t m, double* out, int precision, double kerneloffset, double kernelcutoff);
+
+/* Adjoint of the linear solve: A^T lambda = ybar with the saved factors (the
+ * reverse rule of IAD.implicit_linear at src/FLOWPanel_linearsolver.jl:73:
+ * lambda = A^-T ybar, Abar = -lambda x^T, bbar = lambda). ybar/lambda N x k. */
+int fp_adjoint_solve(fp_ctx* ctx, const double* ybar, int64_t k, double* lambda);
+
+/* Time of the last kernel launches, for the benchmark's roofline: the device
+ * time (ms) of the named stage's dominant kernel and its launch count. */
+int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
+#define FP_STAGE_ASSEMBLE 0
+#define FP_STAGE_FACTOR 1
+#define FP_STAGE_SOLVE 2
+#define FP_STAGE_UIND 3
+
+/* Measurement utility (no counterpart in the reference): sustained FMA
+ * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, in
+ * TFLOP/s, the denominator of the compute-bound kernels' roofline. */
+int fp_measure_fma_peak(int device, int fp64, double* tflops);
+
+/* Measurement utility (no counterpart in the reference): number of CUDA kernels
+ * this context has launched since it was created. */
+int fp_kernel_launches(fp_ctx* ctx, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLOWPANEL_B200_H */

@@ -1,0 +1,375 @@
+"""ORACLE — test infrastructure only.
+
+Python face of the CPU restatement of FLOWPanel.jl's panel-method hot path
+(``fp_oracle.hpp``). Only the tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` may import this module, and only as the
+checker: the product path is the CUDA library and never routes through here.
+
+* element kernels, geometry, assembly and induced velocity: the C++ restatement
+  (``_build/libfporacle.so``), bit-faithful to the reference's operation order;
+* LU / ``ldiv!``: LAPACK ``dgetrf``/``dgetrs`` through scipy, the routine family
+  Julia's ``LinearAlgebra.lu!`` calls (src/FLOWPanel_linearsolver.jl:57-78,173-234);
+* GMRES: a restatement of Krylov.jl's restarted GMRES with the reference's
+  defaults (memory=50, atol=rtol=sqrt(eps)) (src/FLOWPanel_linearsolver.jl:136-147);
+* post-processing Cp / F / LDS: src/FLOWPanel_postprocess.jl:1059-1689.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libfporacle.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def build():
+    """Compile the restatement with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.fpo_opcount.restype = C.c_longlong
+        for name in ("fpo_U_semiinfinite_vortex", "fpo_U_semiinfinite_horseshoe",
+                     "fpo_phi_semiinfinite_doublet", "fpo_phi_semiinfinite_doublet2",
+                     "fpo_assemble_vortexring", "fpo_uind_vortexring"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _pts(a):
+    """(n,3) float64 C-contiguous == 3 x n column-major."""
+    a = _f64(a)
+    assert a.ndim == 2 and a.shape[1] == 3
+    return a
+
+
+# ----------------------------------------------------------------- elements
+def U_constant_source(nodes, panel, strength, targets, dot_with=None, offset=1e-8):
+    nodes, targets = _pts(nodes), _pts(targets)
+    panel = _i32(panel)
+    nt = targets.shape[0]
+    out = np.zeros(nt if dot_with is not None else (nt, 3))
+    dw = _pts(dot_with) if dot_with is not None else None
+    lib().fpo_U_constant_source(_d(nodes), _i(panel), len(panel), C.c_double(strength), _d(targets),
+                                C.c_longlong(nt), _d(out), _d(dw) if dw is not None else None,
+                                C.c_double(offset))
+    return out
+
+
+def phi_constant_source(nodes, panel, strength, targets, offset=1e-8):
+    nodes, targets = _pts(nodes), _pts(targets)
+    panel = _i32(panel)
+    out = np.zeros(targets.shape[0])
+    lib().fpo_phi_constant_source(_d(nodes), _i(panel), len(panel), C.c_double(strength), _d(targets),
+                                  C.c_longlong(len(out)), _d(out), C.c_double(offset))
+    return out
+
+
+def U_vortexring(nodes, panel, strength, targets, dot_with=None, cutoff=1e-14, offset=1e-8):
+    nodes, targets = _pts(nodes), _pts(targets)
+    panel = _i32(panel)
+    nt = targets.shape[0]
+    out = np.zeros(nt if dot_with is not None else (nt, 3))
+    dw = _pts(dot_with) if dot_with is not None else None
+    lib().fpo_U_vortexring(_d(nodes), _i(panel), len(panel), C.c_double(strength), _d(targets),
+                           C.c_longlong(nt), _d(out), _d(dw) if dw is not None else None,
+                           C.c_double(cutoff), C.c_double(offset))
+    return out
+
+
+def phi_constant_doublet(nodes, panel, strength, targets):
+    nodes, targets = _pts(nodes), _pts(targets)
+    panel = _i32(panel)
+    out = np.zeros(targets.shape[0])
+    lib().fpo_phi_constant_doublet(_d(nodes), _i(panel), len(panel), C.c_double(strength), _d(targets),
+                                   C.c_longlong(len(out)), _d(out))
+    return out
+
+
+def U_semiinfinite_horseshoe(nodes, TE, da, db, strength, targets, dot_with=None,
+                             cutoff=1e-14, offset=1e-8):
+    nodes, targets = _pts(nodes), _pts(targets)
+    nt = targets.shape[0]
+    out = np.zeros(nt if dot_with is not None else (nt, 3))
+    dw = _pts(dot_with) if dot_with is not None else None
+    rc = lib().fpo_U_semiinfinite_horseshoe(_d(nodes), int(TE[0]), int(TE[1]), _d(_f64(da)), _d(_f64(db)),
+                                            C.c_double(strength), _d(targets), C.c_longlong(nt), _d(out),
+                                            _d(dw) if dw is not None else None, C.c_double(cutoff),
+                                            C.c_double(offset))
+    if rc:
+        raise ValueError("Found non-unitary semi-infinite direction")
+    return out
+
+
+def phi_semiinfinite_doublet(nodes, TE, d, strength, targets, db=None, infinitelength=1e12):
+    nodes, targets = _pts(nodes), _pts(targets)
+    out = np.zeros(targets.shape[0])
+    if db is None:
+        rc = lib().fpo_phi_semiinfinite_doublet(_d(nodes), int(TE[0]), int(TE[1]), _d(_f64(d)),
+                                                C.c_double(strength), _d(targets),
+                                                C.c_longlong(len(out)), _d(out))
+    else:
+        rc = lib().fpo_phi_semiinfinite_doublet2(_d(nodes), int(TE[0]), int(TE[1]), _d(_f64(d)),
+                                                 _d(_f64(db)), C.c_double(strength), _d(targets),
+                                                 C.c_longlong(len(out)), _d(out),
+                                                 C.c_double(infinitelength))
+    if rc:
+        raise ValueError("Invalid semi-infinite direction(s)")
+    return out
+
+
+def grad_phi(kind, nodes, panel, strength, X, d=(1.0, 0.0, 0.0), offset=0.0):
+    """grad(phi) at X by forward-mode duals. kind: 'source' | 'doublet' | 'semiinfinite'."""
+    k = {"source": 0, "doublet": 1, "semiinfinite": 2}[kind]
+    nodes = _pts(nodes)
+    panel = _i32(panel)
+    g = np.zeros(3)
+    lib().fpo_grad_phi(k, _d(nodes), nodes.shape[0], _i(panel), len(panel), _d(_f64(d)),
+                       C.c_double(strength), _d(_f64(X)), C.c_double(offset), _d(g))
+    return g
+
+
+def jac_U(kind, nodes, panel, strength, X, d=(1.0, 0.0, 0.0), cutoff=0.0, offset=0.0):
+    """(U, dU_i/dX_j) at X by forward-mode duals. kind: 'source' | 'ring' | 'horseshoe'."""
+    k = {"source": 0, "ring": 1, "horseshoe": 2}[kind]
+    nodes = _pts(nodes)
+    panel = _i32(panel)
+    U = np.zeros(3)
+    J = np.zeros(9)
+    lib().fpo_jac_U(k, _d(nodes), nodes.shape[0], _i(panel), len(panel), _d(_f64(d)),
+                    C.c_double(strength), _d(_f64(X)), C.c_double(cutoff), C.c_double(offset),
+                    _d(U), _d(J))
+    return U, J.reshape(3, 3)
+
+
+def opcount(which, nn=4):
+    """Operations per interaction as written in the reference (see fpo_opcount)."""
+    k = {"filament": 0, "ring": 1, "semiinfinite": 2, "horseshoe": 3, "source": 4}[which]
+    return int(lib().fpo_opcount(k, nn))
+
+
+# ----------------------------------------------------------------- geometry
+def geometry(mesh, off=None, l=None):
+    """Normals, control points and areas of every panel.
+
+    ``off``/``l`` per panel (CPoffset with the MultiBody sign rule already applied,
+    and the characteristic length)."""
+    npan = mesh.npanels
+    nodes = _pts(mesh.nodes)
+    offs, pn = _i32(mesh.panel_offsets), _i32(mesh.panel_nodes)
+    off = _f64(np.broadcast_to(0.0 if off is None else off, (npan,)))
+    l = _f64(np.broadcast_to(1.0 if l is None else l, (npan,)))
+    normals = np.zeros((npan, 3))
+    cps = np.zeros((npan, 3))
+    areas = np.zeros(npan)
+    lib().fpo_geometry(_d(nodes), _i(offs), _i(pn), C.c_longlong(npan), _d(off), _d(l),
+                       _d(normals), _d(cps), _d(areas))
+    return normals, cps, areas
+
+
+# ----------------------------------------------------------------- assembly
+def assemble_vortexring(mesh, cps, normals, Das, Dbs, offset=1e-8, cutoff=1e-14, nthreads=0):
+    """Dense vortex-ring AIC with Kutta wake columns; returns G (ncp x npanels, Fortran order)."""
+    cps, normals = _pts(cps), _pts(normals)
+    ncp = cps.shape[0]
+    G = np.zeros((ncp, mesh.npanels), order="F")
+    sh = _i32(mesh.shedding.reshape(-1, 6)) if mesh.nsheddings else np.zeros((0, 6), np.int32)
+    Das, Dbs = _pts(np.reshape(Das, (-1, 3))), _pts(np.reshape(Dbs, (-1, 3)))
+    rc = lib().fpo_assemble_vortexring(_d(_pts(mesh.nodes)), _i(_i32(mesh.panel_offsets)),
+                                       _i(_i32(mesh.panel_nodes)), C.c_longlong(mesh.npanels),
+                                       _d(cps), _d(normals), C.c_longlong(ncp), _i(sh),
+                                       C.c_longlong(len(sh)), _d(Das), _d(Dbs),
+                                       C.c_double(offset), C.c_double(cutoff),
+                                       G.ctypes.data_as(_dp), nthreads)
+    if rc:
+        raise ValueError("Found non-unitary semi-infinite direction")
+    return G
+
+
+def assemble_source(mesh, cps, normals, offset=1e-8, nthreads=0):
+    cps, normals = _pts(cps), _pts(normals)
+    ncp = cps.shape[0]
+    G = np.zeros((ncp, mesh.npanels), order="F")
+    lib().fpo_assemble_source(_d(_pts(mesh.nodes)), _i(_i32(mesh.panel_offsets)),
+                              _i(_i32(mesh.panel_nodes)), C.c_longlong(mesh.npanels), _d(cps),
+                              _d(normals), C.c_longlong(ncp), C.c_double(offset),
+                              G.ctypes.data_as(_dp), nthreads)
+    return G
+
+
+def rhs_noflowthrough(Uinfs, normals):
+    """calc_bc_noflowthrough!: RHS_i = -U_i . n_i (src/FLOWPanel_linearsolver.jl:297-312)."""
+    Uinfs, normals = _pts(Uinfs), _pts(normals)
+    return -(Uinfs[:, 0] * normals[:, 0] + Uinfs[:, 1] * normals[:, 1] + Uinfs[:, 2] * normals[:, 2])
+
+
+def uind_vortexring(mesh, strength, Das, Dbs, targets, offset=1e-8, cutoff=1e-14, nthreads=0):
+    targets = _pts(targets)
+    out = np.zeros((targets.shape[0], 3))
+    sh = _i32(mesh.shedding.reshape(-1, 6)) if mesh.nsheddings else np.zeros((0, 6), np.int32)
+    rc = lib().fpo_uind_vortexring(_d(_pts(mesh.nodes)), _i(_i32(mesh.panel_offsets)),
+                                   _i(_i32(mesh.panel_nodes)), C.c_longlong(mesh.npanels),
+                                   _d(_f64(strength)), _i(sh), C.c_longlong(len(sh)),
+                                   _d(_pts(np.reshape(Das, (-1, 3)))), _d(_pts(np.reshape(Dbs, (-1, 3)))),
+                                   C.c_double(offset), C.c_double(cutoff), _d(targets),
+                                   C.c_longlong(targets.shape[0]), _d(out), nthreads)
+    if rc:
+        raise ValueError("Found non-unitary semi-infinite direction")
+    return out
+
+
+def uind_source(mesh, strength, targets, offset=1e-8, nthreads=0):
+    targets = _pts(targets)
+    out = np.zeros((targets.shape[0], 3))
+    lib().fpo_uind_source(_d(_pts(mesh.nodes)), _i(_i32(mesh.panel_offsets)),
+                          _i(_i32(mesh.panel_nodes)), C.c_longlong(mesh.npanels),
+                          _d(_f64(strength)), C.c_double(offset), _d(targets),
+                          C.c_longlong(targets.shape[0]), _d(out), nthreads)
+    return out
+
+
+# ----------------------------------------------------------------- linear solvers
+def lu_factor(G):
+    """LAPACK dgetrf (partial pivoting), as Julia's LA.lu! (src/FLOWPanel_linearsolver.jl:173-185)."""
+    import scipy.linalg as sla
+    return sla.lu_factor(np.asfortranarray(G), check_finite=False)
+
+
+def lu_solve(lu, b):
+    import scipy.linalg as sla
+    return sla.lu_solve(lu, b, check_finite=False)
+
+
+def solve_ludiv(G, b):
+    """solve_ludiv!: src/FLOWPanel_linearsolver.jl:57-78."""
+    return lu_solve(lu_factor(G), b)
+
+
+def gmres(A, b, memory=50, atol=None, rtol=None, itmax=None, x0=None):
+    """Restarted GMRES(memory) restating Krylov.jl 0.9's algorithm as the reference
+    calls it (src/FLOWPanel_linearsolver.jl:136-147): modified Gram-Schmidt
+    Arnoldi, Givens rotations, stop when ||r|| <= atol + rtol * ||b||.
+    Returns (x, niter, converged)."""
+    eps = np.finfo(np.float64).eps
+    atol = np.sqrt(eps) if atol is None else atol
+    rtol = np.sqrt(eps) if rtol is None else rtol
+    n = len(b)
+    itmax = 2 * n if itmax is None else itmax
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    r = b - A @ x if x0 is not None else b.copy()
+    bnorm = np.linalg.norm(b)
+    eps_stop = atol + rtol * bnorm
+    beta = np.linalg.norm(r)
+    it = 0
+    if beta <= eps_stop:
+        return x, 0, True
+    while it < itmax:
+        V = np.zeros((memory + 1, n))
+        H = np.zeros((memory + 1, memory))
+        cs, sn = np.zeros(memory), np.zeros(memory)
+        g = np.zeros(memory + 1)
+        g[0] = beta
+        V[0] = r / beta
+        k_done = 0
+        for k in range(memory):
+            w = A @ V[k]
+            for i in range(k + 1):
+                H[i, k] = np.dot(V[i], w)
+                w = w - H[i, k] * V[i]
+            H[k + 1, k] = np.linalg.norm(w)
+            if H[k + 1, k] != 0:
+                V[k + 1] = w / H[k + 1, k]
+            for i in range(k):
+                t = cs[i] * H[i, k] + sn[i] * H[i + 1, k]
+                H[i + 1, k] = -sn[i] * H[i, k] + cs[i] * H[i + 1, k]
+                H[i, k] = t
+            den = np.hypot(H[k, k], H[k + 1, k])
+            cs[k], sn[k] = H[k, k] / den, H[k + 1, k] / den
+            H[k, k] = den
+            H[k + 1, k] = 0.0
+            g[k + 1] = -sn[k] * g[k]
+            g[k] = cs[k] * g[k]
+            it += 1
+            k_done = k + 1
+            if abs(g[k + 1]) <= eps_stop or it >= itmax:
+                break
+        y = np.linalg.solve(np.triu(H[:k_done, :k_done]), g[:k_done])
+        x = x + V[:k_done].T @ y
+        r = b - A @ x
+        beta = np.linalg.norm(r)
+        if beta <= eps_stop:
+            return x, it, True
+    return x, it, False
+
+
+# ----------------------------------------------------------------- post-processing
+def calcfield_Cp(Us, Uref, shedding=None, correct_kuttacondition=True):
+    """calcfield_Cp!: Cp = 1 - (|U|/Uref)^2 with the TE Kutta average over
+    (pi, pi+1, pj, pj-1) (src/FLOWPanel_postprocess.jl:1059-1112)."""
+    Us = np.asarray(Us, dtype=np.float64)
+    Cp = 1 - (np.sqrt(np.sum(Us * Us, axis=1)) / Uref) ** 2
+    if correct_kuttacondition and shedding is not None:
+        for (pi, nia, nib, pj, nja, njb) in np.reshape(shedding, (-1, 6)):
+            if pj != -1:
+                ave = (Cp[pi] + Cp[pi + 1] + Cp[pj] + Cp[pj - 1]) / 4
+                Cp[[pi, pi + 1, pj, pj - 1]] = ave
+            else:
+                ave = (Cp[pi] + Cp[pi + 1]) / 2
+                Cp[[pi, pi + 1]] = ave
+    return Cp
+
+
+def calcfield_F(Cps, areas, normals, Uinf, rho, shedding=None, correct_kuttacondition=True):
+    """calcfield_F!: F = -Cp q A n (normals already flipped by sign(CPoffset))
+    with the TE override (src/FLOWPanel_postprocess.jl:1199-1307)."""
+    normals = np.asarray(normals, dtype=np.float64)
+    F = (-0.5 * rho * Uinf ** 2 * np.asarray(Cps) * np.asarray(areas))[:, None] * normals
+    if correct_kuttacondition and shedding is not None:
+        q = 0.5 * rho * Uinf ** 2
+        for (pi, nia, nib, pj, nja, njb) in np.reshape(shedding, (-1, 6)):
+            if pj != -1:
+                idx = [pi, pi + 1, pj, pj - 1]
+                ave = (Cps[pi] + Cps[pi + 1] + Cps[pj] + Cps[pj - 1]) / 4
+            else:
+                idx = [pi, pi + 1]
+                ave = (Cps[pi] + Cps[pi + 1]) / 2
+            for i in idx:
+                F[i] = -ave * q * areas[i] * normals[i]
+    return F
+
+
+def calcfield_LDS(Fs, Lhat, Dhat, Shat=None):
+    """calcfield_LDS!: project the summed force on L, D, S (src/FLOWPanel_postprocess.jl:1615-1652)."""
+    Lhat, Dhat = np.asarray(Lhat, float), np.asarray(Dhat, float)
+    Shat = np.cross(Lhat, Dhat) if Shat is None else np.asarray(Shat, float)
+    Ftot = np.sum(np.asarray(Fs), axis=0)
+    return np.stack([Lhat * np.dot(Ftot, Lhat), Dhat * np.dot(Ftot, Dhat), Shat * np.dot(Ftot, Shat)], axis=1)

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle.
+
+Tolerances: AIC entries 1e-12 of the largest entry (same formulas; FMA and
+reciprocal rewrites move the last bits); FP64 strengths 1e-10 relative (the
+bar of the plain form); mixed-precision strengths 1e-10 relative after FP64
+refinement; FP32 off-body velocity 1e-4 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import freestream
+
+pytestmark = pytest.mark.gpu
+
+
+def _wing_setup(fp, nc=20, ns=24, tri=False, aoa=4.2):
+    w = fp.meshes.swept_wing("0012", nc, ns)
+    if tri:
+        w = fp.meshes.triangulate(w)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    V = freestream(aoa)
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    return w, body, normals, cps, D, U
+
+
+@pytest.mark.parametrize("tri", [False, True])
+def test_ring_aic_matches_oracle(fp, O, ctx, tri):
+    w, body, normals, cps, D, U = _wing_setup(fp, tri=tri)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    ctx.assemble(fp._capi.FP_ELEMENT_VORTEXRING)
+    G = ctx.get_aic()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    assert np.abs(G - Gr).max() <= 1e-12 * np.abs(Gr).max()
+    big = np.abs(Gr) > 1e-3 * np.abs(Gr).max()
+    assert np.max(np.abs(G[big] - Gr[big]) / np.abs(Gr[big])) < 1e-11
+
+
+def test_ring_aic_shared_wake_columns(fp, O, ctx):
+    """Two shedding edges on one panel column take the serial wake path."""
+    w, body, normals, cps, D, U = _wing_setup(fp, 12, 8)
+    sh = np.concatenate([w.shedding, w.shedding[:1]])
+    D2 = np.concatenate([D, D[:1]])
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(sh, D2, D2)
+    ctx.assemble(fp._capi.FP_ELEMENT_VORTEXRING)
+    G = ctx.get_aic()
+    w2 = fp.meshes.Mesh(w.nodes, w.panel_offsets, w.panel_nodes, sh, w.bodies)
+    Gr = O.assemble_vortexring(w2, cps, normals, D2, D2)
+    assert np.abs(G - Gr).max() <= 1e-12 * np.abs(Gr).max()
+
+
+def test_source_aic_matches_oracle(fp, O, ctx):
+    s = fp.meshes.sphere(1.0, 10, 20)
+    body = fp.NonLiftingBody(s)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    ctx.set_geometry(s.nodes, s.panel_offsets, s.panel_nodes, cps, normals)
+    ctx.assemble(fp._capi.FP_ELEMENT_SOURCE)
+    G = ctx.get_aic()
+    Gr = O.assemble_source(s, cps, normals)
+    assert np.abs(G - Gr).max() <= 1e-12 * np.abs(Gr).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_wing_solve_matches_oracle(fp, O, ctx, precision):
+    w, body, normals, cps, D, U = _wing_setup(fp, 40, 48)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", precision))
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+    assert st.rel_residual < 1e-11
+    if precision == "fp64":
+        assert st.max_abs_L > 0
+
+
+def test_multi_rhs_sweep(fp, O, ctx):
+    """Angle-of-attack sweep as many right-hand sides on one factorisation (fixed wake)."""
+    w, body, normals, cps, D, U = _wing_setup(fp, 20, 24)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    aoas = np.arange(-10, 11, 4.0)
+    Us = np.stack([np.tile(freestream(a), (w.npanels, 1)) for a in aoas])
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    lu = O.lu_factor(Gr)
+    for prec in ("fp64", "mixed"):
+        X, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, Us, opts=fp._capi.make_opts("ludiv", prec))
+        for q in range(len(aoas)):
+            xr = O.lu_solve(lu, O.rhs_noflowthrough(Us[q], normals))
+            assert np.linalg.norm(X[q] - xr) / np.linalg.norm(xr) < 1e-10
+
+
+def test_gmres_matches_oracle(fp, O, ctx):
+    w, body, normals, cps, D, U = _wing_setup(fp, 20, 24)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    opts = fp._capi.make_opts("gmres", "fp64", gmres_atol=1e-13, gmres_rtol=1e-13)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=opts)
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    b = O.rhs_noflowthrough(U, normals)
+    xr = O.solve_ludiv(Gr, b)
+    assert st.used_gmres == 1 and st.gmres_iters > 0
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-9
+    # same restarted GMRES(50) on the CPU converges in a comparable number of steps
+    xg, it, conv = O.gmres(Gr, b, atol=1e-13, rtol=1e-13)
+    assert conv and abs(it - st.gmres_iters) <= max(5, 0.2 * it)
+
+
+def test_uind_matches_oracle(fp, O, ctx):
+    w, body, normals, cps, D, U = _wing_setup(fp, 20, 24)
+    rng = np.random.default_rng(3)
+    gamma = rng.standard_normal(w.npanels)
+    probes = np.concatenate([cps + 0.05 * normals, rng.uniform(-3, 3, (500, 3))])
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    ref = O.uind_vortexring(w, gamma, D, D, probes)
+    base = rng.standard_normal(probes.shape)
+    got = ctx.uind(fp._capi.FP_ELEMENT_VORTEXRING, gamma, probes, base.copy())
+    scale = np.abs(ref).max()
+    assert np.abs(got - base - ref).max() <= 1e-12 * scale
+    got32 = ctx.uind(fp._capi.FP_ELEMENT_VORTEXRING, gamma, probes, None, fp._capi.FP_PREC_MIXED)
+    assert np.abs(got32 - ref).max() <= 1e-4 * scale
+
+
+def test_uind_source_matches_oracle(fp, O, ctx):
+    s = fp.meshes.sphere(1.0, 10, 20)
+    body = fp.NonLiftingBody(s)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    rng = np.random.default_rng(5)
+    sig = rng.standard_normal(s.npanels)
+    probes = np.concatenate([cps, rng.uniform(-2, 2, (300, 3))])
+    ctx.set_geometry(s.nodes, s.panel_offsets, s.panel_nodes, cps, normals)
+    got = ctx.uind(fp._capi.FP_ELEMENT_SOURCE, sig, probes)
+    ref = O.uind_source(s, sig, probes)
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_sphere_host_api_analytic_cp(fp):
+    """solve + calcfield_U + calcfield_Cp through the host mirror; Cp against
+    1 - 9/4 sin^2(theta) (examples/sphere.jl:86-87)."""
+    s = fp.meshes.sphere(1.0, 30, 60)
+    body = fp.NonLiftingBody(s)
+    U = np.tile([1.0, 0, 0], (s.npanels, 1))
+    solver = fp.B200Solver("backslash", "fp64")
+    fp.solve(body, U, solver=solver)
+    Us = fp.calcfield_U(body, body, solver=solver)
+    Cp = fp.calcfield_Cp(body, 1.0)
+    cps = fp.calc_controlpoints(body)
+    th = np.arccos(np.clip(cps[:, 0] / np.linalg.norm(cps, axis=1), -1, 1))
+    err = Cp - (1 - 9 / 4 * np.sin(th) ** 2)
+    assert np.sqrt(np.mean(err ** 2)) < 0.02 and np.abs(err).max() < 0.05
+    solver.close()
+
+
+def test_errors_mirror_reference(fp, ctx):
+    cap = fp._capi
+    w = fp.meshes.swept_wing("0012", 8, 4)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes)
+    bad = np.tile([1.0, 0.0, 0.1], (w.nsheddings, 1))
+    with pytest.raises(cap.FlowPanelError) as e:
+        ctx.set_wake(w.shedding, bad, bad)
+    assert e.value.code == cap.FP_EINVAL and "non-unitary" in str(e.value)
+    offs = np.array([0, 5], np.int32)
+    with pytest.raises(cap.FlowPanelError) as e:
+        ctx.set_geometry(w.nodes, offs, np.arange(5, dtype=np.int32))
+    assert e.value.code == cap.FP_EINVAL
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes)
+    with pytest.raises(cap.FlowPanelError) as e:
+        ctx.factor()
+    assert e.value.code == cap.FP_ESTATE
