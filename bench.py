@@ -223,6 +223,13 @@ def run_ours(args, rank, ws, dist):
     launches = ctx.kernel_launches() - launches0
     ms_mixed, stg_m, st_m = res["mixed"]
     ms_fp64, stg_d, st_d = res["fp64"]
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile": True, "mixed_ms": ms_mixed, "fp64_ms": ms_fp64,
+                              "stages_mixed": stg_m.tolist(), "stages_fp64": stg_d.tolist(),
+                              "ir_iters": st_m.ir_iters, "launches": launches}), flush=True)
+        ctx.close()
+        return
 
     # e2e through the public C ABI with host buffers
     e2e = []
@@ -294,6 +301,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="timed device steps only (for ncu launch lists): no e2e, accuracy or CPU legs")
     args = ap.parse_args()
     rank, ws, dist = dist_init()
     try:

@@ -114,7 +114,7 @@ int gmres_solve(fp_ctx* c, const double* b, double* x, int64_t k, const fp_solve
     if (c->d_h) cudaFree(c->d_h);
     c->d_V = nullptr; c->d_h = nullptr;
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_V, (size_t)(m + 3) * ld * sizeof(double)));
-    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_h, (size_t)(2 * m + 8) * sizeof(double)));
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_h, (size_t)(2 * (m + 1) + 16) * sizeof(double)));
     c->cap_gmres_m = m;
   }
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * n * sizeof(double)));

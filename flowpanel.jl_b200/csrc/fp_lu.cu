@@ -245,50 +245,65 @@ k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ C
 bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
                      int64_t nn, int kk);
 
+// C (m x nn) -= A (m x kk) B (kk x nn); all three are sub-blocks of one
+// column-major matrix with leading dimension lda.
 template <class T>
-static int trailing_update(fp_ctx* c, T* A, int64_t lda, int64_t m, int64_t nn, int kk,
-                           int64_t k) {
-  const T* L21 = A + k * lda + (k + kk);
-  const T* U12 = A + (k + kk) * lda + k;
-  T* C = A + (k + kk) * lda + (k + kk);
+static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int64_t m, int64_t nn,
+                    int kk) {
+  if (m <= 0 || nn <= 0 || kk <= 0) return FP_OK;
   if (sizeof(T) == 4) {
-    if (tc_gemm_sub_f32(c, (const float*)L21, (const float*)U12, (float*)C, lda, m, nn, kk))
-      return FP_OK;
+    if (tc_gemm_sub_f32(c, (const float*)Am, (const float*)Bm, (float*)Cm, lda, m, nn, kk)) return FP_OK;
     constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
     dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
-    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(L21, U12, C, lda, m, nn, kk);
+    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk);
     ++c->nlaunch;
   } else {
-    constexpr int BM = 64, BN = 64, BK = 16, TM = 4, TN = 4;
+    constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
     dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
-    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(L21, U12, C, lda, m, nn, kk);
+    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk);
     ++c->nlaunch;
   }
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;
 }
 
+// Two-level blocked right-looking LU. Outer panels of kOuterNB columns; inside
+// a panel, NB-wide blocks are factored (local pivoting), their U12 rows formed
+// for every column to the right, and the update is applied only to the panel
+// columns (full height) and to the panel rows (to the right), so that the
+// trailing matrix is updated once per outer panel with K = kOuterNB.
+constexpr int kOuterNB = 256;
+
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
-  for (int64_t k = 0; k < n; k += NB) {
-    const int nb = (int)std::min<int64_t>(NB, n - k);
-    const int64_t below = n - k - nb;
-    const unsigned g1 = (unsigned)std::max<int64_t>(1, (below + kPanelThreads - 1) / kPanelThreads);
-    k_panel<T><<<g1, kPanelThreads, 0, c->stream>>>(A, lda, n, k, ipiv, cert, c->d_status);
-    ++c->nlaunch;
-    FP_CUDA_TRY(c->err, cudaGetLastError());
-    if (n - nb > 0) {
-      const int64_t nother = n - nb;
-      const unsigned g2 = (unsigned)std::min<int64_t>((nother + kSwapWarps - 1) / kSwapWarps, 4 * 148);
-      k_swap_u12<T><<<g2, kSwapWarps * 32, 0, c->stream>>>(A, lda, n, k, ipiv);
+  auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
+  for (int64_t K0 = 0; K0 < n; K0 += kOuterNB) {
+    const int64_t kend = std::min<int64_t>(K0 + kOuterNB, n);
+    for (int64_t k = K0; k < kend; k += NB) {
+      const int nb = (int)std::min<int64_t>(NB, n - k);
+      const int64_t below = n - k - nb;
+      const unsigned g1 = (unsigned)std::max<int64_t>(1, (below + kPanelThreads - 1) / kPanelThreads);
+      k_panel<T><<<g1, kPanelThreads, 0, c->stream>>>(A, lda, n, k, ipiv, cert, c->d_status);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
+      if (n - nb > 0) {
+        const int64_t nother = n - nb;
+        const unsigned g2 = (unsigned)std::min<int64_t>((nother + kSwapWarps - 1) / kSwapWarps, 4 * 148);
+        k_swap_u12<T><<<g2, kSwapWarps * 32, 0, c->stream>>>(A, lda, n, k, ipiv);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      }
+      const int64_t k1 = k + nb;
+      // (a) remaining panel columns, full height
+      if (int rc = gemm_sub<T>(c, at(k1, k), at(k, k1), at(k1, k1), lda, n - k1, kend - k1, nb)) return rc;
+      // (b) remaining panel rows, columns right of the panel
+      if (int rc = gemm_sub<T>(c, at(k1, k), at(k, kend), at(k1, kend), lda, kend - k1, n - kend, nb)) return rc;
     }
-    if (below > 0) {
-      int rc = trailing_update<T>(c, A, lda, below, below, nb, k);
-      if (rc) return rc;
-    }
+    // outer trailing update with K = kend - K0
+    if (int rc = gemm_sub<T>(c, at(kend, K0), at(K0, kend), at(kend, kend), lda, n - kend, n - kend,
+                             (int)(kend - K0)))
+      return rc;
   }
   return FP_OK;
 }
@@ -370,78 +385,84 @@ __global__ void k_apply_piv(T* __restrict__ B, int64_t ldb, int64_t n, int64_t k
 // Persistent blocked triangular solve (one sweep), KR right-hand sides.
 // LOWER: L y = b (unit lower, forward); else U x = y (upper, backward).
 // The solution overwrites B. flags[b] = 1 once block b is final.
+// Every dependency tile of the factors is final before the solve starts, so a
+// CTA issues the loads of the next tile into shared memory before it waits for
+// the flag of the block whose solution it multiplies.
 constexpr int kTrsThreads = 256;
 template <class T, bool LOWER, int KR>
 __global__ void __launch_bounds__(kTrsThreads)
 k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv,
       T* __restrict__ B, int64_t ldb, unsigned int* __restrict__ flags,
       unsigned int* __restrict__ ticket, int* __restrict__ status) {
+  __shared__ T tile[NB][NB + 1];   // tile[l][r] = A(k0 + r, c0 + l)
   __shared__ T acc[KR][NB];
   __shared__ T y[KR][NB];
-  __shared__ int blk_s;
+  __shared__ int blk_s, stop_s;
+  constexpr int PER = NB * NB / kTrsThreads;   // tile elements per thread
   const int64_t nblk = (n + NB - 1) / NB;
   const int tid = threadIdx.x;
   const int r = tid % NB;          // row within the block
   const int qg = tid / NB;         // RHS lane group
   constexpr int QG = kTrsThreads / NB;
   for (;;) {
-    if (tid == 0) blk_s = (int)atomicAdd(ticket, 1u);
+    if (tid == 0) { blk_s = (int)atomicAdd(ticket, 1u); stop_s = 0; }
     __syncthreads();
     const int64_t tk = blk_s;
-    __syncthreads();
     if (tk >= nblk) return;
     const int64_t b = LOWER ? tk : nblk - 1 - tk;
     const int64_t k0 = b * NB;
     const int nb = (int)imin64(NB, n - k0);
     for (int q = qg; q < KR; q += QG) acc[q][r] = (r < nb) ? B[q * ldb + k0 + r] : T(0);
-    // dependencies
     for (int64_t s = 0; s < tk; ++s) {
       const int64_t cb = LOWER ? s : nblk - 1 - s;
       const int64_t c0 = cb * NB;
       const int cn = (int)imin64(NB, n - c0);
+      T v[PER];
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int e = tid + u * kTrsThreads;
+        const int rr = e % NB, ll = e / NB;
+        v[u] = (rr < nb && ll < cn) ? A[(c0 + ll) * lda + k0 + rr] : T(0);
+      }
       if (tid == 0) {
         int spins = 0;
         while (atomicAdd(&flags[cb], 0u) == 0u) {
-          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); break; }
+          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
           __nanosleep(64);
         }
       }
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int e = tid + u * kTrsThreads;
+        tile[e / NB][e % NB] = v[u];
+      }
       __syncthreads();
-      if (atomicOr(status, 0) & (int)DEV_TIMEOUT) return;
+      if (stop_s) return;
       for (int q = qg; q < KR; q += QG) y[q][r] = (r < cn) ? __ldcg(&B[q * ldb + c0 + r]) : T(0);
       __syncthreads();
-      if (r < nb) {
-        T s0[KR];
-#pragma unroll
-        for (int q = 0; q < KR; ++q) s0[q] = T(0);
-        // this thread accumulates row r for RHS q = qg, qg+QG, ...
-        for (int l = 0; l < cn; ++l) {
-          const T a = A[(c0 + l) * lda + k0 + r];
-#pragma unroll
-          for (int q = 0; q < KR; ++q)
-            if ((q % QG) == qg) s0[q] += a * y[q][l];
-        }
-#pragma unroll
-        for (int q = 0; q < KR; ++q)
-          if ((q % QG) == qg) acc[q][r] -= s0[q];
+      for (int q = qg; q < KR; q += QG) {
+        T s0 = T(0);
+#pragma unroll 16
+        for (int l = 0; l < NB; ++l) s0 += tile[l][r] * y[q][l];
+        acc[q][r] -= s0;
       }
       __syncthreads();
     }
     // x_b = inv(D_bb) acc
-    const T* Di = Dinv + b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
-    if (r < nb) {
-      T s0[KR];
+    {
+      const T* Di = Dinv + b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
 #pragma unroll
-      for (int q = 0; q < KR; ++q) s0[q] = T(0);
-      for (int l = 0; l < NB; ++l) {
-        const T a = Di[l * NB + r];
-#pragma unroll
-        for (int q = 0; q < KR; ++q)
-          if ((q % QG) == qg) s0[q] += a * acc[q][l];
+      for (int u = 0; u < PER; ++u) {
+        const int e = tid + u * kTrsThreads;
+        tile[e / NB][e % NB] = Di[e];    // Di column-major: e = l*NB + rr
       }
-#pragma unroll
-      for (int q = 0; q < KR; ++q)
-        if ((q % QG) == qg) B[q * ldb + k0 + r] = s0[q];
+      __syncthreads();
+      for (int q = qg; q < KR; q += QG) {
+        T s0 = T(0);
+#pragma unroll 16
+        for (int l = 0; l < NB; ++l) s0 += tile[l][r] * acc[q][l];
+        if (r < nb) B[q * ldb + k0 + r] = s0;
+      }
     }
     __threadfence();
     __syncthreads();
