@@ -24,7 +24,7 @@ FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND = range(4)
 EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count", "fp_set_geometry",
            "fp_set_wake", "fp_assemble", "fp_get_aic", "fp_set_rhs", "fp_factor", "fp_solve",
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
-           "fp_kernel_launches")
+           "fp_kernel_launches", "fp_tc_selftest")
 
 
 class SolveOpts(C.Structure):
@@ -81,6 +81,7 @@ def lib():
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
         L.fp_measure_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
         L.fp_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
+        L.fp_tc_selftest.argtypes = [C.c_int, C.c_int64, C.c_int64, C.c_int, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -217,3 +218,12 @@ def measure_fma_peak(device=0, fp64=True):
     if rc:
         raise FlowPanelError(rc, "fp_measure_fma_peak failed")
     return t.value
+
+
+def tc_selftest(m, n, k, device=0):
+    """(err_tc, err_simt, ms_tc) of the tensor-core FP32 update against FP64 (see the header)."""
+    a, b, t = C.c_double(), C.c_double(), C.c_double()
+    rc = lib().fp_tc_selftest(int(device), int(m), int(n), int(k), C.byref(a), C.byref(b), C.byref(t))
+    if rc:
+        raise FlowPanelError(rc, "fp_tc_selftest failed")
+    return a.value, b.value, t.value

@@ -91,6 +91,8 @@ void free_matrices(fp_ctx* c) {
   dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_part);
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
   dfree(c->d_V); dfree(c->d_h);
+  for (int i = 0; i < 4; ++i) dfree(c->d_tc[i]);
+  c->tc_cap = 0;
   c->cap_rhs = 0; c->cap_gmres_m = 0;
   c->assembled = -1; c->factored = -1; c->nrhs = 0;
 }

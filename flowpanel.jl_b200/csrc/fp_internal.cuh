@@ -75,6 +75,9 @@ struct fp_ctx {
   int klaunch[4] = {0, 0, 0, 0};
   fp_stats last{};
   int64_t nlaunch = 0;          // kernels launched by this context
+  bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
+  float* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};   // Ah, Al, Bh, Bl scratch
+  size_t tc_cap = 0;
 };
 
 namespace fpb {

@@ -267,6 +267,16 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
   return FP_OK;
 }
 
+int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
+                      int kk) {
+  constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
+  dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
+  k_gemm_sub<float, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(A, B, C, lda, m, nn, kk);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
 // Two-level blocked right-looking LU. Outer panels of kOuterNB columns; inside
 // a panel, NB-wide blocks are factored (local pivoting), their U12 rows formed
 // for every column to the right, and the update is applied only to the panel

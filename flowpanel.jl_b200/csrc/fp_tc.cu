@@ -1,12 +1,413 @@
-// FP32 trailing update C -= A B of the mixed-precision LU on the tcgen05
-// tensor cores (3xTF32 split). Until the tensor-core kernel is enabled the
-// SIMT FP32 kernel of fp_lu.cu performs the update.
+// FP32 trailing update C -= A B of the mixed-precision LU on the 5th-generation
+// tensor cores (tcgen05, kind::tf32), with the 3xTF32 split
+//     A B ~= Ah Bh + Ah Bl + Al Bh,   Ah = rna_tf32(A), Al = A - Ah (same for B)
+// which keeps the product at FP32-level accuracy (a single TF32 product
+// would leave kappa * u_tf32 ~ 10 on the wing AIC and refinement would not
+// converge).
+//
+// Data flow per 128 x 128 output tile (one CTA, 4 warps):
+//   * split kernels write Ah, Al (K-major copies of the L21 panel) and Bh, Bl
+//     (K-major copies of the U12 panel) to scratch in HBM;
+//   * warp 0 / lane 0 streams 32-wide K blocks of the four operands into a
+//     3-stage shared-memory ring with TMA (SWIZZLE_128B, no multicast);
+//   * warp 1 / lane 0 issues 3 x 4 tcgen05.mma (M=128, N=128, K=8) per K block
+//     into a 128-column TMEM accumulator and frees each stage with
+//     tcgen05.commit;
+//   * all four warps read the accumulator back with tcgen05.ld (warp w owns
+//     TMEM lanes 32w..32w+31 = tile rows) and apply C -= D with coalesced
+//     column accesses.
+// Every mbarrier wait is bounded; on a timeout the kernel records DEV_TIMEOUT,
+// drains its own copies, frees TMEM and returns.
+#include <cuda.h>
+
+#include <cstring>
+
 #include "fp_internal.cuh"
 
 namespace fpb {
+namespace tc {
 
-bool tc_gemm_sub_f32(fp_ctx*, const float*, const float*, float*, int64_t, int64_t, int64_t, int) {
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 128;
+constexpr int TILE_A = BM * BK * 4;                 // 16 KB
+constexpr int TILE_B = BN * BK * 4;                 // 16 KB
+constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr uint32_t TMEM_COLS = 128;
+constexpr int kWaitLimit = 1 << 22;
+// instruction descriptor: D f32 (bits 4-5 = 1), A/B tf32 (bits 7-9, 10-12 = 2),
+// both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+// K-major, SWIZZLE_128B shared-memory matrix descriptor (tile base 1024-B aligned):
+// start address >> 4, LBO 16 B (unused), SBO 1024 B (8 rows x 128 B), version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1u << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(IDESC), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__global__ void __launch_bounds__(THREADS, 1)
+k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+              const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
+              float* __restrict__ C, int64_t ldc, int m, int n, int K, int* __restrict__ status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nk = (K + BK - 1) / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // producer
+    int issued = 0;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1)) { *abort_flag = 1; break; }
+      if (*(volatile int*)abort_flag) break;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      uint8_t* base = smem + s * STAGE_BYTES;
+      tma_load_2d(base, &tmAh, kb * BK, m0, &full[s]);
+      tma_load_2d(base + TILE_A, &tmAl, kb * BK, m0, &full[s]);
+      tma_load_2d(base + 2 * TILE_A, &tmBh, kb * BK, n0, &full[s]);
+      tma_load_2d(base + 2 * TILE_A + TILE_B, &tmBl, kb * BK, n0, &full[s]);
+      ++issued;
+    }
+    if (*(volatile int*)abort_flag) {
+      // drain the copies this CTA issued before leaving
+      for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
+        mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    bool ok = true;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(&full[s], (kb / STAGES) & 1)) { ok = false; *abort_flag = 1; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+      const uint64_t dAh = sdesc(base), dAl = sdesc(base + TILE_A);
+      const uint64_t dBh = sdesc(base + 2 * TILE_A), dBl = sdesc(base + 2 * TILE_A + TILE_B);
+#pragma unroll
+      for (int kk = 0; kk < BK / 8; ++kk) {
+        const uint64_t off = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+        umma_tf32(tmem, dAh + off, dBl + off, (kb | kk) != 0 ? 1u : 0u);
+        umma_tf32(tmem, dAl + off, dBh + off, 1u);
+        umma_tf32(tmem, dAh + off, dBh + off, 1u);
+      }
+      umma_commit(&empty[s]);
+    }
+    if (ok) umma_commit(done);
+  }
+  __syncwarp();
+  // epilogue: every warp waits for the accumulator
+  const bool ok = mbar_wait(done, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int cc = 0; cc < BN; cc += 16) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < m) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = n0 + cc + j;
+          if (col < n) C[(int64_t)col * ldc + row] -= __uint_as_float(r[j]);
+        }
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicOr(status, (int)DEV_TIMEOUT);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  return __uint_as_float(h);
+}
+
+// L21 panel (m x K, column-major, lda) -> K-major copies Ah, Al (m x ldk, row-major).
+__global__ void k_split_A(const float* __restrict__ A, int64_t lda, int m, int K, int ldk,
+                          float* __restrict__ Ah, float* __restrict__ Al) {
+  __shared__ float t[32][33];
+  const int i0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8
+  for (int j = ty; j < 32; j += 8) {
+    const int i = i0 + tx, k = k0 + j;
+    t[j][tx] = (i < m && k < K) ? A[(int64_t)k * lda + i] : 0.f;
+  }
+  __syncthreads();
+  for (int j = ty; j < 32; j += 8) {
+    const int i = i0 + j, k = k0 + tx;
+    if (i < m && k < ldk) {
+      const float v = t[tx][j];
+      const float h = tf32_rna(v);
+      Ah[(int64_t)i * ldk + k] = h;
+      Al[(int64_t)i * ldk + k] = v - h;
+    }
+  }
+}
+
+// U12 panel (K x n, column-major, lda) -> Bh, Bl (K x n, column-major, ldk).
+__global__ void k_split_B(const float* __restrict__ B, int64_t lda, int K, int n, int ldk,
+                          float* __restrict__ Bh, float* __restrict__ Bl) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)ldk * n) return;
+  const int k = (int)(t % ldk);
+  const int64_t j = t / ldk;
+  const float v = (k < K) ? B[j * lda + k] : 0.f;
+  const float h = tf32_rna(v);
+  Bh[t] = h;
+  Bl[t] = v - h;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D fp32 map over a K-major matrix: inner dim K (extent kext, row pitch ldk
+// floats), outer dim rows; box 32 x box_rows, 128-byte swizzle, zero fill.
+static bool make_map(CUtensorMap* tm, const float* base, int kext, int64_t rows, int ldk, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kext, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ldk * 4};
+  cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace tc
+
+// Scratch for the split operands: 4 x N x 256 floats.
+static int ensure_tc_scratch(fp_ctx* c, int64_t rows_max) {
+  const size_t need = (size_t)rows_max * 256;
+  if (c->tc_cap >= need) return FP_OK;
+  for (int i = 0; i < 4; ++i) {
+    if (c->d_tc[i]) cudaFree(c->d_tc[i]);
+    c->d_tc[i] = nullptr;
+  }
+  for (int i = 0; i < 4; ++i) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tc[i], need * sizeof(float)));
+  c->tc_cap = need;
+  return FP_OK;
+}
+
+bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
+                     int64_t nn, int kk) {
+  if (!c->use_tc || kk <= 0 || kk > 256 || m <= 0 || nn <= 0) return false;
+  if (!tc::encode_fn()) return false;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(tc::k_tc_gemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES) !=
+        cudaSuccess)
+      return false;
+    attr_set = true;
+  }
+  if (ensure_tc_scratch(c, std::max<int64_t>(m, nn)) != FP_OK) return false;
+  const int ldk = (int)round_up(kk, 32);
+  float *Ah = c->d_tc[0], *Al = c->d_tc[1], *Bh = c->d_tc[2], *Bl = c->d_tc[3];
+  {
+    dim3 g((unsigned)((m + 31) / 32), (unsigned)((ldk + 31) / 32));
+    tc::k_split_A<<<g, dim3(32, 8), 0, c->stream>>>(A, lda, (int)m, kk, ldk, Ah, Al);
+    ++c->nlaunch;
+    const int64_t t = (int64_t)ldk * nn;
+    tc::k_split_B<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(B, lda, kk, (int)nn, ldk, Bh, Bl);
+    ++c->nlaunch;
+  }
+  CUtensorMap mAh, mAl, mBh, mBl;
+  if (!tc::make_map(&mAh, Ah, kk, m, ldk, tc::BM) || !tc::make_map(&mAl, Al, kk, m, ldk, tc::BM) ||
+      !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN))
+    return false;
+  dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
+  tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, C, lda, (int)m,
+                                                                       (int)nn, kk, c->d_status);
+  ++c->nlaunch;
+  return cudaGetLastError() == cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// Self-test: C0 - A B for random A (m x k), B (k x n), C0 (m x n) by the
+// tensor-core kernel, by the SIMT kernel and in FP64; errors relative to
+// k * max|a| * max|b| (= k).
+__global__ void k_fill_rand(float* a, int64_t n, uint32_t seed) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t h = (uint32_t)t * 2654435761u ^ seed;
+  h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+  a[t] = (float)((double)h / 4294967296.0 * 2.0 - 1.0);
+}
+__global__ void k_ref_f64(const float* A, const float* B, const float* C0, double* R, int64_t ld, int m, int n,
+                          int k) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)m * n) return;
+  const int i = (int)(t % m), j = (int)(t / m);
+  double s = C0[(int64_t)j * ld + i];
+  for (int l = 0; l < k; ++l) s -= (double)A[(int64_t)l * ld + i] * (double)B[(int64_t)j * ld + l];
+  R[(int64_t)j * m + i] = s;
+}
+__global__ void k_maxerr(const float* C, const double* R, int64_t ld, int m, int n, unsigned long long* out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)m * n) return;
+  const int i = (int)(t % m), j = (int)(t / m);
+  const double e = fabs((double)C[(int64_t)j * ld + i] - R[(int64_t)j * m + i]);
+  atomicMax(out, (unsigned long long)__double_as_longlong(e));
+}
+
+int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
+                      int kk);
 
 }  // namespace fpb
+
+extern "C" int fp_tc_selftest(int device, int64_t m, int64_t n, int k, double* err_tc, double* err_simt,
+                              double* ms_tc) {
+  using namespace fpb;
+  if (m <= 0 || n <= 0 || k <= 0 || k > 256 || !err_tc || !err_simt || !ms_tc) return FP_EINVAL;
+  fp_ctx* c = nullptr;
+  if (int rc = fp_ctx_create(device, &c)) return rc;
+  const int64_t ld = round_up(std::max<int64_t>(m, k), 64);
+  const int64_t cols = std::max<int64_t>(n, k);
+  float *A = nullptr, *B = nullptr, *C1 = nullptr, *C2 = nullptr;
+  double* R = nullptr;
+  unsigned long long* e = nullptr;
+  int rc = FP_OK;
+  auto fail = [&](int code) { rc = code; };
+  if (cudaMalloc(&A, ld * cols * 4) || cudaMalloc(&B, ld * cols * 4) || cudaMalloc(&C1, ld * cols * 4) ||
+      cudaMalloc(&C2, ld * cols * 4) || cudaMalloc(&R, m * n * 8) || cudaMalloc(&e, 16)) {
+    fail(FP_ECUDA);
+  } else {
+    const int64_t tot = ld * cols;
+    const unsigned g = (unsigned)((tot + 255) / 256);
+    k_fill_rand<<<g, 256, 0, c->stream>>>(A, tot, 1u);
+    k_fill_rand<<<g, 256, 0, c->stream>>>(B, tot, 2u);
+    k_fill_rand<<<g, 256, 0, c->stream>>>(C1, tot, 3u);
+    cudaMemcpyAsync(C2, C1, tot * 4, cudaMemcpyDeviceToDevice, c->stream);
+    const unsigned gr = (unsigned)((m * n + 255) / 256);
+    k_ref_f64<<<gr, 256, 0, c->stream>>>(A, B, C1, R, ld, (int)m, (int)n, k);
+    cudaEventRecord(c->ev0, c->stream);
+    const bool used = tc_gemm_sub_f32(c, A, B, C1, ld, m, n, k);
+    cudaEventRecord(c->ev1, c->stream);
+    if (!used) fail(FP_EINVAL);
+    if (gemm_sub_simt_f32(c, A, B, C2, ld, m, n, k)) fail(FP_ECUDA);
+    double h[2] = {0, 0};
+    for (int w = 0; w < 2; ++w) {
+      cudaMemsetAsync(e, 0, 8, c->stream);
+      k_maxerr<<<gr, 256, 0, c->stream>>>(w == 0 ? C1 : C2, R, ld, (int)m, (int)n, e);
+      unsigned long long v = 0;
+      cudaMemcpyAsync(&v, e, 8, cudaMemcpyDeviceToHost, c->stream);
+      cudaStreamSynchronize(c->stream);
+      double d;
+      std::memcpy(&d, &v, 8);
+      h[w] = d / k;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    *err_tc = h[0];
+    *err_simt = h[1];
+    *ms_tc = ms;
+    int st = 0;
+    cudaMemcpy(&st, c->d_status, 4, cudaMemcpyDeviceToHost);
+    if (st & DEV_TIMEOUT) fail(FP_ETIMEOUT);
+    if (cudaGetLastError() != cudaSuccess) fail(FP_ECUDA);
+  }
+  cudaFree(A); cudaFree(B); cudaFree(C1); cudaFree(C2); cudaFree(R); cudaFree(e);
+  fp_ctx_destroy(c);
+  return rc;
+}

@@ -160,6 +160,13 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  * this context has launched since it was created. */
 int fp_kernel_launches(fp_ctx* ctx, int64_t* count);
 
+/* Self-test utility (no counterpart in the reference): C0 - A B for seeded
+ * random FP32 A (m x k), B (k x n) on device `device` by the tcgen05 3xTF32
+ * kernel of the mixed-precision LU and by the SIMT FP32 kernel, each compared
+ * with an FP64 evaluation; errors are max|C - C_fp64| / k (|a|, |b| <= 1). */
+int fp_tc_selftest(int device, int64_t m, int64_t n, int k, double* err_tc, double* err_simt,
+                   double* ms_tc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,38 @@
+"""The tcgen05 3xTF32 trailing update of the mixed-precision LU, on the GPU.
+
+C0 - A B for seeded random FP32 operands in [-1, 1], against an FP64
+evaluation. Tolerance: error / k <= 1e-6 (FP32-level; a single TF32 product
+would sit near 1e-4), and no worse than 4x the SIMT FP32 kernel's error.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("m,n,k", [(128, 128, 32), (300, 200, 64), (257, 130, 40), (1000, 777, 256),
+                                   (129, 1500, 224)])
+def test_tc_update_matches_fp64(fp, m, n, k):
+    err_tc, err_simt, ms = fp._capi.tc_selftest(m, n, k)
+    assert err_tc < 1e-6, (err_tc, err_simt)
+    assert err_tc <= 4 * err_simt + 1e-7, (err_tc, err_simt)
+
+
+def test_mixed_lu_refines_in_few_steps(fp, O, ctx):
+    """With the tensor-core update the FP32 factors stay FP32-accurate: the
+    FP64 refinement converges to 1e-12 in a handful of steps, without GMRES."""
+    w = fp.meshes.swept_wing("0012", 60, 80)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(4.2)
+    V = np.array([np.cos(a), 0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
+    assert st.used_gmres == 0 and st.ir_iters <= 5, st.asdict()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
