@@ -207,12 +207,13 @@ def run_ours(args, rank, ws, dist):
 
     # warm-up
     for _ in range(args.warmup):
-        device_step("mixed")
-        device_step("fp64")
+        for prec in (("mixed", "fp64") if args.precision == "both" else (args.precision,)):
+            device_step(prec)
     launches0 = ctx.kernel_launches()
     res = {}
+    precs = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     with ClockSampler(device) as clk:
-        for prec in ("mixed", "fp64"):
+        for prec in precs:
             barrier(dist)
             tot, stages = 0.0, np.zeros(3)
             for _ in range(args.steps):
@@ -221,15 +222,15 @@ def run_ours(args, rank, ws, dist):
                 stages += [st.ms_assemble, st.ms_factor, st.ms_solve]
             res[prec] = (max_over_ranks(dist, tot / args.steps), stages / args.steps, st)
     launches = ctx.kernel_launches() - launches0
-    ms_mixed, stg_m, st_m = res["mixed"]
-    ms_fp64, stg_d, st_d = res["fp64"]
     if args.profile:
         if rank == 0:
-            print(json.dumps({"profile": True, "mixed_ms": ms_mixed, "fp64_ms": ms_fp64,
-                              "stages_mixed": stg_m.tolist(), "stages_fp64": stg_d.tolist(),
-                              "ir_iters": st_m.ir_iters, "launches": launches}), flush=True)
+            print(json.dumps({"profile": True, "launches": launches,
+                              **{p: {"ms": res[p][0], "stages": res[p][1].tolist(), "ir_iters": res[p][2].ir_iters}
+                                 for p in res}}), flush=True)
         ctx.close()
         return
+    ms_mixed, stg_m, st_m = res["mixed"]
+    ms_fp64, stg_d, st_d = res["fp64"]
 
     # e2e through the public C ABI with host buffers
     e2e = []
@@ -301,6 +302,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="with --profile: which form to time")
     ap.add_argument("--profile", action="store_true",
                     help="timed device steps only (for ncu launch lists): no e2e, accuracy or CPU legs")
     args = ap.parse_args()

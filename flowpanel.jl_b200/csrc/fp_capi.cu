@@ -89,6 +89,7 @@ int time_end(fp_ctx* c, double* ms) {
 void free_matrices(fp_ctx* c) {
   dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
   dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_part);
+  if (c->d_linv) { cudaFree(c->d_linv); c->d_linv = nullptr; }
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
   dfree(c->d_V); dfree(c->d_h);
   for (int i = 0; i < 4; ++i) dfree(c->d_tc[i]);
@@ -368,6 +369,7 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
   if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, c->N * sizeof(int32_t)));
   if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * c->N * sizeof(double)));
+  if (!c->d_linv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_linv, (size_t)kLuNB * kLuNB * sizeof(double)));
   if (precision == FP_PREC_FP64) {
     if (!c->d_LU) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_LU, elems * sizeof(double)));
     if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));

@@ -31,21 +31,25 @@ constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
 template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
 
 // ----------------------------------------------------------------------------
-// (1) diagonal-block factorisation (redundant per CTA) + L21 slab solve
+// (1) diagonal-block factorisation (redundant per CTA) + L21 slab solve.
+// CTA 0 also writes the factored block, the pivots and inv(L11) (for (2)).
 template <class T>
 __global__ void __launch_bounds__(kPanelThreads)
 k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
-        float* __restrict__ cert, int* __restrict__ status) {
+        float* __restrict__ cert, int* __restrict__ status, T* __restrict__ linv) {
   __shared__ T S[NB][NB + 1];   // S[c][r]: column-major with padding
   __shared__ int piv_s;
   __shared__ int lpiv[NB];
   __shared__ float red[kPanelThreads / 32];
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tr = tid & (NB - 1);          // row owned in the 2-D update
+  const int tc = tid / NB;                // column phase (kPanelThreads / NB of them)
+  constexpr int CP = kPanelThreads / NB;
 
   // load the diagonal block (padding: identity)
   for (int q = tid; q < NB * NB; q += kPanelThreads) {
-    const int r = q % NB, cc = q / NB;
+    const int r = q & (NB - 1), cc = q / NB;
     T v;
     if (r < nb && cc < nb) v = A[(k + cc) * lda + (k + r)];
     else v = (r == cc) ? T(1) : T(0);
@@ -80,28 +84,42 @@ k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restric
     const T pv = S[j][j];
     if (pv == T(0)) {
       if (blockIdx.x == 0 && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-    } else {
-      const T rp = T(1) / pv;
-      for (int r = j + 1 + tid; r < nb; r += kPanelThreads) S[j][r] *= rp;
+    } else if (tc == 0 && tr > j && tr < nb) {
+      S[j][tr] *= T(1) / pv;
     }
     __syncthreads();
-    const int m = nb - j - 1;
-    for (int q = tid; q < m * m; q += kPanelThreads) {
-      const int r = j + 1 + q % m, cc = j + 1 + q / m;
-      S[cc][r] -= S[j][r] * S[cc][j];
+    // rank-1 update of the trailing block: thread (tr, tc) owns row tr, columns j+1+tc, +CP, ...
+    if (tr > j && tr < nb) {
+      const T l = S[j][tr];
+      for (int cc = j + 1 + tc; cc < nb; cc += CP) S[cc][tr] -= l * S[cc][j];
     }
     __syncthreads();
   }
 
   if (blockIdx.x == 0) {
-    for (int q = tid; q < nb * nb; q += kPanelThreads) {
-      const int r = q % nb, cc = q / nb;
-      A[(k + cc) * lda + (k + r)] = S[cc][r];
+    for (int q = tid; q < NB * NB; q += kPanelThreads) {
+      const int r = q & (NB - 1), cc = q / NB;
+      if (r < nb && cc < nb) A[(k + cc) * lda + (k + r)] = S[cc][r];
     }
     for (int j = tid; j < nb; j += kPanelThreads) ipiv[k + j] = (int32_t)(k + lpiv[j]);
+    // inv(L11), column t by thread t (right-looking, independent updates)
+    if (tid < NB) {
+      T x[NB];
+#pragma unroll
+      for (int r = 0; r < NB; ++r) x[r] = (r == tid) ? T(1) : T(0);
+#pragma unroll
+      for (int j = 0; j < NB; ++j) {
+        const T xj = x[j];
+#pragma unroll
+        for (int r = j + 1; r < NB; ++r) x[r] -= S[j][r] * xj;
+      }
+#pragma unroll
+      for (int r = 0; r < NB; ++r) linv[tid * NB + r] = x[r];
+    }
   }
 
-  // L21 rows of this CTA: x U11 = a
+  // L21 rows of this CTA: x U11 = a, right-looking (the order of a right-side
+  // upper-triangular TRSM): x_j = a_j / U_jj, then a_l -= x_j U_jl for l > j.
   const int64_t r0 = k + nb + (int64_t)blockIdx.x * kPanelThreads;
   const int64_t r = r0 + tid;
   float lmax = 0.f;
@@ -112,12 +130,11 @@ k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restric
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       if (j < nb) {
-        T s = x[j];
+        const T xj = x[j] / S[j][j];
+        x[j] = xj;
+        lmax = fmaxf(lmax, (float)tabs(xj));
 #pragma unroll
-        for (int l = 0; l < j; ++l) s -= x[l] * S[j][l];
-        s = s / S[j][j];
-        x[j] = s;
-        lmax = fmaxf(lmax, (float)tabs(s));
+        for (int l = j + 1; l < NB; ++l) x[l] -= xj * S[l][j];
       }
     }
 #pragma unroll
@@ -137,51 +154,62 @@ k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restric
 }
 
 // ----------------------------------------------------------------------------
-// (2) row swaps of the block on all other columns; U12 = L11^-1 A12 for the
-// columns right of the block. One warp per column, L11 in shared memory.
-constexpr int kSwapWarps = 4;
+// (2) row swaps of the block on all other columns; U12 = inv(L11) P A12 for
+// the columns right of the block, as a product with the inverse written by
+// k_panel (no sequential substitution). 32 columns per CTA iteration.
+constexpr int kSwapThreads = 256;
+template <class T> constexpr int swap_cols() { return sizeof(T) == 8 ? 16 : 32; }
 template <class T>
-__global__ void __launch_bounds__(kSwapWarps * 32)
-k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv) {
-  __shared__ T L[NB][NB + 1];      // L[c][r]
-  __shared__ T col[kSwapWarps][NB];
-  __shared__ int lp[NB];
+__global__ void __launch_bounds__(kSwapThreads)
+k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv,
+           const T* __restrict__ linv) {
+  __shared__ T Li[NB][NB + 1];          // Li[l][r] = inv(L11)(r, l)
+  constexpr int kSwapCols = swap_cols<T>();
+  __shared__ T tile[kSwapCols][NB + 1]; // tile[cc][r] = A(k + r, c)
+  __shared__ int perm[NB];
   const int nb = (int)imin64(NB, n - k);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int q = tid; q < nb * nb; q += blockDim.x) {
-    const int r = q % nb, cc = q / nb;
-    L[cc][r] = A[(k + cc) * lda + (k + r)];
+  const int tid = threadIdx.x;
+  for (int q = tid; q < NB * NB; q += kSwapThreads) {
+    const int r = q & (NB - 1), l = q / NB;
+    Li[l][r] = (r < nb && l < nb) ? linv[l * NB + r] : ((r == l) ? T(1) : T(0));
   }
-  for (int j = tid; j < nb; j += blockDim.x) lp[j] = (int)(ipiv[k + j] - k);
+  if (tid == 0) {
+    for (int j = 0; j < NB; ++j) perm[j] = j;
+    for (int j = 0; j < nb; ++j) {
+      const int p = (int)(ipiv[k + j] - k);
+      const int t0 = perm[j]; perm[j] = perm[p]; perm[p] = t0;
+    }
+  }
   __syncthreads();
-  const int64_t nother = n - nb;   // columns outside the diagonal block
-  for (int64_t q = (int64_t)blockIdx.x * kSwapWarps + warp; q < nother; q += (int64_t)gridDim.x * kSwapWarps) {
-    const int64_t c = (q < k) ? q : q + nb;
-    T* colp = A + c * lda + k;
-    for (int r = lane; r < nb; r += 32) col[warp][r] = colp[r];
-    __syncwarp();
-    if (lane == 0) {
-      for (int j = 0; j < nb; ++j) {
-        const int p = lp[j];
-        if (p != j) { const T t0 = col[warp][j]; col[warp][j] = col[warp][p]; col[warp][p] = t0; }
+  const int64_t nother = n - nb;
+  const int64_t ngroups = (nother + kSwapCols - 1) / kSwapCols;
+  for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
+    for (int e = tid; e < NB * kSwapCols; e += kSwapThreads) {
+      const int r = e & (NB - 1), cc = e / NB;
+      const int64_t q = g * kSwapCols + cc;
+      T v = T(0);
+      if (q < nother && r < nb) {
+        const int64_t c = (q < k) ? q : q + nb;
+        v = A[c * lda + k + r];
       }
+      tile[cc][r] = v;
     }
-    __syncwarp();
-    if (c >= k + nb) {
-      // forward substitution with the unit lower L11; lanes own rows lane, lane+32
-      T x0 = (lane < nb) ? col[warp][lane] : T(0);
-      T x1 = (lane + 32 < nb) ? col[warp][lane + 32] : T(0);
-      for (int j = 0; j < nb; ++j) {
-        const T xj = __shfl_sync(0xffffffffu, (j < 32) ? x0 : x1, j & 31);
-        if (lane > j) x0 -= L[j][lane] * xj;
-        if (lane + 32 > j && lane + 32 < nb) x1 -= L[j][lane + 32] * xj;
+    __syncthreads();
+    for (int e = tid; e < NB * kSwapCols; e += kSwapThreads) {
+      const int r = e & (NB - 1), cc = e / NB;
+      const int64_t q = g * kSwapCols + cc;
+      if (q >= nother || r >= nb) continue;
+      const int64_t c = (q < k) ? q : q + nb;
+      T out;
+      if (c < k) {
+        out = tile[cc][perm[r]];
+      } else {
+        out = T(0);
+        for (int l = 0; l <= r; ++l) out += Li[l][r] * tile[cc][perm[l]];
       }
-      if (lane < nb) col[warp][lane] = x0;
-      if (lane + 32 < nb) col[warp][lane + 32] = x1;
-      __syncwarp();
+      A[c * lda + k + r] = out;
     }
-    for (int r = lane; r < nb; r += 32) colp[r] = col[warp][r];
-    __syncwarp();
+    __syncthreads();
   }
 }
 
@@ -294,13 +322,14 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
       const unsigned g1 = (unsigned)std::max<int64_t>(1, (below + kPanelThreads - 1) / kPanelThreads);
-      k_panel<T><<<g1, kPanelThreads, 0, c->stream>>>(A, lda, n, k, ipiv, cert, c->d_status);
+      T* linv = reinterpret_cast<T*>(c->d_linv);
+      k_panel<T><<<g1, kPanelThreads, 0, c->stream>>>(A, lda, n, k, ipiv, cert, c->d_status, linv);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
       if (n - nb > 0) {
         const int64_t nother = n - nb;
-        const unsigned g2 = (unsigned)std::min<int64_t>((nother + kSwapWarps - 1) / kSwapWarps, 4 * 148);
-        k_swap_u12<T><<<g2, kSwapWarps * 32, 0, c->stream>>>(A, lda, n, k, ipiv);
+        const unsigned g2 = (unsigned)std::min<int64_t>((nother + swap_cols<T>() - 1) / swap_cols<T>(), 2 * num_sms());
+        k_swap_u12<T><<<g2, kSwapThreads, 0, c->stream>>>(A, lda, n, k, ipiv, linv);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }

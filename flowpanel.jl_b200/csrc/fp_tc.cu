@@ -128,6 +128,16 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
+  // Prefetch this thread's row of the C tile (warp w owns rows 32w..32w+31):
+  // the loads are in flight while the operands stream in and the MMAs run.
+  const int row = m0 + warp * 32 + lane;
+  const bool row_ok = row < m;
+  const int ncol = min(BN, n - n0);
+  constexpr int HALF = BN / 2;
+  float cv[HALF];
+#pragma unroll
+  for (int j = 0; j < HALF; ++j) cv[j] = (row_ok && j < ncol) ? C[(int64_t)(n0 + j) * ldc + row] : 0.f;
+
   if (warp == 0 && lane == 0) {
     // producer
     int issued = 0;
@@ -170,27 +180,38 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     if (ok) umma_commit(done);
   }
   __syncwarp();
-  // epilogue: every warp waits for the accumulator
+  // epilogue: every warp waits for the accumulator, subtracts it from its rows
   const bool ok = mbar_wait(done, 0);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
-    const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
-    for (int cc = 0; cc < BN; cc += 16) {
-      uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < m) {
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1) {
+        // second half: its loads overlap the first half's stores
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int col = n0 + cc + j;
-          if (col < n) C[(int64_t)col * ldc + row] -= __uint_as_float(r[j]);
-        }
+        for (int j = 0; j < HALF; ++j)
+          cv[j] = (row_ok && HALF + j < ncol) ? C[(int64_t)(n0 + HALF + j) * ldc + row] : 0.f;
+      }
+#pragma unroll
+      for (int cc = 0; cc < HALF; cc += 32) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * HALF + cc);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+            "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 32; ++j) cv[cc + j] -= __uint_as_float(r[j]);
+      }
+      if (row_ok) {
+#pragma unroll
+        for (int j = 0; j < HALF; ++j)
+          if (h * HALF + j < ncol) C[(int64_t)(n0 + h * HALF + j) * ldc + row] = cv[j];
       }
     }
   } else if (threadIdx.x == 0) {
