@@ -158,7 +158,7 @@ k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restric
 // the columns right of the block, as a product with the inverse written by
 // k_panel (no sequential substitution). 32 columns per CTA iteration.
 constexpr int kSwapThreads = 256;
-template <class T> constexpr int swap_cols() { return sizeof(T) == 8 ? 16 : 32; }
+template <class T> __host__ __device__ constexpr int swap_cols() { return sizeof(T) == 8 ? 16 : 32; }
 template <class T>
 __global__ void __launch_bounds__(kSwapThreads)
 k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv,
