@@ -31,162 +31,222 @@ constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
 template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
 
 // ----------------------------------------------------------------------------
-// (1) diagonal-block factorisation (redundant per CTA) + L21 slab solve.
-// CTA 0 also writes the factored block, the pivots and inv(L11) (for (2)).
+// (1) k_diag: one CTA of NB threads factors the NB x NB diagonal block with
+// partial pivoting over its rows. Thread r holds row r in registers; per
+// pivot step: argmax over the column (warp shuffles + one exchange through
+// shared memory), the pivot row and row j swap through shared memory, every
+// row below updates itself from the broadcast pivot row. The step loop stays
+// rolled (it holds barriers); register accesses are predicated sweeps with
+// static indices. Writes back the block and the pivots, and inv(L11),
+// inv(U11) to `work` for (2).
 template <class T>
-__global__ void __launch_bounds__(kPanelThreads)
-k_panel(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
-        float* __restrict__ cert, int* __restrict__ status, T* __restrict__ linv) {
-  __shared__ T S[NB][NB + 1];   // S[c][r]: column-major with padding
-  __shared__ int piv_s;
+__global__ void __launch_bounds__(NB)
+k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
+       int* __restrict__ status, T* __restrict__ work) {
+  __shared__ T S[NB][NB + 1];        // factored block, S[c][r]
+  __shared__ T urow[NB];             // pivot row of the current step
+  __shared__ T jrow[NB];             // row j before the swap
+  __shared__ T wbest[2];
+  __shared__ int wbi[2];
   __shared__ int lpiv[NB];
-  __shared__ float red[kPanelThreads / 32];
   const int nb = (int)imin64(NB, n - k);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tr = tid & (NB - 1);          // row owned in the 2-D update
-  const int tc = tid / NB;                // column phase (kPanelThreads / NB of them)
-  constexpr int CP = kPanelThreads / NB;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
 
-  // load the diagonal block (padding: identity)
-  for (int q = tid; q < NB * NB; q += kPanelThreads) {
-    const int r = q & (NB - 1), cc = q / NB;
-    T v;
-    if (r < nb && cc < nb) v = A[(k + cc) * lda + (k + r)];
-    else v = (r == cc) ? T(1) : T(0);
-    S[cc][r] = v;
-  }
-  __syncthreads();
+  T a[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c)
+    a[c] = (t < nb && c < nb) ? A[(k + c) * lda + (k + t)] : ((t == c) ? T(1) : T(0));
 
+  bool zero = false;
+#pragma unroll 1
   for (int j = 0; j < nb; ++j) {
-    if (warp == 0) {
-      T best = T(-1);
-      int bi = j;
-      for (int r = j + lane; r < nb; r += 32) {
-        const T v = tabs(S[j][r]);
-        if (v > best) { best = v; bi = r; }
-      }
+    T aj = T(0);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const T ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    for (int c = 0; c < NB; ++c)
+      if (c == j) aj = a[c];
+    // argmax |a[j]| over rows j..nb-1 (first index on ties, like idamax)
+    T best = (t >= j && t < nb) ? tabs(aj) : T(-1);
+    int bi = t;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; }
+    __syncthreads();
+    int p = wbi[0];
+    if (wbest[1] > wbest[0] || (wbest[1] == wbest[0] && wbi[1] < wbi[0])) p = wbi[1];
+    if (t == p) {
+#pragma unroll
+      for (int c = 0; c < NB; ++c) urow[c] = a[c];
+    }
+    if (t == j && p != j) {
+#pragma unroll
+      for (int c = 0; c < NB; ++c) jrow[c] = a[c];
+    }
+    if (t == 0) lpiv[j] = p;
+    __syncthreads();
+    if (p != j) {
+      if (t == j) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c) a[c] = urow[c];
+      } else if (t == p) {
+#pragma unroll
+        for (int c = 0; c < NB; ++c) a[c] = jrow[c];
       }
-      if (lane == 0) { piv_s = bi; lpiv[j] = bi; }
     }
-    __syncthreads();
-    const int p = piv_s;
-    if (p != j && tid < NB) {
-      const T t0 = S[tid][j];
-      S[tid][j] = S[tid][p];
-      S[tid][p] = t0;
-    }
-    __syncthreads();
-    const T pv = S[j][j];
+    const T pv = urow[j];
     if (pv == T(0)) {
-      if (blockIdx.x == 0 && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-    } else if (tc == 0 && tr > j && tr < nb) {
-      S[j][tr] *= T(1) / pv;
-    }
-    __syncthreads();
-    // rank-1 update of the trailing block: thread (tr, tc) owns row tr, columns j+1+tc, +CP, ...
-    if (tr > j && tr < nb) {
-      const T l = S[j][tr];
-      for (int cc = j + 1 + tc; cc < nb; cc += CP) S[cc][tr] -= l * S[cc][j];
-    }
-    __syncthreads();
-  }
-
-  if (blockIdx.x == 0) {
-    for (int q = tid; q < NB * NB; q += kPanelThreads) {
-      const int r = q & (NB - 1), cc = q / NB;
-      if (r < nb && cc < nb) A[(k + cc) * lda + (k + r)] = S[cc][r];
-    }
-    for (int j = tid; j < nb; j += kPanelThreads) ipiv[k + j] = (int32_t)(k + lpiv[j]);
-    // inv(L11), column t by thread t (right-looking, independent updates)
-    if (tid < NB) {
-      T x[NB];
+      zero = true;
+    } else if (t > j && t < nb) {
+      T l = T(0);
 #pragma unroll
-      for (int r = 0; r < NB; ++r) x[r] = (r == tid) ? T(1) : T(0);
+      for (int c = 0; c < NB; ++c)
+        if (c == j) l = a[c] * (T(1) / pv);
 #pragma unroll
-      for (int j = 0; j < NB; ++j) {
-        const T xj = x[j];
-#pragma unroll
-        for (int r = j + 1; r < NB; ++r) x[r] -= S[j][r] * xj;
-      }
-#pragma unroll
-      for (int r = 0; r < NB; ++r) linv[tid * NB + r] = x[r];
-    }
-  }
-
-  // L21 rows of this CTA: x U11 = a, right-looking (the order of a right-side
-  // upper-triangular TRSM): x_j = a_j / U_jj, then a_l -= x_j U_jl for l > j.
-  const int64_t r0 = k + nb + (int64_t)blockIdx.x * kPanelThreads;
-  const int64_t r = r0 + tid;
-  float lmax = 0.f;
-  if (r < n) {
-    T x[NB];
-#pragma unroll
-    for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? A[(k + j) * lda + r] : T(0);
-#pragma unroll
-    for (int j = 0; j < NB; ++j) {
-      if (j < nb) {
-        const T xj = x[j] / S[j][j];
-        x[j] = xj;
-        lmax = fmaxf(lmax, (float)tabs(xj));
-#pragma unroll
-        for (int l = j + 1; l < NB; ++l) x[l] -= xj * S[l][j];
+      for (int c = 0; c < NB; ++c) {
+        if (c == j) a[c] = l;
+        else if (c > j) a[c] -= l * urow[c];
       }
     }
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-      if (j < nb) A[(k + j) * lda + r] = x[j];
   }
-  // block max -> certificate
+  if (zero && t == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-  if (lane == 0) red[warp] = lmax;
+  for (int c = 0; c < NB; ++c) S[c][t] = a[c];
+  if (t < nb) {
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+      if (c < nb) A[(k + c) * lda + (k + t)] = a[c];
+  }
   __syncthreads();
-  if (tid == 0) {
-    float mm = red[0];
-    for (int w = 1; w < kPanelThreads / 32; ++w) mm = fmaxf(mm, red[w]);
-    if (mm > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(mm));
+  if (t < nb) ipiv[k + t] = (int32_t)(k + lpiv[t]);
+  // inv(L11) column t: x_r -= L(r, j) x_j for r > j (right-looking)
+#pragma unroll
+  for (int r = 0; r < NB; ++r) a[r] = (r == t) ? T(1) : T(0);
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    const T xj = a[j];
+#pragma unroll
+    for (int r = j + 1; r < NB; ++r) a[r] -= S[j][r] * xj;
   }
+  T* Li = work;
+  T* Ui = work + NB * NB;
+#pragma unroll
+  for (int r = 0; r < NB; ++r) Li[t * NB + r] = a[r];
+  // inv(U11) column t: x_j /= U(j, j); x_r -= U(r, j) x_j for r < j (backward)
+#pragma unroll
+  for (int r = 0; r < NB; ++r) a[r] = (r == t) ? T(1) : T(0);
+#pragma unroll
+  for (int j = NB - 1; j >= 0; --j) {
+    const T xj = a[j] / S[j][j];
+    a[j] = xj;
+#pragma unroll
+    for (int r = 0; r < j; ++r) a[r] -= S[j][r] * xj;
+  }
+#pragma unroll
+  for (int r = 0; r < NB; ++r) Ui[t * NB + r] = a[r];
 }
 
 // ----------------------------------------------------------------------------
-// (2) row swaps of the block on all other columns; U12 = inv(L11) P A12 for
-// the columns right of the block, as a product with the inverse written by
-// k_panel (no sequential substitution). 32 columns per CTA iteration.
-constexpr int kSwapThreads = 256;
-template <class T> __host__ __device__ constexpr int swap_cols() { return sizeof(T) == 8 ? 16 : 32; }
+// (2) k_apply, after k_diag; two kinds of CTA in one launch:
+//  * blockIdx < nrowblk: L21 = A21 inv(U11) for NB rows below the block, with
+//    max|L21| (the GEPP certificate);
+//  * the others: row swaps of the block on every other column and
+//    U12 = inv(L11) P A12 for the columns right of the block.
+// Both are small tiled products against an NB x NB inverse in shared memory.
+constexpr int kApplyThreads = 256;
+template <class T> __host__ __device__ constexpr int apply_cols() { return sizeof(T) == 8 ? 32 : 64; }
+template <class T> constexpr size_t apply_smem() {
+  return (size_t)NB * (NB + 1) * sizeof(T) + (size_t)apply_cols<T>() * (NB + 1) * sizeof(T) +
+         2 * NB * sizeof(int) + 64;
+}
+
 template <class T>
-__global__ void __launch_bounds__(kSwapThreads)
-k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv,
-           const T* __restrict__ linv) {
-  __shared__ T Li[NB][NB + 1];          // Li[l][r] = inv(L11)(r, l)
-  constexpr int kSwapCols = swap_cols<T>();
-  __shared__ T tile[kSwapCols][NB + 1]; // tile[cc][r] = A(k + r, c)
-  __shared__ int perm[NB];
+__global__ void __launch_bounds__(kApplyThreads)
+k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv,
+        const T* __restrict__ work, float* __restrict__ cert, int nrowblk) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  constexpr int CW = apply_cols<T>();
+  T (*M)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm);      // inverse, M[l][r] = inv(r, l)
+  T (*tile)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm + (size_t)NB * (NB + 1) * sizeof(T));
+  int* perm = reinterpret_cast<int*>(dsm + (size_t)NB * (NB + 1) * sizeof(T) + (size_t)CW * (NB + 1) * sizeof(T));
+  int* lp = perm + NB;
+  __shared__ float red[kApplyThreads / 32];
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x;
-  for (int q = tid; q < NB * NB; q += kSwapThreads) {
+  const bool l21 = (int)blockIdx.x < nrowblk;
+  const T* inv = l21 ? work + NB * NB : work;   // inv(U11) or inv(L11)
+  for (int q = tid; q < NB * NB; q += kApplyThreads) {
     const int r = q & (NB - 1), l = q / NB;
-    Li[l][r] = (r < nb && l < nb) ? linv[l * NB + r] : ((r == l) ? T(1) : T(0));
+    M[l][r] = (r < nb && l < nb) ? inv[l * NB + r] : ((r == l) ? T(1) : T(0));
   }
+  if (l21) {
+    // rows r0 .. r0+NB of L21: out(r, c) = sum_{l <= c} A21(r, l) inv(U)(l, c),
+    // A21 staged CW columns at a time in tile[l][r]
+    const int64_t r0 = k + nb + (int64_t)blockIdx.x * NB;
+    constexpr int PER = NB * NB / kApplyThreads;   // outputs per thread
+    T accv[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) accv[u] = T(0);
+    for (int h0 = 0; h0 < NB; h0 += CW) {
+      __syncthreads();
+      for (int q = tid; q < NB * CW; q += kApplyThreads) {
+        const int r = q & (NB - 1), l = q / NB;
+        const int64_t gr = r0 + r;
+        tile[l][r] = (gr < n && h0 + l < nb) ? A[(k + h0 + l) * lda + gr] : T(0);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int e = tid + u * kApplyThreads;
+        const int r = e & (NB - 1), c = e / NB;
+        T s0 = accv[u];
+        const int lend = min(CW, c + 1 - h0);
+        for (int l = 0; l < lend; ++l) s0 += tile[l][r] * M[c][h0 + l];
+        accv[u] = s0;
+      }
+    }
+    float lmax = 0.f;
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int e = tid + u * kApplyThreads;
+      const int r = e & (NB - 1), c = e / NB;
+      const int64_t gr = r0 + r;
+      if (gr < n && c < nb) {
+        A[(k + c) * lda + gr] = accv[u];
+        lmax = fmaxf(lmax, (float)tabs(accv[u]));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if ((tid & 31) == 0) red[tid >> 5] = lmax;
+    __syncthreads();
+    if (tid == 0) {
+      float mm = red[0];
+      for (int w = 1; w < kApplyThreads / 32; ++w) mm = fmaxf(mm, red[w]);
+      if (mm > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(mm));
+    }
+    return;
+  }
+  // swaps + U12
+  if (tid < nb) lp[tid] = (int)(ipiv[k + tid] - k);
+  __syncthreads();
   if (tid == 0) {
     for (int j = 0; j < NB; ++j) perm[j] = j;
     for (int j = 0; j < nb; ++j) {
-      const int p = (int)(ipiv[k + j] - k);
+      const int p = lp[j];
       const int t0 = perm[j]; perm[j] = perm[p]; perm[p] = t0;
     }
   }
   __syncthreads();
   const int64_t nother = n - nb;
-  const int64_t ngroups = (nother + kSwapCols - 1) / kSwapCols;
-  for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
-    for (int e = tid; e < NB * kSwapCols; e += kSwapThreads) {
+  const int64_t ngroups = (nother + CW - 1) / CW;
+  const int nblocks = (int)gridDim.x - nrowblk;
+  for (int64_t g = (int)blockIdx.x - nrowblk; g < ngroups; g += nblocks) {
+    for (int e = tid; e < NB * CW; e += kApplyThreads) {
       const int r = e & (NB - 1), cc = e / NB;
-      const int64_t q = g * kSwapCols + cc;
+      const int64_t q = g * CW + cc;
       T v = T(0);
       if (q < nother && r < nb) {
         const int64_t c = (q < k) ? q : q + nb;
@@ -195,9 +255,9 @@ k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* 
       tile[cc][r] = v;
     }
     __syncthreads();
-    for (int e = tid; e < NB * kSwapCols; e += kSwapThreads) {
+    for (int e = tid; e < NB * CW; e += kApplyThreads) {
       const int r = e & (NB - 1), cc = e / NB;
-      const int64_t q = g * kSwapCols + cc;
+      const int64_t q = g * CW + cc;
       if (q >= nother || r >= nb) continue;
       const int64_t c = (q < k) ? q : q + nb;
       T out;
@@ -205,7 +265,7 @@ k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* 
         out = tile[cc][perm[r]];
       } else {
         out = T(0);
-        for (int l = 0; l <= r; ++l) out += Li[l][r] * tile[cc][perm[l]];
+        for (int l = 0; l <= r; ++l) out += M[l][r] * tile[cc][perm[l]];
       }
       A[c * lda + k + r] = out;
     }
@@ -214,56 +274,88 @@ k_swap_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* 
 }
 
 // ----------------------------------------------------------------------------
-// (3) trailing update C -= A B, SIMT register tiles (FP64 path).
+// (3) trailing update C -= A B, SIMT register tiles (the FP64 path). Global
+// loads of the next K slice go to registers while the current slice is
+// multiplied from shared memory (double buffer). Consecutive threads own
+// consecutive rows, so the C read-modify-write is coalesced.
 template <class T, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ Cm, int64_t lda,
            int64_t m, int64_t nn, int kk) {
   constexpr int NT = (BM / TM) * (BN / TN);
-  __shared__ T As[BK][BM + 1];
-  __shared__ T Bs[BK][BN + 1];
+  constexpr int LA = BK * BM / NT;
+  constexpr int LB = BK * BN / NT;
+  constexpr int TX = BM / TM;
+  __shared__ T As[2][BK][BM + 2];
+  __shared__ T Bs[2][BK][BN + 2];
   const int tid = threadIdx.x;
-  const int tx = tid % (BN / TN), ty = tid / (BN / TN);
+  const int tx = tid % TX, ty = tid / TX;
   const int64_t i0 = (int64_t)blockIdx.x * BM, j0 = (int64_t)blockIdx.y * BN;
   T acc[TM][TN];
 #pragma unroll
   for (int a = 0; a < TM; ++a)
 #pragma unroll
     for (int b = 0; b < TN; ++b) acc[a][b] = T(0);
-  for (int k0 = 0; k0 < kk; k0 += BK) {
-    for (int q = tid; q < BK * BM; q += NT) {
+  T ra[LA], rb[LB];
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < LA; ++u) {
+      const int q = tid + u * NT;
       const int ii = q % BM, kq = q / BM;
       const int64_t gi = i0 + ii;
-      As[kq][ii] = (gi < m && k0 + kq < kk) ? Am[(int64_t)(k0 + kq) * lda + gi] : T(0);
+      ra[u] = (gi < m && k0 + kq < kk) ? Am[(int64_t)(k0 + kq) * lda + gi] : T(0);
     }
-    for (int q = tid; q < BK * BN; q += NT) {
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int q = tid + u * NT;
       const int kq = q % BK, jj = q / BK;
       const int64_t gj = j0 + jj;
-      Bs[kq][jj] = (gj < nn && k0 + kq < kk) ? Bm[gj * lda + k0 + kq] : T(0);
+      rb[u] = (gj < nn && k0 + kq < kk) ? Bm[gj * lda + k0 + kq] : T(0);
     }
-    __syncthreads();
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int u = 0; u < LA; ++u) {
+      const int q = tid + u * NT;
+      As[buf][q / BM][q % BM] = ra[u];
+    }
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int q = tid + u * NT;
+      Bs[buf][q % BK][q / BK] = rb[u];
+    }
+  };
+  gload(0);
+  sstore(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = 0; k0 < kk; k0 += BK) {
+    const bool more = k0 + BK < kk;
+    if (more) gload(k0 + BK);
 #pragma unroll
     for (int kq = 0; kq < BK; ++kq) {
       T a[TM], b[TN];
 #pragma unroll
-      for (int u = 0; u < TM; ++u) a[u] = As[kq][ty + u * (BM / TM)];
+      for (int u = 0; u < TM; ++u) a[u] = As[buf][kq][tx + u * TX];
 #pragma unroll
-      for (int v = 0; v < TN; ++v) b[v] = Bs[kq][tx + v * (BN / TN)];
+      for (int v = 0; v < TN; ++v) b[v] = Bs[buf][kq][ty + v * (BN / TN)];
 #pragma unroll
       for (int u = 0; u < TM; ++u)
 #pragma unroll
         for (int v = 0; v < TN; ++v) acc[u][v] += a[u] * b[v];
     }
+    if (more) sstore(buf ^ 1);
     __syncthreads();
+    buf ^= 1;
   }
 #pragma unroll
-  for (int u = 0; u < TM; ++u) {
-    const int64_t gi = i0 + ty + u * (BM / TM);
-    if (gi >= m) continue;
+  for (int v = 0; v < TN; ++v) {
+    const int64_t gj = j0 + ty + v * (BN / TN);
+    if (gj >= nn) continue;
 #pragma unroll
-    for (int v = 0; v < TN; ++v) {
-      const int64_t gj = j0 + tx + v * (BN / TN);
-      if (gj < nn) Cm[gj * lda + gi] -= acc[u][v];
+    for (int u = 0; u < TM; ++u) {
+      const int64_t gi = i0 + tx + u * TX;
+      if (gi < m) Cm[gj * lda + gi] -= acc[u][v];
     }
   }
 }
@@ -279,7 +371,7 @@ template <class T>
 static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int64_t m, int64_t nn,
                     int kk) {
   if (m <= 0 || nn <= 0 || kk <= 0) return FP_OK;
-  if (sizeof(T) == 4) {
+  if constexpr (sizeof(T) == 4) {
     if (tc_gemm_sub_f32(c, (const float*)Am, (const float*)Bm, (float*)Cm, lda, m, nn, kk)) return FP_OK;
     constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
     dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
@@ -315,23 +407,27 @@ constexpr int kOuterNB = 256;
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
+  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem<T>()));
   auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
   for (int64_t K0 = 0; K0 < n; K0 += kOuterNB) {
     const int64_t kend = std::min<int64_t>(K0 + kOuterNB, n);
     for (int64_t k = K0; k < kend; k += NB) {
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
-      const unsigned g1 = (unsigned)std::max<int64_t>(1, (below + kPanelThreads - 1) / kPanelThreads);
-      T* linv = reinterpret_cast<T*>(c->d_linv);
-      k_panel<T><<<g1, kPanelThreads, 0, c->stream>>>(A, lda, n, k, ipiv, cert, c->d_status, linv);
+      T* work = reinterpret_cast<T*>(c->d_linv);
+      k_diag<T><<<1, NB, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, work);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
-      if (n - nb > 0) {
-        const int64_t nother = n - nb;
-        const unsigned g2 = (unsigned)std::min<int64_t>((nother + swap_cols<T>() - 1) / swap_cols<T>(), 2 * num_sms());
-        k_swap_u12<T><<<g2, kSwapThreads, 0, c->stream>>>(A, lda, n, k, ipiv, linv);
-        ++c->nlaunch;
-        FP_CUDA_TRY(c->err, cudaGetLastError());
+      {
+        const int nrowblk = (int)((below + NB - 1) / NB);
+        const int64_t ngroups = (n - nb + apply_cols<T>() - 1) / apply_cols<T>();
+        const int ncolblk = (int)std::min<int64_t>(ngroups, 2 * num_sms());
+        const unsigned g = (unsigned)(nrowblk + ncolblk);
+        if (g > 0) {
+          k_apply<T><<<g, kApplyThreads, apply_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, work, cert, nrowblk);
+          ++c->nlaunch;
+          FP_CUDA_TRY(c->err, cudaGetLastError());
+        }
       }
       const int64_t k1 = k + nb;
       // (a) remaining panel columns, full height
