@@ -369,7 +369,7 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
   if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, c->N * sizeof(int32_t)));
   if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * c->N * sizeof(double)));
-  if (!c->d_linv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_linv, (size_t)kLuNB * kLuNB * sizeof(double)));
+  if (!c->d_linv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_linv, (size_t)2 * kLuNB * kLuNB * sizeof(double)));
   if (precision == FP_PREC_FP64) {
     if (!c->d_LU) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_LU, elems * sizeof(double)));
     if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));

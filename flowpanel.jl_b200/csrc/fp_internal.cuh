@@ -59,7 +59,7 @@ struct fp_ctx {
   double* d_dinv64 = nullptr;           // inverses of the FP64 diagonal blocks
   float* d_dinv32 = nullptr;            // inverses of the FP32 diagonal blocks
   double* d_part = nullptr;             // GEMV partial sums
-  void* d_linv = nullptr;               // inv(L11) of the current block (NB x NB, FP64 size)
+  void* d_linv = nullptr;               // inv(L11), inv(U11) of the current block (2 x NB x NB, FP64 size)
   double* d_norms = nullptr;            // column norms (2 x cap_rhs)
   int64_t cap_rhs = 0;                  // allocated RHS columns
   size_t cap_flags = 0;
