@@ -31,121 +31,110 @@ constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
 template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
 
 // ----------------------------------------------------------------------------
-// (1) k_diag: one CTA of NB threads factors the NB x NB diagonal block with
-// partial pivoting over its rows. Thread r holds row r in registers; per
-// pivot step: argmax over the column (warp shuffles + one exchange through
-// shared memory), the pivot row and row j swap through shared memory, every
-// row below updates itself from the broadcast pivot row. The step loop stays
-// rolled (it holds barriers); register accesses are predicated sweeps with
-// static indices. Writes back the block and the pivots, and inv(L11),
-// inv(U11) to `work` for (2).
+// (1) k_diag: one CTA factors the NB x NB diagonal block with partial pivoting
+// over its rows, in shared memory. 256 threads: thread (r, q) owns row r and
+// the column quarter q of the trailing update. Per pivot step j, three phases
+// separated by barriers:
+//   A  argmax of |column j| over rows j..nb-1 (warps 0-1, shuffles), and the
+//      scaled multipliers of step j-1 written into column j-1;
+//   B  swap of rows j and p (one column per thread);
+//   C  rank-1 update of the columns right of j; each thread forms its row's
+//      multiplier itself, so column j is only written in the next phase A.
+// Writes back the block and the pivots, and inv(L11), inv(U11) to `work`.
+constexpr int kDiagThreads = 256;
 template <class T>
-__global__ void __launch_bounds__(NB)
+__global__ void __launch_bounds__(kDiagThreads)
 k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
        int* __restrict__ status, T* __restrict__ work) {
-  __shared__ T S[NB][NB + 1];        // factored block, S[c][r]
-  __shared__ T urow[NB];             // pivot row of the current step
-  __shared__ T jrow[NB];             // row j before the swap
+  __shared__ T S[NB][NB + 1];   // S[c][r]
+  __shared__ T lcol[NB];        // scaled multipliers of the previous step
   __shared__ T wbest[2];
   __shared__ int wbi[2];
   __shared__ int lpiv[NB];
   const int nb = (int)imin64(NB, n - k);
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-
-  T a[NB];
-#pragma unroll
-  for (int c = 0; c < NB; ++c)
-    a[c] = (t < nb && c < nb) ? A[(k + c) * lda + (k + t)] : ((t == c) ? T(1) : T(0));
-
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r = tid & (NB - 1), q = tid >> 6;   // q in 0..3, 16 columns each
+  for (int e = tid; e < NB * NB; e += kDiagThreads) {
+    const int rr = e & (NB - 1), cc = e >> 6;
+    S[cc][rr] = (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
+  }
+  __syncthreads();
   bool zero = false;
-#pragma unroll 1
   for (int j = 0; j < nb; ++j) {
-    T aj = T(0);
+    // phase A
+    if (tid < NB) {
+      if (j > 0 && r >= j && r < nb) S[j - 1][r] = lcol[r];
+      T best = (r >= j && r < nb) ? tabs(S[j][r]) : T(-1);
+      int bi = r;
 #pragma unroll
-    for (int c = 0; c < NB; ++c)
-      if (c == j) aj = a[c];
-    // argmax |a[j]| over rows j..nb-1 (first index on ties, like idamax)
-    T best = (t >= j && t < nb) ? tabs(aj) : T(-1);
-    int bi = t;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; }
     }
-    if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; }
     __syncthreads();
     int p = wbi[0];
     if (wbest[1] > wbest[0] || (wbest[1] == wbest[0] && wbi[1] < wbi[0])) p = wbi[1];
-    if (t == p) {
-#pragma unroll
-      for (int c = 0; c < NB; ++c) urow[c] = a[c];
+    // phase B
+    if (tid < NB && p != j) {
+      const T t0 = S[tid][j];
+      S[tid][j] = S[tid][p];
+      S[tid][p] = t0;
     }
-    if (t == j && p != j) {
-#pragma unroll
-      for (int c = 0; c < NB; ++c) jrow[c] = a[c];
-    }
-    if (t == 0) lpiv[j] = p;
+    if (tid == 0) lpiv[j] = p;
     __syncthreads();
-    if (p != j) {
-      if (t == j) {
-#pragma unroll
-        for (int c = 0; c < NB; ++c) a[c] = urow[c];
-      } else if (t == p) {
-#pragma unroll
-        for (int c = 0; c < NB; ++c) a[c] = jrow[c];
-      }
-    }
-    const T pv = urow[j];
+    // phase C
+    const T pv = S[j][j];
     if (pv == T(0)) {
       zero = true;
-    } else if (t > j && t < nb) {
-      T l = T(0);
+    } else if (r > j && r < nb) {
+      const T l = S[j][r] * (T(1) / pv);
+      if (q == 0) lcol[r] = l;
+      const int c0 = q * (NB / 4);
 #pragma unroll
-      for (int c = 0; c < NB; ++c)
-        if (c == j) l = a[c] * (T(1) / pv);
-#pragma unroll
-      for (int c = 0; c < NB; ++c) {
-        if (c == j) a[c] = l;
-        else if (c > j) a[c] -= l * urow[c];
+      for (int cc = 0; cc < NB / 4; ++cc) {
+        const int c = c0 + cc;
+        if (c > j && c < nb) S[c][r] -= l * S[c][j];
       }
     }
+    __syncthreads();
   }
-  if (zero && t == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-#pragma unroll
-  for (int c = 0; c < NB; ++c) S[c][t] = a[c];
-  if (t < nb) {
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-      if (c < nb) A[(k + c) * lda + (k + t)] = a[c];
-  }
+  if (zero && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
   __syncthreads();
-  if (t < nb) ipiv[k + t] = (int32_t)(k + lpiv[t]);
-  // inv(L11) column t: x_r -= L(r, j) x_j for r > j (right-looking)
-#pragma unroll
-  for (int r = 0; r < NB; ++r) a[r] = (r == t) ? T(1) : T(0);
-#pragma unroll
-  for (int j = 0; j < NB; ++j) {
-    const T xj = a[j];
-#pragma unroll
-    for (int r = j + 1; r < NB; ++r) a[r] -= S[j][r] * xj;
+  for (int e = tid; e < NB * NB; e += kDiagThreads) {
+    const int rr = e & (NB - 1), cc = e >> 6;
+    if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[cc][rr];
   }
-  T* Li = work;
-  T* Ui = work + NB * NB;
+  if (tid < nb) ipiv[k + tid] = (int32_t)(k + lpiv[tid]);
+  // inverses: warps 0-1 form inv(L11) (column tid), warps 2-3 inv(U11) (column tid - NB)
+  if (tid < 2 * NB) {
+    const bool low = tid < NB;
+    const int col = low ? tid : tid - NB;
+    T x[NB];
 #pragma unroll
-  for (int r = 0; r < NB; ++r) Li[t * NB + r] = a[r];
-  // inv(U11) column t: x_j /= U(j, j); x_r -= U(r, j) x_j for r < j (backward)
+    for (int rr = 0; rr < NB; ++rr) x[rr] = (rr == col) ? T(1) : T(0);
+    if (low) {
 #pragma unroll
-  for (int r = 0; r < NB; ++r) a[r] = (r == t) ? T(1) : T(0);
+      for (int jj = 0; jj < NB; ++jj) {
+        const T xj = x[jj];
 #pragma unroll
-  for (int j = NB - 1; j >= 0; --j) {
-    const T xj = a[j] / S[j][j];
-    a[j] = xj;
+        for (int rr = jj + 1; rr < NB; ++rr) x[rr] -= S[jj][rr] * xj;
+      }
+    } else {
 #pragma unroll
-    for (int r = 0; r < j; ++r) a[r] -= S[j][r] * xj;
+      for (int jj = NB - 1; jj >= 0; --jj) {
+        const T xj = x[jj] / S[jj][jj];
+        x[jj] = xj;
+#pragma unroll
+        for (int rr = 0; rr < jj; ++rr) x[rr] -= S[jj][rr] * xj;
+      }
+    }
+    T* dst = work + (low ? 0 : NB * NB) + col * NB;
+#pragma unroll
+    for (int rr = 0; rr < NB; ++rr) dst[rr] = x[rr];
   }
-#pragma unroll
-  for (int r = 0; r < NB; ++r) Ui[t * NB + r] = a[r];
 }
 
 // ----------------------------------------------------------------------------
@@ -415,7 +404,7 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
       T* work = reinterpret_cast<T*>(c->d_linv);
-      k_diag<T><<<1, NB, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, work);
+      k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, work);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
       {
