@@ -40,14 +40,22 @@ template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a
 //   B  swap of rows j and p (one column per thread);
 //   C  rank-1 update of the columns right of j; each thread forms its row's
 //      multiplier itself, so column j is only written in the next phase A.
-// Writes back the block and the pivots, and inv(L11), inv(U11) to `work`.
+// Then inv(L11) (threads 0-127) and inv(U11) (threads 128-255) by column
+// sweeps in shared memory, one barrier per step, and everything is written
+// out: the block and the pivots to A / ipiv, the inverses to `work`.
 constexpr int kDiagThreads = 256;
+constexpr int kDP = NB + 1;   // padded leading dimension in shared memory
+template <class T> constexpr size_t diag_smem() { return (size_t)3 * NB * kDP * sizeof(T); }
+
 template <class T>
 __global__ void __launch_bounds__(kDiagThreads)
 k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
        int* __restrict__ status, T* __restrict__ work) {
-  __shared__ T S[NB][NB + 1];   // S[c][r]
-  __shared__ T lcol[NB];        // scaled multipliers of the previous step
+  extern __shared__ __align__(16) unsigned char dsm_diag[];
+  T (*S)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag);                  // S[c][r]
+  T (*XL)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag + (size_t)NB * kDP * sizeof(T));      // XL[r][c]
+  T (*XU)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag + (size_t)2 * NB * kDP * sizeof(T));  // XU[r][c]
+  __shared__ T lcol[NB];
   __shared__ T wbest[2];
   __shared__ int wbi[2];
   __shared__ int lpiv[NB];
@@ -57,6 +65,8 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
     S[cc][rr] = (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
+    XL[cc][rr] = (rr == cc) ? T(1) : T(0);
+    XU[cc][rr] = (rr == cc) ? T(1) : T(0);
   }
   __syncthreads();
   bool zero = false;
@@ -102,39 +112,39 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
     __syncthreads();
   }
   if (zero && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
+  // inverses. Lower: step s = jj, X(rr, c) -= L(rr, jj) X(jj, c) for rr > jj, c <= jj.
+  // Upper: step s, jj = NB-1-s: row jj+1 is divided by U(jj+1, jj+1) (deferred so
+  // that it is not read and written in one phase), and
+  // X(rr, c) -= U(rr, jj) / U(jj, jj) X(jj, c) for rr < jj, c >= jj.
+  const bool lowg = tid < 2 * NB;
+  const int lt = lowg ? tid : tid - 2 * NB;
+  const int tr = lt & (NB - 1), tc = lt >> 6;   // tc in 0..1
+  for (int s = 0; s < NB; ++s) {
+    if (lowg) {
+      const int jj = s;
+      if (tr > jj) {
+        const T lv = S[jj][tr];
+        for (int c = tc; c <= jj; c += 2) XL[tr][c] -= lv * XL[jj][c];
+      }
+    } else {
+      const int jj = NB - 1 - s;
+      if (s > 0 && tc == 0 && tr >= jj + 1) XU[jj + 1][tr] *= T(1) / S[jj + 1][jj + 1];
+      if (tr < jj) {
+        const T uv = S[jj][tr] / S[jj][jj];
+        for (int c = jj + tc; c < NB; c += 2) XU[tr][c] -= uv * XU[jj][c];
+      }
+    }
+    __syncthreads();
+  }
+  if (!lowg && tc == 0) XU[0][tr] *= T(1) / S[0][0];
   __syncthreads();
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
     if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[cc][rr];
+    work[cc * NB + rr] = XL[rr][cc];
+    work[NB * NB + cc * NB + rr] = XU[rr][cc];
   }
   if (tid < nb) ipiv[k + tid] = (int32_t)(k + lpiv[tid]);
-  // inverses: warps 0-1 form inv(L11) (column tid), warps 2-3 inv(U11) (column tid - NB)
-  if (tid < 2 * NB) {
-    const bool low = tid < NB;
-    const int col = low ? tid : tid - NB;
-    T x[NB];
-#pragma unroll
-    for (int rr = 0; rr < NB; ++rr) x[rr] = (rr == col) ? T(1) : T(0);
-    if (low) {
-#pragma unroll
-      for (int jj = 0; jj < NB; ++jj) {
-        const T xj = x[jj];
-#pragma unroll
-        for (int rr = jj + 1; rr < NB; ++rr) x[rr] -= S[jj][rr] * xj;
-      }
-    } else {
-#pragma unroll
-      for (int jj = NB - 1; jj >= 0; --jj) {
-        const T xj = x[jj] / S[jj][jj];
-        x[jj] = xj;
-#pragma unroll
-        for (int rr = 0; rr < jj; ++rr) x[rr] -= S[jj][rr] * xj;
-      }
-    }
-    T* dst = work + (low ? 0 : NB * NB) + col * NB;
-#pragma unroll
-    for (int rr = 0; rr < NB; ++rr) dst[rr] = x[rr];
-  }
 }
 
 // ----------------------------------------------------------------------------
@@ -143,12 +153,13 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
 //    max|L21| (the GEPP certificate);
 //  * the others: row swaps of the block on every other column and
 //    U12 = inv(L11) P A12 for the columns right of the block.
-// Both are small tiled products against an NB x NB inverse in shared memory.
+// Both are NB x NB x NB products against an inverse in shared memory; each
+// thread computes a 4 x 4 register tile (rows tx+16i, columns ty+16j), so
+// consecutive threads touch consecutive rows of the column-major matrix.
 constexpr int kApplyThreads = 256;
-template <class T> __host__ __device__ constexpr int apply_cols() { return sizeof(T) == 8 ? 32 : 64; }
+constexpr int kAP = NB + 1;
 template <class T> constexpr size_t apply_smem() {
-  return (size_t)NB * (NB + 1) * sizeof(T) + (size_t)apply_cols<T>() * (NB + 1) * sizeof(T) +
-         2 * NB * sizeof(int) + 64;
+  return (size_t)2 * NB * kAP * sizeof(T) + 2 * NB * sizeof(int) + 64;
 }
 
 template <class T>
@@ -156,55 +167,57 @@ __global__ void __launch_bounds__(kApplyThreads)
 k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv,
         const T* __restrict__ work, float* __restrict__ cert, int nrowblk) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  constexpr int CW = apply_cols<T>();
-  T (*M)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm);      // inverse, M[l][r] = inv(r, l)
-  T (*tile)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm + (size_t)NB * (NB + 1) * sizeof(T));
-  int* perm = reinterpret_cast<int*>(dsm + (size_t)NB * (NB + 1) * sizeof(T) + (size_t)CW * (NB + 1) * sizeof(T));
+  T (*M)[kAP] = reinterpret_cast<T (*)[kAP]>(dsm);                                   // M[l][r] = inv(r, l)
+  T (*tile)[kAP] = reinterpret_cast<T (*)[kAP]>(dsm + (size_t)NB * kAP * sizeof(T));  // tile[c][r]
+  int* perm = reinterpret_cast<int*>(dsm + (size_t)2 * NB * kAP * sizeof(T));
   int* lp = perm + NB;
   __shared__ float red[kApplyThreads / 32];
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;
   const bool l21 = (int)blockIdx.x < nrowblk;
   const T* inv = l21 ? work + NB * NB : work;   // inv(U11) or inv(L11)
-  for (int q = tid; q < NB * NB; q += kApplyThreads) {
-    const int r = q & (NB - 1), l = q / NB;
+  for (int e = tid; e < NB * NB; e += kApplyThreads) {
+    const int r = e & (NB - 1), l = e >> 6;
     M[l][r] = (r < nb && l < nb) ? inv[l * NB + r] : ((r == l) ? T(1) : T(0));
   }
   if (l21) {
-    // rows r0 .. r0+NB of L21: out(r, c) = sum_{l <= c} A21(r, l) inv(U)(l, c),
-    // A21 staged CW columns at a time in tile[l][r]
+    // out(r, c) = sum_l A21(r, l) inv(U)(l, c);  tile[l][r] = A21(r0 + r, k + l)
     const int64_t r0 = k + nb + (int64_t)blockIdx.x * NB;
-    constexpr int PER = NB * NB / kApplyThreads;   // outputs per thread
-    T accv[PER];
+    for (int e = tid; e < NB * NB; e += kApplyThreads) {
+      const int r = e & (NB - 1), l = e >> 6;
+      const int64_t gr = r0 + r;
+      tile[l][r] = (gr < n && l < nb) ? A[(k + l) * lda + gr] : T(0);
+    }
+    __syncthreads();
+    T acc[4][4];
 #pragma unroll
-    for (int u = 0; u < PER; ++u) accv[u] = T(0);
-    for (int h0 = 0; h0 < NB; h0 += CW) {
-      __syncthreads();
-      for (int q = tid; q < NB * CW; q += kApplyThreads) {
-        const int r = q & (NB - 1), l = q / NB;
-        const int64_t gr = r0 + r;
-        tile[l][r] = (gr < n && h0 + l < nb) ? A[(k + h0 + l) * lda + gr] : T(0);
-      }
-      __syncthreads();
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int u = 0; u < PER; ++u) {
-        const int e = tid + u * kApplyThreads;
-        const int r = e & (NB - 1), c = e / NB;
-        T s0 = accv[u];
-        const int lend = min(CW, c + 1 - h0);
-        for (int l = 0; l < lend; ++l) s0 += tile[l][r] * M[c][h0 + l];
-        accv[u] = s0;
-      }
+      for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+#pragma unroll 4
+    for (int l = 0; l < NB; ++l) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = tile[l][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = M[ty + 16 * j][l];   // inv(U)(l, c)
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
     }
     float lmax = 0.f;
 #pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int e = tid + u * kApplyThreads;
-      const int r = e & (NB - 1), c = e / NB;
-      const int64_t gr = r0 + r;
-      if (gr < n && c < nb) {
-        A[(k + c) * lda + gr] = accv[u];
-        lmax = fmaxf(lmax, (float)tabs(accv[u]));
+    for (int j = 0; j < 4; ++j) {
+      const int c = ty + 16 * j;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int64_t gr = r0 + tx + 16 * i;
+        if (gr < n && c < nb) {
+          A[(k + c) * lda + gr] = acc[i][j];
+          lmax = fmaxf(lmax, (float)tabs(acc[i][j]));
+        }
       }
     }
 #pragma unroll
@@ -230,33 +243,51 @@ k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __r
   }
   __syncthreads();
   const int64_t nother = n - nb;
-  const int64_t ngroups = (nother + CW - 1) / CW;
+  const int64_t ngroups = (nother + NB - 1) / NB;
   const int nblocks = (int)gridDim.x - nrowblk;
   for (int64_t g = (int)blockIdx.x - nrowblk; g < ngroups; g += nblocks) {
-    for (int e = tid; e < NB * CW; e += kApplyThreads) {
-      const int r = e & (NB - 1), cc = e / NB;
-      const int64_t q = g * CW + cc;
+    for (int e = tid; e < NB * NB; e += kApplyThreads) {
+      const int r = e & (NB - 1), cc = e >> 6;
+      const int64_t qq = g * NB + cc;
       T v = T(0);
-      if (q < nother && r < nb) {
-        const int64_t c = (q < k) ? q : q + nb;
+      if (qq < nother && r < nb) {
+        const int64_t c = (qq < k) ? qq : qq + nb;
         v = A[c * lda + k + r];
       }
       tile[cc][r] = v;
     }
     __syncthreads();
-    for (int e = tid; e < NB * CW; e += kApplyThreads) {
-      const int r = e & (NB - 1), cc = e / NB;
-      const int64_t q = g * CW + cc;
-      if (q >= nother || r >= nb) continue;
-      const int64_t c = (q < k) ? q : q + nb;
-      T out;
-      if (c < k) {
-        out = tile[cc][perm[r]];
-      } else {
-        out = T(0);
-        for (int l = 0; l <= r; ++l) out += M[l][r] * tile[cc][perm[l]];
+    // out(r, cc) = sum_l inv(L)(r, l) tile[cc][perm[l]]   (columns right of the block)
+    //            = tile[cc][perm[r]]                       (columns left of the block)
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+#pragma unroll 4
+    for (int l = 0; l < NB; ++l) {
+      const int pl = perm[l];
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = M[l][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = tile[ty + 16 * j][pl];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int cc = ty + 16 * j;
+      const int64_t qq = g * NB + cc;
+      if (qq >= nother) continue;
+      const int64_t c = (qq < k) ? qq : qq + nb;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = tx + 16 * i;
+        if (r < nb) A[c * lda + k + r] = (c < k) ? tile[cc][perm[r]] : acc[i][j];
       }
-      A[c * lda + k + r] = out;
     }
     __syncthreads();
   }
@@ -397,6 +428,7 @@ template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
   FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem<T>()));
+  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem<T>()));
   auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
   for (int64_t K0 = 0; K0 < n; K0 += kOuterNB) {
     const int64_t kend = std::min<int64_t>(K0 + kOuterNB, n);
@@ -404,12 +436,12 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
       T* work = reinterpret_cast<T*>(c->d_linv);
-      k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, work);
+      k_diag<T><<<1, kDiagThreads, diag_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, c->d_status, work);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
       {
         const int nrowblk = (int)((below + NB - 1) / NB);
-        const int64_t ngroups = (n - nb + apply_cols<T>() - 1) / apply_cols<T>();
+        const int64_t ngroups = (n - nb + NB - 1) / NB;
         const int ncolblk = (int)std::min<int64_t>(ngroups, 2 * num_sms());
         const unsigned g = (unsigned)(nrowblk + ncolblk);
         if (g > 0) {
