@@ -32,17 +32,18 @@ template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a
 
 // ----------------------------------------------------------------------------
 // (1) k_diag: one CTA factors the NB x NB diagonal block with partial pivoting
-// over its rows, in shared memory. 256 threads: thread (r, q) owns row r and
-// the column quarter q of the trailing update. Per pivot step j, three phases
-// separated by barriers:
-//   A  argmax of |column j| over rows j..nb-1 (warps 0-1, shuffles), and the
-//      scaled multipliers of step j-1 written into column j-1;
-//   B  swap of rows j and p (one column per thread);
-//   C  rank-1 update of the columns right of j; each thread forms its row's
-//      multiplier itself, so column j is only written in the next phase A.
-// Then inv(L11) (threads 0-127) and inv(U11) (threads 128-255) by column
-// sweeps in shared memory, one barrier per step, and everything is written
-// out: the block and the pivots to A / ipiv, the inverses to `work`.
+// over its rows, in shared memory. Rows are never moved during the
+// elimination: thread (pr, q) owns physical row pr and the columns c = q mod 4
+// of the trailing update; a pivot row is marked used and each unused row
+// updates itself from it. Per pivot step j two phases separated by barriers:
+//   A  argmax of |column j| over the unused rows (warps 0-1, shuffles), the
+//      winner's reciprocal formed by the winning warp;
+//   C  every unused row forms its multiplier (its own column-j entry) and
+//      updates its columns right of j from the pivot row.
+// Thread 0 keeps the logical order (LAPACK's ipiv: at step j, swap logical
+// rows j and the pivot's position). Then inv(L11) (threads 0-127) and
+// inv(U11) (threads 128-255) by column sweeps in shared memory, and the block
+// (in logical order), the pivots and the inverses are written out.
 constexpr int kDiagThreads = 256;
 constexpr int kDP = NB + 1;   // padded leading dimension in shared memory
 template <class T> constexpr size_t diag_smem() { return (size_t)3 * NB * kDP * sizeof(T); }
@@ -52,95 +53,103 @@ __global__ void __launch_bounds__(kDiagThreads)
 k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
        int* __restrict__ status, T* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char dsm_diag[];
-  T (*S)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag);                  // S[c][r]
+  T (*S)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag);                                     // S[c][pr]
   T (*XL)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag + (size_t)NB * kDP * sizeof(T));      // XL[r][c]
   T (*XU)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag + (size_t)2 * NB * kDP * sizeof(T));  // XU[r][c]
-  __shared__ T lcol[NB];
-  __shared__ T wbest[2];
+  __shared__ T wbest[2], wrcp[2];
+  __shared__ T lcol[NB];       // multipliers of the previous step (written into S one step later)
   __shared__ int wbi[2];
+  __shared__ int used[NB];
+  __shared__ int order[NB];    // order[j] = physical row of logical row j
+  __shared__ int pos[NB];      // pos[pr] = logical position of physical row pr
   __shared__ int lpiv[NB];
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int r = tid & (NB - 1), q = tid >> 6;   // q in 0..3, 16 columns each
+  const int pr = tid & (NB - 1), q = tid >> 6;
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
     S[cc][rr] = (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
+  }
+  if (tid < NB) { used[tid] = 0; order[tid] = tid; pos[tid] = tid; }
+  __syncthreads();
+  bool zero = false;
+  T rp = T(1);
+  for (int j = 0; j < nb; ++j) {
+    // phase A: argmax over unused rows of column j; multipliers of step j-1 stored
+    if (tid < NB) {
+      if (j > 0 && rp != T(0) && pr < nb && !used[pr]) S[j - 1][pr] = lcol[pr];
+      const T v = S[j][pr];
+      T best = (pr < nb && !used[pr]) ? tabs(v) : T(-1);
+      T sv = v;
+      int bi = pr;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const T os = __shfl_xor_sync(0xffffffffu, sv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        // ties: the row earliest in the current logical order wins (LAPACK idamax)
+        if (ob > best || (ob == best && pos[oi] < pos[bi])) { best = ob; bi = oi; sv = os; }
+      }
+      if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; wrcp[warp] = (sv != T(0)) ? T(1) / sv : T(0); }
+    }
+    __syncthreads();
+    int w = 0;
+    if (wbest[1] > wbest[0] || (wbest[1] == wbest[0] && pos[wbi[1]] < pos[wbi[0]])) w = 1;
+    const int p = wbi[w];
+    rp = wrcp[w];
+    if (tid == 0) {
+      // logical swap of rows j and p (LAPACK ipiv), pivot marked used
+      const int lj = j, lp = pos[p];
+      lpiv[j] = lp;
+      const int rj = order[lj];
+      order[lj] = p; order[lp] = rj;
+      pos[p] = lj; pos[rj] = lp;
+      used[p] = 1;
+      if (rp == T(0)) zero = true;
+    }
+    // phase C: unused rows (not p) eliminate column j
+    if (pr < nb && pr != p && !used[pr] && rp != T(0)) {
+      const T l = S[j][pr] * rp;
+      if (q == 0) lcol[pr] = l;
+      for (int c = j + 1 + ((q - (j + 1)) & 3); c < nb; c += 4) S[c][pr] -= l * S[c][p];
+    }
+    __syncthreads();
+  }
+  if (zero) atomicOr(status, (int)DEV_ZERO_PIVOT);
+  // inverses from the logically ordered block: L(rr, jj) = S[jj][order[rr]] (rr > jj),
+  // U(rr, jj) = S[jj][order[rr]] (rr <= jj)
+  for (int e = tid; e < NB * NB; e += kDiagThreads) {
+    const int rr = e & (NB - 1), cc = e >> 6;
     XL[cc][rr] = (rr == cc) ? T(1) : T(0);
     XU[cc][rr] = (rr == cc) ? T(1) : T(0);
   }
   __syncthreads();
-  bool zero = false;
-  for (int j = 0; j < nb; ++j) {
-    // phase A
-    if (tid < NB) {
-      if (j > 0 && r >= j && r < nb) S[j - 1][r] = lcol[r];
-      T best = (r >= j && r < nb) ? tabs(S[j][r]) : T(-1);
-      int bi = r;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const T ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; }
-    }
-    __syncthreads();
-    int p = wbi[0];
-    if (wbest[1] > wbest[0] || (wbest[1] == wbest[0] && wbi[1] < wbi[0])) p = wbi[1];
-    // phase B
-    if (tid < NB && p != j) {
-      const T t0 = S[tid][j];
-      S[tid][j] = S[tid][p];
-      S[tid][p] = t0;
-    }
-    if (tid == 0) lpiv[j] = p;
-    __syncthreads();
-    // phase C
-    const T pv = S[j][j];
-    if (pv == T(0)) {
-      zero = true;
-    } else if (r > j && r < nb) {
-      const T l = S[j][r] * (T(1) / pv);
-      if (q == 0) lcol[r] = l;
-      const int c0 = q * (NB / 4);
-#pragma unroll
-      for (int cc = 0; cc < NB / 4; ++cc) {
-        const int c = c0 + cc;
-        if (c > j && c < nb) S[c][r] -= l * S[c][j];
-      }
-    }
-    __syncthreads();
-  }
-  if (zero && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-  // inverses. Lower: step s = jj, X(rr, c) -= L(rr, jj) X(jj, c) for rr > jj, c <= jj.
-  // Upper: step s, jj = NB-1-s: row jj+1 is divided by U(jj+1, jj+1) (deferred so
-  // that it is not read and written in one phase), and
-  // X(rr, c) -= U(rr, jj) / U(jj, jj) X(jj, c) for rr < jj, c >= jj.
   const bool lowg = tid < 2 * NB;
   const int lt = lowg ? tid : tid - 2 * NB;
   const int tr = lt & (NB - 1), tc = lt >> 6;   // tc in 0..1
+  const int otr = order[tr];
   for (int s = 0; s < NB; ++s) {
     if (lowg) {
       const int jj = s;
       if (tr > jj) {
-        const T lv = S[jj][tr];
+        const T lv = S[jj][otr];
         for (int c = tc; c <= jj; c += 2) XL[tr][c] -= lv * XL[jj][c];
       }
     } else {
       const int jj = NB - 1 - s;
-      if (s > 0 && tc == 0 && tr >= jj + 1) XU[jj + 1][tr] *= T(1) / S[jj + 1][jj + 1];
+      if (s > 0 && tc == 0 && tr >= jj + 1) XU[jj + 1][tr] *= T(1) / S[jj + 1][order[jj + 1]];
       if (tr < jj) {
-        const T uv = S[jj][tr] / S[jj][jj];
+        const T uv = S[jj][otr] / S[jj][order[jj]];
         for (int c = jj + tc; c < NB; c += 2) XU[tr][c] -= uv * XU[jj][c];
       }
     }
     __syncthreads();
   }
-  if (!lowg && tc == 0) XU[0][tr] *= T(1) / S[0][0];
+  if (!lowg && tc == 0) XU[0][tr] *= T(1) / S[0][order[0]];
   __syncthreads();
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
-    if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[cc][rr];
+    if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[cc][order[rr]];
     work[cc * NB + rr] = XL[rr][cc];
     work[NB * NB + cc * NB + rr] = XU[rr][cc];
   }
