@@ -303,23 +303,50 @@ k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __r
 }
 
 // ----------------------------------------------------------------------------
-// (3) trailing update C -= A B, SIMT register tiles (the FP64 path). Global
-// loads of the next K slice go to registers while the current slice is
-// multiplied from shared memory (double buffer). Consecutive threads own
-// consecutive rows, so the C read-modify-write is coalesced.
+// (3) trailing update C -= A B, SIMT register tiles (the FP64 path). The C tile
+// is fetched into shared memory with cp.async when the CTA starts, so its
+// latency overlaps the K loop; global loads of the next K slice go to
+// registers while the current slice is multiplied from shared memory (double
+// buffer). Consecutive threads own consecutive rows (coalesced C accesses).
+template <class T, int BM, int BN, int BK, int TM, int TN>
+constexpr size_t gemm_smem() {
+  return (size_t)2 * BK * (BM + 2) * sizeof(T) + (size_t)2 * BK * (BN + 2) * sizeof(T) + (size_t)BM * BN * sizeof(T);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+
 template <class T, int BM, int BN, int BK, int TM, int TN>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ Cm, int64_t lda,
-           int64_t m, int64_t nn, int kk) {
+           int64_t m, int64_t nn, int kk, bool pre) {
   constexpr int NT = (BM / TM) * (BN / TN);
   constexpr int LA = BK * BM / NT;
   constexpr int LB = BK * BN / NT;
   constexpr int TX = BM / TM;
-  __shared__ T As[2][BK][BM + 2];
-  __shared__ T Bs[2][BK][BN + 2];
+  constexpr int V16 = 16 / sizeof(T);   // elements per 16-byte copy
+  extern __shared__ __align__(16) unsigned char gsm[];
+  T (*As)[BK][BM + 2] = reinterpret_cast<T (*)[BK][BM + 2]>(gsm);
+  T (*Bs)[BK][BN + 2] = reinterpret_cast<T (*)[BK][BN + 2]>(gsm + (size_t)2 * BK * (BM + 2) * sizeof(T));
+  T (*Cs)[BM] = reinterpret_cast<T (*)[BM]>(gsm + (size_t)2 * BK * (BM + 2) * sizeof(T) +
+                                            (size_t)2 * BK * (BN + 2) * sizeof(T));   // Cs[col][row]
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int64_t i0 = (int64_t)blockIdx.x * BM, j0 = (int64_t)blockIdx.y * BN;
+  // C tile -> shared memory (asynchronous); whole 16-byte pieces of rows < m
+  // only (i0 and lda keep them aligned), the rest is zero and never stored
+  if (pre) {
+    for (int e = tid; e < BM * BN / V16; e += NT) {
+      const int col = e / (BM / V16), rv = (e % (BM / V16)) * V16;
+      const int64_t gi = i0 + rv, gj = j0 + col;
+      const bool ok = (gj < nn) && (gi + V16 <= m);
+      cp_async16(&Cs[col][rv], ok ? (const void*)(Cm + gj * lda + gi) : (const void*)Cm, ok);
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
   T acc[TM][TN];
 #pragma unroll
   for (int a = 0; a < TM; ++a)
@@ -377,14 +404,22 @@ k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ C
     __syncthreads();
     buf ^= 1;
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  const bool full_rows = pre && i0 + BM <= m;
 #pragma unroll
   for (int v = 0; v < TN; ++v) {
-    const int64_t gj = j0 + ty + v * (BN / TN);
+    const int col = ty + v * (BN / TN);
+    const int64_t gj = j0 + col;
     if (gj >= nn) continue;
 #pragma unroll
     for (int u = 0; u < TM; ++u) {
-      const int64_t gi = i0 + tx + u * TX;
-      if (gi < m) Cm[gj * lda + gi] -= acc[u][v];
+      const int row = tx + u * TX;
+      const int64_t gi = i0 + row;
+      if (gi >= m) continue;
+      // rows of a partial 16-byte piece were not prefetched: read them directly
+      const T cv = (full_rows || (pre && (row / V16) * V16 + V16 + i0 <= m)) ? Cs[col][row] : Cm[gj * lda + gi];
+      Cm[gj * lda + gi] = cv - acc[u][v];
     }
   }
 }
@@ -394,6 +429,9 @@ k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ C
 bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
                      int64_t nn, int kk);
 
+int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
+                      int kk);
+
 // C (m x nn) -= A (m x kk) B (kk x nn); all three are sub-blocks of one
 // column-major matrix with leading dimension lda.
 template <class T>
@@ -402,14 +440,19 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
   if (m <= 0 || nn <= 0 || kk <= 0) return FP_OK;
   if constexpr (sizeof(T) == 4) {
     if (tc_gemm_sub_f32(c, (const float*)Am, (const float*)Bm, (float*)Cm, lda, m, nn, kk)) return FP_OK;
-    constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
-    dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
-    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk);
-    ++c->nlaunch;
+    return gemm_sub_simt_f32(c, (const float*)Am, (const float*)Bm, (float*)Cm, lda, m, nn, kk);
   } else {
     constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
+    constexpr size_t sm = gemm_smem<T, BM, BN, BK, TM, TN>();
+    static bool attr = false;
+    if (!attr) {
+      FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_gemm_sub<T, BM, BN, BK, TM, TN>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      attr = true;
+    }
     dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
-    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk);
+    const bool pre = ((reinterpret_cast<uintptr_t>(Cm) | (uintptr_t)(lda * sizeof(T))) & 15) == 0;
+    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk, pre);
     ++c->nlaunch;
   }
   FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -419,8 +462,16 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
 int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
                       int kk) {
   constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
+  constexpr size_t sm = gemm_smem<float, BM, BN, BK, TM, TN>();
+  static bool attr = false;
+  if (!attr) {
+    FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_gemm_sub<float, BM, BN, BK, TM, TN>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
   dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
-  k_gemm_sub<float, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), 0, c->stream>>>(A, B, C, lda, m, nn, kk);
+  const bool pre = ((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(lda * sizeof(float))) & 15) == 0;
+  k_gemm_sub<float, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(A, B, C, lda, m, nn, kk, pre);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;
