@@ -31,216 +31,178 @@ constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
 template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
 
 // ----------------------------------------------------------------------------
-// (1) k_diag: one CTA factors the NB x NB diagonal block with partial pivoting
-// over its rows, in shared memory. Rows are never moved during the
-// elimination: thread (pr, q) owns physical row pr and the columns c = q mod 4
-// of the trailing update; a pivot row is marked used and each unused row
-// updates itself from it. Per pivot step j two phases separated by barriers:
-//   A  argmax of |column j| over the unused rows (warps 0-1, shuffles), the
-//      winner's reciprocal formed by the winning warp;
-//   C  every unused row forms its multiplier (its own column-j entry) and
-//      updates its columns right of j from the pivot row.
-// Thread 0 keeps the logical order (LAPACK's ipiv: at step j, swap logical
-// rows j and the pivot's position). Then inv(L11) (threads 0-127) and
-// inv(U11) (threads 128-255) by column sweeps in shared memory, and the block
-// (in logical order), the pivots and the inverses are written out.
+// (1) k_diag: one CTA of 8 warps factors the NB x NB diagonal block with
+// partial pivoting over its rows, in shared memory, with one block barrier
+// per pivot step. Rows never move: a pivot row is marked used and every other
+// unused row eliminates column j with its own multiplier. Each warp finds the
+// pivot itself (lane l reads rows l and l+32 of column j; a shuffle reduction
+// carries value, sign and logical position; used flags and logical positions
+// of all rows are kept in registers, identically in every warp), so nothing
+// is exchanged through shared memory but the matrix. Warp w updates rows
+// 8w..8w+7, four lanes per row, columns interleaved mod 4; all loads of a
+// lane are issued before its stores. LAPACK's ipiv follows from the logical
+// order (at step j, logical rows j and the pivot's position swap).
 constexpr int kDiagThreads = 256;
 constexpr int kDP = NB + 1;   // padded leading dimension in shared memory
-template <class T> constexpr size_t diag_smem() { return (size_t)3 * NB * kDP * sizeof(T); }
 
 template <class T>
 __global__ void __launch_bounds__(kDiagThreads)
 k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
-       int* __restrict__ status, T* __restrict__ work) {
-  extern __shared__ __align__(16) unsigned char dsm_diag[];
-  T (*S)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag);                                     // S[c][pr]
-  T (*XL)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag + (size_t)NB * kDP * sizeof(T));      // XL[r][c]
-  T (*XU)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm_diag + (size_t)2 * NB * kDP * sizeof(T));  // XU[r][c]
-  __shared__ T wbest[2], wrcp[2];
-  __shared__ T lcol[NB];       // multipliers of the previous step (written into S one step later)
-  __shared__ int wbi[2];
-  __shared__ int used[NB];
-  __shared__ int order[NB];    // order[j] = physical row of logical row j
-  __shared__ int pos[NB];      // pos[pr] = logical position of physical row pr
+       int* __restrict__ status) {
+  __shared__ T S[NB][kDP];     // S[c][pr]
+  __shared__ int order[NB];
   __shared__ int lpiv[NB];
   const int nb = (int)imin64(NB, n - k);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int pr = tid & (NB - 1), q = tid >> 6;
+  const int tid = threadIdx.x, l = tid & 31, warp = tid >> 5;
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
     S[cc][rr] = (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
   }
-  if (tid < NB) { used[tid] = 0; order[tid] = tid; pos[tid] = tid; }
-  __syncthreads();
+  // argmax ownership: rows l and l + 32
+  const int a0 = l, a1 = l + 32;
+  bool used0 = !(a0 < nb), used1 = !(a1 < nb);
+  int pos0 = a0, pos1 = a1;
+  // update ownership: row ur, column phase cp
+  const int ur = 8 * warp + (l & 7), cp = l >> 3;
   bool zero = false;
-  T rp = T(1);
-  for (int j = 0; j < nb; ++j) {
-    // phase A: argmax over unused rows of column j; multipliers of step j-1 stored
-    if (tid < NB) {
-      if (j > 0 && rp != T(0) && pr < nb && !used[pr]) S[j - 1][pr] = lcol[pr];
-      const T v = S[j][pr];
-      T best = (pr < nb && !used[pr]) ? tabs(v) : T(-1);
-      T sv = v;
-      int bi = pr;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const T ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const T os = __shfl_xor_sync(0xffffffffu, sv, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        // ties: the row earliest in the current logical order wins (LAPACK idamax)
-        if (ob > best || (ob == best && pos[oi] < pos[bi])) { best = ob; bi = oi; sv = os; }
-      }
-      if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; wrcp[warp] = (sv != T(0)) ? T(1) / sv : T(0); }
-    }
-    __syncthreads();
-    int w = 0;
-    if (wbest[1] > wbest[0] || (wbest[1] == wbest[0] && pos[wbi[1]] < pos[wbi[0]])) w = 1;
-    const int p = wbi[w];
-    rp = wrcp[w];
-    if (tid == 0) {
-      // logical swap of rows j and p (LAPACK ipiv), pivot marked used
-      const int lj = j, lp = pos[p];
-      lpiv[j] = lp;
-      const int rj = order[lj];
-      order[lj] = p; order[lp] = rj;
-      pos[p] = lj; pos[rj] = lp;
-      used[p] = 1;
-      if (rp == T(0)) zero = true;
-    }
-    // phase C: unused rows (not p) eliminate column j
-    if (pr < nb && pr != p && !used[pr] && rp != T(0)) {
-      const T l = S[j][pr] * rp;
-      if (q == 0) lcol[pr] = l;
-      for (int c = j + 1 + ((q - (j + 1)) & 3); c < nb; c += 4) S[c][pr] -= l * S[c][p];
-    }
-    __syncthreads();
-  }
-  if (zero) atomicOr(status, (int)DEV_ZERO_PIVOT);
-  // inverses from the logically ordered block: L(rr, jj) = S[jj][order[rr]] (rr > jj),
-  // U(rr, jj) = S[jj][order[rr]] (rr <= jj)
-  for (int e = tid; e < NB * NB; e += kDiagThreads) {
-    const int rr = e & (NB - 1), cc = e >> 6;
-    XL[cc][rr] = (rr == cc) ? T(1) : T(0);
-    XU[cc][rr] = (rr == cc) ? T(1) : T(0);
-  }
   __syncthreads();
-  const bool lowg = tid < 2 * NB;
-  const int lt = lowg ? tid : tid - 2 * NB;
-  const int tr = lt & (NB - 1), tc = lt >> 6;   // tc in 0..1
-  const int otr = order[tr];
-  for (int s = 0; s < NB; ++s) {
-    if (lowg) {
-      const int jj = s;
-      if (tr > jj) {
-        const T lv = S[jj][otr];
-        for (int c = tc; c <= jj; c += 2) XL[tr][c] -= lv * XL[jj][c];
+  for (int j = 0; j < nb; ++j) {
+    const T v0 = S[j][a0], v1 = S[j][a1];
+    const T vu = S[j][ur];
+    T best = T(-1), sv = T(0);
+    int bi = 0, bpos = 1 << 30;
+    if (!used0) { best = tabs(v0); sv = v0; bi = a0; bpos = pos0; }
+    if (!used1) {
+      const T b1 = tabs(v1);
+      if (b1 > best || (b1 == best && pos1 < bpos)) { best = b1; sv = v1; bi = a1; bpos = pos1; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const T ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const T os = __shfl_xor_sync(0xffffffffu, sv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+      if (ob > best || (ob == best && op < bpos)) { best = ob; sv = os; bi = oi; bpos = op; }
+    }
+    const int p = bi, lp = bpos;
+    // physical row at logical position j (before this step's swap)
+    const unsigned m0 = __ballot_sync(0xffffffffu, pos0 == j);
+    const unsigned m1 = __ballot_sync(0xffffffffu, pos1 == j);
+    const int rj = m0 ? (__ffs(m0) - 1) : (32 + __ffs(m1) - 1);
+    // used status of my update row (before marking the pivot)
+    const bool uu0 = __shfl_sync(0xffffffffu, used0, ur & 31);
+    const bool uu1 = __shfl_sync(0xffffffffu, used1, ur & 31);
+    const bool urow_used = (ur >> 5) ? uu1 : uu0;
+    if (a0 == p) { pos0 = j; used0 = true; } else if (a0 == rj) { pos0 = lp; }
+    if (a1 == p) { pos1 = j; used1 = true; } else if (a1 == rj) { pos1 = lp; }
+    if (tid == 0) lpiv[j] = lp;
+    const T rp = (sv != T(0)) ? T(1) / sv : T(0);
+    if (rp == T(0)) {
+      zero = true;
+    } else if (ur < nb && ur != p && !urow_used) {
+      const T m = vu * rp;
+      __syncwarp(0xffffffffu & __activemask());
+      if (cp == 0) S[j][ur] = m;
+      const int cs = j + 1 + ((cp - (j + 1)) & 3);
+      T pv[NB / 4], ov[NB / 4];
+#pragma unroll
+      for (int i = 0; i < NB / 4; ++i) {
+        const int c = cs + 4 * i;
+        if (c < nb) { pv[i] = S[c][p]; ov[i] = S[c][ur]; }
       }
-    } else {
-      const int jj = NB - 1 - s;
-      if (s > 0 && tc == 0 && tr >= jj + 1) XU[jj + 1][tr] *= T(1) / S[jj + 1][order[jj + 1]];
-      if (tr < jj) {
-        const T uv = S[jj][otr] / S[jj][order[jj]];
-        for (int c = jj + tc; c < NB; c += 2) XU[tr][c] -= uv * XU[jj][c];
+#pragma unroll
+      for (int i = 0; i < NB / 4; ++i) {
+        const int c = cs + 4 * i;
+        if (c < nb) S[c][ur] = ov[i] - m * pv[i];
       }
     }
     __syncthreads();
   }
-  if (!lowg && tc == 0) XU[0][tr] *= T(1) / S[0][order[0]];
+  if (zero && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
+  if (warp == 0) { order[pos0] = a0; order[pos1] = a1; }
   __syncthreads();
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
     if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[cc][order[rr]];
-    work[cc * NB + rr] = XL[rr][cc];
-    work[NB * NB + cc * NB + rr] = XU[rr][cc];
   }
   if (tid < nb) ipiv[k + tid] = (int32_t)(k + lpiv[tid]);
 }
 
 // ----------------------------------------------------------------------------
-// (2) k_apply, after k_diag; two kinds of CTA in one launch:
-//  * blockIdx < nrowblk: L21 = A21 inv(U11) for NB rows below the block, with
-//    max|L21| (the GEPP certificate);
-//  * the others: row swaps of the block on every other column and
-//    U12 = inv(L11) P A12 for the columns right of the block.
-// Both are NB x NB x NB products against an inverse in shared memory; each
-// thread computes a 4 x 4 register tile (rows tx+16i, columns ty+16j), so
-// consecutive threads touch consecutive rows of the column-major matrix.
-constexpr int kApplyThreads = 256;
-constexpr int kAP = NB + 1;
-template <class T> constexpr size_t apply_smem() {
-  return (size_t)2 * NB * kAP * sizeof(T) + 2 * NB * sizeof(int) + 64;
+// (2) after k_diag, two kernels:
+//  * k_l21: L21 = A21 U11^-1, one row per thread, right-looking
+//    (x_j *= 1/U_jj, then x_l -= x_j U_jl for l > j) with U11 broadcast from
+//    shared memory; the largest |L21| is the GEPP certificate;
+//  * k_u12: for columns outside the block, the row swaps of the block, and for
+//    columns right of it U12 = L11^-1 P A12 by forward substitution (unit lower
+//    L11 broadcast from shared memory), one column per thread; columns are
+//    staged through shared memory so that global accesses are coalesced.
+constexpr int kApplyThreads = 128;
+template <class T> constexpr size_t u12_smem() {
+  return (size_t)NB * kDP * sizeof(T) + (size_t)kApplyThreads * kDP * sizeof(T) + 2 * NB * sizeof(int) + 64;
 }
 
 template <class T>
 __global__ void __launch_bounds__(kApplyThreads)
-k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv,
-        const T* __restrict__ work, float* __restrict__ cert, int nrowblk) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  T (*M)[kAP] = reinterpret_cast<T (*)[kAP]>(dsm);                                   // M[l][r] = inv(r, l)
-  T (*tile)[kAP] = reinterpret_cast<T (*)[kAP]>(dsm + (size_t)NB * kAP * sizeof(T));  // tile[c][r]
-  int* perm = reinterpret_cast<int*>(dsm + (size_t)2 * NB * kAP * sizeof(T));
-  int* lp = perm + NB;
+k_l21(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ cert) {
+  __shared__ T D[NB][kDP];     // D[c][r] = block(r, c)
+  __shared__ T rdiag[NB];
   __shared__ float red[kApplyThreads / 32];
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
-  const bool l21 = (int)blockIdx.x < nrowblk;
-  const T* inv = l21 ? work + NB * NB : work;   // inv(U11) or inv(L11)
   for (int e = tid; e < NB * NB; e += kApplyThreads) {
-    const int r = e & (NB - 1), l = e >> 6;
-    M[l][r] = (r < nb && l < nb) ? inv[l * NB + r] : ((r == l) ? T(1) : T(0));
+    const int r = e & (NB - 1), c = e >> 6;
+    D[c][r] = (r < nb && c < nb) ? A[(k + c) * lda + (k + r)] : ((r == c) ? T(1) : T(0));
   }
-  if (l21) {
-    // out(r, c) = sum_l A21(r, l) inv(U)(l, c);  tile[l][r] = A21(r0 + r, k + l)
-    const int64_t r0 = k + nb + (int64_t)blockIdx.x * NB;
-    for (int e = tid; e < NB * NB; e += kApplyThreads) {
-      const int r = e & (NB - 1), l = e >> 6;
-      const int64_t gr = r0 + r;
-      tile[l][r] = (gr < n && l < nb) ? A[(k + l) * lda + gr] : T(0);
+  __syncthreads();
+  if (tid < NB) rdiag[tid] = T(1) / D[tid][tid];
+  __syncthreads();
+  const int64_t row = k + nb + (int64_t)blockIdx.x * kApplyThreads + tid;
+  float lmax = 0.f;
+  if (row < n) {
+    T x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? A[(k + j) * lda + row] : T(0);
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const T xj = x[j] * rdiag[j];
+      x[j] = xj;
+#pragma unroll
+      for (int l = j + 1; l < NB; ++l) x[l] -= xj * D[l][j];
     }
-    __syncthreads();
-    T acc[4][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-#pragma unroll 4
-    for (int l = 0; l < NB; ++l) {
-      T a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = tile[l][tx + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = M[ty + 16 * j][l];   // inv(U)(l, c)
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
-    }
-    float lmax = 0.f;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int c = ty + 16 * j;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int64_t gr = r0 + tx + 16 * i;
-        if (gr < n && c < nb) {
-          A[(k + c) * lda + gr] = acc[i][j];
-          lmax = fmaxf(lmax, (float)tabs(acc[i][j]));
-        }
+    for (int j = 0; j < NB; ++j) {
+      if (j < nb) {
+        A[(k + j) * lda + row] = x[j];
+        lmax = fmaxf(lmax, (float)tabs(x[j]));
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    if ((tid & 31) == 0) red[tid >> 5] = lmax;
-    __syncthreads();
-    if (tid == 0) {
-      float mm = red[0];
-      for (int w = 1; w < kApplyThreads / 32; ++w) mm = fmaxf(mm, red[w]);
-      if (mm > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(mm));
-    }
-    return;
   }
-  // swaps + U12
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+  if ((tid & 31) == 0) red[tid >> 5] = lmax;
+  __syncthreads();
+  if (tid == 0) {
+    float mm = red[0];
+    for (int w = 1; w < kApplyThreads / 32; ++w) mm = fmaxf(mm, red[w]);
+    if (mm > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(mm));
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kApplyThreads)
+k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  T (*D)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm);                                      // D[c][r] = block(r, c)
+  T (*tile)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm + (size_t)NB * kDP * sizeof(T));     // tile[col][r]
+  int* perm = reinterpret_cast<int*>(dsm + (size_t)NB * kDP * sizeof(T) + (size_t)kApplyThreads * kDP * sizeof(T));
+  int* lp = perm + NB;
+  const int nb = (int)imin64(NB, n - k);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < NB * NB; e += kApplyThreads) {
+    const int r = e & (NB - 1), c = e >> 6;
+    D[c][r] = (r < nb && c < nb) ? A[(k + c) * lda + (k + r)] : ((r == c) ? T(1) : T(0));
+  }
   if (tid < nb) lp[tid] = (int)(ipiv[k + tid] - k);
   __syncthreads();
   if (tid == 0) {
@@ -252,12 +214,12 @@ k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __r
   }
   __syncthreads();
   const int64_t nother = n - nb;
-  const int64_t ngroups = (nother + NB - 1) / NB;
-  const int nblocks = (int)gridDim.x - nrowblk;
-  for (int64_t g = (int)blockIdx.x - nrowblk; g < ngroups; g += nblocks) {
-    for (int e = tid; e < NB * NB; e += kApplyThreads) {
+  {
+    const int64_t g = blockIdx.x;   // one group of kApplyThreads columns per CTA
+    // stage kApplyThreads columns (rows k..k+nb), coalesced along the rows
+    for (int e = tid; e < NB * kApplyThreads; e += kApplyThreads) {
       const int r = e & (NB - 1), cc = e >> 6;
-      const int64_t qq = g * NB + cc;
+      const int64_t qq = g * kApplyThreads + cc;
       T v = T(0);
       if (qq < nother && r < nb) {
         const int64_t c = (qq < k) ? qq : qq + nb;
@@ -266,39 +228,34 @@ k_apply(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __r
       tile[cc][r] = v;
     }
     __syncthreads();
-    // out(r, cc) = sum_l inv(L)(r, l) tile[cc][perm[l]]   (columns right of the block)
-    //            = tile[cc][perm[r]]                       (columns left of the block)
-    T acc[4][4];
+    {
+      const int64_t qq = g * kApplyThreads + tid;
+      if (qq < nother) {
+        const int64_t c = (qq < k) ? qq : qq + nb;
+        T x[NB];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+        for (int r = 0; r < NB; ++r) x[r] = tile[tid][perm[r]];
+        if (c >= k + nb) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
-#pragma unroll 4
-    for (int l = 0; l < NB; ++l) {
-      const int pl = perm[l];
-      T a[4], b[4];
+          for (int j = 0; j < NB; ++j) {
+            const T xj = x[j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = M[l][tx + 16 * i];
+            for (int r = j + 1; r < NB; ++r) x[r] -= D[j][r] * xj;
+          }
+        }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = tile[ty + 16 * j][pl];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int cc = ty + 16 * j;
-      const int64_t qq = g * NB + cc;
-      if (qq >= nother) continue;
-      const int64_t c = (qq < k) ? qq : qq + nb;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int r = tx + 16 * i;
-        if (r < nb) A[c * lda + k + r] = (c < k) ? tile[cc][perm[r]] : acc[i][j];
+        for (int r = 0; r < NB; ++r) tile[tid][r] = x[r];
       }
     }
     __syncthreads();
+    for (int e = tid; e < NB * kApplyThreads; e += kApplyThreads) {
+      const int r = e & (NB - 1), cc = e >> 6;
+      const int64_t qq = g * kApplyThreads + cc;
+      if (qq < nother && r < nb) {
+        const int64_t c = (qq < k) ? qq : qq + nb;
+        A[c * lda + k + r] = tile[cc][r];
+      }
+    }
   }
 }
 
@@ -487,28 +444,27 @@ constexpr int kOuterNB = 256;
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
-  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem<T>()));
-  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem<T>()));
+  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_u12<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem<T>()));
   auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
   for (int64_t K0 = 0; K0 < n; K0 += kOuterNB) {
     const int64_t kend = std::min<int64_t>(K0 + kOuterNB, n);
     for (int64_t k = K0; k < kend; k += NB) {
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
-      T* work = reinterpret_cast<T*>(c->d_linv);
-      k_diag<T><<<1, kDiagThreads, diag_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, c->d_status, work);
+      k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
-      {
-        const int nrowblk = (int)((below + NB - 1) / NB);
-        const int64_t ngroups = (n - nb + NB - 1) / NB;
-        const int ncolblk = (int)std::min<int64_t>(ngroups, 2 * num_sms());
-        const unsigned g = (unsigned)(nrowblk + ncolblk);
-        if (g > 0) {
-          k_apply<T><<<g, kApplyThreads, apply_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, work, cert, nrowblk);
-          ++c->nlaunch;
-          FP_CUDA_TRY(c->err, cudaGetLastError());
-        }
+      if (below > 0) {
+        const unsigned g = (unsigned)((below + kApplyThreads - 1) / kApplyThreads);
+        k_l21<T><<<g, kApplyThreads, 0, c->stream>>>(A, lda, n, k, cert);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      }
+      if (n - nb > 0) {
+        const unsigned g = (unsigned)((n - nb + kApplyThreads - 1) / kApplyThreads);
+        k_u12<T><<<g, kApplyThreads, u12_smem<T>(), c->stream>>>(A, lda, n, k, ipiv);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
       }
       const int64_t k1 = k + nb;
       // (a) remaining panel columns, full height
