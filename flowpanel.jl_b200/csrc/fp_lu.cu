@@ -29,46 +29,106 @@ constexpr int kPanelThreads = 128;
 constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
 
 template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
+// Returns p unchanged, but opaque to the compiler: addresses formed from it
+// are not shared with (and kept live from) earlier uses of the same pointer.
+template <class P> __device__ __forceinline__ P* opaque_ptr(P* p) {
+  uint64_t v = reinterpret_cast<uint64_t>(p);
+  asm volatile("mov.b64 %0, %0;" : "+l"(v));
+  return reinterpret_cast<P*>(v);
+}
+
+// ----------------------------------------------------------------------------
+// 16-byte vectors of T (float4 / double2) for the shared-memory sweeps below.
+template <class T> struct V16;
+template <> struct V16<float> { typedef float4 type; static constexpr int n = 4; };
+template <> struct V16<double> { typedef double2 type; static constexpr int n = 2; };
+template <class T> __device__ __forceinline__ T vget(const typename V16<T>::type& v, int i);
+template <> __device__ __forceinline__ float vget<float>(const float4& v, int i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+template <> __device__ __forceinline__ double vget<double>(const double2& v, int i) { return i == 0 ? v.x : v.y; }
+template <class T> __device__ __forceinline__ void vset(typename V16<T>::type& v, int i, T x);
+template <> __device__ __forceinline__ void vset<float>(float4& v, int i, float x) {
+  if (i == 0) v.x = x; else if (i == 1) v.y = x; else if (i == 2) v.z = x; else v.w = x;
+}
+template <> __device__ __forceinline__ void vset<double>(double2& v, int i, double x) {
+  if (i == 0) v.x = x; else v.y = x;
+}
+// Stages an NB x NB block element by element with NT threads: element
+// (r, c) = get(r, c) goes to put(r, c, v), r fastest over the threads (so that
+// column-major global reads coalesce). Each thread issues a batch of up to 16
+// loads before its stores, so that the copy costs a few memory latencies
+// rather than one per element.
+template <int NT, class T, class Get, class Put>
+__device__ __forceinline__ void stage_block(int tid, Get get, Put put) {
+  constexpr int IT = NB * NB / NT;
+  constexpr int BATCH = IT < 16 ? IT : 16;
+#pragma unroll
+  for (int i0 = 0; i0 < IT; i0 += BATCH) {
+    T v[BATCH];
+#pragma unroll
+    for (int u = 0; u < BATCH; ++u) {
+      const int e = tid + (i0 + u) * NT;
+      v[u] = get(e & (NB - 1), e / NB);
+    }
+#pragma unroll
+    for (int u = 0; u < BATCH; ++u) {
+      const int e = tid + (i0 + u) * NT;
+      put(e & (NB - 1), e / NB, v[u]);
+    }
+  }
+}
+// row pitch of an NB-wide row in shared memory: whole 16-byte vectors, not a
+// multiple of 32 banks
+template <class T> __host__ __device__ constexpr int rpitch() { return NB + 16 / (int)sizeof(T); }
 
 // ----------------------------------------------------------------------------
 // (1) k_diag: one CTA of 8 warps factors the NB x NB diagonal block with
-// partial pivoting over its rows, in shared memory, with one block barrier
-// per pivot step. Rows never move: a pivot row is marked used and every other
-// unused row eliminates column j with its own multiplier. Each warp finds the
-// pivot itself (lane l reads rows l and l+32 of column j; a shuffle reduction
-// carries value, sign and logical position; used flags and logical positions
-// of all rows are kept in registers, identically in every warp), so nothing
-// is exchanged through shared memory but the matrix. Warp w updates rows
-// 8w..8w+7, four lanes per row, columns interleaved mod 4; all loads of a
-// lane are issued before its stores. LAPACK's ipiv follows from the logical
-// order (at step j, logical rows j and the pivot's position swap).
+// partial pivoting over its rows, in shared memory (row-major), with one block
+// barrier per pivot step. Rows never move: a pivot row is marked used and
+// every other unused row eliminates column j with its own multiplier. Each
+// warp finds the pivot itself (lane l reads rows l and l+32 of column j; a
+// shuffle reduction carries value, sign and logical position; used flags and
+// logical positions are kept in registers, identically in every warp).
+// Warp w updates rows 8w..8w+7, four lanes per row, 16-byte column chunks
+// interleaved over the lanes; the chunk holding column j also receives the
+// multiplier. Column j is read from a double-buffered copy (colv), which
+// step j - 1 filled with the updated values: the owner of a row writes the
+// multiplier into S at step j while other warps may still be searching
+// column j. LAPACK's ipiv follows from the logical order (at step j, logical
+// rows j and the pivot's position swap).
 constexpr int kDiagThreads = 256;
-constexpr int kDP = NB + 1;   // padded leading dimension in shared memory
 
 template <class T>
 __global__ void __launch_bounds__(kDiagThreads)
 k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
        int* __restrict__ status) {
-  __shared__ T S[NB][kDP];     // S[c][pr]
+  typedef typename V16<T>::type VT;
+  constexpr int V = V16<T>::n, RP = rpitch<T>(), NCH = NB / V;
+  __shared__ __align__(16) T S[NB][RP];   // S[pr][c]
   __shared__ int order[NB];
   __shared__ int lpiv[NB];
+  __shared__ T colv[2][NB];              // column j of S, for step j
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x, l = tid & 31, warp = tid >> 5;
-  for (int e = tid; e < NB * NB; e += kDiagThreads) {
-    const int rr = e & (NB - 1), cc = e >> 6;
-    S[cc][rr] = (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
-  }
-  // argmax ownership: rows l and l + 32
+  stage_block<kDiagThreads, T>(
+      tid,
+      [&](int rr, int cc) {
+        return (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
+      },
+      [&](int rr, int cc, T v) {
+        S[rr][cc] = v;
+        if (cc == 0) colv[0][rr] = v;
+      });
   const int a0 = l, a1 = l + 32;
   bool used0 = !(a0 < nb), used1 = !(a1 < nb);
   int pos0 = a0, pos1 = a1;
-  // update ownership: row ur, column phase cp
   const int ur = 8 * warp + (l & 7), cp = l >> 3;
   bool zero = false;
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
-    const T v0 = S[j][a0], v1 = S[j][a1];
-    const T vu = S[j][ur];
+    const T v0 = colv[j & 1][a0], v1 = colv[j & 1][a1];
+    const T vu = colv[j & 1][ur];
     T best = T(-1), sv = T(0);
     int bi = 0, bpos = 1 << 30;
     if (!used0) { best = tabs(v0); sv = v0; bi = a0; bpos = pos0; }
@@ -85,11 +145,9 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
       if (ob > best || (ob == best && op < bpos)) { best = ob; sv = os; bi = oi; bpos = op; }
     }
     const int p = bi, lp = bpos;
-    // physical row at logical position j (before this step's swap)
     const unsigned m0 = __ballot_sync(0xffffffffu, pos0 == j);
     const unsigned m1 = __ballot_sync(0xffffffffu, pos1 == j);
     const int rj = m0 ? (__ffs(m0) - 1) : (32 + __ffs(m1) - 1);
-    // used status of my update row (before marking the pivot)
     const bool uu0 = __shfl_sync(0xffffffffu, used0, ur & 31);
     const bool uu1 = __shfl_sync(0xffffffffu, used1, ur & 31);
     const bool urow_used = (ur >> 5) ? uu1 : uu0;
@@ -101,21 +159,28 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
       zero = true;
     } else if (ur < nb && ur != p && !urow_used) {
       const T m = vu * rp;
-      __syncwarp(0xffffffffu & __activemask());
-      if (cp == 0) S[j][ur] = m;
-      const int cs = j + 1 + ((cp - (j + 1)) & 3);
-      T pv[NB / 4], ov[NB / 4];
+      const VT* prow = reinterpret_cast<const VT*>(&S[p][0]);
+      VT* orow = reinterpret_cast<VT*>(&S[ur][0]);
+      const int q0 = j / V;                      // chunk holding column j
 #pragma unroll
-      for (int i = 0; i < NB / 4; ++i) {
-        const int c = cs + 4 * i;
-        if (c < nb) { pv[i] = S[c][p]; ov[i] = S[c][ur]; }
-      }
+      for (int i = 0; i < NCH / 4; ++i) {
+        const int qq = cp + 4 * i;
+        if (qq >= q0 && qq * V < nb) {
+          const VT pv = prow[qq];
+          VT ov = orow[qq];
 #pragma unroll
-      for (int i = 0; i < NB / 4; ++i) {
-        const int c = cs + 4 * i;
-        if (c < nb) S[c][ur] = ov[i] - m * pv[i];
+          for (int e = 0; e < V; ++e) {
+            const int c = qq * V + e;
+            if (c == j) vset<T>(ov, e, m);
+            else if (c > j) vset<T>(ov, e, vget<T>(ov, e) - m * vget<T>(pv, e));
+          }
+          orow[qq] = ov;
+        }
       }
     }
+    // the lane holding column j + 1 of row ur publishes it for the next step
+    // (rows not updated here are not written by anyone in this step)
+    if (j + 1 < nb && cp == (((j + 1) / V) & 3)) colv[(j + 1) & 1][ur] = S[ur][j + 1];
     __syncthreads();
   }
   if (zero && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
@@ -123,7 +188,7 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
   __syncthreads();
   for (int e = tid; e < NB * NB; e += kDiagThreads) {
     const int rr = e & (NB - 1), cc = e >> 6;
-    if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[cc][order[rr]];
+    if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[order[rr]][cc];
   }
   if (tid < nb) ipiv[k + tid] = (int32_t)(k + lpiv[tid]);
 }
@@ -131,31 +196,39 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
 // ----------------------------------------------------------------------------
 // (2) after k_diag, two kernels:
 //  * k_l21: L21 = A21 U11^-1, one row per thread, right-looking
-//    (x_j *= 1/U_jj, then x_l -= x_j U_jl for l > j) with U11 broadcast from
-//    shared memory; the largest |L21| is the GEPP certificate;
+//    (x_j *= 1/U_jj, then x_l -= x_j U_jl for l > j) with the rows of U11
+//    read as 16-byte vectors from shared memory; the largest |L21| is the
+//    GEPP certificate;
 //  * k_u12: for columns outside the block, the row swaps of the block, and for
-//    columns right of it U12 = L11^-1 P A12 by forward substitution (unit lower
-//    L11 broadcast from shared memory), one column per thread; columns are
-//    staged through shared memory so that global accesses are coalesced.
-constexpr int kApplyThreads = 128;
+//    columns right of it U12 = L11^-1 P A12 by forward substitution (columns
+//    of the unit lower L11 read as 16-byte vectors), one column per thread;
+//    columns are staged through shared memory so that global accesses are
+//    coalesced.
+constexpr int kApplyThreads = 64;
 template <class T> constexpr size_t u12_smem() {
-  return (size_t)NB * kDP * sizeof(T) + (size_t)kApplyThreads * kDP * sizeof(T) + 2 * NB * sizeof(int) + 64;
+  return (size_t)NB * rpitch<T>() * sizeof(T) + (size_t)kApplyThreads * (NB + 1) * sizeof(T) +
+         2 * NB * sizeof(int) + 64;
 }
 
 template <class T>
 __global__ void __launch_bounds__(kApplyThreads)
 k_l21(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ cert) {
-  __shared__ T D[NB][kDP];     // D[c][r] = block(r, c)
+  typedef typename V16<T>::type VT;
+  constexpr int V = V16<T>::n, RP = rpitch<T>();
+  __shared__ __align__(16) T Ut[NB][RP];   // Ut[j][l] = U(j, l), zero below the diagonal
   __shared__ T rdiag[NB];
   __shared__ float red[kApplyThreads / 32];
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x;
-  for (int e = tid; e < NB * NB; e += kApplyThreads) {
-    const int r = e & (NB - 1), c = e >> 6;
-    D[c][r] = (r < nb && c < nb) ? A[(k + c) * lda + (k + r)] : ((r == c) ? T(1) : T(0));
-  }
+  stage_block<kApplyThreads, T>(
+      tid,
+      [&](int jr, int lc) {   // row jr of U, column lc
+        if (jr < nb && lc < nb) return (lc >= jr) ? A[(k + lc) * lda + (k + jr)] : T(0);
+        return (jr == lc) ? T(1) : T(0);
+      },
+      [&](int jr, int lc, T v) { Ut[jr][lc] = v; });
   __syncthreads();
-  if (tid < NB) rdiag[tid] = T(1) / D[tid][tid];
+  if (tid < NB) rdiag[tid] = T(1) / Ut[tid][tid];
   __syncthreads();
   const int64_t row = k + nb + (int64_t)blockIdx.x * kApplyThreads + tid;
   float lmax = 0.f;
@@ -165,15 +238,27 @@ k_l21(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ 
     for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? A[(k + j) * lda + row] : T(0);
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
+      // keeps the compiler from hoisting later rows of U (and their
+      // registers) above this step
+      asm volatile("" ::: "memory");
       const T xj = x[j] * rdiag[j];
       x[j] = xj;
+      const VT* urow = reinterpret_cast<const VT*>(&Ut[j][0]);
 #pragma unroll
-      for (int l = j + 1; l < NB; ++l) x[l] -= xj * D[l][j];
+      for (int q = (j + 1) / V; q < NB / V; ++q) {
+        const VT u = urow[q];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+          const int lc = q * V + e;
+          if (lc > j) x[lc] -= xj * vget<T>(u, e);
+        }
+      }
     }
+    T* const Ao = opaque_ptr(A);
 #pragma unroll
     for (int j = 0; j < NB; ++j) {
       if (j < nb) {
-        A[(k + j) * lda + row] = x[j];
+        Ao[(k + j) * lda + row] = x[j];
         lmax = fmaxf(lmax, (float)tabs(x[j]));
       }
     }
@@ -192,17 +277,21 @@ k_l21(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ 
 template <class T>
 __global__ void __launch_bounds__(kApplyThreads)
 k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv) {
+  typedef typename V16<T>::type VT;
+  constexpr int V = V16<T>::n, RP = rpitch<T>();
   extern __shared__ __align__(16) unsigned char dsm[];
-  T (*D)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm);                                      // D[c][r] = block(r, c)
-  T (*tile)[kDP] = reinterpret_cast<T (*)[kDP]>(dsm + (size_t)NB * kDP * sizeof(T));     // tile[col][r]
-  int* perm = reinterpret_cast<int*>(dsm + (size_t)NB * kDP * sizeof(T) + (size_t)kApplyThreads * kDP * sizeof(T));
+  T (*Lc)[RP] = reinterpret_cast<T (*)[RP]>(dsm);                                          // Lc[j][r] = L(r, j)
+  T (*tile)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm + (size_t)NB * RP * sizeof(T));   // tile[col][r]
+  int* perm = reinterpret_cast<int*>(dsm + (size_t)NB * RP * sizeof(T) + (size_t)kApplyThreads * (NB + 1) * sizeof(T));
   int* lp = perm + NB;
   const int nb = (int)imin64(NB, n - k);
   const int tid = threadIdx.x;
-  for (int e = tid; e < NB * NB; e += kApplyThreads) {
-    const int r = e & (NB - 1), c = e >> 6;
-    D[c][r] = (r < nb && c < nb) ? A[(k + c) * lda + (k + r)] : ((r == c) ? T(1) : T(0));
-  }
+  stage_block<kApplyThreads, T>(
+      tid,
+      [&](int r, int j) {   // L(r, j): strictly lower part of the block
+        return (r < nb && j < nb && r > j) ? A[(k + j) * lda + (k + r)] : T(0);
+      },
+      [&](int r, int j, T v) { Lc[j][r] = v; });
   if (tid < nb) lp[tid] = (int)(ipiv[k + tid] - k);
   __syncthreads();
   if (tid == 0) {
@@ -212,49 +301,56 @@ k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __res
       const int t0 = perm[j]; perm[j] = perm[p]; perm[p] = t0;
     }
   }
-  __syncthreads();
   const int64_t nother = n - nb;
+  const int64_t g = blockIdx.x;   // one group of kApplyThreads columns per CTA
+  static_assert(kApplyThreads == NB, "the column tile is NB x NB");
+  stage_block<kApplyThreads, T>(
+      tid,
+      [&](int r, int cc) {
+        const int64_t qq = g * kApplyThreads + cc;
+        T v = T(0);
+        if (qq < nother && r < nb) {
+          const int64_t c = (qq < k) ? qq : qq + nb;
+          v = A[c * lda + k + r];
+        }
+        return v;
+      },
+      [&](int r, int cc, T v) { tile[cc][r] = v; });
+  __syncthreads();
   {
-    const int64_t g = blockIdx.x;   // one group of kApplyThreads columns per CTA
-    // stage kApplyThreads columns (rows k..k+nb), coalesced along the rows
-    for (int e = tid; e < NB * kApplyThreads; e += kApplyThreads) {
-      const int r = e & (NB - 1), cc = e >> 6;
-      const int64_t qq = g * kApplyThreads + cc;
-      T v = T(0);
-      if (qq < nother && r < nb) {
-        const int64_t c = (qq < k) ? qq : qq + nb;
-        v = A[c * lda + k + r];
-      }
-      tile[cc][r] = v;
-    }
-    __syncthreads();
-    {
-      const int64_t qq = g * kApplyThreads + tid;
-      if (qq < nother) {
-        const int64_t c = (qq < k) ? qq : qq + nb;
-        T x[NB];
+    const int64_t qq = g * kApplyThreads + tid;
+    if (qq < nother) {
+      const int64_t c = (qq < k) ? qq : qq + nb;
+      T x[NB];
 #pragma unroll
-        for (int r = 0; r < NB; ++r) x[r] = tile[tid][perm[r]];
-        if (c >= k + nb) {
+      for (int r = 0; r < NB; ++r) x[r] = tile[tid][perm[r]];
+      if (c >= k + nb) {
 #pragma unroll
-          for (int j = 0; j < NB; ++j) {
-            const T xj = x[j];
+        for (int j = 0; j < NB; ++j) {
+          const T xj = x[j];
+          const VT* lcol = reinterpret_cast<const VT*>(&Lc[j][0]);
 #pragma unroll
-            for (int r = j + 1; r < NB; ++r) x[r] -= D[j][r] * xj;
+          for (int q = (j + 1) / V; q < NB / V; ++q) {
+            const VT u = lcol[q];
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+              const int r = q * V + e;
+              if (r > j) x[r] -= vget<T>(u, e) * xj;
+            }
           }
         }
+      }
 #pragma unroll
-        for (int r = 0; r < NB; ++r) tile[tid][r] = x[r];
-      }
+      for (int r = 0; r < NB; ++r) tile[tid][r] = x[r];
     }
-    __syncthreads();
-    for (int e = tid; e < NB * kApplyThreads; e += kApplyThreads) {
-      const int r = e & (NB - 1), cc = e >> 6;
-      const int64_t qq = g * kApplyThreads + cc;
-      if (qq < nother && r < nb) {
-        const int64_t c = (qq < k) ? qq : qq + nb;
-        A[c * lda + k + r] = tile[cc][r];
-      }
+  }
+  __syncthreads();
+  for (int e = tid; e < NB * kApplyThreads; e += kApplyThreads) {
+    const int r = e & (NB - 1), cc = e >> 6;
+    const int64_t qq = g * kApplyThreads + cc;
+    if (qq < nother && r < nb) {
+      const int64_t c = (qq < k) ? qq : qq + nb;
+      A[c * lda + k + r] = tile[cc][r];
     }
   }
 }
