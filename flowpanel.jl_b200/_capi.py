@@ -24,7 +24,7 @@ FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND = range(4)
 EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count", "fp_set_geometry",
            "fp_set_wake", "fp_assemble", "fp_get_aic", "fp_set_rhs", "fp_factor", "fp_solve",
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
-           "fp_kernel_launches", "fp_tc_selftest")
+           "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc")
 
 
 class SolveOpts(C.Structure):
@@ -78,6 +78,7 @@ def lib():
                                     C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
         L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
         L.fp_adjoint_solve.argtypes = [vp, _dp, C.c_int64, _dp]
+        L.fp_lu_solve_noalloc.argtypes = [vp, C.c_void_p, C.c_int64, C.c_int64]
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
         L.fp_measure_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
         L.fp_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -198,6 +199,13 @@ class Context:
         lam = np.empty_like(ybar)
         self._chk(self._L.fp_adjoint_solve(self.h, _d(ybar), ybar.shape[0], _d(lam)))
         return lam
+
+    def lu_solve_noalloc(self, dev_ptr, ldb, k=1):
+        """In-place FP64 solve of the N x k column-major device array at
+        ``dev_ptr`` (an integer address on this context's device) with the
+        factors of the last ``factor(FP_PREC_FP64)``; the library allocates
+        no device memory for it."""
+        self._chk(self._L.fp_lu_solve_noalloc(self.h, C.c_void_p(dev_ptr), ldb, k))
 
     def kernel_launches(self):
         n = C.c_int64()

@@ -537,6 +537,16 @@ int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stat
   return FP_OK;
 }
 
+int fp_lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k) {
+  if (check_ctx(c)) return FP_EINVAL;
+  FP_CUDA_TRY(c->err, cudaSetDevice(c->device));
+  if (!B || k <= 0 || ldb < c->N) return c->err.set(FP_EINVAL, "fp_lu_solve_noalloc: B must be N x k with ldb >= N");
+  if (c->factored != FP_PREC_FP64)
+    return c->err.set(FP_ESTATE, "fp_lu_solve_noalloc: no FP64 factors (call fp_factor with FP_PREC_FP64)");
+  if (int rc = lu_solve_noalloc(c, B, ldb, k)) return rc;
+  return consume_status(c);
+}
+
 int fp_solve_body(fp_ctx* c, int element, double kerneloffset, double kernelcutoff,
                   const double* Uinfs, int64_t k, const fp_solve_opts* opts, double* x,
                   fp_stats* stats) {

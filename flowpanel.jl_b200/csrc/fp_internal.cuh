@@ -101,6 +101,9 @@ int convert_f64_f32(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, 
 int axpy_f32_to_f64(fp_ctx* c, const float* d, double* x, int64_t n, int64_t k, int64_t ld);
 template <class T>
 int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda);
+// FP64 solve with the context's factors on caller memory, flags of the
+// triangular solves in a static device array (no device allocation)
+int lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k);
 int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out);
 constexpr int kLuNB = 64;        // block size of the factorisation and the solves
 constexpr int kGemvSplitHost = 16;

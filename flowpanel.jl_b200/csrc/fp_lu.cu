@@ -19,6 +19,8 @@
 // on, subtract their contribution and multiply by the precomputed inverse of
 // the diagonal block.
 #include <cfloat>
+#include <mutex>
+#include <string>
 
 #include "fp_internal.cuh"
 
@@ -922,6 +924,96 @@ int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, doub
   k_colnorm2<<<(unsigned)k, 256, 0, c->stream>>>(a, n, lda, d_out);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+// ----------------------------------------------------------------------------
+// Allocation-free solve with the FP64 factors of a context
+// (fp_lu_solve_noalloc). Some callers cannot let a library allocate device
+// memory while they solve: a host program that hands every byte of the device
+// to its own pool or arena (a Julia session whose CUDA.jl pool holds the
+// device memory, a service with a fixed memory budget), or one that re-solves
+// inside a time-stepping or design loop where a cudaMalloc may synchronise the
+// device or fail once the pool is full. For them the ready flags and the
+// ticket counter of k_trs live in the file-scope array below instead of a
+// context buffer; everything else the solve touches (factors, inverses of the
+// diagonal blocks, pivots, status word) was allocated by fp_factor, and the
+// right-hand sides are the caller's.
+//
+// The array holds one flag per 64-row block plus the ticket, so n is limited
+// to kNoAllocMaxN unknowns (4 KiB per device). Every flag and the ticket must
+// be zero when a sweep starts; each sweep clears them itself with
+// cudaMemsetAsync on the context's stream, so callers initialise nothing.
+// There is one array per device, shared by every context on that device:
+// calls that overlap in time on one device (from several host threads) race
+// on it and return wrong results or FP_ETIMEOUT, so they must be serialised.
+constexpr int64_t kNoAllocMaxN = 65536;
+constexpr int64_t kNoAllocMaxBlocks = kNoAllocMaxN / NB;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) unsigned int g_trs_scratch[kNoAllocMaxBlocks + 1];
+
+static std::mutex g_trs_scratch_mu;
+static unsigned int* g_trs_scratch_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_trs_scratch on the context's device, which must be the
+// current device. The first call on a device resolves it with
+// cudaGetSymbolAddress (which can load this library's device code onto that
+// device); later calls return the cached address.
+static int trs_scratch_address(fp_ctx* c, unsigned int** out) {
+  if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+    return c->err.set(FP_EINVAL, "fp_lu_solve_noalloc: device index beyond " +
+                                     std::to_string(kNoAllocMaxDevices - 1));
+  std::lock_guard<std::mutex> lock(g_trs_scratch_mu);
+  unsigned int*& slot = g_trs_scratch_addr[c->device];
+  if (!slot) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_trs_scratch);
+    if (e != cudaSuccess)
+      return c->err.set(FP_ECUDA, std::string("cudaGetSymbolAddress(g_trs_scratch): ") + cudaGetErrorString(e));
+    slot = static_cast<unsigned int*>(p);
+  }
+  *out = slot;
+  return FP_OK;
+}
+
+template <bool LOWER, int KR>
+static int run_trs_static(fp_ctx* c, int64_t n, double* B, int64_t ldb, unsigned int* flags) {
+  const int64_t nblk = (n + NB - 1) / NB;
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
+  const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
+  k_trs<double, LOWER, KR><<<grid, kTrsThreads, 0, c->stream>>>(c->d_LU, c->ld, n, c->d_dinv64, B, ldb, flags,
+                                                                flags + nblk, c->d_status);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
+int lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k) {
+  const int64_t n = c->N;
+  if (n > kNoAllocMaxN)
+    return c->err.set(FP_EINVAL, "fp_lu_solve_noalloc: " + std::to_string(n) +
+                                     " unknowns exceed the static scratch limit of " +
+                                     std::to_string(kNoAllocMaxN));
+  unsigned int* flags = nullptr;
+  if (int rc = trs_scratch_address(c, &flags)) return rc;
+  const int64_t nblk = (n + NB - 1) / NB;
+  k_apply_piv<double><<<(unsigned)((nblk * k + 127) / 128), 128, 0, c->stream>>>(B, ldb, n, k, c->d_ipiv, false);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  for (int64_t q0 = 0; q0 < k;) {
+    const int64_t left = k - q0;
+    const int kr = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+    double* Bq = B + q0 * ldb;
+    int rc;
+    switch (kr) {
+      case 8: rc = run_trs_static<true, 8>(c, n, Bq, ldb, flags); if (!rc) rc = run_trs_static<false, 8>(c, n, Bq, ldb, flags); break;
+      case 4: rc = run_trs_static<true, 4>(c, n, Bq, ldb, flags); if (!rc) rc = run_trs_static<false, 4>(c, n, Bq, ldb, flags); break;
+      case 2: rc = run_trs_static<true, 2>(c, n, Bq, ldb, flags); if (!rc) rc = run_trs_static<false, 2>(c, n, Bq, ldb, flags); break;
+      default: rc = run_trs_static<true, 1>(c, n, Bq, ldb, flags); if (!rc) rc = run_trs_static<false, 1>(c, n, Bq, ldb, flags); break;
+    }
+    if (rc) return rc;
+    q0 += kr;
+  }
   return FP_OK;
 }
 

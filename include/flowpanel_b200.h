@@ -122,6 +122,26 @@ int fp_factor(fp_ctx* ctx, int precision);
  * x is N x k (column-major) on the host. opts may be NULL (LU, FP64). */
 int fp_solve(fp_ctx* ctx, double* x, int64_t k, const fp_solve_opts* opts, fp_stats* stats);
 
+/* Solve A X = B in place with the FP64 LU factors of the last
+ * fp_factor(ctx, FP_PREC_FP64), on caller-owned DEVICE memory, allocating no
+ * device memory. No counterpart in the reference (its solves allocate their
+ * results); it is for callers that cannot let a library allocate during a
+ * solve: a host program whose own pool or arena holds the device memory (a
+ * Julia session with CUDA.jl's pool, a fixed-budget service), or a loop of
+ * re-solves where a cudaMalloc could synchronise the device or fail.
+ * B: n x k column-major on ctx's device, leading dimension ldb >= n; it is
+ * read and written on ctx's stream, which does not wait for the caller's
+ * streams, so finish writing B first. The call returns when the solve is done.
+ * Limit: n <= 65536 (FP_EINVAL beyond): the triangular solves keep their
+ * ready flags and ticket counter in a fixed static device array (4 KiB per
+ * device); each sweep zeroes them itself, so nothing needs initialising.
+ * The first call on each device resolves that array's address
+ * (cudaGetSymbolAddress, which can load the library's device code onto the
+ * device): make it before any stream capture. Calls that overlap in time on
+ * one device (several host threads, several contexts) share the array and
+ * race, giving wrong results or FP_ETIMEOUT: serialise them. */
+int fp_lu_solve_noalloc(fp_ctx* ctx, double* B, int64_t ldb, int64_t k);
+
 /* End-to-end solve(body, Uinfs, Das, Dbs; solver) for a body already given by
  * fp_set_geometry/fp_set_wake: assemble + RHS + factor + solve
  * (src/FLOWPanel_liftingbody.jl:172-216, src/FLOWPanel_multibody.jl:312-364,
