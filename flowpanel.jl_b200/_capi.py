@@ -18,13 +18,14 @@ FP_OK, FP_EINVAL, FP_ESINGULAR, FP_ENOCONV, FP_ECUDA, FP_ETIMEOUT, FP_ESTATE = r
 FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING = 0, 1
 FP_PREC_FP64, FP_PREC_MIXED = 0, 1
 FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
-FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND = range(4)
+FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP = range(6)
 
 # every symbol the header declares
 EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count", "fp_set_geometry",
            "fp_set_wake", "fp_assemble", "fp_get_aic", "fp_set_rhs", "fp_factor", "fp_solve",
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
-           "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc")
+           "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
+           "fp_uind_vjp")
 
 
 class SolveOpts(C.Structure):
@@ -79,6 +80,8 @@ def lib():
         L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
         L.fp_adjoint_solve.argtypes = [vp, _dp, C.c_int64, _dp]
         L.fp_lu_solve_noalloc.argtypes = [vp, C.c_void_p, C.c_int64, C.c_int64]
+        L.fp_assembly_vjp.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.fp_uind_vjp.argtypes = [vp, _dp, _dp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp]
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
         L.fp_measure_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
         L.fp_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -117,6 +120,7 @@ class Context:
             raise FlowPanelError(rc, f"fp_ctx_create failed on device {device}")
         self.h = h
         self.N = 0
+        self.nsh = 0
 
     def close(self):
         if getattr(self, "h", None):
@@ -141,11 +145,13 @@ class Context:
         self._chk(self._L.fp_set_geometry(self.h, _d(nodes), nodes.shape[0], _i(offs), _i(pn), len(offs) - 1,
                                           _d(cps), _d(normals), _d(cp_offset)))
         self.N = len(offs) - 1
+        self.nsh = 0
 
     def set_wake(self, shedding, Das, Dbs):
         sh = np.ascontiguousarray(np.reshape(shedding, (-1, 6)), dtype=np.int32)
         Das, Dbs = _f64(np.reshape(Das, (-1, 3))), _f64(np.reshape(Dbs, (-1, 3)))
         self._chk(self._L.fp_set_wake(self.h, _i(sh), sh.shape[0], _d(Das), _d(Dbs)))
+        self.nsh = sh.shape[0]
 
     def assemble(self, element, kerneloffset=1e-8, kernelcutoff=1e-14, precision=FP_PREC_FP64):
         self._chk(self._L.fp_assemble(self.h, element, kerneloffset, kernelcutoff, precision))
@@ -199,6 +205,34 @@ class Context:
         lam = np.empty_like(ybar)
         self._chk(self._L.fp_adjoint_solve(self.h, _d(ybar), ybar.shape[0], _d(lam)))
         return lam
+
+    def assembly_vjp(self, Uinfs, nnodes, lam=None, gamma=None):
+        """Gradient of lambda^T (b - A Gamma) (see fp_assembly_vjp); lam / gamma
+        None use the device-resident adjoint / primal solutions. Returns a dict
+        of dnodes (nnodes, 3), dcps, dnormals, dUinfs (N, 3), dDas, dDbs (nsh, 3)."""
+        n = self.N
+        U = _f64(np.reshape(Uinfs, (n, 3)))
+        nsh = self.nsh
+        out = {"dnodes": np.zeros((nnodes, 3)), "dcps": np.zeros((n, 3)), "dnormals": np.zeros((n, 3)),
+               "dUinfs": np.zeros((n, 3)), "dDas": np.zeros((max(nsh, 1), 3)), "dDbs": np.zeros((max(nsh, 1), 3))}
+        self._chk(self._L.fp_assembly_vjp(self.h, _d(_f64(lam)), _d(_f64(gamma)), _d(U), _d(out["dnodes"]),
+                                          _d(out["dcps"]), _d(out["dnormals"]), _d(out["dUinfs"]),
+                                          _d(out["dDas"]), _d(out["dDbs"])))
+        out["dDas"], out["dDbs"] = out["dDas"][:nsh], out["dDbs"][:nsh]
+        return out
+
+    def uind_vjp(self, strengths, targets, wbar, nnodes):
+        """Gradient of sum_i wbar_i . Uind(targets_i) (see fp_uind_vjp)."""
+        X = _f64(np.reshape(targets, (-1, 3)))
+        W = _f64(np.reshape(wbar, (-1, 3)))
+        m = X.shape[0]
+        nsh = self.nsh
+        out = {"dtargets": np.zeros((m, 3)), "dstrengths": np.zeros(self.N), "dnodes": np.zeros((nnodes, 3)),
+               "dDas": np.zeros((max(nsh, 1), 3)), "dDbs": np.zeros((max(nsh, 1), 3))}
+        self._chk(self._L.fp_uind_vjp(self.h, _d(_f64(strengths)), _d(X), m, _d(W), _d(out["dtargets"]),
+                                      _d(out["dstrengths"]), _d(out["dnodes"]), _d(out["dDas"]), _d(out["dDbs"])))
+        out["dDas"], out["dDbs"] = out["dDas"][:nsh], out["dDbs"][:nsh]
+        return out
 
     def lu_solve_noalloc(self, dev_ptr, ldb, k=1):
         """In-place FP64 solve of the N x k column-major device array at

@@ -92,6 +92,10 @@ void free_matrices(fp_ctx* c) {
   if (c->d_linv) { cudaFree(c->d_linv); c->d_linv = nullptr; }
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
   dfree(c->d_V); dfree(c->d_h);
+  dfree(c->d_ab); dfree(c->d_ax); dfree(c->d_ar); dfree(c->d_aw32); dfree(c->d_anorms);
+  c->cap_adj = 0;
+  dfree(c->d_vjp);
+  c->cap_vjp = 0;
   for (int i = 0; i < 4; ++i) dfree(c->d_tc[i]);
   c->tc_cap = 0;
   c->cap_rhs = 0; c->cap_gmres_m = 0;
@@ -239,6 +243,7 @@ int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_panels, pr.data(), npanels * sizeof(PanelRec), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_src, sr.data(), npanels * sizeof(SourceRec), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_tgt, tgt.data(), 6 * npanels * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  c->h_tgt = tgt;
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   c->has_geometry = true;
   c->nsh = 0;
@@ -434,12 +439,13 @@ static void normalize_opts(fp_solve_opts& o) {
 
 // max over RHS of ||r_q|| / ||b_q||
 static int residual_ratio(fp_ctx* c, const double* r, const double* b, int64_t k, double* out,
-                          bool need_b) {
-  if (int rc = colnorm2(c, r, c->N, c->ld, k, c->d_norms)) return rc;
+                          bool need_b, double* norms = nullptr) {
+  if (!norms) norms = c->d_norms;
+  if (int rc = colnorm2(c, r, c->N, c->ld, k, norms)) return rc;
   if (need_b)
-    if (int rc = colnorm2(c, b, c->N, c->ld, k, c->d_norms + k)) return rc;
+    if (int rc = colnorm2(c, b, c->N, c->ld, k, norms + k)) return rc;
   std::vector<double> h(2 * k);
-  FP_CUDA_TRY(c->err, cudaMemcpyAsync(h.data(), c->d_norms, 2 * k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(h.data(), norms, 2 * k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   double m = 0;
   for (int64_t q = 0; q < k; ++q) {
@@ -595,9 +601,247 @@ int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targe
   return FP_OK;
 }
 
+static int ensure_adjoint(fp_ctx* c, int64_t k) {
+  if (k <= c->cap_adj) return FP_OK;
+  dfree(c->d_ab); dfree(c->d_ax); dfree(c->d_ar); dfree(c->d_aw32);
+  c->cap_adj = 0;
+  const size_t n = (size_t)c->ld * k;
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ab, n * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ax, n * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ar, n * sizeof(double)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_aw32, n * sizeof(float)));
+  dfree(c->d_anorms);
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_anorms, 2 * k * sizeof(double)));
+  c->cap_adj = k;
+  return FP_OK;
+}
+
+// A^T lambda = ybar on the device with the saved factors; the solution stays
+// in d_ax. FP64 factors: one transposed LU solve. FP32 factors: iterative
+// refinement with the transposed FP32 solve and the FP64 residual
+// ybar - A^T lambda on the stored FP64 AIC, to a relative residual of 1e-12.
+static int adjoint_device(fp_ctx* c, int64_t k) {
+  const int64_t n = c->N, ld = c->ld;
+  int rc;
+  c->adj_iters = 0;
+  c->adj_relres = 0;
+  if (c->factored == FP_PREC_FP64) {
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_ax, c->d_ab, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    return lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_ax, ld, k, true);
+  }
+  const double tol = 1e-12;
+  const int maxit = 10;
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_ax, 0, ld * k * sizeof(double), c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_ar, c->d_ab, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  double rr = 0, prev = 1e300;
+  bool first = true;
+  for (int it = 0; it < maxit; ++it) {
+    if ((rc = convert_f64_f32(c, c->d_ar, c->d_aw32, n, k, ld, ld))) return rc;
+    if ((rc = lu_solve<float>(c, c->d_G32, n, ld, c->d_ipiv, c->d_aw32, ld, k, true))) return rc;
+    if ((rc = axpy_f32_to_f64(c, c->d_aw32, c->d_ax, n, k, ld))) return rc;
+    if ((rc = gemvT_residual(c, c->d_G, n, ld, c->d_ax, c->d_ab, c->d_ar, k))) return rc;
+    if ((rc = residual_ratio(c, c->d_ar, c->d_ab, k, &rr, first, c->d_anorms))) return rc;
+    first = false;
+    c->adj_iters = it + 1;
+    c->adj_relres = rr;
+    if (rr <= tol) return FP_OK;
+    if (rr > 0.5 * prev) break;
+    prev = rr;
+  }
+  return c->err.set(FP_ENOCONV, "fp_adjoint_solve: refinement with the FP32 factors stalled at relative residual " +
+                                    std::to_string(rr));
+}
+
 int fp_adjoint_solve(fp_ctx* c, const double* ybar, int64_t k, double* lambda) {
   if (check_ctx(c)) return FP_EINVAL;
-  return c->err.set(FP_EINVAL, "fp_adjoint_solve: transposed solve not built yet");
+  FP_CUDA_TRY(c->err, cudaSetDevice(c->device));
+  if (!ybar || !lambda || k <= 0) return c->err.set(FP_EINVAL, "fp_adjoint_solve: bad arguments");
+  if (c->factored < 0) return c->err.set(FP_ESTATE, "fp_adjoint_solve: no factors (call fp_factor)");
+  const int64_t n = c->N, ld = c->ld;
+  int rc;
+  if ((rc = ensure_adjoint(c, k))) return rc;
+  FP_CUDA_TRY(c->err, cudaMemcpy2DAsync(c->d_ab, ld * sizeof(double), ybar, n * sizeof(double), n * sizeof(double), k,
+                                        cudaMemcpyHostToDevice, c->stream));
+  if (time_begin(c)) return FP_ECUDA;
+  rc = adjoint_device(c, k);
+  double ms = 0;
+  if (time_end(c, &ms)) return FP_ECUDA;
+  c->kms[FP_STAGE_ADJOINT] = ms;
+  if (rc) return rc;
+  if ((rc = consume_status(c))) return rc;
+  FP_CUDA_TRY(c->err, cudaMemcpy2DAsync(lambda, n * sizeof(double), c->d_ax, ld * sizeof(double), n * sizeof(double), k,
+                                        cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  return FP_OK;
+}
+
+// Device workspace of the reverse pass for m targets.
+struct VjpBufs {
+  double *x, *w, *gX, *U, *gvert, *gs, *gwake, *lam, *gam;
+  size_t zero_count;   // gX .. gwake are contiguous and zeroed before a pass
+};
+static int vjp_buffers(fp_ctx* c, int64_t m, VjpBufs& b) {
+  const size_t n = (size_t)c->N, nsh = (size_t)c->nsh;
+  const size_t need = 3 * m + 3 * m + 3 * m + 3 * m + 12 * n + n + kWakeGradHost * nsh + n + n;
+  if (need > c->cap_vjp) {
+    dfree(c->d_vjp);
+    c->cap_vjp = 0;
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_vjp, need * sizeof(double)));
+    c->cap_vjp = need;
+  }
+  double* p = c->d_vjp;
+  b.x = p; p += 3 * m;
+  b.w = p; p += 3 * m;
+  b.gX = p; p += 3 * m;
+  b.U = p; p += 3 * m;
+  b.gvert = p; p += 12 * n;
+  b.gs = p; p += n;
+  b.gwake = p; p += kWakeGradHost * nsh;
+  b.lam = p; p += n;
+  b.gam = p;
+  b.zero_count = 3 * m + 3 * m + 12 * n + n + kWakeGradHost * nsh;
+  return FP_OK;
+}
+
+// Adds the per-panel vertex gradients (N x 12) and the wake TE-node
+// gradients to dnodes (3 x nnodes), and writes dDas / dDbs.
+static void scatter_vjp(fp_ctx* c, const std::vector<double>& gvert, const std::vector<double>& gwake,
+                        double* dnodes, double* dDas, double* dDbs) {
+  const int64_t nnodes = (int64_t)c->h_nodes.size() / 3;
+  if (dnodes) {
+    std::fill(dnodes, dnodes + 3 * nnodes, 0.0);
+    for (int64_t j = 0; j < c->N; ++j) {
+      const int o = c->h_offsets[j], nn = c->h_offsets[j + 1] - o;
+      for (int k = 0; k < nn; ++k) {
+        const int64_t ni = c->h_pnodes[o + k];
+        for (int d = 0; d < 3; ++d) dnodes[3 * ni + d] += gvert[12 * j + 3 * k + d];
+      }
+    }
+  }
+  for (int64_t e = 0; e < c->nsh; ++e) {
+    const int32_t* s = c->h_shed.data() + 6 * e;
+    const double* g = gwake.data() + kWakeGradHost * e;
+    if (dnodes) {
+      auto add = [&](int panel, int local, const double* gg) {
+        const int64_t ni = c->h_pnodes[c->h_offsets[panel] + local];
+        for (int d = 0; d < 3; ++d) dnodes[3 * ni + d] += gg[d];
+      };
+      add(s[0], s[1], g + 0);
+      add(s[0], s[2], g + 3);
+      if (s[3] >= 0) {
+        add(s[3], s[4], g + 6);
+        add(s[3], s[5], g + 9);
+      }
+    }
+    if (dDas) for (int d = 0; d < 3; ++d) dDas[3 * e + d] = g[12 + d];
+    if (dDbs) for (int d = 0; d < 3; ++d) dDbs[3 * e + d] = g[15 + d];
+  }
+}
+
+int fp_assembly_vjp(fp_ctx* c, const double* lambda, const double* gamma, const double* Uinfs,
+                    double* dnodes, double* dcps, double* dnormals, double* dUinfs, double* dDas,
+                    double* dDbs) {
+  if (check_ctx(c)) return FP_EINVAL;
+  FP_CUDA_TRY(c->err, cudaSetDevice(c->device));
+  if (c->assembled != FP_ELEMENT_VORTEXRING)
+    return c->err.set(FP_ESTATE, "fp_assembly_vjp: assemble a vortex-ring body first");
+  if (!lambda && c->cap_adj < 1)
+    return c->err.set(FP_ESTATE, "fp_assembly_vjp: no lambda given and no fp_adjoint_solve result on the device");
+  if (!gamma && c->cap_rhs < 1)
+    return c->err.set(FP_ESTATE, "fp_assembly_vjp: no gamma given and no fp_solve result on the device");
+  if ((dnormals || dUinfs) && !Uinfs)
+    return c->err.set(FP_EINVAL, "fp_assembly_vjp: dnormals / dUinfs need Uinfs");
+  const int64_t n = c->N;
+  VjpBufs b;
+  int rc;
+  if ((rc = vjp_buffers(c, n, b))) return rc;
+  if (time_begin(c)) return FP_ECUDA;
+  const double* dl = c->d_ax;
+  const double* dg = c->d_x;
+  if (lambda) {
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(b.lam, lambda, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    dl = b.lam;
+  }
+  if (gamma) {
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(b.gam, gamma, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    dg = b.gam;
+  }
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(b.gX, 0, b.zero_count * sizeof(double), c->stream));
+  if ((rc = launch_vjp_cotangent(c, dl, b.w))) return rc;
+  if ((rc = launch_pair_vjp(c, dg, c->d_tgt, b.w, n, b.gX, b.U, b.gvert, b.gs, b.gwake))) return rc;
+  std::vector<double> hX(3 * n), hU(3 * n), hv(12 * n), hw(kWakeGradHost * c->nsh), hl(n);
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hX.data(), b.gX, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hU.data(), b.U, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hv.data(), b.gvert, 12 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (c->nsh > 0)
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(hw.data(), b.gwake, kWakeGradHost * c->nsh * sizeof(double),
+                                        cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hl.data(), dl, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  double ms = 0;
+  if (time_end(c, &ms)) return FP_ECUDA;
+  c->kms[FP_STAGE_VJP] = ms;
+  // residual r = b - A Gamma with b_i = -Uinf_i . n_i: d(lambda^T r)/dn_i =
+  // -lambda_i (U_i + Uinf_i), d/dUinf_i = -lambda_i n_i, d/dX_i from the kernel
+  const double* T = c->h_tgt.data();
+  for (int64_t i = 0; i < n; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      if (dcps) dcps[3 * i + d] = hX[d * n + i];
+      if (dnormals) dnormals[3 * i + d] = -hl[i] * (hU[d * n + i] + Uinfs[3 * i + d]);
+      if (dUinfs) dUinfs[3 * i + d] = -hl[i] * T[(3 + d) * n + i];
+    }
+  }
+  scatter_vjp(c, hv, hw, dnodes, dDas, dDbs);
+  return FP_OK;
+}
+
+int fp_uind_vjp(fp_ctx* c, const double* strengths, const double* targets, int64_t m, const double* wbar,
+                double* dtargets, double* dstrengths, double* dnodes, double* dDas, double* dDbs) {
+  if (check_ctx(c)) return FP_EINVAL;
+  FP_CUDA_TRY(c->err, cudaSetDevice(c->device));
+  if (c->assembled != FP_ELEMENT_VORTEXRING)
+    return c->err.set(FP_ESTATE, "fp_uind_vjp: assemble a vortex-ring body first");
+  if (!strengths || !targets || !wbar || m <= 0) return c->err.set(FP_EINVAL, "fp_uind_vjp: bad arguments");
+  const int64_t n = c->N;
+  VjpBufs b;
+  int rc;
+  if ((rc = vjp_buffers(c, m, b))) return rc;
+  // targets and cotangents arrive 3 x m (point-major); the kernels read SoA
+  std::vector<double> hx(3 * m), hwv(3 * m);
+  for (int64_t i = 0; i < m; ++i)
+    for (int d = 0; d < 3; ++d) {
+      hx[d * m + i] = targets[3 * i + d];
+      hwv[d * m + i] = wbar[3 * i + d];
+    }
+  if (time_begin(c)) return FP_ECUDA;
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(b.x, hx.data(), 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(b.w, hwv.data(), 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(b.gam, strengths, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(b.gX, 0, b.zero_count * sizeof(double), c->stream));
+  if ((rc = launch_pair_vjp(c, b.gam, b.x, b.w, m, b.gX, nullptr, b.gvert, b.gs, b.gwake))) return rc;
+  std::vector<double> hX(3 * m), hv(12 * n), hs(n), hw(kWakeGradHost * c->nsh);
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hX.data(), b.gX, 3 * m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hv.data(), b.gvert, 12 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(hs.data(), b.gs, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (c->nsh > 0)
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(hw.data(), b.gwake, kWakeGradHost * c->nsh * sizeof(double),
+                                        cudaMemcpyDeviceToHost, c->stream));
+  double ms = 0;
+  if (time_end(c, &ms)) return FP_ECUDA;
+  c->kms[FP_STAGE_VJP] = ms;
+  if (dtargets)
+    for (int64_t i = 0; i < m; ++i)
+      for (int d = 0; d < 3; ++d) dtargets[3 * i + d] = hX[d * m + i];
+  if (dstrengths) {
+    for (int64_t j = 0; j < n; ++j) dstrengths[j] = hs[j];
+    // wake strengths are Gamma_pi (upper) and Gamma_pj (lower)
+    for (int64_t e = 0; e < c->nsh; ++e) {
+      const int32_t* s = c->h_shed.data() + 6 * e;
+      dstrengths[s[0]] += hw[kWakeGradHost * e + 18];
+      if (s[3] >= 0) dstrengths[s[3]] += hw[kWakeGradHost * e + 19];
+    }
+  }
+  scatter_vjp(c, hv, hw, dnodes, dDas, dDbs);
+  return FP_OK;
 }
 
 int fp_kernel_launches(fp_ctx* c, int64_t* count) {
@@ -607,7 +851,7 @@ int fp_kernel_launches(fp_ctx* c, int64_t* count) {
 }
 
 int fp_last_kernel_ms(fp_ctx* c, int stage, double* ms, int* launches) {
-  if (check_ctx(c) || stage < 0 || stage > 3) return FP_EINVAL;
+  if (check_ctx(c) || stage < 0 || stage > FP_STAGE_VJP) return FP_EINVAL;
   if (ms) *ms = c->kms[stage];
   if (launches) *launches = c->klaunch[stage];
   return FP_OK;

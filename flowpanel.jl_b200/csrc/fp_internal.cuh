@@ -39,6 +39,7 @@ struct fp_ctx {
   std::vector<double> h_nodes;
   std::vector<int32_t> h_shed;
   std::vector<double> h_Da, h_Db;
+  std::vector<double> h_tgt;            // 6 x N SoA copy of d_tgt
 
   // device buffers
   fpb::PanelRec* d_panels = nullptr;    // N records
@@ -64,6 +65,18 @@ struct fp_ctx {
   int64_t cap_rhs = 0;                  // allocated RHS columns
   size_t cap_flags = 0;
 
+  // adjoint solves (kept apart from the primal RHS and solution)
+  double* d_ab = nullptr;               // N x k adjoint right-hand sides (ld)
+  double* d_ax = nullptr;               // N x k adjoint solutions
+  double* d_ar = nullptr;               // N x k adjoint residuals
+  float* d_aw32 = nullptr;              // N x k FP32 work
+  double* d_anorms = nullptr;           // column norms (2 x cap_adj)
+  int64_t cap_adj = 0;
+
+  // reverse-mode workspace (fp_assembly_vjp / fp_uind_vjp)
+  double* d_vjp = nullptr;
+  size_t cap_vjp = 0;                   // doubles
+
   // GMRES workspace
   double* d_V = nullptr;                // (m+1) x ld Krylov basis
   double* d_h = nullptr;                // small vectors
@@ -72,8 +85,10 @@ struct fp_ctx {
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double ms_assemble = 0, ms_factor = 0, ms_solve = 0, ms_uind = 0;
-  double kms[4] = {0, 0, 0, 0};
-  int klaunch[4] = {0, 0, 0, 0};
+  double kms[6] = {0, 0, 0, 0, 0, 0};
+  int klaunch[6] = {0, 0, 0, 0, 0, 0};
+  int adj_iters = 0;                    // refinement steps of the last adjoint solve
+  double adj_relres = 0;                // its relative residual
   fp_stats last{};
   int64_t nlaunch = 0;          // kernels launched by this context
   bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
@@ -96,6 +111,9 @@ int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv
              int64_t ldb, int64_t k, bool transpose);
 int gemv_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const double* x,
                   const double* b, double* r, int64_t k);
+// r = b - A^T x (FP64); x, b, r share the leading dimension lda
+int gemvT_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const double* x,
+                   const double* b, double* r, int64_t k);
 int convert_f64_f32(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda,
                     int64_t ldb);
 int axpy_f32_to_f64(fp_ctx* c, const float* d, double* x, int64_t n, int64_t k, int64_t ld);
@@ -113,6 +131,13 @@ int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_target
                      double* d_out, bool fp32);
 int launch_uind_source(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
                        double* d_out);
+
+// reverse mode of the pair kernels (fp_vjp.cu)
+int launch_pair_vjp(fp_ctx* c, const double* d_strength, const double* d_x, const double* d_w,
+                    int64_t m, double* d_gX, double* d_U, double* d_gvert, double* d_gs,
+                    double* d_gwake);
+int launch_vjp_cotangent(fp_ctx* c, const double* d_lambda, double* d_w);
+constexpr int kWakeGradHost = 20;   // per shedding edge: pa, pb, qa, qb, da, db, s_pi, s_pj
 
 // GMRES (fp_gmres.cu)
 int gmres_solve(fp_ctx* c, const double* b, double* x, int64_t k, const fp_solve_opts& o,

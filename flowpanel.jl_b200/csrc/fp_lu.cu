@@ -653,13 +653,16 @@ __global__ void k_apply_piv(T* __restrict__ B, int64_t ldb, int64_t n, int64_t k
 }
 
 // Persistent blocked triangular solve (one sweep), KR right-hand sides.
-// LOWER: L y = b (unit lower, forward); else U x = y (upper, backward).
+// LOWER (the forward sweep over blocks): L y = b (unit lower) or, with TRANS,
+// U^T z = b; otherwise the backward sweep: U x = y, or with TRANS L^T v = z.
+// TRANS reads the dependency tiles A(c, b) instead of A(b, c) and the
+// transposed inverse of the diagonal block.
 // The solution overwrites B. flags[b] = 1 once block b is final.
 // Every dependency tile of the factors is final before the solve starts, so a
 // CTA issues the loads of the next tile into shared memory before it waits for
 // the flag of the block whose solution it multiplies.
 constexpr int kTrsThreads = 256;
-template <class T, bool LOWER, int KR>
+template <class T, bool LOWER, int KR, bool TRANS = false>
 __global__ void __launch_bounds__(kTrsThreads)
 k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv,
       T* __restrict__ B, int64_t ldb, unsigned int* __restrict__ flags,
@@ -691,8 +694,13 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
 #pragma unroll
       for (int u = 0; u < PER; ++u) {
         const int e = tid + u * kTrsThreads;
-        const int rr = e % NB, ll = e / NB;
-        v[u] = (rr < nb && ll < cn) ? A[(c0 + ll) * lda + k0 + rr] : T(0);
+        if (TRANS) {   // tile[l][r] = A(c0 + l, k0 + r), l fastest over threads
+          const int ll = e % NB, rr = e / NB;
+          v[u] = (rr < nb && ll < cn) ? A[(k0 + rr) * lda + c0 + ll] : T(0);
+        } else {
+          const int rr = e % NB, ll = e / NB;
+          v[u] = (rr < nb && ll < cn) ? A[(c0 + ll) * lda + k0 + rr] : T(0);
+        }
       }
       if (tid == 0) {
         int spins = 0;
@@ -704,7 +712,8 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
 #pragma unroll
       for (int u = 0; u < PER; ++u) {
         const int e = tid + u * kTrsThreads;
-        tile[e / NB][e % NB] = v[u];
+        if (TRANS) tile[e % NB][e / NB] = v[u];
+        else tile[e / NB][e % NB] = v[u];
       }
       __syncthreads();
       if (stop_s) return;
@@ -720,11 +729,13 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
     }
     // x_b = inv(D_bb) acc
     {
-      const T* Di = Dinv + b * 2 * NB * NB + (LOWER ? 0 : NB * NB);
+      const T* Di = Dinv + b * 2 * NB * NB + ((LOWER != TRANS) ? 0 : NB * NB);
 #pragma unroll
       for (int u = 0; u < PER; ++u) {
         const int e = tid + u * kTrsThreads;
-        tile[e / NB][e % NB] = Di[e];    // Di column-major: e = l*NB + rr
+        // Di column-major: e = l*NB + rr; TRANS uses Di^T
+        if (TRANS) tile[e % NB][e / NB] = Di[e];
+        else tile[e / NB][e % NB] = Di[e];
       }
       __syncthreads();
       for (int q = qg; q < KR; q += QG) {
@@ -740,27 +751,27 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
   }
 }
 
-template <class T, bool LOWER, int KR>
+template <class T, bool LOWER, int KR, bool TRANS = false>
 static int run_trs(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv, T* B,
                    int64_t ldb) {
   const int64_t nblk = (n + NB - 1) / NB;
   FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
   const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
-  k_trs<T, LOWER, KR><<<grid, kTrsThreads, 0, c->stream>>>(A, lda, n, Dinv, B, ldb, c->d_flags,
-                                                           c->d_flags + nblk, c->d_status);
+  k_trs<T, LOWER, KR, TRANS><<<grid, kTrsThreads, 0, c->stream>>>(A, lda, n, Dinv, B, ldb, c->d_flags,
+                                                                  c->d_flags + nblk, c->d_status);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;
 }
 
-template <class T>
+template <class T, bool TRANS = false>
 static int solve_group(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const T* Dinv, T* B,
                        int64_t ldb, int kr) {
   int rc;
-#define FP_TRS_CASE(KR)                                                        \
-  case KR:                                                                     \
-    if ((rc = run_trs<T, true, KR>(c, LU, n, lda, Dinv, B, ldb))) return rc;   \
-    return run_trs<T, false, KR>(c, LU, n, lda, Dinv, B, ldb);
+#define FP_TRS_CASE(KR)                                                               \
+  case KR:                                                                            \
+    if ((rc = run_trs<T, true, KR, TRANS>(c, LU, n, lda, Dinv, B, ldb))) return rc;   \
+    return run_trs<T, false, KR, TRANS>(c, LU, n, lda, Dinv, B, ldb);
   switch (kr) {
     FP_TRS_CASE(1)
     FP_TRS_CASE(2)
@@ -772,12 +783,27 @@ static int solve_group(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const T* 
 }
 
 // Dinv buffer and flags are sized by the caller (fp_capi.cu) for n.
+// P A = L U. Plain: B <- P B, L y = B, U x = y. Transposed (A^T x = B):
+// U^T z = B, L^T v = z, x = P^T v (the swaps in reverse order).
 template <class T>
 int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv, T* B,
              int64_t ldb, int64_t k, bool transpose) {
-  if (transpose) return c->err.set(FP_EINVAL, "transposed solve not available");
   const int64_t nblk = (n + NB - 1) / NB;
   T* Dinv = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_dinv64 : (void*)c->d_dinv32);
+  if (transpose) {
+    for (int64_t q0 = 0; q0 < k;) {
+      const int64_t left = k - q0;
+      const int kr = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+      int rc = solve_group<T, true>(c, LU, n, lda, Dinv, B + q0 * ldb, ldb, kr);
+      if (rc) return rc;
+      q0 += kr;
+    }
+    const int64_t t = nblk * k;
+    k_apply_piv<T><<<(unsigned)((t + 127) / 128), 128, 0, c->stream>>>(B, ldb, n, k, ipiv, true);
+    ++c->nlaunch;
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+    return FP_OK;
+  }
   {
     const int64_t t = nblk * k;
     k_apply_piv<T><<<(unsigned)((t + 127) / 128), 128, 0, c->stream>>>(B, ldb, n, k, ipiv, false);
@@ -866,6 +892,71 @@ int gemv_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const doub
       k_gemv_finish<1><<<gf, 256, 0, c->stream>>>(c->d_part, n, b + q0 * lda, lda, r + q0 * lda, lda);
       ++c->nlaunch;
     }
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+    q0 += kr;
+  }
+  return FP_OK;
+}
+
+// ----------------------------------------------------------------------------
+// r = b - A^T x (FP64), k right-hand sides: one warp per column j of A (the
+// column is contiguous, read with 16-byte loads when aligned), x read through
+// L1; the dot product reduced by shuffles. HBM-bound: 8 N^2 bytes per pass.
+constexpr int kGemvTThreads = 256;
+template <int KR>
+__global__ void __launch_bounds__(kGemvTThreads)
+k_gemvT_residual(const double* __restrict__ A, int64_t lda, int64_t n, const double* __restrict__ x,
+                 const double* __restrict__ b, double* __restrict__ r, int64_t ldx, bool vec) {
+  const int lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * (kGemvTThreads / 32) + (threadIdx.x >> 5);
+  if (j >= n) return;
+  const double* col = A + j * lda;
+  double s[KR];
+#pragma unroll
+  for (int q = 0; q < KR; ++q) s[q] = 0.0;
+  int64_t i0 = 0;
+  if (vec) {
+    const int64_t n2 = n & ~int64_t(63);
+    for (int64_t i = 2 * lane; i < n2; i += 64) {
+      const double2 a = *reinterpret_cast<const double2*>(col + i);
+#pragma unroll
+      for (int q = 0; q < KR; ++q) {
+        const double2 xv = __ldg(reinterpret_cast<const double2*>(x + q * ldx + i));
+        s[q] += a.x * xv.x;
+        s[q] += a.y * xv.y;
+      }
+    }
+    i0 = n2;
+  }
+  for (int64_t i = i0 + lane; i < n; i += 32) {
+    const double a = col[i];
+#pragma unroll
+    for (int q = 0; q < KR; ++q) s[q] += a * __ldg(&x[q * ldx + i]);
+  }
+#pragma unroll
+  for (int q = 0; q < KR; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < KR; ++q) r[q * ldx + j] = b[q * ldx + j] - s[q];
+  }
+}
+
+int gemvT_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const double* x,
+                   const double* b, double* r, int64_t k) {
+  const bool vec = ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(x) |
+                     (uintptr_t)(lda * sizeof(double))) & 15) == 0;
+  const unsigned g = (unsigned)((n + kGemvTThreads / 32 - 1) / (kGemvTThreads / 32));
+  for (int64_t q0 = 0; q0 < k;) {
+    const int64_t left = k - q0;
+    const int kr = left >= 4 ? 4 : left >= 2 ? 2 : 1;
+    const int64_t o = q0 * lda;
+    if (kr == 4) k_gemvT_residual<4><<<g, kGemvTThreads, 0, c->stream>>>(A, lda, n, x + o, b + o, r + o, lda, vec);
+    else if (kr == 2) k_gemvT_residual<2><<<g, kGemvTThreads, 0, c->stream>>>(A, lda, n, x + o, b + o, r + o, lda, vec);
+    else k_gemvT_residual<1><<<g, kGemvTThreads, 0, c->stream>>>(A, lda, n, x + o, b + o, r + o, lda, vec);
+    ++c->nlaunch;
     FP_CUDA_TRY(c->err, cudaGetLastError());
     q0 += kr;
   }

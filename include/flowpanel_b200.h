@@ -160,8 +160,40 @@ int fp_uind(fp_ctx* ctx, int element, const double* strengths, const double* tar
 
 /* Adjoint of the linear solve: A^T lambda = ybar with the saved factors (the
  * reverse rule of IAD.implicit_linear at src/FLOWPanel_linearsolver.jl:73:
- * lambda = A^-T ybar, Abar = -lambda x^T, bbar = lambda). ybar/lambda N x k. */
+ * lambda = A^-T ybar, Abar = -lambda x^T, bbar = lambda). ybar/lambda N x k on
+ * the host. With FP64 factors one transposed LU solve; with the FP32 factors
+ * of FP_PREC_MIXED, iterative refinement against the FP64 AIC to a relative
+ * residual of 1e-12 (FP_ENOCONV if it stalls). The solution also stays on the
+ * device for fp_assembly_vjp. Device time: fp_last_kernel_ms(FP_STAGE_ADJOINT). */
 int fp_adjoint_solve(fp_ctx* ctx, const double* ybar, int64_t k, double* lambda);
+
+/* Reverse mode of the vortex-ring assembly (the pullback that ForwardDiff
+ * through _G_Uvortexring! and calc_bc_noflowthrough! gives the reference's
+ * ImplicitAD path, src/FLOWPanel_liftingbody.jl:455-572,
+ * src/FLOWPanel_linearsolver.jl:297-312): the gradient of
+ * lambda^T (b - A Gamma), b_i = -Uinf_i . n_i, with respect to the ring and
+ * wake-node coordinates (dnodes, 3 x nnodes), the control points (dcps, 3 x N),
+ * the normals (dnormals, 3 x N), the freestream at each control point
+ * (dUinfs, 3 x N) and the wake directions (dDas, dDbs, 3 x nsh). With
+ * lambda = A^-T dF/dGamma (fp_adjoint_solve) this is the total derivative of
+ * F through the solve. lambda / gamma may be NULL to use the device-resident
+ * results of the last fp_adjoint_solve / fp_solve (first column). Outputs are
+ * overwritten; any may be NULL. dnodes covers the vertices as ring and wake
+ * nodes only: control points and normals are inputs of their own, so their
+ * dependence on the nodes is the caller's chain rule. Device time:
+ * fp_last_kernel_ms(FP_STAGE_VJP). */
+int fp_assembly_vjp(fp_ctx* ctx, const double* lambda, const double* gamma, const double* Uinfs,
+                    double* dnodes, double* dcps, double* dnormals, double* dUinfs, double* dDas,
+                    double* dDbs);
+
+/* Reverse mode of Uind! for the vortex-ring body (src/FLOWPanel_liftingbody.jl:576-661):
+ * the gradient of sum_i wbar_i . Uind(targets_i) with respect to the targets
+ * (dtargets 3 x m), the strengths (dstrengths N, the wake's Gamma_pi / Gamma_pj
+ * included), the nodes (dnodes 3 x nnodes) and the wake directions (dDas,
+ * dDbs). targets and wbar are 3 x m. Outputs are overwritten; any may be NULL. */
+int fp_uind_vjp(fp_ctx* ctx, const double* strengths, const double* targets, int64_t m,
+                const double* wbar, double* dtargets, double* dstrengths, double* dnodes,
+                double* dDas, double* dDbs);
 
 /* Time of the last kernel launches, for the benchmark's roofline: the device
  * time (ms) of the named stage's dominant kernel and its launch count. */
@@ -170,6 +202,8 @@ int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
 #define FP_STAGE_FACTOR 1
 #define FP_STAGE_SOLVE 2
 #define FP_STAGE_UIND 3
+#define FP_STAGE_ADJOINT 4   /* fp_adjoint_solve */
+#define FP_STAGE_VJP 5       /* fp_assembly_vjp / fp_uind_vjp */
 
 /* Measurement utility (no counterpart in the reference): sustained FMA
  * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, in

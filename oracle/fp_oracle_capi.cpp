@@ -307,4 +307,109 @@ long long fpo_opcount(int which, int nn) {
   return -1;
 }
 
+// ------------------------------------------------------------------ forward-mode derivatives
+// Directional derivatives with Dual<1> (the stand-in for ForwardDiff through
+// the reference's CPU path), the oracle of the reverse-mode kernels.
+namespace {
+typedef Dual<1> D1;
+std::vector<D1> seed(const double* v, const double* dv, int64_t n) {
+  std::vector<D1> r(n);
+  for (int64_t i = 0; i < n; ++i) {
+    r[i] = D1(v[i]);
+    r[i].d[0] = dv ? dv[i] : 0.0;
+  }
+  return r;
+}
+// out[3t..] (or out[t] with normals) += velocity of the rings (strengths s)
+// and of the wake horseshoes (s_pi, s_pj) at targets t0..t0+nt-1, in the
+// reference's per-target order (src/FLOWPanel_liftingbody.jl:576-661).
+void body_velocity(const std::vector<D1>& N, const int* offsets, const int* pnodes,
+                   long long npanels, const std::vector<D1>& s, const int* shedding,
+                   long long nsh, const std::vector<D1>& Da, const std::vector<D1>& Db,
+                   const D1* T, long long nt, D1* out, const D1* normals, double cutoff,
+                   double offset) {
+  for (long long j = 0; j < npanels; ++j) {
+    const int* panel = pnodes + offsets[j];
+    const int nn = offsets[j + 1] - offsets[j];
+    U_vortexring<D1>(N.data(), panel, nn, s[j], T, nt, out, normals, cutoff, offset);
+  }
+  for (long long e = 0; e < nsh; ++e) {
+    const int* sh = shedding + 6 * e;
+    const int pi = sh[0], nia = sh[1], nib = sh[2], pj = sh[3], nja = sh[4], njb = sh[5];
+    const int* pan = pnodes + offsets[pi];
+    const D1* da = Da.data() + 3 * e;
+    const D1* db = Db.data() + 3 * e;
+    U_semiinfinite_horseshoe<D1>(N.data(), pan[nia], pan[nib], da[0], da[1], da[2], db[0], db[1],
+                                 db[2], s[pi], T, nt, out, normals, cutoff, offset);
+    if (pj != -1) {
+      const int* panj = pnodes + offsets[pj];
+      U_semiinfinite_horseshoe<D1>(N.data(), panj[nja], panj[njb], db[0], db[1], db[2], da[0],
+                                   da[1], da[2], s[pj], T, nt, out, normals, cutoff, offset);
+    }
+  }
+}
+}  // namespace
+
+// F = sum_i lambda_i (b_i - (A gamma)_i), b_i = -Uinf_i . n_i, A the vortex-ring
+// AIC with Kutta wake columns (src/FLOWPanel_liftingbody.jl:455-572,
+// src/FLOWPanel_linearsolver.jl:297-312); F and its derivative along the
+// given directions (any direction pointer may be NULL = 0).
+void fpo_residual_jvp(const double* nodes, const double* dnodes, long long nnodes,
+                      const int* offsets, const int* pnodes, long long npanels, const double* cps,
+                      const double* dcps, const double* normals, const double* dnormals,
+                      const int* shedding, long long nsh, const double* Das, const double* dDas,
+                      const double* Dbs, const double* dDbs, const double* Uinfs,
+                      const double* dUinfs, const double* lambda, const double* gamma,
+                      double offset, double cutoff, double* F, double* dF, int nthreads) {
+  const std::vector<D1> N = seed(nodes, dnodes, 3 * nnodes);
+  const std::vector<D1> X = seed(cps, dcps, 3 * npanels);
+  const std::vector<D1> Nr = seed(normals, dnormals, 3 * npanels);
+  const std::vector<D1> Da = seed(Das, dDas, 3 * nsh), Db = seed(Dbs, dDbs, 3 * nsh);
+  const std::vector<D1> U = seed(Uinfs, dUinfs, 3 * npanels);
+  const std::vector<D1> s = seed(gamma, nullptr, npanels);
+  std::vector<D1> AG(npanels, D1(0.0));
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const long long CH = 16;
+#pragma omp parallel for schedule(dynamic)
+  for (long long t0 = 0; t0 < npanels; t0 += CH) {
+    const long long nt = (npanels - t0 < CH) ? npanels - t0 : CH;
+    body_velocity(N, offsets, pnodes, npanels, s, shedding, nsh, Da, Db, X.data() + 3 * t0, nt,
+                  AG.data() + t0, Nr.data() + 3 * t0, cutoff, offset);
+  }
+  D1 acc(0.0);
+  for (long long i = 0; i < npanels; ++i) {
+    const D1 b = -(U[3 * i] * Nr[3 * i] + U[3 * i + 1] * Nr[3 * i + 1] + U[3 * i + 2] * Nr[3 * i + 2]);
+    acc += D1(lambda[i]) * (b - AG[i]);
+  }
+  *F = acc.v;
+  *dF = acc.d[0];
+}
+
+// F = sum_i wbar_i . Uind(targets_i) of the vortex-ring body with strengths;
+// F and its derivative along (dnodes, dtargets, dstrengths, dDas, dDbs).
+void fpo_uind_jvp(const double* nodes, const double* dnodes, long long nnodes, const int* offsets,
+                  const int* pnodes, long long npanels, const double* strengths,
+                  const double* dstrengths, const int* shedding, long long nsh, const double* Das,
+                  const double* dDas, const double* Dbs, const double* dDbs,
+                  const double* targets, const double* dtargets, long long m, const double* wbar,
+                  double offset, double cutoff, double* F, double* dF, int nthreads) {
+  const std::vector<D1> N = seed(nodes, dnodes, 3 * nnodes);
+  const std::vector<D1> X = seed(targets, dtargets, 3 * m);
+  const std::vector<D1> Da = seed(Das, dDas, 3 * nsh), Db = seed(Dbs, dDbs, 3 * nsh);
+  const std::vector<D1> s = seed(strengths, dstrengths, npanels);
+  std::vector<D1> Uo(3 * m, D1(0.0));
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const long long CH = 16;
+#pragma omp parallel for schedule(dynamic)
+  for (long long t0 = 0; t0 < m; t0 += CH) {
+    const long long nt = (m - t0 < CH) ? m - t0 : CH;
+    body_velocity(N, offsets, pnodes, npanels, s, shedding, nsh, Da, Db, X.data() + 3 * t0, nt,
+                  Uo.data() + 3 * t0, nullptr, cutoff, offset);
+  }
+  D1 acc(0.0);
+  for (long long i = 0; i < 3 * m; ++i) acc += D1(wbar[i]) * Uo[i];
+  *F = acc.v;
+  *dF = acc.d[0];
+}
+
 }  // extern "C"

@@ -257,6 +257,52 @@ def uind_source(mesh, strength, targets, offset=1e-8, nthreads=0):
     return out
 
 
+# ----------------------------------------------------------------- forward-mode derivatives
+def _opt(a, shape):
+    return None if a is None else _d(_f64(np.reshape(a, shape)))
+
+
+def residual_jvp(mesh, cps, normals, Das, Dbs, Uinfs, lam, gamma, dnodes=None, dcps=None,
+                 dnormals=None, dDas=None, dDbs=None, dUinfs=None, offset=1e-8, cutoff=1e-14,
+                 nthreads=0):
+    """F = lam . (b - A gamma) (vortex-ring AIC with Kutta wake columns,
+    b = -Uinf . n) and dF along the given directions, by Dual numbers (the
+    oracle of the reverse-mode assembly). Returns (F, dF)."""
+    n = mesh.npanels
+    sh = _i32(mesh.shedding.reshape(-1, 6)) if mesh.nsheddings else np.zeros((0, 6), np.int32)
+    nsh = len(sh)
+    F, dF = C.c_double(), C.c_double()
+    lib().fpo_residual_jvp(_d(_pts(mesh.nodes)), _opt(dnodes, (-1, 3)), C.c_longlong(mesh.nodes.shape[0]),
+                           _i(_i32(mesh.panel_offsets)), _i(_i32(mesh.panel_nodes)), C.c_longlong(n),
+                           _d(_pts(cps)), _opt(dcps, (n, 3)), _d(_pts(normals)), _opt(dnormals, (n, 3)),
+                           _i(sh), C.c_longlong(nsh), _d(_pts(np.reshape(Das, (-1, 3)))), _opt(dDas, (nsh, 3)),
+                           _d(_pts(np.reshape(Dbs, (-1, 3)))), _opt(dDbs, (nsh, 3)),
+                           _d(_pts(np.reshape(Uinfs, (n, 3)))), _opt(dUinfs, (n, 3)), _d(_f64(lam)),
+                           _d(_f64(gamma)), C.c_double(offset), C.c_double(cutoff), C.byref(F), C.byref(dF),
+                           nthreads)
+    return F.value, dF.value
+
+
+def uind_jvp(mesh, strengths, Das, Dbs, targets, wbar, dnodes=None, dtargets=None, dstrengths=None,
+             dDas=None, dDbs=None, offset=1e-8, cutoff=1e-14, nthreads=0):
+    """F = sum_i wbar_i . Uind(targets_i) and dF along the given directions
+    (Dual numbers). Returns (F, dF)."""
+    n = mesh.npanels
+    targets = _pts(targets)
+    m = targets.shape[0]
+    sh = _i32(mesh.shedding.reshape(-1, 6)) if mesh.nsheddings else np.zeros((0, 6), np.int32)
+    nsh = len(sh)
+    F, dF = C.c_double(), C.c_double()
+    lib().fpo_uind_jvp(_d(_pts(mesh.nodes)), _opt(dnodes, (-1, 3)), C.c_longlong(mesh.nodes.shape[0]),
+                       _i(_i32(mesh.panel_offsets)), _i(_i32(mesh.panel_nodes)), C.c_longlong(n),
+                       _d(_f64(strengths)), _opt(dstrengths, (n,)), _i(sh), C.c_longlong(nsh),
+                       _d(_pts(np.reshape(Das, (-1, 3)))), _opt(dDas, (nsh, 3)),
+                       _d(_pts(np.reshape(Dbs, (-1, 3)))), _opt(dDbs, (nsh, 3)), _d(targets),
+                       _opt(dtargets, (m, 3)), C.c_longlong(m), _d(_pts(np.reshape(wbar, (m, 3)))),
+                       C.c_double(offset), C.c_double(cutoff), C.byref(F), C.byref(dF), nthreads)
+    return F.value, dF.value
+
+
 # ----------------------------------------------------------------- linear solvers
 def lu_factor(G):
     """LAPACK dgetrf (partial pivoting), as Julia's LA.lu! (src/FLOWPanel_linearsolver.jl:173-185)."""
