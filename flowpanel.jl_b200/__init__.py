@@ -13,3 +13,11 @@ from .bodies import (B200Solver, MultiBody, NonLiftingBody, RigidWakeBody, Uind,
 __all__ = ["B200Solver", "MultiBody", "NonLiftingBody", "RigidWakeBody", "solve", "Uind", "calcfield_U",
            "calcfield_Cp", "calcfield_F", "calcfield_LDS", "calc_normals", "calc_controlpoints",
            "calc_areas", "meshes"]
+
+
+def __getattr__(name):
+    # the reverse-mode module imports torch; load it on first use
+    if name == "adjoint":
+        import importlib
+        return importlib.import_module(__name__ + ".adjoint")
+    raise AttributeError(name)

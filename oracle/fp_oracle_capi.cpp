@@ -353,14 +353,16 @@ void body_velocity(const std::vector<D1>& N, const int* offsets, const int* pnod
 // F = sum_i lambda_i (b_i - (A gamma)_i), b_i = -Uinf_i . n_i, A the vortex-ring
 // AIC with Kutta wake columns (src/FLOWPanel_liftingbody.jl:455-572,
 // src/FLOWPanel_linearsolver.jl:297-312); F and its derivative along the
-// given directions (any direction pointer may be NULL = 0).
+// given directions (any direction pointer may be NULL = 0); optionally the
+// residual vector r = b - A gamma and its derivative dr (lambda may be NULL).
 void fpo_residual_jvp(const double* nodes, const double* dnodes, long long nnodes,
                       const int* offsets, const int* pnodes, long long npanels, const double* cps,
                       const double* dcps, const double* normals, const double* dnormals,
                       const int* shedding, long long nsh, const double* Das, const double* dDas,
                       const double* Dbs, const double* dDbs, const double* Uinfs,
                       const double* dUinfs, const double* lambda, const double* gamma,
-                      double offset, double cutoff, double* F, double* dF, int nthreads) {
+                      double offset, double cutoff, double* F, double* dF, double* r,
+                      double* dr, int nthreads) {
   const std::vector<D1> N = seed(nodes, dnodes, 3 * nnodes);
   const std::vector<D1> X = seed(cps, dcps, 3 * npanels);
   const std::vector<D1> Nr = seed(normals, dnormals, 3 * npanels);
@@ -379,20 +381,25 @@ void fpo_residual_jvp(const double* nodes, const double* dnodes, long long nnode
   D1 acc(0.0);
   for (long long i = 0; i < npanels; ++i) {
     const D1 b = -(U[3 * i] * Nr[3 * i] + U[3 * i + 1] * Nr[3 * i + 1] + U[3 * i + 2] * Nr[3 * i + 2]);
-    acc += D1(lambda[i]) * (b - AG[i]);
+    const D1 ri = b - AG[i];
+    if (r) r[i] = ri.v;
+    if (dr) dr[i] = ri.d[0];
+    if (lambda) acc += D1(lambda[i]) * ri;
   }
   *F = acc.v;
   *dF = acc.d[0];
 }
 
 // F = sum_i wbar_i . Uind(targets_i) of the vortex-ring body with strengths;
-// F and its derivative along (dnodes, dtargets, dstrengths, dDas, dDbs).
+// F and its derivative along (dnodes, dtargets, dstrengths, dDas, dDbs);
+// optionally the velocities U (3 x m) and their derivatives dU (wbar may be NULL).
 void fpo_uind_jvp(const double* nodes, const double* dnodes, long long nnodes, const int* offsets,
                   const int* pnodes, long long npanels, const double* strengths,
                   const double* dstrengths, const int* shedding, long long nsh, const double* Das,
                   const double* dDas, const double* Dbs, const double* dDbs,
                   const double* targets, const double* dtargets, long long m, const double* wbar,
-                  double offset, double cutoff, double* F, double* dF, int nthreads) {
+                  double offset, double cutoff, double* F, double* dF, double* U, double* dU,
+                  int nthreads) {
   const std::vector<D1> N = seed(nodes, dnodes, 3 * nnodes);
   const std::vector<D1> X = seed(targets, dtargets, 3 * m);
   const std::vector<D1> Da = seed(Das, dDas, 3 * nsh), Db = seed(Dbs, dDbs, 3 * nsh);
@@ -407,7 +414,11 @@ void fpo_uind_jvp(const double* nodes, const double* dnodes, long long nnodes, c
                   Uo.data() + 3 * t0, nullptr, cutoff, offset);
   }
   D1 acc(0.0);
-  for (long long i = 0; i < 3 * m; ++i) acc += D1(wbar[i]) * Uo[i];
+  for (long long i = 0; i < 3 * m; ++i) {
+    if (U) U[i] = Uo[i].v;
+    if (dU) dU[i] = Uo[i].d[0];
+    if (wbar) acc += D1(wbar[i]) * Uo[i];
+  }
   *F = acc.v;
   *dF = acc.d[0];
 }

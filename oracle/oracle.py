@@ -264,11 +264,14 @@ def _opt(a, shape):
 
 def residual_jvp(mesh, cps, normals, Das, Dbs, Uinfs, lam, gamma, dnodes=None, dcps=None,
                  dnormals=None, dDas=None, dDbs=None, dUinfs=None, offset=1e-8, cutoff=1e-14,
-                 nthreads=0):
+                 nthreads=0, vector=False):
     """F = lam . (b - A gamma) (vortex-ring AIC with Kutta wake columns,
     b = -Uinf . n) and dF along the given directions, by Dual numbers (the
-    oracle of the reverse-mode assembly). Returns (F, dF)."""
+    oracle of the reverse-mode assembly). Returns (F, dF), or with
+    ``vector=True`` the residual r = b - A gamma and its derivative dr."""
     n = mesh.npanels
+    r = np.zeros(n) if vector else None
+    dr = np.zeros(n) if vector else None
     sh = _i32(mesh.shedding.reshape(-1, 6)) if mesh.nsheddings else np.zeros((0, 6), np.int32)
     nsh = len(sh)
     F, dF = C.c_double(), C.c_double()
@@ -277,19 +280,23 @@ def residual_jvp(mesh, cps, normals, Das, Dbs, Uinfs, lam, gamma, dnodes=None, d
                            _d(_pts(cps)), _opt(dcps, (n, 3)), _d(_pts(normals)), _opt(dnormals, (n, 3)),
                            _i(sh), C.c_longlong(nsh), _d(_pts(np.reshape(Das, (-1, 3)))), _opt(dDas, (nsh, 3)),
                            _d(_pts(np.reshape(Dbs, (-1, 3)))), _opt(dDbs, (nsh, 3)),
-                           _d(_pts(np.reshape(Uinfs, (n, 3)))), _opt(dUinfs, (n, 3)), _d(_f64(lam)),
-                           _d(_f64(gamma)), C.c_double(offset), C.c_double(cutoff), C.byref(F), C.byref(dF),
-                           nthreads)
-    return F.value, dF.value
+                           _d(_pts(np.reshape(Uinfs, (n, 3)))), _opt(dUinfs, (n, 3)),
+                           None if lam is None else _d(_f64(lam)), _d(_f64(gamma)), C.c_double(offset),
+                           C.c_double(cutoff), C.byref(F), C.byref(dF), None if r is None else _d(r),
+                           None if dr is None else _d(dr), nthreads)
+    return (r, dr) if vector else (F.value, dF.value)
 
 
 def uind_jvp(mesh, strengths, Das, Dbs, targets, wbar, dnodes=None, dtargets=None, dstrengths=None,
-             dDas=None, dDbs=None, offset=1e-8, cutoff=1e-14, nthreads=0):
+             dDas=None, dDbs=None, offset=1e-8, cutoff=1e-14, nthreads=0, vector=False):
     """F = sum_i wbar_i . Uind(targets_i) and dF along the given directions
-    (Dual numbers). Returns (F, dF)."""
+    (Dual numbers). Returns (F, dF), or with ``vector=True`` the velocities
+    U (m, 3) and their derivatives dU."""
     n = mesh.npanels
     targets = _pts(targets)
     m = targets.shape[0]
+    U = np.zeros((m, 3)) if vector else None
+    dU = np.zeros((m, 3)) if vector else None
     sh = _i32(mesh.shedding.reshape(-1, 6)) if mesh.nsheddings else np.zeros((0, 6), np.int32)
     nsh = len(sh)
     F, dF = C.c_double(), C.c_double()
@@ -298,9 +305,11 @@ def uind_jvp(mesh, strengths, Das, Dbs, targets, wbar, dnodes=None, dtargets=Non
                        _d(_f64(strengths)), _opt(dstrengths, (n,)), _i(sh), C.c_longlong(nsh),
                        _d(_pts(np.reshape(Das, (-1, 3)))), _opt(dDas, (nsh, 3)),
                        _d(_pts(np.reshape(Dbs, (-1, 3)))), _opt(dDbs, (nsh, 3)), _d(targets),
-                       _opt(dtargets, (m, 3)), C.c_longlong(m), _d(_pts(np.reshape(wbar, (m, 3)))),
-                       C.c_double(offset), C.c_double(cutoff), C.byref(F), C.byref(dF), nthreads)
-    return F.value, dF.value
+                       _opt(dtargets, (m, 3)), C.c_longlong(m),
+                       None if wbar is None else _d(_pts(np.reshape(wbar, (m, 3)))),
+                       C.c_double(offset), C.c_double(cutoff), C.byref(F), C.byref(dF),
+                       None if U is None else _d(U), None if dU is None else _d(dU), nthreads)
+    return (U, dU) if vector else (F.value, dF.value)
 
 
 # ----------------------------------------------------------------- linear solvers
