@@ -119,6 +119,33 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def measured_peak(key, fallback):
+    """A peak from MEASURED_PEAKS.json (driver-measured on this pool), else
+    the stated fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)[key]), f"of measured ({key}, MEASURED_PEAKS.json)"
+    except Exception:
+        return fallback, "of fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of `kernel`, from the committed ncu summary profiles/<kernel>*.txt (a line
+    'traffic_bytes_per_launch: <bytes>'), scaled there to this workload."""
+    d = os.path.join(ROOT, "profiles")
+    try:
+        for name in sorted(os.listdir(d)):
+            if name.startswith(kernel) and name.endswith(".txt"):
+                with open(os.path.join(d, name)) as fh:
+                    for line in fh:
+                        if line.startswith("traffic_bytes_per_launch:"):
+                            return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
@@ -189,7 +216,7 @@ def run_ours(args, rank, ws, dist):
     fp = ge.load_package()
     cap = fp._capi
     device = int(os.environ.get("LOCAL_RANK", "0"))
-    w, body, normals, cps, V, D, U = wing_problem(fp)
+    w, body, normals, cps, V, D, U = wing_problem(fp, args.n_chord, args.n_span)
     N = w.npanels
     ctx = cap.Context(device)
     ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
@@ -212,15 +239,19 @@ def run_ours(args, rank, ws, dist):
     launches0 = ctx.kernel_launches()
     res = {}
     precs = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
+    ktime = {}
     with ClockSampler(device) as clk:
         for prec in precs:
             barrier(dist)
+            ctx.kernel_timing(True)
             tot, stages = 0.0, np.zeros(3)
             for _ in range(args.steps):
                 ms, st = device_step(prec)
                 tot += ms
                 stages += [st.ms_assemble, st.ms_factor, st.ms_solve]
             res[prec] = (max_over_ranks(dist, tot / args.steps), stages / args.steps, st)
+            ktime[prec] = ctx.kernel_timing_read()
+            ctx.kernel_timing(False)
     launches = ctx.kernel_launches() - launches0
     if args.profile:
         if rank == 0:
@@ -231,6 +262,21 @@ def run_ours(args, rank, ws, dist):
         return
     ms_mixed, stg_m, st_m = res["mixed"]
     ms_fp64, stg_d, st_d = res["fp64"]
+
+    # adjoint of each form: A^T lambda = ybar on the saved factors + the
+    # reverse-mode assembly (gradient w.r.t. nodes, CPs, normals, Uinf, wake)
+    ybar = np.random.default_rng(7).standard_normal(N)
+    adj = {}
+    for prec in ("mixed", "fp64"):
+        device_step(prec)
+        a_ms = v_ms = 0.0
+        for i in range(args.warmup + args.steps):
+            ctx.adjoint_solve(ybar[None, :])
+            ctx.assembly_vjp(U, w.nodes.shape[0])
+            if i >= args.warmup:
+                a_ms += ctx.last_kernel_ms(cap.FP_STAGE_ADJOINT)[0]
+                v_ms += ctx.last_kernel_ms(cap.FP_STAGE_VJP)[0]
+        adj[prec] = (max_over_ranks(dist, a_ms / args.steps), max_over_ranks(dist, v_ms / args.steps))
 
     # e2e through the public C ABI with host buffers
     e2e = []
@@ -251,12 +297,19 @@ def run_ours(args, rank, ws, dist):
     CLm = lift_coefficient(fp, body, x_m, V, U, D, solver)
     CLd = lift_coefficient(fp, body, x_d, V, U, D, solver)
     rel_gamma = float(np.linalg.norm(x_m - x_d) / np.linalg.norm(x_d))
-    # roofline of the assembly kernel (FP64 pipe): ops pinned by the oracle's
-    # operation counter (248 per quad-ring interaction) per launch / device time
+    # roofline of the dominant kernel of the mixed solve, the tcgen05 3xTF32
+    # trailing update: algorithmic flops (2 m n k per launch) over its summed
+    # per-launch device time in the timed region
+    tc_launches, tc_ms, tc_flops = ktime["mixed"]
+    tc_tflops = tc_flops / (tc_ms * 1e-3) / 1e12 if tc_ms > 0 else 0.0
+    peak_tc, peak_src = measured_peak("bf16_tflops", 1590.0)
+    traffic = profile_traffic("k_tc_gemm_sub")
+    # FP64 pipe roofline of the assembly: ops pinned by the oracle's operation
+    # counter (248 per quad-ring interaction, 290 per horseshoe) / device time
     peak64 = cap.measure_fma_peak(device, True)
-    asm_ms, _ = ctx.last_kernel_ms(cap.FP_STAGE_ASSEMBLE)
     ops = 248.0 * N * N + 290.0 * 2 * w.nsheddings * N
     achieved = ops / (stg_d[0] * 1e-3) / 1e12
+    d_launches, d_ms, d_flops = ktime["fp64"]
     cpu = None
     if not args.no_cpu_baseline:
         O = ge.load_oracle()
@@ -280,13 +333,26 @@ def run_ours(args, rank, ws, dist):
                          "rel_gamma_mixed_vs_fp64": rel_gamma, "ir_iters": st_m.ir_iters,
                          "used_gmres": st_m.used_gmres, "rel_residual_mixed": st_m.rel_residual,
                          "gepp_certified_fp64": bool(st_d.gepp_certified), "max_abs_L": st_d.max_abs_L},
-            "adjoint_over_primal": None,
+            "adjoint_over_primal": (adj["mixed"][0] + adj["mixed"][1]) / ms_mixed,
+            "adjoint": {"mixed": {"adjoint_solve_ms": adj["mixed"][0], "assembly_vjp_ms": adj["mixed"][1],
+                                  "over_primal": (adj["mixed"][0] + adj["mixed"][1]) / ms_mixed},
+                        "fp64": {"adjoint_solve_ms": adj["fp64"][0], "assembly_vjp_ms": adj["fp64"][1],
+                                 "over_primal": (adj["fp64"][0] + adj["fp64"][1]) / ms_fp64}},
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 3 * 8 * N,
                     "d2h_bytes_per_step": 8 * N},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "fp64", "kernel": "k_asm_ring+k_asm_wake", "achieved": achieved,
-                         "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
-                         "peak_source": "measured FP64 FMA throughput (fp_measure_fma_peak)"},
+            "roofline": {"bound": "tensor", "kernel": "k_tc_gemm_sub (tcgen05 3xTF32 trailing update)",
+                         "achieved": tc_tflops, "peak": peak_tc, "unit": "TFLOP/s",
+                         "frac": tc_tflops / peak_tc, "traffic": traffic,
+                         "launches": tc_launches, "ms_total": tc_ms,
+                         "peak_source": peak_src + " (dense BF16; the TF32 pipe is half of it, and 3xTF32 "
+                                        "issues 3 tensor MMAs per algorithmic flop)"},
+            "assembly_roofline": {"bound": "fp64 pipe", "kernel": "k_asm_ring+k_asm_wake",
+                                  "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                                  "frac": achieved / peak64,
+                                  "peak_source": "measured FP64 FMA throughput (fp_measure_fma_peak)"},
+            "fp64_trailing_update": {"kernel": "k_gemm_sub<double> (SIMT FP64)", "launches": d_launches,
+                                     "ms_total": d_ms, "tflops": d_flops / (d_ms * 1e-3) / 1e12 if d_ms else 0},
             "clocks": clk.summary()}
     if cpu:
         line["cpu_baseline"] = cpu
@@ -306,6 +372,8 @@ def main():
                     help="with --profile: which form to time")
     ap.add_argument("--profile", action="store_true",
                     help="timed device steps only (for ncu launch lists): no e2e, accuracy or CPU legs")
+    ap.add_argument("--n-chord", type=int, default=N_CHORD, help="with --profile: smaller wings for ncu")
+    ap.add_argument("--n-span", type=int, default=N_SPAN)
     args = ap.parse_args()
     rank, ws, dist = dist_init()
     try:

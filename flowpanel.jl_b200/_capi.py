@@ -25,7 +25,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_set_wake", "fp_assemble", "fp_get_aic", "fp_set_rhs", "fp_factor", "fp_solve",
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
-           "fp_uind_vjp")
+           "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read")
 
 
 class SolveOpts(C.Structure):
@@ -82,6 +82,8 @@ def lib():
         L.fp_lu_solve_noalloc.argtypes = [vp, C.c_void_p, C.c_int64, C.c_int64]
         L.fp_assembly_vjp.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.fp_uind_vjp.argtypes = [vp, _dp, _dp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.fp_kernel_timing.argtypes = [vp, C.c_int]
+        L.fp_kernel_timing_read.argtypes = [vp, C.POINTER(C.c_int64), _dp, _dp]
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
         L.fp_measure_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
         L.fp_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -240,6 +242,15 @@ class Context:
         factors of the last ``factor(FP_PREC_FP64)``; the library allocates
         no device memory for it."""
         self._chk(self._L.fp_lu_solve_noalloc(self.h, C.c_void_p(dev_ptr), ldb, k))
+
+    def kernel_timing(self, enable=True):
+        """Per-launch event timing of the factorisation's trailing update."""
+        self._chk(self._L.fp_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_timing_read(self):
+        n, ms, fl = C.c_int64(), C.c_double(), C.c_double()
+        self._chk(self._L.fp_kernel_timing_read(self.h, C.byref(n), C.byref(ms), C.byref(fl)))
+        return n.value, ms.value, fl.value
 
     def kernel_launches(self):
         n = C.c_int64()

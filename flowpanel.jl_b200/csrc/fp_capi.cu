@@ -73,6 +73,17 @@ int ensure_rhs(fp_ctx* c, int64_t k) {
   return FP_OK;
 }
 
+// Device staging buffer of at least n doubles, kept across calls (no
+// allocation in the steady state of repeated solves / field evaluations).
+int ensure_stage(fp_ctx* c, size_t n) {
+  if (n <= c->cap_stage) return FP_OK;
+  dfree(c->d_stage);
+  c->cap_stage = 0;
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_stage, n * sizeof(double)));
+  c->cap_stage = n;
+  return FP_OK;
+}
+
 int time_begin(fp_ctx* c) {
   FP_CUDA_TRY(c->err, cudaEventRecord(c->ev0, c->stream));
   return FP_OK;
@@ -96,6 +107,8 @@ void free_matrices(fp_ctx* c) {
   c->cap_adj = 0;
   dfree(c->d_vjp);
   c->cap_vjp = 0;
+  dfree(c->d_stage);
+  c->cap_stage = 0;
   for (int i = 0; i < 4; ++i) dfree(c->d_tc[i]);
   c->tc_cap = 0;
   c->cap_rhs = 0; c->cap_gmres_m = 0;
@@ -140,6 +153,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   dfree(c->d_status); dfree(c->d_cert);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->ktimer.pool) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return FP_OK;
@@ -357,13 +371,10 @@ int fp_set_rhs(fp_ctx* c, const double* Uinfs, int64_t k) {
   if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_set_rhs: no geometry");
   if (!Uinfs || k <= 0) return c->err.set(FP_EINVAL, "fp_set_rhs: bad arguments");
   if (int rc = ensure_rhs(c, k)) return rc;
-  double* dU = nullptr;
-  const size_t bytes = 3 * (size_t)c->N * k * sizeof(double);
-  FP_CUDA_TRY(c->err, cudaMallocAsync(&dU, bytes, c->stream));
-  FP_CUDA_TRY(c->err, cudaMemcpyAsync(dU, Uinfs, bytes, cudaMemcpyHostToDevice, c->stream));
-  int rc = launch_rhs(c, dU, k);
-  cudaFreeAsync(dU, c->stream);
-  if (rc) return rc;
+  const size_t elems = 3 * (size_t)c->N * k;
+  if (int rc = ensure_stage(c, elems)) return rc;
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_stage, Uinfs, elems * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (int rc = launch_rhs(c, c->d_stage, k)) return rc;
   c->nrhs = k;
   return FP_OK;
 }
@@ -409,6 +420,7 @@ int fp_factor(fp_ctx* c, int precision) {
   }
   if (rc) return rc;
   if (time_end(c, &c->ms_factor)) return FP_ECUDA;
+  kt_collect(c);
   c->kms[FP_STAGE_FACTOR] = c->ms_factor;
   if ((rc = consume_status(c))) return rc;
   float cert = 0.f;
@@ -579,10 +591,10 @@ int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targe
   if (m == 0) return FP_OK;
   c->kern_offset = kerneloffset;
   c->kern_cutoff = kernelcutoff;
-  double *ds = nullptr, *dt = nullptr, *dout = nullptr;
-  FP_CUDA_TRY(c->err, cudaMallocAsync(&ds, c->N * sizeof(double), c->stream));
-  FP_CUDA_TRY(c->err, cudaMallocAsync(&dt, 3 * m * sizeof(double), c->stream));
-  FP_CUDA_TRY(c->err, cudaMallocAsync(&dout, 3 * m * sizeof(double), c->stream));
+  if (int rc = ensure_stage(c, (size_t)c->N + 6 * (size_t)m)) return rc;
+  double* ds = c->d_stage;
+  double* dt = ds + c->N;
+  double* dout = dt + 3 * m;
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(ds, strengths, c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(dt, targets, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(dout, out, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -594,9 +606,6 @@ int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targe
   c->kms[FP_STAGE_UIND] = c->ms_uind;
   c->klaunch[FP_STAGE_UIND] = 1;
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(out, dout, 3 * m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  cudaFreeAsync(ds, c->stream);
-  cudaFreeAsync(dt, c->stream);
-  cudaFreeAsync(dout, c->stream);
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   return FP_OK;
 }
@@ -841,6 +850,26 @@ int fp_uind_vjp(fp_ctx* c, const double* strengths, const double* targets, int64
     }
   }
   scatter_vjp(c, hv, hw, dnodes, dDas, dDbs);
+  return FP_OK;
+}
+
+int fp_kernel_timing(fp_ctx* c, int enable) {
+  if (check_ctx(c)) return FP_EINVAL;
+  KernelTimer& t = c->ktimer;
+  t.on = enable != 0;
+  t.used = 0;
+  t.work.clear();
+  t.launches = 0;
+  t.ms = 0;
+  t.flops = 0;
+  return FP_OK;
+}
+
+int fp_kernel_timing_read(fp_ctx* c, int64_t* launches, double* ms, double* flops) {
+  if (check_ctx(c)) return FP_EINVAL;
+  if (launches) *launches = c->ktimer.launches;
+  if (ms) *ms = c->ktimer.ms;
+  if (flops) *flops = c->ktimer.flops;
   return FP_OK;
 }
 

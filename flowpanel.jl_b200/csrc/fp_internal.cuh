@@ -16,6 +16,17 @@ struct WakeRec {
   int pi, pj;
 };
 
+// Opt-in per-launch timing of one kernel (CUDA events on the context's stream
+// around each launch), for the roofline of the factorisation's trailing update.
+struct KernelTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;   // pairs (start, stop), reused
+  size_t used = 0;                 // events recorded since the last collect
+  std::vector<double> work;        // algorithmic flops of each timed launch
+  int64_t launches = 0;
+  double ms = 0, flops = 0;
+};
+
 struct fp_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -73,6 +84,10 @@ struct fp_ctx {
   double* d_anorms = nullptr;           // column norms (2 x cap_adj)
   int64_t cap_adj = 0;
 
+  // persistent staging of per-call inputs (fp_set_rhs, fp_uind)
+  double* d_stage = nullptr;
+  size_t cap_stage = 0;                 // doubles
+
   // reverse-mode workspace (fp_assembly_vjp / fp_uind_vjp)
   double* d_vjp = nullptr;
   size_t cap_vjp = 0;                   // doubles
@@ -91,6 +106,7 @@ struct fp_ctx {
   double adj_relres = 0;                // its relative residual
   fp_stats last{};
   int64_t nlaunch = 0;          // kernels launched by this context
+  KernelTimer ktimer;           // trailing-update launches of fp_factor
   bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
   float* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};   // Ah, Al, Bh, Bl scratch
   size_t tc_cap = 0;
@@ -144,4 +160,38 @@ int gmres_solve(fp_ctx* c, const double* b, double* x, int64_t k, const fp_solve
                 bool precondition, int* iters, double* relres);
 
 int num_sms();
+
+// KernelTimer: kt_begin records the start event of a launch (returns its
+// slot, or -1 when timing is off or an event cannot be made), kt_end the stop
+// event and the launch's algorithmic flops; kt_collect sums the elapsed times
+// after the stream has been synchronised.
+inline int kt_begin(fp_ctx* c) {
+  KernelTimer& t = c->ktimer;
+  if (!t.on) return -1;
+  while (t.pool.size() < t.used + 2) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    t.pool.push_back(e);
+  }
+  const int slot = (int)t.used;
+  cudaEventRecord(t.pool[slot], c->stream);
+  t.used += 2;
+  return slot;
+}
+inline void kt_end(fp_ctx* c, int slot, double flops) {
+  if (slot < 0) return;
+  cudaEventRecord(c->ktimer.pool[slot + 1], c->stream);
+  c->ktimer.work.push_back(flops);
+}
+inline void kt_collect(fp_ctx* c) {
+  KernelTimer& t = c->ktimer;
+  for (size_t s = 0; s + 1 < t.used; s += 2) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, t.pool[s], t.pool[s + 1]) == cudaSuccess) t.ms += ms;
+    t.flops += t.work[s / 2];
+    ++t.launches;
+  }
+  t.used = 0;
+  t.work.clear();
+}
 }  // namespace fpb

@@ -338,8 +338,10 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
       !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN))
     return false;
   dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
+  const int slot = kt_begin(c);
   tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, C, lda, (int)m,
                                                                        (int)nn, kk, c->d_status);
+  kt_end(c, slot, 2.0 * (double)m * (double)nn * (double)kk);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;
 }

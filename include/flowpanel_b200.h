@@ -195,6 +195,16 @@ int fp_uind_vjp(fp_ctx* ctx, const double* strengths, const double* targets, int
                 const double* wbar, double* dtargets, double* dstrengths, double* dnodes,
                 double* dDas, double* dDbs);
 
+/* Per-launch timing of the factorisation's trailing-update kernel (the
+ * tcgen05 3xTF32 kernel for FP32 factors, the SIMT FP64 kernel for FP64
+ * factors), for a roofline; no counterpart in the reference. enable != 0
+ * turns it on and clears the sums; every later fp_factor records CUDA events
+ * on the context's stream around each such launch and adds, after the factor
+ * completes, the number of launches, their device time (ms) and their
+ * algorithmic flops (2 m n k each). */
+int fp_kernel_timing(fp_ctx* ctx, int enable);
+int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* flops);
+
 /* Time of the last kernel launches, for the benchmark's roofline: the device
  * time (ms) of the named stage's dominant kernel and its launch count. */
 int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
