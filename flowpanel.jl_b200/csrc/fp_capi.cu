@@ -109,8 +109,10 @@ void free_matrices(fp_ctx* c) {
   c->cap_vjp = 0;
   dfree(c->d_stage);
   c->cap_stage = 0;
-  for (int i = 0; i < 4; ++i) dfree(c->d_tc[i]);
-  c->tc_cap = 0;
+  for (int s = 0; s < 2; ++s) {
+    for (int i = 0; i < 4; ++i) dfree(c->d_tc[s][i]);
+    c->tc_cap[s] = 0;
+  }
   c->cap_rhs = 0; c->cap_gmres_m = 0;
   c->assembled = -1; c->factored = -1; c->nrhs = 0;
 }
@@ -133,7 +135,15 @@ int fp_ctx_create(int device, fp_ctx** out) {
   if (device < 0 || device >= n) return FP_EINVAL;
   fp_ctx* c = new fp_ctx();
   c->device = device;
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  // the context's stream carries the factorisation's critical path (panels):
+  // give it the highest priority; stream2 (the bulk trailing update) the lowest
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_panel, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_rest, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_cert, sizeof(float)) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
@@ -148,12 +158,16 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (!c) return FP_EINVAL;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream2) cudaStreamSynchronize(c->stream2);
   free_matrices(c);
   dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt); dfree(c->d_wake);
   dfree(c->d_status); dfree(c->d_cert);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->ktimer.pool) cudaEventDestroy(e);
+  if (c->ev_panel) cudaEventDestroy(c->ev_panel);
+  if (c->ev_rest) cudaEventDestroy(c->ev_rest);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return FP_OK;

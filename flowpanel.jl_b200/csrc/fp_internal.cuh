@@ -108,8 +108,14 @@ struct fp_ctx {
   int64_t nlaunch = 0;          // kernels launched by this context
   KernelTimer ktimer;           // trailing-update launches of fp_factor
   bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
-  float* d_tc[4] = {nullptr, nullptr, nullptr, nullptr};   // Ah, Al, Bh, Bl scratch
-  size_t tc_cap = 0;
+  // split operands (Ah, Al, Bh, Bl) of the tensor-core update, one set per
+  // stream of the look-ahead factorisation (slot 0: c->stream, 1: stream2)
+  float* d_tc[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
+  size_t tc_cap[2] = {0, 0};
+  int tc_slot = 0;                      // scratch set of the current launches
+  cudaStream_t stream2 = nullptr;       // second stream of the look-ahead factorisation
+  cudaEvent_t ev_panel = nullptr;       // panel factored (stream -> stream2)
+  cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)
 };
 
 namespace fpb {
@@ -140,6 +146,8 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda);
 int lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k);
 int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out);
 constexpr int kLuNB = 64;        // block size of the factorisation and the solves
+// split-operand scratch of the tensor-core update for scratch set `slot` (fp_tc.cu)
+int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max);
 constexpr int kGemvSplitHost = 16;
 
 // induced velocity (fp_field.cu)

@@ -201,11 +201,11 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
 //    (x_j *= 1/U_jj, then x_l -= x_j U_jl for l > j) with the rows of U11
 //    read as 16-byte vectors from shared memory; the largest |L21| is the
 //    GEPP certificate;
-//  * k_u12: for columns outside the block, the row swaps of the block, and for
-//    columns right of it U12 = L11^-1 P A12 by forward substitution (columns
-//    of the unit lower L11 read as 16-byte vectors), one column per thread;
-//    columns are staged through shared memory so that global accesses are
-//    coalesced.
+//  * k_u12: on the columns [cl0, cl1) left of the block and [cr0, cr1)
+//    right of it, the row swaps of the block (mode bit 1) and, on the right
+//    columns, U12 = L11^-1 A12 by forward substitution (mode bit 2; columns
+//    of the unit lower L11 read as 16-byte vectors); one column per thread,
+//    columns staged through shared memory so that global accesses coalesce.
 constexpr int kApplyThreads = 64;
 template <class T> constexpr size_t u12_smem() {
   return (size_t)NB * rpitch<T>() * sizeof(T) + (size_t)kApplyThreads * (NB + 1) * sizeof(T) +
@@ -278,7 +278,8 @@ k_l21(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ 
 
 template <class T>
 __global__ void __launch_bounds__(kApplyThreads)
-k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv) {
+k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv, int64_t cl0,
+      int64_t cl1, int64_t cr0, int64_t cr1, int mode) {
   typedef typename V16<T>::type VT;
   constexpr int V = V16<T>::n, RP = rpitch<T>();
   extern __shared__ __align__(16) unsigned char dsm[];
@@ -298,12 +299,15 @@ k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __res
   __syncthreads();
   if (tid == 0) {
     for (int j = 0; j < NB; ++j) perm[j] = j;
-    for (int j = 0; j < nb; ++j) {
-      const int p = lp[j];
-      const int t0 = perm[j]; perm[j] = perm[p]; perm[p] = t0;
+    if (mode & 1) {
+      for (int j = 0; j < nb; ++j) {
+        const int p = lp[j];
+        const int t0 = perm[j]; perm[j] = perm[p]; perm[p] = t0;
+      }
     }
   }
-  const int64_t nother = n - nb;
+  const int64_t nl = cl1 - cl0;
+  const int64_t nother = nl + (cr1 - cr0);
   const int64_t g = blockIdx.x;   // one group of kApplyThreads columns per CTA
   static_assert(kApplyThreads == NB, "the column tile is NB x NB");
   stage_block<kApplyThreads, T>(
@@ -312,7 +316,7 @@ k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __res
         const int64_t qq = g * kApplyThreads + cc;
         T v = T(0);
         if (qq < nother && r < nb) {
-          const int64_t c = (qq < k) ? qq : qq + nb;
+          const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
           v = A[c * lda + k + r];
         }
         return v;
@@ -322,11 +326,11 @@ k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __res
   {
     const int64_t qq = g * kApplyThreads + tid;
     if (qq < nother) {
-      const int64_t c = (qq < k) ? qq : qq + nb;
+      const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
       T x[NB];
 #pragma unroll
       for (int r = 0; r < NB; ++r) x[r] = tile[tid][perm[r]];
-      if (c >= k + nb) {
+      if ((mode & 2) && c >= k + nb) {
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
           const T xj = x[j];
@@ -351,7 +355,7 @@ k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __res
     const int r = e & (NB - 1), cc = e >> 6;
     const int64_t qq = g * kApplyThreads + cc;
     if (qq < nother && r < nb) {
-      const int64_t c = (qq < k) ? qq : qq + nb;
+      const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
       A[c * lda + k + r] = tile[cc][r];
     }
   }
@@ -534,20 +538,65 @@ int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64
   return FP_OK;
 }
 
-// Two-level blocked right-looking LU. Outer panels of kOuterNB columns; inside
-// a panel, NB-wide blocks are factored (local pivoting), their U12 rows formed
-// for every column to the right, and the update is applied only to the panel
-// columns (full height) and to the panel rows (to the right), so that the
-// trailing matrix is updated once per outer panel with K = kOuterNB.
+// Two-level blocked right-looking LU with look-ahead. Outer panels of
+// kOuterNB columns; inside a panel, NB-wide blocks are factored (pivots local
+// to the diagonal block), their L21 formed, and the update applied to the
+// panel's own columns only. Two streams share the work of each panel P:
+//  * c->stream (high priority, the critical path): factor P; then, once the
+//    previous panel's trailing update is done, the row swaps and U12 of P's
+//    rows in the next panel's columns and the update of those columns
+//    (K = kOuterNB), so that the next panel can start;
+//  * c->stream2 (after P is factored): the row swaps of P in the columns left
+//    of P, its U12 rows in the columns beyond the next panel, and the
+//    trailing update of those columns, which overlaps the next panel.
+// Row swaps stay inside 64-row blocks, so the swaps of different blocks
+// commute, and a row update (C_r -= L_r U) commutes with a swap of the rows
+// of both C and L. Step (1) leaves P's L rows swapped by all of P's blocks,
+// so a strip of columns outside P first receives all of P's swaps and only
+// then the per-block substitutions and updates. Columns are split between the
+// streams so that no element is written by both at once.
 constexpr int kOuterNB = 256;
+
+// Routes the launches of a section to stream2 and its tensor-core scratch.
+struct OnStream2 {
+  fp_ctx* c;
+  cudaStream_t s0;
+  int slot0;
+  explicit OnStream2(fp_ctx* c_) : c(c_), s0(c_->stream), slot0(c_->tc_slot) {
+    c->stream = c->stream2;
+    c->tc_slot = 1;
+  }
+  ~OnStream2() {
+    c->stream = s0;
+    c->tc_slot = slot0;
+  }
+};
 
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
   FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_u12<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem<T>()));
+  if (sizeof(T) == 4 && c->use_tc) {   // both scratch sets before any concurrent launch
+    if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
+    if (int rc = ensure_tc_scratch(c, 1, n)) return rc;
+  }
   auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
+  auto u12 = [&](int64_t k, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1, int mode) -> int {
+    const int64_t cols = (cl1 - cl0) + (cr1 - cr0);
+    if (cols <= 0) return FP_OK;
+    const unsigned g = (unsigned)((cols + kApplyThreads - 1) / kApplyThreads);
+    k_u12<T><<<g, kApplyThreads, u12_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, cl0, cl1, cr0, cr1, mode);
+    ++c->nlaunch;
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+    return FP_OK;
+  };
+  // stream2 starts after everything already queued on c->stream
+  FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream2, c->ev_rest, 0));
   for (int64_t K0 = 0; K0 < n; K0 += kOuterNB) {
     const int64_t kend = std::min<int64_t>(K0 + kOuterNB, n);
+    const int64_t knext = std::min<int64_t>(kend + kOuterNB, n);   // next panel: columns [kend, knext)
+    // (1) factor the panel's columns, full height
     for (int64_t k = K0; k < kend; k += NB) {
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
@@ -560,23 +609,50 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
-      if (n - nb > 0) {
-        const unsigned g = (unsigned)((n - nb + kApplyThreads - 1) / kApplyThreads);
-        k_u12<T><<<g, kApplyThreads, u12_smem<T>(), c->stream>>>(A, lda, n, k, ipiv);
-        ++c->nlaunch;
-        FP_CUDA_TRY(c->err, cudaGetLastError());
-      }
       const int64_t k1 = k + nb;
-      // (a) remaining panel columns, full height
-      if (int rc = gemm_sub<T>(c, at(k1, k), at(k, k1), at(k1, k1), lda, n - k1, kend - k1, nb)) return rc;
-      // (b) remaining panel rows, columns right of the panel
-      if (int rc = gemm_sub<T>(c, at(k1, k), at(k, kend), at(k1, kend), lda, kend - k1, n - kend, nb)) return rc;
+      if (int rc = u12(k, K0, k, k1, kend, 3)) return rc;
+      if (kend > k1)
+        if (int rc = gemm_sub<T>(c, at(k1, k), at(k, k1), at(k1, k1), lda, n - k1, kend - k1, nb)) return rc;
     }
-    // outer trailing update with K = kend - K0
-    if (int rc = gemm_sub<T>(c, at(kend, K0), at(K0, kend), at(kend, kend), lda, n - kend, n - kend,
-                             (int)(kend - K0)))
-      return rc;
+    FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_panel, c->stream));
+    // (2) the next panel's columns: P's swaps and U12 rows, then their update
+    if (knext > kend) {
+      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
+      for (int64_t k = K0; k < kend; k += NB)
+        if (int rc = u12(k, 0, 0, kend, knext, 1)) return rc;
+      for (int64_t k = K0; k < kend; k += NB) {
+        const int64_t k1 = std::min<int64_t>(k + NB, n);
+        if (int rc = u12(k, 0, 0, kend, knext, 2)) return rc;
+        if (kend > k1)
+          if (int rc = gemm_sub<T>(c, at(k1, k), at(k, kend), at(k1, kend), lda, kend - k1, knext - kend, NB))
+            return rc;
+      }
+      if (int rc = gemm_sub<T>(c, at(kend, K0), at(K0, kend), at(kend, kend), lda, n - kend, knext - kend,
+                               (int)(kend - K0)))
+        return rc;
+    }
+    // (3) on stream2: swaps left of P, U12 rows beyond the next panel, their update
+    {
+      OnStream2 on2(c);
+      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
+      for (int64_t k = K0; k < kend; k += NB)
+        if (int rc = u12(k, 0, K0, knext, n, 1)) return rc;
+      for (int64_t k = K0; k < kend; k += NB) {
+        const int64_t k1 = std::min<int64_t>(k + NB, n);
+        if (int rc = u12(k, 0, 0, knext, n, 2)) return rc;
+        if (kend > k1 && n > knext)
+          if (int rc = gemm_sub<T>(c, at(k1, k), at(k, knext), at(k1, knext), lda, kend - k1, n - knext, NB))
+            return rc;
+      }
+      if (n > knext)
+        if (int rc = gemm_sub<T>(c, at(kend, K0), at(K0, knext), at(kend, knext), lda, n - kend, n - knext,
+                                 (int)(kend - K0)))
+          return rc;
+      FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
+    }
   }
+  // join: c->stream continues after the last work on stream2
+  FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
   return FP_OK;
 }
 

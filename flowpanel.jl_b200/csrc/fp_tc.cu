@@ -299,15 +299,16 @@ static bool make_map(CUtensorMap* tm, const float* base, int kext, int64_t rows,
 }  // namespace tc
 
 // Scratch for the split operands: 4 x N x 256 floats.
-static int ensure_tc_scratch(fp_ctx* c, int64_t rows_max) {
+int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max) {
   const size_t need = (size_t)rows_max * 256;
-  if (c->tc_cap >= need) return FP_OK;
+  if (c->tc_cap[slot] >= need) return FP_OK;
   for (int i = 0; i < 4; ++i) {
-    if (c->d_tc[i]) cudaFree(c->d_tc[i]);
-    c->d_tc[i] = nullptr;
+    if (c->d_tc[slot][i]) cudaFree(c->d_tc[slot][i]);
+    c->d_tc[slot][i] = nullptr;
   }
-  for (int i = 0; i < 4; ++i) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tc[i], need * sizeof(float)));
-  c->tc_cap = need;
+  c->tc_cap[slot] = 0;
+  for (int i = 0; i < 4; ++i) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tc[slot][i], need * sizeof(float)));
+  c->tc_cap[slot] = need;
   return FP_OK;
 }
 
@@ -322,9 +323,10 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
       return false;
     attr_set = true;
   }
-  if (ensure_tc_scratch(c, std::max<int64_t>(m, nn)) != FP_OK) return false;
+  const int slot = c->tc_slot;
+  if (ensure_tc_scratch(c, slot, std::max<int64_t>(m, nn)) != FP_OK) return false;
   const int ldk = (int)round_up(kk, 32);
-  float *Ah = c->d_tc[0], *Al = c->d_tc[1], *Bh = c->d_tc[2], *Bl = c->d_tc[3];
+  float *Ah = c->d_tc[slot][0], *Al = c->d_tc[slot][1], *Bh = c->d_tc[slot][2], *Bl = c->d_tc[slot][3];
   {
     dim3 g((unsigned)((m + 31) / 32), (unsigned)((ldk + 31) / 32));
     tc::k_split_A<<<g, dim3(32, 8), 0, c->stream>>>(A, lda, (int)m, kk, ldk, Ah, Al);
@@ -338,10 +340,10 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
       !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN))
     return false;
   dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
-  const int slot = kt_begin(c);
+  const int ev = kt_begin(c);
   tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, C, lda, (int)m,
                                                                        (int)nn, kk, c->d_status);
-  kt_end(c, slot, 2.0 * (double)m * (double)nn * (double)kk);
+  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;
 }
