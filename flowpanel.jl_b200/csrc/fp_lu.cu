@@ -85,114 +85,120 @@ __device__ __forceinline__ void stage_block(int tid, Get get, Put put) {
 template <class T> __host__ __device__ constexpr int rpitch() { return NB + 16 / (int)sizeof(T); }
 
 // ----------------------------------------------------------------------------
-// (1) k_diag: one CTA of 8 warps factors the NB x NB diagonal block with
-// partial pivoting over its rows, in shared memory (row-major), with one block
-// barrier per pivot step. Rows never move: a pivot row is marked used and
-// every other unused row eliminates column j with its own multiplier. Each
-// warp finds the pivot itself (lane l reads rows l and l+32 of column j; a
-// shuffle reduction carries value, sign and logical position; used flags and
-// logical positions are kept in registers, identically in every warp).
-// Warp w updates rows 8w..8w+7, four lanes per row, 16-byte column chunks
-// interleaved over the lanes; the chunk holding column j also receives the
-// multiplier. Column j is read from a double-buffered copy (colv), which
-// step j - 1 filled with the updated values: the owner of a row writes the
-// multiplier into S at step j while other warps may still be searching
-// column j. LAPACK's ipiv follows from the logical order (at step j, logical
-// rows j and the pivot's position swap).
-constexpr int kDiagThreads = 256;
+// (1) k_diag: two warps factor the NB x NB diagonal block with partial
+// pivoting over its rows. Thread t owns row t of the block and keeps it in
+// registers for the whole factorisation (the 64-step loop is unrolled, so
+// every column index is static). Rows never move: a pivot row is marked used
+// and every other unused row eliminates column j with its own multiplier.
+// The pivot is LAPACK's: the largest |a| in column j among the unused rows,
+// the first in the current logical order on ties. Each warp reduces an
+// integer key (the bits of |a| plus one, 0 for used rows; FP64 in two 32-bit
+// halves) with __reduce_max_sync, ties by logical position with
+// __reduce_min_sync; the two warps' candidates meet in shared memory. The
+// winning thread then writes its row once (16-byte stores) and every other
+// row reads it back with broadcast 16-byte loads into its FMAs.
+// LAPACK's ipiv follows from the logical order: at step j, logical rows j and
+// the pivot's position swap.
+constexpr int kDiagThreads = NB;
+
+__device__ __forceinline__ void bar_diag() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+
+template <class T> struct PivKey;
+template <> struct PivKey<float> {
+  __device__ static void of(float v, bool used, unsigned& hi, unsigned& lo) {
+    hi = used ? 0u : __float_as_uint(fabsf(v)) + 1u;
+    lo = 0u;
+  }
+};
+template <> struct PivKey<double> {
+  __device__ static void of(double v, bool used, unsigned& hi, unsigned& lo) {
+    const unsigned long long b = used ? 0ull : (unsigned long long)__double_as_longlong(fabs(v)) + 1ull;
+    hi = (unsigned)(b >> 32);
+    lo = (unsigned)b;
+  }
+};
 
 template <class T>
 __global__ void __launch_bounds__(kDiagThreads)
 k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
        int* __restrict__ status) {
   typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, RP = rpitch<T>(), NCH = NB / V;
-  __shared__ __align__(16) T S[NB][RP];   // S[pr][c]
-  __shared__ int order[NB];
+  constexpr int V = V16<T>::n, NCH = NB / V;
+  __shared__ __align__(16) T prow[NB];     // the pivot row of the current step
+  __shared__ unsigned cand[2][4];          // per warp: key hi, key lo, logical pos, thread
   __shared__ int lpiv[NB];
-  __shared__ T colv[2][NB];              // column j of S, for step j
   const int nb = (int)imin64(NB, n - k);
-  const int tid = threadIdx.x, l = tid & 31, warp = tid >> 5;
-  stage_block<kDiagThreads, T>(
-      tid,
-      [&](int rr, int cc) {
-        return (rr < nb && cc < nb) ? A[(k + cc) * lda + (k + rr)] : ((rr == cc) ? T(1) : T(0));
-      },
-      [&](int rr, int cc, T v) {
-        S[rr][cc] = v;
-        if (cc == 0) colv[0][rr] = v;
-      });
-  const int a0 = l, a1 = l + 32;
-  bool used0 = !(a0 < nb), used1 = !(a1 < nb);
-  int pos0 = a0, pos1 = a1;
-  const int ur = 8 * warp + (l & 7), cp = l >> 3;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  T R[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c)
+    R[c] = (t < nb && c < nb) ? A[(k + c) * lda + (k + t)] : ((t == c) ? T(1) : T(0));
+  bool used = !(t < nb);
+  int pos = t;
   bool zero = false;
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    const T v0 = colv[j & 1][a0], v1 = colv[j & 1][a1];
-    const T vu = colv[j & 1][ur];
-    T best = T(-1), sv = T(0);
-    int bi = 0, bpos = 1 << 30;
-    if (!used0) { best = tabs(v0); sv = v0; bi = a0; bpos = pos0; }
-    if (!used1) {
-      const T b1 = tabs(v1);
-      if (b1 > best || (b1 == best && pos1 < bpos)) { best = b1; sv = v1; bi = a1; bpos = pos1; }
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const T os = __shfl_xor_sync(0xffffffffu, sv, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
-      if (ob > best || (ob == best && op < bpos)) { best = ob; sv = os; bi = oi; bpos = op; }
-    }
-    const int p = bi, lp = bpos;
-    const unsigned m0 = __ballot_sync(0xffffffffu, pos0 == j);
-    const unsigned m1 = __ballot_sync(0xffffffffu, pos1 == j);
-    const int rj = m0 ? (__ffs(m0) - 1) : (32 + __ffs(m1) - 1);
-    const bool uu0 = __shfl_sync(0xffffffffu, used0, ur & 31);
-    const bool uu1 = __shfl_sync(0xffffffffu, used1, ur & 31);
-    const bool urow_used = (ur >> 5) ? uu1 : uu0;
-    if (a0 == p) { pos0 = j; used0 = true; } else if (a0 == rj) { pos0 = lp; }
-    if (a1 == p) { pos1 = j; used1 = true; } else if (a1 == rj) { pos1 = lp; }
-    if (tid == 0) lpiv[j] = lp;
-    const T rp = (sv != T(0)) ? T(1) / sv : T(0);
-    if (rp == T(0)) {
-      zero = true;
-    } else if (ur < nb && ur != p && !urow_used) {
-      const T m = vu * rp;
-      const VT* prow = reinterpret_cast<const VT*>(&S[p][0]);
-      VT* orow = reinterpret_cast<VT*>(&S[ur][0]);
-      const int q0 = j / V;                      // chunk holding column j
+  for (int j = 0; j < NB; ++j) {
+    if (j < nb) {
+      unsigned hi, lo;
+      PivKey<T>::of(R[j], used, hi, lo);
+      const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+      const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+      const bool top = hi == mh && lo == ml;
+      const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
+      if (lane == 0) {
+        cand[warp][0] = mh;
+        cand[warp][1] = ml;
+        cand[warp][2] = pm;
+      }
+      if (top && (unsigned)pos == pm) cand[warp][3] = (unsigned)t;
+      bar_diag();
+      const unsigned h0 = cand[0][0], l0 = cand[0][1], p0 = cand[0][2];
+      const unsigned h1 = cand[1][0], l1 = cand[1][1], p1 = cand[1][2];
+      const bool w1 = (h1 > h0) || (h1 == h0 && (l1 > l0 || (l1 == l0 && p1 < p0)));
+      const int pr = (int)cand[w1 ? 1 : 0][3];   // pivot row (thread)
+      const int lp = (int)(w1 ? p1 : p0);        // its logical position
+      if (t == pr) {
+        VT* out = reinterpret_cast<VT*>(prow);
 #pragma unroll
-      for (int i = 0; i < NCH / 4; ++i) {
-        const int qq = cp + 4 * i;
-        if (qq >= q0 && qq * V < nb) {
-          const VT pv = prow[qq];
-          VT ov = orow[qq];
+        for (int q = j / V; q < NCH; ++q) {
+          VT v;
+#pragma unroll
+          for (int e = 0; e < V; ++e) vset<T>(v, e, R[q * V + e]);
+          out[q] = v;
+        }
+      }
+      bar_diag();
+      const T sv = prow[j];
+      if (t == pr) { pos = j; used = true; } else if (pos == j) { pos = lp; }
+      if (t == 0) lpiv[j] = lp;
+      const T rp = (sv != T(0)) ? T(1) / sv : T(0);
+      if (rp == T(0)) {
+        zero = true;
+      } else if (!used) {
+        const T m = R[j] * rp;
+        R[j] = m;
+        const VT* in = reinterpret_cast<const VT*>(prow);
+#pragma unroll
+        for (int q = j / V; q < NCH; ++q) {
+          const VT pv = in[q];
 #pragma unroll
           for (int e = 0; e < V; ++e) {
-            const int c = qq * V + e;
-            if (c == j) vset<T>(ov, e, m);
-            else if (c > j) vset<T>(ov, e, vget<T>(ov, e) - m * vget<T>(pv, e));
+            const int c = q * V + e;
+            if (c > j) R[c] -= m * vget<T>(pv, e);
           }
-          orow[qq] = ov;
         }
       }
     }
-    // the lane holding column j + 1 of row ur publishes it for the next step
-    // (rows not updated here are not written by anyone in this step)
-    if (j + 1 < nb && cp == (((j + 1) / V) & 3)) colv[(j + 1) & 1][ur] = S[ur][j + 1];
-    __syncthreads();
   }
-  if (zero && tid == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-  if (warp == 0) { order[pos0] = a0; order[pos1] = a1; }
-  __syncthreads();
-  for (int e = tid; e < NB * NB; e += kDiagThreads) {
-    const int rr = e & (NB - 1), cc = e >> 6;
-    if (rr < nb && cc < nb) A[(k + cc) * lda + (k + rr)] = S[order[rr]][cc];
+  if (zero && t == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
+  // write back in logical row order: row t goes to position pos
+  if (t < nb) {
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+      if (c < nb) A[(k + c) * lda + (k + pos)] = R[c];
   }
-  if (tid < nb) ipiv[k + tid] = (int32_t)(k + lpiv[tid]);
+  bar_diag();
+  if (t < nb) ipiv[k + t] = (int32_t)(k + lpiv[t]);
 }
 
 // ----------------------------------------------------------------------------
@@ -358,6 +364,149 @@ k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __res
       const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
       A[c * lda + k + r] = tile[cc][r];
     }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// (2b) k_strip: a strip of columns outside a factored panel (the panel's w
+// rows, w <= kStripRows, starting at row K0). On the columns [cl0, cl1) it
+// applies the row swaps of all the panel's 64-row blocks; on [cr0, cr1) the
+// swaps and then U12 = L_panel^-1 A12 (L_panel: the panel's unit lower
+// w x w triangle), block by block: forward substitution with the diagonal
+// block's L, then the update of the later row blocks with L's off-diagonal
+// block. One CTA owns 64 columns, all w rows in shared memory, so the strip
+// costs one launch instead of a pass per block and step.
+constexpr int kStripRows = 256;
+constexpr int kStripCols = 64;
+constexpr int kStripThreads = 256;
+template <class T> __host__ __device__ constexpr int strip_pitch() { return kStripRows + 16 / (int)sizeof(T); }
+template <class T> constexpr size_t strip_smem() {
+  return (size_t)kStripCols * strip_pitch<T>() * sizeof(T)      // tile[col][row]
+         + (size_t)NB * rpitch<T>() * sizeof(T)                  // Lc[j][r] = L(r, j) of a diagonal block
+         + (size_t)NB * rpitch<T>() * sizeof(T)                  // Lo[j][r] = L(r, j) of an off-diagonal block
+         + (size_t)kStripRows * sizeof(int) + 64;                // row sources
+}
+
+template <class T>
+__global__ void __launch_bounds__(kStripThreads)
+k_strip(T* __restrict__ A, int64_t lda, int64_t K0, int w, const int32_t* __restrict__ ipiv, int64_t cl0,
+        int64_t cl1, int64_t cr0, int64_t cr1) {
+  typedef typename V16<T>::type VT;
+  constexpr int V = V16<T>::n, RP = rpitch<T>(), TP = strip_pitch<T>();
+  extern __shared__ __align__(16) unsigned char ssm[];
+  T (*tile)[TP] = reinterpret_cast<T (*)[TP]>(ssm);
+  T (*Lc)[RP] = reinterpret_cast<T (*)[RP]>(ssm + (size_t)kStripCols * TP * sizeof(T));
+  T (*Lo)[RP] = reinterpret_cast<T (*)[RP]>(ssm + (size_t)kStripCols * TP * sizeof(T) + (size_t)NB * RP * sizeof(T));
+  int* src = reinterpret_cast<int*>(ssm + (size_t)kStripCols * TP * sizeof(T) + (size_t)2 * NB * RP * sizeof(T));
+  const int tid = threadIdx.x;
+  const int nblk = (w + NB - 1) / NB;
+  const int64_t nl = cl1 - cl0, nr = cr1 - cr0;
+  const int64_t gl = (nl + kStripCols - 1) / kStripCols;
+  const bool right = (int64_t)blockIdx.x >= gl;
+  const int64_t c0 = right ? cr0 + ((int64_t)blockIdx.x - gl) * kStripCols : cl0 + (int64_t)blockIdx.x * kStripCols;
+  const int ncol = (int)imin64(kStripCols, right ? cr1 - c0 : cl1 - c0);
+  // source row of each panel row after the swaps of its block (LAPACK order)
+  if (tid < nblk) {
+    const int b0 = tid * NB, nbb = min(NB, w - b0);
+    for (int j = 0; j < nbb; ++j) src[b0 + j] = b0 + j;
+    for (int j = 0; j < nbb; ++j) {
+      const int p = (int)(ipiv[K0 + b0 + j] - K0);
+      const int t0 = src[b0 + j]; src[b0 + j] = src[p]; src[p] = t0;
+    }
+  }
+  __syncthreads();
+  int moved = 0;
+  for (int r = tid; r < w; r += kStripThreads) moved |= (src[r] != r);
+  if (!right && !__syncthreads_or(moved)) return;   // no swaps: nothing to do on the left columns
+  const int wr = nblk * NB;   // rows past w (a partial last block) are zero
+  for (int e = tid; e < kStripCols * wr; e += kStripThreads) {
+    const int r = e % wr, cc = e / wr;
+    if (cc < ncol) tile[cc][r] = (r < w) ? A[(c0 + cc) * lda + K0 + src[r]] : T(0);
+  }
+  __syncthreads();
+  if (right) {
+    for (int b = 0; b < nblk; ++b) {
+      const int b0 = b * NB, nbb = min(NB, w - b0);
+      // L of the diagonal block, column-major by j: Lc[j][r] = L(b0 + r, b0 + j), strictly lower
+      stage_block<kStripThreads, T>(
+          tid,
+          [&](int r, int j) {
+            return (r < nbb && j < nbb && r > j) ? A[(K0 + b0 + j) * lda + K0 + b0 + r] : T(0);
+          },
+          [&](int r, int j, T v) { Lc[j][r] = v; });
+      __syncthreads();
+      if (tid < ncol) {   // forward substitution, one column per thread
+        T x[NB];
+        const VT* col = reinterpret_cast<const VT*>(&tile[tid][b0]);
+#pragma unroll
+        for (int q = 0; q < NB / V; ++q) {
+          const VT v = col[q];
+#pragma unroll
+          for (int e = 0; e < V; ++e) x[q * V + e] = vget<T>(v, e);
+        }
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+          const T xj = x[j];
+          const VT* lcol = reinterpret_cast<const VT*>(&Lc[j][0]);
+#pragma unroll
+          for (int q = (j + 1) / V; q < NB / V; ++q) {
+            const VT u = lcol[q];
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+              const int r = q * V + e;
+              if (r > j) x[r] -= vget<T>(u, e) * xj;
+            }
+          }
+        }
+        VT* out = reinterpret_cast<VT*>(&tile[tid][b0]);
+#pragma unroll
+        for (int q = 0; q < NB / V; ++q) {
+          VT v;
+#pragma unroll
+          for (int e = 0; e < V; ++e) vset<T>(v, e, x[q * V + e]);
+          out[q] = v;
+        }
+      }
+      __syncthreads();
+      // later row blocks: tile[rows of b2] -= L(b2, b) tile[rows of b]
+      for (int b2 = b + 1; b2 < nblk; ++b2) {
+        const int r0 = b2 * NB, nr2 = min(NB, w - r0);
+        stage_block<kStripThreads, T>(
+            tid,
+            [&](int r, int j) { return (r < nr2 && j < nbb) ? A[(K0 + b0 + j) * lda + K0 + r0 + r] : T(0); },
+            [&](int r, int j, T v) { Lo[j][r] = v; });
+        __syncthreads();
+        // thread: rows 4*(tid%16).., columns 4*(tid/16)..
+        const int rr = 4 * (tid & 15), cc = 4 * (tid >> 4);
+        T acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int d = 0; d < 4; ++d) acc[a][d] = T(0);
+#pragma unroll 8
+        for (int j = 0; j < NB; ++j) {
+          T lv[4], xv[4];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) lv[a] = Lo[j][rr + a];
+#pragma unroll
+          for (int d = 0; d < 4; ++d) xv[d] = tile[cc + d][b0 + j];
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int d = 0; d < 4; ++d) acc[a][d] += lv[a] * xv[d];
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+            if (rr + a < nr2) tile[cc + d][r0 + rr + a] -= acc[a][d];
+        __syncthreads();
+      }
+    }
+  }
+  for (int e = tid; e < kStripCols * w; e += kStripThreads) {
+    const int r = e % w, cc = e / w;
+    if (cc < ncol && (right || src[r] != r)) A[(c0 + cc) * lda + K0 + r] = tile[cc][r];
   }
 }
 
@@ -553,7 +702,7 @@ int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64
 // commute, and a row update (C_r -= L_r U) commutes with a swap of the rows
 // of both C and L. Step (1) leaves P's L rows swapped by all of P's blocks,
 // so a strip of columns outside P first receives all of P's swaps and only
-// then the per-block substitutions and updates. Columns are split between the
+// then the per-block substitutions and updates (k_strip). Columns are split between the
 // streams so that no element is written by both at once.
 constexpr int kOuterNB = 256;
 
@@ -590,6 +739,16 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     FP_CUDA_TRY(c->err, cudaGetLastError());
     return FP_OK;
   };
+  static_assert(kOuterNB == kStripRows, "a strip holds one outer panel's rows");
+  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_strip<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem<T>()));
+  auto strip = [&](int64_t K0, int w, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1) -> int {
+    const int64_t g = (cl1 - cl0 + kStripCols - 1) / kStripCols + (cr1 - cr0 + kStripCols - 1) / kStripCols;
+    if (g <= 0) return FP_OK;
+    k_strip<T><<<(unsigned)g, kStripThreads, strip_smem<T>(), c->stream>>>(A, lda, K0, w, ipiv, cl0, cl1, cr0, cr1);
+    ++c->nlaunch;
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+    return FP_OK;
+  };
   // stream2 starts after everything already queued on c->stream
   FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream2, c->ev_rest, 0));
@@ -618,15 +777,7 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     // (2) the next panel's columns: P's swaps and U12 rows, then their update
     if (knext > kend) {
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
-      for (int64_t k = K0; k < kend; k += NB)
-        if (int rc = u12(k, 0, 0, kend, knext, 1)) return rc;
-      for (int64_t k = K0; k < kend; k += NB) {
-        const int64_t k1 = std::min<int64_t>(k + NB, n);
-        if (int rc = u12(k, 0, 0, kend, knext, 2)) return rc;
-        if (kend > k1)
-          if (int rc = gemm_sub<T>(c, at(k1, k), at(k, kend), at(k1, kend), lda, kend - k1, knext - kend, NB))
-            return rc;
-      }
+      if (int rc = strip(K0, (int)(kend - K0), 0, 0, kend, knext)) return rc;
       if (int rc = gemm_sub<T>(c, at(kend, K0), at(K0, kend), at(kend, kend), lda, n - kend, knext - kend,
                                (int)(kend - K0)))
         return rc;
@@ -635,15 +786,7 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     {
       OnStream2 on2(c);
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
-      for (int64_t k = K0; k < kend; k += NB)
-        if (int rc = u12(k, 0, K0, knext, n, 1)) return rc;
-      for (int64_t k = K0; k < kend; k += NB) {
-        const int64_t k1 = std::min<int64_t>(k + NB, n);
-        if (int rc = u12(k, 0, 0, knext, n, 2)) return rc;
-        if (kend > k1 && n > knext)
-          if (int rc = gemm_sub<T>(c, at(k1, k), at(k, knext), at(k1, knext), lda, kend - k1, n - knext, NB))
-            return rc;
-      }
+      if (int rc = strip(K0, (int)(kend - K0), 0, K0, knext, n)) return rc;
       if (n > knext)
         if (int rc = gemm_sub<T>(c, at(kend, K0), at(K0, knext), at(kend, knext), lda, n - kend, n - knext,
                                  (int)(kend - K0)))
