@@ -70,6 +70,8 @@ struct fp_ctx {
   float* d_cert = nullptr;              // max |L| certificate
   double* d_dinv64 = nullptr;           // inverses of the FP64 diagonal blocks
   float* d_dinv32 = nullptr;            // inverses of the FP32 diagonal blocks
+  double* d_dinv128_64 = nullptr;       // inverses of the 128-row diagonal blocks (FP64 factors)
+  float* d_dinv128_32 = nullptr;        // inverses of the 128-row diagonal blocks (FP32 factors)
   double* d_part = nullptr;             // GEMV partial sums
   void* d_linv = nullptr;               // inv(L11), inv(U11) of the current block (2 x NB x NB, FP64 size)
   double* d_norms = nullptr;            // column norms (2 x cap_rhs)

@@ -972,6 +972,226 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
   }
 }
 
+// ----------------------------------------------------------------------------
+// Single-RHS sweep over 128-row blocks (k_trs1): block b needs y_s of every
+// earlier block s (in sweep order); a CTA streams the row block's tiles with
+// 16-byte loads issued before it waits, each warp reading the flags of up to
+// 32 upcoming blocks with one acquire load per lane and consuming every block
+// already complete, partial sums per thread (4 rows x 16 columns of a tile),
+// reduced once; then x_b = inv(D_bb) (b_b - sum) with inv(D_bb) staged in
+// shared memory while the CTA streams. The chain of dependent blocks is
+// n/128 long.
+constexpr int SB = 128;
+constexpr int kTrs1Threads = 256;
+template <class T> constexpr size_t trs1_smem() {
+  return (size_t)SB * (SB + 1) * sizeof(T) + (size_t)8 * SB * sizeof(T) + (size_t)2 * SB * sizeof(T) + 64;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned int* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
+
+template <class T, bool LOWER>
+__global__ void __launch_bounds__(kTrs1Threads)
+k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv128, T* __restrict__ B,
+       unsigned int* __restrict__ flags, unsigned int* __restrict__ ticket, int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  T (*Ds)[SB + 1] = reinterpret_cast<T (*)[SB + 1]>(tsm);                    // Ds[l][r] = inv(D)(r, l)
+  T (*red)[SB] = reinterpret_cast<T (*)[SB]>(tsm + (size_t)SB * (SB + 1) * sizeof(T));   // per phase
+  T* accs = reinterpret_cast<T*>(tsm + (size_t)SB * (SB + 1) * sizeof(T) + (size_t)8 * SB * sizeof(T));
+  T* xpart = accs + SB;
+  __shared__ int blk_s, stop_s;
+  const int64_t nblk = (n + SB - 1) / SB;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int rg = tid & 31, ph = tid >> 5;   // rows 4rg..4rg+3, columns ph, ph+8, ...
+  for (;;) {
+    if (tid == 0) { blk_s = (int)atomicAdd(ticket, 1u); stop_s = 0; }
+    __syncthreads();
+    const int64_t tk = blk_s;
+    if (tk >= nblk) return;
+    const int64_t b = LOWER ? tk : nblk - 1 - tk;
+    const int64_t k0 = b * SB;
+    const int nb = (int)imin64(SB, n - k0);
+    const T* Di = Dinv128 + b * 2 * SB * SB + (LOWER ? 0 : SB * SB);
+    for (int e = tid; e < SB * SB; e += kTrs1Threads) Ds[e / SB][e % SB] = Di[e];   // Di column-major: e = l*SB + r
+    T sum[4] = {T(0), T(0), T(0), T(0)};
+    const bool rows_full = 4 * rg + 4 <= nb;
+    int64_t ready = 0;   // dependencies known complete (this warp)
+    for (int64_t s = 0; s < tk; ++s) {
+      const int64_t cb = LOWER ? s : nblk - 1 - s;
+      const int64_t c0 = cb * SB;
+      const int cn = (int)imin64(SB, n - c0);
+      // this thread's part of the tile: 4 rows x 16 columns
+      T a[16][4];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int col = ph + 8 * i;
+        if (col < cn && rows_full) {
+          const T* src = A + (c0 + col) * lda + k0 + 4 * rg;
+          if (sizeof(T) == 4) {
+            const float4 v = *reinterpret_cast<const float4*>(src);
+            a[i][0] = v.x; a[i][1] = v.y; a[i][2] = v.z; a[i][3] = v.w;
+          } else {
+            const double2 v0 = *reinterpret_cast<const double2*>(src);
+            const double2 v1 = *reinterpret_cast<const double2*>(src + 2);
+            a[i][0] = v0.x; a[i][1] = v0.y; a[i][2] = v1.x; a[i][3] = v1.y;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) a[i][j] = (col < cn && 4 * rg + j < nb) ? A[(c0 + col) * lda + k0 + 4 * rg + j] : T(0);
+        }
+      }
+      if (s >= ready) {   // read the flags of up to 32 blocks at once
+        int spins = 0;
+        for (;;) {
+          const int64_t sq = s + lane;
+          const int64_t fb = LOWER ? sq : nblk - 1 - sq;
+          const unsigned f = (sq < tk) ? ld_acquire(&flags[fb]) : 0u;
+          const unsigned m = __ballot_sync(0xffffffffu, f != 0u);
+          const int cnt = __ffs(~m) - 1;   // consecutive ready blocks from s
+          if (m == 0xffffffffu) { ready = s + 32; break; }
+          if (cnt > 0) { ready = s + cnt; break; }
+          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+          __nanosleep(32);
+        }
+        __syncwarp();
+        if (stop_s) break;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int col = ph + 8 * i;
+        const T yv = (col < cn) ? ld_cg(&B[c0 + col]) : T(0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) sum[j] += a[i][j] * yv;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) red[ph][4 * rg + j] = sum[j];
+    __syncthreads();
+    if (stop_s) return;
+    if (tid < SB) {
+      T s0 = T(0);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) s0 += red[q][tid];
+      accs[tid] = (tid < nb) ? B[k0 + tid] - s0 : T(0);
+    }
+    __syncthreads();
+    {   // x = inv(D) acc: thread (r, half) sums half of the columns
+      const int r = tid % SB, h = tid / SB;
+      T s0 = T(0);
+#pragma unroll 8
+      for (int l = h * (SB / 2); l < (h + 1) * (SB / 2); ++l) s0 += Ds[l][r] * accs[l];
+      if (h == 1) xpart[r] = s0;
+      __syncthreads();
+      if (h == 0 && r < nb) B[k0 + r] = s0 + xpart[r];
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(&flags[b], 1u);
+  }
+}
+
+// Inverses of the 128-row diagonal blocks from those of the 64-row blocks:
+// inv(L_B) = [[Li0, 0], [-Li1 L21 Li0, Li1]], inv(U_B) = [[Ui0, -Ui0 U12 Ui1],
+// [0, Ui1]]; Dinv128[B] = inv(L_B), inv(U_B), SB x SB column-major each.
+template <class T> constexpr size_t dinv128_smem() { return (size_t)4 * NB * (NB + 1) * sizeof(T); }
+
+template <class T>
+__global__ void __launch_bounds__(256)
+k_dinv128(const T* __restrict__ LU, int64_t lda, int64_t n, const T* __restrict__ Dinv64, T* __restrict__ Dinv128) {
+  extern __shared__ __align__(16) unsigned char dsm3[];
+  T (*X)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm3);   // [r][c]
+  T (*Y)[NB + 1] = X + NB;
+  T (*Z)[NB + 1] = X + 2 * NB;
+  T (*W)[NB + 1] = X + 3 * NB;
+  const int tid = threadIdx.x;
+  const int64_t B = blockIdx.x;
+  const int64_t i0 = 2 * B, k0 = B * SB;
+  const bool two = k0 + NB < n;
+  const int n1 = two ? (int)imin64(NB, n - k0 - NB) : 0;
+  T* outL = Dinv128 + B * 2 * SB * SB;
+  T* outU = outL + SB * SB;
+  for (int e = tid; e < SB * SB; e += 256) { outL[e] = T(0); outU[e] = T(0); }
+  __syncthreads();
+  // diagonal quadrants: the 64-row inverses (identity for a missing second block)
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int r = e % NB, c = e / NB;
+    const T* L0 = Dinv64 + i0 * 2 * NB * NB;
+    outL[c * SB + r] = L0[e];
+    outU[c * SB + r] = L0[NB * NB + e];
+    T l1 = (r == c) ? T(1) : T(0), u1 = l1;
+    if (two) {
+      const T* L1 = Dinv64 + (i0 + 1) * 2 * NB * NB;
+      l1 = L1[e];
+      u1 = L1[NB * NB + e];
+    }
+    outL[(NB + c) * SB + NB + r] = l1;
+    outU[(NB + c) * SB + NB + r] = u1;
+  }
+  if (!two) return;
+  auto mm = [&](T (*C)[NB + 1], T (*P)[NB + 1], T (*Q)[NB + 1], T sgn) {   // C = sgn * P Q
+    for (int e = tid; e < NB * NB; e += 256) {
+      const int r = e % NB, c = e / NB;
+      T s = T(0);
+      for (int l = 0; l < NB; ++l) s += P[r][l] * Q[l][c];
+      C[r][c] = sgn * s;
+    }
+  };
+  const T* L0 = Dinv64 + i0 * 2 * NB * NB;
+  const T* L1 = Dinv64 + (i0 + 1) * 2 * NB * NB;
+  // lower: X = L21, Y = Li0 -> Z = L21 Li0; Y = Li1 -> W = -Li1 Z
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int r = e % NB, c = e / NB;
+    X[r][c] = (r < n1) ? LU[(k0 + c) * lda + k0 + NB + r] : T(0);
+    Y[r][c] = L0[e];
+  }
+  __syncthreads();
+  mm(Z, X, Y, T(1));
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += 256) Y[e % NB][e / NB] = L1[e];
+  __syncthreads();
+  mm(W, Y, Z, T(-1));
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int r = e % NB, c = e / NB;
+    outL[c * SB + NB + r] = W[r][c];
+  }
+  // upper: X = U12, Y = Ui1 -> Z = U12 Ui1; Y = Ui0 -> W = -Ui0 Z
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int r = e % NB, c = e / NB;
+    X[r][c] = (c < n1) ? LU[(k0 + NB + c) * lda + k0 + r] : T(0);
+    Y[r][c] = L1[NB * NB + e];
+  }
+  __syncthreads();
+  mm(Z, X, Y, T(1));
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += 256) Y[e % NB][e / NB] = L0[NB * NB + e];
+  __syncthreads();
+  mm(W, Y, Z, T(-1));
+  __syncthreads();
+  for (int e = tid; e < NB * NB; e += 256) {
+    const int r = e % NB, c = e / NB;
+    outU[(NB + c) * SB + r] = W[r][c];
+  }
+}
+
+template <class T, bool LOWER>
+static int run_trs1(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv128, T* B) {
+  const int64_t nblk = (n + SB - 1) / SB;
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
+  const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
+  k_trs1<T, LOWER><<<grid, kTrs1Threads, trs1_smem<T>(), c->stream>>>(A, lda, n, Dinv128, B, c->d_flags,
+                                                                      c->d_flags + nblk, c->d_status);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+
 template <class T, bool LOWER, int KR, bool TRANS = false>
 static int run_trs(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv, T* B,
                    int64_t ldb) {
@@ -1031,6 +1251,17 @@ int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv
     ++c->nlaunch;
     FP_CUDA_TRY(c->err, cudaGetLastError());
   }
+  if (k == 1) {   // one right-hand side: the 128-row streaming sweeps
+    const T* D128 = reinterpret_cast<const T*>(sizeof(T) == 8 ? (void*)c->d_dinv128_64 : (void*)c->d_dinv128_32);
+    static bool attr = false;
+    if (!attr) {
+      FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_trs1<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trs1_smem<T>()));
+      FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_trs1<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trs1_smem<T>()));
+      attr = true;
+    }
+    if (int rc = run_trs1<T, true>(c, LU, n, lda, D128, B)) return rc;
+    return run_trs1<T, false>(c, LU, n, lda, D128, B);
+  }
   for (int64_t q0 = 0; q0 < k;) {
     const int64_t left = k - q0;
     const int kr = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
@@ -1046,6 +1277,15 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda) {
   const int64_t nblk = (n + NB - 1) / NB;
   T* Dinv = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_dinv64 : (void*)c->d_dinv32);
   k_diag_inv<T><<<(unsigned)nblk, NB, 0, c->stream>>>(LU, lda, n, Dinv);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  T* D128 = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_dinv128_64 : (void*)c->d_dinv128_32);
+  static bool attr = false;
+  if (!attr) {
+    FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_dinv128<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dinv128_smem<T>()));
+    attr = true;
+  }
+  k_dinv128<T><<<(unsigned)((n + SB - 1) / SB), 256, dinv128_smem<T>(), c->stream>>>(LU, lda, n, Dinv, D128);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;
