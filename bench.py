@@ -119,6 +119,36 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def batch_throughput(fp, device, nwings=64, nslots=8, reps=2):
+    """Config 3b: 64 wings drawn from default_rng(0) (sweep U[0,45], AR U[4,10],
+    taper U[0.3,1], tip twist U[-4,0], 2k-8k panels), mixed precision, solved
+    by fp_batch_solve with nslots device contexts against the same solves
+    one at a time (one slot). Wall time of the whole batch, host set-up
+    included. Returns a dict."""
+    cap = fp._capi
+    wings, params = fp.meshes.random_wings(nwings, seed=0)
+    bodies = [fp.RigidWakeBody(w) for w in wings]
+    V = np.array([np.cos(np.deg2rad(AOA)), 0.0, np.sin(np.deg2rad(AOA))])
+    Us = [np.tile(V, (b.ncells, 1)) for b in bodies]
+    Ds = [np.tile(V, (b.nsheddings, 1)) for b in bodies]
+    out = {"config": f"{nwings} wings from default_rng(0), {min(b.ncells for b in bodies)}-"
+                     f"{max(b.ncells for b in bodies)} panels ({sum(b.ncells for b in bodies)} total), mixed",
+           "nslots": nslots}
+    for label, slots in (("sequential", 1), ("batched", nslots)):
+        batch = cap.Batch(device, slots)
+        fp.solve_batch(bodies, Us, Ds, Ds, precision="mixed", batch=batch)   # warm-up, buffers sized
+        best = 1e30
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fp.solve_batch(bodies, Us, Ds, Ds, precision="mixed", batch=batch)
+            best = min(best, time.perf_counter() - t0)
+        batch.close()
+        out[f"{label}_s"] = best
+        out[f"{label}_wings_per_s"] = nwings / best
+    out["speedup"] = out["sequential_s"] / out["batched_s"]
+    return out
+
+
 def measured_peak(key, fallback):
     """A peak from MEASURED_PEAKS.json (driver-measured on this pool), else
     the stated fallback."""
@@ -310,6 +340,7 @@ def run_ours(args, rank, ws, dist):
     ops = 248.0 * N * N + 290.0 * 2 * w.nsheddings * N
     achieved = ops / (stg_d[0] * 1e-3) / 1e12
     d_launches, d_ms, d_flops = ktime["fp64"]
+    batched = batch_throughput(fp, device) if not args.no_batch else None
     cpu = None
     if not args.no_cpu_baseline:
         O = ge.load_oracle()
@@ -353,6 +384,7 @@ def run_ours(args, rank, ws, dist):
                                   "peak_source": "measured FP64 FMA throughput (fp_measure_fma_peak)"},
             "fp64_trailing_update": {"kernel": "k_gemm_sub<double> (SIMT FP64)", "launches": d_launches,
                                      "ms_total": d_ms, "tflops": d_flops / (d_ms * 1e-3) / 1e12 if d_ms else 0},
+            "batched_wings": batched,
             "clocks": clk.summary()}
     if cpu:
         line["cpu_baseline"] = cpu
@@ -368,6 +400,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-wing batched throughput leg")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="with --profile: which form to time")
     ap.add_argument("--profile", action="store_true",

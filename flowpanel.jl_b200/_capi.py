@@ -25,7 +25,8 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_set_wake", "fp_assemble", "fp_get_aic", "fp_set_rhs", "fp_factor", "fp_solve",
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
-           "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read")
+           "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
+           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve")
 
 
 class SolveOpts(C.Structure):
@@ -41,6 +42,14 @@ class Stats(C.Structure):
 
     def asdict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class BodyDesc(C.Structure):
+    _fields_ = [("nodes", C.POINTER(C.c_double)), ("nnodes", C.c_int64),
+                ("panel_offsets", C.POINTER(C.c_int32)), ("panel_nodes", C.POINTER(C.c_int32)),
+                ("npanels", C.c_int64), ("cps", C.POINTER(C.c_double)), ("normals", C.POINTER(C.c_double)),
+                ("shedding", C.POINTER(C.c_int32)), ("nsh", C.c_int64), ("Das", C.POINTER(C.c_double)),
+                ("Dbs", C.POINTER(C.c_double)), ("Uinfs", C.POINTER(C.c_double)), ("x", C.POINTER(C.c_double))]
 
 
 class FlowPanelError(RuntimeError):
@@ -82,6 +91,12 @@ def lib():
         L.fp_lu_solve_noalloc.argtypes = [vp, C.c_void_p, C.c_int64, C.c_int64]
         L.fp_assembly_vjp.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.fp_uind_vjp.argtypes = [vp, _dp, _dp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.fp_batch_create.argtypes = [C.c_int, C.c_int, C.POINTER(vp)]
+        L.fp_batch_destroy.argtypes = [vp]
+        L.fp_batch_last_error.argtypes = [vp]
+        L.fp_batch_last_error.restype = C.c_char_p
+        L.fp_batch_solve.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_int64, C.POINTER(BodyDesc),
+                                     C.POINTER(SolveOpts), C.POINTER(Stats)]
         L.fp_kernel_timing.argtypes = [vp, C.c_int]
         L.fp_kernel_timing_read.argtypes = [vp, C.POINTER(C.c_int64), _dp, _dp]
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
@@ -280,3 +295,54 @@ def tc_selftest(m, n, k, device=0):
     if rc:
         raise FlowPanelError(rc, "fp_tc_selftest failed")
     return a.value, b.value, t.value
+
+
+class Batch:
+    """nslots device contexts solving many bodies concurrently (fp_batch_*)."""
+
+    def __init__(self, device=0, nslots=4):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.fp_batch_create(int(device), int(nslots), C.byref(h))
+        if rc:
+            raise FlowPanelError(rc, f"fp_batch_create failed on device {device}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.fp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, element, problems, kerneloffset=1e-8, kernelcutoff=1e-14, opts=None):
+        """problems: list of dicts with nodes, panel_offsets, panel_nodes, Uinfs (N, 3)
+        and optionally cps, normals, shedding, Das, Dbs. Returns (strengths list, stats list)."""
+        keep, descs, outs = [], [], []
+        for p in problems:
+            nodes = _f64(p["nodes"])
+            offs = np.ascontiguousarray(p["panel_offsets"], dtype=np.int32)
+            pn = np.ascontiguousarray(p["panel_nodes"], dtype=np.int32)
+            n = len(offs) - 1
+            U = _f64(np.reshape(p["Uinfs"], (n, 3)))
+            cps, normals = _f64(p.get("cps")), _f64(p.get("normals"))
+            sh = p.get("shedding")
+            sh = np.ascontiguousarray(np.reshape(sh, (-1, 6)), dtype=np.int32) if sh is not None else None
+            Da = _f64(np.reshape(p["Das"], (-1, 3))) if p.get("Das") is not None else None
+            Db = _f64(np.reshape(p["Dbs"], (-1, 3))) if p.get("Dbs") is not None else None
+            x = np.zeros(n)
+            keep.append((nodes, offs, pn, U, cps, normals, sh, Da, Db, x))
+            outs.append(x)
+            descs.append(BodyDesc(_d(nodes), nodes.shape[0], _i(offs), _i(pn), n, _d(cps), _d(normals), _i(sh),
+                                  0 if sh is None else sh.shape[0], _d(Da), _d(Db), _d(U), _d(x)))
+        arr = (BodyDesc * len(descs))(*descs)
+        st = (Stats * len(descs))()
+        rc = self._L.fp_batch_solve(self.h, element, kerneloffset, kernelcutoff, len(descs), arr,
+                                    C.byref(opts) if opts is not None else None, st)
+        if rc:
+            raise FlowPanelError(rc, self._L.fp_batch_last_error(self.h).decode())
+        return outs, [s.asdict() for s in st]

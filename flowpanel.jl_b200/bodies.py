@@ -259,6 +259,51 @@ def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200So
     return body
 
 
+def solve_batch(bodies: List[AbstractBody], Uinfs, Das=None, Dbs=None, method="ludiv", precision="mixed",
+                device=0, nslots=4, batch=None):
+    """Solve many bodies of one element type concurrently on one device
+    (fp_batch_solve: nslots device contexts, largest bodies first). Each
+    body's strengths and fields are stored as ``solve`` stores them, and each
+    equals the result of solving that body alone. Uinfs, Das, Dbs are lists
+    with one entry per body. Returns the per-body statistics."""
+    if not bodies:
+        return []
+    kinds = {b.kind for b in bodies}
+    if len(kinds) != 1:
+        raise ValueError("solve_batch: all bodies must use the same element type")
+    lifting = bodies[0].kind == "vortexring"
+    problems = []
+    for i, b in enumerate(bodies):
+        U = np.asarray(Uinfs[i], dtype=np.float64)
+        if U.shape != (b.ncells, 3):
+            raise ValueError(f"Invalid Uinfs of body {i}; expected size ({b.ncells}, 3), got {U.shape}")
+        normals = calc_normals(b)
+        p = dict(nodes=b.mesh.nodes, panel_offsets=b.mesh.panel_offsets, panel_nodes=b.mesh.panel_nodes,
+                 Uinfs=U, normals=normals, cps=calc_controlpoints(b, normals))
+        if lifting:
+            p.update(shedding=b.mesh.shedding, Das=np.asarray(Das[i], float), Dbs=np.asarray(Dbs[i], float))
+        problems.append(p)
+    opts = _capi.make_opts("gmres" if method == "gmres" else "ludiv", precision)
+    own = batch is None
+    batch = batch or _capi.Batch(device, nslots)
+    try:
+        xs, stats = batch.solve(bodies[0].element, problems, bodies[0].kerneloffset, bodies[0].kernelcutoff, opts)
+    finally:
+        if own:
+            batch.close()
+    for i, (b, x) in enumerate(zip(bodies, xs)):
+        b.strength = x
+        b.solved = True
+        b.add_field("Uinf", "vector", problems[i]["Uinfs"], "cell")
+        if lifting:
+            b.add_field("Da", "vector", problems[i]["Das"], "system")
+            b.add_field("Db", "vector", problems[i]["Dbs"], "system")
+            b.add_field("Gamma", "scalar", x, "cell")
+        else:
+            b.add_field("sigma", "scalar", x, "cell")
+    return stats
+
+
 def Uind(body: AbstractBody, targets, out, solver: Optional[B200Solver] = None, precision="fp64"):
     """Uind!: add the velocity induced by the solved body at targets (M, 3) to out
     (src/FLOWPanel_abstractbody.jl:101-110)."""

@@ -9,13 +9,16 @@
 using namespace fpb;
 
 namespace fpb {
-int num_sms() {
-  static int sms = 0;
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
+int num_sms() {   // of the current device, cached per device
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::atomic<int>& slot = cache[dev & 63];
+  int sms = slot.load(std::memory_order_relaxed);
+  if (sms <= 0) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 148;
+    slot.store(sms, std::memory_order_relaxed);
   }
   return sms;
 }
@@ -197,9 +200,14 @@ int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_
   }
   for (int64_t i = 0; i < 3 * nnodes; ++i)
     if (!std::isfinite(nodes[i])) return c->err.set(FP_EINVAL, "fp_set_geometry: non-finite node coordinate");
-  if (c->N != npanels) free_matrices(c);
+  // device buffers only grow: a smaller body reuses them (leading dimension
+  // unchanged), so a sequence of bodies allocates for the largest only
+  if (npanels > c->capN) {
+    free_matrices(c);
+    c->capN = npanels;
+    c->ld = round_up(npanels, 64);
+  }
   c->N = npanels;
-  c->ld = round_up(npanels, 64);
   c->h_nodes.assign(nodes, nodes + 3 * nnodes);
   c->h_offsets.assign(offsets, offsets + npanels + 1);
   c->h_pnodes.assign(pnodes, pnodes + offsets[npanels]);
@@ -265,10 +273,14 @@ int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_
       tgt[(3 + d) * npanels + p] = nr[d];
     }
   }
-  dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt);
-  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_panels, npanels * sizeof(PanelRec)));
-  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_src, npanels * sizeof(SourceRec)));
-  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tgt, 6 * npanels * sizeof(double)));
+  if (npanels > c->cap_geom) {
+    dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt);
+    c->cap_geom = 0;
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_panels, npanels * sizeof(PanelRec)));
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_src, npanels * sizeof(SourceRec)));
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tgt, 6 * npanels * sizeof(double)));
+    c->cap_geom = npanels;
+  }
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_panels, pr.data(), npanels * sizeof(PanelRec), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_src, sr.data(), npanels * sizeof(SourceRec), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_tgt, tgt.data(), 6 * npanels * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -276,7 +288,6 @@ int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   c->has_geometry = true;
   c->nsh = 0;
-  dfree(c->d_wake);
   return FP_OK;
 }
 
@@ -321,9 +332,13 @@ int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* D
     if (touched[pi]++) disjoint = false;
     if (pj >= 0 && touched[pj]++) disjoint = false;
   }
-  dfree(c->d_wake);
-  if (nsh > 0) {
+  if (nsh > c->cap_wake) {
+    dfree(c->d_wake);
+    c->cap_wake = 0;
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_wake, nsh * sizeof(WakeRec)));
+    c->cap_wake = nsh;
+  }
+  if (nsh > 0) {
     FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_wake, w.data(), nsh * sizeof(WakeRec), cudaMemcpyHostToDevice, c->stream));
     FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   }
@@ -345,7 +360,7 @@ int fp_assemble(fp_ctx* c, int element, double kerneloffset, double kernelcutoff
     return c->err.set(FP_EINVAL, "fp_assemble: unknown element");
   if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED)
     return c->err.set(FP_EINVAL, "fp_assemble: unknown precision");
-  const size_t elems = (size_t)c->ld * c->N;
+  const size_t elems = (size_t)c->ld * c->capN;   // for the largest body the buffers hold
   if (!c->d_G) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G, elems * sizeof(double)));
     FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G, 0, elems * sizeof(double), c->stream));
@@ -394,23 +409,26 @@ int fp_set_rhs(fp_ctx* c, const double* Uinfs, int64_t k) {
   return FP_OK;
 }
 
+// Sized for capN (the largest problem the context's buffers hold), so that
+// any later body of up to capN unknowns reuses them.
 static int alloc_factor_buffers(fp_ctx* c, int precision) {
-  const size_t elems = (size_t)c->ld * c->N;
-  const int64_t nblk = (c->N + kLuNB - 1) / kLuNB;
-  if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, c->N * sizeof(int32_t)));
+  const int64_t N = c->capN;
+  const size_t elems = (size_t)c->ld * N;
+  const int64_t nblk = (N + kLuNB - 1) / kLuNB;
+  if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, N * sizeof(int32_t)));
   if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
-  if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * c->N * sizeof(double)));
+  if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * N * sizeof(double)));
   if (!c->d_linv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_linv, (size_t)2 * kLuNB * kLuNB * sizeof(double)));
   if (precision == FP_PREC_FP64) {
     if (!c->d_LU) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_LU, elems * sizeof(double)));
     if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));
     if (!c->d_dinv128_64)
-      FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_64, ((c->N + 127) / 128) * 2 * 128 * 128 * sizeof(double)));
+      FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_64, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(double)));
   } else {
     if (!c->d_G32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G32, elems * sizeof(float)));
     if (!c->d_dinv32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv32, nblk * 2 * kLuNB * kLuNB * sizeof(float)));
     if (!c->d_dinv128_32)
-      FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_32, ((c->N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
+      FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
   }
   return FP_OK;
 }

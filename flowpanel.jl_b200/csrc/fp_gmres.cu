@@ -117,7 +117,7 @@ int gmres_solve(fp_ctx* c, const double* b, double* x, int64_t k, const fp_solve
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_h, (size_t)(2 * (m + 1) + 16) * sizeof(double)));
     c->cap_gmres_m = m;
   }
-  if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * n * sizeof(double)));
+  if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * c->capN * sizeof(double)));
   double* V = c->d_V;
   double* w = c->d_V + (size_t)(m + 1) * ld;   // work vector
   double* u = c->d_V + (size_t)(m + 2) * ld;   // correction

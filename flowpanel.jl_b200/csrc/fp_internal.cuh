@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -34,7 +35,10 @@ struct fp_ctx {
 
   // sizes
   int64_t N = 0;        // panels == unknowns == control points
-  int64_t ld = 0;       // leading dimension of the device matrices
+  int64_t ld = 0;       // leading dimension of the device matrices (>= N, set by capN)
+  int64_t capN = 0;     // matrix buffers hold problems of up to capN unknowns (grow-only)
+  int64_t cap_geom = 0; // panel records allocated
+  int64_t cap_wake = 0; // wake records allocated
   int64_t nsh = 0;
   bool wake_disjoint = true;   // every wake column touched by one edge only
   bool has_geometry = false;
@@ -170,6 +174,22 @@ int gmres_solve(fp_ctx* c, const double* b, double* x, int64_t k, const fp_solve
                 bool precondition, int* iters, double* relres);
 
 int num_sms();
+
+// Raises a kernel's dynamic shared-memory limit once per device. Thread-safe:
+// a repeated call from a racing thread only sets the same value again.
+struct SmemAttr {
+  std::atomic<unsigned long long> done{0};
+  template <class K>
+  cudaError_t ensure(K* kernel, int bytes) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+    return e;
+  }
+};
 
 // KernelTimer: kt_begin records the start event of a launch (returns its
 // slot, or -1 when timing is off or an event cannot be made), kt_end the stop

@@ -652,12 +652,8 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
   } else {
     constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
     constexpr size_t sm = gemm_smem<T, BM, BN, BK, TM, TN>();
-    static bool attr = false;
-    if (!attr) {
-      FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_gemm_sub<T, BM, BN, BK, TM, TN>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      attr = true;
-    }
+    static SmemAttr attr;
+    FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub<T, BM, BN, BK, TM, TN>, (int)sm));
     dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
     const bool pre = ((reinterpret_cast<uintptr_t>(Cm) | (uintptr_t)(lda * sizeof(T))) & 15) == 0;
     const int slot = kt_begin(c);
@@ -673,12 +669,8 @@ int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64
                       int kk) {
   constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8;
   constexpr size_t sm = gemm_smem<float, BM, BN, BK, TM, TN>();
-  static bool attr = false;
-  if (!attr) {
-    FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_gemm_sub<float, BM, BN, BK, TM, TN>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    attr = true;
-  }
+  static SmemAttr attr;
+  FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub<float, BM, BN, BK, TM, TN>, (int)sm));
   dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
   const bool pre = ((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(lda * sizeof(float))) & 15) == 0;
   k_gemm_sub<float, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(A, B, C, lda, m, nn, kk, pre);
@@ -724,7 +716,8 @@ struct OnStream2 {
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
-  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_u12<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)u12_smem<T>()));
+  static SmemAttr attr_u12;
+  FP_CUDA_TRY(c->err, attr_u12.ensure(k_u12<T>, (int)u12_smem<T>()));
   if (sizeof(T) == 4 && c->use_tc) {   // both scratch sets before any concurrent launch
     if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
     if (int rc = ensure_tc_scratch(c, 1, n)) return rc;
@@ -740,7 +733,8 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     return FP_OK;
   };
   static_assert(kOuterNB == kStripRows, "a strip holds one outer panel's rows");
-  FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_strip<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem<T>()));
+  static SmemAttr attr_strip;
+  FP_CUDA_TRY(c->err, attr_strip.ensure(k_strip<T>, (int)strip_smem<T>()));
   auto strip = [&](int64_t K0, int w, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1) -> int {
     const int64_t g = (cl1 - cl0 + kStripCols - 1) / kStripCols + (cr1 - cr0 + kStripCols - 1) / kStripCols;
     if (g <= 0) return FP_OK;
@@ -1253,12 +1247,9 @@ int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv
   }
   if (k == 1) {   // one right-hand side: the 128-row streaming sweeps
     const T* D128 = reinterpret_cast<const T*>(sizeof(T) == 8 ? (void*)c->d_dinv128_64 : (void*)c->d_dinv128_32);
-    static bool attr = false;
-    if (!attr) {
-      FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_trs1<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trs1_smem<T>()));
-      FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_trs1<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trs1_smem<T>()));
-      attr = true;
-    }
+    static SmemAttr attr_lo, attr_up;
+    FP_CUDA_TRY(c->err, attr_lo.ensure(k_trs1<T, true>, (int)trs1_smem<T>()));
+    FP_CUDA_TRY(c->err, attr_up.ensure(k_trs1<T, false>, (int)trs1_smem<T>()));
     if (int rc = run_trs1<T, true>(c, LU, n, lda, D128, B)) return rc;
     return run_trs1<T, false>(c, LU, n, lda, D128, B);
   }
@@ -1280,11 +1271,8 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda) {
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   T* D128 = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_dinv128_64 : (void*)c->d_dinv128_32);
-  static bool attr = false;
-  if (!attr) {
-    FP_CUDA_TRY(c->err, cudaFuncSetAttribute(k_dinv128<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dinv128_smem<T>()));
-    attr = true;
-  }
+  static SmemAttr attr;
+  FP_CUDA_TRY(c->err, attr.ensure(k_dinv128<T>, (int)dinv128_smem<T>()));
   k_dinv128<T><<<(unsigned)((n + SB - 1) / SB), 256, dinv128_smem<T>(), c->stream>>>(LU, lda, n, Dinv, D128);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());

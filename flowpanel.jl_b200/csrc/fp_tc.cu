@@ -268,17 +268,16 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+static EncodeTiledFn resolve_encode_fn() {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    return reinterpret_cast<EncodeTiledFn>(p);
+  return nullptr;
+}
 static EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+  static const EncodeTiledFn fn = resolve_encode_fn();   // initialised once, thread-safe
   return fn;
 }
 
@@ -316,13 +315,8 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
                      int64_t nn, int kk) {
   if (!c->use_tc || kk <= 0 || kk > 256 || m <= 0 || nn <= 0) return false;
   if (!tc::encode_fn()) return false;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(tc::k_tc_gemm_sub, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES) !=
-        cudaSuccess)
-      return false;
-    attr_set = true;
-  }
+  static SmemAttr attr;
+  if (attr.ensure(tc::k_tc_gemm_sub, tc::SMEM_BYTES) != cudaSuccess) return false;
   const int slot = c->tc_slot;
   if (ensure_tc_scratch(c, slot, std::max<int64_t>(m, nn)) != FP_OK) return false;
   const int ldk = (int)round_up(kk, 32);

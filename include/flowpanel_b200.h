@@ -150,6 +150,40 @@ int fp_solve_body(fp_ctx* ctx, int element, double kerneloffset, double kernelcu
                   const double* Uinfs, int64_t k, const fp_solve_opts* opts, double* x,
                   fp_stats* stats);
 
+/* One body of a batch: the arguments of fp_set_geometry, fp_set_wake and
+ * fp_solve_body for one body (host arrays, read during the call only; cps and
+ * normals may be NULL; shedding/Das/Dbs unused for FP_ELEMENT_SOURCE). */
+typedef struct fp_body_desc {
+  const double* nodes;          /* 3 x nnodes */
+  int64_t nnodes;
+  const int32_t* panel_offsets; /* npanels + 1 */
+  const int32_t* panel_nodes;
+  int64_t npanels;
+  const double* cps;            /* 3 x npanels or NULL */
+  const double* normals;        /* 3 x npanels or NULL */
+  const int32_t* shedding;      /* 6 x nsh */
+  int64_t nsh;
+  const double* Das;            /* 3 x nsh */
+  const double* Dbs;            /* 3 x nsh */
+  const double* Uinfs;          /* 3 x npanels */
+  double* x;                    /* out: npanels strengths */
+} fp_body_desc;
+
+/* Batched solves of many bodies of uneven panel counts (the batching form;
+ * no counterpart in the reference, whose solve takes one body at a time).
+ * A batch owns nslots contexts on one device; fp_batch_solve assembles,
+ * factors and solves every body with opts (as fp_solve_body does, so each
+ * result equals a single solve's), nslots bodies at a time, largest first,
+ * one host thread per slot. stats (nbody entries) may be NULL. On failure the
+ * status of the first failing body is returned and fp_batch_last_error names
+ * it; the other bodies are still solved. */
+typedef struct fp_batch fp_batch;
+int fp_batch_create(int device, int nslots, fp_batch** out);
+int fp_batch_destroy(fp_batch* batch);
+const char* fp_batch_last_error(fp_batch* batch);
+int fp_batch_solve(fp_batch* batch, int element, double kerneloffset, double kernelcutoff, int64_t nbody,
+                   const fp_body_desc* bodies, const fp_solve_opts* opts, fp_stats* stats);
+
 /* Induced velocity Uind! of the solved body on m targets, accumulated into
  * out (3 x m): vortex rings + wake horseshoes with (Gamma_pi, Gamma_pj)
  * (src/FLOWPanel_liftingbody.jl:576-661) or constant sources
