@@ -323,3 +323,85 @@ def wing_body(fuse_nx=120, fuse_nt=80, wing_nc=150, wing_ns=180, AR=8.0, taper=0
     # place the wing root quarter chord near the fuselage mid-length, low wing
     wing.nodes = wing.nodes + np.array([-1.0, 0.0, -0.2])
     return concat([fuse, wing])
+
+
+def _point_triangle_distance(P, A, B, C):
+    """Distances from points P (k, 3) to triangles (A, B, C) (k, 3 each), row by
+    row (closest-point regions of the triangle: vertices, edges, face)."""
+    ab, ac, ap = B - A, C - A, P - A
+    d1, d2 = np.einsum("ij,ij->i", ab, ap), np.einsum("ij,ij->i", ac, ap)
+    bp, cp = P - B, P - C
+    d3, d4 = np.einsum("ij,ij->i", ab, bp), np.einsum("ij,ij->i", ac, bp)
+    d5, d6 = np.einsum("ij,ij->i", ab, cp), np.einsum("ij,ij->i", ac, cp)
+    va = d3 * d6 - d5 * d4
+    vb = d5 * d2 - d1 * d6
+    vc = d1 * d4 - d3 * d2
+    denom = va + vb + vc
+    with np.errstate(divide="ignore", invalid="ignore"):
+        v = vb / denom
+        w = vc / denom
+    Q = A + ab * v[:, None] + ac * w[:, None]   # interior projection
+    # edge and vertex regions
+    def seg(X, Y):
+        d = Y - X
+        t = np.clip(np.einsum("ij,ij->i", P - X, d) / np.maximum(np.einsum("ij,ij->i", d, d), 1e-300), 0, 1)
+        return X + d * t[:, None]
+    inside = (va >= 0) & (vb >= 0) & (vc >= 0) & (denom > 0)
+    cands = [seg(A, B), seg(B, C), seg(C, A)]
+    dist = np.min([np.linalg.norm(P - q, axis=1) for q in cands], axis=0)
+    dq = np.linalg.norm(P - Q, axis=1)
+    return np.where(inside, np.minimum(dq, dist), dist)
+
+
+def panel_distance(mesh: Mesh, P, panels):
+    """Distance from each point P[i] to panel panels[i] (triangles and planar
+    quads, the quad as two triangles)."""
+    offs = mesh.panel_offsets
+    nn = offs[panels + 1] - offs[panels]
+    i0 = mesh.panel_nodes[offs[panels]]
+    i1 = mesh.panel_nodes[offs[panels] + 1]
+    i2 = mesh.panel_nodes[offs[panels] + 2]
+    X = mesh.nodes
+    d = _point_triangle_distance(P, X[i0], X[i1], X[i2])
+    q = nn == 4
+    if q.any():
+        i3 = mesh.panel_nodes[offs[panels[q]] + 3]
+        d[q] = np.minimum(d[q], _point_triangle_distance(P[q], X[i0[q]], X[i2[q]], X[i3]))
+    return d
+
+
+def probe_box(mesh: Mesh, n=1_000_000, lo=(-6.0, -6.0, -2.0), hi=(6.0, 6.0, 2.0), min_dist=0.01, seed=5):
+    """n probe points uniform in the box [lo, hi] from default_rng(seed),
+    rejecting points closer than min_dist to any panel (exact point-to-panel
+    distance for the points near the surface). Draws in batches until n
+    points are kept; returns (n, 3)."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    offs = mesh.panel_offsets
+    cen = np.add.reduceat(mesh.nodes[mesh.panel_nodes], offs[:-1], axis=0) / np.diff(offs)[:, None]
+    rad = np.zeros(mesh.npanels)
+    for k in range(4):
+        sel = np.diff(offs) > k
+        idx = mesh.panel_nodes[offs[:-1][sel] + k]
+        rad[sel] = np.maximum(rad[sel], np.linalg.norm(mesh.nodes[idx] - cen[sel], axis=1))
+    R = rad.max() + min_dist
+    tree = cKDTree(cen)
+    kept = []
+    total = 0
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    while total < n:
+        P = lo + (hi - lo) * rng.random((max(n - total, 1) + n // 10 + 16, 3))
+        near = tree.query_ball_point(P, R)
+        ok = np.ones(len(P), bool)
+        cand = [(i, j) for i, lst in enumerate(near) if lst for j in lst]
+        if cand:
+            ci = np.array([c[0] for c in cand])
+            cj = np.array([c[1] for c in cand])
+            d = panel_distance(mesh, P[ci], cj)
+            bad = np.unique(ci[d < min_dist])
+            ok[bad] = False
+        P = P[ok]
+        kept.append(P)
+        total += len(P)
+    return np.concatenate(kept)[:n]
