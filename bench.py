@@ -160,16 +160,18 @@ def measured_peak(key, fallback):
 
 
 def profile_traffic(kernel):
-    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
-    of `kernel`, from the committed ncu summary profiles/<kernel>*.txt (a line
-    'traffic_bytes_per_launch: <bytes>'), scaled there to this workload."""
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per updated
+    output element of `kernel`, from the committed ncu summary
+    profiles/<kernel>*.txt (a line 'traffic_bytes_per_C_element: <bytes>');
+    the bench scales it to its own average launch (traffic grows with the
+    m x n elements each launch updates)."""
     d = os.path.join(ROOT, "profiles")
     try:
         for name in sorted(os.listdir(d)):
             if name.startswith(kernel) and name.endswith(".txt"):
                 with open(os.path.join(d, name)) as fh:
                     for line in fh:
-                        if line.startswith("traffic_bytes_per_launch:"):
+                        if line.startswith("traffic_bytes_per_C_element:"):
                             return float(line.split(":", 1)[1])
     except OSError:
         pass
@@ -330,16 +332,17 @@ def run_ours(args, rank, ws, dist):
     # roofline of the dominant kernel of the mixed solve, the tcgen05 3xTF32
     # trailing update: algorithmic flops (2 m n k per launch) over its summed
     # per-launch device time in the timed region
-    tc_launches, tc_ms, tc_flops = ktime["mixed"]
+    tc_launches, tc_ms, tc_flops, tc_elems = ktime["mixed"]
     tc_tflops = tc_flops / (tc_ms * 1e-3) / 1e12 if tc_ms > 0 else 0.0
     peak_tc, peak_src = measured_peak("bf16_tflops", 1590.0)
-    traffic = profile_traffic("k_tc_gemm_sub")
+    per_elem = profile_traffic("k_tc_gemm_sub")   # DRAM bytes per updated C element, from ncu
+    traffic = per_elem * tc_elems / tc_launches if (per_elem and tc_launches) else None
     # FP64 pipe roofline of the assembly: ops pinned by the oracle's operation
     # counter (248 per quad-ring interaction, 290 per horseshoe) / device time
     peak64 = cap.measure_fma_peak(device, True)
     ops = 248.0 * N * N + 290.0 * 2 * w.nsheddings * N
     achieved = ops / (stg_d[0] * 1e-3) / 1e12
-    d_launches, d_ms, d_flops = ktime["fp64"]
+    d_launches, d_ms, d_flops, _ = ktime["fp64"]
     batched = batch_throughput(fp, device) if not args.no_batch else None
     cpu = None
     if not args.no_cpu_baseline:

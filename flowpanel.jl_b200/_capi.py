@@ -98,7 +98,7 @@ def lib():
         L.fp_batch_solve.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_int64, C.POINTER(BodyDesc),
                                      C.POINTER(SolveOpts), C.POINTER(Stats)]
         L.fp_kernel_timing.argtypes = [vp, C.c_int]
-        L.fp_kernel_timing_read.argtypes = [vp, C.POINTER(C.c_int64), _dp, _dp]
+        L.fp_kernel_timing_read.argtypes = [vp, C.POINTER(C.c_int64), _dp, _dp, _dp]
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
         L.fp_measure_fma_peak.argtypes = [C.c_int, C.c_int, _dp]
         L.fp_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -263,9 +263,9 @@ class Context:
         self._chk(self._L.fp_kernel_timing(self.h, 1 if enable else 0))
 
     def kernel_timing_read(self):
-        n, ms, fl = C.c_int64(), C.c_double(), C.c_double()
-        self._chk(self._L.fp_kernel_timing_read(self.h, C.byref(n), C.byref(ms), C.byref(fl)))
-        return n.value, ms.value, fl.value
+        n, ms, fl, el = C.c_int64(), C.c_double(), C.c_double(), C.c_double()
+        self._chk(self._L.fp_kernel_timing_read(self.h, C.byref(n), C.byref(ms), C.byref(fl), C.byref(el)))
+        return n.value, ms.value, fl.value, el.value
 
     def kernel_launches(self):
         n = C.c_int64()

@@ -899,14 +899,17 @@ int fp_kernel_timing(fp_ctx* c, int enable) {
   t.launches = 0;
   t.ms = 0;
   t.flops = 0;
+  t.units = 0;
+  t.elems.clear();
   return FP_OK;
 }
 
-int fp_kernel_timing_read(fp_ctx* c, int64_t* launches, double* ms, double* flops) {
+int fp_kernel_timing_read(fp_ctx* c, int64_t* launches, double* ms, double* flops, double* elems) {
   if (check_ctx(c)) return FP_EINVAL;
   if (launches) *launches = c->ktimer.launches;
   if (ms) *ms = c->ktimer.ms;
   if (flops) *flops = c->ktimer.flops;
+  if (elems) *elems = c->ktimer.units;
   return FP_OK;
 }
 

@@ -24,8 +24,9 @@ struct KernelTimer {
   std::vector<cudaEvent_t> pool;   // pairs (start, stop), reused
   size_t used = 0;                 // events recorded since the last collect
   std::vector<double> work;        // algorithmic flops of each timed launch
+  std::vector<double> elems;       // output elements (m x n) of each timed launch
   int64_t launches = 0;
-  double ms = 0, flops = 0;
+  double ms = 0, flops = 0, units = 0;
 };
 
 struct fp_ctx {
@@ -208,10 +209,11 @@ inline int kt_begin(fp_ctx* c) {
   t.used += 2;
   return slot;
 }
-inline void kt_end(fp_ctx* c, int slot, double flops) {
+inline void kt_end(fp_ctx* c, int slot, double flops, double elems) {
   if (slot < 0) return;
   cudaEventRecord(c->ktimer.pool[slot + 1], c->stream);
   c->ktimer.work.push_back(flops);
+  c->ktimer.elems.push_back(elems);
 }
 inline void kt_collect(fp_ctx* c) {
   KernelTimer& t = c->ktimer;
@@ -219,9 +221,11 @@ inline void kt_collect(fp_ctx* c) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, t.pool[s], t.pool[s + 1]) == cudaSuccess) t.ms += ms;
     t.flops += t.work[s / 2];
+    t.units += t.elems[s / 2];
     ++t.launches;
   }
   t.used = 0;
   t.work.clear();
+  t.elems.clear();
 }
 }  // namespace fpb

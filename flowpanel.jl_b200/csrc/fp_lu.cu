@@ -658,7 +658,7 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
     const bool pre = ((reinterpret_cast<uintptr_t>(Cm) | (uintptr_t)(lda * sizeof(T))) & 15) == 0;
     const int slot = kt_begin(c);
     k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk, pre);
-    kt_end(c, slot, 2.0 * (double)m * (double)nn * (double)kk);
+    kt_end(c, slot, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
     ++c->nlaunch;
   }
   FP_CUDA_TRY(c->err, cudaGetLastError());

@@ -337,7 +337,7 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
   const int ev = kt_begin(c);
   tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, C, lda, (int)m,
                                                                        (int)nn, kk, c->d_status);
-  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk);
+  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;
 }

@@ -234,10 +234,11 @@ int fp_uind_vjp(fp_ctx* ctx, const double* strengths, const double* targets, int
  * factors), for a roofline; no counterpart in the reference. enable != 0
  * turns it on and clears the sums; every later fp_factor records CUDA events
  * on the context's stream around each such launch and adds, after the factor
- * completes, the number of launches, their device time (ms) and their
- * algorithmic flops (2 m n k each). */
+ * completes, the number of launches, their device time (ms), their
+ * algorithmic flops (2 m n k each) and the output elements they update (m n
+ * each). */
 int fp_kernel_timing(fp_ctx* ctx, int enable);
-int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* flops);
+int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* flops, double* elems);
 
 /* Time of the last kernel launches, for the benchmark's roofline: the device
  * time (ms) of the named stage's dominant kernel and its launch count. */
