@@ -8,8 +8,10 @@
 // Data flow per 128 x 128 output tile (one CTA, 4 warps):
 //   * split kernels write Ah, Al (K-major copies of the L21 panel) and Bh, Bl
 //     (K-major copies of the U12 panel) to scratch in HBM;
-//   * warp 0 / lane 0 streams 32-wide K blocks of the four operands into a
-//     3-stage shared-memory ring with TMA (SWIZZLE_128B, no multicast);
+//   * warp 0 / lane 0 streams 16-wide K blocks of the four operands into a
+//     3-stage shared-memory ring with TMA (SWIZZLE_64B, no multicast); the
+//     ring (96 KB) leaves room for a second CTA on the SM, whose epilogue
+//     overlaps this one's MMAs;
 //   * warp 1 / lane 0 issues 3 x 4 tcgen05.mma (M=128, N=128, K=8) per K block
 //     into a 128-column TMEM accumulator and frees each stage with
 //     tcgen05.commit;
@@ -27,9 +29,9 @@
 namespace fpb {
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 128;
-constexpr int TILE_A = BM * BK * 4;                 // 16 KB
-constexpr int TILE_B = BN * BK * 4;                 // 16 KB
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 128;
+constexpr int TILE_A = BM * BK * 4;                 // 8 KB
+constexpr int TILE_B = BN * BK * 4;                 // 8 KB
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr uint32_t TMEM_COLS = 128;
@@ -73,14 +75,19 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* tm, in
       "l"(reinterpret_cast<uint64_t>(tm)), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
-// K-major, SWIZZLE_128B shared-memory matrix descriptor (tile base 1024-B aligned):
-// start address >> 4, LBO 16 B (unused), SBO 1024 B (8 rows x 128 B), version 1.
+// K-major shared-memory matrix descriptor for BK-float (BK * 4-byte) rows
+// with the matching swizzle (tile base 1024-B aligned): start address >> 4,
+// LBO 16 B (unused), SBO = one 8-row swizzle atom (8 x BK * 4 bytes),
+// version 1, layout 64B swizzle (4) for 64-byte rows, 128B swizzle (2) for
+// 128-byte rows.
+constexpr uint32_t ROW_BYTES = BK * 4;
+constexpr uint32_t SWZ_LAYOUT = ROW_BYTES == 64 ? 4u : 2u;
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
   uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
   d |= (uint64_t)1u << 16;
-  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)((8u * ROW_BYTES) >> 4) << 32;
   d |= (uint64_t)1u << 46;
-  d |= (uint64_t)2u << 61;
+  d |= (uint64_t)SWZ_LAYOUT << 61;
   return d;
 }
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
@@ -96,7 +103,7 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                : "memory");
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
               float* __restrict__ C, int64_t ldc, int m, int n, int K, int* __restrict__ status) {
@@ -282,7 +289,8 @@ static EncodeTiledFn encode_fn() {
 }
 
 // 2-D fp32 map over a K-major matrix: inner dim K (extent kext, row pitch ldk
-// floats), outer dim rows; box 32 x box_rows, 128-byte swizzle, zero fill.
+// floats), outer dim rows; box BK x box_rows, swizzle of BK * 4-byte rows,
+// zero fill.
 static bool make_map(CUtensorMap* tm, const float* base, int kext, int64_t rows, int ldk, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
@@ -291,7 +299,8 @@ static bool make_map(CUtensorMap* tm, const float* base, int kext, int64_t rows,
   cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
   cuuint32_t es[2] = {1, 1};
   return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, ROW_BYTES == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
