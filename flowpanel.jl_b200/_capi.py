@@ -26,7 +26,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
-           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve")
+           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read")
 
 
 class SolveOpts(C.Structure):
@@ -97,6 +97,9 @@ def lib():
         L.fp_batch_last_error.restype = C.c_char_p
         L.fp_batch_solve.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_int64, C.POINTER(BodyDesc),
                                      C.POINTER(SolveOpts), C.POINTER(Stats)]
+        L.fp_trace.argtypes = [vp, C.c_int]
+        L.fp_trace_read.argtypes = [vp, C.c_int64, _ip, _ip, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_int64)]
         L.fp_kernel_timing.argtypes = [vp, C.c_int]
         L.fp_kernel_timing_read.argtypes = [vp, C.POINTER(C.c_int64), _dp, _dp, _dp]
         L.fp_last_kernel_ms.argtypes = [vp, C.c_int, _dp, C.POINTER(C.c_int)]
@@ -257,6 +260,21 @@ class Context:
         factors of the last ``factor(FP_PREC_FP64)``; the library allocates
         no device memory for it."""
         self._chk(self._L.fp_lu_solve_noalloc(self.h, C.c_void_p(dev_ptr), ldb, k))
+
+    def trace(self, enable=True):
+        """Record a timeline of the next factorisations (fp_trace)."""
+        self._chk(self._L.fp_trace(self.h, 1 if enable else 0))
+
+    def trace_read(self):
+        """(tags, streams, t0_ms, t1_ms) of the last traced factorisation."""
+        n = C.c_int64()
+        self._chk(self._L.fp_trace_read(self.h, 0, None, None, None, None, C.byref(n)))
+        k = n.value
+        tags, streams = np.zeros(k, np.int32), np.zeros(k, np.int32)
+        t0, t1 = np.zeros(k, np.float32), np.zeros(k, np.float32)
+        self._chk(self._L.fp_trace_read(self.h, k, _i(tags), _i(streams), t0.ctypes.data_as(C.POINTER(C.c_float)),
+                                        t1.ctypes.data_as(C.POINTER(C.c_float)), C.byref(n)))
+        return tags, streams, t0, t1
 
     def kernel_timing(self, enable=True):
         """Per-launch event timing of the factorisation's trailing update."""

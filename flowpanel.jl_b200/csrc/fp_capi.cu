@@ -169,6 +169,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->ktimer.pool) cudaEventDestroy(e);
+  for (cudaEvent_t e : c->trace.pool) cudaEventDestroy(e);
   if (c->ev_panel) cudaEventDestroy(c->ev_panel);
   if (c->ev_rest) cudaEventDestroy(c->ev_rest);
   if (c->stream2) cudaStreamDestroy(c->stream2);
@@ -458,6 +459,7 @@ int fp_factor(fp_ctx* c, int precision) {
   if (rc) return rc;
   if (time_end(c, &c->ms_factor)) return FP_ECUDA;
   kt_collect(c);
+  tr_collect(c);
   c->kms[FP_STAGE_FACTOR] = c->ms_factor;
   if ((rc = consume_status(c))) return rc;
   float cert = 0.f;
@@ -910,6 +912,28 @@ int fp_kernel_timing_read(fp_ctx* c, int64_t* launches, double* ms, double* flop
   if (ms) *ms = c->ktimer.ms;
   if (flops) *flops = c->ktimer.flops;
   if (elems) *elems = c->ktimer.units;
+  return FP_OK;
+}
+
+int fp_trace(fp_ctx* c, int enable) {
+  if (check_ctx(c)) return FP_EINVAL;
+  c->trace.on = enable != 0;
+  c->trace.recs.clear();
+  c->trace.used = 0;
+  c->trace.base = -1;
+  return FP_OK;
+}
+
+int fp_trace_read(fp_ctx* c, int64_t cap, int* tags, int* streams, float* t0, float* t1, int64_t* count) {
+  if (check_ctx(c) || !count) return FP_EINVAL;
+  const Trace& t = c->trace;
+  *count = (int64_t)t.t0.size();
+  for (int64_t i = 0; i < std::min<int64_t>(cap, *count); ++i) {
+    if (tags) tags[i] = t.tags[i];
+    if (streams) streams[i] = t.streams[i];
+    if (t0) t0[i] = t.t0[i];
+    if (t1) t1[i] = t.t1[i];
+  }
   return FP_OK;
 }
 

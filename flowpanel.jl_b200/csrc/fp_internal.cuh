@@ -29,6 +29,20 @@ struct KernelTimer {
   double ms = 0, flops = 0, units = 0;
 };
 
+// Opt-in timeline of the factorisation: CUDA events around every launch of
+// lu_factor on either stream, tagged by kernel; times relative to a base event
+// at the start of the factorisation (fp_trace / fp_trace_read).
+struct TraceRec { int tag, stream, slot; };
+struct Trace {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  std::vector<TraceRec> recs;
+  size_t used = 0;
+  int base = -1;
+  std::vector<float> t0, t1;   // collected, ms from the base event
+  std::vector<int> tags, streams;
+};
+
 struct fp_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -114,6 +128,7 @@ struct fp_ctx {
   fp_stats last{};
   int64_t nlaunch = 0;          // kernels launched by this context
   KernelTimer ktimer;           // trailing-update launches of fp_factor
+  Trace trace;                  // timeline of fp_factor (off by default)
   bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
   // split operands (Ah, Al, Bh, Bl) of the tensor-core update, one set per
   // stream of the look-ahead factorisation (slot 0: c->stream, 1: stream2)
@@ -227,5 +242,46 @@ inline void kt_collect(fp_ctx* c) {
   t.used = 0;
   t.work.clear();
   t.elems.clear();
+}
+
+// Trace: tr_event records one event on the current stream and returns its
+// slot (-1 when tracing is off); TraceScope brackets one launch.
+enum TraceTag { TR_DIAG = 0, TR_L21, TR_U12, TR_STRIP, TR_GEMM_TC, TR_SPLIT_A, TR_SPLIT_B, TR_GEMM_SIMT };
+inline int tr_event(fp_ctx* c) {
+  Trace& t = c->trace;
+  if (!t.on) return -1;
+  if (t.pool.size() < t.used + 1) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    t.pool.push_back(e);
+  }
+  const int s = (int)t.used++;
+  cudaEventRecord(t.pool[s], c->stream);
+  return s;
+}
+struct TraceScope {
+  fp_ctx* c;
+  int tag, s;
+  TraceScope(fp_ctx* c_, int tag_) : c(c_), tag(tag_), s(tr_event(c_)) {}
+  ~TraceScope() {
+    if (s < 0) return;
+    const int e = tr_event(c);
+    if (e < 0) return;
+    c->trace.recs.push_back(TraceRec{tag, c->stream == c->stream2 ? 1 : 0, s});
+  }
+};
+inline void tr_collect(fp_ctx* c) {
+  Trace& t = c->trace;
+  t.t0.clear(); t.t1.clear(); t.tags.clear(); t.streams.clear();
+  if (!t.on || t.base < 0) return;
+  for (const TraceRec& r : t.recs) {
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, t.pool[t.base], t.pool[r.slot]);
+    cudaEventElapsedTime(&b, t.pool[t.base], t.pool[r.slot + 1]);
+    t.t0.push_back(a); t.t1.push_back(b); t.tags.push_back(r.tag); t.streams.push_back(r.stream);
+  }
+  t.recs.clear();
+  t.used = 0;
+  t.base = -1;
 }
 }  // namespace fpb

@@ -657,6 +657,7 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
     dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
     const bool pre = ((reinterpret_cast<uintptr_t>(Cm) | (uintptr_t)(lda * sizeof(T))) & 15) == 0;
     const int slot = kt_begin(c);
+    TraceScope tr(c, TR_GEMM_SIMT);
     k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk, pre);
     kt_end(c, slot, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
     ++c->nlaunch;
@@ -727,6 +728,7 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     const int64_t cols = (cl1 - cl0) + (cr1 - cr0);
     if (cols <= 0) return FP_OK;
     const unsigned g = (unsigned)((cols + kApplyThreads - 1) / kApplyThreads);
+    TraceScope tr(c, TR_U12);
     k_u12<T><<<g, kApplyThreads, u12_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, cl0, cl1, cr0, cr1, mode);
     ++c->nlaunch;
     FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -738,11 +740,13 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
   auto strip = [&](int64_t K0, int w, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1) -> int {
     const int64_t g = (cl1 - cl0 + kStripCols - 1) / kStripCols + (cr1 - cr0 + kStripCols - 1) / kStripCols;
     if (g <= 0) return FP_OK;
+    TraceScope tr(c, TR_STRIP);
     k_strip<T><<<(unsigned)g, kStripThreads, strip_smem<T>(), c->stream>>>(A, lda, K0, w, ipiv, cl0, cl1, cr0, cr1);
     ++c->nlaunch;
     FP_CUDA_TRY(c->err, cudaGetLastError());
     return FP_OK;
   };
+  c->trace.base = tr_event(c);
   // stream2 starts after everything already queued on c->stream
   FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream2, c->ev_rest, 0));
@@ -753,11 +757,15 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     for (int64_t k = K0; k < kend; k += NB) {
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
-      k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status);
+      {
+        TraceScope tr(c, TR_DIAG);
+        k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status);
+      }
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
       if (below > 0) {
         const unsigned g = (unsigned)((below + kApplyThreads - 1) / kApplyThreads);
+        TraceScope tr(c, TR_L21);
         k_l21<T><<<g, kApplyThreads, 0, c->stream>>>(A, lda, n, k, cert);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());

@@ -16,8 +16,11 @@
 //     into a 128-column TMEM accumulator and frees each stage with
 //     tcgen05.commit;
 //   * all four warps read the accumulator back with tcgen05.ld (warp w owns
-//     TMEM lanes 32w..32w+31 = tile rows) and apply C -= D with coalesced
-//     column accesses.
+//     TMEM lanes 32w..32w+31 = tile rows), stage -D in the drained ring and
+//     add it to C with one TMA reduce-add per warp (cp.reduce.async.bulk.tensor
+//     .add), so no C value passes through registers and the kernel keeps few
+//     registers: a panel kernel of the factorisation fits beside two of these
+//     CTAs on an SM.
 // Every mbarrier wait is bounded; on a timeout the kernel records DEV_TIMEOUT,
 // drains its own copies, frees TMEM and returns.
 #include <cuda.h>
@@ -90,6 +93,13 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
   d |= (uint64_t)SWZ_LAYOUT << 61;
   return d;
 }
+// C[y.., x..] += box at src (fp32 add in L2), tracked by the bulk group
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* tm, const void* src, int x, int y) {
+  asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(tm)),
+               "r"(smem_u32(src)), "r"(x), "r"(y)
+               : "memory");
+}
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -106,7 +116,7 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 __global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
-              float* __restrict__ C, int64_t ldc, int m, int n, int K, int* __restrict__ status) {
+              const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -134,16 +144,6 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-
-  // Prefetch this thread's row of the C tile (warp w owns rows 32w..32w+31):
-  // the loads are in flight while the operands stream in and the MMAs run.
-  const int row = m0 + warp * 32 + lane;
-  const bool row_ok = row < m;
-  const int ncol = min(BN, n - n0);
-  constexpr int HALF = BN / 2;
-  float cv[HALF];
-#pragma unroll
-  for (int j = 0; j < HALF; ++j) cv[j] = (row_ok && j < ncol) ? C[(int64_t)(n0 + j) * ldc + row] : 0.f;
 
   if (warp == 0 && lane == 0) {
     // producer
@@ -187,39 +187,35 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     if (ok) umma_commit(done);
   }
   __syncwarp();
-  // epilogue: every warp waits for the accumulator, subtracts it from its rows
+  // epilogue: every warp waits for the accumulator, stages -D for its 32 rows
+  // column by column ([column][row], 32 rows = 128 B per column) in the ring,
+  // whose operands the MMAs have all consumed, and adds it to C with TMA
   const bool ok = mbar_wait(done, 0);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
+    float* stg = reinterpret_cast<float*>(smem) + warp * 32 * BN;
 #pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1) {
-        // second half: its loads overlap the first half's stores
+    for (int cc = 0; cc < BN; cc += 32) {
+      uint32_t r[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < HALF; ++j)
-          cv[j] = (row_ok && HALF + j < ncol) ? C[(int64_t)(n0 + HALF + j) * ldc + row] : 0.f;
-      }
-#pragma unroll
-      for (int cc = 0; cc < HALF; cc += 32) {
-        uint32_t r[32];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * HALF + cc);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-            "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 32; ++j) cv[cc + j] -= __uint_as_float(r[j]);
-      }
-      if (row_ok) {
-#pragma unroll
-        for (int j = 0; j < HALF; ++j)
-          if (h * HALF + j < ncol) C[(int64_t)(n0 + h * HALF + j) * ldc + row] = cv[j];
-      }
+      for (int j = 0; j < 32; ++j) stg[(cc + j) * 32 + lane] = -__uint_as_float(r[j]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0 && m0 + warp * 32 < m) {
+      tma_reduce_add_2d(&tmC, stg, m0 + warp * 32, n0);
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
   } else if (threadIdx.x == 0) {
     atomicOr(status, (int)DEV_TIMEOUT);
@@ -304,6 +300,21 @@ static bool make_map(CUtensorMap* tm, const float* base, int kext, int64_t rows,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2-D fp32 map over the column-major block C (m rows x n columns, column
+// pitch ldc floats) for the epilogue's reduce-add: inner dim the rows, box
+// 32 rows x BN columns, no swizzle.
+static bool make_map_c(CUtensorMap* tm, float* C, int64_t m, int64_t n, int64_t ldc) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)n};
+  cuuint64_t strides[1] = {(cuuint64_t)ldc * 4};
+  cuuint32_t box[2] = {32u, (cuuint32_t)BN};
+  cuuint32_t es[2] = {1, 1};
+  return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace tc
 
 // Scratch for the split operands: 4 x N x 256 floats.
@@ -324,6 +335,8 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
                      int64_t nn, int kk) {
   if (!c->use_tc || kk <= 0 || kk > 256 || m <= 0 || nn <= 0) return false;
   if (!tc::encode_fn()) return false;
+  // the reduce-add needs a 16-byte aligned C and column pitch
+  if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(lda * 4)) & 15) != 0) return false;
   static SmemAttr attr;
   if (attr.ensure(tc::k_tc_gemm_sub, tc::SMEM_BYTES) != cudaSuccess) return false;
   const int slot = c->tc_slot;
@@ -332,20 +345,28 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
   float *Ah = c->d_tc[slot][0], *Al = c->d_tc[slot][1], *Bh = c->d_tc[slot][2], *Bl = c->d_tc[slot][3];
   {
     dim3 g((unsigned)((m + 31) / 32), (unsigned)((ldk + 31) / 32));
-    tc::k_split_A<<<g, dim3(32, 8), 0, c->stream>>>(A, lda, (int)m, kk, ldk, Ah, Al);
+    {
+      TraceScope tr(c, TR_SPLIT_A);
+      tc::k_split_A<<<g, dim3(32, 8), 0, c->stream>>>(A, lda, (int)m, kk, ldk, Ah, Al);
+    }
     ++c->nlaunch;
     const int64_t t = (int64_t)ldk * nn;
-    tc::k_split_B<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(B, lda, kk, (int)nn, ldk, Bh, Bl);
+    {
+      TraceScope tr(c, TR_SPLIT_B);
+      tc::k_split_B<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(B, lda, kk, (int)nn, ldk, Bh, Bl);
+    }
     ++c->nlaunch;
   }
-  CUtensorMap mAh, mAl, mBh, mBl;
+  CUtensorMap mAh, mAl, mBh, mBl, mC;
   if (!tc::make_map(&mAh, Ah, kk, m, ldk, tc::BM) || !tc::make_map(&mAl, Al, kk, m, ldk, tc::BM) ||
-      !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN))
+      !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN) ||
+      !tc::make_map_c(&mC, C, m, nn, lda))
     return false;
   dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
   const int ev = kt_begin(c);
-  tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, C, lda, (int)m,
-                                                                       (int)nn, kk, c->d_status);
+  TraceScope tr(c, TR_GEMM_TC);
+  tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk,
+                                                                       c->d_status);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;
