@@ -104,7 +104,7 @@ void free_matrices(fp_ctx* c) {
   dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
   dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_part);
   dfree(c->d_dinv128_64); dfree(c->d_dinv128_32);
-  if (c->d_linv) { cudaFree(c->d_linv); c->d_linv = nullptr; }
+  if (c->d_minv) { cudaFree(c->d_minv); c->d_minv = nullptr; }
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
   dfree(c->d_V); dfree(c->d_h);
   dfree(c->d_ab); dfree(c->d_ax); dfree(c->d_ar); dfree(c->d_aw32); dfree(c->d_anorms);
@@ -150,7 +150,8 @@ int fp_ctx_create(int device, fp_ctx** out) {
       cudaEventCreateWithFlags(&c->ev_rest, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaMalloc(&c->d_status, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_cert, sizeof(float)) != cudaSuccess ||
-      cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&c->d_ticket, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess || cudaMemset(c->d_ticket, 0, sizeof(unsigned)) != cudaSuccess) {
     delete c;
     return FP_ECUDA;
   }
@@ -165,7 +166,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->stream2) cudaStreamSynchronize(c->stream2);
   free_matrices(c);
   dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt); dfree(c->d_wake);
-  dfree(c->d_status); dfree(c->d_cert);
+  dfree(c->d_status); dfree(c->d_cert); dfree(c->d_ticket);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->ktimer.pool) cudaEventDestroy(e);
@@ -419,7 +420,7 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
   if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, N * sizeof(int32_t)));
   if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * N * sizeof(double)));
-  if (!c->d_linv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_linv, (size_t)2 * kLuNB * kLuNB * sizeof(double)));
+  if (!c->d_minv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_minv, kMinvBytes + (size_t)kPanelSlots * kLuNB * sizeof(int)));
   if (precision == FP_PREC_FP64) {
     if (!c->d_LU) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_LU, elems * sizeof(double)));
     if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));

@@ -87,12 +87,13 @@ struct fp_ctx {
   int* d_status = nullptr;              // device status word(s)
   unsigned int* d_flags = nullptr;      // triangular-solve flags
   float* d_cert = nullptr;              // max |L| certificate
+  unsigned* d_ticket = nullptr;         // ticket of the factorisation's block launches (zero between launches)
   double* d_dinv64 = nullptr;           // inverses of the FP64 diagonal blocks
   float* d_dinv32 = nullptr;            // inverses of the FP32 diagonal blocks
   double* d_dinv128_64 = nullptr;       // inverses of the 128-row diagonal blocks (FP64 factors)
   float* d_dinv128_32 = nullptr;        // inverses of the 128-row diagonal blocks (FP32 factors)
   double* d_part = nullptr;             // GEMV partial sums
-  void* d_linv = nullptr;               // inv(L11), inv(U11) of the current block (2 x NB x NB, FP64 size)
+  void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)
   double* d_norms = nullptr;            // column norms (2 x cap_rhs)
   int64_t cap_rhs = 0;                  // allocated RHS columns
   size_t cap_flags = 0;
@@ -168,6 +169,8 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda);
 int lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k);
 int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out);
 constexpr int kLuNB = 64;        // block size of the factorisation and the solves
+constexpr int kPanelSlots = 4;   // blocks per outer panel of the factorisation
+constexpr size_t kMinvBytes = (size_t)kPanelSlots * kLuNB * kLuNB * sizeof(double);
 // split-operand scratch of the tensor-core update for scratch set `slot` (fp_tc.cu)
 int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max);
 constexpr int kGemvSplitHost = 16;
@@ -246,7 +249,7 @@ inline void kt_collect(fp_ctx* c) {
 
 // Trace: tr_event records one event on the current stream and returns its
 // slot (-1 when tracing is off); TraceScope brackets one launch.
-enum TraceTag { TR_DIAG = 0, TR_L21, TR_U12, TR_STRIP, TR_GEMM_TC, TR_SPLIT_A, TR_SPLIT_B, TR_GEMM_SIMT };
+enum TraceTag { TR_DIAG = 0, TR_L21 /* k_blk */, TR_U12 /* k_pfix */, TR_STRIP, TR_GEMM_TC, TR_SPLIT_A, TR_SPLIT_B, TR_GEMM_SIMT };
 inline int tr_event(fp_ctx* c) {
   Trace& t = c->trace;
   if (!t.on) return -1;

@@ -8,11 +8,15 @@
 // (src/FLOWPanel_linearsolver.jl:173-234). The wing AICs of this path need
 // only adjacent-row swaps at the trailing edge, which the block search finds.
 //
-// Per block step: (1) k_panel: every CTA factors the diagonal block
-// redundantly in shared memory, CTA 0 writes it back, each CTA solves its own
-// slab of L21 rows; (2) k_swap_u12: row swaps on the other columns and
-// U12 = L11^-1 A12; (3) the trailing update A22 -= L21 U12 (SIMT FP64 GEMM,
-// or the 3xTF32 tcgen05 kernel of fp_tc.cu for the FP32 factors).
+// Per 64-block step: (1) k_diag factors the diagonal block (one CTA) and
+// forms M' = L11^-1 P11; (2) k_blk forms L21, and the update of the panel's
+// own columns as (L21 M') A12 with A12 as it lies, and, in its last CTA among
+// those holding the next block's rows, factors the next diagonal block. After
+// the panel's blocks, (3) k_pfix writes U12 = M' A12 and the row swaps left of
+// each block. Columns outside the panel get the panel's swaps and U12 from
+// k_strip and the trailing update from a GEMM (SIMT FP64, or the 3xTF32
+// tcgen05 kernel of fp_tc.cu for the FP32 factors), on two streams (see
+// lu_factor).
 //
 // Triangular solves run in one persistent kernel per sweep: CTAs take row
 // blocks by ticket (atomic counter), wait (bounded) for the blocks they depend
@@ -86,19 +90,28 @@ template <class T> __host__ __device__ constexpr int rpitch() { return NB + 16 /
 
 // ----------------------------------------------------------------------------
 // (1) k_diag: two warps factor the NB x NB diagonal block with partial
-// pivoting over its rows. Thread t owns row t of the block and keeps it in
-// registers for the whole factorisation (the 64-step loop is unrolled, so
-// every column index is static). Rows never move: a pivot row is marked used
-// and every other unused row eliminates column j with its own multiplier.
-// The pivot is LAPACK's: the largest |a| in column j among the unused rows,
-// the first in the current logical order on ties. Each warp reduces an
-// integer key (the bits of |a| plus one, 0 for used rows; FP64 in two 32-bit
-// halves) with __reduce_max_sync, ties by logical position with
-// __reduce_min_sync; the two warps' candidates meet in shared memory. The
-// winning thread then writes its row once (16-byte stores) and every other
-// row reads it back with broadcast 16-byte loads into its FMAs.
-// LAPACK's ipiv follows from the logical order: at step j, logical rows j and
-// the pivot's position swap.
+// pivoting over its rows. Thread t owns row t of the block and keeps its
+// not yet eliminated part in registers, shifted so that R[0] is always the
+// current column: step j forms R[c] <- R[c + 1] - m * U(j, j + 1 + c) for all
+// c with static indices (zeros enter at the end), so the step loop stays
+// rolled and its body (about 150 instructions) stays in the instruction
+// cache, where a fully unrolled loop spent most of its time waiting for
+// instructions. Rows never move: a pivot row is marked used and every other
+// unused row eliminates column j with its own multiplier. The pivot is
+// LAPACK's: the largest |a| in column j among the unused rows, the first in
+// the current logical order on ties. Each warp reduces an integer key (the
+// bits of |a| plus one, 0 for used rows; FP64 in two 32-bit halves) with
+// __reduce_max_sync, ties by logical position with __reduce_min_sync; the two
+// warps' candidates meet in shared memory. The winning thread writes its
+// shifted row once (16-byte stores) and every other row reads it back with
+// broadcast 16-byte loads into its FMAs. Multipliers and U rows collect in
+// shared memory (S[thread][column]) and go out in logical row order at the
+// end. LAPACK's ipiv follows from the logical order: at step j, logical rows
+// j and the pivot's position swap. Per-step shared buffers alternate between
+// two copies, so one barrier orders each step's reads before the next step's
+// writes. Last, M' = L11^-1 P11 (P11's columns in physical row order) is
+// formed for the block's update, and the row order kept for the panel's
+// fix-up (k_pfix).
 constexpr int kDiagThreads = NB;
 
 __device__ __forceinline__ void bar_diag() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
@@ -118,252 +131,365 @@ template <> struct PivKey<double> {
   }
 };
 
+// shared workspace of diag_factor: prow[2][NB], S / Lsh [NB][RP], pval[2],
+// cand[2][2][4], lpiv[NB], rowat[NB]
+template <class T> __host__ __device__ constexpr int diag_ws_bytes() {
+  return 2 * NB * (int)sizeof(T) + NB * rpitch<T>() * (int)sizeof(T) + 16 + 64 + 2 * NB * 4;
+}
+
+// Threads 0..63 of the calling CTA factor the diagonal block at k (k_diag;
+// k_blk runs it for the next block once that block's rows are final). A is
+// read through L2, so another CTA's stores, ordered before by a fence and an
+// atomic, are seen.
 template <class T>
-__global__ void __launch_bounds__(kDiagThreads)
-k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
-       int* __restrict__ status) {
+__device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int64_t n, int64_t k,
+                                            int32_t* __restrict__ ipiv, int* __restrict__ status,
+                                            T* __restrict__ Minv, int* __restrict__ rowat_out, unsigned char* ws) {
   typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, NCH = NB / V;
-  __shared__ __align__(16) T prow[NB];     // the pivot row of the current step
-  __shared__ unsigned cand[2][4];          // per warp: key hi, key lo, logical pos, thread
-  __shared__ int lpiv[NB];
+  constexpr int V = V16<T>::n, NCH = NB / V, RP = rpitch<T>();
+  T (*prow)[NB] = reinterpret_cast<T (*)[NB]>(ws);   // pivot row of a step, shifted: prow[c] = U(j, j + 1 + c)
+  T* const buf = reinterpret_cast<T*>(ws + 2 * NB * sizeof(T));   // S, then Lsh
+  T* const pval = buf + NB * RP;                                   // the pivot U(j, j)
+  // per step parity and warp: key hi, key lo, logical pos, thread
+  unsigned (*cand)[2][4] = reinterpret_cast<unsigned (*)[2][4]>(reinterpret_cast<unsigned char*>(pval) + 16);
+  int* const lpiv = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(pval) + 16 + 64);
+  int* const rowat = lpiv + NB;
+  // S[t][c]: row t's entry of L (c < its step) or U
+  T (*S)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(buf);
   const int nb = (int)imin64(NB, n - k);
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   T R[NB];
 #pragma unroll
   for (int c = 0; c < NB; ++c)
-    R[c] = (t < nb && c < nb) ? A[(k + c) * lda + (k + t)] : ((t == c) ? T(1) : T(0));
+    R[c] = (t < nb && c < nb) ? __ldcg(&A[(k + c) * lda + (k + t)]) : ((t == c) ? T(1) : T(0));
   bool used = !(t < nb);
   int pos = t;
   bool zero = false;
+#pragma unroll 1
+  for (int j = 0; j < nb; ++j) {
+    const int par = j & 1;
+    unsigned hi, lo;
+    PivKey<T>::of(R[0], used, hi, lo);
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    const bool top = hi == mh && lo == ml;
+    const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
+    if (lane == 0) {
+      cand[par][warp][0] = mh;
+      cand[par][warp][1] = ml;
+      cand[par][warp][2] = pm;
+    }
+    if (top && (unsigned)pos == pm) cand[par][warp][3] = (unsigned)t;
+    bar_diag();
+    const unsigned h0 = cand[par][0][0], l0 = cand[par][0][1], p0 = cand[par][0][2];
+    const unsigned h1 = cand[par][1][0], l1 = cand[par][1][1], p1 = cand[par][1][2];
+    const bool w1 = (h1 > h0) || (h1 == h0 && (l1 > l0 || (l1 == l0 && p1 < p0)));
+    const int pr = (int)cand[par][w1 ? 1 : 0][3];   // pivot row (thread)
+    const int lp = (int)(w1 ? p1 : p0);             // its logical position
+    if (t == pr) {
+      VT* out = reinterpret_cast<VT*>(prow[par]);
 #pragma unroll
-  for (int j = 0; j < NB; ++j) {
-    if (j < nb) {
-      unsigned hi, lo;
-      PivKey<T>::of(R[j], used, hi, lo);
-      const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
-      const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
-      const bool top = hi == mh && lo == ml;
-      const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
-      if (lane == 0) {
-        cand[warp][0] = mh;
-        cand[warp][1] = ml;
-        cand[warp][2] = pm;
-      }
-      if (top && (unsigned)pos == pm) cand[warp][3] = (unsigned)t;
-      bar_diag();
-      const unsigned h0 = cand[0][0], l0 = cand[0][1], p0 = cand[0][2];
-      const unsigned h1 = cand[1][0], l1 = cand[1][1], p1 = cand[1][2];
-      const bool w1 = (h1 > h0) || (h1 == h0 && (l1 > l0 || (l1 == l0 && p1 < p0)));
-      const int pr = (int)cand[w1 ? 1 : 0][3];   // pivot row (thread)
-      const int lp = (int)(w1 ? p1 : p0);        // its logical position
-      if (t == pr) {
-        VT* out = reinterpret_cast<VT*>(prow);
+      for (int q = 0; q < NCH; ++q) {
+        VT v;
 #pragma unroll
-        for (int q = j / V; q < NCH; ++q) {
-          VT v;
-#pragma unroll
-          for (int e = 0; e < V; ++e) vset<T>(v, e, R[q * V + e]);
-          out[q] = v;
+        for (int e = 0; e < V; ++e) {
+          const int c = q * V + e;
+          vset<T>(v, e, c + 1 < NB ? R[c + 1] : T(0));
         }
+        out[q] = v;
       }
-      bar_diag();
-      const T sv = prow[j];
-      if (t == pr) { pos = j; used = true; } else if (pos == j) { pos = lp; }
-      if (t == 0) lpiv[j] = lp;
-      const T rp = (sv != T(0)) ? T(1) / sv : T(0);
-      if (rp == T(0)) {
-        zero = true;
-      } else if (!used) {
-        const T m = R[j] * rp;
-        R[j] = m;
-        const VT* in = reinterpret_cast<const VT*>(prow);
+      pval[par] = R[0];
+    }
+    bar_diag();
+    const T sv = pval[par];
+    if (t == pr) { pos = j; used = true; } else if (pos == j) { pos = lp; }
+    if (t == 0) lpiv[j] = lp;
+    // the pivot's row of U goes to S[pr][j..], one element per thread
+    if (t == 0) S[pr][j] = sv;
+    if (t < NB - 1 - j) S[pr][j + 1 + t] = prow[par][t];
+    const T rp = (sv != T(0)) ? T(1) / sv : T(0);
+    zero |= (rp == T(0));
+    const T m = R[0] * rp;   // 0 on a zero pivot: the row only shifts
+    if (!used) S[t][j] = m;
+    const VT* in = reinterpret_cast<const VT*>(prow[par]);
 #pragma unroll
-        for (int q = j / V; q < NCH; ++q) {
-          const VT pv = in[q];
+    for (int q = 0; q < NCH; ++q) {
+      const VT pv = in[q];
 #pragma unroll
-          for (int e = 0; e < V; ++e) {
-            const int c = q * V + e;
-            if (c > j) R[c] -= m * vget<T>(pv, e);
-          }
-        }
+      for (int e = 0; e < V; ++e) {
+        const int c = q * V + e;
+        R[c] = (c + 1 < NB ? R[c + 1] : T(0)) - m * vget<T>(pv, e);
       }
     }
   }
   if (zero && t == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-  // write back in logical row order: row t goes to position pos
-  if (t < nb) {
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-      if (c < nb) A[(k + c) * lda + (k + pos)] = R[c];
+  if (t < nb) rowat[pos] = t;
+  bar_diag();
+  // write back in logical row order, rows fastest over the threads
+  for (int e = t; e < nb * nb; e += kDiagThreads) {
+    const int s = e % nb, c = e / nb;
+    A[(k + c) * lda + (k + s)] = S[rowat[s]][c];
+  }
+  if (t < nb) ipiv[k + t] = (int32_t)(k + lpiv[t]);
+  rowat_out[t] = (t < nb) ? rowat[t] : t;
+  bar_diag();   // the factors are in A (visible to the CTA); S is free
+  // M' = L11^-1 P11 with P11's columns in physical row order (M' A12 = U12
+  // for A12 as it lies): column r solves L y = e_pos(r), one column per
+  // thread, with L's columns shifted as the factorisation's rows were:
+  // Lsh[j][c] = L(j + 1 + c, j), zero past the end.
+  T (*Lsh)[RP] = reinterpret_cast<T (*)[RP]>(buf);
+  for (int e = t; e < NB * NB; e += kDiagThreads) {
+    const int c = e % NB, j = e / NB;
+    Lsh[j][c] = (j + 1 + c < nb) ? A[(k + j) * lda + (k + j + 1 + c)] : T(0);
   }
   bar_diag();
-  if (t < nb) ipiv[k + t] = (int32_t)(k + lpiv[t]);
+  T y[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) y[c] = (c == pos) ? T(1) : T(0);
+#pragma unroll 1
+  for (int j = 0; j < NB; ++j) {
+    const T yj = y[0];
+    Minv[j * NB + t] = yj;
+    const VT* lrow = reinterpret_cast<const VT*>(&Lsh[j][0]);
+#pragma unroll
+    for (int q = 0; q < NCH; ++q) {
+      const VT lv = lrow[q];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const int c = q * V + e;
+        y[c] = (c + 1 < NB ? y[c + 1] : T(0)) - yj * vget<T>(lv, e);
+      }
+    }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kDiagThreads)
+k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict__ ipiv,
+       int* __restrict__ status, T* __restrict__ Minv, int* __restrict__ rowat_out) {
+  __shared__ __align__(16) unsigned char ws[diag_ws_bytes<T>()];
+  diag_factor<T>(A, lda, n, k, ipiv, status, Minv, rowat_out, ws);
 }
 
 // ----------------------------------------------------------------------------
-// (2) after k_diag, two kernels:
-//  * k_l21: L21 = A21 U11^-1, one row per thread, right-looking
-//    (x_j *= 1/U_jj, then x_l -= x_j U_jl for l > j) with the rows of U11
-//    read as 16-byte vectors from shared memory; the largest |L21| is the
+// (2) k_blk: the rest of a block step in one launch. CTA b owns the rows
+// [k1 + b RT, +RT) below the factored diagonal block (k1 = k + NB):
+//  * L21 = A21 U11^-1 by substitution, one row per thread of warp 0, the row
+//    kept shifted in registers as in k_diag (rolled loop over the 64
+//    columns, 16-byte broadcast reads of the shifted U rows); max|L21| is the
 //    GEPP certificate;
-//  * k_u12: on the columns [cl0, cl1) left of the block and [cr0, cr1)
-//    right of it, the row swaps of the block (mode bit 1) and, on the right
-//    columns, U12 = L11^-1 A12 by forward substitution (mode bit 2; columns
-//    of the unit lower L11 read as 16-byte vectors); one column per thread,
-//    columns staged through shared memory so that global accesses coalesce.
-constexpr int kApplyThreads = 64;
-template <class T> constexpr size_t u12_smem() {
-  return (size_t)NB * rpitch<T>() * sizeof(T) + (size_t)kApplyThreads * (NB + 1) * sizeof(T) +
-         2 * NB * sizeof(int) + 64;
+//  * W = L21 M' with M' = L11^-1 P11 from k_diag;
+//  * C -= W A12 on the panel's columns right of the block, with A12 as it
+//    lies (rows not yet swapped): W A12 = L21 U12, so no CTA needs U12, which
+//    k_pfix writes after the panel, and the CTAs never wait for one another;
+//  * the last of the CTAs owning the next block's rows (ticket) factors the
+//    next diagonal block while the other CTAs still update.
+// The shared memory (27 KB for FP32) lets a CTA run beside two CTAs of the
+// tensor-core update on the same SM.
+constexpr int kBlkRows = 32, kBlkThreads = 128;
+template <class T> __host__ __device__ constexpr int blk_lpitch() { return kBlkRows + 16 / (int)sizeof(T); }
+template <class T> constexpr size_t blk_smem() {
+  return (size_t)NB * rpitch<T>() * sizeof(T) + (size_t)NB * blk_lpitch<T>() * sizeof(T) + NB * sizeof(T) + 64;
+}
+static_assert(blk_smem<float>() >= (size_t)diag_ws_bytes<float>() && blk_smem<double>() >= (size_t)diag_ws_bytes<double>(),
+              "k_blk's shared memory holds diag_factor's workspace");
+
+// acc[i][l] += sum_j P[j][r0 + i] Q[j][c0 + l] over j < NB (both [j][.] in
+// shared memory, 16-byte aligned rows)
+template <class T, int PP, int QP>
+__device__ __forceinline__ void mm4x4(const T (*P)[PP], const T (*Q)[QP], int r0, int c0, T (&acc)[4][4]) {
+  typedef typename V16<T>::type VT;
+  constexpr int V = V16<T>::n;
+#pragma unroll 4
+  for (int j = 0; j < NB; ++j) {
+    T a[4], b[4];
+#pragma unroll
+    for (int h = 0; h < 4 / V; ++h) {
+      const VT va = *reinterpret_cast<const VT*>(&P[j][r0 + h * V]);
+      const VT vb = *reinterpret_cast<const VT*>(&Q[j][c0 + h * V]);
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        a[h * V + e] = vget<T>(va, e);
+        b[h * V + e] = vget<T>(vb, e);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) acc[i][l] += a[i] * b[l];
+  }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kApplyThreads)
-k_l21(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ cert) {
+__global__ void __launch_bounds__(kBlkThreads, sizeof(T) == 4 ? 3 : 2)
+k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const T* __restrict__ Minv,
+      float* __restrict__ cert, int next, int32_t* __restrict__ ipiv, int* __restrict__ status,
+      T* __restrict__ Minv_next, int* __restrict__ rowat_next, unsigned* __restrict__ ticket) {
   typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, RP = rpitch<T>();
-  __shared__ __align__(16) T Ut[NB][RP];   // Ut[j][l] = U(j, l), zero below the diagonal
-  __shared__ T rdiag[NB];
-  __shared__ float red[kApplyThreads / 32];
-  const int nb = (int)imin64(NB, n - k);
+  constexpr int V = V16<T>::n, NCH = NB / V, RP = rpitch<T>(), LP = blk_lpitch<T>();
+  extern __shared__ __align__(16) unsigned char bsm[];
+  T (*Bs)[RP] = reinterpret_cast<T (*)[RP]>(bsm);   // shifted U11 rows, then M', then A12 chunks
+  T (*Ls)[LP] = reinterpret_cast<T (*)[LP]>(bsm + (size_t)NB * RP * sizeof(T));   // L21, then W: [column][row]
+  T* rd = reinterpret_cast<T*>(bsm + (size_t)NB * RP * sizeof(T) + (size_t)NB * LP * sizeof(T));
   const int tid = threadIdx.x;
-  stage_block<kApplyThreads, T>(
-      tid,
-      [&](int jr, int lc) {   // row jr of U, column lc
-        if (jr < nb && lc < nb) return (lc >= jr) ? A[(k + lc) * lda + (k + jr)] : T(0);
-        return (jr == lc) ? T(1) : T(0);
-      },
-      [&](int jr, int lc, T v) { Ut[jr][lc] = v; });
+  const int64_t k1 = k + NB;
+  const int64_t row0 = k1 + (int64_t)blockIdx.x * kBlkRows;
+  const int rows = (int)imin64(kBlkRows, n - row0);
+  // Bs[j][c] = U(j, j + 1 + c), zero past the row's end; rd[j] = 1 / U(j, j)
+  stage_block<kBlkThreads, T>(
+      tid, [&](int j, int l) { return (l >= j) ? A[(k + l) * lda + (k + j)] : T(0); },
+      [&](int j, int l, T v) {
+        if (l == j) rd[j] = T(1) / v;
+        Bs[j][l > j ? l - j - 1 : NB - 1 - j + l] = (l > j) ? v : T(0);
+      });
   __syncthreads();
-  if (tid < NB) rdiag[tid] = T(1) / Ut[tid][tid];
-  __syncthreads();
-  const int64_t row = k + nb + (int64_t)blockIdx.x * kApplyThreads + tid;
-  float lmax = 0.f;
-  if (row < n) {
+  if (tid < kBlkRows) {
     T x[NB];
 #pragma unroll
-    for (int j = 0; j < NB; ++j) x[j] = (j < nb) ? A[(k + j) * lda + row] : T(0);
-#pragma unroll
+    for (int c = 0; c < NB; ++c) x[c] = (tid < rows) ? A[(k + c) * lda + row0 + tid] : T(0);
+    float lmax = 0.f;
+#pragma unroll 1
     for (int j = 0; j < NB; ++j) {
-      // keeps the compiler from hoisting later rows of U (and their
-      // registers) above this step
-      asm volatile("" ::: "memory");
-      const T xj = x[j] * rdiag[j];
-      x[j] = xj;
-      const VT* urow = reinterpret_cast<const VT*>(&Ut[j][0]);
+      const T xj = x[0] * rd[j];
+      Ls[j][tid] = xj;
+      if (tid < rows) A[(k + j) * lda + row0 + tid] = xj;
+      lmax = fmaxf(lmax, (float)tabs(xj));
+      const VT* urow = reinterpret_cast<const VT*>(&Bs[j][0]);
 #pragma unroll
-      for (int q = (j + 1) / V; q < NB / V; ++q) {
+      for (int q = 0; q < NCH; ++q) {
         const VT u = urow[q];
 #pragma unroll
         for (int e = 0; e < V; ++e) {
-          const int lc = q * V + e;
-          if (lc > j) x[lc] -= xj * vget<T>(u, e);
+          const int c = q * V + e;
+          x[c] = (c + 1 < NB ? x[c + 1] : T(0)) - xj * vget<T>(u, e);
         }
       }
     }
-    T* const Ao = opaque_ptr(A);
 #pragma unroll
-    for (int j = 0; j < NB; ++j) {
-      if (j < nb) {
-        Ao[(k + j) * lda + row] = x[j];
-        lmax = fmaxf(lmax, (float)tabs(x[j]));
+    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if (tid == 0 && lmax > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(lmax));
+  }
+  const int64_t nn = kend - k1;
+  if (nn <= 0) return;   // then there is no next block in the panel
+  __syncthreads();
+  // M' -> Bs[j][c]
+  stage_block<kBlkThreads, T>(
+      tid, [&](int c, int j) { return Minv[j * NB + c]; }, [&](int c, int j, T v) { Bs[j][c] = v; });
+  __syncthreads();
+  // thread (rg, cg): rows 4 rg.. of the CTA's 32, columns 4 cg.. of 64
+  const int rg = tid & 7, cg = tid >> 3;
+  {
+    T w[4][4] = {};
+    mm4x4<T, LP, RP>(Ls, Bs, 4 * rg, 4 * cg, w);
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) Ls[4 * cg + l][4 * rg + i] = w[i][l];   // Ls[j][r] = W(r, j)
+  }
+  for (int64_t c0 = 0; c0 < nn; c0 += NB) {
+    const int nc = (int)imin64(NB, nn - c0);
+    __syncthreads();
+    // A12 chunk as it lies: Bs[j][cc] = A(k + j, k1 + c0 + cc)
+    stage_block<kBlkThreads, T>(
+        tid, [&](int j, int cc) { return (cc < nc) ? A[(k1 + c0 + cc) * lda + (k + j)] : T(0); },
+        [&](int j, int cc, T v) { Bs[j][cc] = v; });
+    __syncthreads();
+    T acc[4][4] = {};
+    mm4x4<T, LP, RP>(Ls, Bs, 4 * rg, 4 * cg, acc);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int cc = 4 * cg + l;
+      if (cc >= nc) continue;
+      T* col = A + (k1 + c0 + cc) * lda + row0 + 4 * rg;
+      if (4 * rg + 4 <= rows) {
+#pragma unroll
+        for (int h = 0; h < 4 / V; ++h) {
+          VT v = reinterpret_cast<VT*>(col)[h];
+#pragma unroll
+          for (int e = 0; e < V; ++e) vset<T>(v, e, vget<T>(v, e) - acc[h * V + e][l]);
+          reinterpret_cast<VT*>(col)[h] = v;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (4 * rg + i < rows) col[i] -= acc[i][l];
       }
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-  if ((tid & 31) == 0) red[tid >> 5] = lmax;
+  // The next block's diagonal block (rows and columns k1..k1+63, inside the
+  // panel) is final once the CTAs owning its rows are done: the last of them
+  // (ticket) factors it while the other CTAs still update, so the next
+  // block's step can start as soon as this launch ends.
+  const unsigned owners = (unsigned)imin64(NB / kBlkRows, gridDim.x);
+  if (!next || blockIdx.x >= owners) return;
+  __shared__ unsigned last;
+  __threadfence();   // this CTA's stores, visible device-wide before its ticket
   __syncthreads();
   if (tid == 0) {
-    float mm = red[0];
-    for (int w = 1; w < kApplyThreads / 32; ++w) mm = fmaxf(mm, red[w]);
-    if (mm > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(mm));
+    const unsigned got = atomicAdd(ticket, 1u);
+    last = (got == owners - 1);
+    if (last) {
+      *ticket = 0u;   // every owner has taken its ticket: ready for the next launch
+      __threadfence();
+    }
   }
+  __syncthreads();
+  if (!last || tid >= kDiagThreads) return;
+  diag_factor<T>(A, lda, n, k1, ipiv, status, Minv_next, rowat_next, bsm);
 }
 
+// ----------------------------------------------------------------------------
+// (3) k_pfix: after a panel's blocks, for each block b of the panel, its row
+// swaps on the panel's columns left of it and U12 = M'_b A12 on the columns
+// right of it, in place (nothing reads these parts before: the blocks' own
+// steps use L21 and A12 as they lie). Task t of nblk (nblk - 1): block
+// b = t / (nblk - 1), i = t % (nblk - 1); i < b: left chunk i, else right
+// chunk i - b; 64 columns per task.
+constexpr int kPfixThreads = 256;
+template <class T> constexpr size_t pfix_smem() { return (size_t)2 * NB * rpitch<T>() * sizeof(T) + 64; }
+
 template <class T>
-__global__ void __launch_bounds__(kApplyThreads)
-k_u12(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, const int32_t* __restrict__ ipiv, int64_t cl0,
-      int64_t cl1, int64_t cr0, int64_t cr1, int mode) {
-  typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, RP = rpitch<T>();
-  extern __shared__ __align__(16) unsigned char dsm[];
-  T (*Lc)[RP] = reinterpret_cast<T (*)[RP]>(dsm);                                          // Lc[j][r] = L(r, j)
-  T (*tile)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(dsm + (size_t)NB * RP * sizeof(T));   // tile[col][r]
-  int* perm = reinterpret_cast<int*>(dsm + (size_t)NB * RP * sizeof(T) + (size_t)kApplyThreads * (NB + 1) * sizeof(T));
-  int* lp = perm + NB;
-  const int nb = (int)imin64(NB, n - k);
+__global__ void __launch_bounds__(kPfixThreads)
+k_pfix(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk, const T* __restrict__ Minv,
+       const int* __restrict__ rowat) {
+  constexpr int RP = rpitch<T>();
+  extern __shared__ __align__(16) unsigned char psm[];
+  T (*X)[RP] = reinterpret_cast<T (*)[RP]>(psm);                                 // X[row j][column]
+  T (*Mt)[RP] = reinterpret_cast<T (*)[RP]>(psm + (size_t)NB * RP * sizeof(T));   // Mt[j][r] = M'(r, j)
   const int tid = threadIdx.x;
-  stage_block<kApplyThreads, T>(
-      tid,
-      [&](int r, int j) {   // L(r, j): strictly lower part of the block
-        return (r < nb && j < nb && r > j) ? A[(k + j) * lda + (k + r)] : T(0);
-      },
-      [&](int r, int j, T v) { Lc[j][r] = v; });
-  if (tid < nb) lp[tid] = (int)(ipiv[k + tid] - k);
-  __syncthreads();
-  if (tid == 0) {
-    for (int j = 0; j < NB; ++j) perm[j] = j;
-    if (mode & 1) {
-      for (int j = 0; j < nb; ++j) {
-        const int p = lp[j];
-        const int t0 = perm[j]; perm[j] = perm[p]; perm[p] = t0;
-      }
+  const int b = (int)blockIdx.x / (nblk - 1), i = (int)blockIdx.x % (nblk - 1);
+  const int64_t kb = K0 + (int64_t)b * NB;
+  const int nbb = (int)imin64(NB, kend - kb);
+  const bool left = i < b;
+  const int64_t c0 = left ? K0 + (int64_t)i * NB : kb + NB + (int64_t)(i - b) * NB;
+  const int nc = (int)imin64(NB, (left ? kb : kend) - c0);
+  if (nc <= 0) return;
+  stage_block<kPfixThreads, T>(
+      tid, [&](int j, int cc) { return (j < nbb && cc < nc) ? A[(c0 + cc) * lda + (kb + j)] : T(0); },
+      [&](int j, int cc, T v) { X[j][cc] = v; });
+  if (left) {
+    const int* ra = rowat + b * NB;
+    __syncthreads();
+    for (int e = tid; e < NB * NB; e += kPfixThreads) {
+      const int s = e & (NB - 1), cc = e / NB;
+      if (s < nbb && cc < nc) A[(c0 + cc) * lda + (kb + s)] = X[ra[s]][cc];
     }
+    return;
   }
-  const int64_t nl = cl1 - cl0;
-  const int64_t nother = nl + (cr1 - cr0);
-  const int64_t g = blockIdx.x;   // one group of kApplyThreads columns per CTA
-  static_assert(kApplyThreads == NB, "the column tile is NB x NB");
-  stage_block<kApplyThreads, T>(
-      tid,
-      [&](int r, int cc) {
-        const int64_t qq = g * kApplyThreads + cc;
-        T v = T(0);
-        if (qq < nother && r < nb) {
-          const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
-          v = A[c * lda + k + r];
-        }
-        return v;
-      },
-      [&](int r, int cc, T v) { tile[cc][r] = v; });
+  const T* M = Minv + (size_t)b * NB * NB;
+  stage_block<kPfixThreads, T>(
+      tid, [&](int j, int r) { return M[r * NB + j]; }, [&](int j, int r, T v) { Mt[j][r] = v; });
   __syncthreads();
-  {
-    const int64_t qq = g * kApplyThreads + tid;
-    if (qq < nother) {
-      const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
-      T x[NB];
+  const int rg = tid & 15, cg = tid >> 4;
+  T acc[4][4] = {};
+  mm4x4<T, RP, RP>(Mt, X, 4 * rg, 4 * cg, acc);
 #pragma unroll
-      for (int r = 0; r < NB; ++r) x[r] = tile[tid][perm[r]];
-      if ((mode & 2) && c >= k + nb) {
+  for (int l = 0; l < 4; ++l) {
+    const int cc = 4 * cg + l;
+    if (cc >= nc) continue;
 #pragma unroll
-        for (int j = 0; j < NB; ++j) {
-          const T xj = x[j];
-          const VT* lcol = reinterpret_cast<const VT*>(&Lc[j][0]);
-#pragma unroll
-          for (int q = (j + 1) / V; q < NB / V; ++q) {
-            const VT u = lcol[q];
-#pragma unroll
-            for (int e = 0; e < V; ++e) {
-              const int r = q * V + e;
-              if (r > j) x[r] -= vget<T>(u, e) * xj;
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < NB; ++r) tile[tid][r] = x[r];
-    }
-  }
-  __syncthreads();
-  for (int e = tid; e < NB * kApplyThreads; e += kApplyThreads) {
-    const int r = e & (NB - 1), cc = e >> 6;
-    const int64_t qq = g * kApplyThreads + cc;
-    if (qq < nother && r < nb) {
-      const int64_t c = (qq < nl) ? cl0 + qq : cr0 + (qq - nl);
-      A[c * lda + k + r] = tile[cc][r];
-    }
+    for (int r = 0; r < 4; ++r) A[(c0 + cc) * lda + (kb + 4 * rg + r)] = acc[r][l];
   }
 }
 
@@ -717,23 +843,18 @@ struct OnStream2 {
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
-  static SmemAttr attr_u12;
-  FP_CUDA_TRY(c->err, attr_u12.ensure(k_u12<T>, (int)u12_smem<T>()));
+  static SmemAttr attr_blk, attr_pfix;
+  FP_CUDA_TRY(c->err, attr_blk.ensure(k_blk<T>, (int)blk_smem<T>()));
+  FP_CUDA_TRY(c->err, attr_pfix.ensure(k_pfix<T>, (int)pfix_smem<T>()));
+  // M' and the row order of each block of the current panel
+  static_assert(kOuterNB / NB <= kPanelSlots, "one scratch slot per block of a panel");
+  T* const minv = reinterpret_cast<T*>(c->d_minv);
+  int* const rowat = reinterpret_cast<int*>(reinterpret_cast<char*>(c->d_minv) + kMinvBytes);
   if (sizeof(T) == 4 && c->use_tc) {   // both scratch sets before any concurrent launch
     if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
     if (int rc = ensure_tc_scratch(c, 1, n)) return rc;
   }
   auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
-  auto u12 = [&](int64_t k, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1, int mode) -> int {
-    const int64_t cols = (cl1 - cl0) + (cr1 - cr0);
-    if (cols <= 0) return FP_OK;
-    const unsigned g = (unsigned)((cols + kApplyThreads - 1) / kApplyThreads);
-    TraceScope tr(c, TR_U12);
-    k_u12<T><<<g, kApplyThreads, u12_smem<T>(), c->stream>>>(A, lda, n, k, ipiv, cl0, cl1, cr0, cr1, mode);
-    ++c->nlaunch;
-    FP_CUDA_TRY(c->err, cudaGetLastError());
-    return FP_OK;
-  };
   static_assert(kOuterNB == kStripRows, "a strip holds one outer panel's rows");
   static SmemAttr attr_strip;
   FP_CUDA_TRY(c->err, attr_strip.ensure(k_strip<T>, (int)strip_smem<T>()));
@@ -757,23 +878,32 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     for (int64_t k = K0; k < kend; k += NB) {
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
-      {
+      const int slot = (int)((k - K0) / NB);
+      if (k == K0) {   // later blocks of the panel are factored at the end of the previous k_blk
         TraceScope tr(c, TR_DIAG);
-        k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status);
-      }
-      ++c->nlaunch;
-      FP_CUDA_TRY(c->err, cudaGetLastError());
-      if (below > 0) {
-        const unsigned g = (unsigned)((below + kApplyThreads - 1) / kApplyThreads);
-        TraceScope tr(c, TR_L21);
-        k_l21<T><<<g, kApplyThreads, 0, c->stream>>>(A, lda, n, k, cert);
+        k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, minv + slot * NB * NB,
+                                                     rowat + slot * NB);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
-      const int64_t k1 = k + nb;
-      if (int rc = u12(k, K0, k, k1, kend, 3)) return rc;
-      if (kend > k1)
-        if (int rc = gemm_sub<T>(c, at(k1, k), at(k, k1), at(k1, k1), lda, n - k1, kend - k1, nb)) return rc;
+      if (below > 0) {   // then nb == NB
+        const unsigned g = (unsigned)((below + kBlkRows - 1) / kBlkRows);
+        const int next = k + NB < kend;
+        TraceScope tr(c, TR_L21);
+        k_blk<T><<<g, kBlkThreads, blk_smem<T>(), c->stream>>>(A, lda, n, k, kend, minv + slot * NB * NB, cert, next,
+                                                               ipiv, c->d_status, minv + (slot + 1) * NB * NB,
+                                                               rowat + (slot + 1) * NB, c->d_ticket);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      }
+    }
+    const int nblk = (int)((kend - K0 + NB - 1) / NB);
+    if (nblk > 1) {
+      TraceScope tr(c, TR_U12);
+      k_pfix<T><<<(unsigned)(nblk * (nblk - 1)), kPfixThreads, pfix_smem<T>(), c->stream>>>(A, lda, K0, kend, nblk,
+                                                                                          minv, rowat);
+      ++c->nlaunch;
+      FP_CUDA_TRY(c->err, cudaGetLastError());
     }
     FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_panel, c->stream));
     // (2) the next panel's columns: P's swaps and U12 rows, then their update

@@ -243,8 +243,9 @@ int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* fl
 /* Timeline of the next factorisations (no counterpart in the reference): with
  * enable != 0, every fp_factor records CUDA events around each of its kernel
  * launches on both of its streams; fp_trace_read returns, for the last
- * factorisation, each launch's kernel tag (0 diagonal block, 1 L21, 2 U12,
- * 3 column strip, 4 tensor-core update, 5/6 operand splits, 7 SIMT update),
+ * factorisation, each launch's kernel tag (0 diagonal block, 1 block update,
+ * 2 panel fix-up, 3 column strip, 4 tensor-core update, 5/6 operand splits,
+ * 7 SIMT update),
  * its stream (0 the panel stream, 1 the trailing-update stream) and its start
  * and end in ms from the start of the factorisation; count = launches. */
 int fp_trace(fp_ctx* ctx, int enable);
