@@ -420,7 +420,7 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
   if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, N * sizeof(int32_t)));
   if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * N * sizeof(double)));
-  if (!c->d_minv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_minv, kMinvBytes + (size_t)kPanelSlots * kLuNB * sizeof(int)));
+  if (!c->d_minv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_minv, kMinvBytes + (size_t)2 * kPanelSlots * kLuNB * sizeof(int)));
   if (precision == FP_PREC_FP64) {
     if (!c->d_LU) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_LU, elems * sizeof(double)));
     if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));

@@ -31,7 +31,6 @@
 namespace fpb {
 
 constexpr int NB = 64;          // block size of the factorisation and of the solves
-constexpr int kPanelThreads = 128;
 constexpr int kSpinLimit = 1 << 22;   // bounded waits in the persistent solve
 
 template <class T> __device__ __forceinline__ T tabs(T a) { return a < T(0) ? -a : a; }
@@ -102,9 +101,10 @@ template <class T> __host__ __device__ constexpr int rpitch() { return NB + 16 /
 // the current logical order on ties. Each warp reduces an integer key (the
 // bits of |a| plus one, 0 for used rows; FP64 in two 32-bit halves) with
 // __reduce_max_sync, ties by logical position with __reduce_min_sync; the two
-// warps' candidates meet in shared memory. The winning thread writes its
-// shifted row once (16-byte stores) and every other row reads it back with
-// broadcast 16-byte loads into its FMAs. Multipliers and U rows collect in
+// warps' candidates meet in shared memory. The winning thread writes its row
+// as its registers hold it (aligned 16-byte stores, no register moves) and
+// every other row reads it back with broadcast 16-byte loads, taking element
+// c + 1 into its FMA for column c. Multipliers and U rows collect in
 // shared memory (S[thread][column]) and go out in logical row order at the
 // end. LAPACK's ipiv follows from the logical order: at step j, logical rows
 // j and the pivot's position swap. Per-step shared buffers alternate between
@@ -131,7 +131,7 @@ template <> struct PivKey<double> {
   }
 };
 
-// shared workspace of diag_factor: prow[2][NB], S / Lsh [NB][RP], pval[2],
+// shared workspace of diag_factor: prow[2][NB], S / Lsh [NB][RP], 2 spare,
 // cand[2][2][4], lpiv[NB], rowat[NB]
 template <class T> __host__ __device__ constexpr int diag_ws_bytes() {
   return 2 * NB * (int)sizeof(T) + NB * rpitch<T>() * (int)sizeof(T) + 16 + 64 + 2 * NB * 4;
@@ -147,9 +147,9 @@ __device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int6
                                             T* __restrict__ Minv, int* __restrict__ rowat_out, unsigned char* ws) {
   typedef typename V16<T>::type VT;
   constexpr int V = V16<T>::n, NCH = NB / V, RP = rpitch<T>();
-  T (*prow)[NB] = reinterpret_cast<T (*)[NB]>(ws);   // pivot row of a step, shifted: prow[c] = U(j, j + 1 + c)
+  T (*prow)[NB] = reinterpret_cast<T (*)[NB]>(ws);   // pivot row of a step, as held: prow[c] = U(j, j + c)
   T* const buf = reinterpret_cast<T*>(ws + 2 * NB * sizeof(T));   // S, then Lsh
-  T* const pval = buf + NB * RP;                                   // the pivot U(j, j)
+  T* const pval = buf + NB * RP;                                   // (spare)
   // per step parity and warp: key hi, key lo, logical pos, thread
   unsigned (*cand)[2][4] = reinterpret_cast<unsigned (*)[2][4]>(reinterpret_cast<unsigned char*>(pval) + 16);
   int* const lpiv = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(pval) + 16 + 64);
@@ -171,7 +171,7 @@ __device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int6
     unsigned hi, lo;
     PivKey<T>::of(R[0], used, hi, lo);
     const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
-    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    const unsigned ml = (sizeof(T) == 8) ? __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u) : 0u;
     const bool top = hi == mh && lo == ml;
     const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
     if (lane == 0) {
@@ -186,41 +186,36 @@ __device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int6
     const bool w1 = (h1 > h0) || (h1 == h0 && (l1 > l0 || (l1 == l0 && p1 < p0)));
     const int pr = (int)cand[par][w1 ? 1 : 0][3];   // pivot row (thread)
     const int lp = (int)(w1 ? p1 : p0);             // its logical position
-    if (t == pr) {
+    if (t == pr) {   // the row as it lies in registers: whole 16-byte stores
       VT* out = reinterpret_cast<VT*>(prow[par]);
 #pragma unroll
       for (int q = 0; q < NCH; ++q) {
         VT v;
 #pragma unroll
-        for (int e = 0; e < V; ++e) {
-          const int c = q * V + e;
-          vset<T>(v, e, c + 1 < NB ? R[c + 1] : T(0));
-        }
+        for (int e = 0; e < V; ++e) vset<T>(v, e, R[q * V + e]);
         out[q] = v;
       }
-      pval[par] = R[0];
     }
     bar_diag();
-    const T sv = pval[par];
+    const T sv = prow[par][0];
     if (t == pr) { pos = j; used = true; } else if (pos == j) { pos = lp; }
     if (t == 0) lpiv[j] = lp;
     // the pivot's row of U goes to S[pr][j..], one element per thread
-    if (t == 0) S[pr][j] = sv;
-    if (t < NB - 1 - j) S[pr][j + 1 + t] = prow[par][t];
+    if (t < NB - j) S[pr][j + t] = prow[par][t];
     const T rp = (sv != T(0)) ? T(1) / sv : T(0);
     zero |= (rp == T(0));
     const T m = R[0] * rp;   // 0 on a zero pivot: the row only shifts
     if (!used) S[t][j] = m;
     const VT* in = reinterpret_cast<const VT*>(prow[par]);
+    T pv[NB];
 #pragma unroll
     for (int q = 0; q < NCH; ++q) {
-      const VT pv = in[q];
+      const VT v = in[q];
 #pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const int c = q * V + e;
-        R[c] = (c + 1 < NB ? R[c + 1] : T(0)) - m * vget<T>(pv, e);
-      }
+      for (int e = 0; e < V; ++e) pv[q * V + e] = vget<T>(v, e);
     }
+#pragma unroll
+    for (int c = 0; c < NB; ++c) R[c] = (c + 1 < NB) ? R[c + 1] - m * pv[c + 1] : T(0);
   }
   if (zero && t == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
   if (t < nb) rowat[pos] = t;
@@ -495,144 +490,133 @@ k_pfix(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk, const
 
 // ----------------------------------------------------------------------------
 // (2b) k_strip: a strip of columns outside a factored panel (the panel's w
-// rows, w <= kStripRows, starting at row K0). On the columns [cl0, cl1) it
-// applies the row swaps of all the panel's 64-row blocks; on [cr0, cr1) the
-// swaps and then U12 = L_panel^-1 A12 (L_panel: the panel's unit lower
-// w x w triangle), block by block: forward substitution with the diagonal
-// block's L, then the update of the later row blocks with L's off-diagonal
-// block. One CTA owns 64 columns, all w rows in shared memory, so the strip
-// costs one launch instead of a pass per block and step.
+// rows from K0, w <= kStripRows, in nblk 64-row blocks). On the columns
+// [cl0, cl1) it puts each block's rows in their logical order; on [cr0, cr1)
+// it forms U12 = L_panel^-1 P_panel A12 block by block,
+//     U_b = L_bb^-1 (P_b X_b - sum_{b' < b} L_bb' U_b'),
+// with L_bb^-1 = M'_b P_b^T (M' of k_diag, columns taken in logical order)
+// and L_bb' the panel's L (k_pfix left it in logical row order); each U_b is
+// written in place and read back by the later blocks. Every product is a
+// 64 x 64 x 32 tile product from shared memory with a rolled K loop, so the
+// code stays small. One CTA owns 32 columns.
 constexpr int kStripRows = 256;
-constexpr int kStripCols = 64;
+constexpr int kStripCols = 32;
 constexpr int kStripThreads = 256;
-template <class T> __host__ __device__ constexpr int strip_pitch() { return kStripRows + 16 / (int)sizeof(T); }
+template <class T> __host__ __device__ constexpr int strip_qpitch() { return kStripCols + 16 / (int)sizeof(T); }
 template <class T> constexpr size_t strip_smem() {
-  return (size_t)kStripCols * strip_pitch<T>() * sizeof(T)      // tile[col][row]
-         + (size_t)NB * rpitch<T>() * sizeof(T)                  // Lc[j][r] = L(r, j) of a diagonal block
-         + (size_t)NB * rpitch<T>() * sizeof(T)                  // Lo[j][r] = L(r, j) of an off-diagonal block
-         + (size_t)kStripRows * sizeof(int) + 64;                // row sources
+  return (size_t)NB * rpitch<T>() * sizeof(T) + (size_t)NB * strip_qpitch<T>() * sizeof(T) + 64;
+}
+
+// acc[i][l] += sum_j P[j][r0 + i] Q[j][c0 + l], 4 rows x 2 columns
+template <class T, int PP, int QP>
+__device__ __forceinline__ void mm4x2(const T (*P)[PP], const T (*Q)[QP], int r0, int c0, T (&acc)[4][2]) {
+  typedef typename V16<T>::type VT;
+  constexpr int V = V16<T>::n;
+#pragma unroll 4
+  for (int j = 0; j < NB; ++j) {
+    T a[4];
+#pragma unroll
+    for (int h = 0; h < 4 / V; ++h) {
+      const VT va = *reinterpret_cast<const VT*>(&P[j][r0 + h * V]);
+#pragma unroll
+      for (int e = 0; e < V; ++e) a[h * V + e] = vget<T>(va, e);
+    }
+    const T b0 = Q[j][c0], b1 = Q[j][c0 + 1];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      acc[i][0] += a[i] * b0;
+      acc[i][1] += a[i] * b1;
+    }
+  }
 }
 
 template <class T>
 __global__ void __launch_bounds__(kStripThreads)
-k_strip(T* __restrict__ A, int64_t lda, int64_t K0, int w, const int32_t* __restrict__ ipiv, int64_t cl0,
-        int64_t cl1, int64_t cr0, int64_t cr1) {
-  typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, RP = rpitch<T>(), TP = strip_pitch<T>();
+k_strip(T* __restrict__ A, int64_t lda, int64_t K0, int w, const T* __restrict__ Minv,
+        const int* __restrict__ rowat, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1) {
+  constexpr int RP = rpitch<T>(), QP = strip_qpitch<T>();
   extern __shared__ __align__(16) unsigned char ssm[];
-  T (*tile)[TP] = reinterpret_cast<T (*)[TP]>(ssm);
-  T (*Lc)[RP] = reinterpret_cast<T (*)[RP]>(ssm + (size_t)kStripCols * TP * sizeof(T));
-  T (*Lo)[RP] = reinterpret_cast<T (*)[RP]>(ssm + (size_t)kStripCols * TP * sizeof(T) + (size_t)NB * RP * sizeof(T));
-  int* src = reinterpret_cast<int*>(ssm + (size_t)kStripCols * TP * sizeof(T) + (size_t)2 * NB * RP * sizeof(T));
+  T (*Pt)[RP] = reinterpret_cast<T (*)[RP]>(ssm);                                 // Pt[j][r]
+  T (*Q)[QP] = reinterpret_cast<T (*)[QP]>(ssm + (size_t)NB * RP * sizeof(T));   // Q[j][c]
   const int tid = threadIdx.x;
   const int nblk = (w + NB - 1) / NB;
-  const int64_t nl = cl1 - cl0, nr = cr1 - cr0;
+  const int64_t nl = cl1 - cl0;
   const int64_t gl = (nl + kStripCols - 1) / kStripCols;
   const bool right = (int64_t)blockIdx.x >= gl;
   const int64_t c0 = right ? cr0 + ((int64_t)blockIdx.x - gl) * kStripCols : cl0 + (int64_t)blockIdx.x * kStripCols;
-  const int ncol = (int)imin64(kStripCols, right ? cr1 - c0 : cl1 - c0);
-  // source row of each panel row after the swaps of its block (LAPACK order)
-  if (tid < nblk) {
-    const int b0 = tid * NB, nbb = min(NB, w - b0);
-    for (int j = 0; j < nbb; ++j) src[b0 + j] = b0 + j;
-    for (int j = 0; j < nbb; ++j) {
-      const int p = (int)(ipiv[K0 + b0 + j] - K0);
-      const int t0 = src[b0 + j]; src[b0 + j] = src[p]; src[p] = t0;
-    }
-  }
-  __syncthreads();
-  int moved = 0;
-  for (int r = tid; r < w; r += kStripThreads) moved |= (src[r] != r);
-  if (!right && !__syncthreads_or(moved)) return;   // no swaps: nothing to do on the left columns
-  const int wr = nblk * NB;   // rows past w (a partial last block) are zero
-  for (int e = tid; e < kStripCols * wr; e += kStripThreads) {
-    const int r = e % wr, cc = e / wr;
-    if (cc < ncol) tile[cc][r] = (r < w) ? A[(c0 + cc) * lda + K0 + src[r]] : T(0);
-  }
-  __syncthreads();
-  if (right) {
+  const int nc = (int)imin64(kStripCols, right ? cr1 - c0 : cl1 - c0);
+  if (!right) {
+    // each block's rows in logical order: row s <- row rowat[s]
     for (int b = 0; b < nblk; ++b) {
-      const int b0 = b * NB, nbb = min(NB, w - b0);
-      // L of the diagonal block, column-major by j: Lc[j][r] = L(b0 + r, b0 + j), strictly lower
-      stage_block<kStripThreads, T>(
-          tid,
-          [&](int r, int j) {
-            return (r < nbb && j < nbb && r > j) ? A[(K0 + b0 + j) * lda + K0 + b0 + r] : T(0);
-          },
-          [&](int r, int j, T v) { Lc[j][r] = v; });
-      __syncthreads();
-      if (tid < ncol) {   // forward substitution, one column per thread
-        T x[NB];
-        const VT* col = reinterpret_cast<const VT*>(&tile[tid][b0]);
-#pragma unroll
-        for (int q = 0; q < NB / V; ++q) {
-          const VT v = col[q];
-#pragma unroll
-          for (int e = 0; e < V; ++e) x[q * V + e] = vget<T>(v, e);
-        }
-#pragma unroll
-        for (int j = 0; j < NB; ++j) {
-          const T xj = x[j];
-          const VT* lcol = reinterpret_cast<const VT*>(&Lc[j][0]);
-#pragma unroll
-          for (int q = (j + 1) / V; q < NB / V; ++q) {
-            const VT u = lcol[q];
-#pragma unroll
-            for (int e = 0; e < V; ++e) {
-              const int r = q * V + e;
-              if (r > j) x[r] -= vget<T>(u, e) * xj;
-            }
-          }
-        }
-        VT* out = reinterpret_cast<VT*>(&tile[tid][b0]);
-#pragma unroll
-        for (int q = 0; q < NB / V; ++q) {
-          VT v;
-#pragma unroll
-          for (int e = 0; e < V; ++e) vset<T>(v, e, x[q * V + e]);
-          out[q] = v;
-        }
+      const int nbb = min(NB, w - b * NB);
+      const int* ra = rowat + b * NB;
+      const int64_t rb = K0 + (int64_t)b * NB;
+      int moved = 0;
+      for (int s = tid; s < nbb; s += kStripThreads) moved |= (ra[s] != s);
+      if (!__syncthreads_or(moved)) continue;
+      for (int e = tid; e < NB * kStripCols; e += kStripThreads) {
+        const int s = e & (NB - 1), cc = e / NB;
+        if (s < nbb && cc < nc) Q[s][cc] = A[(c0 + cc) * lda + rb + s];
       }
       __syncthreads();
-      // later row blocks: tile[rows of b2] -= L(b2, b) tile[rows of b]
-      for (int b2 = b + 1; b2 < nblk; ++b2) {
-        const int r0 = b2 * NB, nr2 = min(NB, w - r0);
-        stage_block<kStripThreads, T>(
-            tid,
-            [&](int r, int j) { return (r < nr2 && j < nbb) ? A[(K0 + b0 + j) * lda + K0 + r0 + r] : T(0); },
-            [&](int r, int j, T v) { Lo[j][r] = v; });
-        __syncthreads();
-        // thread: rows 4*(tid%16).., columns 4*(tid/16)..
-        const int rr = 4 * (tid & 15), cc = 4 * (tid >> 4);
-        T acc[4][4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-          for (int d = 0; d < 4; ++d) acc[a][d] = T(0);
-#pragma unroll 8
-        for (int j = 0; j < NB; ++j) {
-          T lv[4], xv[4];
-#pragma unroll
-          for (int a = 0; a < 4; ++a) lv[a] = Lo[j][rr + a];
-#pragma unroll
-          for (int d = 0; d < 4; ++d) xv[d] = tile[cc + d][b0 + j];
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int d = 0; d < 4; ++d) acc[a][d] += lv[a] * xv[d];
-        }
-#pragma unroll
-        for (int d = 0; d < 4; ++d)
-#pragma unroll
-          for (int a = 0; a < 4; ++a)
-            if (rr + a < nr2) tile[cc + d][r0 + rr + a] -= acc[a][d];
-        __syncthreads();
+      for (int e = tid; e < NB * kStripCols; e += kStripThreads) {
+        const int s = e & (NB - 1), cc = e / NB;
+        if (s < nbb && cc < nc) A[(c0 + cc) * lda + rb + s] = Q[ra[s]][cc];
       }
+      __syncthreads();
     }
+    return;
   }
-  for (int e = tid; e < kStripCols * w; e += kStripThreads) {
-    const int r = e % w, cc = e / w;
-    if (cc < ncol && (right || src[r] != r)) A[(c0 + cc) * lda + K0 + r] = tile[cc][r];
+  const int rg = tid & 15, cg = tid >> 4;   // rows 4 rg.., columns 2 cg..
+  for (int b = 0; b < nblk; ++b) {
+    const int nbb = min(NB, w - b * NB);
+    const int* ra = rowat + b * NB;
+    const int64_t rb = K0 + (int64_t)b * NB;
+    T acc[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        const int r = 4 * rg + i, cc = 2 * cg + l;
+        acc[i][l] = (r < nbb && cc < nc) ? A[(c0 + cc) * lda + rb + ra[r]] : T(0);
+      }
+    for (int b2 = 0; b2 < b; ++b2) {
+      const int64_t rb2 = K0 + (int64_t)b2 * NB;
+      __syncthreads();
+      stage_block<kStripThreads, T>(
+          tid, [&](int r, int j) { return (r < nbb) ? A[(rb2 + j) * lda + rb + r] : T(0); },
+          [&](int r, int j, T v) { Pt[j][r] = v; });   // Pt[j][r] = L(b row r, b2 column j)
+      for (int e = tid; e < NB * kStripCols; e += kStripThreads) {
+        const int j = e & (NB - 1), cc = e / NB;
+        Q[j][cc] = (cc < nc) ? A[(c0 + cc) * lda + rb2 + j] : T(0);   // U_b2
+      }
+      __syncthreads();
+      T d[4][2] = {};
+      mm4x2<T, RP, QP>(Pt, Q, 4 * rg, 2 * cg, d);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int l = 0; l < 2; ++l) acc[i][l] -= d[i][l];
+    }
+    __syncthreads();
+    // Y -> Q[r][c]; Pt[s][r] = L_bb^-1(r, s) = M'(r, rowat[s])
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int l = 0; l < 2; ++l) Q[4 * rg + i][2 * cg + l] = acc[i][l];
+    const T* M = Minv + (size_t)b * NB * NB;
+    stage_block<kStripThreads, T>(
+        tid, [&](int r, int s) { return M[r * NB + ra[s]]; }, [&](int r, int s, T v) { Pt[s][r] = v; });
+    __syncthreads();
+    T u[4][2] = {};
+    mm4x2<T, RP, QP>(Pt, Q, 4 * rg, 2 * cg, u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        const int r = 4 * rg + i, cc = 2 * cg + l;
+        if (r < nbb && cc < nc) A[(c0 + cc) * lda + rb + r] = u[i][l];
+      }
   }
 }
 
@@ -846,7 +830,7 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
   static SmemAttr attr_blk, attr_pfix;
   FP_CUDA_TRY(c->err, attr_blk.ensure(k_blk<T>, (int)blk_smem<T>()));
   FP_CUDA_TRY(c->err, attr_pfix.ensure(k_pfix<T>, (int)pfix_smem<T>()));
-  // M' and the row order of each block of the current panel
+  // M' and the row order of each block of a panel, two sets of slots
   static_assert(kOuterNB / NB <= kPanelSlots, "one scratch slot per block of a panel");
   T* const minv = reinterpret_cast<T*>(c->d_minv);
   int* const rowat = reinterpret_cast<int*>(reinterpret_cast<char*>(c->d_minv) + kMinvBytes);
@@ -858,11 +842,16 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
   static_assert(kOuterNB == kStripRows, "a strip holds one outer panel's rows");
   static SmemAttr attr_strip;
   FP_CUDA_TRY(c->err, attr_strip.ensure(k_strip<T>, (int)strip_smem<T>()));
+  // slots of the panel starting at K0 (two sets: stream2's strip of panel P
+  // reads its set while panel P + 1 fills the other)
+  auto pminv = [&](int64_t K0) { return minv + ((K0 / kOuterNB) & 1) * kPanelSlots * NB * NB; };
+  auto prowat = [&](int64_t K0) { return rowat + ((K0 / kOuterNB) & 1) * kPanelSlots * NB; };
   auto strip = [&](int64_t K0, int w, int64_t cl0, int64_t cl1, int64_t cr0, int64_t cr1) -> int {
     const int64_t g = (cl1 - cl0 + kStripCols - 1) / kStripCols + (cr1 - cr0 + kStripCols - 1) / kStripCols;
     if (g <= 0) return FP_OK;
     TraceScope tr(c, TR_STRIP);
-    k_strip<T><<<(unsigned)g, kStripThreads, strip_smem<T>(), c->stream>>>(A, lda, K0, w, ipiv, cl0, cl1, cr0, cr1);
+    k_strip<T><<<(unsigned)g, kStripThreads, strip_smem<T>(), c->stream>>>(A, lda, K0, w, pminv(K0), prowat(K0), cl0,
+                                                                           cl1, cr0, cr1);
     ++c->nlaunch;
     FP_CUDA_TRY(c->err, cudaGetLastError());
     return FP_OK;
@@ -879,10 +868,12 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
       const int slot = (int)((k - K0) / NB);
+      T* const mv = pminv(K0);
+      int* const ra = prowat(K0);
       if (k == K0) {   // later blocks of the panel are factored at the end of the previous k_blk
         TraceScope tr(c, TR_DIAG);
-        k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, minv + slot * NB * NB,
-                                                     rowat + slot * NB);
+        k_diag<T><<<1, kDiagThreads, 0, c->stream>>>(A, lda, n, k, ipiv, c->d_status, mv + slot * NB * NB,
+                                                     ra + slot * NB);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
@@ -890,9 +881,9 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
         const unsigned g = (unsigned)((below + kBlkRows - 1) / kBlkRows);
         const int next = k + NB < kend;
         TraceScope tr(c, TR_L21);
-        k_blk<T><<<g, kBlkThreads, blk_smem<T>(), c->stream>>>(A, lda, n, k, kend, minv + slot * NB * NB, cert, next,
-                                                               ipiv, c->d_status, minv + (slot + 1) * NB * NB,
-                                                               rowat + (slot + 1) * NB, c->d_ticket);
+        k_blk<T><<<g, kBlkThreads, blk_smem<T>(), c->stream>>>(A, lda, n, k, kend, mv + slot * NB * NB, cert, next,
+                                                               ipiv, c->d_status, mv + (slot + 1) * NB * NB,
+                                                               ra + (slot + 1) * NB, c->d_ticket);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
@@ -901,7 +892,7 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     if (nblk > 1) {
       TraceScope tr(c, TR_U12);
       k_pfix<T><<<(unsigned)(nblk * (nblk - 1)), kPfixThreads, pfix_smem<T>(), c->stream>>>(A, lda, K0, kend, nblk,
-                                                                                          minv, rowat);
+                                                                                          pminv(K0), prowat(K0));
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
