@@ -88,33 +88,34 @@ __device__ __forceinline__ void stage_block(int tid, Get get, Put put) {
 template <class T> __host__ __device__ constexpr int rpitch() { return NB + 16 / (int)sizeof(T); }
 
 // ----------------------------------------------------------------------------
-// (1) k_diag: two warps factor the NB x NB diagonal block with partial
-// pivoting over its rows. Thread t owns row t of the block and keeps its
-// not yet eliminated part in registers, shifted so that R[0] is always the
-// current column: step j forms R[c] <- R[c + 1] - m * U(j, j + 1 + c) for all
-// c with static indices (zeros enter at the end), so the step loop stays
-// rolled and its body (about 150 instructions) stays in the instruction
-// cache, where a fully unrolled loop spent most of its time waiting for
-// instructions. Rows never move: a pivot row is marked used and every other
-// unused row eliminates column j with its own multiplier. The pivot is
-// LAPACK's: the largest |a| in column j among the unused rows, the first in
-// the current logical order on ties. Each warp reduces an integer key (the
-// bits of |a| plus one, 0 for used rows; FP64 in two 32-bit halves) with
-// __reduce_max_sync, ties by logical position with __reduce_min_sync; the two
-// warps' candidates meet in shared memory. The winning thread writes its row
-// as its registers hold it (aligned 16-byte stores, no register moves) and
-// every other row reads it back with broadcast 16-byte loads, taking element
-// c + 1 into its FMA for column c. Multipliers and U rows collect in
-// shared memory (S[thread][column]) and go out in logical row order at the
-// end. LAPACK's ipiv follows from the logical order: at step j, logical rows
-// j and the pivot's position swap. Per-step shared buffers alternate between
-// two copies, so one barrier orders each step's reads before the next step's
+// (1) k_diag: four warps factor the NB x NB diagonal block with partial
+// pivoting over its rows. Each row belongs to a pair of adjacent lanes, each
+// holding 32 of its not yet eliminated entries in registers, shifted so that
+// the even lane's R[0] is always the current column: step j forms
+// R[c] <- R[c + 1] - m U(j, j + 1 + c) with static indices (the odd lane's
+// first entry moves to the even lane by one shuffle, zeros enter at the end),
+// so the step loop stays rolled and small enough for the instruction cache,
+// and each lane does 32 FMAs a step on its own SM sub-partition. Rows never
+// move: a pivot row is marked used and every other unused row eliminates
+// column j with its own multiplier. The pivot is LAPACK's: the largest |a| in
+// column j among the unused rows, the first in the current logical order on
+// ties. Each warp reduces an integer key (the bits of |a| plus one, 0 for used
+// rows; FP64 in two 32-bit halves) with __reduce_max_sync, ties by logical
+// position with __reduce_min_sync; the four warps' candidates meet in shared
+// memory together with each warp's best row (aligned 16-byte stores of the
+// registers as they are), so one barrier per step suffices; every row reads
+// the winner back with broadcast 16-byte loads. Multipliers and U rows collect in
+// shared memory (S[row][column]) and go out in logical row order at the end.
+// LAPACK's ipiv follows from the logical order: at step j, logical rows j and
+// the pivot's position swap. Per-step shared buffers alternate between two
+// copies, so one barrier orders each step's reads before the next step's
 // writes. Last, M' = L11^-1 P11 (P11's columns in physical row order) is
-// formed for the block's update, and the row order kept for the panel's
-// fix-up (k_pfix).
-constexpr int kDiagThreads = NB;
+// formed for the block's update, two lanes per column in the same way, and
+// the row order kept for the panel's fix-up (k_pfix).
+constexpr int kDiagThreads = 2 * NB;
+constexpr int kHalf = NB / 2;   // entries of a row per lane
 
-__device__ __forceinline__ void bar_diag() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+__device__ __forceinline__ void bar_diag() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 template <class T> struct PivKey;
 template <> struct PivKey<float> {
@@ -131,94 +132,127 @@ template <> struct PivKey<double> {
   }
 };
 
-// shared workspace of diag_factor: prow[2][NB], S / Lsh [NB][RP], 2 spare,
-// cand[2][2][4], lpiv[NB], rowat[NB]
+// shared workspace of diag_factor: pcand[2][4][NB], S / Lsh [NB][RP],
+// cand[2][4] (uint4), lpiv[NB], rowat[NB]
 template <class T> __host__ __device__ constexpr int diag_ws_bytes() {
-  return 2 * NB * (int)sizeof(T) + NB * rpitch<T>() * (int)sizeof(T) + 16 + 64 + 2 * NB * 4;
+  return 2 * 4 * NB * (int)sizeof(T) + NB * rpitch<T>() * (int)sizeof(T) + 128 + 2 * NB * 4;
 }
 
-// Threads 0..63 of the calling CTA factor the diagonal block at k (k_diag;
+template <class T> __device__ __forceinline__ T rcp_rn(T x);
+template <> __device__ __forceinline__ float rcp_rn<float>(float x) { return __frcp_rn(x); }
+template <> __device__ __forceinline__ double rcp_rn<double>(double x) { return __drcp_rn(x); }
+
+// The 128 threads of the calling CTA factor the diagonal block at k (k_diag;
 // k_blk runs it for the next block once that block's rows are final). A is
 // read through L2, so another CTA's stores, ordered before by a fence and an
-// atomic, are seen.
+// atomic, are seen. One barrier per step: each warp's best row publishes
+// itself (its key and its whole row) in the step's slot for that warp, and
+// after the barrier every thread picks the best of the four and reads that
+// row. The key is (|a| bits + 1, 63 - logical position, row), compared as
+// unsigned words in that order.
 template <class T>
 __device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int64_t n, int64_t k,
                                             int32_t* __restrict__ ipiv, int* __restrict__ status,
                                             T* __restrict__ Minv, int* __restrict__ rowat_out, unsigned char* ws) {
   typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, NCH = NB / V, RP = rpitch<T>();
-  T (*prow)[NB] = reinterpret_cast<T (*)[NB]>(ws);   // pivot row of a step, as held: prow[c] = U(j, j + c)
-  T* const buf = reinterpret_cast<T*>(ws + 2 * NB * sizeof(T));   // S, then Lsh
-  T* const pval = buf + NB * RP;                                   // (spare)
-  // per step parity and warp: key hi, key lo, logical pos, thread
-  unsigned (*cand)[2][4] = reinterpret_cast<unsigned (*)[2][4]>(reinterpret_cast<unsigned char*>(pval) + 16);
-  int* const lpiv = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(pval) + 16 + 64);
+  constexpr int V = V16<T>::n, RP = rpitch<T>(), HQ = kHalf / V;
+  T (*pcand)[4][NB] = reinterpret_cast<T (*)[4][NB]>(ws);           // candidate rows, per parity and warp
+  T* const buf = reinterpret_cast<T*>(ws + 2 * 4 * NB * sizeof(T));  // S, then Lsh
+  uint4 (*cand)[4] = reinterpret_cast<uint4 (*)[4]>(buf + NB * RP);  // per parity and warp: key
+  int* const lpiv = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(cand) + 128);
   int* const rowat = lpiv + NB;
-  // S[t][c]: row t's entry of L (c < its step) or U
+  // S[r][c]: row r's entry of L (c < its step) or U
   T (*S)[NB + 1] = reinterpret_cast<T (*)[NB + 1]>(buf);
   const int nb = (int)imin64(NB, n - k);
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  T R[NB];
+  const int h = lane & 1;                       // which half of the row
+  const int row = warp * 16 + (lane >> 1);      // the row of this lane pair
+  const int g0 = h * kHalf;                     // first column of this half
+  T R[kHalf];
 #pragma unroll
-  for (int c = 0; c < NB; ++c)
-    R[c] = (t < nb && c < nb) ? __ldcg(&A[(k + c) * lda + (k + t)]) : ((t == c) ? T(1) : T(0));
-  bool used = !(t < nb);
-  int pos = t;
+  for (int c = 0; c < kHalf; ++c) {
+    const int g = g0 + c;
+    R[c] = (row < nb && g < nb) ? __ldcg(&A[(k + g) * lda + (k + row)]) : ((row == g) ? T(1) : T(0));
+  }
+  bool used = !(row < nb);
+  int pos = row;
   bool zero = false;
-#pragma unroll 1
-  for (int j = 0; j < nb; ++j) {
-    const int par = j & 1;
+  T cur = __shfl_sync(0xffffffffu, R[0], lane & ~1);   // the row's entry in the current column
+  // this warp's best unused row for the next step: key words and, after the
+  // row's update, its row in pcand
+  auto reduce_key = [&](unsigned& mh, unsigned& ml, unsigned& mlow) {
     unsigned hi, lo;
-    PivKey<T>::of(R[0], used, hi, lo);
-    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
-    const unsigned ml = (sizeof(T) == 8) ? __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u) : 0u;
+    PivKey<T>::of(cur, used, hi, lo);
+    mh = __reduce_max_sync(0xffffffffu, hi);
+    ml = (sizeof(T) == 8) ? __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u) : 0u;
     const bool top = hi == mh && lo == ml;
-    const unsigned pm = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
-    if (lane == 0) {
-      cand[par][warp][0] = mh;
-      cand[par][warp][1] = ml;
-      cand[par][warp][2] = pm;
-    }
-    if (top && (unsigned)pos == pm) cand[par][warp][3] = (unsigned)t;
-    bar_diag();
-    const unsigned h0 = cand[par][0][0], l0 = cand[par][0][1], p0 = cand[par][0][2];
-    const unsigned h1 = cand[par][1][0], l1 = cand[par][1][1], p1 = cand[par][1][2];
-    const bool w1 = (h1 > h0) || (h1 == h0 && (l1 > l0 || (l1 == l0 && p1 < p0)));
-    const int pr = (int)cand[par][w1 ? 1 : 0][3];   // pivot row (thread)
-    const int lp = (int)(w1 ? p1 : p0);             // its logical position
-    if (t == pr) {   // the row as it lies in registers: whole 16-byte stores
-      VT* out = reinterpret_cast<VT*>(prow[par]);
+    mlow = __reduce_max_sync(0xffffffffu, top ? ((unsigned)(63 - pos) << 6) | (unsigned)row : 0u);
+  };
+  auto publish_row = [&](int par, unsigned mh, unsigned ml, unsigned mlow) {
+    if (lane == 0) cand[par][warp] = make_uint4(mh, ml, mlow, 0u);
+    if ((unsigned)row == (mlow & 63u)) {   // this warp's best row: whole 16-byte stores of both halves
+      VT* out = reinterpret_cast<VT*>(&pcand[par][warp][g0]);
 #pragma unroll
-      for (int q = 0; q < NCH; ++q) {
+      for (int q = 0; q < HQ; ++q) {
         VT v;
 #pragma unroll
         for (int e = 0; e < V; ++e) vset<T>(v, e, R[q * V + e]);
         out[q] = v;
       }
     }
+  };
+  if (nb > 0) {
+    unsigned mh, ml, mlow;
+    reduce_key(mh, ml, mlow);
+    publish_row(0, mh, ml, mlow);
+  }
+#pragma unroll 1
+  for (int j = 0; j < nb; ++j) {
+    const int par = j & 1;
     bar_diag();
-    const T sv = prow[par][0];
-    if (t == pr) { pos = j; used = true; } else if (pos == j) { pos = lp; }
+    uint4 best = cand[par][0];
+    int w = 0;
+#pragma unroll
+    for (int q = 1; q < 4; ++q) {
+      const uint4 c4 = cand[par][q];
+      const unsigned long long kq = ((unsigned long long)c4.x << 32) | c4.y;
+      const unsigned long long kb = ((unsigned long long)best.x << 32) | best.y;
+      if (kq > kb || (kq == kb && c4.z > best.z)) { best = c4; w = q; }
+    }
+    const int pr = (int)(best.z & 63u);         // pivot row
+    const int lp = 63 - (int)(best.z >> 6);     // its logical position
+    const T* prow = pcand[par][w];
+    const T piv = prow[0];
+    const T rp = (piv != T(0)) ? rcp_rn<T>(piv) : T(0);
+    if (row == pr) { pos = j; used = true; } else if (pos == j) { pos = lp; }
     if (t == 0) lpiv[j] = lp;
     // the pivot's row of U goes to S[pr][j..], one element per thread
-    if (t < NB - j) S[pr][j + t] = prow[par][t];
-    const T rp = (sv != T(0)) ? T(1) / sv : T(0);
+    if (t < NB - j) S[pr][j + t] = prow[t];
     zero |= (rp == T(0));
-    const T m = R[0] * rp;   // 0 on a zero pivot: the row only shifts
-    if (!used) S[t][j] = m;
-    const VT* in = reinterpret_cast<const VT*>(prow[par]);
-    T pv[NB];
+    const T m = cur * rp;   // 0 on a zero pivot: the row only shifts
+    if (!used && h == 0) S[row][j] = m;
+    T pv[kHalf];
+    const VT* in = reinterpret_cast<const VT*>(&prow[g0]);
 #pragma unroll
-    for (int q = 0; q < NCH; ++q) {
+    for (int q = 0; q < HQ; ++q) {
       const VT v = in[q];
 #pragma unroll
       for (int e = 0; e < V; ++e) pv[q * V + e] = vget<T>(v, e);
     }
+    const T pnext = (h == 0) ? prow[kHalf] : T(0);
+    const T nxt = __shfl_down_sync(0xffffffffu, R[0], 1);   // the odd lane's first entry
+    // the next step's column first: its key reductions overlap the rest
+    R[0] = R[1] - m * pv[1];
+    cur = __shfl_sync(0xffffffffu, R[0], lane & ~1);
+    unsigned mh = 0, ml = 0, mlow = 0;
+    if (j + 1 < nb) reduce_key(mh, ml, mlow);
 #pragma unroll
-    for (int c = 0; c < NB; ++c) R[c] = (c + 1 < NB) ? R[c + 1] - m * pv[c + 1] : T(0);
+    for (int c = 1; c < kHalf - 1; ++c) R[c] = R[c + 1] - m * pv[c + 1];
+    R[kHalf - 1] = (h == 0 ? nxt : T(0)) - m * pnext;
+    if (j + 1 < nb) publish_row(par ^ 1, mh, ml, mlow);
   }
   if (zero && t == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-  if (t < nb) rowat[pos] = t;
+  if (h == 0 && row < nb) rowat[pos] = row;
   bar_diag();
   // write back in logical row order, rows fastest over the threads
   for (int e = t; e < nb * nb; e += kDiagThreads) {
@@ -226,11 +260,11 @@ __device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int6
     A[(k + c) * lda + (k + s)] = S[rowat[s]][c];
   }
   if (t < nb) ipiv[k + t] = (int32_t)(k + lpiv[t]);
-  rowat_out[t] = (t < nb) ? rowat[t] : t;
+  if (t < NB) rowat_out[t] = (t < nb) ? rowat[t] : t;
   bar_diag();   // the factors are in A (visible to the CTA); S is free
   // M' = L11^-1 P11 with P11's columns in physical row order (M' A12 = U12
-  // for A12 as it lies): column r solves L y = e_pos(r), one column per
-  // thread, with L's columns shifted as the factorisation's rows were:
+  // for A12 as it lies): column r solves L y = e_pos(r), held by the lane
+  // pair of row r, with L's columns shifted as the factorisation's rows were:
   // Lsh[j][c] = L(j + 1 + c, j), zero past the end.
   T (*Lsh)[RP] = reinterpret_cast<T (*)[RP]>(buf);
   for (int e = t; e < NB * NB; e += kDiagThreads) {
@@ -238,23 +272,25 @@ __device__ __forceinline__ void diag_factor(T* __restrict__ A, int64_t lda, int6
     Lsh[j][c] = (j + 1 + c < nb) ? A[(k + j) * lda + (k + j + 1 + c)] : T(0);
   }
   bar_diag();
-  T y[NB];
+  T y[kHalf];
 #pragma unroll
-  for (int c = 0; c < NB; ++c) y[c] = (c == pos) ? T(1) : T(0);
+  for (int c = 0; c < kHalf; ++c) y[c] = (g0 + c == pos) ? T(1) : T(0);
 #pragma unroll 1
   for (int j = 0; j < NB; ++j) {
-    const T yj = y[0];
-    Minv[j * NB + t] = yj;
-    const VT* lrow = reinterpret_cast<const VT*>(&Lsh[j][0]);
+    const T yj = __shfl_sync(0xffffffffu, y[0], lane & ~1);
+    const T nxt = __shfl_down_sync(0xffffffffu, y[0], 1);
+    if (h == 0) Minv[j * NB + row] = yj;
+    T lv[kHalf];
+    const VT* lrow = reinterpret_cast<const VT*>(&Lsh[j][g0]);
 #pragma unroll
-    for (int q = 0; q < NCH; ++q) {
-      const VT lv = lrow[q];
+    for (int q = 0; q < HQ; ++q) {
+      const VT v = lrow[q];
 #pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const int c = q * V + e;
-        y[c] = (c + 1 < NB ? y[c + 1] : T(0)) - yj * vget<T>(lv, e);
-      }
+      for (int e = 0; e < V; ++e) lv[q * V + e] = vget<T>(v, e);
     }
+#pragma unroll
+    for (int c = 0; c < kHalf - 1; ++c) y[c] = y[c + 1] - yj * lv[c];
+    y[kHalf - 1] = (h == 0 ? nxt : T(0)) - yj * lv[kHalf - 1];
   }
 }
 
@@ -430,7 +466,8 @@ k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const 
     }
   }
   __syncthreads();
-  if (!last || tid >= kDiagThreads) return;
+  if (!last) return;
+  static_assert(kDiagThreads == kBlkThreads, "the whole CTA factors the next diagonal block");
   diag_factor<T>(A, lda, n, k1, ipiv, status, Minv_next, rowat_next, bsm);
 }
 
