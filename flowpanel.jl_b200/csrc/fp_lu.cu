@@ -305,8 +305,8 @@ k_diag(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int32_t* __restrict
 // ----------------------------------------------------------------------------
 // (2) k_blk: the rest of a block step in one launch. CTA b owns the rows
 // [k1 + b RT, +RT) below the factored diagonal block (k1 = k + NB):
-//  * L21 = A21 U11^-1 by substitution, one row per thread of warp 0, the row
-//    kept shifted in registers as in k_diag (rolled loop over the 64
+//  * L21 = A21 U11^-1 by substitution, four lanes per row (16 entries each),
+//    the row kept shifted in registers as in k_diag (rolled loop over the 64
 //    columns, 16-byte broadcast reads of the shifted U rows); max|L21| is the
 //    GEPP certificate;
 //  * W = L21 M' with M' = L11^-1 P11 from k_diag;
@@ -357,7 +357,7 @@ k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const 
       float* __restrict__ cert, int next, int32_t* __restrict__ ipiv, int* __restrict__ status,
       T* __restrict__ Minv_next, int* __restrict__ rowat_next, unsigned* __restrict__ ticket) {
   typedef typename V16<T>::type VT;
-  constexpr int V = V16<T>::n, NCH = NB / V, RP = rpitch<T>(), LP = blk_lpitch<T>();
+  constexpr int V = V16<T>::n, RP = rpitch<T>(), LP = blk_lpitch<T>();
   extern __shared__ __align__(16) unsigned char bsm[];
   T (*Bs)[RP] = reinterpret_cast<T (*)[RP]>(bsm);   // shifted U11 rows, then M', then A12 chunks
   T (*Ls)[LP] = reinterpret_cast<T (*)[LP]>(bsm + (size_t)NB * RP * sizeof(T));   // L21, then W: [column][row]
@@ -374,31 +374,41 @@ k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const 
         Bs[j][l > j ? l - j - 1 : NB - 1 - j + l] = (l > j) ? v : T(0);
       });
   __syncthreads();
-  if (tid < kBlkRows) {
-    T x[NB];
+  {
+    // four lanes per row, 16 of its entries each, shifted as in k_diag: the
+    // quarter-0 lane holds the current column; the next quarter's first entry
+    // moves down by one shuffle a step
+    constexpr int QW = NB / 4;
+    const int r = tid >> 2, qtr = tid & 3, lane = tid & 31;
+    const int64_t grow = row0 + r;
+    T x[QW];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) x[c] = (tid < rows) ? A[(k + c) * lda + row0 + tid] : T(0);
+    for (int c = 0; c < QW; ++c) x[c] = (r < rows) ? A[(k + qtr * QW + c) * lda + grow] : T(0);
     float lmax = 0.f;
 #pragma unroll 1
     for (int j = 0; j < NB; ++j) {
-      const T xj = x[0] * rd[j];
-      Ls[j][tid] = xj;
-      if (tid < rows) A[(k + j) * lda + row0 + tid] = xj;
-      lmax = fmaxf(lmax, (float)tabs(xj));
-      const VT* urow = reinterpret_cast<const VT*>(&Bs[j][0]);
-#pragma unroll
-      for (int q = 0; q < NCH; ++q) {
-        const VT u = urow[q];
-#pragma unroll
-        for (int e = 0; e < V; ++e) {
-          const int c = q * V + e;
-          x[c] = (c + 1 < NB ? x[c + 1] : T(0)) - xj * vget<T>(u, e);
-        }
+      const T xj = __shfl_sync(0xffffffffu, x[0], lane & ~3) * rd[j];
+      const T nxt = __shfl_down_sync(0xffffffffu, x[0], 1);
+      if (qtr == 0) {
+        Ls[j][r] = xj;
+        if (r < rows) A[(k + j) * lda + grow] = xj;
+        lmax = fmaxf(lmax, (float)tabs(xj));
       }
+      T u[QW];
+      const VT* urow = reinterpret_cast<const VT*>(&Bs[j][qtr * QW]);
+#pragma unroll
+      for (int q = 0; q < QW / V; ++q) {
+        const VT v = urow[q];
+#pragma unroll
+        for (int e = 0; e < V; ++e) u[q * V + e] = vget<T>(v, e);
+      }
+#pragma unroll
+      for (int c = 0; c < QW - 1; ++c) x[c] = x[c + 1] - xj * u[c];
+      x[QW - 1] = (qtr < 3 ? nxt : T(0)) - xj * u[QW - 1];
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    if (tid == 0 && lmax > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(lmax));
+    if (lane == 0 && lmax > 0.f) atomicMax(reinterpret_cast<int*>(cert), __float_as_int(lmax));
   }
   const int64_t nn = kend - k1;
   if (nn <= 0) return;   // then there is no next block in the panel

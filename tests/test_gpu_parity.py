@@ -174,3 +174,27 @@ def test_errors_mirror_reference(fp, ctx):
     with pytest.raises(cap.FlowPanelError) as e:
         ctx.factor()
     assert e.value.code == cap.FP_ESTATE
+
+
+def test_factor_trace(fp, ctx):
+    """fp_trace: every launch of a factorisation on both streams, in order
+    on each stream, inside the factorisation's span; no trace when off."""
+    w, body, normals, cps, D, U = _wing_setup(fp, nc=24, ns=30)   # 720 panels: three outer panels
+    cap = fp._capi
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    ctx.assemble(cap.FP_ELEMENT_VORTEXRING, precision=cap.FP_PREC_MIXED)
+    ctx.trace(True)
+    ctx.factor(cap.FP_PREC_MIXED)
+    ctx.trace(False)
+    tags, streams, t0, t1 = ctx.trace_read()
+    assert len(tags) > 10
+    assert set(np.unique(tags)) <= set(range(8)) and {0, 1, 2, 3} <= set(np.unique(tags))
+    assert set(np.unique(streams)) == {0, 1}
+    assert np.all(t1 >= t0) and np.all(t0 >= 0)
+    for s in (0, 1):
+        o = np.argsort(t0[streams == s])
+        a, b = t0[streams == s][o], t1[streams == s][o]
+        assert np.all(a[1:] >= b[:-1] - 1e-3)   # launches on one stream do not overlap
+    ctx.factor(cap.FP_PREC_MIXED)
+    assert len(ctx.trace_read()[0]) == 0
