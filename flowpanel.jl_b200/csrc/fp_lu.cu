@@ -1188,6 +1188,9 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
     const int nb = (int)imin64(SB, n - k0);
     const T* Di = Dinv128 + b * 2 * SB * SB + (LOWER ? 0 : SB * SB);
     for (int e = tid; e < SB * SB; e += kTrs1Threads) Ds[e / SB][e % SB] = Di[e];   // Di column-major: e = l*SB + r
+    // this block's right-hand side, written only by this CTA: fetched now,
+    // off the chain of dependent blocks
+    const T rhs = (tid < nb) ? B[k0 + tid] : T(0);
     T sum[4] = {T(0), T(0), T(0), T(0)};
     const bool rows_full = 4 * rg + 4 <= nb;
     int64_t ready = 0;   // dependencies known complete (this warp)
@@ -1247,7 +1250,7 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
       T s0 = T(0);
 #pragma unroll
       for (int q = 0; q < 8; ++q) s0 += red[q][tid];
-      accs[tid] = (tid < nb) ? B[k0 + tid] - s0 : T(0);
+      accs[tid] = (tid < nb) ? rhs - s0 : T(0);
     }
     __syncthreads();
     {   // x = inv(D) acc: thread (r, half) sums half of the columns
@@ -1259,9 +1262,13 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
       __syncthreads();
       if (h == 0 && r < nb) B[k0 + r] = s0 + xpart[r];
     }
-    __threadfence();
+    // publish: the barrier orders the CTA's stores before thread 0's fence
+    // (cumulative), which orders them before the flag
     __syncthreads();
-    if (tid == 0) atomicExch(&flags[b], 1u);
+    if (tid == 0) {
+      __threadfence();
+      atomicExch(&flags[b], 1u);
+    }
   }
 }
 
