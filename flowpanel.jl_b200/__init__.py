@@ -8,9 +8,10 @@ directory by ``__graft_entry__.load_package``).
 from . import _capi, meshes  # noqa: F401
 from .bodies import (B200Solver, MultiBody, NonLiftingBody, RigidWakeBody, Uind,  # noqa: F401
                      calc_areas, calc_controlpoints, calc_normals, calcfield_Cp, calcfield_F,
-                     calcfield_LDS, calcfield_U, solve, solve_batch)
+                     calcfield_LDS, calcfield_U, phi, solve, solve_batch)
 
-__all__ = ["B200Solver", "MultiBody", "NonLiftingBody", "RigidWakeBody", "solve", "solve_batch", "Uind", "calcfield_U",
+__all__ = ["B200Solver", "MultiBody", "NonLiftingBody", "RigidWakeBody", "solve", "solve_batch", "Uind", "phi",
+           "calcfield_U",
            "calcfield_Cp", "calcfield_F", "calcfield_LDS", "calc_normals", "calc_controlpoints",
            "calc_areas", "meshes"]
 

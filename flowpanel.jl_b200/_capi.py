@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libflowpanel_b200.so")
 
 FP_OK, FP_EINVAL, FP_ESINGULAR, FP_ENOCONV, FP_ECUDA, FP_ETIMEOUT, FP_ESTATE = range(7)
-FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING = 0, 1
+FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING, FP_ELEMENT_SOURCE_DOUBLET = 0, 1, 2
 FP_PREC_FP64, FP_PREC_MIXED = 0, 1
 FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
 FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP = range(6)
@@ -26,7 +26,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
-           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read")
+           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi")
 
 
 class SolveOpts(C.Structure):
@@ -87,6 +87,7 @@ def lib():
         L.fp_solve_body.argtypes = [vp, C.c_int, C.c_double, C.c_double, _dp, C.c_int64,
                                     C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
         L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
+        L.fp_phi.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_double]
         L.fp_adjoint_solve.argtypes = [vp, _dp, C.c_int64, _dp]
         L.fp_lu_solve_noalloc.argtypes = [vp, C.c_void_p, C.c_int64, C.c_int64]
         L.fp_assembly_vjp.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -112,6 +113,13 @@ def lib():
 
 def _d(a):
     return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _strengths(s):
+    """Strengths as the ABI takes them: N values, or N x 2 column-major (all
+    sources, then all doublets) for a source+doublet body."""
+    s = np.asarray(s, dtype=np.float64)
+    return np.ascontiguousarray(s.T).ravel() if s.ndim == 2 else _f64(s)
 
 
 def _i(a):
@@ -216,8 +224,18 @@ class Context:
         targets = _f64(np.reshape(targets, (-1, 3)))
         m = targets.shape[0]
         out = np.zeros((m, 3)) if out is None else np.ascontiguousarray(out, dtype=np.float64)
-        self._chk(self._L.fp_uind(self.h, element, _d(_f64(strengths)), _d(targets), m, _d(out), precision,
-                                  kerneloffset, kernelcutoff))
+        self._chk(self._L.fp_uind(self.h, element, _d(_strengths(strengths)), _d(targets), m, _d(out),
+                                  precision, kerneloffset, kernelcutoff))
+        return out
+
+    def phi(self, element, strengths, targets, out=None, kerneloffset=1e-8):
+        """Potential at targets (M, 3) added to out (M,) (fp_phi). strengths: N, or
+        (N, 2) (sources, doublets) for FP_ELEMENT_SOURCE_DOUBLET."""
+        targets = _f64(np.reshape(targets, (-1, 3)))
+        m = targets.shape[0]
+        out = np.zeros(m) if out is None else np.ascontiguousarray(out, dtype=np.float64)
+        self._chk(self._L.fp_phi(self.h, element, _d(_strengths(strengths)), _d(targets), m, _d(out),
+                                 kerneloffset))
         return out
 
     def adjoint_solve(self, ybar):

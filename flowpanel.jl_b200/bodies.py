@@ -68,9 +68,23 @@ class AbstractBody:
 
 
 class NonLiftingBody(AbstractBody):
-    """NonLiftingBody{ConstantSource} (src/FLOWPanel_nonliftingbody.jl:32-72)."""
+    """NonLiftingBody{E} (src/FLOWPanel_nonliftingbody.jl:32-72) with E one of
+    "ConstantSource" (the default), "ConstantDoublet" or
+    "ConstantSource+ConstantDoublet" (the reference's
+    Union{ConstantSource, ConstantDoublet}, two strengths per panel)."""
+    _ELEMENTS = {"ConstantSource": ("source", _capi.FP_ELEMENT_SOURCE),
+                 "ConstantDoublet": ("doublet", _capi.FP_ELEMENT_VORTEXRING),
+                 "ConstantSource+ConstantDoublet": ("source+doublet", _capi.FP_ELEMENT_SOURCE_DOUBLET)}
     kind = "source"
     element = _capi.FP_ELEMENT_SOURCE
+
+    def __init__(self, mesh: Mesh, *args, element="ConstantSource", **kwargs):
+        if element not in self._ELEMENTS:
+            raise ValueError(f"unknown element {element}; expected one of {list(self._ELEMENTS)}")
+        self.kind, self.element = self._ELEMENTS[element]
+        super().__init__(mesh, *args, **kwargs)
+        if self.kind == "source+doublet":
+            self.strength = np.zeros((self.ncells, 2))
 
 
 class RigidWakeBody(AbstractBody):
@@ -225,10 +239,21 @@ class B200Solver:
 
 def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200Solver] = None):
     """solve(body, Uinfs[, Das, Dbs]; solver): assemble, factor and solve on the
-    GPU, then store the strengths and the fields like the reference."""
+    GPU, then store the strengths and the fields like the reference. A
+    source+doublet NonLiftingBody follows its reference method
+    (src/FLOWPanel_nonliftingbody.jl:425-600): sigma = -Uinf . n and
+    mu = the potential of the sources of strength -sigma at the control points;
+    like the reference it returns mu and stores nothing."""
     Uinfs = np.asarray(Uinfs, dtype=np.float64)
     if Uinfs.shape != (body.ncells, 3):
         raise ValueError(f"Invalid Uinfs; expected size ({body.ncells}, 3), got {Uinfs.shape}")
+    if body.kind == "source+doublet":
+        normals = calc_normals(body)
+        CPs = calc_controlpoints(body, normals)
+        sigma = -np.einsum("ij,ij->i", normals, Uinfs)
+        solver = solver or B200Solver()
+        solver.load(body, normals, CPs)
+        return solver.ctx.phi(_capi.FP_ELEMENT_SOURCE, -sigma, CPs, None, body.kerneloffset)
     lifting = body.kind == "vortexring"
     if lifting:
         if Das is None or Dbs is None:
@@ -253,6 +278,8 @@ def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200So
         body.add_field("Da", "vector", Das, "system")
         body.add_field("Db", "vector", Dbs, "system")
         body.add_field("Gamma", "scalar", body.strength, "cell")
+    elif body.kind == "doublet":
+        body.add_field("mu", "scalar", body.strength, "cell")
     else:
         body.add_field("sigma", "scalar", body.strength, "cell")
     body._solver = solver
@@ -304,21 +331,37 @@ def solve_batch(bodies: List[AbstractBody], Uinfs, Das=None, Dbs=None, method="l
     return stats
 
 
+def _field_solver(body: AbstractBody, solver: Optional[B200Solver]):
+    """A solver whose context holds the body's geometry (and wake)."""
+    solver = solver or getattr(body, "_solver", None) or B200Solver()
+    if solver._geom_of != id(body):
+        solver.load(body)
+        if body.kind == "vortexring" and body.nsheddings:
+            Da = body.get_field("Da")["field_data"]
+            Db = body.get_field("Db")["field_data"]
+            solver.ctx.set_wake(body.mesh.shedding, Da, Db)
+    return solver
+
+
 def Uind(body: AbstractBody, targets, out, solver: Optional[B200Solver] = None, precision="fp64"):
     """Uind!: add the velocity induced by the solved body at targets (M, 3) to out
     (src/FLOWPanel_abstractbody.jl:101-110)."""
     if not body.solved:
         raise RuntimeError("Source body hasn't been solved yet. Please call `solve(...)` function first.")
-    solver = solver or getattr(body, "_solver", None) or B200Solver()
-    if solver._geom_of != id(body):
-        solver.load(body)
-        if body.kind == "vortexring":
-            Da = body.get_field("Da")["field_data"]
-            Db = body.get_field("Db")["field_data"]
-            solver.ctx.set_wake(body.mesh.shedding, Da, Db)
+    solver = _field_solver(body, solver)
     prec = _capi.FP_PREC_MIXED if precision == "mixed" else _capi.FP_PREC_FP64
     return solver.ctx.uind(body.element, body.strength, targets, out, prec,
                            body.kerneloffset, body.kernelcutoff)
+
+
+def phi(body: AbstractBody, targets, out, solver: Optional[B200Solver] = None):
+    """phi!: add the potential induced by the solved body at targets (M, 3) to
+    out (M,) (src/FLOWPanel_abstractbody.jl:118-127): sources, doublets, both,
+    or vortex rings with the wake's semi-infinite doublets."""
+    if not body.solved:
+        raise RuntimeError("Body hasn't been solved yet. Please call `solve()` function first.")
+    solver = _field_solver(body, solver)
+    return solver.ctx.phi(body.element, body.strength, targets, out, body.kerneloffset)
 
 
 def calcfield_U(sourcebody: AbstractBody, targetbody: AbstractBody, offset=None,

@@ -1,6 +1,7 @@
 // C ABI of the B200 panel-method library: context, geometry, orchestration.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -304,6 +305,7 @@ int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* D
   std::vector<WakeRec> w(nsh);
   std::vector<int> touched(c->N, 0);
   bool disjoint = true;
+  int64_t opposite = -1;   // first edge whose da, db are opposite or orthogonal
   for (int64_t e = 0; e < nsh; ++e) {
     const int32_t* s = shedding + 6 * e;
     const double* da = Das + 3 * e;
@@ -331,6 +333,7 @@ int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* D
     for (int d = 0; d < 3; ++d) { r.da[d] = da[d]; r.db[d] = db[d]; }
     r.pi = pi;
     r.pj = pj;
+    if (da[0] * db[0] + da[1] * db[1] + da[2] * db[2] <= 0 && opposite < 0) opposite = e;
     if (touched[pi]++) disjoint = false;
     if (pj >= 0 && touched[pj]++) disjoint = false;
   }
@@ -347,6 +350,7 @@ int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* D
   c->h_shed.assign(shedding, shedding + 6 * nsh);
   c->h_Da.assign(Das, Das + 3 * nsh);
   c->h_Db.assign(Dbs, Dbs + 3 * nsh);
+  c->wake_opposite = opposite;
   c->nsh = nsh;
   c->wake_disjoint = disjoint;
   c->assembled = -1;
@@ -631,21 +635,68 @@ int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targe
   if (m == 0) return FP_OK;
   c->kern_offset = kerneloffset;
   c->kern_cutoff = kernelcutoff;
-  if (int rc = ensure_stage(c, (size_t)c->N + 6 * (size_t)m)) return rc;
+  const int64_t ns = element == FP_ELEMENT_SOURCE_DOUBLET ? 2 * c->N : c->N;
+  if (int rc = ensure_stage(c, (size_t)ns + 6 * (size_t)m)) return rc;
   double* ds = c->d_stage;
-  double* dt = ds + c->N;
+  double* dt = ds + ns;
   double* dout = dt + 3 * m;
-  FP_CUDA_TRY(c->err, cudaMemcpyAsync(ds, strengths, c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(ds, strengths, ns * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(dt, targets, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(dout, out, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (time_begin(c)) return FP_ECUDA;
-  int rc = element == FP_ELEMENT_VORTEXRING ? launch_uind_ring(c, ds, dt, m, dout, precision == FP_PREC_MIXED)
-                                            : launch_uind_source(c, ds, dt, m, dout);
+  int rc;
+  if (element == FP_ELEMENT_VORTEXRING) {
+    rc = launch_uind_ring(c, ds, dt, m, dout, precision == FP_PREC_MIXED);
+  } else if (element == FP_ELEMENT_SOURCE_DOUBLET) {   // sources, then doublets (rings without wake)
+    const int64_t nsh = c->nsh;
+    c->nsh = 0;
+    rc = launch_uind_source(c, ds, dt, m, dout);
+    if (!rc) rc = launch_uind_ring(c, ds + c->N, dt, m, dout, false);
+    c->nsh = nsh;
+  } else {
+    rc = launch_uind_source(c, ds, dt, m, dout);
+  }
   if (rc) return rc;
   if (time_end(c, &c->ms_uind)) return FP_ECUDA;
   c->kms[FP_STAGE_UIND] = c->ms_uind;
   c->klaunch[FP_STAGE_UIND] = 1;
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(out, dout, 3 * m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  return FP_OK;
+}
+
+int fp_phi(fp_ctx* c, int element, const double* strengths, const double* targets, int64_t m, double* out,
+           double kerneloffset) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_phi: no geometry");
+  if (element != FP_ELEMENT_SOURCE && element != FP_ELEMENT_VORTEXRING && element != FP_ELEMENT_SOURCE_DOUBLET)
+    return c->err.set(FP_EINVAL, "fp_phi: unknown element");
+  if (!strengths || (m > 0 && (!targets || !out)) || m < 0) return c->err.set(FP_EINVAL, "fp_phi: bad arguments");
+  const bool wake = element == FP_ELEMENT_VORTEXRING && c->nsh > 0;
+  if (wake && c->wake_opposite >= 0) {
+    const double* da = c->h_Da.data() + 3 * c->wake_opposite;
+    const double* db = c->h_Db.data() + 3 * c->wake_opposite;
+    char msg[256];
+    std::snprintf(msg, sizeof(msg),
+                  "Invalid semi-infinite directions: da=[%g, %g, %g] is opposite or orthogonal to db=[%g, %g, %g]",
+                  da[0], da[1], da[2], db[0], db[1], db[2]);
+    return c->err.set(FP_EINVAL, msg);
+  }
+  if (m == 0) return FP_OK;
+  c->kern_offset = kerneloffset;
+  const int64_t ns = element == FP_ELEMENT_SOURCE_DOUBLET ? 2 * c->N : c->N;
+  if (int rc = ensure_stage(c, (size_t)ns + 4 * (size_t)m)) return rc;
+  double* ds = c->d_stage;
+  double* dt = ds + ns;
+  double* dout = dt + 3 * m;
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(ds, strengths, ns * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(dt, targets, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(dout, out, m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const double* sigma = element == FP_ELEMENT_VORTEXRING ? nullptr : ds;
+  const double* mu = element == FP_ELEMENT_SOURCE ? nullptr : (element == FP_ELEMENT_SOURCE_DOUBLET ? ds + c->N : ds);
+  if (int rc = launch_phi(c, sigma, mu, dt, m, dout, wake)) return rc;
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(out, dout, m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   return FP_OK;
 }

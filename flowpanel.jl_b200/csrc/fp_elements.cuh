@@ -269,4 +269,141 @@ __device__ __forceinline__ void source_vel(const SourceRec& R, double X1, double
   w = V1 * R.t[2] + V2 * R.o[2] + V3 * R.n[2];
 }
 
+// ---------------------------------------------------------------- potentials
+// All in FP64 and in the panel's flipped frame (o, t, -n) held by SourceRec;
+// unit strength, the caller scales.
+
+// Constant-source potential (src/FLOWPanel_elements.jl:152-241, Hess & Smith).
+__device__ __forceinline__ double source_phi(const SourceRec& R, double X1, double X2, double X3, double offset) {
+  const double dx = X1 - R.O[0], dy = X2 - R.O[1], dz = X3 - R.O[2];
+  const double x = R.t[0] * dx + R.t[1] * dy + R.t[2] * dz;
+  const double y = R.o[0] * dx + R.o[1] * dy + R.o[2] * dz;
+  const double z = R.n[0] * dx + R.n[1] * dy + R.n[2] * dz;
+  const double az = fabs(z);
+  double phi = 0, dtheta = 2 * kPi;
+  const int nn = R.nn;
+  for (int i = 0; i < nn; ++i) {
+    const int j = (i + 1 == nn) ? 0 : i + 1;
+    const double xi = R.xs[i], yi = R.ys[i], zi = R.zs[i];
+    const double xj = R.xs[j], yj = R.ys[j], zj = R.zs[j];
+    const double dij = R.dij[i];
+    const double ri = sqrt((x - xi) * (x - xi) + (y - yi) * (y - yi) + (z - zi) * (z - zi));
+    const double rj = sqrt((x - xj) * (x - xj) + (y - yj) * (y - yj) + (z - zj) * (z - zj));
+    const double Qij = log((ri + rj + dij) / (ri + rj - dij + offset));
+    const double Sij = R.S[i], Cij = R.Cc[i];
+    const double siji = (xi - x) * Cij + (yi - y) * Sij;
+    const double sijj = (xj - x) * Cij + (yj - y) * Sij;
+    const double Rij = (x - xi) * Sij - (y - yi) * Cij;
+    const double Jij = atan2(Rij * az * (ri * sijj - rj * siji), ri * rj * Rij * Rij + z * z * sijj * siji);
+    phi -= Rij * Qij + az * Jij;
+    dtheta *= (Rij >= 0);
+  }
+  phi += az * dtheta;
+  return phi * (1 / (4 * kPi));
+}
+
+// Hess-Smith solid angle over a polygon in local coordinates (xs, ys, zs) at
+// local (x, y, z): the doublet potential's kernel (src/FLOWPanel_elements.jl:796-833).
+template <int NNMAX>
+__device__ __forceinline__ double solid_angle(double x, double y, double z, const double* xs, const double* ys,
+                                              const double* zs, const double* dijs, const double* Ss,
+                                              const double* Cs, int nn) {
+  double V3 = 0, dtheta = 2 * kPi;
+  int nR0 = 0;
+#pragma unroll
+  for (int i = 0; i < NNMAX; ++i) {
+    if (i >= nn) break;
+    const int j = (i + 1 == nn) ? 0 : i + 1;
+    const double xi = xs[i], yi = ys[i], zi = zs[i];
+    const double xj = xs[j], yj = ys[j], zj = zs[j];
+    double dij, Sij, Cij;
+    if (dijs) {
+      dij = dijs[i]; Sij = Ss[i]; Cij = Cs[i];
+    } else {
+      dij = sqrt((xj - xi) * (xj - xi) + (yj - yi) * (yj - yi) + (zj - zi) * (zj - zi));
+      Sij = (yj - yi) / dij;
+      Cij = (xj - xi) / dij;
+    }
+    const double ri = sqrt((x - xi) * (x - xi) + (y - yi) * (y - yi) + (z - zi) * (z - zi));
+    const double rj = sqrt((x - xj) * (x - xj) + (y - yj) * (y - yj) + (z - zj) * (z - zj));
+    const double siji = (xi - x) * Cij + (yi - y) * Sij;
+    const double sijj = (xj - x) * Cij + (yj - y) * Sij;
+    const double Rij = (x - xi) * Sij - (y - yi) * Cij;
+    const double Jij = atan2(Rij * fabs(z) * (ri * sijj - rj * siji), ri * rj * Rij * Rij + z * z * sijj * siji);
+    V3 -= Jij;
+    dtheta *= (Rij >= 0);
+    nR0 += (Rij == 0);
+  }
+  V3 += dtheta;
+  V3 *= (z > 0) ? 1.0 : ((z < 0) ? -1.0 : 0.0);
+  V3 *= (double)!(nR0 > 1);
+  return V3 * (1 / (4 * kPi));
+}
+
+// Constant-doublet potential (src/FLOWPanel_elements.jl:751-847).
+__device__ __forceinline__ double doublet_phi(const SourceRec& R, double X1, double X2, double X3) {
+  const double dx = X1 - R.O[0], dy = X2 - R.O[1], dz = X3 - R.O[2];
+  const double x = R.t[0] * dx + R.t[1] * dy + R.t[2] * dz;
+  const double y = R.o[0] * dx + R.o[1] * dy + R.o[2] * dz;
+  const double z = R.n[0] * dx + R.n[1] * dy + R.n[2] * dz;
+  return solid_angle<4>(x, y, z, R.xs, R.ys, R.zs, R.dij, R.S, R.Cc, R.nn);
+}
+
+// Semi-infinite doublet potential along one direction d from the shedding
+// edge (p_i, p_j) (src/FLOWPanel_elements.jl:959-1092, Moran App. F): the
+// bound triangle (p_a, p_i, p_j), p_a the foot of p_j on the line through
+// p_i along d, plus the semi-infinite strip from (p_a, p_j).
+__device__ __forceinline__ double semiinf_doublet_phi(const double* p_i, const double* p_j, const double* d,
+                                                      double X1, double X2, double X3) {
+  const double pijdotd = (p_j[0] - p_i[0]) * d[0] + (p_j[1] - p_i[1]) * d[1] + (p_j[2] - p_i[2]) * d[2];
+  const double pa[3] = {p_i[0] + pijdotd * d[0], p_i[1] + pijdotd * d[1], p_i[2] + pijdotd * d[2]};
+  const double nrm = sqrt((p_j[0] - pa[0]) * (p_j[0] - pa[0]) + (p_j[1] - pa[1]) * (p_j[1] - pa[1]) +
+                          (p_j[2] - pa[2]) * (p_j[2] - pa[2]));
+  const double ex[3] = {d[0], d[1], d[2]};
+  const double ey[3] = {(p_j[0] - pa[0]) / nrm, (p_j[1] - pa[1]) / nrm, (p_j[2] - pa[2]) / nrm};
+  const double ez[3] = {ex[1] * ey[2] - ex[2] * ey[1], ex[2] * ey[0] - ex[0] * ey[2], ex[0] * ey[1] - ex[1] * ey[0]};
+  auto loc = [&](const double* e, double a, double b, double c) {
+    return e[0] * (a - p_i[0]) + e[1] * (b - p_i[1]) + e[2] * (c - p_i[2]);
+  };
+  const double xs[3] = {loc(ex, pa[0], pa[1], pa[2]), loc(ex, p_i[0], p_i[1], p_i[2]), loc(ex, p_j[0], p_j[1], p_j[2])};
+  const double ys[3] = {loc(ey, pa[0], pa[1], pa[2]), loc(ey, p_i[0], p_i[1], p_i[2]), loc(ey, p_j[0], p_j[1], p_j[2])};
+  const double zs[3] = {loc(ez, pa[0], pa[1], pa[2]), loc(ez, p_i[0], p_i[1], p_i[2]), loc(ez, p_j[0], p_j[1], p_j[2])};
+  const double xa = xs[0], ya = ys[0], yb = ys[2];
+  const double x = loc(ex, X1, X2, X3), y = loc(ey, X1, X2, X3), z = loc(ez, X1, X2, X3);
+  double phi = 0;
+  if (fabs(pijdotd) > 2 * 2.220446049250313e-16)
+    phi += solid_angle<3>(x, y, z, xs, ys, zs, nullptr, nullptr, nullptr, 3);
+  double val = atan((yb - y) / z) + atan((yb - y) * (x - xa) / (z * sqrt((x - xa) * (x - xa) + (yb - y) * (yb - y) + z * z)));
+  val -= atan((ya - y) / z) + atan((ya - y) * (x - xa) / (z * sqrt((x - xa) * (x - xa) + (ya - y) * (ya - y) + z * z)));
+  return phi + val * (1 / (4 * kPi));
+}
+
+// Semi-infinite doublet with directions (da, db) (src/FLOWPanel_elements.jl:1110-1244):
+// the da part, plus, when db differs, the triangle (p_b + L da, p_b, p_b + L db)
+// with L = infinitelength.
+__device__ __forceinline__ double semiinf_doublet_phi2(const double* p_a, const double* p_b, const double* da,
+                                                       const double* db, double X1, double X2, double X3,
+                                                       double L) {
+  double phi = semiinf_doublet_phi(p_a, p_b, da, X1, X2, X3);
+  const double e2 = 2 * 2.220446049250313e-16;
+  if (fabs(da[0] - db[0]) > e2 || fabs(da[1] - db[1]) > e2 || fabs(da[2] - db[2]) > e2) {
+    const double pda[3] = {p_b[0] + L * da[0], p_b[1] + L * da[1], p_b[2] + L * da[2]};
+    const double pdb[3] = {p_b[0] + L * db[0], p_b[1] + L * db[1], p_b[2] + L * db[2]};
+    double ez[3] = {da[1] * db[2] - da[2] * db[1], da[2] * db[0] - da[0] * db[2], da[0] * db[1] - da[1] * db[0]};
+    const double nz = sqrt(ez[0] * ez[0] + ez[1] * ez[1] + ez[2] * ez[2]);
+    ez[0] = ez[0] / nz; ez[1] = ez[1] / nz; ez[2] = ez[2] / nz;
+    const double ex[3] = {da[0], da[1], da[2]};
+    const double ey[3] = {ez[1] * ex[2] - ez[2] * ex[1], ez[2] * ex[0] - ez[0] * ex[2], ez[0] * ex[1] - ez[1] * ex[0]};
+    auto loc = [&](const double* e, double a, double b, double c) {
+      return e[0] * (a - p_b[0]) + e[1] * (b - p_b[1]) + e[2] * (c - p_b[2]);
+    };
+    const double xs[3] = {loc(ex, pda[0], pda[1], pda[2]), loc(ex, p_b[0], p_b[1], p_b[2]), loc(ex, pdb[0], pdb[1], pdb[2])};
+    const double ys[3] = {loc(ey, pda[0], pda[1], pda[2]), loc(ey, p_b[0], p_b[1], p_b[2]), loc(ey, pdb[0], pdb[1], pdb[2])};
+    const double zs[3] = {loc(ez, pda[0], pda[1], pda[2]), loc(ez, p_b[0], p_b[1], p_b[2]), loc(ez, pdb[0], pdb[1], pdb[2])};
+    phi += solid_angle<3>(loc(ex, X1, X2, X3), loc(ey, X1, X2, X3), loc(ez, X1, X2, X3), xs, ys, zs, nullptr,
+                          nullptr, nullptr, 3);
+  }
+  return phi;
+}
+
 }  // namespace fpb

@@ -1,7 +1,8 @@
-// Induced velocity of a solved body at arbitrary targets (Uind!):
-// vortex rings with their strengths plus the wake horseshoes with
-// (Gamma_pi, Gamma_pj) (src/FLOWPanel_liftingbody.jl:576-661), or constant
-// sources (src/FLOWPanel_nonliftingbody.jl:188-218).
+// Induced velocity (Uind!) and potential (phi!) of a solved body at arbitrary
+// targets. The velocity sums vortex rings with their strengths plus the wake
+// horseshoes with (Gamma_pi, Gamma_pj) (src/FLOWPanel_liftingbody.jl:576-661),
+// or constant sources (src/FLOWPanel_nonliftingbody.jl:188-218); the
+// potential is k_phi below.
 //
 // One thread per target, panels staged through shared memory; each target
 // adds the panels in the reference's order (panels, then shedding edges) on
@@ -86,6 +87,42 @@ k_uind_source(const SourceRec* __restrict__ recs, const double* __restrict__ str
   out[3 * t] = a;
   out[3 * t + 1] = b;
   out[3 * t + 2] = c;
+}
+
+// Potential phi! of a solved body (one thread per target, FP64): for each
+// panel in order, its source and/or doublet potential scaled by its
+// strengths (sigma, mu), then, for a lifting body, each shedding edge's
+// semi-infinite doublets, (da, db) from the upper panel's TE nodes with mu_pi
+// and (db, da) from the lower's with mu_pj (src/FLOWPanel_liftingbody.jl:664-742).
+__global__ void __launch_bounds__(kFieldThreads)
+k_phi(const SourceRec* __restrict__ recs, const double* __restrict__ sigma, const double* __restrict__ mu,
+      int64_t n, const WakeRec* __restrict__ wake, int64_t nsh, const double* __restrict__ targets, int64_t m,
+      double* __restrict__ out, double offset) {
+  const int64_t t = (int64_t)blockIdx.x * kFieldThreads + threadIdx.x;
+  if (t >= m) return;
+  const double X = targets[3 * t], Y = targets[3 * t + 1], Z = targets[3 * t + 2];
+  double phi = out[t];
+  for (int64_t j = 0; j < n; ++j) {
+    const SourceRec& R = recs[j];
+    if (sigma) phi += sigma[j] * source_phi(R, X, Y, Z, offset);
+    if (mu) phi += mu[j] * doublet_phi(R, X, Y, Z);
+  }
+  for (int64_t e = 0; mu && e < nsh; ++e) {
+    const WakeRec& wr = wake[e];
+    phi += mu[wr.pi] * semiinf_doublet_phi2(wr.pa, wr.pb, wr.da, wr.db, X, Y, Z, 1e12);
+    if (wr.pj >= 0) phi += mu[wr.pj] * semiinf_doublet_phi2(wr.qa, wr.qb, wr.db, wr.da, X, Y, Z, 1e12);
+  }
+  out[t] = phi;
+}
+
+int launch_phi(fp_ctx* c, const double* d_sigma, const double* d_mu, const double* d_targets, int64_t m,
+               double* d_out, bool wake) {
+  const unsigned g = (unsigned)((m + kFieldThreads - 1) / kFieldThreads);
+  k_phi<<<g, kFieldThreads, 0, c->stream>>>(c->d_src, d_sigma, d_mu, c->N, c->d_wake, wake ? c->nsh : 0, d_targets,
+                                              m, d_out, c->kern_offset);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
 }
 
 int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,

@@ -55,6 +55,7 @@ struct fp_ctx {
   int64_t cap_geom = 0; // panel records allocated
   int64_t cap_wake = 0; // wake records allocated
   int64_t nsh = 0;
+  int64_t wake_opposite = -1;           // first shedding edge with da . db <= 0, or -1
   bool wake_disjoint = true;   // every wake column touched by one edge only
   bool has_geometry = false;
   int assembled = -1;          // element kind of the assembled G, -1 none
@@ -178,6 +179,8 @@ constexpr int kGemvSplitHost = 16;
 // induced velocity (fp_field.cu)
 int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
                      double* d_out, bool fp32);
+int launch_phi(fp_ctx* c, const double* d_sigma, const double* d_mu, const double* d_targets, int64_t m,
+               double* d_out, bool wake);
 int launch_uind_source(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
                        double* d_out);
 

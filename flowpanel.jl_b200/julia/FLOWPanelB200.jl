@@ -12,6 +12,7 @@
 const FP_OK = Cint(0)
 const FP_ELEMENT_SOURCE = Cint(0)
 const FP_ELEMENT_VORTEXRING = Cint(1)
+const FP_ELEMENT_SOURCE_DOUBLET = Cint(2)
 const FP_PREC_FP64 = Cint(0)
 const FP_PREC_MIXED = Cint(1)
 const FP_SOLVER_LU = Cint(0)
@@ -152,6 +153,20 @@ function Uind_b200!(self, targets::Matrix{Float64}, out::Matrix{Float64}, solver
         (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{Float64}, Cint, Cdouble, Cdouble),
         solver.ctx, FP_ELEMENT_VORTEXRING, s, targets, size(targets, 2), out, FP_PREC_FP64,
         self.kerneloffset, self.kernelcutoff))
+    return out
+end
+
+"""Device path of phi! (src/FLOWPanel_abstractbody.jl:118-127): adds into out (M). `element`
+is FP_ELEMENT_VORTEXRING for a RigidWakeBody{VortexRing} (wake doublets included, as
+src/FLOWPanel_liftingbody.jl:664-742) or a NonLiftingBody{ConstantDoublet}, FP_ELEMENT_SOURCE
+for NonLiftingBody{ConstantSource}, FP_ELEMENT_SOURCE_DOUBLET for the source+doublet body
+(self.strength N x 2, column-major as Julia holds it)."""
+function phi_b200!(self, targets::Matrix{Float64}, out::Vector{Float64}, solver::B200Solver, element::Cint)
+    s = element == FP_ELEMENT_SOURCE_DOUBLET ? Matrix{Float64}(self.strength[:, 1:2]) :
+                                               Vector{Float64}(self.strength[:, 1])
+    GC.@preserve s targets out fp_check(solver, ccall((:fp_phi, libfp), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{Float64}, Cdouble),
+        solver.ctx, element, s, targets, size(targets, 2), out, self.kerneloffset))
     return out
 end
 

@@ -41,7 +41,10 @@ extern "C" {
 
 /* element kinds */
 #define FP_ELEMENT_SOURCE 0      /* NonLiftingBody{ConstantSource} */
-#define FP_ELEMENT_VORTEXRING 1  /* RigidWakeBody / MultiBody {VortexRing} */
+#define FP_ELEMENT_VORTEXRING 1  /* RigidWakeBody / MultiBody {VortexRing}; NonLiftingBody{ConstantDoublet}
+                                    (the same element without a wake) */
+#define FP_ELEMENT_SOURCE_DOUBLET 2  /* NonLiftingBody{Union{ConstantSource, ConstantDoublet}}: strengths N x 2
+                                        (sources, then doublets); fp_uind and fp_phi only */
 
 /* precision forms */
 #define FP_PREC_FP64 0   /* FP64 assembly + FP64 LU (the plain form) */
@@ -186,11 +189,24 @@ int fp_batch_solve(fp_batch* batch, int element, double kerneloffset, double ker
 
 /* Induced velocity Uind! of the solved body on m targets, accumulated into
  * out (3 x m): vortex rings + wake horseshoes with (Gamma_pi, Gamma_pj)
- * (src/FLOWPanel_liftingbody.jl:576-661) or constant sources
- * (src/FLOWPanel_nonliftingbody.jl:188-218), with the body's kerneloffset and
+ * (src/FLOWPanel_liftingbody.jl:576-661), constant sources
+ * (src/FLOWPanel_nonliftingbody.jl:188-218), or sources then doublets
+ * (FP_ELEMENT_SOURCE_DOUBLET, :719-761), with the body's kerneloffset and
  * kernelcutoff. precision FP_PREC_MIXED evaluates in FP32 (off-body probes). */
 int fp_uind(fp_ctx* ctx, int element, const double* strengths, const double* targets,
             int64_t m, double* out, int precision, double kerneloffset, double kernelcutoff);
+
+/* Potential phi! of the solved body on m targets, accumulated into out (m):
+ * constant sources (src/FLOWPanel_nonliftingbody.jl:221-250), constant
+ * doublets (:388-420, FP_ELEMENT_VORTEXRING without a wake), both
+ * (FP_ELEMENT_SOURCE_DOUBLET, :763-815, strengths N x 2), or vortex rings with
+ * the wake's semi-infinite doublets, (da, db) on the upper TE nodes with the
+ * upper panel's strength and (db, da) on the lower's
+ * (src/FLOWPanel_liftingbody.jl:664-742; elements :152-241, 751-847,
+ * 959-1244). FP64. FP_EINVAL with the reference's message when a shedding
+ * edge's da and db are opposite or orthogonal (:1129-1132). */
+int fp_phi(fp_ctx* ctx, int element, const double* strengths, const double* targets, int64_t m,
+           double* out, double kerneloffset);
 
 /* Adjoint of the linear solve: A^T lambda = ybar with the saved factors (the
  * reverse rule of IAD.implicit_linear at src/FLOWPanel_linearsolver.jl:73:

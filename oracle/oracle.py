@@ -147,6 +147,36 @@ def phi_semiinfinite_doublet(nodes, TE, d, strength, targets, db=None, infinitel
     return out
 
 
+def phi_body(mesh, kind, strengths, targets, Das=None, Dbs=None, offset=1e-8):
+    """phi! of a body at targets (M, 3) -> (M,), by the reference's loops over
+    panels and then shedding edges: constant sources
+    (src/FLOWPanel_nonliftingbody.jl:221-250), constant doublets (:388-420),
+    both with strengths (N, 2) (:763-815), or vortex rings plus the wake's
+    semi-infinite doublets, (da, db) on the upper panel's TE nodes with its
+    strength and (db, da) on the lower's (src/FLOWPanel_liftingbody.jl:664-742).
+    kind: 'source' | 'doublet' | 'source+doublet' | 'vortexring'."""
+    targets = _pts(targets)
+    out = np.zeros(targets.shape[0])
+    s = np.asarray(strengths, float)
+    for i in range(mesh.npanels):
+        pan = mesh.panel(i)
+        if kind == "source":
+            out += phi_constant_source(mesh.nodes, pan, s[i], targets, offset)
+        elif kind == "source+doublet":
+            out += phi_constant_source(mesh.nodes, pan, s[i, 0], targets, offset)
+            out += phi_constant_doublet(mesh.nodes, pan, s[i, 1], targets)
+        else:
+            out += phi_constant_doublet(mesh.nodes, pan, s[i], targets)
+    if kind == "vortexring":
+        for e, (pi, nia, nib, pj, nja, njb) in enumerate(np.asarray(mesh.shedding).reshape(-1, 6)):
+            P = mesh.panel(pi)
+            out += phi_semiinfinite_doublet(mesh.nodes, (P[nia], P[nib]), Das[e], s[pi], targets, db=Dbs[e])
+            if pj != -1:
+                Q = mesh.panel(pj)
+                out += phi_semiinfinite_doublet(mesh.nodes, (Q[nja], Q[njb]), Dbs[e], s[pj], targets, db=Das[e])
+    return out
+
+
 def grad_phi(kind, nodes, panel, strength, X, d=(1.0, 0.0, 0.0), offset=0.0):
     """grad(phi) at X by forward-mode duals. kind: 'source' | 'doublet' | 'semiinfinite'."""
     k = {"source": 0, "doublet": 1, "semiinfinite": 2}[kind]
