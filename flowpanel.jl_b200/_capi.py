@@ -26,7 +26,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
-           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi")
+           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls")
 
 
 class SolveOpts(C.Structure):
@@ -88,6 +88,8 @@ def lib():
                                     C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
         L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
         L.fp_phi.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_double]
+        L.fp_solve_ls.argtypes = [vp, C.c_double, C.c_double, _dp, C.c_int64, C.POINTER(C.c_int64), _dp, _dp,
+                                  C.POINTER(Stats)]
         L.fp_adjoint_solve.argtypes = [vp, _dp, C.c_int64, _dp]
         L.fp_lu_solve_noalloc.argtypes = [vp, C.c_void_p, C.c_int64, C.c_int64]
         L.fp_assembly_vjp.argtypes = [vp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
@@ -227,6 +229,18 @@ class Context:
         self._chk(self._L.fp_uind(self.h, element, _d(_strengths(strengths)), _d(targets), m, _d(out),
                                   precision, kerneloffset, kernelcutoff))
         return out
+
+    def solve_ls(self, Uinfs, elprescribe, kerneloffset=1e-8, kernelcutoff=1e-14):
+        """Least-squares solve of a watertight vortex-ring body (fp_solve_ls);
+        elprescribe: [(index (0-based), value), ...]. Returns (Gamma, Stats)."""
+        U = _f64(np.reshape(Uinfs, (-1, 3)))
+        idx = np.ascontiguousarray([int(i) for i, _ in elprescribe], dtype=np.int64)
+        val = np.ascontiguousarray([float(v) for _, v in elprescribe], dtype=np.float64)
+        x = np.zeros(U.shape[0])
+        st = Stats()
+        self._chk(self._L.fp_solve_ls(self.h, kerneloffset, kernelcutoff, _d(U), len(idx),
+                                      idx.ctypes.data_as(C.POINTER(C.c_int64)), _d(val), _d(x), C.byref(st)))
+        return x, st
 
     def phi(self, element, strengths, targets, out=None, kerneloffset=1e-8):
         """Potential at targets (M, 3) added to out (M,) (fp_phi). strengths: N, or

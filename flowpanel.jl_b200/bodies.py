@@ -88,9 +88,30 @@ class NonLiftingBody(AbstractBody):
 
 
 class RigidWakeBody(AbstractBody):
-    """RigidWakeBody{VortexRing, 1} (src/FLOWPanel_liftingbody.jl:43-134)."""
+    """RigidWakeBody{VortexRing, 1} (src/FLOWPanel_liftingbody.jl:43-134); with
+    watertight=True, RigidWakeBody{VortexRing, 2}, solved by least squares with
+    prescribed strengths (:236-447)."""
     kind = "vortexring"
     element = _capi.FP_ELEMENT_VORTEXRING
+
+    def __init__(self, mesh: Mesh, *args, watertight=False, **kwargs):
+        self.watertight = watertight
+        super().__init__(mesh, *args, **kwargs)
+
+
+def calc_elprescribe(body: AbstractBody):
+    """The default prescribed strengths of a least-squares solve, 0-based:
+    the first panel of a watertight body at 0 (calc_elprescribe,
+    src/FLOWPanel_liftingbody.jl:283), and for a MultiBody the first panel of
+    each watertight member (src/FLOWPanel_multibody.jl:565-600)."""
+    if isinstance(body, MultiBody):
+        out, k = [], 0
+        for b in body.bodies:
+            if getattr(b, "watertight", False):
+                out.append((k, 0.0))
+            k += b.ncells
+        return out
+    return [(0, 0.0)] if getattr(body, "watertight", False) else []
 
 
 class MultiBody(AbstractBody):
@@ -237,13 +258,17 @@ class B200Solver:
         self.ctx.close()
 
 
-def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200Solver] = None):
+def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200Solver] = None,
+          elprescribe=None):
     """solve(body, Uinfs[, Das, Dbs]; solver): assemble, factor and solve on the
     GPU, then store the strengths and the fields like the reference. A
     source+doublet NonLiftingBody follows its reference method
     (src/FLOWPanel_nonliftingbody.jl:425-600): sigma = -Uinf . n and
     mu = the potential of the sources of strength -sigma at the control points;
-    like the reference it returns mu and stores nothing."""
+    like the reference it returns mu and stores nothing. A watertight
+    vortex-ring body (or a MultiBody with watertight members, or any
+    ``elprescribe`` given: [(0-based index, value), ...]) is solved by least
+    squares (fp_solve_ls, src/FLOWPanel_liftingbody.jl:236-447)."""
     Uinfs = np.asarray(Uinfs, dtype=np.float64)
     if Uinfs.shape != (body.ncells, 3):
         raise ValueError(f"Invalid Uinfs; expected size ({body.ncells}, 3), got {Uinfs.shape}")
@@ -269,7 +294,13 @@ def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200So
         solver.ctx.set_wake(body.mesh.shedding, Das, Dbs)
     elif lifting:
         solver.ctx.set_wake(np.zeros((0, 6), np.int32), np.zeros((0, 3)), np.zeros((0, 3)))
-    x, st = solver.ctx.solve_body(body.element, Uinfs, body.kerneloffset, body.kernelcutoff, solver.opts)
+    ls = lifting and (elprescribe is not None or getattr(body, "watertight", False) or
+                      (isinstance(body, MultiBody) and any(getattr(b, "watertight", False) for b in body.bodies)))
+    if ls:
+        pres = calc_elprescribe(body) if elprescribe is None else list(elprescribe)
+        x, st = solver.ctx.solve_ls(Uinfs, pres, body.kerneloffset, body.kernelcutoff)
+    else:
+        x, st = solver.ctx.solve_body(body.element, Uinfs, body.kerneloffset, body.kernelcutoff, solver.opts)
     solver.stats = st.asdict()
     body.strength = np.array(x, dtype=np.float64)
     body.solved = True

@@ -23,6 +23,18 @@ int num_sms() {   // of the current device, cached per device
   }
   return sms;
 }
+
+// Device staging buffer of at least n doubles, kept across calls (no
+// allocation in the steady state of repeated solves / field evaluations).
+int ensure_stage(fp_ctx* c, size_t n) {
+  if (n <= c->cap_stage) return FP_OK;
+  if (c->d_stage) cudaFree(c->d_stage);
+  c->d_stage = nullptr;
+  c->cap_stage = 0;
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_stage, n * sizeof(double)));
+  c->cap_stage = n;
+  return FP_OK;
+}
 }  // namespace fpb
 
 namespace {
@@ -77,16 +89,6 @@ int ensure_rhs(fp_ctx* c, int64_t k) {
   return FP_OK;
 }
 
-// Device staging buffer of at least n doubles, kept across calls (no
-// allocation in the steady state of repeated solves / field evaluations).
-int ensure_stage(fp_ctx* c, size_t n) {
-  if (n <= c->cap_stage) return FP_OK;
-  dfree(c->d_stage);
-  c->cap_stage = 0;
-  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_stage, n * sizeof(double)));
-  c->cap_stage = n;
-  return FP_OK;
-}
 
 int time_begin(fp_ctx* c) {
   FP_CUDA_TRY(c->err, cudaEventRecord(c->ev0, c->stream));
@@ -662,6 +664,53 @@ int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targe
   c->klaunch[FP_STAGE_UIND] = 1;
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(out, dout, 3 * m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
+  return FP_OK;
+}
+
+int fp_solve_ls(fp_ctx* c, double kerneloffset, double kernelcutoff, const double* Uinfs, int64_t npres,
+                const int64_t* el_index, const double* el_value, double* x, fp_stats* stats) {
+  if (check_ctx(c)) return FP_EINVAL;
+  cudaSetDevice(c->device);
+  if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_solve_ls: no geometry");
+  if (!Uinfs || !x || npres < 0 || npres >= c->N || (npres > 0 && (!el_index || !el_value)))
+    return c->err.set(FP_EINVAL, "fp_solve_ls: bad arguments");
+  // prescribed elements sorted by index (src/FLOWPanel_liftingbody.jl:399)
+  std::vector<std::pair<int64_t, double>> pres(npres);
+  for (int64_t p = 0; p < npres; ++p) pres[p] = {el_index[p], el_value[p]};
+  std::sort(pres.begin(), pres.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::vector<int> el(npres);
+  std::vector<double> val(npres);
+  for (int64_t p = 0; p < npres; ++p) {
+    if (pres[p].first < 0 || pres[p].first >= c->N || (p > 0 && pres[p].first == pres[p - 1].first))
+      return c->err.set(FP_EINVAL, "fp_solve_ls: prescribed element indices must be distinct and in 0..N-1");
+    el[p] = (int)pres[p].first;
+    val[p] = pres[p].second;
+  }
+  int rc;
+  if ((rc = fp_assemble(c, FP_ELEMENT_VORTEXRING, kerneloffset, kernelcutoff, FP_PREC_FP64))) return rc;
+  if ((rc = fp_set_rhs(c, Uinfs, 1))) return rc;
+  if ((rc = alloc_factor_buffers(c, FP_PREC_FP64))) return rc;
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_cert, 0, sizeof(float), c->stream));
+  std::vector<double> g(c->N - npres);
+  if (time_begin(c)) return FP_ECUDA;
+  if ((rc = ls_solve(c, el.data(), val.data(), (int)npres, g.data()))) return rc;
+  if (time_end(c, &c->ms_factor)) return FP_ECUDA;
+  c->factored = -1;   // the FP64 factor buffer now holds the normal equations' factors
+  c->nrhs = 0;
+  if ((rc = consume_status(c))) return rc;
+  // set_solution: the reduced strengths around the prescribed values
+  for (int64_t j = 0, p = 0, q = 0; j < c->N; ++j) {
+    if (p < npres && el[p] == j) x[j] = val[p++];
+    else x[j] = g[q++];
+  }
+  float cert = 0.f;
+  FP_CUDA_TRY(c->err, cudaMemcpy(&cert, c->d_cert, sizeof(float), cudaMemcpyDeviceToHost));
+  c->last = fp_stats{};
+  c->last.ms_assemble = c->ms_assemble;
+  c->last.ms_factor = c->ms_factor;
+  c->last.max_abs_L = cert;
+  c->last.gepp_certified = cert <= 1.0f;
+  if (stats) *stats = c->last;
   return FP_OK;
 }
 

@@ -179,6 +179,10 @@ constexpr int kGemvSplitHost = 16;
 // induced velocity (fp_field.cu)
 int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
                      double* d_out, bool fp32);
+int ensure_stage(fp_ctx* c, size_t n);   // the staging buffer holds at least n doubles
+// least squares of a watertight vortex-ring body (fp_ls.cu): Gamma_red of the
+// normal equations with the prescribed columns (sorted, distinct) removed
+int ls_solve(fp_ctx* c, const int* h_el, const double* h_val, int npres, double* h_gamma_red);
 int launch_phi(fp_ctx* c, const double* d_sigma, const double* d_mu, const double* d_targets, int64_t m,
                double* d_out, bool wake);
 int launch_uind_source(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,

@@ -196,6 +196,18 @@ int fp_batch_solve(fp_batch* batch, int element, double kerneloffset, double ker
 int fp_uind(fp_ctx* ctx, int element, const double* strengths, const double* targets,
             int64_t m, double* out, int precision, double kerneloffset, double kernelcutoff);
 
+/* Least-squares solve of a watertight vortex-ring body, the
+ * RigidWakeBody{VortexRing, 2} / MultiBody{VortexRing, 2} method
+ * (src/FLOWPanel_liftingbody.jl:236-447, src/FLOWPanel_multibody.jl:373-617):
+ * assembles G (with the wake set by fp_set_wake), moves the npres prescribed
+ * strengths (0-based el_index, values el_value; sorted here, distinct) to the
+ * right-hand side, solves the normal equations Gred^T Gred Gamma = Gred^T r
+ * in FP64 with LU (solve_ludiv!, the default solver) and writes Gamma (N) with
+ * the prescribed values in place (set_solution). Leaves no usable factors of
+ * G (call fp_factor again before fp_solve). */
+int fp_solve_ls(fp_ctx* ctx, double kerneloffset, double kernelcutoff, const double* Uinfs, int64_t npres,
+                const int64_t* el_index, const double* el_value, double* x, fp_stats* stats);
+
 /* Potential phi! of the solved body on m targets, accumulated into out (m):
  * constant sources (src/FLOWPanel_nonliftingbody.jl:221-250), constant
  * doublets (:388-420, FP_ELEMENT_VORTEXRING without a wake), both

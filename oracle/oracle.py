@@ -359,6 +359,29 @@ def solve_ludiv(G, b):
     return lu_solve(lu_factor(G), b)
 
 
+def solve_leastsquares(G, rhs, elprescribe):
+    """The least-squares solve of a watertight vortex-ring body with the AIC G
+    and RHS = -Uinf . n: prescribed strengths moved to the right-hand side,
+    their columns dropped, normal equations Gred^T Gred Gamma = Gred^T r
+    solved by LU (solve_ludiv!), the prescribed values put back
+    (_G_U_RHS_leastsquares! and set_solution, src/FLOWPanel_liftingbody.jl:285-447).
+    elprescribe: [(0-based index, value)]."""
+    pres = sorted(elprescribe, key=lambda t: t[0])
+    r = np.array(rhs, float)
+    for i, v in pres:
+        r = r - v * G[:, i]
+    keep = np.setdiff1d(np.arange(G.shape[1]), [i for i, _ in pres])
+    Gred = G[:, keep]
+    tGred = np.ascontiguousarray(Gred.T)
+    Gls = tGred @ Gred
+    g = solve_ludiv(Gls, tGred @ r)
+    out = np.zeros(G.shape[1])
+    out[keep] = g
+    for i, v in pres:
+        out[i] = v
+    return out, Gls
+
+
 def gmres(A, b, memory=50, atol=None, rtol=None, itmax=None, x0=None):
     """Restarted GMRES(memory) restating Krylov.jl 0.9's algorithm as the reference
     calls it (src/FLOWPanel_linearsolver.jl:136-147): modified Gram-Schmidt
