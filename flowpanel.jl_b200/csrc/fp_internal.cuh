@@ -170,7 +170,8 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda);
 int lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k);
 int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out);
 constexpr int kLuNB = 64;        // block size of the factorisation and the solves
-constexpr int kPanelSlots = 4;   // blocks per outer panel of the factorisation
+constexpr int kOuterPanel = 256;  // columns per outer panel of the factorisation
+constexpr int kPanelSlots = kOuterPanel / kLuNB;   // blocks per outer panel
 constexpr size_t kMinvBytes = (size_t)2 * kPanelSlots * kLuNB * kLuNB * sizeof(double);   // two sets
 // split-operand scratch of the tensor-core update for scratch set `slot` (fp_tc.cu)
 int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max);

@@ -546,7 +546,7 @@ k_pfix(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk, const
 // written in place and read back by the later blocks. Every product is a
 // 64 x 64 x 32 tile product from shared memory with a rolled K loop, so the
 // code stays small. One CTA owns 32 columns.
-constexpr int kStripRows = 256;
+constexpr int kStripRows = kOuterPanel;
 constexpr int kStripCols = 32;
 constexpr int kStripThreads = 256;
 template <class T> __host__ __device__ constexpr int strip_qpitch() { return kStripCols + 16 / (int)sizeof(T); }
@@ -854,7 +854,7 @@ int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64
 // so a strip of columns outside P first receives all of P's swaps and only
 // then the per-block substitutions and updates (k_strip). Columns are split between the
 // streams so that no element is written by both at once.
-constexpr int kOuterNB = 256;
+constexpr int kOuterNB = kOuterPanel;
 
 // Routes the launches of a section to stream2 and its tensor-core scratch.
 struct OnStream2 {

@@ -317,9 +317,9 @@ static bool make_map_c(CUtensorMap* tm, float* C, int64_t m, int64_t n, int64_t 
 
 }  // namespace tc
 
-// Scratch for the split operands: 4 x N x 256 floats.
+// Scratch for the split operands: 4 x N x kOuterPanel floats.
 int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max) {
-  const size_t need = (size_t)rows_max * 256;
+  const size_t need = (size_t)rows_max * kOuterPanel;
   if (c->tc_cap[slot] >= need) return FP_OK;
   for (int i = 0; i < 4; ++i) {
     if (c->d_tc[slot][i]) cudaFree(c->d_tc[slot][i]);
@@ -333,7 +333,7 @@ int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max) {
 
 bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
                      int64_t nn, int kk) {
-  if (!c->use_tc || kk <= 0 || kk > 256 || m <= 0 || nn <= 0) return false;
+  if (!c->use_tc || kk <= 0 || kk > kOuterPanel || m <= 0 || nn <= 0) return false;
   if (!tc::encode_fn()) return false;
   // the reduce-add needs a 16-byte aligned C and column pitch
   if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(lda * 4)) & 15) != 0) return false;
@@ -408,7 +408,7 @@ int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64
 extern "C" int fp_tc_selftest(int device, int64_t m, int64_t n, int k, double* err_tc, double* err_simt,
                               double* ms_tc) {
   using namespace fpb;
-  if (m <= 0 || n <= 0 || k <= 0 || k > 256 || !err_tc || !err_simt || !ms_tc) return FP_EINVAL;
+  if (m <= 0 || n <= 0 || k <= 0 || k > kOuterPanel || !err_tc || !err_simt || !ms_tc) return FP_EINVAL;
   fp_ctx* c = nullptr;
   if (int rc = fp_ctx_create(device, &c)) return rc;
   const int64_t ld = round_up(std::max<int64_t>(m, k), 64);
