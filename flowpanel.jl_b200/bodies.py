@@ -335,9 +335,11 @@ def solve_batch(bodies: List[AbstractBody], Uinfs, Das=None, Dbs=None, method="l
         U = np.asarray(Uinfs[i], dtype=np.float64)
         if U.shape != (b.ncells, 3):
             raise ValueError(f"Invalid Uinfs of body {i}; expected size ({b.ncells}, 3), got {U.shape}")
-        normals = calc_normals(b)
-        p = dict(nodes=b.mesh.nodes, panel_offsets=b.mesh.panel_offsets, panel_nodes=b.mesh.panel_nodes,
-                 Uinfs=U, normals=normals, cps=calc_controlpoints(b, normals))
+        p = dict(nodes=b.mesh.nodes, panel_offsets=b.mesh.panel_offsets, panel_nodes=b.mesh.panel_nodes, Uinfs=U)
+        if isinstance(b, MultiBody) or b.CPoffset != 1e-14 or b.characteristiclength is not None:
+            normals = calc_normals(b)
+            p.update(normals=normals, cps=calc_controlpoints(b, normals))
+        # else: the library's worker threads form them (the default offset 1e-14, l = 1)
         if lifting:
             p.update(shedding=b.mesh.shedding, Das=np.asarray(Das[i], float), Dbs=np.asarray(Dbs[i], float))
         problems.append(p)
