@@ -352,13 +352,22 @@ __device__ __forceinline__ void mm4x4(const T (*P)[PP], const T (*Q)[QP], int r0
 }
 
 template <class T>
+__device__ void pfix_task(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk,
+                          const T* __restrict__ Minv, const int* __restrict__ rowat, int task, unsigned char* smem);
+
+template <class T>
 __global__ void __launch_bounds__(kBlkThreads, sizeof(T) == 4 ? 3 : 2)
 k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const T* __restrict__ Minv,
       float* __restrict__ cert, int next, int32_t* __restrict__ ipiv, int* __restrict__ status,
-      T* __restrict__ Minv_next, int* __restrict__ rowat_next, unsigned* __restrict__ ticket) {
+      T* __restrict__ Minv_next, int* __restrict__ rowat_next, unsigned* __restrict__ ticket, int nmain,
+      int64_t K0, int nblk, const T* __restrict__ slots, const int* __restrict__ rowat) {
   typedef typename V16<T>::type VT;
   constexpr int V = V16<T>::n, RP = rpitch<T>(), LP = blk_lpitch<T>();
   extern __shared__ __align__(16) unsigned char bsm[];
+  if ((int)blockIdx.x >= nmain) {   // extra CTAs of a panel's last block: the panel's fix-up tasks
+    pfix_task<T>(A, lda, K0, kend, nblk, slots, rowat, (int)blockIdx.x - nmain, bsm);
+    return;
+  }
   T (*Bs)[RP] = reinterpret_cast<T (*)[RP]>(bsm);   // shifted U11 rows, then M', then A12 chunks
   T (*Ls)[LP] = reinterpret_cast<T (*)[LP]>(bsm + (size_t)NB * RP * sizeof(T));   // L21, then W: [column][row]
   T* rd = reinterpret_cast<T*>(bsm + (size_t)NB * RP * sizeof(T) + (size_t)NB * LP * sizeof(T));
@@ -462,7 +471,7 @@ k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const 
   // panel) is final once the CTAs owning its rows are done: the last of them
   // (ticket) factors it while the other CTAs still update, so the next
   // block's step can start as soon as this launch ends.
-  const unsigned owners = (unsigned)imin64(NB / kBlkRows, gridDim.x);
+  const unsigned owners = (unsigned)imin64(NB / kBlkRows, nmain);
   if (!next || blockIdx.x >= owners) return;
   __shared__ unsigned last;
   __threadfence();   // this CTA's stores, visible device-wide before its ticket
@@ -487,20 +496,23 @@ k_blk(T* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t kend, const 
 // right of it, in place (nothing reads these parts before: the blocks' own
 // steps use L21 and A12 as they lie). Task t of nblk (nblk - 1): block
 // b = t / (nblk - 1), i = t % (nblk - 1); i < b: left chunk i, else right
-// chunk i - b; 64 columns per task.
-constexpr int kPfixThreads = 256;
-template <class T> constexpr size_t pfix_smem() { return (size_t)2 * NB * rpitch<T>() * sizeof(T) + 64; }
+// chunk i - b; 64 columns per task. The panel's last k_blk runs these tasks
+// in extra CTAs (its own work touches none of these parts); k_pfix runs them
+// when that block has no rows below it (the matrix's last block).
+constexpr int kPfixThreads = 128;
+constexpr int kPfixKC = 16;   // rows of M' staged at a time
+template <class T> __host__ __device__ constexpr size_t pfix_smem() {
+  return (size_t)(NB + kPfixKC) * rpitch<T>() * sizeof(T) + 64;
+}
 
 template <class T>
-__global__ void __launch_bounds__(kPfixThreads)
-k_pfix(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk, const T* __restrict__ Minv,
-       const int* __restrict__ rowat) {
+__device__ void pfix_task(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk,
+                          const T* __restrict__ Minv, const int* __restrict__ rowat, int task, unsigned char* smem) {
   constexpr int RP = rpitch<T>();
-  extern __shared__ __align__(16) unsigned char psm[];
-  T (*X)[RP] = reinterpret_cast<T (*)[RP]>(psm);                                 // X[row j][column]
-  T (*Mt)[RP] = reinterpret_cast<T (*)[RP]>(psm + (size_t)NB * RP * sizeof(T));   // Mt[j][r] = M'(r, j)
+  T (*X)[RP] = reinterpret_cast<T (*)[RP]>(smem);                                 // X[row j][column]
+  T (*Ms)[RP] = reinterpret_cast<T (*)[RP]>(smem + (size_t)NB * RP * sizeof(T));   // Ms[jj][r] = M'(r, j0 + jj)
   const int tid = threadIdx.x;
-  const int b = (int)blockIdx.x / (nblk - 1), i = (int)blockIdx.x % (nblk - 1);
+  const int b = task / (nblk - 1), i = task % (nblk - 1);
   const int64_t kb = K0 + (int64_t)b * NB;
   const int nbb = (int)imin64(NB, kend - kb);
   const bool left = i < b;
@@ -520,19 +532,47 @@ k_pfix(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk, const
     return;
   }
   const T* M = Minv + (size_t)b * NB * NB;
-  stage_block<kPfixThreads, T>(
-      tid, [&](int j, int r) { return M[r * NB + j]; }, [&](int j, int r, T v) { Mt[j][r] = v; });
-  __syncthreads();
-  const int rg = tid & 15, cg = tid >> 4;
-  T acc[4][4] = {};
-  mm4x4<T, RP, RP>(Mt, X, 4 * rg, 4 * cg, acc);
+  const int rg = tid & 15, cg = tid >> 4;   // rows 4 rg.., columns 8 cg..
+  T acc[4][8] = {};
+  for (int j0 = 0; j0 < NB; j0 += kPfixKC) {
+    __syncthreads();
+    for (int e = tid; e < kPfixKC * NB; e += kPfixThreads) {
+      const int jj = e % kPfixKC, r = e / kPfixKC;
+      Ms[jj][r] = M[r * NB + j0 + jj];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int jj = 0; jj < kPfixKC; ++jj) {
+      T a[4], q[8];
 #pragma unroll
-  for (int l = 0; l < 4; ++l) {
-    const int cc = 4 * cg + l;
+      for (int u = 0; u < 4; ++u) a[u] = Ms[jj][4 * rg + u];
+#pragma unroll
+      for (int l = 0; l < 8; ++l) q[l] = X[j0 + jj][8 * cg + l];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int l = 0; l < 8; ++l) acc[u][l] += a[u] * q[l];
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < 8; ++l) {
+    const int cc = 8 * cg + l;
     if (cc >= nc) continue;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) A[(c0 + cc) * lda + (kb + 4 * rg + r)] = acc[r][l];
+    for (int u = 0; u < 4; ++u) A[(c0 + cc) * lda + (kb + 4 * rg + u)] = acc[u][l];
   }
+}
+
+static_assert(kPfixThreads == kBlkThreads && pfix_smem<float>() <= blk_smem<float>() &&
+                  pfix_smem<double>() <= blk_smem<double>(),
+              "the extra CTAs of k_blk run pfix_task");
+
+template <class T>
+__global__ void __launch_bounds__(kPfixThreads)
+k_pfix(T* __restrict__ A, int64_t lda, int64_t K0, int64_t kend, int nblk, const T* __restrict__ Minv,
+       const int* __restrict__ rowat) {
+  extern __shared__ __align__(16) unsigned char psm[];
+  pfix_task<T>(A, lda, K0, kend, nblk, Minv, rowat, (int)blockIdx.x, psm);
 }
 
 // ----------------------------------------------------------------------------
@@ -911,6 +951,8 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
     const int64_t kend = std::min<int64_t>(K0 + kOuterNB, n);
     const int64_t knext = std::min<int64_t>(kend + kOuterNB, n);   // next panel: columns [kend, knext)
     // (1) factor the panel's columns, full height
+    const int nblk = (int)((kend - K0 + NB - 1) / NB);
+    bool fixed = false;   // the panel's fix-up ran in its last k_blk
     for (int64_t k = K0; k < kend; k += NB) {
       const int nb = (int)std::min<int64_t>(NB, n - k);
       const int64_t below = n - k - nb;
@@ -925,18 +967,22 @@ int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cer
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
       if (below > 0) {   // then nb == NB
-        const unsigned g = (unsigned)((below + kBlkRows - 1) / kBlkRows);
+        const int nmain = (int)((below + kBlkRows - 1) / kBlkRows);
         const int next = k + NB < kend;
+        // the panel's last block also runs the panel's fix-up tasks
+        const int fix = (!next && nblk > 1) ? nblk * (nblk - 1) : 0;
+        if (fix) fixed = true;
+        const unsigned g = (unsigned)(nmain + fix);
         TraceScope tr(c, TR_L21);
         k_blk<T><<<g, kBlkThreads, blk_smem<T>(), c->stream>>>(A, lda, n, k, kend, mv + slot * NB * NB, cert, next,
                                                                ipiv, c->d_status, mv + (slot + 1) * NB * NB,
-                                                               ra + (slot + 1) * NB, c->d_ticket);
+                                                               ra + (slot + 1) * NB, c->d_ticket, nmain, K0, nblk,
+                                                               mv, ra);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
     }
-    const int nblk = (int)((kend - K0 + NB - 1) / NB);
-    if (nblk > 1) {
+    if (nblk > 1 && !fixed) {
       TraceScope tr(c, TR_U12);
       k_pfix<T><<<(unsigned)(nblk * (nblk - 1)), kPfixThreads, pfix_smem<T>(), c->stream>>>(A, lda, K0, kend, nblk,
                                                                                           pminv(K0), prowat(K0));
