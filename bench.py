@@ -149,6 +149,35 @@ def batch_throughput(fp, device, nwings=64, nslots=8, reps=2):
     return out
 
 
+def surface_loads_timing(fp, reps=5):
+    """The post-processing of the reference's examples on the triangulated
+    12k wing (100 x 60 quads split in 12,000 triangles, the reference's cell
+    type): U at the control points, + grad(mu), Cp with the Kutta average, F
+    and L/D/S in one fp_surface_loads call. Device time of the call's
+    kernels (median of reps) and the induced-velocity share of it."""
+    cap = fp._capi
+    m = fp.meshes.triangulate(fp.meshes.swept_wing("0012", N_CHORD, N_SPAN // 2, chord=1.0, b=B_SPAN, sweep=45.0))
+    body = fp.RigidWakeBody(m)
+    V = np.array([np.cos(np.deg2rad(AOA)), 0.0, np.sin(np.deg2rad(AOA))])
+    D = np.tile(V, (m.nsheddings, 1))
+    solver = fp.B200Solver(precision="mixed")
+    fp.solve(body, np.tile(V, (m.npanels, 1)), D, D, solver=solver)
+    Shat = np.array([0.0, 1.0, 0.0])
+    Lhat = np.cross(V, Shat)
+    ms, ug = [], []
+    for k in range(reps + 2):
+        fp.surface_loads(body, 1.0, 1.225, Lhat, V, Shat, solver=solver)
+        t, launches = solver.ctx.last_kernel_ms(cap.FP_STAGE_POST)
+        solver.ctx.ugradmu(cap.FP_UGRADMU_COMBINED, body.strength, None)
+        if k >= 2:
+            ms.append(t)
+            ug.append(solver.ctx.last_kernel_ms(cap.FP_STAGE_POST)[0])
+    solver.close()
+    return {"config": f"triangulated swept wing, {m.npanels} triangles, {m.nsheddings} shedding edges",
+            "surface_loads_ms": float(np.median(ms)), "launches": launches,
+            "ugradmu_ms": float(np.median(ug))}
+
+
 def measured_peak(key, fallback):
     """A peak from MEASURED_PEAKS.json (driver-measured on this pool), else
     the stated fallback."""
@@ -344,6 +373,7 @@ def run_ours(args, rank, ws, dist):
     achieved = ops / (stg_d[0] * 1e-3) / 1e12
     d_launches, d_ms, d_flops, _ = ktime["fp64"]
     batched = batch_throughput(fp, device) if not args.no_batch else None
+    post = surface_loads_timing(fp)
     cpu = None
     if not args.no_cpu_baseline:
         O = ge.load_oracle()
@@ -388,6 +418,7 @@ def run_ours(args, rank, ws, dist):
             "fp64_trailing_update": {"kernel": "k_gemm_sub<double> (SIMT FP64)", "launches": d_launches,
                                      "ms_total": d_ms, "tflops": d_flops / (d_ms * 1e-3) / 1e12 if d_ms else 0},
             "batched_wings": batched,
+            "surface_loads": post,
             "clocks": clk.summary()}
     if cpu:
         line["cpu_baseline"] = cpu

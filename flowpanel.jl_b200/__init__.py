@@ -2,18 +2,20 @@
 
 Host mirror of the reference's ``solve`` / ``calcfield_*`` API over the C ABI
 of ``include/flowpanel_b200.h`` (kernels in ``csrc/``); synthetic workload
-meshes in ``meshes``. Import name: ``flowpanel_b200`` (loaded from this
+meshes in ``meshes``, mesh files and trailing-edge detection in ``meshio``. Import name: ``flowpanel_b200`` (loaded from this
 directory by ``__graft_entry__.load_package``).
 """
-from . import _capi, meshes  # noqa: F401
-from .bodies import (B200Solver, MultiBody, NonLiftingBody, RigidWakeBody, Uind,  # noqa: F401
+from . import _capi, meshes, meshio  # noqa: F401
+from .bodies import (B200Solver, MultiBody, NonLiftingBody, RigidWakeBody, Uind, addfields,  # noqa: F401
                      calc_areas, calc_controlpoints, calc_normals, calcfield_Cp, calcfield_F,
-                     calcfield_LDS, calcfield_U, phi, solve, solve_batch)
+                     calcfield_LDS, calcfield_U, calcfield_Ugradmu, calcfield_Ugradmu_cell,
+                     calcfield_Ugradmu_node, phi, solve, solve_batch, surface_loads)
 
 __all__ = ["B200Solver", "MultiBody", "NonLiftingBody", "RigidWakeBody", "solve", "solve_batch", "Uind", "phi",
            "calcfield_U",
-           "calcfield_Cp", "calcfield_F", "calcfield_LDS", "calc_normals", "calc_controlpoints",
-           "calc_areas", "meshes"]
+           "calcfield_Cp", "calcfield_F", "calcfield_LDS", "calcfield_Ugradmu", "calcfield_Ugradmu_cell",
+           "calcfield_Ugradmu_node", "addfields", "surface_loads", "calc_normals", "calc_controlpoints",
+           "calc_areas", "meshes", "meshio"]
 
 
 def __getattr__(name):

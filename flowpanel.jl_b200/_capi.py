@@ -18,7 +18,8 @@ FP_OK, FP_EINVAL, FP_ESINGULAR, FP_ENOCONV, FP_ECUDA, FP_ETIMEOUT, FP_ESTATE = r
 FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING, FP_ELEMENT_SOURCE_DOUBLET = 0, 1, 2
 FP_PREC_FP64, FP_PREC_MIXED = 0, 1
 FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
-FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP = range(6)
+FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP, FP_STAGE_POST = range(7)
+FP_UGRADMU_COMBINED, FP_UGRADMU_CELL, FP_UGRADMU_NODE = 0, 1, 2
 
 # every symbol the header declares
 EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count", "fp_set_geometry",
@@ -26,7 +27,8 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_solve_body", "fp_uind", "fp_adjoint_solve", "fp_last_kernel_ms", "fp_measure_fma_peak",
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
-           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls")
+           "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls",
+           "fp_ugradmu", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads")
 
 
 class SolveOpts(C.Structure):
@@ -88,6 +90,12 @@ def lib():
                                     C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
         L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
         L.fp_phi.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_double]
+        L.fp_ugradmu.argtypes = [vp, C.c_int, _dp, _dp, C.c_double, C.c_int, C.c_double, _dp, _dp, _dp]
+        L.fp_calcfield_cp.argtypes = [vp, _dp, C.c_double, C.c_int, _dp]
+        L.fp_calcfield_f.argtypes = [vp, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
+        L.fp_calcfield_lds.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
+        L.fp_surface_loads.argtypes = [vp, C.c_int, _dp, _dp, _dp, C.c_double, C.c_double, C.c_int, C.c_double,
+                                       C.c_double, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
         L.fp_solve_ls.argtypes = [vp, C.c_double, C.c_double, _dp, C.c_int64, C.POINTER(C.c_int64), _dp, _dp,
                                   C.POINTER(Stats)]
         L.fp_adjoint_solve.argtypes = [vp, _dp, C.c_int64, _dp]
@@ -251,6 +259,56 @@ class Context:
         self._chk(self._L.fp_phi(self.h, element, _d(_strengths(strengths)), _d(targets), m, _d(out),
                                  kerneloffset))
         return out
+
+    def ugradmu(self, scheme, strength, cp_offset=None, anglecrit=30.0, force_cellTE=True, maxgrad=np.inf,
+                out=None, want_parts=False):
+        """grad(mu) surface velocity (fp_ugradmu) of the loaded triangular body:
+        scheme FP_UGRADMU_COMBINED / _CELL / _NODE; returns out (N, 3), with
+        (out, out_cell, out_node) when want_parts (combined scheme only)."""
+        g = _f64(strength)
+        n = g.shape[0]
+        out = np.zeros((n, 3)) if out is None else np.ascontiguousarray(out, dtype=np.float64)
+        oc = np.zeros((n, 3)) if want_parts else None
+        on = np.zeros((n, 3)) if want_parts else None
+        self._chk(self._L.fp_ugradmu(self.h, scheme, _d(g), _d(_f64(cp_offset)), float(anglecrit),
+                                     int(bool(force_cellTE)), float(maxgrad), _d(out), _d(oc), _d(on)))
+        return (out, oc, on) if want_parts else out
+
+    def calcfield_cp(self, Us, Uref, correct_kutta=True, out=None):
+        Us = _f64(np.reshape(Us, (-1, 3)))
+        out = np.zeros(Us.shape[0]) if out is None else np.ascontiguousarray(out, dtype=np.float64)
+        self._chk(self._L.fp_calcfield_cp(self.h, _d(Us), float(Uref), int(bool(correct_kutta)), _d(out)))
+        return out
+
+    def calcfield_f(self, Cps, Uinf, rho, cp_offset=None, correct_kutta=True, out=None):
+        Cps = _f64(Cps)
+        out = np.zeros((Cps.shape[0], 3)) if out is None else np.ascontiguousarray(out, dtype=np.float64)
+        self._chk(self._L.fp_calcfield_f(self.h, _d(Cps), _d(_f64(cp_offset)), float(Uinf), float(rho),
+                                         int(bool(correct_kutta)), _d(out)))
+        return out
+
+    def calcfield_lds(self, Fs, Lhat, Dhat, Shat, out=None):
+        """Returns the 3 x 3 matrix of lift, drag and sideslip vectors (columns)."""
+        Fs = _f64(np.reshape(Fs, (-1, 3)))
+        o = np.zeros(9) if out is None else np.ascontiguousarray(np.asarray(out, float).T).ravel()
+        self._chk(self._L.fp_calcfield_lds(self.h, _d(Fs), _d(_f64(Lhat)), _d(_f64(Dhat)), _d(_f64(Shat)),
+                                           _d(o)))
+        return o.reshape(3, 3).T.copy()
+
+    def surface_loads(self, element, strengths, Uinfs, Uref, rho, Lhat, Dhat, Shat, cp_offset=None,
+                      kerneloffset=1e-8, kernelcutoff=1e-14, ugradmu=True, correct_kutta=True, want_U=True):
+        """fp_surface_loads: (U, Cp, F, LDS) of the solved body."""
+        U0 = _f64(np.reshape(Uinfs, (-1, 3)))
+        n = U0.shape[0]
+        U = np.empty((n, 3)) if want_U else None
+        Cp = np.empty(n)
+        F = np.empty((n, 3))
+        lds = np.empty(9)
+        self._chk(self._L.fp_surface_loads(self.h, element, _d(_strengths(strengths)), _d(U0), _d(_f64(cp_offset)),
+                                           kerneloffset, kernelcutoff, int(bool(ugradmu)), float(Uref), float(rho),
+                                           _d(_f64(Lhat)), _d(_f64(Dhat)), _d(_f64(Shat)),
+                                           int(bool(correct_kutta)), _d(U), _d(Cp), _d(F), _d(lds)))
+        return U, Cp, F, lds.reshape(3, 3).T.copy()
 
     def adjoint_solve(self, ybar):
         ybar = _f64(np.atleast_2d(ybar))

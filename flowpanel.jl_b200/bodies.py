@@ -5,9 +5,10 @@ Names, arguments and error behaviour follow the reference:
 src/FLOWPanel_multibody.jl:312-364, src/FLOWPanel_nonliftingbody.jl:93-130),
 ``calcfield_U/Cp/F/LDS`` (src/FLOWPanel_postprocess.jl:28-110,1059-1689). The
 solver object is the drop-in: ``B200Solver`` owns a device context and runs the
-assembly, factorisation, solve and induced-velocity evaluation on the GPU.
-Geometry preprocessing and the O(N) post-processing stay on the host, as in
-the reference.
+assembly, factorisation, solve, induced-velocity evaluation and the surface
+post-processing (grad(mu) velocity, Cp, forces, L/D/S) on the GPU. Geometry
+preprocessing (normals, control points) stays on the host, as in the
+reference.
 """
 from __future__ import annotations
 
@@ -416,20 +417,91 @@ def calcfield_U(sourcebody: AbstractBody, targetbody: AbstractBody, offset=None,
     return out
 
 
+def _cpoffset_cells(body: AbstractBody):
+    """CPoffset of every panel (each member's own for a MultiBody)."""
+    if isinstance(body, MultiBody):
+        return body._default_off()
+    return np.full(body.ncells, float(body.CPoffset))
+
+
+def _doublet_strength(body: AbstractBody, Gammai=0):
+    if not body.solved:
+        raise RuntimeError("Body hasn't been solved yet. Please call `solve()` function first.")
+    s = np.asarray(body.strength, float)
+    if s.ndim == 2:
+        return np.ascontiguousarray(s[:, Gammai if body.kind != "source+doublet" else 1])
+    return s
+
+
+def calcfield_Ugradmu(body: AbstractBody, sharpTE=False, force_cellTE=True, anglecrit=30.0, Gammai=0,
+                      fieldname="Ugradmu", addfield=True, solver: Optional[B200Solver] = None, want_parts=False):
+    """calcfield_Ugradmu: surface velocity -1/2 grad(mu) of a solved body with
+    triangular panels, the cell scheme except where a cell has a free edge or
+    a neighbour more than ``anglecrit`` degrees off, which take the node scheme
+    (src/FLOWPanel_postprocess.jl:825-1042), on the device (fp_ugradmu).
+    Returns (N, 3); with ``want_parts`` also the cell and node fields.
+    ``sharpTE`` needs the structured-grid layout of a GeometricTools loft
+    (loop_dim, dimsplit), which these meshes do not carry."""
+    if sharpTE:
+        raise NotImplementedError("sharpTE=true needs the structured-grid layout of a GeometricTools loft")
+    g = _doublet_strength(body, Gammai)
+    solver = _field_solver(body, solver)
+    out, oc, on = solver.ctx.ugradmu(_capi.FP_UGRADMU_COMBINED, g, _cpoffset_cells(body), anglecrit, force_cellTE,
+                                     want_parts=True)
+    if addfield:
+        body.add_field(fieldname, "vector", out, "cell")
+    return (out, oc, on) if want_parts else out
+
+
+def calcfield_Ugradmu_cell(body: AbstractBody, Gammai=0, maxgrad=np.inf, fieldname="Ugradmu", addfield=True,
+                           solver: Optional[B200Solver] = None):
+    """calcfield_Ugradmu_cell (src/FLOWPanel_postprocess.jl:139-616): Green-Gauss
+    gradient with the inverse-distance face value; the trailing-edge cells'
+    face terms are added back; rows whose norm reaches ``maxgrad`` are zeroed."""
+    g = _doublet_strength(body, Gammai)
+    solver = _field_solver(body, solver)
+    out = solver.ctx.ugradmu(_capi.FP_UGRADMU_CELL, g, _cpoffset_cells(body), maxgrad=maxgrad)
+    if addfield:
+        body.add_field(fieldname, "vector", out, "cell")
+    return out
+
+
+def calcfield_Ugradmu_node(body: AbstractBody, Gammai=0, sharpTE=False, fieldname="Ugradmu", addfield=True,
+                           solver: Optional[B200Solver] = None):
+    """calcfield_Ugradmu_node (src/FLOWPanel_postprocess.jl:622-819): -1/2 the
+    linear gradient of the area-weighted nodal values."""
+    if sharpTE:
+        raise NotImplementedError("sharpTE=true needs the structured-grid layout of a GeometricTools loft")
+    g = _doublet_strength(body, Gammai)
+    solver = _field_solver(body, solver)
+    out = solver.ctx.ugradmu(_capi.FP_UGRADMU_NODE, g, _cpoffset_cells(body))
+    if addfield:
+        body.add_field(fieldname, "vector", out, "cell")
+    return out
+
+
+def addfields(body: AbstractBody, sourcefieldname, targetfieldname):
+    """addfields: add field ``sourcefieldname`` into ``targetfieldname``
+    (src/FLOWPanel_abstractbody.jl addfields)."""
+    src = np.asarray(body.get_field(sourcefieldname)["field_data"], float)
+    tgt = body.get_field(targetfieldname)
+    tgt["field_data"] = np.asarray(tgt["field_data"], float) + src
+    return body
+
+
 def calcfield_Cp(body: AbstractBody, Uref, U_fieldname="U", Us=None, correct_kuttacondition=True,
-                 clip=None, fieldname="Cp", addfield=True):
+                 clip=None, fieldname="Cp", addfield=True, solver: Optional[B200Solver] = None):
     """calcfield_Cp!: Cp = 1 - (|U|/Uref)^2, Kutta average over (pi, pi+1, pj, pj-1)
-    at each shedding edge (src/FLOWPanel_postprocess.jl:1059-1112)."""
-    Us = np.asarray(body.get_field(U_fieldname)["field_data"] if Us is None else Us, float)
-    Cp = 1 - (np.linalg.norm(Us, axis=1) / Uref) ** 2
-    if correct_kuttacondition and body.kind == "vortexring":
-        for (pi, nia, nib, pj, nja, njb) in body.mesh.shedding:
-            if pj != -1:
-                ave = (Cp[pi] + Cp[pi + 1] + Cp[pj] + Cp[pj - 1]) / 4
-                Cp[[pi, pi + 1, pj, pj - 1]] = ave
-            else:
-                ave = (Cp[pi] + Cp[pi + 1]) / 2
-                Cp[[pi, pi + 1]] = ave
+    of each shedding row in order (src/FLOWPanel_postprocess.jl:1059-1112), on
+    the device (fp_calcfield_cp); ``clip`` is applied afterwards on the host."""
+    if Us is None:
+        if not body.check_field(U_fieldname):
+            raise RuntimeError(f"Field {U_fieldname} not found; Please run "
+                               f"`calcfield_U(args...; fieldname={U_fieldname}, optargs...)`")
+        Us = body.get_field(U_fieldname)["field_data"]
+    Us = np.asarray(Us, float)
+    solver = _field_solver(body, solver)
+    Cp = solver.ctx.calcfield_cp(Us, Uref, correct_kuttacondition and body.kind == "vortexring")
     if clip is not None:
         Cp = np.array([clip(v) for v in Cp])
     if addfield:
@@ -438,41 +510,66 @@ def calcfield_Cp(body: AbstractBody, Uref, U_fieldname="U", Us=None, correct_kut
 
 
 def calcfield_F(body: AbstractBody, Uinf, rho, Cp_fieldname="Cp", correct_kuttacondition=True,
-                fieldname="F", addfield=True):
+                fieldname="F", addfield=True, solver: Optional[B200Solver] = None):
     """calcfield_F!: F = -Cp (rho Uinf^2 / 2) A n with normals flipped by
-    sign(CPoffset) and the TE override (src/FLOWPanel_postprocess.jl:1199-1392)."""
+    sign(CPoffset) and the TE override (src/FLOWPanel_postprocess.jl:1199-1392),
+    on the device (fp_calcfield_f)."""
+    if not body.check_field(Cp_fieldname):
+        raise RuntimeError(f"Field {Cp_fieldname} not found; Please run "
+                           f"`calcfield_Cp(args...; fieldname={Cp_fieldname}, optargs...)`")
     Cps = np.asarray(body.get_field(Cp_fieldname)["field_data"], float)
-    areas = calc_areas(body)
-    normals = calc_normals(body, flipbyCPoffset=True)
-    q = 0.5 * rho * Uinf ** 2
-    F = (-q * Cps * areas)[:, None] * normals
-    if correct_kuttacondition and body.kind == "vortexring":
-        for (pi, nia, nib, pj, nja, njb) in body.mesh.shedding:
-            if pj != -1:
-                idx = [pi, pi + 1, pj, pj - 1]
-                ave = (Cps[pi] + Cps[pi + 1] + Cps[pj] + Cps[pj - 1]) / 4
-            else:
-                idx = [pi, pi + 1]
-                ave = (Cps[pi] + Cps[pi + 1]) / 2
-            for i in idx:
-                F[i] = -ave * q * areas[i] * normals[i]
+    solver = _field_solver(body, solver)
+    F = solver.ctx.calcfield_f(Cps, Uinf, rho, _cpoffset_cells(body),
+                               correct_kuttacondition and body.kind == "vortexring")
     if addfield:
         body.add_field(fieldname, "vector", F, "cell")
     return F
 
 
-def calcfield_LDS(body: AbstractBody, Lhat, Dhat, Shat=None, F_fieldname="F", addfield=True):
+def calcfield_LDS(body: AbstractBody, Lhat, Dhat, Shat=None, F_fieldname="F", addfield=True,
+                  solver: Optional[B200Solver] = None):
     """calcfield_LDS!: lift, drag and sideslip vectors (columns) from the summed
-    force (src/FLOWPanel_postprocess.jl:1615-1689)."""
+    force (src/FLOWPanel_postprocess.jl:1615-1689), on the device
+    (fp_calcfield_lds)."""
     Lhat, Dhat = np.asarray(Lhat, float), np.asarray(Dhat, float)
     Shat = np.cross(Lhat, Dhat) if Shat is None else np.asarray(Shat, float)
     for v, nm in ((Lhat, "Lhat"), (Dhat, "Dhat"), (Shat, "Shat")):
         if abs(np.linalg.norm(v) - 1) > 2 * np.finfo(float).eps:
             raise ValueError(f"{nm}={v} is not a unitary vector")
-    Ftot = np.sum(np.asarray(body.get_field(F_fieldname)["field_data"], float), axis=0)
-    out = np.stack([Lhat * np.dot(Ftot, Lhat), Dhat * np.dot(Ftot, Dhat), Shat * np.dot(Ftot, Shat)], axis=1)
+    if not body.check_field(F_fieldname):
+        raise RuntimeError(f"Field {F_fieldname} not found; Please run "
+                           f"`calcfield_F(args...; fieldname={F_fieldname}, optargs...)`")
+    Fs = np.asarray(body.get_field(F_fieldname)["field_data"], float)
+    solver = _field_solver(body, solver)
+    out = solver.ctx.calcfield_lds(Fs, Lhat, Dhat, Shat)
     if addfield:
         body.add_field("L", "vector", out[:, 0], "system")
         body.add_field("D", "vector", out[:, 1], "system")
         body.add_field("S", "vector", out[:, 2], "system")
     return out
+
+
+def surface_loads(body: AbstractBody, magVinf, rho, Lhat, Dhat, Shat=None, ugradmu=True,
+                  correct_kuttacondition=True, solver: Optional[B200Solver] = None, addfield=True):
+    """The post-processing sequence of the reference's examples in one pass on
+    the device (examples/sweptwing_solverbenchmark.jl:14-66): calcfield_U at the
+    control points, + calcfield_Ugradmu (when ``ugradmu``), calcfield_Cp with
+    Uref = magVinf, calcfield_F with Uinf = magVinf and rho, calcfield_LDS.
+    Returns the 3 x 3 L/D/S matrix and stores the U, Cp, F, L, D, S fields."""
+    if not body.solved:
+        raise RuntimeError("Body hasn't been solved yet. Please call `solve()` function first.")
+    Lhat, Dhat = np.asarray(Lhat, float), np.asarray(Dhat, float)
+    Shat = np.cross(Lhat, Dhat) if Shat is None else np.asarray(Shat, float)
+    Uinfs = np.asarray(body.get_field("Uinf")["field_data"], float)
+    solver = _field_solver(body, solver)
+    U, Cp, F, LDS = solver.ctx.surface_loads(body.element, body.strength, Uinfs, magVinf, rho, Lhat, Dhat, Shat,
+                                             _cpoffset_cells(body), body.kerneloffset, body.kernelcutoff,
+                                             ugradmu, correct_kuttacondition and body.kind == "vortexring")
+    if addfield:
+        body.add_field("U", "vector", U, "cell")
+        body.add_field("Cp", "scalar", Cp, "cell")
+        body.add_field("F", "vector", F, "cell")
+        body.add_field("L", "vector", LDS[:, 0], "system")
+        body.add_field("D", "vector", LDS[:, 1], "system")
+        body.add_field("S", "vector", LDS[:, 2], "system")
+    return LDS

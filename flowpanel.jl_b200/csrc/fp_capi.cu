@@ -168,6 +168,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
   free_matrices(c);
+  post_free(c);
   dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt); dfree(c->d_wake);
   dfree(c->d_status); dfree(c->d_cert); dfree(c->d_ticket);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -293,6 +294,9 @@ int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   c->has_geometry = true;
   c->nsh = 0;
+  c->h_shed.clear();
+  c->topo_valid = false;
+  c->kutta_valid = false;
   return FP_OK;
 }
 
@@ -354,6 +358,7 @@ int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* D
   c->h_Db.assign(Dbs, Dbs + 3 * nsh);
   c->wake_opposite = opposite;
   c->nsh = nsh;
+  c->kutta_valid = false;
   c->wake_disjoint = disjoint;
   c->assembled = -1;
   c->factored = -1;
@@ -1045,7 +1050,7 @@ int fp_kernel_launches(fp_ctx* c, int64_t* count) {
 }
 
 int fp_last_kernel_ms(fp_ctx* c, int stage, double* ms, int* launches) {
-  if (check_ctx(c) || stage < 0 || stage > FP_STAGE_VJP) return FP_EINVAL;
+  if (check_ctx(c) || stage < 0 || stage > FP_STAGE_POST) return FP_EINVAL;
   if (ms) *ms = c->kms[stage];
   if (launches) *launches = c->klaunch[stage];
   return FP_OK;

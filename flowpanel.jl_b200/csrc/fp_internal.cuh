@@ -123,8 +123,8 @@ struct fp_ctx {
   // timing
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double ms_assemble = 0, ms_factor = 0, ms_solve = 0, ms_uind = 0;
-  double kms[6] = {0, 0, 0, 0, 0, 0};
-  int klaunch[6] = {0, 0, 0, 0, 0, 0};
+  double kms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int klaunch[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int adj_iters = 0;                    // refinement steps of the last adjoint solve
   double adj_relres = 0;                // its relative residual
   fp_stats last{};
@@ -140,6 +140,26 @@ struct fp_ctx {
   cudaStream_t stream2 = nullptr;       // second stream of the look-ahead factorisation
   cudaEvent_t ev_panel = nullptr;       // panel factored (stream -> stream2)
   cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)
+
+  // surface post-processing (fp_post.cu). The mesh topology of a triangular
+  // body is built on first use after fp_set_geometry, the Kutta-average
+  // tables on first use after fp_set_wake.
+  bool topo_valid = false;
+  bool kutta_valid = false;
+  int64_t topo_nnodes = 0;
+  int32_t* d_nb = nullptr;              // 3 x N (AoS): cell across edge k (local nodes k -> k+1), -1 at a free edge
+  int32_t* d_voff = nullptr;            // nnodes + 1: CSR of the cells around each node (ascending)
+  int32_t* d_vcell = nullptr;           // 3N
+  double* d_area = nullptr;             // N panel areas
+  int32_t* d_teflag = nullptr;          // N: times the cell is a shedding pi/pj (low 16 bits), bit 16 = forced cell value
+  int32_t* d_krow = nullptr;            // nsh x 4 slots of (pi, pi+1, pj, pj-1) in d_kcell, -1 absent
+  int32_t* d_kcell = nullptr;           // distinct cells of the Kutta rows
+  int32_t* d_klast = nullptr;           // per distinct cell: the last row that overwrites its force
+  int64_t nkcell = 0;
+  double* d_post = nullptr;             // post-processing work (fields of N cells and the nodes)
+  double* d_uscr = nullptr;             // partial sums of the chunked induced-velocity kernels
+  size_t cap_uscr = 0;                  // doubles
+  size_t cap_post = 0;                  // doubles
 };
 
 namespace fpb {
@@ -188,6 +208,8 @@ int launch_phi(fp_ctx* c, const double* d_sigma, const double* d_mu, const doubl
                double* d_out, bool wake);
 int launch_uind_source(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
                        double* d_out);
+// surface post-processing (fp_post.cu)
+void post_free(fp_ctx* c);
 
 // reverse mode of the pair kernels (fp_vjp.cu)
 int launch_pair_vjp(fp_ctx* c, const double* d_strength, const double* d_x, const double* d_w,

@@ -220,6 +220,62 @@ int fp_solve_ls(fp_ctx* ctx, double kerneloffset, double kernelcutoff, const dou
 int fp_phi(fp_ctx* ctx, int element, const double* strengths, const double* targets, int64_t m,
            double* out, double kerneloffset);
 
+/* Surface velocity from the gradient of the doublet strength of a solved body
+ * with triangular panels, added to out (N x 3):
+ *   FP_UGRADMU_COMBINED  calcfield_Ugradmu! (src/FLOWPanel_postprocess.jl:825-941):
+ *       the cell scheme, except on cells with a free edge or a neighbour whose
+ *       normal is more than anglecrit degrees off, which take the node scheme
+ *       (with the cell values on the trailing-edge cells pi, pi+1, pj, pj-1
+ *       when force_cellTE); out_cell / out_node (N x 3, may be NULL) receive
+ *       the two schemes' fields;
+ *   FP_UGRADMU_CELL      calcfield_Ugradmu_cell! (:139-540): Green-Gauss with
+ *       the inverse-distance face value, the face terms of the shedding rows'
+ *       pi/pj cells added back, rows whose norm reaches maxgrad zeroed;
+ *   FP_UGRADMU_NODE      calcfield_Ugradmu_node! (:622-748, sharpTE = false):
+ *       out is overwritten with -1/2 the gradient of the area-weighted nodal
+ *       values.
+ * strength: the N doublet strengths (Gammai column); cp_offset: per panel
+ * CPoffset (its sign flips the field, NULL = all positive). Neighbours are the
+ * panels sharing an edge (the wake's shedding rows from fp_set_wake).
+ * FP_EINVAL for a non-triangular panel or an edge of more than two panels.
+ * FP64; device time: fp_last_kernel_ms(FP_STAGE_POST). */
+#define FP_UGRADMU_COMBINED 0
+#define FP_UGRADMU_CELL 1
+#define FP_UGRADMU_NODE 2
+int fp_ugradmu(fp_ctx* ctx, int scheme, const double* strength, const double* cp_offset, double anglecrit,
+               int force_cellTE, double maxgrad, double* out, double* out_cell, double* out_node);
+
+/* calcfield_Cp! (src/FLOWPanel_postprocess.jl:1059-1112): out (N) +=
+ * 1 - (|U|/Uref)^2 for the velocities Us (N x 3), then, with correct_kutta,
+ * the average over (pi, pi+1, pj, pj-1) of each shedding row in row order. */
+int fp_calcfield_cp(fp_ctx* ctx, const double* Us, double Uref, int correct_kutta, double* out);
+
+/* calcfield_F! (src/FLOWPanel_postprocess.jl:1199-1307): out (N x 3) +=
+ * -Cp (rho Uinf^2 / 2) A n with the normals flipped by sign(cp_offset), then,
+ * with correct_kutta, the forces of each shedding row's cells overwritten
+ * from their average Cp. */
+int fp_calcfield_f(fp_ctx* ctx, const double* Cps, const double* cp_offset, double Uinf, double rho,
+                   int correct_kutta, double* out);
+
+/* calcfield_LDS! (src/FLOWPanel_postprocess.jl:1615-1652): out (3 x 3,
+ * column-major: lift, drag, sideslip vectors) from the sum of Fs (N x 3) added
+ * to out's third column, projected on the unit vectors Lhat, Dhat, Shat
+ * (FP_EINVAL with the reference's message when one is not unitary). */
+int fp_calcfield_lds(fp_ctx* ctx, const double* Fs, const double* Lhat, const double* Dhat, const double* Shat,
+                     double* out);
+
+/* The surface loads of a solved body in one pass on the device, the sequence
+ * of examples/sweptwing_solverbenchmark.jl:14-66: U = Uinfs + Uind at the
+ * control points (calcfield_U), + the combined grad(mu) velocity when ugradmu
+ * (anglecrit 30, force_cellTE), Cp with Uref and the Kutta average when
+ * correct_kutta, F with Uinf = Uref and rho, and L/D/S. Outputs: U (N x 3,
+ * may be NULL), Cp (N), F (N x 3), LDS (3 x 3 column-major). Device time
+ * (induced velocity to L/D/S): fp_last_kernel_ms(FP_STAGE_POST). */
+int fp_surface_loads(fp_ctx* ctx, int element, const double* strengths, const double* Uinfs,
+                     const double* cp_offset, double kerneloffset, double kernelcutoff, int ugradmu,
+                     double Uref, double rho, const double* Lhat, const double* Dhat, const double* Shat,
+                     int correct_kutta, double* U, double* Cp, double* F, double* LDS);
+
 /* Adjoint of the linear solve: A^T lambda = ybar with the saved factors (the
  * reverse rule of IAD.implicit_linear at src/FLOWPanel_linearsolver.jl:73:
  * lambda = A^-T ybar, Abar = -lambda x^T, bbar = lambda). ybar/lambda N x k on
@@ -288,6 +344,7 @@ int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
 #define FP_STAGE_UIND 3
 #define FP_STAGE_ADJOINT 4   /* fp_adjoint_solve */
 #define FP_STAGE_VJP 5       /* fp_assembly_vjp / fp_uind_vjp */
+#define FP_STAGE_POST 6      /* fp_ugradmu / fp_surface_loads */
 
 /* Measurement utility (no counterpart in the reference): sustained FMA
  * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, in

@@ -481,3 +481,166 @@ def calcfield_LDS(Fs, Lhat, Dhat, Shat=None):
     Shat = np.cross(Lhat, Dhat) if Shat is None else np.asarray(Shat, float)
     Ftot = np.sum(np.asarray(Fs), axis=0)
     return np.stack([Lhat * np.dot(Ftot, Lhat), Dhat * np.dot(Ftot, Dhat), Shat * np.dot(Ftot, Shat)], axis=1)
+
+
+# ----------------------------------------------------------------- surface velocity from grad(mu)
+# calcfield_Ugradmu_cell! / _node! / calcfield_Ugradmu! of
+# src/FLOWPanel_postprocess.jl:139-1042, on triangular cells. The mesh queries
+# they make of GeometricTools (unvendored, version 2 per Project.toml:29) are
+# restated from their use there:
+#   neighbor(grid, ni, ci; preserveEdge=true) -> the cell across the edge from
+#       the cell's local node ni to ni%3+1, none at a free edge;
+#   get_nodal_data(grid, data; areas) -> per node, the area-weighted mean of the
+#       data of the cells that contain it;
+#   project_3d_2d! + get_tri_gradient! -> the in-plane gradient of the linear
+#       interpolant of three nodal values, expressed in 3D.
+def mesh_neighbors(mesh):
+    """(N, 3) int: the cell across edge k (local nodes k -> k+1) of each
+    triangle, -1 at a free edge."""
+    offs, pn = mesh.panel_offsets, mesh.panel_nodes
+    if np.any(np.diff(offs) != 3):
+        raise ValueError("the grad(mu) schemes need triangular cells")
+    owners = {}
+    for c in range(mesh.npanels):
+        p = pn[offs[c]:offs[c] + 3]
+        for k in range(3):
+            a, b = int(p[k]), int(p[(k + 1) % 3])
+            owners.setdefault((min(a, b), max(a, b)), []).append((c, k))
+    nb = -np.ones((mesh.npanels, 3), np.int64)
+    for lst in owners.values():
+        if len(lst) == 2:
+            (c0, k0), (c1, k1) = lst
+            nb[c0, k0] = c1
+            nb[c1, k1] = c0
+        elif len(lst) > 2:
+            raise ValueError("an edge is shared by more than two cells")
+    return nb
+
+
+def nodal_data(mesh, values, areas):
+    """Area-weighted mean of the cell values around every node."""
+    offs, pn = mesh.panel_offsets, mesh.panel_nodes
+    num = np.zeros(mesh.nnodes)
+    den = np.zeros(mesh.nnodes)
+    for c in range(mesh.npanels):
+        for v in pn[offs[c]:offs[c + 1]]:
+            num[v] += areas[c] * values[c]
+            den[v] += areas[c]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(den > 0, num / np.where(den > 0, den, 1.0), 0.0)
+
+
+def _gg_term(P, tri, k, nc, cpc, cpn, gc, gn, area, hs):
+    """One Green-Gauss face term of the cell scheme times hs = 0.5*sign(CPoffset)
+    (postprocess.jl:189-247)."""
+    ei, ej = k, (k + 1) % 3
+    r1 = P[tri[ej], 0] - P[tri[ei], 0]
+    r2 = P[tri[ej], 1] - P[tri[ei], 1]
+    r3 = P[tri[ej], 2] - P[tri[ei], 2]
+    d1 = r2 * nc[2] - r3 * nc[1]
+    d2 = r3 * nc[0] - r1 * nc[2]
+    d3 = r1 * nc[1] - r2 * nc[0]
+    dmag = np.sqrt(d1 * d1 + d2 * d2 + d3 * d3)
+    d1, d2, d3 = d1 / dmag, d2 / dmag, d3 / dmag
+    vm = P[tri[ei]] - cpc
+    vn = P[tri[ei]] - cpn
+    r = np.array([r1, r2, r3])
+    dMain = np.linalg.norm(np.cross(vm, r))
+    dNear = np.linalg.norm(np.cross(vn, r))
+    f = dNear / (dMain + dNear)
+    face = f * gc + (1.0 - f) * gn
+    mag = face * np.sqrt(r1 * r1 + r2 * r2 + r3 * r3) / area
+    return np.array([hs * d1 * mag, hs * d2 * mag, hs * d3 * mag])
+
+
+def ugradmu_cell(mesh, gammas, areas, normals, cps, cpsign, nb=None, maxgrad=np.inf):
+    """calcfield_Ugradmu_cell! (src/FLOWPanel_postprocess.jl:270-540, the
+    RigidWakeBody method; without shedding rows it is the AbstractBody method
+    of :139-268): Green-Gauss over the cell's edges with the inverse-distance
+    face value, then the face terms of the trailing-edge cells added back.
+    ``cpsign`` is sign(CPoffset) per cell (1 where CPoffset = 0)."""
+    P = np.asarray(mesh.nodes, float)
+    nb = mesh_neighbors(mesh) if nb is None else nb
+    offs, pn = mesh.panel_offsets, mesh.panel_nodes
+    out = np.zeros((mesh.npanels, 3))
+
+    def terms(ci):
+        tri = pn[offs[ci]:offs[ci] + 3]
+        for k in range(3):
+            n = nb[ci, k]
+            if n >= 0:
+                yield _gg_term(P, tri, k, normals[ci], cps[ci], cps[n], gammas[ci], gammas[n], areas[ci],
+                               0.5 * cpsign[ci])
+
+    for ci in range(mesh.npanels):
+        for t in terms(ci):
+            out[ci] -= t
+    for (pi, nia, nib, pj, nja, njb) in np.reshape(mesh.shedding, (-1, 6)):
+        for ci in ((pi, pj) if pj != -1 else (pi,)):
+            for t in terms(ci):
+                out[ci] += t
+    big = np.linalg.norm(out, axis=1) >= maxgrad
+    out[big] = 0.0
+    return out
+
+
+def tri_gradient(p1, p2, p3, v1, v2, v3):
+    """In-plane gradient of the linear function through (p_k, v_k)."""
+    e1 = p2 - p1
+    x2 = np.linalg.norm(e1)
+    e1 = e1 / x2
+    w = p3 - p1
+    x3 = np.dot(w, e1)
+    e2 = w - x3 * e1
+    y3 = np.linalg.norm(e2)
+    e2 = e2 / y3
+    gx = (v2 - v1) / x2
+    gy = (v3 - v1 - gx * x3) / y3
+    return gx * e1 + gy * e2
+
+
+def ugradmu_node(mesh, gammas, areas, cpsign):
+    """calcfield_Ugradmu_node! (src/FLOWPanel_postprocess.jl:622-748 with
+    sharpTE=false): nodal values as the area-weighted mean of the cells around
+    each node, the cell's linear gradient of them (the nodal values take the
+    sign of CPoffset), times -1/2."""
+    P = np.asarray(mesh.nodes, float)
+    nodal = nodal_data(mesh, gammas, areas)
+    offs, pn = mesh.panel_offsets, mesh.panel_nodes
+    out = np.zeros((mesh.npanels, 3))
+    for ci in range(mesh.npanels):
+        v = pn[offs[ci]:offs[ci] + 3]
+        s = cpsign[ci]
+        out[ci] = tri_gradient(P[v[0]], P[v[1]], P[v[2]], s * nodal[v[0]], s * nodal[v[1]], s * nodal[v[2]])
+    return -0.5 * out
+
+
+def ugradmu(mesh, gammas, areas, normals, cps, cpsign, force_cellTE=True, anglecrit=30.0):
+    """calcfield_Ugradmu! (src/FLOWPanel_postprocess.jl:825-941): the cell
+    scheme, except where a cell has a free edge or a neighbour whose normal is
+    more than ``anglecrit`` degrees off, which take the node scheme (with the
+    cell values forced on the TE cells pi, pi+1, pj, pj-1). Returns
+    (out, out_cell, out_node)."""
+    import math
+
+    nb = mesh_neighbors(mesh)
+    oc = ugradmu_cell(mesh, gammas, areas, normals, cps, cpsign, nb)
+    on = ugradmu_node(mesh, gammas, areas, cpsign)
+    if force_cellTE:
+        for (pi, nia, nib, pj, nja, njb) in np.reshape(mesh.shedding, (-1, 6)):
+            on[pi] = oc[pi]
+            on[pi + 1] = oc[pi + 1]
+            if pj != -1:
+                on[pj] = oc[pj]
+                on[pj - 1] = oc[pj - 1]
+    cc = math.cos(math.radians(anglecrit))
+    out = np.zeros((mesh.npanels, 3))
+    for ci in range(mesh.npanels):
+        use_node = False
+        for k in range(3):
+            n = nb[ci, k]
+            if n < 0 or np.dot(normals[ci], normals[n]) < cc:
+                use_node = True
+                break
+        out[ci] = on[ci] if use_node else oc[ci]
+    return out, oc, on
