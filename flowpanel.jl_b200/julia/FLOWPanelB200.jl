@@ -17,6 +17,9 @@ const FP_PREC_FP64 = Cint(0)
 const FP_PREC_MIXED = Cint(1)
 const FP_SOLVER_LU = Cint(0)
 const FP_SOLVER_GMRES = Cint(1)
+const FP_UGRADMU_COMBINED = Cint(0)
+const FP_UGRADMU_CELL = Cint(1)
+const FP_UGRADMU_NODE = Cint(2)
 
 struct FPSolveOpts
     solver::Cint
@@ -168,6 +171,42 @@ function phi_b200!(self, targets::Matrix{Float64}, out::Vector{Float64}, solver:
         (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{Float64}, Cdouble),
         solver.ctx, element, s, targets, size(targets, 2), out, self.kerneloffset))
     return out
+end
+
+"""Device path of calcfield_Ugradmu! / _cell! / _node! (src/FLOWPanel_postprocess.jl:139-941) for a
+solved body with triangular panels: `scheme` FP_UGRADMU_COMBINED (out_cell and out_node
+receive the two schemes' fields), FP_UGRADMU_CELL (adds into out, maxgrad) or FP_UGRADMU_NODE
+(overwrites out). `cpoffset` holds every panel's CPoffset (each member's own in a MultiBody)."""
+function Ugradmu_b200!(self, out::Matrix{Float64}, solver::B200Solver, cpoffset::Vector{Float64};
+                       scheme=FP_UGRADMU_COMBINED, out_cell=nothing, out_node=nothing,
+                       anglecrit=30.0, force_cellTE=true, maxgrad=Inf, Gammai=1)
+    s = Vector{Float64}(self.strength[:, Gammai])
+    oc = out_cell === nothing ? C_NULL : out_cell
+    on = out_node === nothing ? C_NULL : out_node
+    GC.@preserve s cpoffset out out_cell out_node fp_check(solver, ccall((:fp_ugradmu, libfp), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Cdouble, Cint, Cdouble, Ptr{Float64}, Ptr{Float64},
+         Ptr{Float64}),
+        solver.ctx, scheme, s, cpoffset, anglecrit, Cint(force_cellTE), maxgrad, out, oc, on))
+    return out
+end
+
+"""Device path of the examples' post-processing (calcfield_U + calcfield_Ugradmu + addfields +
+calcfield_Cp + calcfield_F + calcfield_LDS, examples/sweptwing_solverbenchmark.jl:14-66):
+returns (U 3 x N, Cp N, F 3 x N, LDS 3 x 3)."""
+function surface_loads_b200(self, solver::B200Solver, cpoffset::Vector{Float64}, magVinf, rho,
+                            Lhat, Dhat, Shat; element=FP_ELEMENT_VORTEXRING, ugradmu=true,
+                            correct_kuttacondition=true)
+    N = self.ncells
+    s = Vector{Float64}(self.strength[:, 1])
+    Uinfs = hcat(get_field(self, "Uinf")["field_data"]...)
+    U, Cp, F, LDS = zeros(3, N), zeros(N), zeros(3, N), zeros(3, 3)
+    L, D, S = Vector{Float64}(Lhat), Vector{Float64}(Dhat), Vector{Float64}(Shat)
+    GC.@preserve s Uinfs cpoffset L D S U Cp F LDS fp_check(solver, ccall((:fp_surface_loads, libfp), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cdouble, Cdouble, Cint, Cdouble, Cdouble,
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+        solver.ctx, element, s, Uinfs, cpoffset, self.kerneloffset, self.kernelcutoff, Cint(ugradmu),
+        magVinf, rho, L, D, S, Cint(correct_kuttacondition), U, Cp, F, LDS))
+    return U, Cp, F, LDS
 end
 
 # ChainRulesCore pullback of Gamma = A(nodes, CPs, normals, Das, Dbs) \ b(Uinfs, normals):
