@@ -530,8 +530,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-wing batched throughput leg")
-    ap.add_argument("--workload", default="wing12k", choices=["wing12k", "wingbody"],
-                    help="wingbody: the 36.6k-panel wing-body solve and 1M-probe field evaluation")
+    ap.add_argument("--workload", default="wing12k", choices=["wing12k", "wingbody", "surface"],
+                    help="wingbody: the 36.6k-panel wing-body solve and 1M-probe field evaluation; "
+                         "surface: the post-processing (U, grad(mu), Cp, F, L/D/S) of a 12k-triangle wing")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="with --profile: which form to time")
     ap.add_argument("--profile", action="store_true",
@@ -545,6 +546,9 @@ def main():
             run_reference(args, rank, ws, dist)
         elif args.workload == "wingbody":
             run_wingbody(args, rank, ws, dist)
+        elif args.workload == "surface":
+            if rank == 0:
+                print(json.dumps({"workload": "surface", **surface_loads_timing(ge.load_package())}), flush=True)
         else:
             run_ours(args, rank, ws, dist)
     finally:
