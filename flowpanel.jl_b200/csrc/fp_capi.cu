@@ -106,7 +106,7 @@ int time_end(fp_ctx* c, double* ms) {
 void free_matrices(fp_ctx* c) {
   dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
   dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_part);
-  dfree(c->d_dinv128_64); dfree(c->d_dinv128_32);
+  dfree(c->d_dinv128_64); dfree(c->d_dinv128_32); dfree(c->d_mprev64); dfree(c->d_mprev32);
   if (c->d_minv) { cudaFree(c->d_minv); c->d_minv = nullptr; }
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
   dfree(c->d_V); dfree(c->d_h);
@@ -437,11 +437,15 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
     if (!c->d_dinv64) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv64, nblk * 2 * kLuNB * kLuNB * sizeof(double)));
     if (!c->d_dinv128_64)
       FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_64, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(double)));
+    if (!c->d_mprev64)
+      FP_CUDA_TRY(c->err, cudaMalloc(&c->d_mprev64, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(double)));
   } else {
     if (!c->d_G32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G32, elems * sizeof(float)));
     if (!c->d_dinv32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv32, nblk * 2 * kLuNB * kLuNB * sizeof(float)));
     if (!c->d_dinv128_32)
       FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
+    if (!c->d_mprev32)
+      FP_CUDA_TRY(c->err, cudaMalloc(&c->d_mprev32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
   }
   return FP_OK;
 }

@@ -93,6 +93,8 @@ struct fp_ctx {
   float* d_dinv32 = nullptr;            // inverses of the FP32 diagonal blocks
   double* d_dinv128_64 = nullptr;       // inverses of the 128-row diagonal blocks (FP64 factors)
   float* d_dinv128_32 = nullptr;        // inverses of the 128-row diagonal blocks (FP32 factors)
+  double* d_mprev64 = nullptr;          // inv(D_bb) T(b, p) of each 128-row block's predecessor, per sweep (FP64)
+  float* d_mprev32 = nullptr;           // the same for the FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)
   double* d_norms = nullptr;            // column norms (2 x cap_rhs)

@@ -1194,13 +1194,16 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
 // 16-byte loads issued before it waits, each warp reading the flags of up to
 // 32 upcoming blocks with one acquire load per lane and consuming every block
 // already complete, partial sums per thread (4 rows x 16 columns of a tile),
-// reduced once; then x_b = inv(D_bb) (b_b - sum) with inv(D_bb) staged in
-// shared memory while the CTA streams. The chain of dependent blocks is
-// n/128 long.
+// reduced once. The blocks before the predecessor p (b - 1 forward, b + 1
+// backward) give x' = inv(D_bb) (b_b - sum) before p is done; then
+// x_b = x' - Mprev_b y_p with Mprev_b = inv(D_bb) T(b, p) (k_mprev, once per
+// factorisation), so the step on the chain of n/128 dependent blocks is one
+// tile product and one reduction. The flag is published with a release store
+// after the barrier that orders the CTA's stores of x_b.
 constexpr int SB = 128;
 constexpr int kTrs1Threads = 256;
 template <class T> constexpr size_t trs1_smem() {
-  return (size_t)SB * (SB + 1) * sizeof(T) + (size_t)8 * SB * sizeof(T) + (size_t)2 * SB * sizeof(T) + 64;
+  return (size_t)SB * (SB + 1) * sizeof(T) + (size_t)8 * SB * sizeof(T) + (size_t)3 * SB * sizeof(T) + 64;
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned int* p) {
@@ -1208,18 +1211,50 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned int* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ void st_release(unsigned int* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
 
+// this thread's 4 rows x 16 columns of an SB x SB column-major tile (leading
+// dimension ld) at rows 4 rg.., columns ph + 8 i; zero outside rows < nr,
+// columns < nc
+template <class T>
+__device__ __forceinline__ void load_tile4x16(const T* __restrict__ src, int64_t ld, int rg, int ph, int nr, int nc,
+                                              T (&a)[16][4]) {
+  const bool rows_full = 4 * rg + 4 <= nr;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int col = ph + 8 * i;
+    if (col < nc && rows_full) {
+      const T* s = src + col * ld + 4 * rg;
+      if (sizeof(T) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(s);
+        a[i][0] = v.x; a[i][1] = v.y; a[i][2] = v.z; a[i][3] = v.w;
+      } else {
+        const double2 v0 = *reinterpret_cast<const double2*>(s);
+        const double2 v1 = *reinterpret_cast<const double2*>(s + 2);
+        a[i][0] = v0.x; a[i][1] = v0.y; a[i][2] = v1.x; a[i][3] = v1.y;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) a[i][j] = (col < nc && 4 * rg + j < nr) ? src[col * ld + 4 * rg + j] : T(0);
+    }
+  }
+}
+
 template <class T, bool LOWER>
 __global__ void __launch_bounds__(kTrs1Threads)
-k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv128, T* __restrict__ B,
-       unsigned int* __restrict__ flags, unsigned int* __restrict__ ticket, int* __restrict__ status) {
+k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv128, const T* __restrict__ Mprev,
+       T* __restrict__ B, unsigned int* __restrict__ flags, unsigned int* __restrict__ ticket,
+       int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char tsm[];
   T (*Ds)[SB + 1] = reinterpret_cast<T (*)[SB + 1]>(tsm);                    // Ds[l][r] = inv(D)(r, l)
   T (*red)[SB] = reinterpret_cast<T (*)[SB]>(tsm + (size_t)SB * (SB + 1) * sizeof(T));   // per phase
   T* accs = reinterpret_cast<T*>(tsm + (size_t)SB * (SB + 1) * sizeof(T) + (size_t)8 * SB * sizeof(T));
   T* xpart = accs + SB;
+  T* xfin = xpart + SB;
   __shared__ int blk_s, stop_s;
   const int64_t nblk = (n + SB - 1) / SB;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -1238,32 +1273,13 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
     // off the chain of dependent blocks
     const T rhs = (tid < nb) ? B[k0 + tid] : T(0);
     T sum[4] = {T(0), T(0), T(0), T(0)};
-    const bool rows_full = 4 * rg + 4 <= nb;
     int64_t ready = 0;   // dependencies known complete (this warp)
-    for (int64_t s = 0; s < tk; ++s) {
+    for (int64_t s = 0; s + 1 < tk; ++s) {   // every earlier block but the predecessor
       const int64_t cb = LOWER ? s : nblk - 1 - s;
       const int64_t c0 = cb * SB;
       const int cn = (int)imin64(SB, n - c0);
-      // this thread's part of the tile: 4 rows x 16 columns
       T a[16][4];
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int col = ph + 8 * i;
-        if (col < cn && rows_full) {
-          const T* src = A + (c0 + col) * lda + k0 + 4 * rg;
-          if (sizeof(T) == 4) {
-            const float4 v = *reinterpret_cast<const float4*>(src);
-            a[i][0] = v.x; a[i][1] = v.y; a[i][2] = v.z; a[i][3] = v.w;
-          } else {
-            const double2 v0 = *reinterpret_cast<const double2*>(src);
-            const double2 v1 = *reinterpret_cast<const double2*>(src + 2);
-            a[i][0] = v0.x; a[i][1] = v0.y; a[i][2] = v1.x; a[i][3] = v1.y;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; ++j) a[i][j] = (col < cn && 4 * rg + j < nb) ? A[(c0 + col) * lda + k0 + 4 * rg + j] : T(0);
-        }
-      }
+      load_tile4x16<T>(A + c0 * lda + k0, lda, rg, ph, nb, cn, a);
       if (s >= ready) {   // read the flags of up to 32 blocks at once
         int spins = 0;
         for (;;) {
@@ -1299,23 +1315,109 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
       accs[tid] = (tid < nb) ? rhs - s0 : T(0);
     }
     __syncthreads();
-    {   // x = inv(D) acc: thread (r, half) sums half of the columns
-      const int r = tid % SB, h = tid / SB;
+    const int r = tid % SB, h = tid / SB;
+    {   // x' = inv(D) acc: thread (r, half) sums half of the columns
       T s0 = T(0);
 #pragma unroll 8
       for (int l = h * (SB / 2); l < (h + 1) * (SB / 2); ++l) s0 += Ds[l][r] * accs[l];
       if (h == 1) xpart[r] = s0;
       __syncthreads();
-      if (h == 0 && r < nb) B[k0 + r] = s0 + xpart[r];
+      if (h == 0) xfin[r] = s0 + xpart[r];
     }
-    // publish: the barrier orders the CTA's stores before thread 0's fence
-    // (cumulative), which orders them before the flag
+    if (tk > 0) {   // x_b = x' - Mprev_b y_p, on the chain
+      // the predecessor's tile Mprev_b, loaded before the wait
+      const int64_t pb = LOWER ? b - 1 : b + 1;
+      const int np = (int)imin64(SB, n - pb * SB);
+      T mp[16][4];
+      load_tile4x16<T>(Mprev + (b * 2 + (LOWER ? 0 : 1)) * SB * SB, SB, rg, ph, nb, np, mp);
+      if (lane == 0) {
+        int spins = 0;
+        while (!ld_acquire(&flags[pb])) {
+          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+          __nanosleep(32);
+        }
+      }
+      __syncwarp();
+      T s2[4] = {T(0), T(0), T(0), T(0)};
+      const int64_t p0 = pb * SB;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int col = ph + 8 * i;
+        const T yv = (col < np) ? ld_cg(&B[p0 + col]) : T(0);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) s2[j] += mp[i][j] * yv;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) red[ph][4 * rg + j] = s2[j];
+      __syncthreads();
+      if (stop_s) return;
+      if (h == 0 && r < nb) {
+        T s0 = T(0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s0 += red[q][r];
+        B[k0 + r] = xfin[r] - s0;
+      }
+    } else {
+      __syncthreads();
+      if (h == 0 && r < nb) B[k0 + r] = xfin[r];
+    }
+    // publish: the barrier orders the CTA's stores of x_b before thread 0's
+    // release store of the flag
     __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      atomicExch(&flags[b], 1u);
+    if (tid == 0) st_release(&flags[b], 1u);
+  }
+}
+
+// Mprev_b = inv(D_bb) T(b, p) for the predecessor p of block b in each sweep
+// (forward: p = b - 1, T = L; backward: p = b + 1, T = U), SB x SB
+// column-major per block and sweep (zero past the matrix's rows and
+// columns). blockIdx.y: 0 forward, 1 backward.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_mprev(const T* __restrict__ LU, int64_t lda, int64_t n, const T* __restrict__ Dinv128, T* __restrict__ Mprev) {
+  constexpr int KC = sizeof(T) == 4 ? 32 : 16;
+  __shared__ __align__(16) T Dsh[KC][SB + 4];   // Dsh[l][r] = inv(D)(r, l0 + l)
+  __shared__ __align__(16) T Tsh[KC][SB + 4];   // Tsh[l][c] = T(l0 + l, c)
+  const int64_t nblk = (n + SB - 1) / SB;
+  const int64_t b = blockIdx.x;
+  const bool lower = blockIdx.y == 0;
+  const int64_t p = lower ? b - 1 : b + 1;
+  if (p < 0 || p >= nblk) return;   // the sweep's first block has no predecessor
+  const int64_t k0 = b * SB, p0 = p * SB;
+  const int nb = (int)imin64(SB, n - k0), np = (int)imin64(SB, n - p0);
+  const T* Di = Dinv128 + b * 2 * SB * SB + (lower ? 0 : SB * SB);
+  T* out = Mprev + (b * 2 + (lower ? 0 : 1)) * SB * SB;
+  const int tid = threadIdx.x;
+  const int r0 = 8 * (tid & 15), c0 = 8 * (tid >> 4);
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+  for (int l0 = 0; l0 < SB; l0 += KC) {
+    __syncthreads();
+    for (int e = tid; e < KC * SB; e += 256) {
+      const int r = e % SB, l = e / SB;
+      Dsh[l][r] = Di[(l0 + l) * SB + r];
+      const int ll = e % KC, c = e / KC;
+      Tsh[ll][c] = (l0 + ll < nb && c < np) ? LU[(p0 + c) * lda + k0 + l0 + ll] : T(0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int l = 0; l < KC; ++l) {
+      T x[8], y[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) { x[i] = Dsh[l][r0 + i]; y[i] = Tsh[l][c0 + i]; }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] += x[i] * y[j];
     }
   }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) out[(c0 + j) * SB + r0 + i] = acc[i][j];
 }
 
 // Inverses of the 128-row diagonal blocks from those of the 64-row blocks:
@@ -1404,11 +1506,11 @@ k_dinv128(const T* __restrict__ LU, int64_t lda, int64_t n, const T* __restrict_
 }
 
 template <class T, bool LOWER>
-static int run_trs1(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv128, T* B) {
+static int run_trs1(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv128, const T* Mprev, T* B) {
   const int64_t nblk = (n + SB - 1) / SB;
   FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
   const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
-  k_trs1<T, LOWER><<<grid, kTrs1Threads, trs1_smem<T>(), c->stream>>>(A, lda, n, Dinv128, B, c->d_flags,
+  k_trs1<T, LOWER><<<grid, kTrs1Threads, trs1_smem<T>(), c->stream>>>(A, lda, n, Dinv128, Mprev, B, c->d_flags,
                                                                       c->d_flags + nblk, c->d_status);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1476,11 +1578,12 @@ int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv
   }
   if (k == 1) {   // one right-hand side: the 128-row streaming sweeps
     const T* D128 = reinterpret_cast<const T*>(sizeof(T) == 8 ? (void*)c->d_dinv128_64 : (void*)c->d_dinv128_32);
+    const T* Mp = reinterpret_cast<const T*>(sizeof(T) == 8 ? (void*)c->d_mprev64 : (void*)c->d_mprev32);
     static SmemAttr attr_lo, attr_up;
     FP_CUDA_TRY(c->err, attr_lo.ensure(k_trs1<T, true>, (int)trs1_smem<T>()));
     FP_CUDA_TRY(c->err, attr_up.ensure(k_trs1<T, false>, (int)trs1_smem<T>()));
-    if (int rc = run_trs1<T, true>(c, LU, n, lda, D128, B)) return rc;
-    return run_trs1<T, false>(c, LU, n, lda, D128, B);
+    if (int rc = run_trs1<T, true>(c, LU, n, lda, D128, Mp, B)) return rc;
+    return run_trs1<T, false>(c, LU, n, lda, D128, Mp, B);
   }
   for (int64_t q0 = 0; q0 < k;) {
     const int64_t left = k - q0;
@@ -1503,6 +1606,10 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda) {
   static SmemAttr attr;
   FP_CUDA_TRY(c->err, attr.ensure(k_dinv128<T>, (int)dinv128_smem<T>()));
   k_dinv128<T><<<(unsigned)((n + SB - 1) / SB), 256, dinv128_smem<T>(), c->stream>>>(LU, lda, n, Dinv, D128);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  T* Mp = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_mprev64 : (void*)c->d_mprev32);
+  k_mprev<T><<<dim3((unsigned)((n + SB - 1) / SB), 2), 256, 0, c->stream>>>(LU, lda, n, D128, Mp);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;
