@@ -105,7 +105,7 @@ int time_end(fp_ctx* c, double* ms) {
 
 void free_matrices(fp_ctx* c) {
   dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
-  dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_part);
+  dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_mbox); dfree(c->d_part);
   dfree(c->d_dinv128_64); dfree(c->d_dinv128_32); dfree(c->d_mprev64); dfree(c->d_mprev32);
   if (c->d_minv) { cudaFree(c->d_minv); c->d_minv = nullptr; }
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
@@ -430,6 +430,11 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
   const int64_t nblk = (N + kLuNB - 1) / kLuNB;
   if (!c->d_ipiv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ipiv, N * sizeof(int32_t)));
   if (!c->d_flags) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_flags, (nblk + 2) * sizeof(unsigned int)));
+  if (!c->d_mbox) {
+    const size_t words = (size_t)((N + 127) / 128) * 128;
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_mbox, words * sizeof(unsigned long long)));
+    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_mbox, 0, words * sizeof(unsigned long long), c->stream));
+  }
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * N * sizeof(double)));
   if (!c->d_minv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_minv, kMinvBytes + (size_t)2 * kPanelSlots * kLuNB * sizeof(int)));
   if (precision == FP_PREC_FP64) {

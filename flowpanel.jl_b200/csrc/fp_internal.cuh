@@ -87,6 +87,8 @@ struct fp_ctx {
   float* d_w32 = nullptr;               // N x k FP32 work
   int* d_status = nullptr;              // device status word(s)
   unsigned int* d_flags = nullptr;      // triangular-solve flags
+  unsigned long long* d_mbox = nullptr; // per 128-row block, 128 (epoch, FP32 value) words of the single-RHS sweep
+  unsigned trs_epoch = 0;               // epoch of the last sweep launched
   float* d_cert = nullptr;              // max |L| certificate
   unsigned* d_ticket = nullptr;         // ticket of the factorisation's block launches (zero between launches)
   double* d_dinv64 = nullptr;           // inverses of the FP64 diagonal blocks

@@ -1199,7 +1199,12 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
 // x_b = x' - Mprev_b y_p with Mprev_b = inv(D_bb) T(b, p) (k_mprev, once per
 // factorisation), so the step on the chain of n/128 dependent blocks is one
 // tile product and one reduction. The flag is published with a release store
-// after the barrier that orders the CTA's stores of x_b.
+// after the barrier that orders the CTA's stores of x_b. With FP32 factors
+// the immediate successor does not wait for the flag: every x_b value also
+// goes to the block's mailbox as one 64-bit word (the sweep's epoch, the
+// value's bits), which is valid on its own once its epoch matches, so the
+// successor polls the 16 values it needs directly (one L2 round trip on the
+// chain instead of the stores' release, the flag and a second load).
 constexpr int SB = 128;
 constexpr int kTrs1Threads = 256;
 template <class T> constexpr size_t trs1_smem() {
@@ -1213,6 +1218,14 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned int* p) {
 }
 __device__ __forceinline__ void st_release(unsigned int* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ double ld_cg(const double* p) { return __ldcg(p); }
@@ -1248,7 +1261,7 @@ template <class T, bool LOWER>
 __global__ void __launch_bounds__(kTrs1Threads)
 k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv128, const T* __restrict__ Mprev,
        T* __restrict__ B, unsigned int* __restrict__ flags, unsigned int* __restrict__ ticket,
-       int* __restrict__ status) {
+       int* __restrict__ status, unsigned long long* __restrict__ mbox, unsigned epoch) {
   extern __shared__ __align__(16) unsigned char tsm[];
   T (*Ds)[SB + 1] = reinterpret_cast<T (*)[SB + 1]>(tsm);                    // Ds[l][r] = inv(D)(r, l)
   T (*red)[SB] = reinterpret_cast<T (*)[SB]>(tsm + (size_t)SB * (SB + 1) * sizeof(T));   // per phase
@@ -1330,22 +1343,43 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
       const int np = (int)imin64(SB, n - pb * SB);
       T mp[16][4];
       load_tile4x16<T>(Mprev + (b * 2 + (LOWER ? 0 : 1)) * SB * SB, SB, rg, ph, nb, np, mp);
-      if (lane == 0) {
-        int spins = 0;
-        while (!ld_acquire(&flags[pb])) {
-          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
-          __nanosleep(32);
-        }
-      }
-      __syncwarp();
       T s2[4] = {T(0), T(0), T(0), T(0)};
       const int64_t p0 = pb * SB;
+      if constexpr (sizeof(T) == 4) {
+        // lanes 0..15 poll the mailbox words of columns ph + 8 lane
+        float yl = 0.f;
+        const int col = ph + 8 * lane;
+        if (lane < 16 && col < np) {
+          int spins = 0;
+          for (;;) {
+            const unsigned long long w = ld_relaxed_u64(&mbox[p0 + col]);
+            if ((unsigned)(w >> 32) == epoch) { yl = __uint_as_float((unsigned)w); break; }
+            if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+          }
+        }
+        __syncwarp();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int col = ph + 8 * i;
-        const T yv = (col < np) ? ld_cg(&B[p0 + col]) : T(0);
+        for (int i = 0; i < 16; ++i) {
+          const T yv = __shfl_sync(0xffffffffu, yl, i);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) s2[j] += mp[i][j] * yv;
+          for (int j = 0; j < 4; ++j) s2[j] += mp[i][j] * yv;
+        }
+      } else {
+        if (lane == 0) {
+          int spins = 0;
+          while (!ld_acquire(&flags[pb])) {
+            if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+            __nanosleep(32);
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int col = ph + 8 * i;
+          const T yv = (col < np) ? ld_cg(&B[p0 + col]) : T(0);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) s2[j] += mp[i][j] * yv;
+        }
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) red[ph][4 * rg + j] = s2[j];
@@ -1355,11 +1389,19 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
         T s0 = T(0);
 #pragma unroll
         for (int q = 0; q < 8; ++q) s0 += red[q][r];
-        B[k0 + r] = xfin[r] - s0;
+        const T xv = xfin[r] - s0;
+        if constexpr (sizeof(T) == 4)
+          st_relaxed_u64(&mbox[k0 + r], ((unsigned long long)epoch << 32) | __float_as_uint(xv));
+        B[k0 + r] = xv;
       }
     } else {
       __syncthreads();
-      if (h == 0 && r < nb) B[k0 + r] = xfin[r];
+      if (h == 0 && r < nb) {
+        const T xv = xfin[r];
+        if constexpr (sizeof(T) == 4)
+          st_relaxed_u64(&mbox[k0 + r], ((unsigned long long)epoch << 32) | __float_as_uint(xv));
+        B[k0 + r] = xv;
+      }
     }
     // publish: the barrier orders the CTA's stores of x_b before thread 0's
     // release store of the flag
@@ -1510,8 +1552,10 @@ static int run_trs1(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv
   const int64_t nblk = (n + SB - 1) / SB;
   FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
   const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
+  if (++c->trs_epoch == 0) ++c->trs_epoch;   // epoch 0 marks words never written
   k_trs1<T, LOWER><<<grid, kTrs1Threads, trs1_smem<T>(), c->stream>>>(A, lda, n, Dinv128, Mprev, B, c->d_flags,
-                                                                      c->d_flags + nblk, c->d_status);
+                                                                      c->d_flags + nblk, c->d_status, c->d_mbox,
+                                                                      c->trs_epoch);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;

@@ -117,6 +117,31 @@ $EndElements
     assert b.npanels == 2 and np.array_equal(np.diff(b.panel_offsets), [3, 4])
     assert np.array_equal(b.panel_nodes, [0, 1, 2, 0, 1, 2, 3])
     assert np.allclose(a.nodes, b.nodes)
+    # a trailing-edge line mesh (line elements only, as the Cessna example's
+    # TE files): its nodes are the points of the line, it has no panels
+    line = """$MeshFormat
+4.1 0 8
+$EndMeshFormat
+$Nodes
+1 3 1 3
+1 1 0 3
+1
+2
+3
+0 0 0
+0.5 0 0
+1 0 0
+$EndNodes
+$Elements
+1 2 1 2
+1 1 1 2
+1 1 2
+2 2 3
+$EndElements
+"""
+    (tmp_path / "te.msh").write_text(line)
+    te = fp.meshio.read_msh(tmp_path / "te.msh")
+    assert te.npanels == 0 and te.nnodes == 3 and np.allclose(te.nodes[:, 0], [0, 0.5, 1])
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference example data not present")
