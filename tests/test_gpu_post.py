@@ -182,3 +182,24 @@ def test_openvsp_wing_least_squares(fp, O):
     o, _, _ = O.ugradmu(mesh, body.strength, areas, normals, cps, -np.ones(mesh.npanels))
     d = fp.calcfield_Ugradmu(body)
     assert close(d, o)
+
+
+def test_kutta_many_shedding_rows(fp, O):
+    """1,100 shedding rows: the Kutta tables exceed the one-CTA kernel's shared
+    memory, so the recurrence runs in global memory; same results."""
+    m = fp.meshes.triangulate(fp.meshes.swept_wing("0012", 4, 2200, chord=1.0, b=40.0, sweep=10.0))
+    assert m.nsheddings == 2200
+    normals, cps, areas = O.geometry(m, off=m.cpoffset())
+    rng = np.random.default_rng(11)
+    U = rng.standard_normal((m.npanels, 3))
+    c = fp._capi.Context(0)
+    try:
+        c.set_geometry(m.nodes, m.panel_offsets, m.panel_nodes, cps, normals)
+        D = np.tile([1.0, 0.0, 0.0], (m.nsheddings, 1))
+        c.set_wake(m.shedding, D, D)
+        Cp = O.calcfield_Cp(U, 1.3, m.shedding)
+        assert close(c.calcfield_cp(U, 1.3, True), Cp, 1e-13)
+        F = O.calcfield_F(Cp, areas, normals, 1.3, 1.2, m.shedding)
+        assert close(c.calcfield_f(Cp, 1.3, 1.2, m.cpoffset(), True), F, 1e-13)
+    finally:
+        c.close()
