@@ -549,13 +549,17 @@ def calcfield_LDS(body: AbstractBody, Lhat, Dhat, Shat=None, F_fieldname="F", ad
     return out
 
 
-def surface_loads(body: AbstractBody, magVinf, rho, Lhat, Dhat, Shat=None, ugradmu=True,
+def surface_loads(body: AbstractBody, magVinf, rho, Lhat, Dhat, Shat=None, ugradmu=None,
                   correct_kuttacondition=True, solver: Optional[B200Solver] = None, addfield=True):
     """The post-processing sequence of the reference's examples in one pass on
     the device (examples/sweptwing_solverbenchmark.jl:14-66): calcfield_U at the
     control points, + calcfield_Ugradmu (when ``ugradmu``), calcfield_Cp with
     Uref = magVinf, calcfield_F with Uinf = magVinf and rho, calcfield_LDS.
-    Returns the 3 x 3 L/D/S matrix and stores the U, Cp, F, L, D, S fields."""
+    Returns the 3 x 3 L/D/S matrix and stores the U, Cp, F, L, D, S fields.
+    ``ugradmu`` defaults to True for bodies with doublet strengths (vortex
+    rings, doublets) and False for source bodies, which have none."""
+    if ugradmu is None:
+        ugradmu = body.kind != "source"
     if not body.solved:
         raise RuntimeError("Body hasn't been solved yet. Please call `solve()` function first.")
     Lhat, Dhat = np.asarray(Lhat, float), np.asarray(Dhat, float)
