@@ -155,6 +155,17 @@ def test_sphere_host_api_analytic_cp(fp):
     th = np.arccos(np.clip(cps[:, 0] / np.linalg.norm(cps, axis=1), -1, 1))
     err = Cp - (1 - 9 / 4 * np.sin(th) ** 2)
     assert np.sqrt(np.mean(err ** 2)) < 0.02 and np.abs(err).max() < 0.05
+    # the same loads in one device pass (source body: no grad(mu) term)
+    Dhat = np.array([1.0, 0.0, 0.0])
+    Lhat = np.array([0.0, 0.0, 1.0])
+    LDS = fp.surface_loads(body, 1.0, 1.225, Lhat, Dhat, solver=solver)
+    Cp1 = body.get_field("Cp")["field_data"]
+    F1 = body.get_field("F")["field_data"]
+    assert np.abs(Cp1 - Cp).max() < 1e-12
+    F = fp.calcfield_F(body, 1.0, 1.225, solver=solver)
+    assert np.abs(F1 - F).max() < 1e-12
+    # a closed body in potential flow: no net force (d'Alembert), to the mesh's accuracy
+    assert np.abs(LDS).max() < 0.05 * 0.5 * 1.225 * np.pi
     solver.close()
 
 
