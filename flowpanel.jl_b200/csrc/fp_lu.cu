@@ -1200,11 +1200,11 @@ k_trs(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Din
 // factorisation), so the step on the chain of n/128 dependent blocks is one
 // tile product and one reduction. The flag is published with a release store
 // after the barrier that orders the CTA's stores of x_b. With FP32 factors
-// the immediate successor does not wait for the flag: every x_b value also
-// goes to the block's mailbox as one 64-bit word (the sweep's epoch, the
-// value's bits), which is valid on its own once its epoch matches, so the
-// successor polls the 16 values it needs directly (one L2 round trip on the
-// chain instead of the stores' release, the flag and a second load).
+// no block waits for a flag: every x_b value also goes to the block's mailbox
+// as one 64-bit word (the sweep's epoch, the value's bits), which is valid on
+// its own once its epoch matches, so each later block polls the 16 values a
+// warp needs directly (one L2 round trip per dependency instead of the
+// stores' release, the flag and a second load).
 constexpr int SB = 128;
 constexpr int kTrs1Threads = 256;
 template <class T> constexpr size_t trs1_smem() {
@@ -1287,34 +1287,66 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
     const T rhs = (tid < nb) ? B[k0 + tid] : T(0);
     T sum[4] = {T(0), T(0), T(0), T(0)};
     int64_t ready = 0;   // dependencies known complete (this warp)
-    for (int64_t s = 0; s + 1 < tk; ++s) {   // every earlier block but the predecessor
-      const int64_t cb = LOWER ? s : nblk - 1 - s;
-      const int64_t c0 = cb * SB;
-      const int cn = (int)imin64(SB, n - c0);
-      T a[16][4];
-      load_tile4x16<T>(A + c0 * lda + k0, lda, rg, ph, nb, cn, a);
-      if (s >= ready) {   // read the flags of up to 32 blocks at once
-        int spins = 0;
-        for (;;) {
-          const int64_t sq = s + lane;
-          const int64_t fb = LOWER ? sq : nblk - 1 - sq;
-          const unsigned f = (sq < tk) ? ld_acquire(&flags[fb]) : 0u;
-          const unsigned m = __ballot_sync(0xffffffffu, f != 0u);
-          const int cnt = __ffs(~m) - 1;   // consecutive ready blocks from s
-          if (m == 0xffffffffu) { ready = s + 32; break; }
-          if (cnt > 0) { ready = s + cnt; break; }
-          if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
-          __nanosleep(32);
+    if constexpr (sizeof(T) == 4) {
+      // every earlier block but the predecessor, its values from its mailbox:
+      // lanes 0..15 poll the words of columns ph + 8 lane (spinning first,
+      // then backing off), the warp shares them by shuffles
+      for (int64_t s = 0; s + 1 < tk; ++s) {
+        const int64_t cb = LOWER ? s : nblk - 1 - s;
+        const int64_t c0 = cb * SB;
+        const int cn = (int)imin64(SB, n - c0);
+        T a[16][4];
+        load_tile4x16<T>(A + c0 * lda + k0, lda, rg, ph, nb, cn, a);
+        float yl = 0.f;
+        const int col = ph + 8 * lane;
+        if (lane < 16 && col < cn) {
+          int spins = 0;
+          for (;;) {
+            const unsigned long long w = ld_relaxed_u64(&mbox[c0 + col]);
+            if ((unsigned)(w >> 32) == epoch) { yl = __uint_as_float((unsigned)w); break; }
+            if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+            if (spins > 64) __nanosleep(32);
+          }
         }
         __syncwarp();
         if (stop_s) break;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const T yv = __shfl_sync(0xffffffffu, yl, i);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) sum[j] += a[i][j] * yv;
+        }
       }
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int col = ph + 8 * i;
-        const T yv = (col < cn) ? ld_cg(&B[c0 + col]) : T(0);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) sum[j] += a[i][j] * yv;
+    } else {
+      for (int64_t s = 0; s + 1 < tk; ++s) {   // every earlier block but the predecessor
+        const int64_t cb = LOWER ? s : nblk - 1 - s;
+        const int64_t c0 = cb * SB;
+        const int cn = (int)imin64(SB, n - c0);
+        T a[16][4];
+        load_tile4x16<T>(A + c0 * lda + k0, lda, rg, ph, nb, cn, a);
+        if (s >= ready) {   // read the flags of up to 32 blocks at once
+          int spins = 0;
+          for (;;) {
+            const int64_t sq = s + lane;
+            const int64_t fb = LOWER ? sq : nblk - 1 - sq;
+            const unsigned f = (sq < tk) ? ld_acquire(&flags[fb]) : 0u;
+            const unsigned m = __ballot_sync(0xffffffffu, f != 0u);
+            const int cnt = __ffs(~m) - 1;   // consecutive ready blocks from s
+            if (m == 0xffffffffu) { ready = s + 32; break; }
+            if (cnt > 0) { ready = s + cnt; break; }
+            if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+            __nanosleep(32);
+          }
+          __syncwarp();
+          if (stop_s) break;
+        }
+  #pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int col = ph + 8 * i;
+          const T yv = (col < cn) ? ld_cg(&B[c0 + col]) : T(0);
+  #pragma unroll
+          for (int j = 0; j < 4; ++j) sum[j] += a[i][j] * yv;
+        }
       }
     }
 #pragma unroll
