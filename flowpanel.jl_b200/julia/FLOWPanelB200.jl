@@ -1,6 +1,8 @@
 # Julia face of libflowpanel_b200.so: the GPU solver type for FLOWPanel.jl's
-# `solve(body, Uinfs, Das, Dbs; solver=B200Solver(...))`, its `Uind!` device
-# path and the ChainRulesCore pullback of the solve. Every function is one
+# `solve(body, Uinfs, Das, Dbs; solver=B200Solver(...))`, its `Uind!` and
+# `phi!` device paths, the grad(mu) surface velocity and surface loads of
+# `calcfield_Ugradmu` / `Cp` / `F` / `LDS`, and the ChainRulesCore pullback of
+# the solve. Every function is one
 # `ccall` into include/flowpanel_b200.h; array layouts are FLOWPanel's own
 # (3 x N Float64 column-major, passed without copies).
 #
