@@ -188,3 +188,38 @@ def test_calc_shedding_single_sided_and_periodic(fp):
     sh = fp.meshio.calc_shedding(m, sq, periodic=True, tolerance=1e-3)
     assert len(sh) == 4 and sh[-1][0] == 1   # the closing edge (3, 0) belongs to the second triangle
     assert len(fp.meshio.calc_shedding(m, np.array([[5.0, 5.0, 5.0]]), tolerance=1e-3)) == 0
+
+
+def test_calc_shedding_errors_and_ties(fp):
+    """An edge of three panels is refused; nodes at the same sample keep node order."""
+    nodes = np.array([[0, 0, 0], [1, 0, 0], [0.5, 1, 0], [0.5, -1, 0], [0.5, 0, 1]], float)
+    m = fp.meshes.Mesh(nodes, np.array([0, 3, 6, 9], np.int32),
+                       np.array([0, 1, 2, 1, 0, 3, 0, 1, 4], np.int32))
+    with pytest.raises(ValueError, match="more than two panels"):
+        fp.meshio.calc_shedding(m, fp.meshio.sample_line([[0, 0, 0], [1, 0, 0]], 11), tolerance=1e-3)
+    pairs = fp.meshio.identify_edge(np.array([[0, 0, 0], [0, 0, 1e-9], [1, 0, 0]], float),
+                                    np.array([[0, 0, 0], [1, 0, 0]], float), 1e-6)
+    assert pairs == [(0, 0), (1, 0), (2, 1)]
+
+
+def test_vtu_polygon_cells(fp, tmp_path):
+    """VTK_POLYGON cells of 3 and 4 nodes are panels; larger polygons are refused."""
+    pts = " ".join(str(v) for v in [0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0, 2, 0, 0, 2, 1, 0])
+    def vtu(conn, offs, types):
+        return f"""<?xml version="1.0"?>
+<VTKFile type="UnstructuredGrid" version="0.1" byte_order="LittleEndian">
+  <UnstructuredGrid><Piece NumberOfPoints="6" NumberOfCells="{len(types.split())}">
+    <Points><DataArray type="Float32" NumberOfComponents="3" format="ascii">{pts}</DataArray></Points>
+    <Cells>
+      <DataArray type="Int64" Name="connectivity" format="ascii">{conn}</DataArray>
+      <DataArray type="Int64" Name="offsets" format="ascii">{offs}</DataArray>
+      <DataArray type="UInt8" Name="types" format="ascii">{types}</DataArray>
+    </Cells>
+  </Piece></UnstructuredGrid>
+</VTKFile>"""
+    (tmp_path / "p.vtu").write_text(vtu("0 1 2 3 1 4 5 2", "4 8", "7 9"))
+    m = fp.meshio.read_vtu(tmp_path / "p.vtu")
+    assert m.npanels == 2 and np.array_equal(np.diff(m.panel_offsets), [4, 4])
+    (tmp_path / "q.vtu").write_text(vtu("0 1 4 5 2 3", "6", "7"))
+    with pytest.raises(ValueError, match="polygon with 6 nodes"):
+        fp.meshio.read_vtu(tmp_path / "q.vtu")
