@@ -2,8 +2,9 @@
  * flowpanel_b200.h — C ABI of the B200 (sm_100a) panel-method hot path.
  *
  * Drop-in boundary for FLOWPanel.jl's dense solve path: a Julia solver object
- * calls these entry points through `ccall`; the Python
- * host mirror in flowpanel.jl_b200/ calls them through ctypes.
+ * calls these entry points through `ccall` (the bindings are in
+ * flowpanel.jl_b200/julia/FLOWPanelB200.jl); the Python host mirror in
+ * flowpanel.jl_b200/ calls them through ctypes.
  *
  * Conventions (Julia's column-major layouts, passed zero-copy):
  *   nodes       3 x nnodes  double   (x0,y0,z0,x1,...)
