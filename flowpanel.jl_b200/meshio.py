@@ -11,6 +11,8 @@ test/runtests_meshes2.jl:68-93). Here the same inputs become the flat
   data, optionally zlib-compressed, 32- or 64-bit headers);
 * :func:`read_msh` -- Gmsh ASCII 2.2 and 4.1 (surface elements only);
 * :func:`write_vtu` -- the inverse of :func:`read_vtu` (appended raw, zlib);
+* :func:`read_stl` (ASCII or binary, facet vertices welded into nodes) and
+  :func:`read_obj` (Wavefront OBJ), two more of the formats GeoIO reads;
 * :func:`calc_shedding` -- the shedding matrix of an unstructured mesh from a
   sampled trailing-edge line.
 
@@ -237,6 +239,86 @@ def read_msh(path, kind="vortexring", name=None, CPoffset=1e-14) -> Mesh:
     except KeyError as e:
         raise ValueError(f"read_msh: element references unknown node tag {e}") from None
     return _mesh_from_cells(np.asarray(xyz, np.float64).reshape(-1, 3), cells, kind, name or str(path), CPoffset)
+
+
+# ----------------------------------------------------------------------------- STL / OBJ
+def weld_nodes(points, tolerance=0.0):
+    """Merge points closer than ``tolerance`` (exact duplicates when 0); returns
+    (unique nodes in first-appearance order, index of each input point)."""
+    points = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    if tolerance <= 0.0:
+        _, first, inv = np.unique(points, axis=0, return_index=True, return_inverse=True)
+    else:
+        from scipy.spatial import cKDTree
+        pairs = cKDTree(points).query_pairs(tolerance, output_type="ndarray")
+        root = np.arange(len(points))
+
+        def find(i):
+            while root[i] != i:
+                root[i] = root[root[i]]
+                i = root[i]
+            return i
+        for i, j in pairs:
+            ri, rj = find(i), find(j)
+            if ri != rj:
+                root[max(ri, rj)] = min(ri, rj)
+        lab = np.array([find(i) for i in range(len(points))])
+        _, first, inv = np.unique(lab, return_index=True, return_inverse=True)
+    inv = np.asarray(inv).ravel()
+    order = np.argsort(first, kind="stable")          # first-appearance order
+    rank = np.empty_like(order)
+    rank[order] = np.arange(len(order))
+    return points[np.sort(first)], rank[inv]
+
+
+def read_stl(path, kind="vortexring", name=None, CPoffset=1e-14, tolerance=0.0) -> Mesh:
+    """Read an STL file (ASCII or binary) as triangles in file order; the
+    per-facet vertices are welded into shared nodes (exact duplicates, or
+    within ``tolerance``), so neighbouring facets share their edges."""
+    with open(path, "rb") as f:
+        blob = f.read()
+    tris = None
+    if len(blob) >= 84:
+        ntri = struct.unpack_from("<I", blob, 80)[0]
+        if 84 + 50 * ntri == len(blob):
+            rec = np.frombuffer(blob, dtype=np.dtype([("n", "<f4", 3), ("v", "<f4", (3, 3)), ("a", "<u2")]),
+                                count=ntri, offset=84)
+            tris = rec["v"].astype(np.float64).reshape(-1, 3)
+    if tris is None:
+        text = blob.decode("ascii", errors="replace").split()
+        if not text or text[0].lower() != "solid":
+            raise ValueError(f"read_stl: {path} is neither binary nor ASCII STL")
+        vs = [[float(text[i + 1]), float(text[i + 2]), float(text[i + 3])]
+              for i, t in enumerate(text) if t.lower() == "vertex"]
+        if len(vs) % 3:
+            raise ValueError("read_stl: facets must have three vertices")
+        tris = np.asarray(vs, np.float64).reshape(-1, 3)
+    nodes, idx = weld_nodes(tris, tolerance)
+    cells = idx.reshape(-1, 3).tolist()
+    return _mesh_from_cells(nodes, cells, kind, name or str(path), CPoffset)
+
+
+def read_obj(path, kind="vortexring", name=None, CPoffset=1e-14) -> Mesh:
+    """Read the vertices and the 3- and 4-vertex faces of a Wavefront OBJ file
+    (``f`` entries may carry /texture/normal indices; negative indices count
+    from the end)."""
+    nodes, cells = [], []
+    with open(path, "r") as f:
+        for line in f:
+            p = line.split()
+            if not p:
+                continue
+            if p[0] == "v":
+                nodes.append([float(p[1]), float(p[2]), float(p[3])])
+            elif p[0] == "f":
+                ids = []
+                for tok in p[1:]:
+                    i = int(tok.split("/")[0])
+                    ids.append(i - 1 if i > 0 else len(nodes) + i)
+                if not 3 <= len(ids) <= 4:
+                    raise ValueError(f"read_obj: face with {len(ids)} vertices (3 or 4 supported)")
+                cells.append(ids)
+    return _mesh_from_cells(np.asarray(nodes, np.float64).reshape(-1, 3), cells, kind, name or str(path), CPoffset)
 
 
 # ----------------------------------------------------------------------------- trailing edge

@@ -223,3 +223,32 @@ def test_vtu_polygon_cells(fp, tmp_path):
     (tmp_path / "q.vtu").write_text(vtu("0 1 4 5 2 3", "6", "7"))
     with pytest.raises(ValueError, match="polygon with 6 nodes"):
         fp.meshio.read_vtu(tmp_path / "q.vtu")
+
+
+def test_stl_and_obj(fp, O, tmp_path):
+    """STL (ASCII and binary, vertices welded) and OBJ faces give the mesh back."""
+    import struct
+    m = fp.meshes.triangulate(fp.meshes.sphere(1.0, 6, 8))
+    P = m.nodes
+    tri = m.panel_nodes.reshape(-1, 3)
+    lines = ["solid s"]
+    for t in tri:
+        lines += ["facet normal 0 0 0", "outer loop"] + ["vertex %.17g %.17g %.17g" % tuple(P[i]) for i in t] + \
+                 ["endloop", "endfacet"]
+    (tmp_path / "a.stl").write_text("\n".join(lines + ["endsolid s"]))
+    b = bytearray(80) + struct.pack("<I", len(tri))
+    for t in tri:
+        b += struct.pack("<3f", 0, 0, 0) + struct.pack("<9f", *P[t].astype(np.float32).ravel()) + b"\0\0"
+    (tmp_path / "b.stl").write_bytes(bytes(b))
+    for f, tol in (("a.stl", 0.0), ("b.stl", 1e-6)):
+        r = fp.meshio.read_stl(tmp_path / f, tolerance=tol)
+        assert r.npanels == len(tri)
+        # the welded mesh is watertight like the original: every edge has two panels
+        assert (O.mesh_neighbors(r) >= 0).all()
+        assert np.abs(r.nodes[r.panel_nodes] - P[m.panel_nodes]).max() < 1e-6
+    obj = ["v %.17g %.17g %.17g" % tuple(p) for p in P] + \
+          ["f " + " ".join(f"{i + 1}/1/1" for i in t) for t in tri[:-1]] + \
+          ["f " + " ".join(str(i - m.nnodes) for i in tri[-1])]
+    (tmp_path / "c.obj").write_text("\n".join(obj))
+    r = fp.meshio.read_obj(tmp_path / "c.obj")
+    assert np.array_equal(r.panel_nodes, m.panel_nodes) and np.array_equal(r.nodes, P)
