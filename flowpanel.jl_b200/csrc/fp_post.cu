@@ -435,7 +435,14 @@ int build_kutta(fp_ctx* c) {
     if (pi + 1 >= N || (pj != -1 && pj < 1))
       return c->err.set(FP_EINVAL, "shedding row " + std::to_string(r) +
                                        ": the Kutta average needs panels pi+1 and pj-1 to exist");
-    if (++te[pi] > 0xffff || (pj >= 0 && ++te[pj] > 0xffff))
+    // the low 16 bits count the rows a cell is pi or pj of; bit 16 (forced
+    // cell value) may already be set by another row's pi+1 or pj-1
+    auto bump = [&](int32_t p) {
+      if ((te[p] & 0xffff) == 0xffff) return false;
+      ++te[p];
+      return true;
+    };
+    if (!bump(pi) || (pj >= 0 && !bump(pj)))
       return c->err.set(FP_EINVAL, "fp_ugradmu: a panel appears in too many shedding rows");
     const int32_t cells[4] = {pi, pi + 1, pj, pj - 1};
     const int ncell = pj != -1 ? 4 : 2;

@@ -203,3 +203,30 @@ def test_kutta_many_shedding_rows(fp, O):
         assert close(c.calcfield_f(Cp, 1.3, 1.2, m.cpoffset(), True), F, 1e-13)
     finally:
         c.close()
+
+
+def test_overlapping_shedding_rows(fp, O):
+    """Rows whose cells overlap (one row's pi is the previous row's pi+1): the
+    grad(mu) add-backs and the in-order Kutta averages equal the oracle's."""
+    from test_oracle_ugradmu import flat_grid
+    m = flat_grid(fp, 8)
+    m.shedding = np.array([[5, 1, 0, -1, -1, -1], [6, 1, 0, -1, -1, -1], [40, 1, 0, 22, 1, 0]], np.int32)
+    normals, cps, areas = O.geometry(m)
+    rng = np.random.default_rng(13)
+    g = rng.standard_normal(m.npanels)
+    U = rng.standard_normal((m.npanels, 3))
+    c = fp._capi.Context(0)
+    try:
+        c.set_geometry(m.nodes, m.panel_offsets, m.panel_nodes, cps, normals)
+        D = np.tile([1.0, 0.0, 0.0], (3, 1))
+        c.set_wake(m.shedding, D, D)
+        s = np.ones(m.npanels)
+        d, dc, dn = c.ugradmu(fp._capi.FP_UGRADMU_COMBINED, g, None, want_parts=True)
+        o, oc, on = O.ugradmu(m, g, areas, normals, cps, s)
+        assert close(d, o) and close(dc, oc) and close(dn, on)
+        Cp = O.calcfield_Cp(U, 1.0, m.shedding)
+        assert close(c.calcfield_cp(U, 1.0, True), Cp, 1e-13)
+        F = O.calcfield_F(Cp, areas, normals, 1.0, 1.2, m.shedding)
+        assert close(c.calcfield_f(Cp, 1.0, 1.2, None, True), F, 1e-13)
+    finally:
+        c.close()
