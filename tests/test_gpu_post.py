@@ -230,3 +230,20 @@ def test_overlapping_shedding_rows(fp, O):
         assert close(c.calcfield_f(Cp, 1.0, 1.2, None, True), F, 1e-13)
     finally:
         c.close()
+
+
+def test_kutta_rows_need_neighbours(fp, O):
+    """A shedding row on the last panel has no pi+1 for the Kutta average: the
+    call fails with the reason instead of reading past the panels."""
+    from test_oracle_ugradmu import flat_grid
+    m = flat_grid(fp, 4)
+    normals, cps, _ = O.geometry(m)
+    c = fp._capi.Context(0)
+    try:
+        c.set_geometry(m.nodes, m.panel_offsets, m.panel_nodes, cps, normals)
+        last = m.npanels - 1
+        c.set_wake(np.array([[last, 1, 0, -1, -1, -1]], np.int32), np.array([[1.0, 0, 0]]), np.array([[1.0, 0, 0]]))
+        with pytest.raises(fp._capi.FlowPanelError, match="pi\\+1 and pj-1"):
+            c.calcfield_cp(np.ones((m.npanels, 3)), 1.0, True)
+    finally:
+        c.close()
