@@ -16,7 +16,8 @@ LIB_PATH = os.path.join(HERE, "_build", "libflowpanel_b200.so")
 
 FP_OK, FP_EINVAL, FP_ESINGULAR, FP_ENOCONV, FP_ECUDA, FP_ETIMEOUT, FP_ESTATE = range(7)
 FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING, FP_ELEMENT_SOURCE_DOUBLET = 0, 1, 2
-FP_PREC_FP64, FP_PREC_MIXED = 0, 1
+FP_PREC_FP64, FP_PREC_MIXED, FP_PREC_MIXED_GEPP = 0, 1, 2
+_PRECISIONS = {"fp64": FP_PREC_FP64, "mixed": FP_PREC_MIXED, "mixed_gepp": FP_PREC_MIXED_GEPP}
 FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
 FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP, FP_STAGE_POST = range(7)
 FP_UGRADMU_COMBINED, FP_UGRADMU_CELL, FP_UGRADMU_NODE = 0, 1, 2
@@ -34,7 +35,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
 class SolveOpts(C.Structure):
     _fields_ = [("solver", C.c_int), ("precision", C.c_int), ("ir_tol", C.c_double),
                 ("ir_maxiter", C.c_int), ("gmres_memory", C.c_int), ("gmres_atol", C.c_double),
-                ("gmres_rtol", C.c_double), ("gmres_itmax", C.c_int)]
+                ("gmres_rtol", C.c_double), ("gmres_itmax", C.c_int), ("gmres_restart", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -141,10 +142,13 @@ def _f64(a):
 
 
 def make_opts(solver="ludiv", precision="fp64", ir_tol=1e-12, ir_maxiter=10, gmres_memory=50,
-              gmres_atol=-1.0, gmres_rtol=-1.0, gmres_itmax=0):
+              gmres_atol=-1.0, gmres_rtol=-1.0, gmres_itmax=0, gmres_restart=False):
+    """fp_solve_opts. GMRES defaults to the reference's Krylov.jl gmres (no
+    restart: gmres_memory only sizes the first basis storage);
+    gmres_restart=True gives GMRES(gmres_memory)."""
     return SolveOpts(FP_SOLVER_GMRES if solver == "gmres" else FP_SOLVER_LU,
-                     FP_PREC_MIXED if precision == "mixed" else FP_PREC_FP64, ir_tol, ir_maxiter,
-                     gmres_memory, gmres_atol, gmres_rtol, gmres_itmax)
+                     _PRECISIONS[precision], ir_tol, ir_maxiter,
+                     gmres_memory, gmres_atol, gmres_rtol, gmres_itmax, 1 if gmres_restart else 0)
 
 
 class Context:

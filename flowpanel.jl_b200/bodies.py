@@ -229,14 +229,16 @@ class B200Solver:
     src/FLOWPanel_linearsolver.jl:24-157's solvers, owning assembly too).
 
     method: "ludiv" | "backslash" (LU, same on the device) | "gmres"
-    precision: "fp64" (plain) | "mixed" (FP32 factors + FP64 refinement)
+    precision: "fp64" (plain) | "mixed" (FP32 factors with a static row order
+        + FP64 refinement) | "mixed_gepp" (FP32 factors pivoted as the FP64
+        form + FP64 refinement)
     """
 
     def __init__(self, method="ludiv", precision="fp64", device=0, ir_tol=1e-12, ir_maxiter=10,
                  gmres_memory=50, atol=None, rtol=None, itmax=0):
         if method not in ("ludiv", "backslash", "gmres"):
             raise ValueError(f"unknown method {method}")
-        if precision not in ("fp64", "mixed"):
+        if precision not in ("fp64", "mixed", "mixed_gepp"):
             raise ValueError(f"unknown precision {precision}")
         self.method, self.precision = method, precision
         self.opts = _capi.make_opts("gmres" if method == "gmres" else "ludiv", precision, ir_tol, ir_maxiter,
@@ -383,7 +385,7 @@ def Uind(body: AbstractBody, targets, out, solver: Optional[B200Solver] = None, 
     if not body.solved:
         raise RuntimeError("Source body hasn't been solved yet. Please call `solve(...)` function first.")
     solver = _field_solver(body, solver)
-    prec = _capi.FP_PREC_MIXED if precision == "mixed" else _capi.FP_PREC_FP64
+    prec = _capi.FP_PREC_FP64 if precision == "fp64" else _capi.FP_PREC_MIXED
     return solver.ctx.uind(body.element, body.strength, targets, out, prec,
                            body.kerneloffset, body.kernelcutoff)
 

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libflowpanel_b200.so")
-SOURCES = ["fp_capi.cu", "fp_assembly.cu", "fp_lu.cu", "fp_field.cu", "fp_gmres.cu", "fp_tc.cu", "fp_peak.cu", "fp_vjp.cu", "fp_batch.cu", "fp_ls.cu", "fp_post.cu"]
+SOURCES = ["fp_capi.cu", "fp_assembly.cu", "fp_lu.cu", "fp_field.cu", "fp_gmres.cu", "fp_tc.cu", "fp_peak.cu", "fp_vjp.cu", "fp_batch.cu", "fp_ls.cu", "fp_post.cu", "fp_lu_static.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++", "-I" + os.path.join(HERE, "..", "include")]

@@ -371,14 +371,14 @@ int fp_assemble(fp_ctx* c, int element, double kerneloffset, double kernelcutoff
   if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_assemble: no geometry");
   if (element != FP_ELEMENT_SOURCE && element != FP_ELEMENT_VORTEXRING)
     return c->err.set(FP_EINVAL, "fp_assemble: unknown element");
-  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED)
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP)
     return c->err.set(FP_EINVAL, "fp_assemble: unknown precision");
   const size_t elems = (size_t)c->ld * c->capN;   // for the largest body the buffers hold
   if (!c->d_G) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G, elems * sizeof(double)));
     FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G, 0, elems * sizeof(double), c->stream));
   }
-  const bool w32 = precision == FP_PREC_MIXED;
+  const bool w32 = precision != FP_PREC_FP64;
   if (w32 && !c->d_G32) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G32, elems * sizeof(float)));
     FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G32, 0, elems * sizeof(float), c->stream));
@@ -459,26 +459,54 @@ int fp_factor(fp_ctx* c, int precision) {
   if (check_ctx(c)) return FP_EINVAL;
   cudaSetDevice(c->device);
   if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_factor: assemble first");
-  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED)
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP)
     return c->err.set(FP_EINVAL, "fp_factor: unknown precision");
   if (int rc = alloc_factor_buffers(c, precision)) return rc;
   if (time_begin(c)) return FP_ECUDA;
   int rc;
+  double ms_static = 0;
+  c->static_order = false;
   if (precision == FP_PREC_FP64) {
     FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_LU, c->d_G, (size_t)c->ld * c->N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     rc = lu_factor<double>(c, c->d_LU, c->N, c->ld, c->d_ipiv, c->d_cert);
     if (!rc) rc = lu_diag_inverses<double>(c, c->d_LU, c->N, c->ld);
   } else {
-    if (c->assembled_prec != FP_PREC_MIXED) {
+    if (c->assembled_prec != FP_PREC_MIXED && c->assembled_prec != FP_PREC_MIXED_GEPP) {
       rc = convert_f64_f32(c, c->d_G, c->d_G32, c->N, c->N, c->ld, c->ld);
       if (rc) return rc;
     }
-    rc = lu_factor<float>(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert);
-    if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
+    bool pivoted = precision == FP_PREC_MIXED_GEPP;
+    if (!pivoted) {
+      // static row order; a zero or non-finite pivot falls back to the pivoted
+      // factorisation of a fresh FP32 copy of the AIC
+      rc = lu_factor_static(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert);
+      if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
+      if (rc) return rc;
+      if (time_end(c, &ms_static)) return FP_ECUDA;
+      int st = 0;
+      FP_CUDA_TRY(c->err, cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+      if (st & DEV_ZERO_PIVOT) {
+        FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
+        if (time_begin(c)) return FP_ECUDA;
+        if ((rc = convert_f64_f32(c, c->d_G, c->d_G32, c->N, c->N, c->ld, c->ld))) return rc;
+        pivoted = true;
+      } else {
+        c->static_order = true;
+      }
+    }
+    if (pivoted) {
+      rc = lu_factor<float>(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert);
+      if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
+    }
     c->assembled_prec = -2;   // the FP32 copy now holds factors
   }
   if (rc) return rc;
-  if (time_end(c, &c->ms_factor)) return FP_ECUDA;
+  if (c->static_order) {
+    c->ms_factor = ms_static;
+  } else {
+    if (time_end(c, &c->ms_factor)) return FP_ECUDA;
+    c->ms_factor += ms_static;
+  }
   kt_collect(c);
   tr_collect(c);
   c->kms[FP_STAGE_FACTOR] = c->ms_factor;
@@ -488,7 +516,7 @@ int fp_factor(fp_ctx* c, int precision) {
   c->last.max_abs_L = cert;
   c->last.gepp_certified = cert <= 1.0f;
   c->last.ms_factor = c->ms_factor;
-  c->factored = precision;
+  c->factored = precision == FP_PREC_FP64 ? FP_PREC_FP64 : FP_PREC_MIXED;   // both FP32 forms
   return FP_OK;
 }
 
@@ -501,6 +529,7 @@ static void default_opts(fp_solve_opts& o) {
   o.gmres_atol = -1;
   o.gmres_rtol = -1;
   o.gmres_itmax = 0;
+  o.gmres_restart = 0;
 }
 
 static void normalize_opts(fp_solve_opts& o) {
@@ -527,6 +556,76 @@ static int residual_ratio(fp_ctx* c, const double* r, const double* b, int64_t k
   }
   *out = m;
   return FP_OK;
+}
+
+// FP64 factors whose certificate failed (a block-local pivot differs from
+// partial pivoting over the whole column, so growth is not bounded as
+// LAPACK's is): refine x against the FP64 AIC, r = b - G x, x += LU^-1 r,
+// until the relative residual stops halving (the FP64 level) or reaches
+// 1e-15; if it is then above opts.ir_tol, GMRES-IR preconditioned by the same
+// factors takes over. Statistics as for the mixed form.
+static int refine_fp64(fp_ctx* c, int64_t k, const fp_solve_opts& o) {
+  const int64_t n = c->N, ld = c->ld;
+  double prev = 1e300, rr = 0;
+  int rc;
+  for (int it = 0; it <= o.ir_maxiter; ++it) {
+    if ((rc = gemv_residual(c, c->d_G, n, ld, c->d_x, c->d_rhs, c->d_r, k))) return rc;
+    if ((rc = residual_ratio(c, c->d_r, c->d_rhs, k, &rr, it == 0))) return rc;
+    if ((rc = consume_status(c))) return rc;
+    if (rr <= 1e-15 || rr > 0.5 * prev || it == o.ir_maxiter) break;
+    prev = rr;
+    if ((rc = lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_r, ld, k, false))) return rc;
+    if ((rc = axpy_f64(c, c->d_r, c->d_x, n, k, ld))) return rc;
+    c->last.ir_iters = it + 1;
+  }
+  c->last.rel_residual = rr;
+  if (rr <= o.ir_tol) return FP_OK;
+  int it = 0;
+  fp_solve_opts g = o;
+  g.gmres_atol = 0.0;
+  g.gmres_rtol = o.ir_tol;
+  rc = gmres_solve(c, c->d_rhs, c->d_x, k, g, true, &it, &rr);
+  c->last.gmres_iters = it;
+  c->last.used_gmres = 1;
+  c->last.rel_residual = rr;
+  return rc;
+}
+
+// Mixed-precision iterative refinement with the FP32 factors: x0 = A32^-1 b;
+// r = b - A x (FP64, on the stored FP64 AIC); x += A32^-1 r, until
+// ||r||/||b|| <= opts.ir_tol; when the residual stops halving, GMRES-IR
+// (right-preconditioned by the same factors) takes over.
+static int refine_mixed(fp_ctx* c, int64_t k, const fp_solve_opts& o) {
+  const int64_t n = c->N, ld = c->ld;
+  int rc;
+  FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_x, 0, ld * k * sizeof(double), c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_r, c->d_rhs, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  double prev = 1e300, rr = 0;
+  bool converged = false, first = true;
+  for (int it = 0; it < o.ir_maxiter; ++it) {
+    if ((rc = convert_f64_f32(c, c->d_r, c->d_w32, n, k, ld, ld))) return rc;
+    if ((rc = lu_solve<float>(c, c->d_G32, n, ld, c->d_ipiv, c->d_w32, ld, k, false))) return rc;
+    if ((rc = axpy_f32_to_f64(c, c->d_w32, c->d_x, n, k, ld))) return rc;
+    if ((rc = gemv_residual(c, c->d_G, n, ld, c->d_x, c->d_rhs, c->d_r, k))) return rc;
+    if ((rc = residual_ratio(c, c->d_r, c->d_rhs, k, &rr, first))) return rc;
+    if ((rc = consume_status(c))) return rc;
+    first = false;
+    c->last.ir_iters = it + 1;
+    if (rr <= o.ir_tol) { converged = true; break; }
+    if (!(rr <= 0.5 * prev)) break;   // stagnating, diverging or not finite: hand over to GMRES-IR
+    prev = rr;
+  }
+  c->last.rel_residual = rr;
+  if (converged) return FP_OK;
+  int it = 0;
+  fp_solve_opts g = o;
+  g.gmres_atol = 0.0;
+  g.gmres_rtol = o.ir_tol;
+  rc = gmres_solve(c, c->d_rhs, c->d_x, k, g, true, &it, &rr);
+  c->last.gmres_iters = it;
+  c->last.used_gmres = 1;
+  c->last.rel_residual = rr;
+  return rc;
 }
 
 int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stats* stats) {
@@ -560,38 +659,26 @@ int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stat
     if (c->factored != FP_PREC_FP64) return c->err.set(FP_ESTATE, "fp_solve: no FP64 factors (call fp_factor)");
     FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_x, c->d_rhs, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if ((rc = lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_x, ld, k, false))) return rc;
+    if (!c->last.gepp_certified && (rc = refine_fp64(c, k, o))) {
+      time_end(c, &c->ms_solve);
+      return rc;
+    }
   } else {
     if (c->factored != FP_PREC_MIXED) return c->err.set(FP_ESTATE, "fp_solve: no FP32 factors (call fp_factor)");
-    // mixed-precision iterative refinement: x0 = A32^-1 b; r = b - A x (FP64); d = A32^-1 r
-    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_x, 0, ld * k * sizeof(double), c->stream));
-    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_r, c->d_rhs, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    double prev = 1e300, rr = 0;
-    bool converged = false, first = true;
-    for (int it = 0; it < o.ir_maxiter; ++it) {
-      if ((rc = convert_f64_f32(c, c->d_r, c->d_w32, n, k, ld, ld))) return rc;
-      if ((rc = lu_solve<float>(c, c->d_G32, n, ld, c->d_ipiv, c->d_w32, ld, k, false))) return rc;
-      if ((rc = axpy_f32_to_f64(c, c->d_w32, c->d_x, n, k, ld))) return rc;
-      if ((rc = gemv_residual(c, c->d_G, n, ld, c->d_x, c->d_rhs, c->d_r, k))) return rc;
-      if ((rc = residual_ratio(c, c->d_r, c->d_rhs, k, &rr, first))) return rc;
-      if ((rc = consume_status(c))) return rc;
-      first = false;
-      c->last.ir_iters = it + 1;
-      if (rr <= o.ir_tol) { converged = true; break; }
-      if (rr > 0.5 * prev) break;   // stagnating or diverging: hand over to GMRES-IR
-      prev = rr;
+    rc = refine_mixed(c, k, o);
+    if (rc == FP_ENOCONV && c->static_order) {
+      // the statically ordered FP32 factors were not good enough even for
+      // GMRES-IR: factor again with pivoting and refine once more
+      double ms_first = 0;
+      time_end(c, &ms_first);
+      if ((rc = fp_factor(c, FP_PREC_MIXED_GEPP))) return rc;
+      c->last.ir_iters = 0;
+      c->last.gmres_iters = 0;
+      c->last.used_gmres = 0;
+      if (time_begin(c)) return FP_ECUDA;
+      rc = refine_mixed(c, k, o);
     }
-    c->last.rel_residual = rr;
-    if (!converged) {
-      int it = 0;
-      fp_solve_opts g = o;
-      g.gmres_atol = 0.0;
-      g.gmres_rtol = o.ir_tol;
-      rc = gmres_solve(c, c->d_rhs, c->d_x, k, g, true, &it, &rr);
-      c->last.gmres_iters = it;
-      c->last.used_gmres = 1;
-      c->last.rel_residual = rr;
-      if (rc) { time_end(c, &c->ms_solve); return rc; }
-    }
+    if (rc) { time_end(c, &c->ms_solve); return rc; }
   }
   if (time_end(c, &c->ms_solve)) return FP_ECUDA;
   c->kms[FP_STAGE_SOLVE] = c->ms_solve;
@@ -621,6 +708,9 @@ int fp_lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k) {
   if (!B || k <= 0 || ldb < c->N) return c->err.set(FP_EINVAL, "fp_lu_solve_noalloc: B must be N x k with ldb >= N");
   if (c->factored != FP_PREC_FP64)
     return c->err.set(FP_ESTATE, "fp_lu_solve_noalloc: no FP64 factors (call fp_factor with FP_PREC_FP64)");
+  if (!c->last.gepp_certified)
+    return c->err.set(FP_ESTATE, "fp_lu_solve_noalloc: the FP64 factors are not certified (a block-local pivot "
+                                 "differs from partial pivoting); fp_solve refines such factors");
   if (int rc = lu_solve_noalloc(c, B, ldb, k)) return rc;
   return consume_status(c);
 }
@@ -636,7 +726,7 @@ int fp_solve_body(fp_ctx* c, int element, double kerneloffset, double kernelcuto
   const int prec = (o.solver == FP_SOLVER_LU) ? o.precision : FP_PREC_FP64;
   if ((rc = fp_assemble(c, element, kerneloffset, kernelcutoff, prec))) return rc;
   if ((rc = fp_set_rhs(c, Uinfs, k))) return rc;
-  if (o.solver == FP_SOLVER_LU || o.precision == FP_PREC_MIXED)
+  if (o.solver == FP_SOLVER_LU || o.precision != FP_PREC_FP64)
     if ((rc = fp_factor(c, o.precision))) return rc;
   return fp_solve(c, x, k, &o, stats);
 }
@@ -662,7 +752,7 @@ int fp_uind(fp_ctx* c, int element, const double* strengths, const double* targe
   if (time_begin(c)) return FP_ECUDA;
   int rc;
   if (element == FP_ELEMENT_VORTEXRING) {
-    rc = launch_uind_ring(c, ds, dt, m, dout, precision == FP_PREC_MIXED);
+    rc = launch_uind_ring(c, ds, dt, m, dout, precision != FP_PREC_FP64);
   } else if (element == FP_ELEMENT_SOURCE_DOUBLET) {   // sources, then doublets (rings without wake)
     const int64_t nsh = c->nsh;
     c->nsh = 0;
@@ -790,7 +880,23 @@ static int adjoint_device(fp_ctx* c, int64_t k) {
   c->adj_relres = 0;
   if (c->factored == FP_PREC_FP64) {
     FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_ax, c->d_ab, ld * k * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    return lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_ax, ld, k, true);
+    if ((rc = lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_ax, ld, k, true))) return rc;
+    if (c->last.gepp_certified) return FP_OK;
+    // uncertified block-local pivots: refine against the FP64 AIC (transposed)
+    double rr = 0, prev = 1e300;
+    for (int it = 0;; ++it) {
+      if ((rc = gemvT_residual(c, c->d_G, n, ld, c->d_ax, c->d_ab, c->d_ar, k))) return rc;
+      if ((rc = residual_ratio(c, c->d_ar, c->d_ab, k, &rr, it == 0, c->d_anorms))) return rc;
+      c->adj_relres = rr;
+      if (rr <= 1e-15 || rr > 0.5 * prev || it == 10) break;
+      prev = rr;
+      if ((rc = lu_solve<double>(c, c->d_LU, n, ld, c->d_ipiv, c->d_ar, ld, k, true))) return rc;
+      if ((rc = axpy_f64(c, c->d_ar, c->d_ax, n, k, ld))) return rc;
+      c->adj_iters = it + 1;
+    }
+    if (rr <= 1e-12) return FP_OK;
+    return c->err.set(FP_ENOCONV, "fp_adjoint_solve: refinement of the uncertified FP64 factors stalled at "
+                                  "relative residual " + std::to_string(rr));
   }
   const double tol = 1e-12;
   const int maxit = 10;

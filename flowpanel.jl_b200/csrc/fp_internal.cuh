@@ -60,7 +60,8 @@ struct fp_ctx {
   bool has_geometry = false;
   int assembled = -1;          // element kind of the assembled G, -1 none
   int assembled_prec = -1;
-  int factored = -1;           // FP_PREC_* of the factors, -1 none
+  int factored = -1;           // FP_PREC_FP64 or FP_PREC_MIXED (either FP32 form) of the factors, -1 none
+  bool static_order = false;   // the FP32 factors were formed without pivot search (fp_lu_static.cu)
   int64_t nrhs = 0;
   double kern_offset = 1e-8;   // kerneloffset of the assembled body
   double kern_cutoff = 1e-14;  // kernelcutoff of the assembled body
@@ -187,6 +188,7 @@ int gemvT_residual(fp_ctx* c, const double* A, int64_t n, int64_t lda, const dou
 int convert_f64_f32(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda,
                     int64_t ldb);
 int axpy_f32_to_f64(fp_ctx* c, const float* d, double* x, int64_t n, int64_t k, int64_t ld);
+int axpy_f64(fp_ctx* c, const double* d, double* x, int64_t n, int64_t k, int64_t ld);
 template <class T>
 int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda);
 // FP64 solve with the context's factors on caller memory, flags of the
@@ -200,6 +202,22 @@ constexpr size_t kMinvBytes = (size_t)2 * kPanelSlots * kLuNB * kLuNB * sizeof(d
 // split-operand scratch of the tensor-core update for scratch set `slot` (fp_tc.cu)
 int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max);
 constexpr int kGemvSplitHost = 16;
+// FP32 LU with a static row order (no pivot search) for the mixed form
+// (fp_lu_static.cu): panels of kStaticPanel columns, identity ipiv, max|L| in
+// cert; DEV_ZERO_PIVOT in the status word on a zero or non-finite pivot
+constexpr int kStaticPanel = 128;
+int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert);
+// FP32 trailing update on tensor cores (fp_tc.cu); returns false if the
+// shape is not supported, in which case the SIMT kernel runs.
+bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
+                     int64_t nn, int kk);
+// The same from operands already split into 3xTF32 hi / lo parts, K-major
+// with ldk floats per row (Ah, Al: m rows; Bh, Bl: nn columns); C column-major (ldc).
+bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const float* Bh, const float* Bl, int ldk,
+                          float* C, int64_t ldc, int64_t m, int64_t nn, int kk);
+// C -= A B on the SIMT pipe (FP32), all three blocks of one matrix (lda)
+int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
+                      int kk);
 
 // induced velocity (fp_field.cu)
 int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_targets, int64_t m,
@@ -241,6 +259,21 @@ struct SmemAttr {
     const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
     return e;
+  }
+};
+
+// Routes the launches of a section to stream2 and its tensor-core scratch.
+struct OnStream2 {
+  fp_ctx* c;
+  cudaStream_t s0;
+  int slot0;
+  explicit OnStream2(fp_ctx* c_) : c(c_), s0(c_->stream), slot0(c_->tc_slot) {
+    c->stream = c->stream2;
+    c->tc_slot = 1;
+  }
+  ~OnStream2() {
+    c->stream = s0;
+    c->tc_slot = slot0;
   }
 };
 

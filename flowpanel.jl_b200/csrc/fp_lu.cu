@@ -23,7 +23,6 @@
 // on, subtract their contribution and multiply by the precomputed inverse of
 // the diagonal block.
 #include <cfloat>
-#include <mutex>
 #include <string>
 
 #include "fp_internal.cuh"
@@ -829,13 +828,6 @@ k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ C
   }
 }
 
-// FP32 trailing update on tensor cores (fp_tc.cu); returns false if the
-// shape is not supported, in which case the SIMT kernel runs.
-bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,
-                     int64_t nn, int kk);
-
-int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
-                      int kk);
 
 // C (m x nn) -= A (m x kk) B (kk x nn); all three are sub-blocks of one
 // column-major matrix with leading dimension lda.
@@ -895,21 +887,6 @@ int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64
 // then the per-block substitutions and updates (k_strip). Columns are split between the
 // streams so that no element is written by both at once.
 constexpr int kOuterNB = kOuterPanel;
-
-// Routes the launches of a section to stream2 and its tensor-core scratch.
-struct OnStream2 {
-  fp_ctx* c;
-  cudaStream_t s0;
-  int slot0;
-  explicit OnStream2(fp_ctx* c_) : c(c_), s0(c_->stream), slot0(c_->tc_slot) {
-    c->stream = c->stream2;
-    c->tc_slot = 1;
-  }
-  ~OnStream2() {
-    c->stream = s0;
-    c->tc_slot = slot0;
-  }
-};
 
 template <class T>
 int lu_factor(fp_ctx* c, T* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
@@ -1855,6 +1832,19 @@ int axpy_f32_to_f64(fp_ctx* c, const float* d, double* x, int64_t n, int64_t k, 
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;
 }
+__global__ void k_axpy_f64(const double* __restrict__ d, double* __restrict__ x, int64_t n, int64_t k, int64_t ld) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * k) return;
+  const int64_t i = t % n, q = t / n;
+  x[q * ld + i] += d[q * ld + i];
+}
+int axpy_f64(fp_ctx* c, const double* d, double* x, int64_t n, int64_t k, int64_t ld) {
+  const int64_t t = n * k;
+  k_axpy_f64<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(d, x, n, k, ld);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
 
 // column norms ||a_q||_2^2 for q < k (one CTA per column)
 __global__ void k_colnorm2(const double* __restrict__ a, int64_t n, int64_t lda, double* __restrict__ out) {
@@ -1901,30 +1891,19 @@ int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, doub
 // on it and return wrong results or FP_ETIMEOUT, so they must be serialised.
 constexpr int64_t kNoAllocMaxN = 65536;
 constexpr int64_t kNoAllocMaxBlocks = kNoAllocMaxN / NB;
-constexpr int kNoAllocMaxDevices = 64;
 static __device__ __align__(256) unsigned int g_trs_scratch[kNoAllocMaxBlocks + 1];
 
-static std::mutex g_trs_scratch_mu;
-static unsigned int* g_trs_scratch_addr[kNoAllocMaxDevices] = {};
-
 // Device address of g_trs_scratch on the context's device, which must be the
-// current device. The first call on a device resolves it with
-// cudaGetSymbolAddress (which can load this library's device code onto that
-// device); later calls return the cached address.
+// current device, resolved on every call with cudaGetSymbolAddress: that
+// allocates nothing once this library's device code is loaded on the device
+// (the first call may load it), and it follows the module when a device reset
+// (cudaDeviceReset, CUDA.device_reset!) reloads it at another address.
 static int trs_scratch_address(fp_ctx* c, unsigned int** out) {
-  if (c->device < 0 || c->device >= kNoAllocMaxDevices)
-    return c->err.set(FP_EINVAL, "fp_lu_solve_noalloc: device index beyond " +
-                                     std::to_string(kNoAllocMaxDevices - 1));
-  std::lock_guard<std::mutex> lock(g_trs_scratch_mu);
-  unsigned int*& slot = g_trs_scratch_addr[c->device];
-  if (!slot) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_trs_scratch);
-    if (e != cudaSuccess)
-      return c->err.set(FP_ECUDA, std::string("cudaGetSymbolAddress(g_trs_scratch): ") + cudaGetErrorString(e));
-    slot = static_cast<unsigned int*>(p);
-  }
-  *out = slot;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_trs_scratch);
+  if (e != cudaSuccess)
+    return c->err.set(FP_ECUDA, std::string("cudaGetSymbolAddress(g_trs_scratch): ") + cudaGetErrorString(e));
+  *out = static_cast<unsigned int*>(p);
   return FP_OK;
 }
 

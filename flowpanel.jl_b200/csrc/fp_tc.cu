@@ -372,6 +372,32 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
   return cudaGetLastError() == cudaSuccess;
 }
 
+bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const float* Bh, const float* Bl, int ldk,
+                          float* C, int64_t ldc, int64_t m, int64_t nn, int kk) {
+  if (kk <= 0 || kk > ldk || m <= 0 || nn <= 0 || (ldk & 3) != 0) return false;
+  if (!tc::encode_fn()) return false;
+  // TMA: 16-byte aligned bases and pitches
+  if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(ldc * 4) | reinterpret_cast<uintptr_t>(Ah) |
+        reinterpret_cast<uintptr_t>(Al) | reinterpret_cast<uintptr_t>(Bh) | reinterpret_cast<uintptr_t>(Bl)) &
+       15) != 0)
+    return false;
+  static SmemAttr attr;
+  if (attr.ensure(tc::k_tc_gemm_sub, tc::SMEM_BYTES) != cudaSuccess) return false;
+  CUtensorMap mAh, mAl, mBh, mBl, mC;
+  if (!tc::make_map(&mAh, Ah, kk, m, ldk, tc::BM) || !tc::make_map(&mAl, Al, kk, m, ldk, tc::BM) ||
+      !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN) ||
+      !tc::make_map_c(&mC, C, m, nn, ldc))
+    return false;
+  dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
+  const int ev = kt_begin(c);
+  TraceScope tr(c, TR_GEMM_TC);
+  tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk,
+                                                                       c->d_status);
+  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
+  ++c->nlaunch;
+  return cudaGetLastError() == cudaSuccess;
+}
+
 // ---------------------------------------------------------------------------
 // Self-test: C0 - A B for random A (m x k), B (k x n), C0 (m x n) by the
 // tensor-core kernel, by the SIMT kernel and in FP64; errors relative to

@@ -17,6 +17,7 @@ const FP_ELEMENT_VORTEXRING = Cint(1)
 const FP_ELEMENT_SOURCE_DOUBLET = Cint(2)
 const FP_PREC_FP64 = Cint(0)
 const FP_PREC_MIXED = Cint(1)
+const FP_PREC_MIXED_GEPP = Cint(2)
 const FP_SOLVER_LU = Cint(0)
 const FP_SOLVER_GMRES = Cint(1)
 const FP_UGRADMU_COMBINED = Cint(0)
@@ -32,6 +33,7 @@ struct FPSolveOpts
     gmres_atol::Cdouble
     gmres_rtol::Cdouble
     gmres_itmax::Cint
+    gmres_restart::Cint   # 0: Krylov.jl's gmres without restart (the reference's call); 1: GMRES(memory)
 end
 
 struct FPStats
@@ -51,8 +53,9 @@ end
 
 GPU drop-in for the `solver` keyword of `solve`: owns a device context that
 assembles, factors and solves on a B200. `method` is `:ludiv`, `:backslash`
-(both LU) or `:gmres`; `precision` is `:fp64` (plain) or `:mixed` (FP32
-tensor-core factors with FP64 refinement).
+(both LU) or `:gmres`; `precision` is `:fp64` (plain), `:mixed` (FP32
+tensor-core factors with a static row order and FP64 refinement) or
+`:mixed_gepp` (the same factors pivoted as the FP64 form).
 """
 mutable struct B200Solver
     ctx::Ptr{Cvoid}
@@ -67,8 +70,9 @@ mutable struct B200Solver
         rc = ccall((:fp_ctx_create, libfp), Cint, (Cint, Ref{Ptr{Cvoid}}), device, r)
         rc == FP_OK || error("fp_ctx_create failed on device $device (status $rc)")
         opts = FPSolveOpts(method == :gmres ? FP_SOLVER_GMRES : FP_SOLVER_LU,
-                           precision == :mixed ? FP_PREC_MIXED : FP_PREC_FP64, ir_tol, ir_maxiter,
-                           gmres_memory, atol, rtol, itmax)
+                           precision == :mixed ? FP_PREC_MIXED :
+                           precision == :mixed_gepp ? FP_PREC_MIXED_GEPP : FP_PREC_FP64, ir_tol, ir_maxiter,
+                           gmres_memory, atol, rtol, itmax, Cint(0))
         s = new(r[], opts, nothing, Int32[], Int32[], zeros(Int32, 6, 0))
         finalizer(x -> ccall((:fp_ctx_destroy, libfp), Cint, (Ptr{Cvoid},), x.ctx), s)
         return s

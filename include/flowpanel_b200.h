@@ -49,7 +49,11 @@ extern "C" {
 
 /* precision forms */
 #define FP_PREC_FP64 0   /* FP64 assembly + FP64 LU (the plain form) */
-#define FP_PREC_MIXED 1  /* FP32 factor (3xTF32 tensor-core update) + FP64 refinement */
+#define FP_PREC_MIXED 1  /* FP32 factors with a static row order (no pivot search; 3xTF32 tensor-core
+                            update) + FP64 refinement, GMRES-IR behind it; a zero pivot, or refinement
+                            that fails, falls back to FP_PREC_MIXED_GEPP */
+#define FP_PREC_MIXED_GEPP 2  /* FP32 factors pivoted as the FP64 form (partial pivoting inside each
+                                 64-row diagonal block) + FP64 refinement */
 
 /* solvers */
 #define FP_SOLVER_LU 0     /* solve_ludiv! / solve_backslash! */
@@ -66,6 +70,8 @@ typedef struct fp_solve_opts {
   double gmres_atol;   /* <0: sqrt(eps) */
   double gmres_rtol;   /* <0: sqrt(eps) */
   int gmres_itmax;     /* <=0: 2N */
+  int gmres_restart;   /* 0: one Arnoldi process whose basis grows past gmres_memory (Krylov.jl 0.9's
+                          gmres with restart = false, the reference's call); 1: GMRES(gmres_memory) */
 } fp_solve_opts;
 
 typedef struct fp_stats {
@@ -139,9 +145,11 @@ int fp_solve(fp_ctx* ctx, double* x, int64_t k, const fp_solve_opts* opts, fp_st
  * Limit: n <= 65536 (FP_EINVAL beyond): the triangular solves keep their
  * ready flags and ticket counter in a fixed static device array (4 KiB per
  * device); each sweep zeroes them itself, so nothing needs initialising.
- * The first call on each device resolves that array's address
- * (cudaGetSymbolAddress, which can load the library's device code onto the
- * device): make it before any stream capture. Calls that overlap in time on
+ * Every call resolves that array's address with cudaGetSymbolAddress; the
+ * first call on a device can load the library's device code onto it, so make
+ * that call before any stream capture. FP64 factors whose block-local pivots
+ * are not certified (fp_stats.gepp_certified == 0) are refused with
+ * FP_ESTATE: fp_solve refines those. Calls that overlap in time on
  * one device (several host threads, several contexts) share the array and
  * race, giving wrong results or FP_ETIMEOUT: serialise them. */
 int fp_lu_solve_noalloc(fp_ctx* ctx, double* B, int64_t ldb, int64_t k);

@@ -382,58 +382,69 @@ def solve_leastsquares(G, rhs, elprescribe):
     return out, Gls
 
 
-def gmres(A, b, memory=50, atol=None, rtol=None, itmax=None, x0=None):
-    """Restarted GMRES(memory) restating Krylov.jl 0.9's algorithm as the reference
-    calls it (src/FLOWPanel_linearsolver.jl:136-147): modified Gram-Schmidt
-    Arnoldi, Givens rotations, stop when ||r|| <= atol + rtol * ||b||.
+def gmres(A, b, memory=50, atol=None, rtol=None, itmax=None, x0=None, restart=False):
+    """GMRES as the reference calls it (src/FLOWPanel_linearsolver.jl:136-147):
+    Krylov.jl 0.9's gmres, whose default restart=false runs one Arnoldi process
+    (modified Gram-Schmidt) with a basis that grows past `memory` (a storage
+    hint), Givens rotations on the Hessenberg columns, and stops when the
+    rotated residual estimate |z_{k+1}| <= atol + rtol ||r0|| (or on a
+    breakdown h_{k+1,k} <= eps^(3/4), or after itmax = 2n steps).
+    restart=True gives GMRES(memory), restarted from the true residual.
     Returns (x, niter, converged)."""
     eps = np.finfo(np.float64).eps
     atol = np.sqrt(eps) if atol is None else atol
     rtol = np.sqrt(eps) if rtol is None else rtol
+    btol = eps ** 0.75
     n = len(b)
     itmax = 2 * n if itmax is None else itmax
     x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
     r = b - A @ x if x0 is not None else b.copy()
-    bnorm = np.linalg.norm(b)
-    eps_stop = atol + rtol * bnorm
     beta = np.linalg.norm(r)
+    eps_stop = atol + rtol * beta
     it = 0
     if beta <= eps_stop:
         return x, 0, True
     while it < itmax:
-        V = np.zeros((memory + 1, n))
-        H = np.zeros((memory + 1, memory))
-        cs, sn = np.zeros(memory), np.zeros(memory)
-        g = np.zeros(memory + 1)
-        g[0] = beta
-        V[0] = r / beta
-        k_done = 0
-        for k in range(memory):
+        V = [r / beta]
+        cols = []                        # rotated Hessenberg columns
+        cs, sn, z = [], [], [beta]
+        solved = False
+        while it < itmax and not (restart and len(cols) >= memory):
+            k = len(cols)
             w = A @ V[k]
-            for i in range(k + 1):
-                H[i, k] = np.dot(V[i], w)
-                w = w - H[i, k] * V[i]
-            H[k + 1, k] = np.linalg.norm(w)
-            if H[k + 1, k] != 0:
-                V[k + 1] = w / H[k + 1, k]
+            h = np.zeros(k + 2)
+            for i in range(k + 1):       # modified Gram-Schmidt
+                h[i] = np.dot(V[i], w)
+                w = w - h[i] * V[i]
+            h[k + 1] = np.linalg.norm(w)
+            breakdown = h[k + 1] <= btol
+            if not breakdown:
+                V.append(w / h[k + 1])
             for i in range(k):
-                t = cs[i] * H[i, k] + sn[i] * H[i + 1, k]
-                H[i + 1, k] = -sn[i] * H[i, k] + cs[i] * H[i + 1, k]
-                H[i, k] = t
-            den = np.hypot(H[k, k], H[k + 1, k])
-            cs[k], sn[k] = H[k, k] / den, H[k + 1, k] / den
-            H[k, k] = den
-            H[k + 1, k] = 0.0
-            g[k + 1] = -sn[k] * g[k]
-            g[k] = cs[k] * g[k]
+                t = cs[i] * h[i] + sn[i] * h[i + 1]
+                h[i + 1] = -sn[i] * h[i] + cs[i] * h[i + 1]
+                h[i] = t
+            den = np.hypot(h[k], h[k + 1])
+            cs.append(h[k] / den)
+            sn.append(h[k + 1] / den)
+            h[k], h[k + 1] = den, 0.0
+            z.append(-sn[k] * z[k])
+            z[k] = cs[k] * z[k]
+            cols.append(h)
             it += 1
-            k_done = k + 1
-            if abs(g[k + 1]) <= eps_stop or it >= itmax:
+            solved = abs(z[k + 1]) <= eps_stop
+            if solved or breakdown:
                 break
-        y = np.linalg.solve(np.triu(H[:k_done, :k_done]), g[:k_done])
-        x = x + V[:k_done].T @ y
+        kd = len(cols)
+        R = np.zeros((kd, kd))
+        for j, h in enumerate(cols):
+            R[:j + 1, j] = h[:j + 1]
+        y = np.linalg.solve(np.triu(R), np.asarray(z[:kd]))
+        x = x + np.asarray(V[:kd]).T @ y
         r = b - A @ x
         beta = np.linalg.norm(r)
+        if not restart:
+            return x, it, solved
         if beta <= eps_stop:
             return x, it, True
     return x, it, False

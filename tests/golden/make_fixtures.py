@@ -44,4 +44,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2 and not os.environ.get("FLOWPANEL_REFERENCE"):
+        sys.exit("usage: make_fixtures.py /path/to/FLOWPanel.jl  (or set FLOWPANEL_REFERENCE)")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ["FLOWPANEL_REFERENCE"])

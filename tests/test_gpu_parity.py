@@ -65,7 +65,7 @@ def test_source_aic_matches_oracle(fp, O, ctx):
     assert np.abs(G - Gr).max() <= 1e-12 * np.abs(Gr).max()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_gepp"])
 def test_wing_solve_matches_oracle(fp, O, ctx, precision):
     w, body, normals, cps, D, U = _wing_setup(fp, 40, 48)
     ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
@@ -88,7 +88,7 @@ def test_multi_rhs_sweep(fp, O, ctx):
     Us = np.stack([np.tile(freestream(a), (w.npanels, 1)) for a in aoas])
     Gr = O.assemble_vortexring(w, cps, normals, D, D)
     lu = O.lu_factor(Gr)
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed", "mixed_gepp"):
         X, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, Us, opts=fp._capi.make_opts("ludiv", prec))
         for q in range(len(aoas)):
             xr = O.lu_solve(lu, O.rhs_noflowthrough(Us[q], normals))
@@ -106,9 +106,15 @@ def test_gmres_matches_oracle(fp, O, ctx):
     xr = O.solve_ludiv(Gr, b)
     assert st.used_gmres == 1 and st.gmres_iters > 0
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-9
-    # same restarted GMRES(50) on the CPU converges in a comparable number of steps
+    # the oracle's GMRES (Krylov.jl's unrestarted process) takes the same steps
     xg, it, conv = O.gmres(Gr, b, atol=1e-13, rtol=1e-13)
-    assert conv and abs(it - st.gmres_iters) <= max(5, 0.2 * it)
+    assert conv and abs(it - st.gmres_iters) <= 2
+    # GMRES(50) through the restart option converges too
+    opts = fp._capi.make_opts("gmres", "fp64", gmres_atol=1e-13, gmres_rtol=1e-13, gmres_restart=True)
+    x2, st2 = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=opts)
+    assert np.linalg.norm(x2 - xr) / np.linalg.norm(xr) < 1e-9
+    xg2, it2, conv2 = O.gmres(Gr, b, atol=1e-13, rtol=1e-13, restart=True)
+    assert conv2 and abs(it2 - st2.gmres_iters) <= max(5, 0.2 * it2)
 
 
 def test_uind_matches_oracle(fp, O, ctx):
@@ -209,3 +215,123 @@ def test_factor_trace(fp, ctx):
         assert np.all(a[1:] >= b[:-1] - 1e-3)   # launches on one stream do not overlap
     ctx.factor(cap.FP_PREC_MIXED)
     assert len(ctx.trace_read()[0]) == 0
+
+
+# ------------------------------------------------------------------ pinned to the reference's records
+@pytest.fixture(scope="module")
+def vtu_wing(fp, O):
+    from test_oracle_ugradmu import vtu_wing_oracle
+    w = vtu_wing_oracle(fp, O)
+    w["G"] = O.assemble_vortexring(w["mesh"], w["cps"], w["normals"], w["D"], w["D"])
+    w["b"] = O.rhs_noflowthrough(w["Uinfs"], w["normals"])
+    return w
+
+
+@pytest.mark.parametrize("tol,niter", [(1e-8, 286), (1e-2, 88), (1e-1, 25)])
+def test_gmres_published_iterations_vtu_wing(fp, O, ctx, vtu_wing, tol, niter):
+    """solve_gmres! on the reference's swept-wing mesh takes the iteration
+    counts the reference records (docs/resources/data/sweptwing000-gmres{8,2,1}.md:
+    286, 88, 25; examples/sweptwing_solverbenchmark.jl:100-155). The device
+    orthogonalises by classical Gram-Schmidt twice instead of modified
+    Gram-Schmidt, which can move the step where the estimate crosses the
+    tolerance by one. Strengths: relative to the oracle's GMRES iterate,
+    max(1e-6, 1e-2 tol): an iterate stopped at a loose tolerance carries more
+    of the orthogonalisation's rounding than a converged one (3e-5 at 1e-2)."""
+    w = vtu_wing
+    m = w["mesh"]
+    ctx.set_geometry(m.nodes, m.panel_offsets, m.panel_nodes, w["cps"], w["normals"])
+    ctx.set_wake(m.shedding, w["D"], w["D"])
+    opts = fp._capi.make_opts("gmres", "fp64", gmres_atol=tol, gmres_rtol=tol)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, w["Uinfs"], opts=opts)
+    assert st.used_gmres == 1
+    assert abs(st.gmres_iters - niter) <= 1, st.gmres_iters
+    xo, ito, conv = O.gmres(w["G"], w["b"], atol=tol, rtol=tol)
+    assert conv and ito == niter
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < max(1e-6, 1e-2 * tol)
+
+
+def test_mixed_gmres_ir_fallback(fp, O, ctx):
+    """With one refinement step allowed the mixed solve hands over to GMRES-IR
+    (right-preconditioned by the FP32 factors) and still reaches the FP64
+    solution to 1e-10."""
+    w, body, normals, cps, D, U = _wing_setup(fp, 40, 48)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    opts = fp._capi.make_opts("ludiv", "mixed", ir_maxiter=1)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=opts)
+    assert st.ir_iters == 1 and st.used_gmres == 1 and st.gmres_iters > 0, st.asdict()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+    assert st.rel_residual < 1e-11
+
+
+@pytest.mark.parametrize("tri", [False, True])
+def test_sphere_strengths_match_oracle(fp, O, ctx, tri):
+    """Config-1 sphere (30 x 60 cells: 1,800 source panels with 3-node pole
+    rows, or 3,600 triangles): sigma = G \\ lambda against the oracle's
+    assembly and LAPACK solve (src/FLOWPanel_nonliftingbody.jl:93-130) to
+    1e-10 relative."""
+    s = fp.meshes.sphere(1.0, 30, 60)
+    if tri:
+        s = fp.meshes.triangulate(s)
+    body = fp.NonLiftingBody(s)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    U = np.tile([1.0, 0.0, 0.0], (s.npanels, 1))
+    ctx.set_geometry(s.nodes, s.panel_offsets, s.panel_nodes, cps, normals)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_SOURCE, U, opts=fp._capi.make_opts("ludiv", "fp64"))
+    Gr = O.assemble_source(s, cps, normals)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+    assert st.gepp_certified == 1
+
+
+def _shuffled_wing(fp, nc, ns, seed):
+    """The wing with its panels listed in a seeded random order (as an
+    unstructured mesher may list them); shedding rows follow their panels."""
+    w = fp.meshes.swept_wing("0012", nc, ns)
+    perm = np.random.default_rng(seed).permutation(w.npanels)   # new panel i = old panel perm[i]
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(w.npanels)
+    counts = np.diff(w.panel_offsets)[perm]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    pn = np.concatenate([w.panel(p) for p in perm]).astype(np.int32)
+    sh = w.shedding.copy()
+    sh[:, 0] = inv[sh[:, 0]]
+    sh[:, 3] = np.where(sh[:, 3] >= 0, inv[np.maximum(sh[:, 3], 0)], -1)
+    return fp.meshes.Mesh(w.nodes, offs, pn, sh, w.bodies)
+
+
+def test_uncertified_pivots_are_refined(fp, O, ctx):
+    """Panels in a shuffled order put column maxima outside the 64-row
+    diagonal blocks, so the block-local pivots are not LAPACK's (max|L| > 1).
+    The FP64 solve then refines against the FP64 AIC and still matches
+    LAPACK's solution to 1e-10, as does the adjoint (transposed) solve; the
+    allocation-free solve refuses those factors."""
+    import ctypes
+    w = _shuffled_wing(fp, 20, 24, seed=0)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    V = freestream(4.2)
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "fp64"))
+    assert st.gepp_certified == 0 and st.max_abs_L > 1.0, st.asdict()
+    assert st.ir_iters >= 1
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    lu = O.lu_factor(Gr)
+    xr = O.lu_solve(lu, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+    ybar = np.random.default_rng(1).standard_normal(w.npanels)
+    lam = ctx.adjoint_solve(ybar)
+    lr = np.linalg.solve(Gr.T, ybar)
+    assert np.linalg.norm(lam.ravel() - lr) / np.linalg.norm(lr) < 1e-10
+    fake = ctypes.c_void_p(1 << 40)   # never dereferenced: the call is refused first
+    assert fp._capi.lib().fp_lu_solve_noalloc(ctx.h, fake, w.npanels, 1) == fp._capi.FP_ESTATE
+    # the mixed form's static row order on the same shuffled panels still refines to the FP64 solution
+    xm, stm = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
+    assert np.linalg.norm(xm - xr) / np.linalg.norm(xr) < 1e-10, stm.asdict()

@@ -18,10 +18,15 @@ def test_tc_update_matches_fp64(fp, m, n, k):
     assert err_tc <= 4 * err_simt + 1e-7, (err_tc, err_simt)
 
 
-def test_mixed_lu_refines_in_few_steps(fp, O, ctx):
+@pytest.mark.parametrize("nc,ns", [(8, 4), (12, 8), (20, 24), (40, 48), (60, 80)])
+@pytest.mark.parametrize("precision", ["mixed", "mixed_gepp"])
+def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
     """With the tensor-core update the FP32 factors stay FP32-accurate: the
-    FP64 refinement converges to 1e-12 in a handful of steps, without GMRES."""
-    w = fp.meshes.swept_wing("0012", 60, 80)
+    FP64 refinement converges to 1e-12 in a handful of steps, without GMRES,
+    for the static row order (mixed) and the pivoted factors (mixed_gepp);
+    sizes from one partial panel (32, 96 panels) to many panels with a partial
+    last one (480, 1920, 4800)."""
+    w = fp.meshes.swept_wing("0012", nc, ns)
     body = fp.RigidWakeBody(w)
     normals = fp.calc_normals(body)
     cps = fp.calc_controlpoints(body, normals)
@@ -31,8 +36,9 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx):
     U = np.tile(V, (w.npanels, 1))
     ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
     ctx.set_wake(w.shedding, D, D)
-    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", precision))
     assert st.used_gmres == 0 and st.ir_iters <= 5, st.asdict()
+    assert st.max_abs_L < 10.0   # multipliers of order one (0 when there are no rows below a diagonal block)
     Gr = O.assemble_vortexring(w, cps, normals, D, D)
     xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10

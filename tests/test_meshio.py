@@ -6,7 +6,10 @@ import numpy as np
 import pytest
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_DATA = "/root/reference/examples/data"
+# the reference checkout's example data, when FLOWPANEL_REFERENCE names a checkout
+# (the fixture comparison below is skipped otherwise)
+REF_DATA = os.path.join(os.environ.get("FLOWPANEL_REFERENCE", ""), "examples", "data") \
+    if os.environ.get("FLOWPANEL_REFERENCE") else ""
 
 # trailing edges of test/runtests_meshes.jl:198-206 (left half; the right one mirrors y)
 TE_X1 = {"L": [1.74244, -1.2446, 1.38094e-07], "R": [1.74244, 1.2446, 1.38094e-07]}
@@ -144,7 +147,8 @@ $EndElements
     assert te.npanels == 0 and te.nnodes == 3 and np.allclose(te.nodes[:, 0], [0, 0.5, 1])
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference example data not present")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA),
+                    reason="set FLOWPANEL_REFERENCE to a FLOWPanel.jl checkout to compare the fixtures")
 def test_fixtures_match_reference_files(fp):
     for side, f in (("L", "sweptwing-left000.vtu"), ("R", "sweptwing-right000.vtu")):
         m = fp.meshio.read_vtu(os.path.join(REF_DATA, f))

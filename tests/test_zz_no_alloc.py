@@ -55,11 +55,18 @@ def test_noalloc_matches_fp_solve_twice(fp, nc, ns, k):
         b = _rhs(normals, Vs)
         ldb = n + 5   # a leading dimension larger than N
         scale = np.abs(x_ref).max()
+        Bs = []
         for call in range(2):
             B = torch.zeros((k, ldb), dtype=torch.float64, device="cuda:0")
             B[:, :n] = torch.from_numpy(b)
-            torch.cuda.synchronize()   # the library's stream does not wait for torch's
+            Bs.append(B)
+        torch.cuda.synchronize()   # the library's stream does not wait for torch's
+        for call, B in enumerate(Bs):
+            free0 = torch.cuda.mem_get_info(0)[0]
             ctx.lu_solve_noalloc(B.data_ptr(), ldb, k)
+            free1 = torch.cuda.mem_get_info(0)[0]
+            if call == 1:   # the first call may load device code; after it nothing is allocated
+                assert free1 == free0, f"device free memory moved by {free0 - free1} bytes"
             x = B[:, :n].cpu().numpy()
             err = np.abs(x - x_ref).max() / scale
             assert err <= TOL, f"call {call}: max relative difference {err:.3e}"
