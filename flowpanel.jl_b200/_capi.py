@@ -16,8 +16,8 @@ LIB_PATH = os.path.join(HERE, "_build", "libflowpanel_b200.so")
 
 FP_OK, FP_EINVAL, FP_ESINGULAR, FP_ENOCONV, FP_ECUDA, FP_ETIMEOUT, FP_ESTATE = range(7)
 FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING, FP_ELEMENT_SOURCE_DOUBLET = 0, 1, 2
-FP_PREC_FP64, FP_PREC_MIXED, FP_PREC_MIXED_GEPP = 0, 1, 2
-_PRECISIONS = {"fp64": FP_PREC_FP64, "mixed": FP_PREC_MIXED, "mixed_gepp": FP_PREC_MIXED_GEPP}
+FP_PREC_FP64, FP_PREC_MIXED, FP_PREC_MIXED_GEPP, FP_PREC_BF16 = 0, 1, 2, 3
+_PRECISIONS = {"fp64": FP_PREC_FP64, "mixed": FP_PREC_MIXED, "mixed_gepp": FP_PREC_MIXED_GEPP, "bf16": FP_PREC_BF16}
 FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
 FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP, FP_STAGE_POST = range(7)
 FP_UGRADMU_COMBINED, FP_UGRADMU_CELL, FP_UGRADMU_NODE = 0, 1, 2
@@ -29,7 +29,9 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
            "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls",
-           "fp_ugradmu", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads")
+           "fp_ugradmu", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads",
+           "fp_set_tuning")
+FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES = 0, 1, 2
 
 
 class SolveOpts(C.Structure):
@@ -86,6 +88,7 @@ def lib():
         L.fp_get_aic.argtypes = [vp, _dp]
         L.fp_set_rhs.argtypes = [vp, _dp, C.c_int64]
         L.fp_factor.argtypes = [vp, C.c_int]
+        L.fp_set_tuning.argtypes = [vp, C.c_int, C.c_int]
         L.fp_solve.argtypes = [vp, _dp, C.c_int64, C.POINTER(SolveOpts), C.POINTER(Stats)]
         L.fp_solve_body.argtypes = [vp, C.c_int, C.c_double, C.c_double, _dp, C.c_int64,
                                     C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
@@ -369,6 +372,10 @@ class Context:
         self._chk(self._L.fp_trace_read(self.h, k, _i(tags), _i(streams), t0.ctypes.data_as(C.POINTER(C.c_float)),
                                         t1.ctypes.data_as(C.POINTER(C.c_float)), C.byref(n)))
         return tags, streams, t0, t1
+
+    def set_tuning(self, knob, value):
+        """fp_set_tuning: FP_TUNE_TC_STAGES (2 or 3), FP_TUNE_LU_OVERLAP (0 or 1)."""
+        self._chk(self._L.fp_set_tuning(self.h, int(knob), int(value)))
 
     def kernel_timing(self, enable=True):
         """Per-launch event timing of the factorisation's trailing update."""

@@ -231,14 +231,15 @@ class B200Solver:
     method: "ludiv" | "backslash" (LU, same on the device) | "gmres"
     precision: "fp64" (plain) | "mixed" (FP32 factors with a static row order
         + FP64 refinement) | "mixed_gepp" (FP32 factors pivoted as the FP64
-        form + FP64 refinement)
+        form + FP64 refinement) | "bf16" (BF16 tensor-core operands, GMRES-IR
+        with FP64 residuals; the largest meshes)
     """
 
     def __init__(self, method="ludiv", precision="fp64", device=0, ir_tol=1e-12, ir_maxiter=10,
                  gmres_memory=50, atol=None, rtol=None, itmax=0):
         if method not in ("ludiv", "backslash", "gmres"):
             raise ValueError(f"unknown method {method}")
-        if precision not in ("fp64", "mixed", "mixed_gepp"):
+        if precision not in ("fp64", "mixed", "mixed_gepp", "bf16"):
             raise ValueError(f"unknown precision {precision}")
         self.method, self.precision = method, precision
         self.opts = _capi.make_opts("gmres" if method == "gmres" else "ludiv", precision, ir_tol, ir_maxiter,

@@ -371,14 +371,16 @@ int fp_assemble(fp_ctx* c, int element, double kerneloffset, double kernelcutoff
   if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_assemble: no geometry");
   if (element != FP_ELEMENT_SOURCE && element != FP_ELEMENT_VORTEXRING)
     return c->err.set(FP_EINVAL, "fp_assemble: unknown element");
-  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP)
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP &&
+      precision != FP_PREC_BF16)
     return c->err.set(FP_EINVAL, "fp_assemble: unknown precision");
   const size_t elems = (size_t)c->ld * c->capN;   // for the largest body the buffers hold
   if (!c->d_G) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G, elems * sizeof(double)));
     FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G, 0, elems * sizeof(double), c->stream));
   }
-  const bool w32 = precision != FP_PREC_FP64;
+  // the FP32 copy for the FP32 factorisations (the BF16 form rounds its copy from G at fp_factor)
+  const bool w32 = precision == FP_PREC_MIXED || precision == FP_PREC_MIXED_GEPP;
   if (w32 && !c->d_G32) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G32, elems * sizeof(float)));
     FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_G32, 0, elems * sizeof(float), c->stream));
@@ -459,7 +461,8 @@ int fp_factor(fp_ctx* c, int precision) {
   if (check_ctx(c)) return FP_EINVAL;
   cudaSetDevice(c->device);
   if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_factor: assemble first");
-  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP)
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP &&
+      precision != FP_PREC_BF16)
     return c->err.set(FP_EINVAL, "fp_factor: unknown precision");
   if (int rc = alloc_factor_buffers(c, precision)) return rc;
   if (time_begin(c)) return FP_ECUDA;
@@ -471,7 +474,11 @@ int fp_factor(fp_ctx* c, int precision) {
     rc = lu_factor<double>(c, c->d_LU, c->N, c->ld, c->d_ipiv, c->d_cert);
     if (!rc) rc = lu_diag_inverses<double>(c, c->d_LU, c->N, c->ld);
   } else {
-    if (c->assembled_prec != FP_PREC_MIXED && c->assembled_prec != FP_PREC_MIXED_GEPP) {
+    const bool bf16 = precision == FP_PREC_BF16;
+    if (bf16) {   // the AIC the factorisation starts from is the BF16-rounded one
+      rc = convert_f64_bf16(c, c->d_G, c->d_G32, c->N, c->N, c->ld, c->ld);
+      if (rc) return rc;
+    } else if (c->assembled_prec != FP_PREC_MIXED && c->assembled_prec != FP_PREC_MIXED_GEPP) {
       rc = convert_f64_f32(c, c->d_G, c->d_G32, c->N, c->N, c->ld, c->ld);
       if (rc) return rc;
     }
@@ -479,7 +486,7 @@ int fp_factor(fp_ctx* c, int precision) {
     if (!pivoted) {
       // static row order; a zero or non-finite pivot falls back to the pivoted
       // factorisation of a fresh FP32 copy of the AIC
-      rc = lu_factor_static(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert);
+      rc = lu_factor_static(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert, bf16);
       if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
       if (rc) return rc;
       if (time_end(c, &ms_static)) return FP_ECUDA;
@@ -700,6 +707,25 @@ int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stat
   c->last.ms_solve = c->ms_solve;
   if (stats) *stats = c->last;
   return FP_OK;
+}
+
+int fp_set_tuning(fp_ctx* c, int knob, int value) {
+  if (check_ctx(c)) return FP_EINVAL;
+  switch (knob) {
+    case FP_TUNE_TC_STAGES:
+      if (value != 2 && value != 3) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_STAGES is 2 or 3");
+      c->tc_stages = value;
+      return FP_OK;
+    case FP_TUNE_LU_OVERLAP:
+      c->lu_overlap = value != 0;
+      return FP_OK;
+    case FP_TUNE_TC_TILES:
+      if (value < 0 || value > 64) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_TILES is 0..64");
+      c->tc_tiles = value;
+      return FP_OK;
+    default:
+      return c->err.set(FP_EINVAL, "fp_set_tuning: unknown knob");
+  }
 }
 
 int fp_lu_solve_noalloc(fp_ctx* c, double* B, int64_t ldb, int64_t k) {

@@ -137,6 +137,9 @@ struct fp_ctx {
   KernelTimer ktimer;           // trailing-update launches of fp_factor
   Trace trace;                  // timeline of fp_factor (off by default)
   bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
+  int tc_stages = 2;            // ring depth of that update in the static-order LU (fp_set_tuning)
+  int tc_tiles = 0;             // static-order LU: output tiles per CTA of the multi-tile update, 0 = one-tile kernel
+  bool lu_overlap = true;       // static-order LU: trailing update on the second stream (fp_set_tuning)
   // split operands (Ah, Al, Bh, Bl) of the tensor-core update, one set per
   // stream of the look-ahead factorisation (slot 0: c->stream, 1: stream2)
   float* d_tc[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};
@@ -206,7 +209,12 @@ constexpr int kGemvSplitHost = 16;
 // (fp_lu_static.cu): panels of kStaticPanel columns, identity ipiv, max|L| in
 // cert; DEV_ZERO_PIVOT in the status word on a zero or non-finite pivot
 constexpr int kStaticPanel = 128;
-int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert);
+// bf16: the trailing update multiplies BF16 operands (kind::f16, FP32 accumulation)
+int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert, bool bf16 = false);
+bool tc_gemm_sub_bf16(fp_ctx* c, const void* Ah, const void* Bh, int ldk, float* C, int64_t ldc, int64_t m,
+                      int64_t nn, int kk);
+// b = FP32 copy of the FP64 a rounded to BF16 values
+int convert_f64_bf16(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda, int64_t ldb);
 // FP32 trailing update on tensor cores (fp_tc.cu); returns false if the
 // shape is not supported, in which case the SIMT kernel runs.
 bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m,

@@ -22,6 +22,8 @@
 // blocks by ticket (atomic counter), wait (bounded) for the blocks they depend
 // on, subtract their contribution and multiply by the precomputed inverse of
 // the diagonal block.
+#include <cuda_bf16.h>
+
 #include <cfloat>
 #include <string>
 
@@ -829,6 +831,105 @@ k_gemm_sub(const T* __restrict__ Am, const T* __restrict__ Bm, T* __restrict__ C
 }
 
 
+// ----------------------------------------------------------------------------
+// FP64 trailing update C -= A B: 128 x 128 tiles, 256 threads with 8 x 8
+// register tiles, 16-deep K slices streamed by cp.async through a 3-stage
+// shared-memory ring (the next two slices are in flight while one is
+// multiplied), C read and written once at the end. A slice of A is 16
+// columns of 128 rows (Asm[k][row]); a slice of B is 16 rows of 128 columns,
+// kept column by column (Bsm[col][k]), so both come in 16-byte pieces of the
+// column-major matrix.
+namespace d64 {
+constexpr int BM = 128, BN = 128, BK = 16, TM = 8, TN = 8, STAGES = 3, NT = (BM / TM) * (BN / TN);
+constexpr int BP = BK + 2;   // row pitch of Bsm (doubles): 16-byte rows
+__host__ __device__ constexpr size_t stage_doubles() { return (size_t)BK * BM + (size_t)BN * BP; }
+constexpr size_t smem() { return STAGES * stage_doubles() * sizeof(double); }
+}  // namespace d64
+
+__device__ __forceinline__ void cp_async16_sz(void* smem, const void* gmem, int bytes) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(d64::NT, 1)
+k_gemm_sub_f64(const double* __restrict__ Am, const double* __restrict__ Bm, double* __restrict__ Cm, int64_t lda,
+               int64_t m, int64_t nn, int kk) {
+  using namespace d64;
+  extern __shared__ __align__(16) unsigned char gsm[];
+  double* const ring = reinterpret_cast<double*>(gsm);
+  const int tid = threadIdx.x;
+  const int tx = tid % (BM / TM), ty = tid / (BM / TM);
+  const int64_t i0 = (int64_t)blockIdx.x * BM, j0 = (int64_t)blockIdx.y * BN;
+  const int nk = (kk + BK - 1) / BK;
+  // one K slice into stage s: 1024 16-byte pieces of A and 1024 of B, 4 + 4 per thread
+  auto issue = [&](int kb, int s) {
+    double* As = ring + (size_t)s * stage_doubles();
+    double* Bs = As + BK * BM;
+    const int k0 = kb * BK;
+#pragma unroll
+    for (int u = 0; u < (BK * BM / 2) / NT; ++u) {
+      const int q = tid + u * NT;
+      const int kq = q / (BM / 2), ii = (q % (BM / 2)) * 2;
+      const int64_t gi = i0 + ii;
+      const bool kin = k0 + kq < kk;
+      const int rows = kin ? (int)imin64(2, m - gi) : 0;
+      const double* src = (rows > 0) ? Am + (int64_t)(k0 + kq) * lda + gi : Am;
+      cp_async16_sz(As + kq * BM + ii, src, rows > 0 ? rows * 8 : 0);
+    }
+#pragma unroll
+    for (int u = 0; u < (BK * BN / 2) / NT; ++u) {
+      const int q = tid + u * NT;
+      const int jj = q / (BK / 2), kq = (q % (BK / 2)) * 2;
+      const int64_t gj = j0 + jj;
+      const int ks = (gj < nn) ? (int)imin64(2, kk - (k0 + kq)) : 0;
+      const double* src = (ks > 0) ? Bm + gj * lda + k0 + kq : Bm;
+      cp_async16_sz(Bs + jj * BP + kq, src, ks > 0 ? ks * 8 : 0);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nk) issue(s, s);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  double acc[TM][TN];
+#pragma unroll
+  for (int a = 0; a < TM; ++a)
+#pragma unroll
+    for (int b = 0; b < TN; ++b) acc[a][b] = 0.0;
+#pragma unroll 1
+  for (int kb = 0; kb < nk; ++kb) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");
+    __syncthreads();   // slice kb has landed for every thread; slot (kb - 1) % STAGES is free
+    if (kb + STAGES - 1 < nk) issue(kb + STAGES - 1, (kb + STAGES - 1) % STAGES);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const double* As = ring + (size_t)(kb % STAGES) * stage_doubles();
+    const double* Bs = As + BK * BM;
+#pragma unroll
+    for (int kq = 0; kq < BK; ++kq) {
+      double a[TM], b[TN];
+#pragma unroll
+      for (int u = 0; u < TM; ++u) a[u] = As[kq * BM + tx + u * (BM / TM)];
+#pragma unroll
+      for (int v = 0; v < TN; ++v) b[v] = Bs[(ty + v * (BN / TN)) * BP + kq];
+#pragma unroll
+      for (int u = 0; u < TM; ++u)
+#pragma unroll
+        for (int v = 0; v < TN; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+#pragma unroll
+  for (int v = 0; v < TN; ++v) {
+    const int64_t gj = j0 + ty + v * (BN / TN);
+    if (gj >= nn) continue;
+#pragma unroll
+    for (int u = 0; u < TM; ++u) {
+      const int64_t gi = i0 + tx + u * (BM / TM);
+      if (gi < m) Cm[gj * lda + gi] -= acc[u][v];
+    }
+  }
+}
+
 // C (m x nn) -= A (m x kk) B (kk x nn); all three are sub-blocks of one
 // column-major matrix with leading dimension lda.
 template <class T>
@@ -839,15 +940,26 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
     if (tc_gemm_sub_f32(c, (const float*)Am, (const float*)Bm, (float*)Cm, lda, m, nn, kk)) return FP_OK;
     return gemm_sub_simt_f32(c, (const float*)Am, (const float*)Bm, (float*)Cm, lda, m, nn, kk);
   } else {
-    constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
-    constexpr size_t sm = gemm_smem<T, BM, BN, BK, TM, TN>();
-    static SmemAttr attr;
-    FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub<T, BM, BN, BK, TM, TN>, (int)sm));
-    dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
-    const bool pre = ((reinterpret_cast<uintptr_t>(Cm) | (uintptr_t)(lda * sizeof(T))) & 15) == 0;
+    // cp.async moves 16-byte pieces: the blocks' row offsets and lda must keep them aligned
+    const uintptr_t mis = (reinterpret_cast<uintptr_t>(Am) | reinterpret_cast<uintptr_t>(Bm) |
+                           (uintptr_t)(lda * sizeof(T))) & 15;
     const int slot = kt_begin(c);
     TraceScope tr(c, TR_GEMM_SIMT);
-    k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk, pre);
+    if (mis == 0) {
+      static SmemAttr attr;
+      FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub_f64, (int)d64::smem()));
+      dim3 g((unsigned)((m + d64::BM - 1) / d64::BM), (unsigned)((nn + d64::BN - 1) / d64::BN));
+      k_gemm_sub_f64<<<g, d64::NT, d64::smem(), c->stream>>>((const double*)Am, (const double*)Bm, (double*)Cm, lda, m,
+                                                             nn, kk);
+    } else {
+      constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
+      constexpr size_t sm = gemm_smem<T, BM, BN, BK, TM, TN>();
+      static SmemAttr attr;
+      FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub<T, BM, BN, BK, TM, TN>, (int)sm));
+      dim3 g((unsigned)((m + BM - 1) / BM), (unsigned)((nn + BN - 1) / BN));
+      const bool pre = ((reinterpret_cast<uintptr_t>(Cm) | (uintptr_t)(lda * sizeof(T))) & 15) == 0;
+      k_gemm_sub<T, BM, BN, BK, TM, TN><<<g, (BM / TM) * (BN / TN), sm, c->stream>>>(Am, Bm, Cm, lda, m, nn, kk, pre);
+    }
     kt_end(c, slot, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
     ++c->nlaunch;
   }
@@ -1821,6 +1933,20 @@ int convert_f64_f32(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, 
                     int64_t ldb) {
   const int64_t t = n * k;
   k_f64_to_f32<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(a, b, n, k, lda, ldb);
+  ++c->nlaunch;
+  FP_CUDA_TRY(c->err, cudaGetLastError());
+  return FP_OK;
+}
+__global__ void k_f64_to_bf16f32(const double* __restrict__ a, float* __restrict__ b, int64_t n, int64_t k,
+                                 int64_t lda, int64_t ldb) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * k) return;
+  const int64_t i = t % n, q = t / n;
+  b[q * ldb + i] = __bfloat162float(__float2bfloat16_rn((float)a[q * lda + i]));
+}
+int convert_f64_bf16(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda, int64_t ldb) {
+  const int64_t t = n * k;
+  k_f64_to_bf16f32<<<(unsigned)((t + 255) / 256), 256, 0, c->stream>>>(a, b, n, k, lda, ldb);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;

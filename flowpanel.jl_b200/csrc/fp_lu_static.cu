@@ -29,6 +29,8 @@
 // then (after the previous panel's trailing update) K2 and K3 on the next
 // panel's columns; the second stream runs K2 and K5 on the columns beyond.
 // The panel width equals the triangular solves' 128-row blocks.
+#include <cuda_bf16.h>
+
 #include <cfloat>
 
 #include "fp_internal.cuh"
@@ -40,8 +42,7 @@ constexpr int PW = kStaticPanel;   // panel width (128)
 constexpr int IB = 32;             // inner block of the diagonal factor
 constexpr int NIB = PW / IB;       // inner blocks per panel
 constexpr int SP = PW + 4;         // shared row pitch (floats) of 128-wide rows: 16-byte rows, not 32 banks
-constexpr int DP = IB + 4;         // pitch of the 32 x 32 inverses (16-byte rows for float4 reads)
-constexpr int kDiagThreads = 512;
+constexpr int kDiagThreads = 256;
 constexpr unsigned FULL = 0xffffffffu;
 
 // dinv layout per panel: [t][0] = inv(L_tt) (unit lower), [t][1] = inv(U_tt),
@@ -55,18 +56,294 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(h);
 }
 
+// 1/x from the special-function unit (relative error ~1e-7): the FP32
+// factors only precondition FP64 refinement, so correct rounding buys nothing
+__device__ __forceinline__ float rcp_fast(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 __device__ __forceinline__ void atomic_max_pos(float* addr, float v) {
   if (v > 0.f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
+}
+
+// Staging helpers: global <-> shared copies of column-major blocks with
+// 16-byte loads, all of a thread's loads issued before its shared stores.
+// Column c of the block starts at g + c * ld (rows contiguous); element
+// (r, c) goes to or comes from s(r, c). Rows past `rows` / columns past
+// `cols` read as zero (or `pad(r, c)`) and are not written.
+// Piece q covers rows r..r+3 of column c. With 16 or more columns, a warp's
+// 32 pieces are two row quads x 16 columns, so that the transposing shared
+// accesses of a row-major copy (pitch = 4 mod 32 floats) hit 32 distinct
+// banks and each 32-byte sector of global memory is read by one pair of lanes.
+template <int ROWS, int COLS>
+__device__ __forceinline__ void piece(int q, int& r, int& c) {
+  constexpr int R4 = ROWS / 4;
+  if constexpr (COLS % 16 == 0 && R4 % 2 == 0) {
+    const int h = q & 1, cl = (q >> 1) & 15, rest = q >> 5;
+    const int g = rest % (R4 / 2), cb = rest / (R4 / 2);
+    r = (2 * g + h) * 4;
+    c = cb * 16 + cl;
+  } else {
+    c = q / R4;
+    r = (q % R4) * 4;
+  }
+}
+template <int NT, int ROWS, int COLS, class S, class Pad>
+__device__ __forceinline__ void load_block(const float* __restrict__ g, int64_t ld, int rows, int cols, S s, Pad pad,
+                                           int tid) {
+  constexpr int R4 = ROWS / 4, NV = R4 * COLS, PER = (NV + NT - 1) / NT;
+  float4 v[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int q = tid + u * NT;
+    int r, c;
+    piece<ROWS, COLS>(q, r, c);
+    if (q < NV && c < cols && r + 4 <= rows) {
+      v[u] = __ldcg(reinterpret_cast<const float4*>(g + (int64_t)c * ld + r));
+    } else if (q < NV) {
+      float t[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) t[i] = (c < cols && r + i < rows) ? __ldcg(g + (int64_t)c * ld + r + i) : pad(r + i, c);
+      v[u] = make_float4(t[0], t[1], t[2], t[3]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int q = tid + u * NT;
+    if (q < NV) {
+      int r, c;
+      piece<ROWS, COLS>(q, r, c);
+      s(r, c, v[u].x); s(r + 1, c, v[u].y); s(r + 2, c, v[u].z); s(r + 3, c, v[u].w);
+    }
+  }
+}
+template <int NT, int ROWS, int COLS, class S>
+__device__ __forceinline__ void store_block(float* __restrict__ g, int64_t ld, int rows, int cols, S s, int tid) {
+  constexpr int R4 = ROWS / 4, NV = R4 * COLS, PER = (NV + NT - 1) / NT;
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int q = tid + u * NT;
+    int r, c;
+    piece<ROWS, COLS>(q, r, c);
+    if (q >= NV || c >= cols) continue;
+    if (r + 4 <= rows) {
+      *reinterpret_cast<float4*>(g + (int64_t)c * ld + r) = make_float4(s(r, c), s(r + 1, c), s(r + 2, c), s(r + 3, c));
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (r + i < rows) g[(int64_t)c * ld + r + i] = s(r + i, c);
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
 // K1: the PW x PW diagonal block at (k, k), factored in place (unit L below,
 // U on and above the diagonal); the inverses of its IB x IB diagonal blocks
 // of L and U go to dinv. Rows and columns past n are padded with the identity.
+// 256 threads and 85 KB of shared memory, so that the CTA fits on an SM
+// beside two CTAs of the tensor-core update of the second stream.
+//
+// Per inner block kb (columns k0 .. k0 + 31):
+//   (a) warp 0 eliminates the IB x IB diagonal block (eliminate);
+//   (b) warps 2..7 form the block's L rows below (one thread per row,
+//       substitution with U_kk) and U columns right (one thread per column,
+//       substitution with L_kk) while warps 0 and 1 invert L_kk and U_kk for
+//       the other panel kernels (invert);
+//   (c) all warps update the rest of the block; the next diagonal block's
+//       tiles come first, so that warp 0 eliminates it while warps 1..7
+//       update the rest.
 constexpr size_t pdiag_smem() {
   return (size_t)PW * SP * sizeof(float)        // As
          + (size_t)IB * SP * sizeof(float)      // LT: the inner block's L columns, transposed
-         + (size_t)2 * IB * DP * sizeof(float); // inverses of the current inner block
+         + (size_t)2 * IB * sizeof(float);      // pivot row, two buffers
+}
+
+// Warp 0: the IB x IB block at (k0, k0) of As factored in place. Lane i
+// holds row i shifted so that R[0] is the current column (static register
+// indices, rolled step loop); the pivot row goes to the other lanes through
+// a shared buffer (two, alternating, one __syncwarp a step); a row stops
+// shifting once it is the pivot row, so at the end lane i holds U(i, i..)
+// and writes it.
+__device__ __forceinline__ void eliminate(float (*As)[SP], float* pbuf, int k0, int lane, float& lmax, int* status) {
+  float Rw[IB];
+  const float4* rp = reinterpret_cast<const float4*>(&As[k0 + lane][k0]);
+#pragma unroll
+  for (int q = 0; q < IB / 4; ++q) {
+    const float4 v = rp[q];
+    Rw[4 * q] = v.x; Rw[4 * q + 1] = v.y; Rw[4 * q + 2] = v.z; Rw[4 * q + 3] = v.w;
+  }
+  bool bad = false;
+#pragma unroll 1
+  for (int j = 0; j < IB; ++j) {
+    float4* pb = reinterpret_cast<float4*>(pbuf + (j & 1) * IB);
+    if (lane == j)
+#pragma unroll
+      for (int q = 0; q < IB / 4; ++q) pb[q] = make_float4(Rw[4 * q], Rw[4 * q + 1], Rw[4 * q + 2], Rw[4 * q + 3]);
+    __syncwarp();
+    float pv[IB];
+#pragma unroll
+    for (int q = 0; q < IB / 4; ++q) {
+      const float4 v = pb[q];
+      pv[4 * q] = v.x; pv[4 * q + 1] = v.y; pv[4 * q + 2] = v.z; pv[4 * q + 3] = v.w;
+    }
+    bad |= !(fabsf(pv[0]) > 0.f && fabsf(pv[0]) <= FLT_MAX);
+    const float rpiv = rcp_fast(pv[0]);
+    if (lane > j) {
+      const float l = Rw[0] * rpiv;
+      As[k0 + lane][k0 + j] = l;
+      lmax = fmaxf(lmax, fabsf(l));
+#pragma unroll
+      for (int c = 0; c < IB - 1; ++c) Rw[c] = fmaf(-l, pv[c + 1], Rw[c + 1]);
+      Rw[IB - 1] = 0.f;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < IB; ++c)
+    if (c < IB - lane) As[k0 + lane][k0 + lane + c] = Rw[c];
+  if (bad && lane == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
+}
+
+// Warp 0: inv(U_kk) -> dinv[.., 1]; warp 1: inv(L_kk) -> dinv[.., 0]; lane c
+// forms column c by substitution in registers (constant loop bounds, so the
+// loops unroll and the column stays in registers), four partial sums.
+__device__ __forceinline__ void invert(const float (*As)[SP], float* __restrict__ dinv, int kb, int warp, int lane) {
+  const int k0 = kb * IB;
+  if (warp == 0) {
+    float x[IB];
+#pragma unroll
+    for (int i = IB - 1; i >= 0; --i) {
+      float s[4] = {(lane == i) ? 1.f : 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int g = 0; g < IB / 4; ++g) {
+        if (4 * g + 3 <= i) continue;
+        const float4 a = *reinterpret_cast<const float4*>(&As[k0 + i][k0 + 4 * g]);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4 * g + e > i) s[e] = fmaf(-av[e], x[4 * g + e], s[e]);
+      }
+      x[i] = ((s[0] + s[1]) + (s[2] + s[3])) * rcp_fast(As[k0 + i][k0 + i]);
+    }
+#pragma unroll
+    for (int i = 0; i < IB; ++i) dinv[dinv_off(kb, 1) + i * IB + lane] = x[i];
+  } else if (warp == 1) {
+    float y[IB];
+#pragma unroll
+    for (int i = 0; i < IB; ++i) {
+      float s[4] = {(lane == i) ? 1.f : 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int g = 0; g < IB / 4; ++g) {
+        if (4 * g >= i) continue;
+        const float4 a = *reinterpret_cast<const float4*>(&As[k0 + i][k0 + 4 * g]);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4 * g + e < i) s[e] = fmaf(-av[e], y[4 * g + e], s[e]);
+      }
+      y[i] = (s[0] + s[1]) + (s[2] + s[3]);
+    }
+#pragma unroll
+    for (int i = 0; i < IB; ++i) dinv[dinv_off(kb, 0) + i * IB + lane] = y[i];
+  }
+}
+
+// (b) task `task` of 2R: task < R is row i = k1 + task of L(., kb) =
+// A(i, kb) inv(U_kk), by right-looking substitution (row s of U_kk is
+// contiguous); else column j = k1 + task - R of U(kb, .) = inv(L_kk) A(kb, j),
+// by left-looking substitution (row t of L_kk is contiguous). Each thread
+// owns its row or column, so results go straight back to As (and L's
+// transpose to LT).
+__device__ __forceinline__ void substitute(float (*As)[SP], float (*LT)[SP], int k0, int R, int task, float& lmax) {
+  const int k1 = k0 + IB;
+  float x[IB];
+  if (task < R) {
+    const int i = k1 + task;
+#pragma unroll
+    for (int q = 0; q < IB / 4; ++q) {
+      const float4 v = *reinterpret_cast<const float4*>(&As[i][k0 + 4 * q]);
+      x[4 * q] = v.x; x[4 * q + 1] = v.y; x[4 * q + 2] = v.z; x[4 * q + 3] = v.w;
+    }
+#pragma unroll
+    for (int s = 0; s < IB; ++s) {
+      x[s] *= rcp_fast(As[k0 + s][k0 + s]);
+#pragma unroll
+      for (int g = 0; g < IB / 4; ++g) {
+        if (4 * g + 3 <= s) continue;
+        const float4 u = *reinterpret_cast<const float4*>(&As[k0 + s][k0 + 4 * g]);
+        const float uv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4 * g + e > s) x[4 * g + e] = fmaf(-x[s], uv[e], x[4 * g + e]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < IB / 4; ++q)
+      *reinterpret_cast<float4*>(&As[i][k0 + 4 * q]) = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+#pragma unroll
+    for (int t = 0; t < IB; ++t) {
+      LT[t][i] = x[t];
+      lmax = fmaxf(lmax, fabsf(x[t]));
+    }
+  } else {
+    const int j = k1 + task - R;
+#pragma unroll
+    for (int t = 0; t < IB; ++t) {
+      float s[4] = {As[k0 + t][j], 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int g = 0; g < IB / 4; ++g) {
+        if (4 * g >= t) continue;
+        const float4 l = *reinterpret_cast<const float4*>(&As[k0 + t][k0 + 4 * g]);
+        const float lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4 * g + e < t) s[e] = fmaf(-lv[e], x[4 * g + e], s[e]);
+      }
+      x[t] = (s[0] + s[1]) + (s[2] + s[3]);
+    }
+#pragma unroll
+    for (int t = 0; t < IB; ++t) As[k0 + t][j] = x[t];
+  }
+}
+
+// (c) for the 4 x 4 tiles [first, last) of the update of the block after the
+// inner block k0 (R x R from row and column k1 = k0 + IB), in an order where
+// the next diagonal block's 64 tiles come first:
+// As(i, j) -= sum_t LT(t, i) As(k0 + t, j).
+__device__ __forceinline__ void update_tiles(float (*As)[SP], const float (*LT)[SP], int k0, int R, int first,
+                                             int last, int stride) {
+  const int k1 = k0 + IB, RQ = R / 4;
+  for (int tile = first; tile < last; tile += stride) {
+    int iq, jq;
+    if (tile < 64) {   // the next diagonal block
+      iq = tile >> 3; jq = tile & 7;
+    } else {           // the rest, row quad by row quad
+      const int t = tile - 64;
+      const int rest_cols = RQ - 8;
+      if (t < 8 * rest_cols) { iq = t / rest_cols; jq = 8 + t % rest_cols; }
+      else { const int u = t - 8 * rest_cols; iq = 8 + u / RQ; jq = u % RQ; }
+    }
+    const int i0 = k1 + 4 * iq, j0 = k1 + 4 * jq;
+    float acc[4][4] = {};
+#pragma unroll 8
+    for (int t = 0; t < IB; ++t) {
+      const float4 l = *reinterpret_cast<const float4*>(&LT[t][i0]);
+      const float4 u = *reinterpret_cast<const float4*>(&As[k0 + t][j0]);
+      const float lv[4] = {l.x, l.y, l.z, l.w}, uv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(lv[i], uv[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float4* p = reinterpret_cast<float4*>(&As[i0 + i][j0]);
+      float4 v = *p;
+      v.x -= acc[i][0]; v.y -= acc[i][1]; v.z -= acc[i][2]; v.w -= acc[i][3];
+      *p = v;
+    }
+  }
 }
 
 __global__ void __launch_bounds__(kDiagThreads, 1)
@@ -75,286 +352,139 @@ k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restr
   extern __shared__ __align__(16) unsigned char smem[];
   float (*As)[SP] = reinterpret_cast<float (*)[SP]>(smem);
   float (*LT)[SP] = reinterpret_cast<float (*)[SP]>(smem + (size_t)PW * SP * sizeof(float));
-  float (*Li)[DP] = reinterpret_cast<float (*)[DP]>(smem + (size_t)(PW + IB) * SP * sizeof(float));
-  float (*Ui)[DP] = Li + IB;
+  float* pbuf = reinterpret_cast<float*>(LT + IB);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nb = (int)imin64(PW, n - k);
-  for (int e = tid; e < PW * PW; e += kDiagThreads) {
-    const int r = e % PW, c = e / PW;   // rows fastest: coalesced column reads
-    As[r][c] = (r < nb && c < nb) ? __ldcg(&A[(k + c) * lda + k + r]) : (r == c ? 1.f : 0.f);
-  }
+  load_block<kDiagThreads, PW, PW>(
+      A + k * lda + k, lda, nb, nb, [&](int r, int c, float v) { As[r][c] = v; },
+      [](int r, int c) { return r == c ? 1.f : 0.f; }, tid);
   __syncthreads();
   float lmax = 0.f;
+  if (warp == 0) eliminate(As, pbuf, 0, lane, lmax, status);
+  __syncthreads();
 #pragma unroll 1
   for (int kb = 0; kb < NIB; ++kb) {
-    const int k0 = kb * IB, k1 = k0 + IB, R = PW - k1;   // R rows (and columns) after the inner block
-    // (a) warp 0 eliminates the IB x IB block. Lane i holds row i shifted so
-    // that R[0] is the current column (static register indices, rolled step
-    // loop); a row stops shifting once it is the pivot row, so at the end lane
-    // i holds U(i, i..) and writes it; each step's multipliers go to As.
-    if (warp == 0) {
-      float Rw[IB];
-      const float4* rp = reinterpret_cast<const float4*>(&As[k0 + lane][k0]);
-#pragma unroll
-      for (int q = 0; q < IB / 4; ++q) {
-        const float4 v = rp[q];
-        Rw[4 * q] = v.x; Rw[4 * q + 1] = v.y; Rw[4 * q + 2] = v.z; Rw[4 * q + 3] = v.w;
-      }
-      bool bad = false;
-#pragma unroll 1
-      for (int j = 0; j < IB; ++j) {
-        float pv[IB];
-#pragma unroll
-        for (int c = 0; c < IB; ++c) pv[c] = __shfl_sync(FULL, Rw[c], j);
-        bad |= !(fabsf(pv[0]) > 0.f && fabsf(pv[0]) <= FLT_MAX);
-        if (lane > j) {
-          const float l = Rw[0] / pv[0];
-          As[k0 + lane][k0 + j] = l;
-          lmax = fmaxf(lmax, fabsf(l));
-#pragma unroll
-          for (int c = 0; c < IB - 1; ++c) Rw[c] = fmaf(-l, pv[c + 1], Rw[c + 1]);
-          Rw[IB - 1] = 0.f;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < IB; ++c)
-        if (c < IB - lane) As[k0 + lane][k0 + lane + c] = Rw[c];
-      if (bad && lane == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
-    }
-    __syncthreads();
-    // (a2) warp 0: inv(U_kk), warp 1: inv(L_kk); lane c forms column c by
-    // substitution, its entries kept in the inverse's own column
-    if (warp == 0) {
-#pragma unroll 1
-      for (int i = IB - 1; i >= 0; --i) {
-        float s0 = (lane == i) ? 1.f : 0.f, s1 = 0.f;
-        int t = i + 1;
-#pragma unroll 1
-        for (; t + 1 < IB; t += 2) {
-          s0 = fmaf(-As[k0 + i][k0 + t], Ui[t][lane], s0);
-          s1 = fmaf(-As[k0 + i][k0 + t + 1], Ui[t + 1][lane], s1);
-        }
-        if (t < IB) s0 = fmaf(-As[k0 + i][k0 + t], Ui[t][lane], s0);
-        Ui[i][lane] = (s0 + s1) / As[k0 + i][k0 + i];
-      }
-    } else if (warp == 1) {
-#pragma unroll 1
-      for (int i = 0; i < IB; ++i) {
-        float s0 = (lane == i) ? 1.f : 0.f, s1 = 0.f;
-        int t = 0;
-#pragma unroll 1
-        for (; t + 1 < i; t += 2) {
-          s0 = fmaf(-As[k0 + i][k0 + t], Li[t][lane], s0);
-          s1 = fmaf(-As[k0 + i][k0 + t + 1], Li[t + 1][lane], s1);
-        }
-        if (t < i) s0 = fmaf(-As[k0 + i][k0 + t], Li[t][lane], s0);
-        Li[i][lane] = s0 + s1;
-      }
-    }
-    __syncthreads();
-    for (int e = tid; e < 2 * IB * IB; e += kDiagThreads) {   // keep both inverses for the panel's products
-      const int which = e / (IB * IB), r = (e / IB) % IB, c = e % IB;
-      dinv[dinv_off(kb, which) + r * IB + c] = which ? Ui[r][c] : Li[r][c];
-    }
+    const int k0 = kb * IB, R = PW - k0 - IB;   // R rows (and columns) after the inner block
+    if (warp < 2) invert(As, dinv, kb, warp, lane);
+    else if (tid - 64 < 2 * R) substitute(As, LT, k0, R, tid - 64, lmax);
     if (R == 0) break;
-    // (b) rows below: L(i, kb) = A(i, kb) inv(U_kk) into LT (transposed);
-    // columns right: U(kb, j) = inv(L_kk) A(kb, j) into registers. Both read
-    // parts of As that the other part's results replace, so As is written
-    // after the barrier.
-    {
-      if (tid < (R / 4) * 8) {   // (row quad, 4-column group)
-        const int tg = tid & 7, iq = tid >> 3;
-        const int t0 = 4 * tg, i0 = k1 + 4 * iq;
-        float acc[4][4] = {};
-        for (int s = 0; s <= t0 + 3; ++s) {
-          const float4 u = *reinterpret_cast<const float4*>(&Ui[s][t0]);   // inv(U)[s][t] = 0 for s > t
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float a = As[i0 + i][k0 + s];
-            acc[i][0] = fmaf(a, u.x, acc[i][0]);
-            acc[i][1] = fmaf(a, u.y, acc[i][1]);
-            acc[i][2] = fmaf(a, u.z, acc[i][2]);
-            acc[i][3] = fmaf(a, u.w, acc[i][3]);
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int c = 0; c < 4; ++c) LT[t0 + c][i0 + i] = acc[i][c];
-      }
-      // (32-column group, inner row quad): at most 24 tasks, so two per warp
-      constexpr int NW = kDiagThreads / 32;
-      const int ntask_c = (R / 32) * 8;
-      float uc[2][4] = {};
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int task = warp + q * NW;
-        if (task < ntask_c) {
-          const int tq = task & 7, jg = task >> 3;
-          const int j = k1 + 32 * jg + lane, t0 = 4 * tq;
-          for (int s = 0; s <= t0 + 3; ++s) {
-            const float a = As[k0 + s][j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) uc[q][i] = fmaf(Li[t0 + i][s], a, uc[q][i]);   // inv(L)[t][s] = 0 for s > t
-          }
-        }
-      }
-      __syncthreads();
-      for (int e = tid; e < R * IB; e += kDiagThreads) {
-        const int i = e / IB, t = e % IB;
-        const float v = LT[t][k1 + i];
-        As[k1 + i][k0 + t] = v;
-        lmax = fmaxf(lmax, fabsf(v));
-      }
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int task = warp + q * NW;
-        if (task < ntask_c) {
-          const int tq = task & 7, jg = task >> 3;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) As[k0 + 4 * tq + i][k1 + 32 * jg + lane] = uc[q][i];
-        }
-      }
-    }
     __syncthreads();
-    // (c) trailing update of the block: As(i, j) -= sum_t LT(t, i) As(k0 + t, j), i, j >= k1;
-    // thread tile 4 x 4
-    {
-      const int tiles = (R / 4) * (R / 4);
-      for (int tile = tid; tile < tiles; tile += kDiagThreads) {
-        const int jq = tile % (R / 4), iq = tile / (R / 4);
-        const int i0 = k1 + 4 * iq, j0 = k1 + 4 * jq;
-        float acc[4][4] = {};
-#pragma unroll 8
-        for (int t = 0; t < IB; ++t) {
-          const float4 l = *reinterpret_cast<const float4*>(&LT[t][i0]);
-          const float4 u = *reinterpret_cast<const float4*>(&As[k0 + t][j0]);
-          const float lv[4] = {l.x, l.y, l.z, l.w}, uv[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(lv[i], uv[j], acc[i][j]);
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          float4* p = reinterpret_cast<float4*>(&As[i0 + i][j0]);
-          float4 v = *p;
-          v.x -= acc[i][0]; v.y -= acc[i][1]; v.z -= acc[i][2]; v.w -= acc[i][3];
-          *p = v;
-        }
-      }
-    }
+    const int tiles = (R / 4) * (R / 4);
+    update_tiles(As, LT, k0, R, tid, 64, kDiagThreads);
+    __syncthreads();
+    if (warp == 0) eliminate(As, pbuf, k0 + IB, lane, lmax, status);
+    else update_tiles(As, LT, k0, R, 64 + (tid - 32), tiles, kDiagThreads - 32);
     __syncthreads();
   }
-  // write the factors back (rows fastest: coalesced)
-  for (int e = tid; e < nb * nb; e += kDiagThreads) {
-    const int r = e % nb, c = e / nb;
-    A[(k + c) * lda + k + r] = As[r][c];
-  }
+  __syncthreads();
+  // write the factors back (16-byte stores down the columns)
+  store_block<kDiagThreads, PW, PW>(A + k * lda + k, lda, nb, nb, [&](int r, int c) { return As[r][c]; }, tid);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
   if (lane == 0) atomic_max_pos(cert, lmax);
 }
 
 // ---------------------------------------------------------------------------
-// Register-tiled product over shared memory: acc[i][j] += sum_{s < K}
-// P[r0 + i][s] Q[s][c0 + j] (P row pitch PP, Q row pitch QP; 4 x 4 tile).
-template <int PP, int QP>
-__device__ __forceinline__ void tile4x4(const float (*P)[PP], const float (*Q)[QP], int r0, int c0, int K,
-                                        float (&acc)[4][4]) {
-#pragma unroll 4
-  for (int s = 0; s < K; ++s) {
-    const float4 q = *reinterpret_cast<const float4*>(&Q[s][c0]);
-    const float qv[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const float p = P[r0 + i][s];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(p, qv[j], acc[i][j]);
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// K6: L21 = A21 U^-1 for the rows [r0 + 64 b, +64) below the panel at k, by
+// K6: L21 = A21 U^-1 for the rows [r0 + 32 b, +32) below the panel at k, by
 // block substitution over the four inner column blocks t:
 //   Y_t = A21_t - sum_{s < t} L_s U(s, t),   L_t = Y_t inv(U_tt).
-// Writes L21 in place and its split Ah = rna_tf32(L21), Al = L21 - Ah
-// (K-major: row (r - r0) of ldk = PW floats); max|L21| into cert.
-constexpr int L21_ROWS = 64, L21_THREADS = 128;   // 16 x 8 thread tiles of 4 x 4 over 64 x 32
+// The row block, the panel's U above the diagonal blocks and the four
+// inverses are staged once (one round of loads), then the four steps run from
+// shared memory. Writes L21 in place and its split Ah = rna_tf32(L21),
+// Al = L21 - Ah (K-major: row (r - r0) of ldk = PW floats); max|L21| into
+// cert. Thread tile: 2 rows x 4 columns of the 32 x 32 block.
+constexpr int L21_ROWS = 32, L21_THREADS = 128;
 constexpr int XP = PW + 4;   // row pitch of the row block
+constexpr int UP = IB + 4;   // row pitch of the 32-wide blocks
+constexpr int UBP = PW - IB + 4;   // row pitch of U(0..95, 32..127)
 constexpr size_t l21_smem() {
-  return (size_t)L21_ROWS * XP * sizeof(float) + (size_t)(PW - IB) * (IB + 4) * sizeof(float) +
-         (size_t)IB * (IB + 4) * sizeof(float);
+  return (size_t)L21_ROWS * XP * sizeof(float) + (size_t)(PW - IB) * UBP * sizeof(float) +
+         (size_t)NIB * IB * UP * sizeof(float);
 }
 
+template <bool BF16>
 __global__ void __launch_bounds__(L21_THREADS)
 k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, const float* __restrict__ dinv,
       float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
   extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int UP = IB + 4;
   float (*X)[XP] = reinterpret_cast<float (*)[XP]>(smem);
-  float (*Ub)[UP] = reinterpret_cast<float (*)[UP]>(smem + (size_t)L21_ROWS * XP * sizeof(float));   // U(s-blocks, t)
-  float (*Ut)[UP] = Ub + (PW - IB);                                                                     // inv(U_tt)
+  // Ub[s][c - IB] = U(s, c) for s < 96, c >= 32 (entries below the diagonal blocks are not read)
+  float (*Ub)[UBP] = reinterpret_cast<float (*)[UBP]>(smem + (size_t)L21_ROWS * XP * sizeof(float));
+  float (*Ut)[UP] = reinterpret_cast<float (*)[UP]>(reinterpret_cast<unsigned char*>(Ub) +
+                                                     (size_t)(PW - IB) * UBP * sizeof(float));   // inv(U_tt), 4 x 32 rows
   const int tid = threadIdx.x;
   const int64_t row0 = r0 + (int64_t)blockIdx.x * L21_ROWS;
   const int rows = (int)imin64(L21_ROWS, n - row0);
-  for (int e = tid; e < L21_ROWS * PW; e += L21_THREADS) {
-    const int r = e % L21_ROWS, c = e / L21_ROWS;
-    X[r][c] = (r < rows) ? __ldcg(&A[(k + c) * lda + row0 + r]) : 0.f;
+  load_block<L21_THREADS, L21_ROWS, PW>(
+      A + k * lda + row0, lda, rows, PW, [&](int r, int c, float v) { X[r][c] = v; }, [](int, int) { return 0.f; },
+      tid);
+  load_block<L21_THREADS, PW - IB, PW - IB>(
+      A + (k + IB) * lda + k, lda, PW - IB, PW - IB, [&](int r, int c, float v) { Ub[r][c] = v; },
+      [](int, int) { return 0.f; }, tid);
+  for (int e = tid; e < NIB * IB * IB / 4; e += L21_THREADS) {
+    const int t = e / (IB * IB / 4), r = (e / (IB / 4)) % IB, c = (e % (IB / 4)) * 4;
+    *reinterpret_cast<float4*>(&Ut[t * IB + r][c]) =
+        __ldcg(reinterpret_cast<const float4*>(&dinv[dinv_off(t, 1) + r * IB + c]));
   }
-  const int rg = tid & 15, cg = tid >> 4;   // 16 row quads x 8 column quads = 64 x 32
+  __syncthreads();
+  const int rg = tid & 15, cg = tid >> 4;   // 16 row pairs x 8 column quads = 32 x 32
 #pragma unroll 1
   for (int t = 0; t < NIB; ++t) {
     const int c0 = t * IB;
-    // U(0..c0-1, c0..c0+31) and inv(U_tt)
-    for (int e = tid; e < c0 * IB; e += L21_THREADS) {
-      const int s = e % c0, c = e / c0;
-      Ub[s][c] = __ldcg(&A[(k + c0 + c) * lda + k + s]);
-    }
-    for (int e = tid; e < IB * IB; e += L21_THREADS) Ut[e / IB][e % IB] = dinv[dinv_off(t, 1) + e];
-    __syncthreads();
-    float y[4][4] = {};
-    if (c0 > 0) tile4x4<XP, UP>(X, Ub, 4 * rg, 4 * cg, c0, y);   // sum_s L_s U(s, t) (X's columns < c0 hold L)
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) X[4 * rg + i][c0 + 4 * cg + j] -= y[i][j];
-    __syncthreads();
-    float l[4][4] = {};
-    // L_t = Y_t inv(U_tt): P = X's column block t (pitch XP, offset c0)
+    float y[2][4] = {};
 #pragma unroll 4
-    for (int s = 0; s < IB; ++s) {
-      const float4 q = *reinterpret_cast<const float4*>(&Ut[s][4 * cg]);
+    for (int s = 0; s < c0; ++s) {   // sum_s L_s U(s, t): X's columns < c0 hold L
+      const float4 q = *reinterpret_cast<const float4*>(&Ub[s][c0 - IB + 4 * cg]);
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float p = X[4 * rg + i][c0 + s];
+      for (int i = 0; i < 2; ++i) {
+        const float p = X[2 * rg + i][s];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) y[i][j] = fmaf(p, qv[j], y[i][j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)   // each thread owns its 2 x 4 entries of block t: no other thread reads them yet
+#pragma unroll
+      for (int j = 0; j < 4; ++j) X[2 * rg + i][c0 + 4 * cg + j] -= y[i][j];
+    __syncthreads();
+    float l[2][4] = {};
+#pragma unroll 4
+    for (int s = 0; s < IB; ++s) {   // L_t = Y_t inv(U_tt)
+      const float4 q = *reinterpret_cast<const float4*>(&Ut[t * IB + s][4 * cg]);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const float p = X[2 * rg + i][c0 + s];
 #pragma unroll
         for (int j = 0; j < 4; ++j) l[i][j] = fmaf(p, qv[j], l[i][j]);
       }
     }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) X[4 * rg + i][c0 + 4 * cg + j] = l[i][j];
+      for (int j = 0; j < 4; ++j) X[2 * rg + i][c0 + 4 * cg + j] = l[i][j];
     __syncthreads();
   }
+  store_block<L21_THREADS, L21_ROWS, PW>(A + k * lda + row0, lda, rows, PW, [&](int r, int c) { return X[r][c]; },
+                                        tid);
   float lmax = 0.f;
-  for (int e = tid; e < rows * PW; e += L21_THREADS) {
-    const int r = e % rows, c = e / rows;   // rows fastest: coalesced column stores
-    A[(k + c) * lda + row0 + r] = X[r][c];
-  }
-  for (int e = tid; e < rows * PW; e += L21_THREADS) {
-    const int r = e / PW, c = e % PW;       // columns fastest: K-major split
-    const float v = X[r][c];
-    const float h = tf32_rna(v);
+  constexpr int C4 = PW / 4;
+  for (int e = tid; e < rows * C4; e += L21_THREADS) {   // K-major split: 16-byte stores along each row
+    const int r = e / C4, c = (e % C4) * 4;
+    const float4 v = *reinterpret_cast<const float4*>(&X[r][c]);
     const int64_t o = (row0 - r0 + r) * (int64_t)PW + c;
-    Ah[o] = h;
-    Al[o] = v - h;
-    lmax = fmaxf(lmax, fabsf(v));
+    if (BF16) {   // the operand in BF16 (element offsets in a bf16 array)
+      __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(Ah) + o);
+      d[0] = __floats2bfloat162_rn(v.x, v.y);
+      d[1] = __floats2bfloat162_rn(v.z, v.w);
+    } else {
+      const float4 h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
+      *reinterpret_cast<float4*>(&Ah[o]) = h;
+      *reinterpret_cast<float4*>(&Al[o]) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+    }
+    lmax = fmaxf(lmax, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
@@ -365,46 +495,53 @@ k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, cons
 // K2: U12 = L^-1 A12 for the panel's rows [k, k + PW) and the columns
 // [c0 + CW b, +CW) of [c0, c1), by block substitution over the four inner row
 // blocks t:  Z_t = A12_t - sum_{s < t} L(t, s) U12_s,  U12_t = inv(L_tt) Z_t.
-// Writes U12 in place and its split Bh, Bl (column j - c0 holds its PW
-// values contiguously). Thread tile: RT rows of block t x 4 columns.
+// The column block, the panel's L below the diagonal blocks and the four
+// inverses are staged once. Writes U12 in place and its split Bh, Bl (column
+// j - c0 holds its PW values contiguously). Thread tile: RT rows of block t
+// x 4 columns.
 template <int CW, int RT>
 struct U12Cfg {
   static constexpr int THREADS = (IB / RT) * (CW / 4);
   static constexpr int ZP = CW + 4;   // row pitch of the column block
+  static constexpr int LP = PW - IB + 4;
   static constexpr size_t smem() {
-    return (size_t)PW * ZP * sizeof(float) + (size_t)IB * (PW - IB + 4) * sizeof(float) +
-           (size_t)IB * (IB + 4) * sizeof(float);
+    return (size_t)PW * ZP * sizeof(float) + (size_t)(PW - IB) * LP * sizeof(float) +
+           (size_t)NIB * IB * UP * sizeof(float);
   }
 };
 
-template <int CW, int RT>
+template <int CW, int RT, bool BF16>
 __global__ void __launch_bounds__(U12Cfg<CW, RT>::THREADS)
 k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, const float* __restrict__ dinv,
       float* __restrict__ Bh, float* __restrict__ Bl) {
-  constexpr int T = U12Cfg<CW, RT>::THREADS, ZP = U12Cfg<CW, RT>::ZP, LP = PW - IB + 4, IP = IB + 4;
+  typedef U12Cfg<CW, RT> Cfg;
+  constexpr int T = Cfg::THREADS, ZP = Cfg::ZP, LP = Cfg::LP;
   extern __shared__ __align__(16) unsigned char smem[];
   float (*Z)[ZP] = reinterpret_cast<float (*)[ZP]>(smem);                                    // PW x CW
-  float (*Lb)[LP] = reinterpret_cast<float (*)[LP]>(smem + (size_t)PW * ZP * sizeof(float));  // L(t, 0..t0-1)
-  float (*Lt)[IP] = reinterpret_cast<float (*)[IP]>(reinterpret_cast<unsigned char*>(Lb) +
-                                                     (size_t)IB * LP * sizeof(float));        // inv(L_tt)
+  // Lb[r - IB][s] = L(r, s) for r >= 32, s < 96 (entries right of the diagonal blocks are not read)
+  float (*Lb)[LP] = reinterpret_cast<float (*)[LP]>(smem + (size_t)PW * ZP * sizeof(float));
+  float (*Lt)[UP] = reinterpret_cast<float (*)[UP]>(reinterpret_cast<unsigned char*>(Lb) +
+                                                     (size_t)(PW - IB) * LP * sizeof(float));   // inv(L_tt), 4 x 32 rows
   const int tid = threadIdx.x;
   const int64_t col0 = c0 + (int64_t)blockIdx.x * CW;
   const int cols = (int)imin64(CW, c1 - col0);
-  for (int e = tid; e < PW * CW; e += T) {
-    const int r = e % PW, c = e / PW;
-    Z[r][c] = (c < cols) ? __ldcg(&A[(col0 + c) * lda + k + r]) : 0.f;
+  load_block<T, PW, CW>(
+      A + col0 * lda + k, lda, PW, cols, [&](int r, int c, float v) { Z[r][c] = v; }, [](int, int) { return 0.f; },
+      tid);
+  load_block<T, PW - IB, PW - IB>(
+      A + k * lda + k + IB, lda, PW - IB, PW - IB, [&](int r, int s, float v) { Lb[r][s] = v; },
+      [](int, int) { return 0.f; }, tid);
+  for (int e = tid; e < NIB * IB * IB / 4; e += T) {
+    const int t = e / (IB * IB / 4), r = (e / (IB / 4)) % IB, c = (e % (IB / 4)) * 4;
+    *reinterpret_cast<float4*>(&Lt[t * IB + r][c]) =
+        __ldcg(reinterpret_cast<const float4*>(&dinv[dinv_off(t, 0) + r * IB + c]));
   }
+  __syncthreads();
   constexpr int CQ = CW / 4;
   const int cq = tid % CQ, rq = tid / CQ;   // rq < IB / RT
 #pragma unroll 1
   for (int t = 0; t < NIB; ++t) {
     const int t0 = t * IB;
-    for (int e = tid; e < IB * t0; e += T) {
-      const int r = e % IB, s = e / IB;
-      Lb[r][s] = __ldcg(&A[(k + s) * lda + k + t0 + r]);
-    }
-    for (int e = tid; e < IB * IB; e += T) Lt[e / IB][e % IB] = dinv[dinv_off(t, 0) + e];
-    __syncthreads();
     float z[RT][4] = {};
 #pragma unroll 4
     for (int s = 0; s < t0; ++s) {
@@ -412,14 +549,13 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int i = 0; i < RT; ++i) {
-        const float p = Lb[RT * rq + i][s];
+        const float p = Lb[t0 - IB + RT * rq + i][s];
 #pragma unroll
         for (int j = 0; j < 4; ++j) z[i][j] = fmaf(p, qv[j], z[i][j]);
       }
     }
-    __syncthreads();
 #pragma unroll
-    for (int i = 0; i < RT; ++i)
+    for (int i = 0; i < RT; ++i)   // own entries of block t: nothing else reads them yet
 #pragma unroll
       for (int j = 0; j < 4; ++j) Z[t0 + RT * rq + i][4 * cq + j] -= z[i][j];
     __syncthreads();
@@ -430,7 +566,7 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int i = 0; i < RT; ++i) {
-        const float p = Lt[RT * rq + i][s];
+        const float p = Lt[t * IB + RT * rq + i][s];
 #pragma unroll
         for (int j = 0; j < 4; ++j) u[i][j] = fmaf(p, qv[j], u[i][j]);
       }
@@ -442,14 +578,23 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
       for (int j = 0; j < 4; ++j) Z[t0 + RT * rq + i][4 * cq + j] = u[i][j];
     __syncthreads();
   }
-  for (int e = tid; e < PW * cols; e += T) {
-    const int r = e % PW, c = e / PW;   // rows fastest: coalesced, and K-major for the split
-    const float v = Z[r][c];
-    A[(col0 + c) * lda + k + r] = v;
-    const float h = tf32_rna(v);
+  store_block<T, PW, CW>(A + col0 * lda + k, lda, PW, cols, [&](int r, int c) { return Z[r][c]; }, tid);
+  constexpr int R4 = PW / 4;
+  for (int e = tid; e < cols * R4; e += T) {   // the split, K-major: column j - c0 holds its PW values
+    const int c = e / R4, r = (e % R4) * 4;
+    const float v[4] = {Z[r][c], Z[r + 1][c], Z[r + 2][c], Z[r + 3][c]};
     const int64_t o = (col0 - c0 + c) * (int64_t)PW + r;
-    Bh[o] = h;
-    Bl[o] = v - h;
+    if (BF16) {
+      __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(Bh) + o);
+      d[0] = __floats2bfloat162_rn(v[0], v[1]);
+      d[1] = __floats2bfloat162_rn(v[2], v[3]);
+    } else {
+      float h[4], lo[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) { h[i] = tf32_rna(v[i]); lo[i] = v[i] - h[i]; }
+      *reinterpret_cast<float4*>(&Bh[o]) = make_float4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<float4*>(&Bl[o]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    }
   }
 }
 
@@ -464,17 +609,20 @@ __global__ void k_iota(int32_t* __restrict__ ipiv, int64_t n) {
 // scratch: per panel parity, the 32 x 32 inverses (in c->d_minv) and the
 // split operands Ah, Al (rows below the panel) and Bh, Bl (columns right of
 // it) in the tensor-core scratch set of that parity.
-int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert) {
+int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert, bool bf16) {
   using namespace st;
   static_assert((size_t)2 * kDinvFloats * sizeof(float) <= kMinvBytes, "inverse slots fit the panel scratch");
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
   typedef U12Cfg<8, 1> CfgN;    // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
-  static SmemAttr attr_d, attr_l, attr_un, attr_ur;
+  static SmemAttr attr_d, attr_l, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
   FP_CUDA_TRY(c->err, attr_d.ensure(k_pdiag, (int)pdiag_smem()));
-  FP_CUDA_TRY(c->err, attr_l.ensure(k_l21, (int)l21_smem()));
-  FP_CUDA_TRY(c->err, attr_un.ensure(k_u12<8, 1>, (int)CfgN::smem()));
-  FP_CUDA_TRY(c->err, attr_ur.ensure(k_u12<32, 2>, (int)CfgR::smem()));
+  FP_CUDA_TRY(c->err, attr_l.ensure(k_l21<false>, (int)l21_smem()));
+  FP_CUDA_TRY(c->err, attr_un.ensure(k_u12<8, 1, false>, (int)CfgN::smem()));
+  FP_CUDA_TRY(c->err, attr_ur.ensure(k_u12<32, 2, false>, (int)CfgR::smem()));
+  FP_CUDA_TRY(c->err, attr_lb.ensure(k_l21<true>, (int)l21_smem()));
+  FP_CUDA_TRY(c->err, attr_unb.ensure(k_u12<8, 1, true>, (int)CfgN::smem()));
+  FP_CUDA_TRY(c->err, attr_urb.ensure(k_u12<32, 2, true>, (int)CfgR::smem()));
   if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
   if (int rc = ensure_tc_scratch(c, 1, n)) return rc;
   st::k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(ipiv, n);
@@ -490,9 +638,14 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     const int64_t m = n - kend, nn = ce - cb;
     if (m <= 0 || nn <= 0) return FP_OK;
     float* const* s = c->d_tc[slot];
-    if (c->use_tc && tc_gemm_sub_presplit(c, s[0], s[1], s[2] + boff * PW, s[3] + boff * PW, PW, at(kend, cb), lda, m,
-                                          nn, (int)(std::min<int64_t>(PW, n - K0))))
+    const int kk = (int)std::min<int64_t>(PW, n - K0);
+    if (bf16) {
+      const __nv_bfloat16* bh = reinterpret_cast<const __nv_bfloat16*>(s[2]) + boff * PW;
+      if (c->use_tc && tc_gemm_sub_bf16(c, s[0], bh, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
+    } else if (c->use_tc && tc_gemm_sub_presplit(c, s[0], s[1], s[2] + boff * PW, s[3] + boff * PW, PW, at(kend, cb),
+                                                 lda, m, nn, kk)) {
       return FP_OK;
+    }
     FP_CUDA_TRY(c->err, cudaGetLastError());
     return gemm_sub_simt_f32(c, at(kend, K0), at(K0, cb), at(kend, cb), lda, m, nn, (int)std::min<int64_t>(PW, n - K0));
   };
@@ -510,8 +663,9 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     }
     if (kend < n) {
       TraceScope tr(c, TR_L21);
-      k_l21<<<(unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS), L21_THREADS, l21_smem(), c->stream>>>(
-          A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+      const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
+      if (bf16) k_l21<true><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+      else k_l21<false><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
@@ -521,26 +675,45 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
       {
         TraceScope tr(c, TR_U12);
-        k_u12<8, 1><<<(unsigned)((knext - kend + 7) / 8), CfgN::THREADS, CfgN::smem(), c->stream>>>(
-            A, lda, K0, kend, knext, dinv, s[2], s[3]);
+        const unsigned g = (unsigned)((knext - kend + 7) / 8);
+        if (bf16)
+          k_u12<8, 1, true><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+        else
+          k_u12<8, 1, false><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
       if (int rc = update(slot, kend, K0, kend, knext, 0)) return rc;
     }
-    {
-      OnStream2 on2(c);
-      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
+    // the columns beyond the next panel: on the second stream (look-ahead), or
+    // after the panel's own work on the same stream
+    auto rest = [&]() -> int {
       if (n > knext) {
         {
           TraceScope tr(c, TR_STRIP);
-          k_u12<32, 2><<<(unsigned)((n - knext + 31) / 32), CfgR::THREADS, CfgR::smem(), c->stream>>>(
-              A, lda, K0, knext, n, dinv, s[2] + (knext - kend) * PW, s[3] + (knext - kend) * PW);
+          const unsigned g = (unsigned)((n - knext + 31) / 32);
+          // the B operand of the columns beyond starts (knext - kend) columns in (bf16 or float elements)
+          float* bh = bf16 ? reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(s[2]) + (knext - kend) * PW)
+                           : s[2] + (knext - kend) * PW;
+          if (bf16)
+            k_u12<32, 2, true><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh, nullptr);
+          else
+            k_u12<32, 2, false><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh,
+                                                                            s[3] + (knext - kend) * PW);
           ++c->nlaunch;
           FP_CUDA_TRY(c->err, cudaGetLastError());
         }
         if (int rc = update(slot, kend, K0, knext, n, knext - kend)) return rc;
       }
+      return FP_OK;
+    };
+    if (c->lu_overlap) {
+      OnStream2 on2(c);
+      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
+      if (int rc = rest()) return rc;
+      FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
+    } else {
+      if (int rc = rest()) return rc;
       FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
     }
   }

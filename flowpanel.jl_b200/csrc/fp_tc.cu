@@ -32,11 +32,16 @@
 namespace fpb {
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, THREADS = 128;
+constexpr int BM = 128, BN = 128, BK = 16, THREADS = 128;
 constexpr int TILE_A = BM * BK * 4;                 // 8 KB
 constexpr int TILE_B = BN * BK * 4;                 // 8 KB
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+// the ring's depth: 3 stages (96 KB) for the pivoted factorisation's K = 256
+// panels, 2 (64 KB, still room for the epilogue's 64 KB staging) where
+// the panel kernels of the static-order factorisation must fit beside two
+// of these CTAs on an SM
+template <int STAGES> constexpr int smem_bytes() { return STAGES * STAGE_BYTES + 1024 + 256; }
+static_assert(2 * STAGE_BYTES >= 4 * 32 * BN * 4, "the drained ring holds the epilogue's staging");
 constexpr uint32_t TMEM_COLS = 128;
 constexpr int kWaitLimit = 1 << 22;
 // instruction descriptor: D f32 (bits 4-5 = 1), A/B tf32 (bits 7-9, 10-12 = 2),
@@ -113,6 +118,7 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                : "memory");
 }
 
+template <int STAGES>
 __global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
@@ -226,6 +232,226 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// The same update with several output tiles per CTA and the accumulator
+// double-buffered in TMEM (2 x 128 columns), so that the epilogue of one tile
+// overlaps the MMAs of the next. Warp-specialised, 192 threads:
+//   warp 0 / lane 0   TMA producer: 16-wide K blocks of Ah, Al, Bh, Bl into a
+//                     3-stage ring (full / empty mbarriers);
+//   warp 1 / lane 0   MMA issuer: 3 x 2 tcgen05.mma per K block into
+//                     accumulator t & 1 (after the epilogue has released it),
+//                     tcgen05.commit frees each stage and, after a tile's
+//                     last block, marks the accumulator full;
+//   warps 2..5        epilogue: warp w reads TMEM lanes 32 (w % 4).., i.e.
+//                     the tile's rows 32 (w % 4).., 32 columns at a time,
+//                     stages -D in one of two 4 KB buffers and adds it to C
+//                     by a TMA reduce-add of a 32 x 32 box (the buffer is
+//                     reused once the bulk copy two boxes back has read it),
+//                     then releases the accumulator.
+// A CTA takes tiles_per_cta consecutive tiles (columns fastest within a row
+// of tiles), so CTAs still retire during a long update and the panel kernels
+// of the other stream get SMs. 128 KB of shared memory. Bounded waits as in
+// k_tc_gemm_sub: on a timeout the kernel records DEV_TIMEOUT, each role
+// stops, drains what it issued and the TMEM is freed.
+// With BF16 operands (kind::f16, one MMA per 16-deep step, no lo parts) a
+// K block is 32 elements (the same 64-byte rows) and a stage holds Ah and Bh.
+namespace mt {
+constexpr int STAGES = 3, THREADS = 192;
+constexpr int STG_BYTES = 32 * 32 * 4;   // one epilogue box
+template <bool BF16> __host__ __device__ constexpr int stage_bytes() { return BF16 ? 2 * BM * 64 : STAGE_BYTES; }
+template <bool BF16> __host__ __device__ constexpr int kblock() { return BF16 ? 32 : BK; }
+template <bool BF16> __host__ __device__ constexpr int smem() { return STAGES * stage_bytes<BF16>() + 4 * 2 * STG_BYTES + 1024 + 256; }
+constexpr uint32_t TMEM_COLS = 2 * BN;
+// kind::f16 instruction descriptor: D f32, A/B bf16 (1), both K-major, N >> 3, M >> 4
+constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                ((uint32_t)(BM >> 4) << 24);
+}  // namespace mt
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(mt::IDESC_BF16), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(mt::THREADS, 1)
+k_tc_gemm_multi(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
+                const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
+                const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int tiles_per_cta,
+                int* __restrict__ status) {
+  using namespace mt;
+  constexpr int SB = stage_bytes<BF16>(), KB = kblock<BF16>();
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  float* stage_out = reinterpret_cast<float*>(smem + STAGES * SB);   // [4 warps][2][32 x 32]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * SB + 4 * 2 * STG_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* accf = empty + STAGES;
+  uint64_t* acce = accf + 2;
+  uint64_t* drain = acce + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nk = (K + KB - 1) / KB;
+  const int mt_ = (m + BM - 1) / BM, nt_ = (n + BN - 1) / BN;
+  const int ntiles = mt_ * nt_;
+  const int t0 = blockIdx.x * tiles_per_cta;
+  const int t1 = min(ntiles, t0 + tiles_per_cta);
+  auto tile_mn = [&](int t, int& m0, int& n0) {   // columns fastest: a CTA's tiles share their rows of A
+    m0 = (t / nt_) * BM;
+    n0 = (t % nt_) * BN;
+  };
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    for (int b = 0; b < 2; ++b) { mbar_init(&accf[b], 1); mbar_init(&acce[b], 4); }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(mt::TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {   // producer
+      int it = 0, issued = 0;
+      for (int t = t0; t < t1 && !*(volatile int*)abort_flag; ++t) {
+        int m0, n0;
+        tile_mn(t, m0, n0);
+        for (int kb = 0; kb < nk; ++kb, ++it) {
+          const int s = it % STAGES;
+          if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) { *abort_flag = 1; break; }
+          if (*(volatile int*)abort_flag) break;
+          mbar_expect_tx(&full[s], SB);
+          uint8_t* base = smem + s * SB;
+          if (BF16) {
+            tma_load_2d(base, &tmAh, kb * KB, m0, &full[s]);
+            tma_load_2d(base + SB / 2, &tmBh, kb * KB, n0, &full[s]);
+          } else {
+            tma_load_2d(base, &tmAh, kb * BK, m0, &full[s]);
+            tma_load_2d(base + TILE_A, &tmAl, kb * BK, m0, &full[s]);
+            tma_load_2d(base + 2 * TILE_A, &tmBh, kb * BK, n0, &full[s]);
+            tma_load_2d(base + 2 * TILE_A + TILE_B, &tmBl, kb * BK, n0, &full[s]);
+          }
+          issued = it + 1;
+        }
+      }
+      if (*(volatile int*)abort_flag)   // drain the copies this CTA issued before leaving
+        for (int q = (issued > STAGES ? issued - STAGES : 0); q < issued; ++q)
+          mbar_wait(&full[q % STAGES], (q / STAGES) & 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {   // MMA issuer
+      int it = 0, u = 0;
+      for (int t = t0; t < t1 && !*(volatile int*)abort_flag; ++t, ++u) {
+        const int b = u & 1;
+        if (u >= 2 && !mbar_wait(&acce[b], ((u >> 1) - 1) & 1)) { *abort_flag = 1; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc = tmem + (uint32_t)(b * BN);
+        bool ok = true;
+        for (int kb = 0; kb < nk; ++kb, ++it) {
+          const int s = it % STAGES;
+          if (!mbar_wait(&full[s], (it / STAGES) & 1)) { ok = false; *abort_flag = 1; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t base = smem_u32(smem + s * SB);
+          if (BF16) {
+            const uint64_t dA = sdesc(base), dB = sdesc(base + SB / 2);
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {   // 16 bf16 = 32 bytes along K per MMA
+              const uint64_t off = (uint64_t)((kk * 32) >> 4);
+              umma_bf16(acc, dA + off, dB + off, (kb | kk) != 0 ? 1u : 0u);
+            }
+          } else {
+            const uint64_t dAh = sdesc(base), dAl = sdesc(base + TILE_A);
+            const uint64_t dBh = sdesc(base + 2 * TILE_A), dBl = sdesc(base + 2 * TILE_A + TILE_B);
+#pragma unroll
+            for (int kk = 0; kk < BK / 8; ++kk) {
+              const uint64_t off = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+              umma_tf32(acc, dAh + off, dBl + off, (kb | kk) != 0 ? 1u : 0u);
+              umma_tf32(acc, dAl + off, dBh + off, 1u);
+              umma_tf32(acc, dAh + off, dBh + off, 1u);
+            }
+          }
+          umma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&accf[b]);
+      }
+      if (*(volatile int*)abort_flag && it > 0) {   // MMAs still in flight must finish before TMEM is freed
+        umma_commit(drain);
+        mbar_wait(drain, 0);
+      }
+    }
+  } else {   // epilogue warps 2..5
+    const int q = warp & 3;   // TMEM lanes 32 q .. 32 q + 31 = tile rows
+    float* stg0 = stage_out + (size_t)(warp - 2) * 2 * (STG_BYTES / 4);
+    int u = 0, sb = 0;
+    bool ok = true;
+    for (int t = t0; t < t1 && ok; ++t, ++u) {
+      const int b = u & 1;
+      int m0, n0;
+      tile_mn(t, m0, n0);
+      if (!mbar_wait(&accf[b], (u >> 1) & 1)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+      for (int cc = 0; cc < BN; cc += 32) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + cc);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+              "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        // the bulk copy that last read this staging buffer (two boxes back) is done
+        if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+        __syncwarp();
+        float* stg = stg0 + sb * (STG_BYTES / 4);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) stg[j * 32 + lane] = -__uint_as_float(r[j]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+          if (m0 + q * 32 < m && n0 + cc < n) tma_reduce_add_2d(&tmC, stg, m0 + q * 32, n0 + cc);
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+        sb ^= 1;
+      }
+      // every TMEM read of this accumulator has completed: release it to the MMA warp
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[b]);
+    }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    if (!ok && lane == 0) { *(volatile int*)abort_flag = 1; }
+  }
+  __syncwarp();
+  if (threadIdx.x == 0 && *(volatile int*)abort_flag) atomicOr(status, (int)DEV_TIMEOUT);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(mt::TMEM_COLS) : "memory");
+}
+
 __device__ __forceinline__ float tf32_rna(float x) {
   uint32_t h;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
@@ -302,13 +528,13 @@ static bool make_map(CUtensorMap* tm, const float* base, int kext, int64_t rows,
 
 // 2-D fp32 map over the column-major block C (m rows x n columns, column
 // pitch ldc floats) for the epilogue's reduce-add: inner dim the rows, box
-// 32 rows x BN columns, no swizzle.
-static bool make_map_c(CUtensorMap* tm, float* C, int64_t m, int64_t n, int64_t ldc) {
+// 32 rows x box_cols columns, no swizzle.
+static bool make_map_c(CUtensorMap* tm, float* C, int64_t m, int64_t n, int64_t ldc, int box_cols = BN) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)n};
   cuuint64_t strides[1] = {(cuuint64_t)ldc * 4};
-  cuuint32_t box[2] = {32u, (cuuint32_t)BN};
+  cuuint32_t box[2] = {32u, (cuuint32_t)box_cols};
   cuuint32_t es[2] = {1, 1};
   return fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -338,7 +564,7 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
   // the reduce-add needs a 16-byte aligned C and column pitch
   if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(lda * 4)) & 15) != 0) return false;
   static SmemAttr attr;
-  if (attr.ensure(tc::k_tc_gemm_sub, tc::SMEM_BYTES) != cudaSuccess) return false;
+  if (attr.ensure(tc::k_tc_gemm_sub<3>, tc::smem_bytes<3>()) != cudaSuccess) return false;
   const int slot = c->tc_slot;
   if (ensure_tc_scratch(c, slot, std::max<int64_t>(m, nn)) != FP_OK) return false;
   const int ldk = (int)round_up(kk, 32);
@@ -365,7 +591,7 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
   dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
   const int ev = kt_begin(c);
   TraceScope tr(c, TR_GEMM_TC);
-  tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk,
+  tc::k_tc_gemm_sub<3><<<grid, tc::THREADS, tc::smem_bytes<3>(), c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk,
                                                                        c->d_status);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
@@ -381,18 +607,63 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
         reinterpret_cast<uintptr_t>(Al) | reinterpret_cast<uintptr_t>(Bh) | reinterpret_cast<uintptr_t>(Bl)) &
        15) != 0)
     return false;
-  static SmemAttr attr;
-  if (attr.ensure(tc::k_tc_gemm_sub, tc::SMEM_BYTES) != cudaSuccess) return false;
+  static SmemAttr attr2, attr3, attrm;
+  if (attr2.ensure(tc::k_tc_gemm_sub<2>, tc::smem_bytes<2>()) != cudaSuccess) return false;
+  if (attr3.ensure(tc::k_tc_gemm_sub<3>, tc::smem_bytes<3>()) != cudaSuccess) return false;
+  if (attrm.ensure(tc::k_tc_gemm_multi<false>, tc::mt::smem<false>()) != cudaSuccess) return false;
+  const bool multi = c->tc_tiles > 0;
   CUtensorMap mAh, mAl, mBh, mBl, mC;
   if (!tc::make_map(&mAh, Ah, kk, m, ldk, tc::BM) || !tc::make_map(&mAl, Al, kk, m, ldk, tc::BM) ||
       !tc::make_map(&mBh, Bh, kk, nn, ldk, tc::BN) || !tc::make_map(&mBl, Bl, kk, nn, ldk, tc::BN) ||
-      !tc::make_map_c(&mC, C, m, nn, ldc))
+      !tc::make_map_c(&mC, C, m, nn, ldc, multi ? 32 : tc::BN))
     return false;
   dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
   const int ev = kt_begin(c);
   TraceScope tr(c, TR_GEMM_TC);
-  tc::k_tc_gemm_sub<<<grid, tc::THREADS, tc::SMEM_BYTES, c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk,
-                                                                       c->d_status);
+  if (multi) {
+    const int tiles = (int)(grid.x * grid.y);
+    const unsigned ctas = (unsigned)((tiles + c->tc_tiles - 1) / c->tc_tiles);
+    tc::k_tc_gemm_multi<false><<<ctas, tc::mt::THREADS, tc::mt::smem<false>(), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->tc_tiles, c->d_status);
+  } else if (c->tc_stages == 2)
+    tc::k_tc_gemm_sub<2><<<grid, tc::THREADS, tc::smem_bytes<2>(), c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m,
+                                                                              (int)nn, kk, c->d_status);
+  else
+    tc::k_tc_gemm_sub<3><<<grid, tc::THREADS, tc::smem_bytes<3>(), c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m,
+                                                                              (int)nn, kk, c->d_status);
+  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
+  ++c->nlaunch;
+  return cudaGetLastError() == cudaSuccess;
+}
+
+// C -= A B from BF16 operands (Ah: m rows, Bh: nn columns, K-major with ldk
+// elements a row), FP32 accumulation, on the multi-tile kernel.
+bool tc_gemm_sub_bf16(fp_ctx* c, const void* Ah, const void* Bh, int ldk, float* C, int64_t ldc, int64_t m,
+                      int64_t nn, int kk) {
+  if (kk <= 0 || kk > ldk || m <= 0 || nn <= 0 || (ldk & 7) != 0) return false;
+  if (!tc::encode_fn()) return false;
+  if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(ldc * 4) | reinterpret_cast<uintptr_t>(Ah) |
+        reinterpret_cast<uintptr_t>(Bh)) & 15) != 0)
+    return false;
+  static SmemAttr attr;
+  if (attr.ensure(tc::k_tc_gemm_multi<true>, tc::mt::smem<true>()) != cudaSuccess) return false;
+  auto map16 = [&](CUtensorMap* tm, const void* base, int64_t rows) {
+    cuuint64_t dims[2] = {(cuuint64_t)kk, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ldk * 2};
+    cuuint32_t box[2] = {32u, (cuuint32_t)tc::BM};
+    cuuint32_t es[2] = {1, 1};
+    return tc::encode_fn()(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  CUtensorMap mA, mB, mC;
+  if (!map16(&mA, Ah, m) || !map16(&mB, Bh, nn) || !tc::make_map_c(&mC, C, m, nn, ldc, 32)) return false;
+  const int tiles = (int)(((m + tc::BM - 1) / tc::BM) * ((nn + tc::BN - 1) / tc::BN));
+  const int tpc = c->tc_tiles > 0 ? c->tc_tiles : 4;
+  const int ev = kt_begin(c);
+  TraceScope tr(c, TR_GEMM_TC);
+  tc::k_tc_gemm_multi<true><<<(unsigned)((tiles + tpc - 1) / tpc), tc::mt::THREADS, tc::mt::smem<true>(), c->stream>>>(
+      mA, mA, mB, mB, mC, (int)m, (int)nn, kk, tpc, c->d_status);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;

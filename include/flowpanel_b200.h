@@ -54,6 +54,10 @@ extern "C" {
                             that fails, falls back to FP_PREC_MIXED_GEPP */
 #define FP_PREC_MIXED_GEPP 2  /* FP32 factors pivoted as the FP64 form (partial pivoting inside each
                                  64-row diagonal block) + FP64 refinement */
+#define FP_PREC_BF16 3   /* the largest meshes: the factorisation starts from the BF16-rounded AIC and
+                            its trailing update multiplies BF16 operands (tcgen05 kind::f16) with FP32
+                            accumulation, static row order; refinement hands over to GMRES-IR with
+                            FP64 residuals on the FP64 AIC, which recovers ir_tol */
 
 /* solvers */
 #define FP_SOLVER_LU 0     /* solve_ludiv! / solve_backslash! */
@@ -359,6 +363,21 @@ int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
  * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, in
  * TFLOP/s, the denominator of the compute-bound kernels' roofline. */
 int fp_measure_fma_peak(int device, int fp64, double* tflops);
+
+/* Tuning knobs of a context (no counterpart in the reference; the defaults are
+ * the measured best on B200):
+ *   FP_TUNE_TC_STAGES   2 or 3: depth of the shared-memory ring of the tensor-core
+ *                       trailing update in the static-order FP32 LU (default 2)
+ *   FP_TUNE_LU_OVERLAP  1: that LU updates the columns beyond the next panel on
+ *                       a second stream under the panel work (default); 0: one stream
+ *   FP_TUNE_TC_TILES    output tiles per CTA of that LU's tensor-core update
+ *                       (multi-tile kernel with a double-buffered accumulator);
+ *                       0 (default) selects the one-tile kernel, two CTAs an SM,
+ *                       which measured faster on the 12k wing (10.7 against 13.0 ms) */
+#define FP_TUNE_TC_STAGES 0
+#define FP_TUNE_LU_OVERLAP 1
+#define FP_TUNE_TC_TILES 2
+int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels
  * this context has launched since it was created. */

@@ -42,3 +42,26 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
     Gr = O.assemble_vortexring(w, cps, normals, D, D)
     xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+
+
+@pytest.mark.parametrize("nc,ns", [(20, 24), (60, 80)])
+def test_bf16_form_reaches_fp64_solution(fp, O, ctx, nc, ns):
+    """FP_PREC_BF16: the factorisation starts from the BF16-rounded AIC and its
+    trailing update multiplies BF16 operands with FP32 accumulation; plain
+    refinement stalls on such factors and GMRES-IR with FP64 residuals takes
+    over, reaching the FP64 solution to 1e-10 (ir_tol 1e-12)."""
+    w = fp.meshes.swept_wing("0012", nc, ns)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(4.2)
+    V = np.array([np.cos(a), 0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    x, st = ctx.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "bf16"))
+    assert st.rel_residual < 1e-11, st.asdict()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
