@@ -161,11 +161,11 @@ constexpr size_t pdiag_smem() {
 }
 
 // Warp 0: the IB x IB block at (k0, k0) of As factored in place. Lane i
-// holds row i shifted so that R[0] is the current column (static register
-// indices, rolled step loop); the pivot row goes to the other lanes through
-// a shared buffer (two, alternating, one __syncwarp a step); a row stops
-// shifting once it is the pivot row, so at the end lane i holds U(i, i..)
-// and writes it.
+// holds row i; the step loop is unrolled, so every register index is static
+// and step j touches only columns j.. (the triangle of the work); the pivot
+// row goes to the other lanes through a shared buffer (two, alternating, one
+// __syncwarp a step). Each lane keeps its multipliers in place, so its
+// registers end as its row of L and U.
 __device__ __forceinline__ void eliminate(float (*As)[SP], float* pbuf, int k0, int lane, float& lmax, int* status) {
   float Rw[IB];
   const float4* rp = reinterpret_cast<const float4*>(&As[k0 + lane][k0]);
@@ -175,33 +175,32 @@ __device__ __forceinline__ void eliminate(float (*As)[SP], float* pbuf, int k0, 
     Rw[4 * q] = v.x; Rw[4 * q + 1] = v.y; Rw[4 * q + 2] = v.z; Rw[4 * q + 3] = v.w;
   }
   bool bad = false;
-#pragma unroll 1
+#pragma unroll
   for (int j = 0; j < IB; ++j) {
     float4* pb = reinterpret_cast<float4*>(pbuf + (j & 1) * IB);
     if (lane == j)
 #pragma unroll
-      for (int q = 0; q < IB / 4; ++q) pb[q] = make_float4(Rw[4 * q], Rw[4 * q + 1], Rw[4 * q + 2], Rw[4 * q + 3]);
+      for (int q = j / 4; q < IB / 4; ++q) pb[q] = make_float4(Rw[4 * q], Rw[4 * q + 1], Rw[4 * q + 2], Rw[4 * q + 3]);
     __syncwarp();
     float pv[IB];
 #pragma unroll
-    for (int q = 0; q < IB / 4; ++q) {
+    for (int q = j / 4; q < IB / 4; ++q) {
       const float4 v = pb[q];
       pv[4 * q] = v.x; pv[4 * q + 1] = v.y; pv[4 * q + 2] = v.z; pv[4 * q + 3] = v.w;
     }
-    bad |= !(fabsf(pv[0]) > 0.f && fabsf(pv[0]) <= FLT_MAX);
-    const float rpiv = rcp_fast(pv[0]);
+    bad |= !(fabsf(pv[j]) > 0.f && fabsf(pv[j]) <= FLT_MAX);
+    const float rpiv = rcp_fast(pv[j]);
     if (lane > j) {
-      const float l = Rw[0] * rpiv;
-      As[k0 + lane][k0 + j] = l;
+      const float l = Rw[j] * rpiv;
+      Rw[j] = l;
       lmax = fmaxf(lmax, fabsf(l));
 #pragma unroll
-      for (int c = 0; c < IB - 1; ++c) Rw[c] = fmaf(-l, pv[c + 1], Rw[c + 1]);
-      Rw[IB - 1] = 0.f;
+      for (int c = j + 1; c < IB; ++c) Rw[c] = fmaf(-l, pv[c], Rw[c]);
     }
   }
+  float4* wp = reinterpret_cast<float4*>(&As[k0 + lane][k0]);
 #pragma unroll
-  for (int c = 0; c < IB; ++c)
-    if (c < IB - lane) As[k0 + lane][k0 + lane + c] = Rw[c];
+  for (int q = 0; q < IB / 4; ++q) wp[q] = make_float4(Rw[4 * q], Rw[4 * q + 1], Rw[4 * q + 2], Rw[4 * q + 3]);
   if (bad && lane == 0) atomicOr(status, (int)DEV_ZERO_PIVOT);
 }
 

@@ -221,7 +221,8 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     if (lane == 0 && m0 + warp * 32 < m) {
       tma_reduce_add_2d(&tmC, stg, m0 + warp * 32, n0);
       asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-      asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+      // the CTA may leave once the copy has read the staging buffer; its adds complete in L2
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
     }
   } else if (threadIdx.x == 0) {
     atomicOr(status, (int)DEV_TIMEOUT);
