@@ -51,25 +51,31 @@ def wing_problem(fp, n_chord=N_CHORD, n_span=N_SPAN):
     return w, body, normals, cps, V, D, U
 
 
-def lift_coefficient(fp, body, gamma, V, Uinfs, D, solver):
+def lift_coefficient(fp, body, gamma, V, Uinfs, D, solver, chord=B_SPAN / AR, sref=B_SPAN ** 2 / AR,
+                     with_drag=False):
     """CL as test/runtests_solvers.jl:146-166: probes 0.02*c off the surface,
-    Cp with the Kutta average, F = -Cp q A n, L projected on cross(D, S)."""
+    Cp with the Kutta average, F = -Cp q A n, L projected on cross(D, S);
+    with_drag also returns CD and the Cp field."""
     body.strength = gamma
     body.solved = True
     body.add_field("Uinf", "vector", Uinfs, "cell")
     body.add_field("Da", "vector", D, "system")
     body.add_field("Db", "vector", D, "system")
-    fp.calcfield_U(body, body, offset=0.02, characteristiclength=lambda *a: B_SPAN / AR,
+    fp.calcfield_U(body, body, offset=0.02, characteristiclength=lambda *a: chord,
                    fieldname="Uoff", solver=solver)
-    fp.calcfield_Cp(body, 1.0, U_fieldname="Uoff")
+    Cp = fp.calcfield_Cp(body, 1.0, U_fieldname="Uoff")
     fp.calcfield_F(body, 1.0, 1.225)
     Dhat = V / np.linalg.norm(V)
     Shat = np.array([0.0, 1.0, 0.0])
     Lhat = np.cross(Dhat, Shat)
     LDS = fp.calcfield_LDS(body, Lhat, Dhat)
-    nondim = 0.5 * 1.225 * 1.0 * B_SPAN ** 2 / AR
-    L = LDS[:, 0]
-    return float(np.sign(np.dot(L, Lhat)) * np.linalg.norm(L) / nondim)
+    nondim = 0.5 * 1.225 * 1.0 * sref
+    L, Dr = LDS[:, 0], LDS[:, 1]
+    CL = float(np.sign(np.dot(L, Lhat)) * np.linalg.norm(L) / nondim)
+    if not with_drag:
+        return CL
+    CD = float(np.sign(np.dot(Dr, Dhat)) * np.linalg.norm(Dr) / nondim)
+    return CL, CD, np.array(Cp, copy=True)
 
 
 class ClockSampler:
@@ -480,6 +486,8 @@ def run_ours(args, rank, ws, dist):
     d_launches, d_ms, d_flops, _ = ktime["fp64"]
     batched = batch_throughput(fp, device) if not args.no_batch else None
     post = surface_loads_timing(fp)
+    wingbody = None if args.no_wingbody else wingbody_measure(fp, device, steps=2, warmup=1,
+                                                              cpu=not args.no_cpu_baseline)
     cpu = None
     if not args.no_cpu_baseline:
         O = ge.load_oracle()
@@ -532,6 +540,7 @@ def run_ours(args, rank, ws, dist):
             "aoa_sweep_config3a": aoa,
             "batched_wings": batched,
             "surface_loads": post,
+            "wingbody_config5": wingbody,
             "clocks": clk.summary()}
     if cpu:
         line["cpu_baseline"] = cpu
@@ -540,17 +549,18 @@ def run_ours(args, rank, ws, dist):
     ctx.close()
 
 
-def run_wingbody(args, rank, ws, dist):
+def wingbody_measure(fp, device, steps=3, warmup=1, cpu=True, nprobes=1_000_000):
     """Config 5: prolate-ellipsoid fuselage (120 x 80) + swept NACA 2412 wing
-    (150 x 180), 36,600 vortex-ring panels, rigid wake, AoA 3 deg: mixed solve
-    (FP32 tensor-core LU, FP64 refinement, GMRES-IR if refinement stalls),
-    then velocity and Cp at 1,000,000 probes uniform in a 12 x 12 x 4 m box
-    (default_rng(5)), none within 0.01 m of a panel (FP32 field kernel)."""
-    if rank != 0:
-        return
-    fp = ge.load_package()
+    (150 x 180), 36,600 vortex-ring panels, rigid wake, AoA 3 deg, in the BF16
+    form: the factorisation starts from the BF16-rounded AIC, its trailing
+    update multiplies BF16 operands with FP32 accumulation, and GMRES-IR with
+    FP64 residuals on the FP64 AIC brings the relative residual to 1e-10.
+    Errors of strengths, surface Cp, CL and CD against the device FP64 form
+    (the plain form, which matches the oracle to 1e-10 on the reduced wing-body
+    test). Then velocity and Cp at 1,000,000 probes uniform in a 12 x 12 x 4 m
+    box (default_rng(5)), none within 0.01 m of a panel, by the FP32 kernel,
+    checked against the FP64 kernel on 20,000 of the probes. Returns a dict."""
     cap = fp._capi
-    device = int(os.environ.get("LOCAL_RANK", "0"))
     m = fp.meshes.wing_body()
     body = fp.RigidWakeBody(m)
     N = m.npanels
@@ -565,74 +575,104 @@ def run_wingbody(args, rank, ws, dist):
     ctx.set_wake(m.shedding, D, D)
     ctx.set_rhs(U)
     VR = cap.FP_ELEMENT_VORTEXRING
-    opts = cap.make_opts("ludiv", "mixed")
+    opts = cap.make_opts("ludiv", "bf16", ir_tol=1e-10)
 
     def solve_step():
-        ctx.assemble(VR, 1e-8, 1e-14, cap.FP_PREC_MIXED)
-        ctx.factor(cap.FP_PREC_MIXED)
+        ctx.assemble(VR, 1e-8, 1e-14, cap.FP_PREC_BF16)
+        ctx.factor(cap.FP_PREC_BF16)
         return ctx.solve_device(1, opts)
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         solve_step()
     stg = np.zeros(3)
     with ClockSampler(device) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             st = solve_step()
             stg += [st.ms_assemble, st.ms_factor, st.ms_solve]
-        stg /= args.steps
+        stg /= steps
         gamma, st = ctx.solve(1, opts)
-        probes = fp.meshes.probe_box(m, 1_000_000)
+        probes = fp.meshes.probe_box(m, nprobes)
         M = probes.shape[0]
         ctx.uind(VR, gamma, probes[:1000], np.tile(V, (1000, 1)), cap.FP_PREC_MIXED)   # warm-up
         field_ms = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             Uout = ctx.uind(VR, gamma, probes, np.tile(V, (M, 1)), cap.FP_PREC_MIXED)
             field_ms.append(ctx.last_kernel_ms(cap.FP_STAGE_UIND)[0])
         Cp = 1.0 - np.sum(Uout * Uout, axis=1)
-        U64 = ctx.uind(VR, gamma, probes[:20000], np.tile(V, (20000, 1)), cap.FP_PREC_FP64)
-        f64_ms_per_probe = ctx.last_kernel_ms(cap.FP_STAGE_UIND)[0] / 20000
+    ns64 = min(20000, M)
+    U64 = ctx.uind(VR, gamma, probes[:ns64], np.tile(V, (ns64, 1)), cap.FP_PREC_FP64)
+    f64_ms_per_probe = ctx.last_kernel_ms(cap.FP_STAGE_UIND)[0] / ns64
+    # the FP64 form on the same body, for the errors of the BF16 form
+    x64, st64 = ctx.solve_body(VR, U, opts=cap.make_opts("ludiv", "fp64"))
     fms = float(np.mean(field_ms))
     nquad = int(np.sum(np.diff(m.panel_offsets) == 4))
     ntri = N - nquad
     ops = M * (248.0 * nquad + 186.0 * ntri + 2 * 290.0 * m.nsheddings)
     achieved = ops / (fms * 1e-3) / 1e12
     peak32 = cap.measure_fma_peak(device, False)
-    sub = probes[:2000]
-    ns64 = U64.shape[0]
+    abs_err = np.linalg.norm(Uout[:ns64] - U64, axis=1) / np.linalg.norm(V)   # in freestream-speed units
     rel = np.linalg.norm(Uout[:ns64] - U64, axis=1) / np.linalg.norm(U64, axis=1)
-    rel32 = float(rel.max())
     dCp = np.abs(Cp[:ns64] - (1.0 - np.sum(U64 * U64, axis=1)))
-    line = {"metric": "wing-body 36.6k-panel mixed solve ms + 1M-probe velocity/Cp ms", "value": float(stg.sum() + fms),
-            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-            "data": "synthetic", "dtype": "f64+f32",
-            "config": {"workload": f"wing-body: fuselage 120x80 + NACA2412 wing 150x180 = {N} panels, AoA 3; "
-                                   f"{M} probes in 12x12x4 m box, none within 0.01 m"},
-            "solve_ms": {"assemble": stg[0], "factor": stg[1], "solve": stg[2]},
-            "refinement": {"ir_iters": st.ir_iters, "used_gmres": st.used_gmres, "gmres_iters": st.gmres_iters,
-                           "rel_residual": st.rel_residual},
-            "field_ms": fms, "field_probes_per_s": M / (fms * 1e-3),
-            "field_fp64_ms_per_1M_probes": f64_ms_per_probe * 1e6,
-            "field_rel_err_fp32_vs_fp64": {"max": rel32, "p99_9": float(np.quantile(rel, 0.999)),
-                                            "median": float(np.median(rel)), "probes": int(ns64)},
-            "Cp_abs_err_fp32_vs_fp64": {"max": float(dCp.max()), "p99_9": float(np.quantile(dCp, 0.999))},
-            "Cp_range": [float(Cp.min()), float(Cp.max())],
-            "roofline": {"bound": "fp32 pipe", "kernel": "k_uind_ring<float>", "achieved": achieved, "peak": peak32,
-                         "unit": "TFLOP/s", "frac": achieved / peak32,
-                         "peak_source": "measured FP32 FMA throughput (fp_measure_fma_peak)"},
-            "clocks": clk.summary()}
-    if not args.no_cpu_baseline:
+    croot, taper, AR8 = 1.5, 0.4, 8.0
+    cmean = croot * (1 + taper) / 2
+    b = AR8 * cmean
+    solver = fp.B200Solver("ludiv", "fp64", device=device)
+    CLb, CDb, Cpb = lift_coefficient(fp, body, gamma, V, U, D, solver, chord=cmean, sref=b * cmean, with_drag=True)
+    CLd, CDd, Cpd = lift_coefficient(fp, body, x64, V, U, D, solver, chord=cmean, sref=b * cmean, with_drag=True)
+    solver.close()
+    out = {"config": f"wing-body: fuselage 120x80 + NACA2412 wing 150x180 = {N} panels, AoA 3; "
+                     f"{M} probes in 12x12x4 m box, none within 0.01 m",
+           "form": "bf16: BF16-rounded AIC, BF16 tensor-core operands (kind::f16) with FP32 accumulation, "
+                   "static row order, GMRES-IR with FP64 residuals to 1e-10",
+           "solve_ms": {"assemble": stg[0], "factor": stg[1], "solve": stg[2], "total": float(stg.sum())},
+           "refinement": {"ir_iters": st.ir_iters, "used_gmres": st.used_gmres, "gmres_iters": st.gmres_iters,
+                          "rel_residual": st.rel_residual},
+           "fp64_form_ms": {"assemble": st64.ms_assemble, "factor": st64.ms_factor, "solve": st64.ms_solve},
+           "errors_vs_fp64": {"strength_rel": float(np.linalg.norm(gamma - x64) / np.linalg.norm(x64)),
+                              "Cp_max_abs": float(np.abs(Cpb - Cpd).max()), "CL": CLb, "CL_fp64": CLd,
+                              "abs_dCL": abs(CLb - CLd), "CD": CDb, "CD_fp64": CDd, "abs_dCD": abs(CDb - CDd)},
+           "field_ms": fms, "field_probes_per_s": M / (fms * 1e-3),
+           "field_fp64_ms_per_1M_probes": f64_ms_per_probe * 1e6,
+           "field_err_vs_fp64_kernel_over_Vinf": {"max": float(abs_err.max()),
+                                                  "p99_9": float(np.quantile(abs_err, 0.999)),
+                                                  "median": float(np.median(abs_err)), "probes": int(ns64)},
+           "field_rel_err_vs_fp64_kernel": {"max": float(rel.max()), "p99_9": float(np.quantile(rel, 0.999)),
+                                            "median": float(np.median(rel)), "probes": int(ns64),
+                                            "note": "relative to the local speed, which is near zero inside the bodies"},
+           "Cp_abs_err_vs_fp64_kernel": {"max": float(dCp.max()), "p99_9": float(np.quantile(dCp, 0.999))},
+           "Cp_range": [float(Cp.min()), float(Cp.max())],
+           "field_roofline": {"bound": "fp32 pipe", "kernel": "k_uind_ring<float>",
+                              "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32,
+                              "peak_source": "measured FP32 FMA throughput (fp_measure_fma_peak)"},
+           "clocks": clk.summary()}
+    if cpu:
         O = ge.load_oracle()
         ncores = os.cpu_count() or 1
         ns = 2000
         t0 = time.perf_counter()
-        ref = O.uind_vortexring(m, gamma, D, D, sub[:ns], nthreads=ncores)
+        ref = O.uind_vortexring(m, gamma, D, D, probes[:ns], nthreads=ncores)
         cpu_ms = (time.perf_counter() - t0) * 1e3
-        line["cpu_baseline"] = {"value": cpu_ms * M / ns, "unit": "ms (1M probes, extrapolated)", "cores": ncores,
-                                "kind": "port", "sample": f"{ns} probes with the oracle's threaded Uind, x {M // ns}"}
-        line["field_rel_err_fp32_vs_oracle_max"] = float(np.max(
+        out["field_cpu_baseline"] = {"value": cpu_ms * M / ns, "unit": "ms (1M probes, extrapolated)",
+                                     "cores": ncores, "kind": "port",
+                                     "sample": f"{ns} probes with the oracle's threaded Uind, x {M // ns}"}
+        out["field_rel_err_vs_oracle_max"] = float(np.max(
             np.linalg.norm(Uout[:ns] - (V + ref), axis=1) / np.linalg.norm(V + ref, axis=1)))
-    print(json.dumps(line), flush=True)
     ctx.close()
+    return out
+
+
+def run_wingbody(args, rank, ws, dist):
+    """The config-5 line alone (bench.py --workload wingbody)."""
+    if rank != 0:
+        return
+    fp = ge.load_package()
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    r = wingbody_measure(fp, device, args.steps, args.warmup, cpu=not args.no_cpu_baseline)
+    line = {"metric": "wing-body 36.6k-panel BF16-form solve ms + 1M-probe velocity/Cp ms",
+            "value": r["solve_ms"]["total"] + r["field_ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "data": "synthetic", "dtype": "bf16+f32+f64",
+            "config": {"workload": r["config"]}, **{k: v for k, v in r.items() if k != "config"}}
+    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -643,6 +683,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-wing batched throughput leg")
+    ap.add_argument("--no-wingbody", action="store_true", help="skip the config-5 wing-body leg of the default line")
     ap.add_argument("--workload", default="wing12k", choices=["wing12k", "wingbody", "surface"],
                     help="wingbody: the 36.6k-panel wing-body solve and 1M-probe field evaluation; "
                          "surface: the post-processing (U, grad(mu), Cp, F, L/D/S) of a 12k-triangle wing")

@@ -122,6 +122,10 @@ void free_matrices(fp_ctx* c) {
   }
   c->cap_rhs = 0; c->cap_gmres_m = 0;
   c->assembled = -1; c->factored = -1; c->nrhs = 0;
+  if (c->lu_graph) cudaGraphExecDestroy(c->lu_graph);
+  c->lu_graph = nullptr;
+  c->lu_graph_key.clear();
+  c->lu_graph_seen.clear();
 }
 
 }  // namespace
@@ -457,6 +461,57 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
   return FP_OK;
 }
 
+// The static-order factorisation (lu_factor_static + the diagonal-block
+// inverses of the solves) on c->stream, replayed from a CUDA graph when the
+// same problem (sizes, buffers, form, tuning) was factored before.
+static int factor_static_graph(fp_ctx* c, bool bf16) {
+  auto run = [&]() -> int {
+    int rc = lu_factor_static(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert, bf16);
+    if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
+    return rc;
+  };
+  if (!c->use_graph || c->trace.on || c->ktimer.on) return run();
+  std::vector<uintptr_t> key = {(uintptr_t)c->N, (uintptr_t)c->ld, (uintptr_t)c->d_G32, (uintptr_t)c->d_ipiv,
+                                (uintptr_t)c->d_cert, (uintptr_t)c->d_status, (uintptr_t)c->d_minv,
+                                (uintptr_t)bf16, (uintptr_t)c->tc_stages, (uintptr_t)c->tc_tiles,
+                                (uintptr_t)c->lu_overlap, (uintptr_t)c->use_tc};
+  for (int s = 0; s < 2; ++s)
+    for (int i = 0; i < 4; ++i) key.push_back((uintptr_t)c->d_tc[s][i]);
+  key.push_back((uintptr_t)c->d_dinv32);
+  key.push_back((uintptr_t)c->d_dinv128_32);
+  key.push_back((uintptr_t)c->d_mprev32);
+  if (c->lu_graph && key == c->lu_graph_key) {
+    FP_CUDA_TRY(c->err, cudaGraphLaunch(c->lu_graph, c->stream));
+    return FP_OK;
+  }
+  if (key != c->lu_graph_seen) {   // first time: direct launches (buffers grow here)
+    c->lu_graph_seen = key;
+    return run();
+  }
+  if (c->lu_graph) {
+    cudaGraphExecDestroy(c->lu_graph);
+    c->lu_graph = nullptr;
+  }
+  FP_CUDA_TRY(c->err, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = run();
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return c->err.set(FP_ECUDA, std::string("capture of the factorisation: ") + cudaGetErrorString(e));
+  const cudaError_t ei = cudaGraphInstantiate(&c->lu_graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    c->lu_graph = nullptr;
+    return c->err.set(FP_ECUDA, std::string("instantiating the factorisation graph: ") + cudaGetErrorString(ei));
+  }
+  c->lu_graph_key = key;
+  FP_CUDA_TRY(c->err, cudaGraphLaunch(c->lu_graph, c->stream));
+  return FP_OK;
+}
+
 int fp_factor(fp_ctx* c, int precision) {
   if (check_ctx(c)) return FP_EINVAL;
   cudaSetDevice(c->device);
@@ -486,8 +541,7 @@ int fp_factor(fp_ctx* c, int precision) {
     if (!pivoted) {
       // static row order; a zero or non-finite pivot falls back to the pivoted
       // factorisation of a fresh FP32 copy of the AIC
-      rc = lu_factor_static(c, c->d_G32, c->N, c->ld, c->d_ipiv, c->d_cert, bf16);
-      if (!rc) rc = lu_diag_inverses<float>(c, c->d_G32, c->N, c->ld);
+      rc = factor_static_graph(c, bf16);
       if (rc) return rc;
       if (time_end(c, &ms_static)) return FP_ECUDA;
       int st = 0;
@@ -722,6 +776,9 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
     case FP_TUNE_TC_TILES:
       if (value < 0 || value > 64) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_TILES is 0..64");
       c->tc_tiles = value;
+      return FP_OK;
+    case FP_TUNE_GRAPH:
+      c->use_graph = value != 0;
       return FP_OK;
     default:
       return c->err.set(FP_EINVAL, "fp_set_tuning: unknown knob");

@@ -7,11 +7,8 @@
 // One thread per target, panels staged through shared memory; each target
 // adds the panels in the reference's order (panels, then shedding edges) on
 // top of the value already in out. Compute-bound (FP64 or FP32 pipe). The
-// FP32 form (off-body probes) keeps FP64 where FP32 loses digits: a panel
-// whose centroid lies within kNearFactor of its largest centroid-to-node
-// distance from the target is evaluated in FP64 from the FP64 records (the
-// near-singular edge terms), and so are the wake's horseshoes; these FP64
-// parts sum in FP64 and join the FP32 sum at the end. With
+// FP32 form serves off-body probes: its error grows near the panels, where
+// single-precision positions carry a larger share of the distances. With
 // few targets (the body's own control points) the panels are split in
 // gridDim.y chunks so that the grid fills the device: each chunk writes its
 // partial sum, the last chunk also the shedding edges, and k_uind_reduce adds
@@ -22,9 +19,6 @@ namespace fpb {
 
 constexpr int kFieldThreads = 128;
 constexpr int kFieldTile = 64;
-// near field of the FP32 form: centroid distance below kNearFactor times the
-// panel's largest centroid-to-node distance
-constexpr double kNearFactor = 4.0;
 
 template <class T>
 __global__ void __launch_bounds__(kFieldThreads)
@@ -32,24 +26,18 @@ k_uind_ring(const PanelRec* __restrict__ panels, const double* __restrict__ stre
             const WakeRec* __restrict__ wake, int64_t nsh, const double* __restrict__ targets,
             int64_t m, double* __restrict__ out, double offset, double cutoff2, double offset2,
             double* __restrict__ partial) {
-  constexpr bool kHybrid = sizeof(T) == 4;
-  constexpr int NE = kHybrid ? 18 : 14;   // 12 coordinates, strength, node count (+ centroid, near radius^2)
-  __shared__ T sp[kFieldTile][NE];
+  __shared__ T sp[kFieldTile][14];   // 12 coordinates, strength, node count
   const int64_t t = (int64_t)blockIdx.x * kFieldThreads + threadIdx.x;
   const bool live = t < m;
   const int64_t per = (n + gridDim.y - 1) / gridDim.y;
   const int64_t jb = imin64(n, (int64_t)blockIdx.y * per), je = imin64(n, jb + per);
   const bool last = blockIdx.y == gridDim.y - 1;
-  const double Xd = live ? targets[3 * t] : 0.0, Yd = live ? targets[3 * t + 1] : 0.0,
-               Zd = live ? targets[3 * t + 2] : 0.0;
-  const T X = (T)Xd, Y = (T)Yd, Z = (T)Zd;
-  T u = live && !partial && !kHybrid ? (T)out[3 * t] : T(0);
-  T v = live && !partial && !kHybrid ? (T)out[3 * t + 1] : T(0);
-  T w = live && !partial && !kHybrid ? (T)out[3 * t + 2] : T(0);
-  // FP64 part of the hybrid form: what was in out, the near panels, the wake
-  double ud = live && !partial && kHybrid ? out[3 * t] : 0.0;
-  double vd = live && !partial && kHybrid ? out[3 * t + 1] : 0.0;
-  double wd = live && !partial && kHybrid ? out[3 * t + 2] : 0.0;
+  const T X = live ? (T)targets[3 * t] : T(0);
+  const T Y = live ? (T)targets[3 * t + 1] : T(0);
+  const T Z = live ? (T)targets[3 * t + 2] : T(0);
+  T u = live && !partial ? (T)out[3 * t] : T(0);
+  T v = live && !partial ? (T)out[3 * t + 1] : T(0);
+  T w = live && !partial ? (T)out[3 * t + 2] : T(0);
   const T off = (T)offset, c2 = (T)cutoff2, o2 = (T)offset2;
   for (int64_t j0 = jb; j0 < je; j0 += kFieldTile) {
     const int nt = (int)imin64(kFieldTile, je - j0);
@@ -63,49 +51,15 @@ k_uind_ring(const PanelRec* __restrict__ panels, const double* __restrict__ stre
       else val = P.nn;
       sp[jj][e] = (T)val;
     }
-    if (kHybrid)
-      for (int jj = threadIdx.x; jj < nt; jj += kFieldThreads) {
-        const PanelRec& P = panels[j0 + jj];
-        const int nn = (int)P.nn;
-        double cx = 0, cy = 0, cz = 0;
-        for (int a = 0; a < nn; ++a) { cx += P.p[3 * a]; cy += P.p[3 * a + 1]; cz += P.p[3 * a + 2]; }
-        cx /= nn; cy /= nn; cz /= nn;
-        double r2 = 0;
-        for (int a = 0; a < nn; ++a) {
-          const double dx = P.p[3 * a] - cx, dy = P.p[3 * a + 1] - cy, dz = P.p[3 * a + 2] - cz;
-          r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
-        }
-        sp[jj][14] = (T)cx; sp[jj][15] = (T)cy; sp[jj][16] = (T)cz;
-        sp[jj][17] = (T)(kNearFactor * kNearFactor * r2);
-      }
     __syncthreads();
     if (live) {
-      for (int jj = 0; jj < nt; ++jj) {
-        if (kHybrid) {
-          const T dx = X - sp[jj][14], dy = Y - sp[jj][15], dz = Z - sp[jj][16];
-          if (dx * dx + dy * dy + dz * dz < sp[jj][17]) {   // near: FP64 from the FP64 record
-            const PanelRec& P = panels[j0 + jj];
-            ring_vel<double>(P.p, (int)P.nn, strength[j0 + jj], Xd, Yd, Zd, offset, cutoff2, offset2, ud, vd, wd);
-            continue;
-          }
-        }
+      for (int jj = 0; jj < nt; ++jj)
         ring_vel<T>(sp[jj], (int)sp[jj][13], sp[jj][12], X, Y, Z, off, c2, o2, u, v, w);
-      }
     }
   }
   if (!live) return;
   for (int64_t e = 0; last && e < nsh; ++e) {
     const WakeRec& wr = wake[e];
-    if (kHybrid) {   // the wake's horseshoes in FP64
-      double pa[3] = {wr.pa[0], wr.pa[1], wr.pa[2]}, pb[3] = {wr.pb[0], wr.pb[1], wr.pb[2]};
-      double da[3] = {wr.da[0], wr.da[1], wr.da[2]}, db[3] = {wr.db[0], wr.db[1], wr.db[2]};
-      horseshoe<double>(pa, pb, da, db, strength[wr.pi], Xd, Yd, Zd, offset, cutoff2, offset2, ud, vd, wd);
-      if (wr.pj >= 0) {
-        double qa[3] = {wr.qa[0], wr.qa[1], wr.qa[2]}, qb[3] = {wr.qb[0], wr.qb[1], wr.qb[2]};
-        horseshoe<double>(qa, qb, db, da, strength[wr.pj], Xd, Yd, Zd, offset, cutoff2, offset2, ud, vd, wd);
-      }
-      continue;
-    }
     const T si = (T)strength[wr.pi];
     T pa[3] = {(T)wr.pa[0], (T)wr.pa[1], (T)wr.pa[2]};
     T pb[3] = {(T)wr.pb[0], (T)wr.pb[1], (T)wr.pb[2]};
@@ -120,9 +74,9 @@ k_uind_ring(const PanelRec* __restrict__ panels, const double* __restrict__ stre
     }
   }
   double* dst = partial ? partial + 3 * ((int64_t)blockIdx.y * m + t) : out + 3 * t;
-  dst[0] = (double)u + ud;
-  dst[1] = (double)v + vd;
-  dst[2] = (double)w + wd;
+  dst[0] = (double)u;
+  dst[1] = (double)v;
+  dst[2] = (double)w;
 }
 
 __global__ void __launch_bounds__(kFieldThreads)
@@ -231,9 +185,11 @@ int launch_uind_ring(fp_ctx* c, const double* d_strength, const double* d_target
   const dim3 g((unsigned)((m + kFieldThreads - 1) / kFieldThreads), nchunk);
   const double off = c->kern_offset, cut2 = c->kern_cutoff * c->kern_cutoff, off2 = off * off;
   if (fp32)
-    k_uind_ring<float><<<g, kFieldThreads, 0, c->stream>>>(c->d_panels, d_strength, c->N, c->d_wake, c->nsh, d_targets, m, d_out, off, cut2, off2, part);
+    k_uind_ring<float><<<g, kFieldThreads, 0, c->stream>>>(c->d_panels, d_strength, c->N, c->d_wake, c->nsh,
+                                                           d_targets, m, d_out, off, cut2, off2, part);
   else
-    k_uind_ring<double><<<g, kFieldThreads, 0, c->stream>>>(c->d_panels, d_strength, c->N, c->d_wake, c->nsh, d_targets, m, d_out, off, cut2, off2, part);
+    k_uind_ring<double><<<g, kFieldThreads, 0, c->stream>>>(c->d_panels, d_strength, c->N, c->d_wake, c->nsh,
+                                                            d_targets, m, d_out, off, cut2, off2, part);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return nchunk > 1 ? reduce_chunks(c, nchunk, m, d_out) : FP_OK;

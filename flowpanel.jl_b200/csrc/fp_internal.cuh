@@ -140,6 +140,13 @@ struct fp_ctx {
   int tc_stages = 2;            // ring depth of that update in the static-order LU (fp_set_tuning)
   int tc_tiles = 0;             // static-order LU: output tiles per CTA of the multi-tile update, 0 = one-tile kernel
   bool lu_overlap = true;       // static-order LU: trailing update on the second stream (fp_set_tuning)
+  // The static-order FP32 factorisation replayed as a CUDA graph (both streams,
+  // the diagonal-block inverses included): captured on the second call with
+  // the same key (the first runs the launches directly and grows the scratch
+  // buffers), replayed while the key holds. Off while tracing or timing.
+  bool use_graph = false;
+  cudaGraphExec_t lu_graph = nullptr;
+  std::vector<uintptr_t> lu_graph_key, lu_graph_seen;
   // split operands (Ah, Al, Bh, Bl) of the tensor-core update, one set per
   // stream of the look-ahead factorisation (slot 0: c->stream, 1: stream2)
   float* d_tc[2][4] = {{nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}};

@@ -373,10 +373,16 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *   FP_TUNE_TC_TILES    output tiles per CTA of that LU's tensor-core update
  *                       (multi-tile kernel with a double-buffered accumulator);
  *                       0 (default) selects the one-tile kernel, two CTAs an SM,
- *                       which measured faster on the 12k wing (10.7 against 13.0 ms) */
+ *                       which measured faster on the 12k wing (10.7 against 13.0 ms)
+ *   FP_TUNE_GRAPH       1: the static-order factorisation of a problem factored
+ *                       before (same sizes, buffers and knobs) replays as one CUDA
+ *                       graph; 0 (default): direct launches, which measured faster
+ *                       on the 12k wing (14.8 against 16.4 ms: the captured kernels
+ *                       lose the panel stream's priority) */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
+#define FP_TUNE_GRAPH 3
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels
