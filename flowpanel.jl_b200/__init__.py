@@ -8,12 +8,12 @@ directory by ``__graft_entry__.load_package``).
 from . import _capi, meshes, meshio  # noqa: F401
 from .bodies import (B200Solver, MultiBody, NonLiftingBody, RigidWakeBody, Uind, addfields,  # noqa: F401
                      calc_areas, calc_controlpoints, calc_normals, calcfield_Cp, calcfield_F,
-                     calcfield_LDS, calcfield_U, calcfield_Ugradmu, calcfield_Ugradmu_cell,
+                     calcfield_LDS, calcfield_U, calcfield_Ugradmu, calcfield_Ugradmu_cell, smooth_rows_cells,
                      calcfield_Ugradmu_node, phi, solve, solve_batch, surface_loads)
 
 __all__ = ["B200Solver", "MultiBody", "NonLiftingBody", "RigidWakeBody", "solve", "solve_batch", "Uind", "phi",
            "calcfield_U",
-           "calcfield_Cp", "calcfield_F", "calcfield_LDS", "calcfield_Ugradmu", "calcfield_Ugradmu_cell",
+           "calcfield_Cp", "calcfield_F", "calcfield_LDS", "calcfield_Ugradmu", "calcfield_Ugradmu_cell", "smooth_rows_cells",
            "calcfield_Ugradmu_node", "addfields", "surface_loads", "calc_normals", "calc_controlpoints",
            "calc_areas", "meshes", "meshio"]
 

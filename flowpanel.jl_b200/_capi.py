@@ -29,7 +29,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_kernel_launches", "fp_tc_selftest", "fp_lu_solve_noalloc", "fp_assembly_vjp",
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
            "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls",
-           "fp_ugradmu", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads",
+           "fp_ugradmu", "fp_ugradmu_ex", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads",
            "fp_set_tuning")
 FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH = 0, 1, 2, 3
 
@@ -95,6 +95,8 @@ def lib():
         L.fp_uind.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_int, C.c_double, C.c_double]
         L.fp_phi.argtypes = [vp, C.c_int, _dp, _dp, C.c_int64, _dp, C.c_double]
         L.fp_ugradmu.argtypes = [vp, C.c_int, _dp, _dp, C.c_double, C.c_int, C.c_double, _dp, _dp, _dp]
+        L.fp_ugradmu_ex.argtypes = [vp, C.c_int, _dp, _dp, C.c_double, C.c_int, C.c_double, C.c_int, _ip,
+                                    C.c_int64, C.c_int, _dp, _dp, _dp]
         L.fp_calcfield_cp.argtypes = [vp, _dp, C.c_double, C.c_int, _dp]
         L.fp_calcfield_f.argtypes = [vp, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
         L.fp_calcfield_lds.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
@@ -268,17 +270,23 @@ class Context:
         return out
 
     def ugradmu(self, scheme, strength, cp_offset=None, anglecrit=30.0, force_cellTE=True, maxgrad=np.inf,
-                out=None, want_parts=False):
-        """grad(mu) surface velocity (fp_ugradmu) of the loaded triangular body:
-        scheme FP_UGRADMU_COMBINED / _CELL / _NODE; returns out (N, 3), with
-        (out, out_cell, out_node) when want_parts (combined scheme only)."""
+                out=None, want_parts=False, sharpTE=False, smooth_cells=None, smooth_pass=0):
+        """grad(mu) surface velocity (fp_ugradmu_ex) of the loaded triangular
+        body: scheme FP_UGRADMU_COMBINED / _CELL / _NODE; returns out (N, 3),
+        with (out, out_cell, out_node) when want_parts (combined scheme only).
+        sharpTE: the node scheme's one-sided trailing-edge nodal values;
+        smooth_cells / smooth_pass: the cell scheme's smoothRows cells (in
+        order) and smoothPass."""
         g = _f64(strength)
         n = g.shape[0]
         out = np.zeros((n, 3)) if out is None else np.ascontiguousarray(out, dtype=np.float64)
         oc = np.zeros((n, 3)) if want_parts else None
         on = np.zeros((n, 3)) if want_parts else None
-        self._chk(self._L.fp_ugradmu(self.h, scheme, _d(g), _d(_f64(cp_offset)), float(anglecrit),
-                                     int(bool(force_cellTE)), float(maxgrad), _d(out), _d(oc), _d(on)))
+        sc = np.ascontiguousarray(np.zeros(0) if smooth_cells is None else smooth_cells, dtype=np.int32)
+        self._chk(self._L.fp_ugradmu_ex(self.h, scheme, _d(g), _d(_f64(cp_offset)), float(anglecrit),
+                                        int(bool(force_cellTE)), float(maxgrad), int(bool(sharpTE)),
+                                        sc.ctypes.data_as(_ip) if sc.size else None, int(sc.size),
+                                        int(smooth_pass), _d(out), _d(oc), _d(on)))
         return (out, oc, on) if want_parts else out
 
     def calcfield_cp(self, Us, Uref, correct_kutta=True, out=None):

@@ -441,29 +441,51 @@ def calcfield_Ugradmu(body: AbstractBody, sharpTE=False, force_cellTE=True, angl
     """calcfield_Ugradmu: surface velocity -1/2 grad(mu) of a solved body with
     triangular panels, the cell scheme except where a cell has a free edge or
     a neighbour more than ``anglecrit`` degrees off, which take the node scheme
-    (src/FLOWPanel_postprocess.jl:825-1042), on the device (fp_ugradmu).
+    (src/FLOWPanel_postprocess.jl:825-1042), on the device (fp_ugradmu_ex).
     Returns (N, 3); with ``want_parts`` also the cell and node fields.
-    ``sharpTE`` needs the structured-grid layout of a GeometricTools loft
-    (loop_dim, dimsplit), which these meshes do not carry."""
-    if sharpTE:
-        raise NotImplementedError("sharpTE=true needs the structured-grid layout of a GeometricTools loft")
+    ``sharpTE``: the node scheme's trailing-edge cells take one-sided nodal
+    values at the trailing-edge nodes (see calcfield_Ugradmu_node)."""
     g = _doublet_strength(body, Gammai)
     solver = _field_solver(body, solver)
     out, oc, on = solver.ctx.ugradmu(_capi.FP_UGRADMU_COMBINED, g, _cpoffset_cells(body), anglecrit, force_cellTE,
-                                     want_parts=True)
+                                     want_parts=True, sharpTE=sharpTE)
     if addfield:
         body.add_field(fieldname, "vector", out, "cell")
     return (out, oc, on) if want_parts else out
 
 
+def smooth_rows_cells(smoothRows, ndivscells):
+    """The cells that smoothRows names, in the order the smoothing visits them
+    (src/FLOWPanel_postprocess.jl:500-503: ``for i in smoothRows, j in
+    1:NDIVS[2]``, cell ``linc[i, j]``): ``ndivscells`` = (n1, n2), the cell
+    grid of the triangulated loft (n1 along its first, split dimension),
+    column-major; rows are 1-based as in the reference, 0 meaning none."""
+    n1, n2 = (int(v) for v in ndivscells)
+    rows = [int(i) for i in np.atleast_1d(smoothRows)]
+    if not rows or rows[0] == 0:
+        return np.zeros(0, np.int32)
+    if any(i < 1 or i > n1 for i in rows):
+        raise ValueError(f"smoothRows must lie in 1..{n1}")
+    return np.asarray([(i - 1) + n1 * j for i in rows for j in range(n2)], np.int32)
+
+
 def calcfield_Ugradmu_cell(body: AbstractBody, Gammai=0, maxgrad=np.inf, fieldname="Ugradmu", addfield=True,
-                           solver: Optional[B200Solver] = None):
+                           solver: Optional[B200Solver] = None, smoothPass=0, smoothRows=(0,), ndivscells=None,
+                           smooth_cells=None):
     """calcfield_Ugradmu_cell (src/FLOWPanel_postprocess.jl:139-616): Green-Gauss
     gradient with the inverse-distance face value; the trailing-edge cells'
-    face terms are added back; rows whose norm reaches ``maxgrad`` are zeroed."""
+    face terms are added back; with ``smoothPass`` > 0 the cells of
+    ``smoothRows`` (placed on the loft's cell grid ``ndivscells``, see
+    smooth_rows_cells) or an explicit ``smooth_cells`` list are smoothed
+    (:499-526); then rows whose norm reaches ``maxgrad`` are zeroed."""
     g = _doublet_strength(body, Gammai)
     solver = _field_solver(body, solver)
-    out = solver.ctx.ugradmu(_capi.FP_UGRADMU_CELL, g, _cpoffset_cells(body), maxgrad=maxgrad)
+    if smooth_cells is None and smoothPass and np.atleast_1d(smoothRows)[0] != 0:
+        if ndivscells is None:
+            raise ValueError("smoothRows needs the loft's cell grid: pass ndivscells=(n1, n2) or smooth_cells")
+        smooth_cells = smooth_rows_cells(smoothRows, ndivscells)
+    out = solver.ctx.ugradmu(_capi.FP_UGRADMU_CELL, g, _cpoffset_cells(body), maxgrad=maxgrad,
+                             smooth_cells=smooth_cells, smooth_pass=int(smoothPass))
     if addfield:
         body.add_field(fieldname, "vector", out, "cell")
     return out
@@ -472,12 +494,14 @@ def calcfield_Ugradmu_cell(body: AbstractBody, Gammai=0, maxgrad=np.inf, fieldna
 def calcfield_Ugradmu_node(body: AbstractBody, Gammai=0, sharpTE=False, fieldname="Ugradmu", addfield=True,
                            solver: Optional[B200Solver] = None):
     """calcfield_Ugradmu_node (src/FLOWPanel_postprocess.jl:622-819): -1/2 the
-    linear gradient of the area-weighted nodal values."""
-    if sharpTE:
-        raise NotImplementedError("sharpTE=true needs the structured-grid layout of a GeometricTools loft")
+    linear gradient of the area-weighted nodal values. With ``sharpTE``
+    (:698-742) the trailing-edge cells (each shedding row's upper cells pi,
+    pi+1 and lower cells pj, pj-1: the last and first two loop cells of a
+    loft, :705-708) take at the trailing-edge nodes (the upper edge's nodes)
+    the area-weighted nodal value over their own side's cells only."""
     g = _doublet_strength(body, Gammai)
     solver = _field_solver(body, solver)
-    out = solver.ctx.ugradmu(_capi.FP_UGRADMU_NODE, g, _cpoffset_cells(body))
+    out = solver.ctx.ugradmu(_capi.FP_UGRADMU_NODE, g, _cpoffset_cells(body), sharpTE=sharpTE)
     if addfield:
         body.add_field(fieldname, "vector", out, "cell")
     return out

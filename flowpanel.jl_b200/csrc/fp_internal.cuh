@@ -168,6 +168,12 @@ struct fp_ctx {
   double* d_area = nullptr;             // N panel areas
   int32_t* d_teflag = nullptr;          // N: times the cell is a shedding pi/pj (low 16 bits), bit 16 = forced cell value
   int32_t* d_krow = nullptr;            // nsh x 4 slots of (pi, pi+1, pj, pj-1) in d_kcell, -1 absent
+  // sharp trailing edge (node scheme): the trailing-edge node slot of each
+  // node (-1 if none), and per slot the upper (pi, pi+1) and lower (pj, pj-1)
+  // cells that contain it, as two CSR lists
+  int32_t* d_teslot = nullptr;          // topo_nnodes
+  int32_t* d_tecsr = nullptr;           // [up offsets (nte+1)] [up cells] [lo offsets (nte+1)] [lo cells]
+  int64_t nte = 0, te_up_cells = 0, te_lo_cells = 0;
   int32_t* d_kcell = nullptr;           // distinct cells of the Kutta rows
   int32_t* d_klast = nullptr;           // per distinct cell: the last row that overwrites its force
   int64_t nkcell = 0;

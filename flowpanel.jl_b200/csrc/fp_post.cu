@@ -39,6 +39,8 @@ namespace {
 constexpr int kPostThreads = 128;
 constexpr int kKuttaThreads = 512;
 constexpr int kForcedCell = 1 << 16;     // teflag bit: cell value forced on the node scheme (pi, pi+1, pj, pj-1)
+constexpr int kTeUpper = 1 << 17;        // teflag bit: an upper trailing-edge cell (pi, pi+1) of the sharp-TE node scheme
+constexpr int kTeLower = 1 << 18;        // teflag bit: a lower trailing-edge cell (pj, pj-1)
 constexpr size_t kKuttaSmemMax = 48 * 1024;
 
 template <class T> void dfree(T*& p) {
@@ -56,6 +58,10 @@ struct PostArgs {
   const double* sgn;       // sign(CPoffset) per cell (1 where 0)
   const double* g;         // strengths (the Gammai column)
   const double* nodal;     // nodal values (node scheme)
+  int sharpte;             // node scheme: trailing-edge cells take their side's nodal values at TE nodes
+  const int32_t* teslot;   // node -> trailing-edge slot, -1 if none
+  const double* nodal_te;  // 2 x nte: the upper, then the lower nodal values of the TE nodes
+  int64_t nte;
   int mode;                // FP_UGRADMU_* or -1 for none
   int force_cellTE;
   double cosang;
@@ -173,8 +179,15 @@ __global__ void __launch_bounds__(kPostThreads) k_ugradmu(PostArgs a) {
     }
     if (a.mode == FP_UGRADMU_COMBINED || a.mode == FP_UGRADMU_NODE) {
       const int32_t* tri = a.nb + 3 * N + 3 * c;
+      double nv[3];
+      const int side = (a.teflag[c] & kTeLower) ? 1 : 0;   // a cell of both sides ends with the lower values
+      const bool te_cell = a.sharpte && (a.teflag[c] & (kTeUpper | kTeLower));
+      for (int k = 0; k < 3; ++k) {
+        const int32_t t = te_cell ? a.teslot[tri[k]] : -1;
+        nv[k] = t >= 0 ? a.nodal_te[side * a.nte + t] : a.nodal[tri[k]];
+      }
       double g[3];
-      tri_gradient(P, s * a.nodal[tri[0]], s * a.nodal[tri[1]], s * a.nodal[tri[2]], g);
+      tri_gradient(P, s * nv[0], s * nv[1], s * nv[2], g);
       for (int d = 0; d < 3; ++d) on[d] = -0.5 * g[d];
     }
     if (a.mode == FP_UGRADMU_COMBINED) {
@@ -218,6 +231,58 @@ __global__ void __launch_bounds__(kPostThreads) k_ugradmu(PostArgs a) {
     const double val = a.qneg * cp * a.area[c];
     for (int d = 0; d < 3; ++d) a.F[3 * c + d] = 0.0 + val * (a.tgt[(3 + d) * N + c] * s);
   }
+}
+
+// The trailing-edge nodes' nodal values from one side's cells only: the
+// area-weighted mean over the upper (then the lower) cells that contain the
+// node (GeometricTools' get_nodal_data_TEcells, restated in the weighting of
+// k_nodal). csr: [up offsets][up cells][lo offsets][lo cells].
+__global__ void __launch_bounds__(kPostThreads)
+k_nodal_te(const int32_t* __restrict__ csr, int64_t nte, int64_t nup, const double* __restrict__ area,
+           const double* __restrict__ g, double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * kPostThreads + threadIdx.x;
+  if (i >= 2 * nte) return;
+  const int side = (int)(i / nte);
+  const int64_t t = i % nte;
+  const int32_t* off = csr + (side ? (nte + 1 + nup) : 0);
+  const int32_t* cells = off + nte + 1;
+  double num = 0.0, den = 0.0;
+  for (int32_t k = off[t]; k < off[t + 1]; ++k) {
+    const int32_t c = cells[k];
+    num += area[c] * g[c];
+    den += area[c];
+  }
+  out[i] = den > 0.0 ? num / den : 0.0;
+}
+
+// smoothPass / smoothRows of the cell scheme (postprocess.jl:501-526): passes
+// times, each listed cell in order takes the mean of its neighbours' current
+// values (in place, so later cells see the earlier ones' new values); one
+// thread, as the recurrence is sequential.
+__global__ void k_smooth(const int32_t* __restrict__ nb, const int32_t* __restrict__ cells, int64_t ncells,
+                         int passes, double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int p = 0; p < passes; ++p)
+    for (int64_t q = 0; q < ncells; ++q) {
+      const int32_t c = cells[q];
+      double acc[3] = {0.0, 0.0, 0.0};
+      int cnt = 0;
+      for (int k = 0; k < 3; ++k) {
+        const int32_t n = nb[3 * c + k];
+        if (n < 0) continue;
+        ++cnt;
+        for (int d = 0; d < 3; ++d) acc[d] += out[3 * n + d];
+      }
+      for (int d = 0; d < 3; ++d) out[3 * c + d] = acc[d] / cnt;
+    }
+}
+
+// the cell scheme's maxgrad cut, after the smoothing
+__global__ void __launch_bounds__(kPostThreads) k_maxgrad(double* __restrict__ out, int64_t N, double maxgrad) {
+  const int64_t c = (int64_t)blockIdx.x * kPostThreads + threadIdx.x;
+  if (c >= N) return;
+  const double n = sqrt(out[3 * c] * out[3 * c] + out[3 * c + 1] * out[3 * c + 1] + out[3 * c + 2] * out[3 * c + 2]);
+  if (n >= maxgrad) out[3 * c] = out[3 * c + 1] = out[3 * c + 2] = 0.0;
 }
 
 struct KuttaArgs {
@@ -458,6 +523,54 @@ int build_kutta(fp_ctx* c) {
       klast[slot[cc]] = (int32_t)r;
     }
   }
+  // sharp trailing edge: the upper cells pi, pi+1 and lower cells pj, pj-1,
+  // the TE nodes (the upper edge's nodes) and, per TE node, the cells of
+  // each side that contain it
+  const int64_t nnodes = (int64_t)c->h_nodes.size() / 3;
+  std::vector<int32_t> up, lo, tenodes, teslot(nnodes, -1);
+  for (int64_t r = 0; r < nsh; ++r) {
+    const int32_t* s = c->h_shed.data() + 6 * r;
+    const int32_t pi = s[0], pj = s[3];
+    for (int32_t cc : {pi, pi + 1})
+      if (cc >= 0 && cc < N && !(te[cc] & kTeUpper)) { te[cc] |= kTeUpper; up.push_back(cc); }
+    if (pj != -1)
+      for (int32_t cc : {pj, pj - 1})
+        if (cc >= 0 && cc < N && !(te[cc] & kTeLower)) { te[cc] |= kTeLower; lo.push_back(cc); }
+    for (int k : {s[1], s[2]}) {
+      const int32_t v = c->h_pnodes[c->h_offsets[pi] + k];
+      if (v >= 0 && v < nnodes && teslot[v] < 0) {
+        teslot[v] = (int32_t)tenodes.size();
+        tenodes.push_back(v);
+      }
+    }
+  }
+  const int64_t nte = (int64_t)tenodes.size();
+  std::vector<int32_t> csr;
+  int64_t nup = 0;
+  for (const std::vector<int32_t>* side : {&up, &lo}) {
+    std::vector<std::vector<int32_t>> lists(nte);
+    for (int32_t cc : *side)
+      for (int k = c->h_offsets[cc]; k < c->h_offsets[cc + 1]; ++k) {
+        const int32_t t = teslot[c->h_pnodes[k]];
+        if (t >= 0) lists[t].push_back(cc);
+      }
+    const size_t base = csr.size();
+    csr.resize(base + nte + 1);
+    csr[base] = 0;
+    for (int64_t t = 0; t < nte; ++t) csr[base + t + 1] = csr[base + t] + (int32_t)lists[t].size();
+    for (int64_t t = 0; t < nte; ++t) csr.insert(csr.end(), lists[t].begin(), lists[t].end());
+    if (side == &up) nup = csr[base + nte];
+  }
+  dfree(c->d_teslot); dfree(c->d_tecsr);
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_teslot, std::max<int64_t>(nnodes, 1) * sizeof(int32_t)));
+  FP_CUDA_TRY(c->err, cudaMalloc(&c->d_tecsr, csr.size() * sizeof(int32_t)));
+  if (nnodes > 0)
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_teslot, teslot.data(), nnodes * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                        c->stream));
+  FP_CUDA_TRY(c->err, cudaMemcpyAsync(c->d_tecsr, csr.data(), csr.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                      c->stream));
+  c->nte = nte;
+  c->te_up_cells = nup;
   const int64_t nk = (int64_t)kcell.size();
   dfree(c->d_teflag); dfree(c->d_krow); dfree(c->d_kcell); dfree(c->d_klast);
   FP_CUDA_TRY(c->err, cudaMalloc(&c->d_teflag, N * sizeof(int32_t)));
@@ -558,6 +671,7 @@ bool unit(const double* v) {
 void post_free(fp_ctx* c) {
   dfree(c->d_nb); dfree(c->d_voff); dfree(c->d_vcell); dfree(c->d_area);
   dfree(c->d_teflag); dfree(c->d_krow); dfree(c->d_kcell); dfree(c->d_klast);
+  dfree(c->d_teslot); dfree(c->d_tecsr);
   dfree(c->d_post);
   c->cap_post = 0;
   dfree(c->d_uscr);
@@ -571,6 +685,13 @@ using namespace fpb;
 
 int fp_ugradmu(fp_ctx* c, int scheme, const double* strength, const double* cp_offset, double anglecrit,
                int force_cellTE, double maxgrad, double* out, double* out_cell, double* out_node) {
+  return fp_ugradmu_ex(c, scheme, strength, cp_offset, anglecrit, force_cellTE, maxgrad, 0, nullptr, 0, 0, out,
+                       out_cell, out_node);
+}
+
+int fp_ugradmu_ex(fp_ctx* c, int scheme, const double* strength, const double* cp_offset, double anglecrit,
+                  int force_cellTE, double maxgrad, int sharpTE, const int32_t* smooth_cells, int64_t nsmooth,
+                  int smooth_pass, double* out, double* out_cell, double* out_node) {
   if (!c) return FP_EINVAL;
   FP_CUDA_TRY(c->err, cudaSetDevice(c->device));
   if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_ugradmu: no geometry");
@@ -578,16 +699,25 @@ int fp_ugradmu(fp_ctx* c, int scheme, const double* strength, const double* cp_o
     return c->err.set(FP_EINVAL, "fp_ugradmu: bad arguments");
   if (scheme != FP_UGRADMU_COMBINED && (out_cell || out_node))
     return c->err.set(FP_EINVAL, "fp_ugradmu: out_cell/out_node belong to the combined scheme");
+  if (nsmooth < 0 || smooth_pass < 0 || (nsmooth > 0 && !smooth_cells))
+    return c->err.set(FP_EINVAL, "fp_ugradmu: bad smoothing arguments");
+  for (int64_t q = 0; q < nsmooth; ++q)
+    if (smooth_cells[q] < 0 || smooth_cells[q] >= c->N)
+      return c->err.set(FP_EINVAL, "fp_ugradmu: smoothing cell index out of range");
+  const bool smooth = scheme == FP_UGRADMU_CELL && nsmooth > 0 && smooth_pass > 0;
   int rc;
   if ((rc = build_topology(c)) || (rc = build_kutta(c))) return rc;
   const int64_t N = c->N, nn = c->topo_nnodes;
-  if ((rc = ensure_post(c, (size_t)(2 * N + nn + 9 * N)))) return rc;
+  const int64_t nte = c->nte;
+  if ((rc = ensure_post(c, (size_t)(2 * N + nn + 9 * N + 2 * nte + (nsmooth + 1) / 2 + 1)))) return rc;
   double* d_g = c->d_post;
   double* d_sgn = d_g + N;
   double* d_nodal = d_sgn + N;
   double* d_out = d_nodal + nn;
   double* d_oc = d_out + 3 * N;
   double* d_on = d_oc + 3 * N;
+  double* d_nte = d_on + 3 * N;
+  int32_t* d_smooth = reinterpret_cast<int32_t*>(d_nte + 2 * nte);
   std::vector<double> sg;
   signs_of(cp_offset, N, sg);
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(d_g, strength, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -598,12 +728,34 @@ int fp_ugradmu(fp_ctx* c, int scheme, const double* strength, const double* cp_o
   a.teflag = c->d_teflag; a.sgn = d_sgn; a.g = d_g; a.mode = scheme; a.force_cellTE = force_cellTE;
   // cosd(anglecrit) with the degree-to-radian factor applied first
   a.cosang = std::cos(anglecrit * (M_PI / 180.0));
-  a.maxgrad = maxgrad;
+  a.maxgrad = smooth ? INFINITY : maxgrad;   // with smoothing, the cut follows it
   a.out = d_out;
   a.out_cell = out_cell ? d_oc : nullptr;
   a.out_node = out_node ? d_on : nullptr;
+  a.sharpte = sharpTE && nte > 0 && scheme != FP_UGRADMU_CELL;
+  a.teslot = c->d_teslot;
+  a.nodal_te = d_nte;
+  a.nte = nte;
+  if (smooth)
+    FP_CUDA_TRY(c->err, cudaMemcpyAsync(d_smooth, smooth_cells, nsmooth * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                        c->stream));
   if (ev_begin(c)) return FP_ECUDA;
+  if (a.sharpte) {
+    k_nodal_te<<<grid_of(2 * nte, kPostThreads), kPostThreads, 0, c->stream>>>(c->d_tecsr, nte, c->te_up_cells,
+                                                                                c->d_area, d_g, d_nte);
+    ++c->nlaunch;
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+  }
   if ((rc = launch_scheme(c, a, d_nodal))) return rc;
+  if (smooth) {
+    k_smooth<<<1, 32, 0, c->stream>>>(c->d_nb, d_smooth, nsmooth, smooth_pass, d_out);
+    ++c->nlaunch;
+    if (std::isfinite(maxgrad)) {
+      k_maxgrad<<<grid_of(N, kPostThreads), kPostThreads, 0, c->stream>>>(d_out, N, maxgrad);
+      ++c->nlaunch;
+    }
+    FP_CUDA_TRY(c->err, cudaGetLastError());
+  }
   double ms = 0;
   if (ev_end(c, &ms)) return FP_ECUDA;
   c->kms[FP_STAGE_POST] = ms;

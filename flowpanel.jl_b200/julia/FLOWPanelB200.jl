@@ -182,17 +182,23 @@ end
 """Device path of calcfield_Ugradmu! / _cell! / _node! (src/FLOWPanel_postprocess.jl:139-941) for a
 solved body with triangular panels: `scheme` FP_UGRADMU_COMBINED (out_cell and out_node
 receive the two schemes' fields), FP_UGRADMU_CELL (adds into out, maxgrad) or FP_UGRADMU_NODE
-(overwrites out). `cpoffset` holds every panel's CPoffset (each member's own in a MultiBody)."""
+(overwrites out). `cpoffset` holds every panel's CPoffset (each member's own in a MultiBody).
+`sharpTE` (node and combined schemes) and `smoothPass` / `smoothRows` (cell scheme, the rows
+placed on the loft's cell grid `ndivscells` = (n1, n2), column-major) as in the reference."""
 function Ugradmu_b200!(self, out::Matrix{Float64}, solver::B200Solver, cpoffset::Vector{Float64};
                        scheme=FP_UGRADMU_COMBINED, out_cell=nothing, out_node=nothing,
-                       anglecrit=30.0, force_cellTE=true, maxgrad=Inf, Gammai=1)
+                       anglecrit=30.0, force_cellTE=true, maxgrad=Inf, Gammai=1, sharpTE=false,
+                       smoothPass=0, smoothRows=(0,), ndivscells=(0, 0))
     s = Vector{Float64}(self.strength[:, Gammai])
     oc = out_cell === nothing ? C_NULL : out_cell
     on = out_node === nothing ? C_NULL : out_node
-    GC.@preserve s cpoffset out out_cell out_node fp_check(solver, ccall((:fp_ugradmu, libfp), Cint,
-        (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Cdouble, Cint, Cdouble, Ptr{Float64}, Ptr{Float64},
-         Ptr{Float64}),
-        solver.ctx, scheme, s, cpoffset, anglecrit, Cint(force_cellTE), maxgrad, out, oc, on))
+    cells = smoothPass == 0 || smoothRows[1] == 0 ? Int32[] :
+            Int32[(i - 1) + ndivscells[1] * (j - 1) for i in smoothRows for j in 1:ndivscells[2]]
+    GC.@preserve s cpoffset out out_cell out_node cells fp_check(solver, ccall((:fp_ugradmu_ex, libfp), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Cdouble, Cint, Cdouble, Cint, Ptr{Int32}, Int64, Cint,
+         Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+        solver.ctx, scheme, s, cpoffset, anglecrit, Cint(force_cellTE), maxgrad, Cint(sharpTE),
+        isempty(cells) ? C_NULL : cells, length(cells), Cint(smoothPass), out, oc, on))
     return out
 end
 

@@ -258,6 +258,23 @@ int fp_phi(fp_ctx* ctx, int element, const double* strengths, const double* targ
 int fp_ugradmu(fp_ctx* ctx, int scheme, const double* strength, const double* cp_offset, double anglecrit,
                int force_cellTE, double maxgrad, double* out, double* out_cell, double* out_node);
 
+/* fp_ugradmu with the schemes' remaining options (fp_ugradmu is this call with
+ * sharpTE = 0 and no smoothing):
+ *   sharpTE (node and combined schemes; calcfield_Ugradmu_node!'s sharpTE,
+ *       src/FLOWPanel_postprocess.jl:698-742): the trailing-edge cells take,
+ *       at the trailing-edge nodes (the nodes of each shedding row's upper
+ *       edge), the area-weighted nodal value over their own side's cells only:
+ *       upper cells pi, pi+1, lower cells pj, pj-1, the lower side last;
+ *   smooth_cells / nsmooth / smooth_pass (cell scheme; smoothRows and
+ *       smoothPass, :499-526): after all gradients, smooth_pass times, each
+ *       listed cell in list order takes the mean of its edge neighbours'
+ *       current values; the maxgrad cut follows the smoothing. The list is
+ *       the cells of smoothRows, in the reference's row-then-span order.
+ * FP_EINVAL for a cell index outside 0..N-1 or negative counts. */
+int fp_ugradmu_ex(fp_ctx* ctx, int scheme, const double* strength, const double* cp_offset, double anglecrit,
+                  int force_cellTE, double maxgrad, int sharpTE, const int32_t* smooth_cells, int64_t nsmooth,
+                  int smooth_pass, double* out, double* out_cell, double* out_node);
+
 /* calcfield_Cp! (src/FLOWPanel_postprocess.jl:1059-1112): out (N) +=
  * 1 - (|U|/Uref)^2 for the velocities Us (N x 3), then, with correct_kutta,
  * the average over (pi, pi+1, pj, pj-1) of each shedding row in row order. */

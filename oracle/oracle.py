@@ -564,7 +564,7 @@ def _gg_term(P, tri, k, nc, cpc, cpn, gc, gn, area, hs):
     return np.array([hs * d1 * mag, hs * d2 * mag, hs * d3 * mag])
 
 
-def ugradmu_cell(mesh, gammas, areas, normals, cps, cpsign, nb=None, maxgrad=np.inf):
+def ugradmu_cell(mesh, gammas, areas, normals, cps, cpsign, nb=None, maxgrad=np.inf, smooth=None, passes=0):
     """calcfield_Ugradmu_cell! (src/FLOWPanel_postprocess.jl:270-540, the
     RigidWakeBody method; without shedding rows it is the AbstractBody method
     of :139-268): Green-Gauss over the cell's edges with the inverse-distance
@@ -590,6 +590,8 @@ def ugradmu_cell(mesh, gammas, areas, normals, cps, cpsign, nb=None, maxgrad=np.
         for ci in ((pi, pj) if pj != -1 else (pi,)):
             for t in terms(ci):
                 out[ci] += t
+    if smooth is not None and passes > 0:
+        smooth_cells(mesh, out, smooth, passes, nb)
     big = np.linalg.norm(out, axis=1) >= maxgrad
     out[big] = 0.0
     return out
@@ -610,23 +612,92 @@ def tri_gradient(p1, p2, p3, v1, v2, v3):
     return gx * e1 + gy * e2
 
 
-def ugradmu_node(mesh, gammas, areas, cpsign):
-    """calcfield_Ugradmu_node! (src/FLOWPanel_postprocess.jl:622-748 with
-    sharpTE=false): nodal values as the area-weighted mean of the cells around
-    each node, the cell's linear gradient of them (the nodal values take the
-    sign of CPoffset), times -1/2."""
+def te_cells(mesh):
+    """The trailing-edge cells of the sharp-TE node scheme: the upper cells
+    pi, pi+1 and the lower cells pj, pj-1 of every shedding row (the last and
+    first two loop cells of a lofted grid, postprocess.jl:705-712), in row
+    order, and the trailing-edge nodes (the upper edge's nodes)."""
+    offs, pn = mesh.panel_offsets, mesh.panel_nodes
+    up, lo, te = [], [], []
+    for (pi, nia, nib, pj, nja, njb) in np.reshape(mesh.shedding, (-1, 6)):
+        for c in (pi, pi + 1):
+            if 0 <= c < mesh.npanels and c not in up:
+                up.append(int(c))
+        if pj != -1:
+            for c in (pj, pj - 1):
+                if 0 <= c < mesh.npanels and c not in lo:
+                    lo.append(int(c))
+        for k in (nia, nib):
+            v = int(pn[offs[pi] + k])
+            if v not in te:
+                te.append(v)
+    return up, lo, te
+
+
+def nodal_data_cells(mesh, values, areas, nodes, cells):
+    """Nodal values at `nodes` from the given cells only: the area-weighted mean
+    over those of `cells` that contain the node (GeometricTools'
+    get_nodal_data_TEcells, restated in the weighting of nodal_data)."""
+    offs, pn = mesh.panel_offsets, mesh.panel_nodes
+    out = {}
+    for v in nodes:
+        num = den = 0.0
+        for c in cells:
+            if v in pn[offs[c]:offs[c + 1]]:
+                num += areas[c] * values[c]
+                den += areas[c]
+        out[v] = num / den if den > 0 else 0.0
+    return out
+
+
+def ugradmu_node(mesh, gammas, areas, cpsign, sharpTE=False):
+    """calcfield_Ugradmu_node! (src/FLOWPanel_postprocess.jl:622-748): nodal
+    values as the area-weighted mean of the cells around each node, the
+    cell's linear gradient of them (the nodal values take the sign of
+    CPoffset), times -1/2. With sharpTE the trailing-edge cells take, at the
+    trailing-edge nodes, the nodal values of their own side only: the upper
+    cells first, then the lower ones (postprocess.jl:698-742)."""
     P = np.asarray(mesh.nodes, float)
     nodal = nodal_data(mesh, gammas, areas)
     offs, pn = mesh.panel_offsets, mesh.panel_nodes
     out = np.zeros((mesh.npanels, 3))
-    for ci in range(mesh.npanels):
+
+    def grad(ci, nod):
         v = pn[offs[ci]:offs[ci] + 3]
         s = cpsign[ci]
-        out[ci] = tri_gradient(P[v[0]], P[v[1]], P[v[2]], s * nodal[v[0]], s * nodal[v[1]], s * nodal[v[2]])
+        return tri_gradient(P[v[0]], P[v[1]], P[v[2]], s * nod[v[0]], s * nod[v[1]], s * nod[v[2]])
+
+    for ci in range(mesh.npanels):
+        out[ci] = grad(ci, nodal)
+    if sharpTE and mesh.nsheddings > 0:
+        up, lo, te = te_cells(mesh)
+        for cells in (up, lo):
+            side = nodal.copy()
+            for v, val in nodal_data_cells(mesh, gammas, areas, te, cells).items():
+                side[v] = val
+            for ci in cells:
+                out[ci] = grad(ci, side)
     return -0.5 * out
 
 
-def ugradmu(mesh, gammas, areas, normals, cps, cpsign, force_cellTE=True, anglecrit=30.0):
+def smooth_cells(mesh, out, cells, passes, nb=None):
+    """smoothPass / smoothRows of calcfield_Ugradmu_cell!
+    (src/FLOWPanel_postprocess.jl:501-526): `passes` times, each listed cell in
+    order takes the mean of its neighbours' current values, in place."""
+    nb = mesh_neighbors(mesh) if nb is None else nb
+    for _ in range(passes):
+        for ci in cells:
+            acc = np.zeros(3)
+            k = 0
+            for n in nb[ci]:
+                if n >= 0:
+                    acc += out[n]
+                    k += 1
+            out[ci] = acc / k
+    return out
+
+
+def ugradmu(mesh, gammas, areas, normals, cps, cpsign, force_cellTE=True, anglecrit=30.0, sharpTE=False):
     """calcfield_Ugradmu! (src/FLOWPanel_postprocess.jl:825-941): the cell
     scheme, except where a cell has a free edge or a neighbour whose normal is
     more than ``anglecrit`` degrees off, which take the node scheme (with the
@@ -636,7 +707,7 @@ def ugradmu(mesh, gammas, areas, normals, cps, cpsign, force_cellTE=True, anglec
 
     nb = mesh_neighbors(mesh)
     oc = ugradmu_cell(mesh, gammas, areas, normals, cps, cpsign, nb)
-    on = ugradmu_node(mesh, gammas, areas, cpsign)
+    on = ugradmu_node(mesh, gammas, areas, cpsign, sharpTE=sharpTE)
     if force_cellTE:
         for (pi, nia, nib, pj, nja, njb) in np.reshape(mesh.shedding, (-1, 6)):
             on[pi] = oc[pi]

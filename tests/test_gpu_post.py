@@ -73,6 +73,36 @@ def test_ugradmu_argument_semantics(fp, O, wing, wctx):
         assert close(d, base + o)
 
 
+def test_ugradmu_sharpte_and_smoothing_match_oracle(fp, O, wing, wctx):
+    """sharpTE (node and combined schemes) and the cell scheme's smoothing
+    (smoothRows / smoothPass, then the maxgrad cut) against the oracle; the
+    smoothed cells are the shedding rows' pi and pi+1 cells, then every 7th
+    cell, twice over."""
+    m, g = wing["mesh"], wing["gam"]
+    a = (m, g, wing["areas"])
+    node = wctx.ugradmu(fp._capi.FP_UGRADMU_NODE, g, wing["cpoff"], sharpTE=True)
+    want = O.ugradmu_node(*a, wing["sgn"], sharpTE=True)
+    assert close(node, want)
+    plain = O.ugradmu_node(*a, wing["sgn"])
+    assert np.abs(want - plain).max() > 1e-3 * np.abs(plain).max()   # sharpTE changes the TE cells
+    up, lo, te = O.te_cells(m)
+    other = np.setdiff1d(np.arange(m.npanels), up + lo)
+    assert close(node[other], plain[other])
+    d, dc, dn = wctx.ugradmu(fp._capi.FP_UGRADMU_COMBINED, g, wing["cpoff"], want_parts=True, sharpTE=True)
+    o, oc, on = O.ugradmu(*a, wing["normals"], wing["cps"], wing["sgn"], sharpTE=True)
+    assert close(d, o) and close(dc, oc) and close(dn, on)
+    sh = m.shedding
+    cells = np.concatenate([sh[:, 0], sh[:, 0] + 1, np.arange(3, m.npanels, 7)]).astype(np.int32)
+    for passes, mg in ((1, np.inf), (2, np.inf), (2, 2.0)):
+        want = O.ugradmu_cell(*a, wing["normals"], wing["cps"], wing["sgn"], maxgrad=mg, smooth=cells,
+                              passes=passes)
+        got = wctx.ugradmu(fp._capi.FP_UGRADMU_CELL, g, wing["cpoff"], maxgrad=mg, smooth_cells=cells,
+                           smooth_pass=passes)
+        assert close(got, want), passes
+    with pytest.raises(fp._capi.FlowPanelError):
+        wctx.ugradmu(fp._capi.FP_UGRADMU_CELL, g, wing["cpoff"], smooth_cells=[m.npanels], smooth_pass=1)
+
+
 def test_calcfields_match_oracle(fp, O, wing, wctx):
     U, Cp, F, LDS, CL, CD, (Lhat, Dhat, Shat) = oracle_loads(O, wing)
     m = wing["mesh"]

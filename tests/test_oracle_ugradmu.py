@@ -101,6 +101,74 @@ def test_trailing_edge_cells_cancel(fp, O):
     assert np.abs(oc[7]).max() > 1e-3
 
 
+def test_sharp_te_uses_one_sided_nodal_values(fp, O):
+    """sharpTE: the node scheme changes only on the TE cells (upper pi, pi+1;
+    lower pj, pj-1), whose gradients use, at the TE nodes, the area-weighted
+    mean over their own side's cells (checked here by a direct evaluation)."""
+    m = flat_grid(fp)
+    m.shedding = np.array([[20, 1, 0, 19, 0, 1]], np.int32)   # 19 and 18 share the TE nodes of 20
+    normals, cps, areas = O.geometry(m)
+    g = np.random.default_rng(5).standard_normal(m.npanels)
+    s = np.ones(m.npanels)
+    plain = O.ugradmu_node(m, g, areas, s)
+    sharp = O.ugradmu_node(m, g, areas, s, sharpTE=True)
+    up, lo, te = O.te_cells(m)
+    assert up == [20, 21] and lo == [19, 18]
+    assert te == [int(m.panel(20)[1]), int(m.panel(20)[0])]
+    other = np.setdiff1d(np.arange(m.npanels), up + lo)
+    assert np.array_equal(sharp[other], plain[other])
+    nodal = O.nodal_data(m, g, areas)
+    P = np.asarray(m.nodes, float)
+    for cells in (up, lo):
+        side = nodal.copy()
+        for v in te:
+            has = [c for c in cells if v in m.panel(c)]
+            side[v] = sum(areas[c] * g[c] for c in has) / sum(areas[c] for c in has)
+        for c in cells:
+            v = m.panel(c)
+            want = -0.5 * O.tri_gradient(P[v[0]], P[v[1]], P[v[2]], side[v[0]], side[v[1]], side[v[2]])
+            assert np.abs(sharp[c] - want).max() < 1e-13
+    assert np.abs(sharp[up + lo] - plain[up + lo]).max() > 1e-6
+
+
+def test_smoothing_is_sequential_neighbour_mean(fp, O):
+    """smoothRows / smoothPass: each listed cell, in order, becomes the mean of
+    its neighbours' current values (a later cell sees an earlier one's new
+    value); a linear strength's exact interior gradient is left unchanged;
+    the maxgrad cut comes after the smoothing."""
+    m = flat_grid(fp)
+    normals, cps, areas = O.geometry(m)
+    nb = O.mesh_neighbors(m)
+    s = np.ones(m.npanels)
+    a = np.array([0.7, -1.3, 0.0])
+    inner = np.flatnonzero(interior(O, m, nb))
+    base = O.ugradmu_cell(m, cps @ a, areas, normals, cps, s)
+    sm = O.ugradmu_cell(m, cps @ a, areas, normals, cps, s, smooth=inner[:10], passes=3)
+    ok = [c for c in inner[:10] if all(n in inner for n in nb[c])]
+    assert len(ok) > 0 and np.abs(sm[ok] - base[ok]).max() < 1e-12
+    g = np.random.default_rng(7).standard_normal(m.npanels)
+    raw = O.ugradmu_cell(m, g, areas, normals, cps, s)
+    c0 = int(inner[0])
+    c1 = int(next(n for n in nb[c0] if n >= 0))
+    want = raw.copy()
+    want[c0] = np.mean([want[n] for n in nb[c0] if n >= 0], axis=0)
+    want[c1] = np.mean([want[n] for n in nb[c1] if n >= 0], axis=0)   # sees the new value of c0
+    got = O.ugradmu_cell(m, g, areas, normals, cps, s, smooth=[c0, c1], passes=1)
+    assert np.abs(got - want).max() < 1e-14
+    mg = float(np.linalg.norm(want[c1]))
+    cut = O.ugradmu_cell(m, g, areas, normals, cps, s, maxgrad=mg, smooth=[c0, c1], passes=1)
+    assert np.all(cut[c1] == 0.0)
+
+
+def test_smooth_rows_cells_order(fp):
+    """smoothRows on a (n1, n2) cell grid: rows outer, span inner, column-major."""
+    cells = fp.smooth_rows_cells([1, 4], (6, 3))
+    assert cells.tolist() == [0, 6, 12, 3, 9, 15]
+    assert fp.smooth_rows_cells((0,), (6, 3)).size == 0
+    with pytest.raises(ValueError):
+        fp.smooth_rows_cells([7], (6, 3))
+
+
 def vtu_wing_oracle(fp, O):
     """The swept wing of examples/sweptwing.jl (AoA 4.2, 30 m/s) from the two
     .vtu half-wing meshes (test/runtests_meshes.jl:190-262), solved and
