@@ -246,6 +246,93 @@ def wing_half(contour, y0, y1, nspan, chord0, chord1, xle0, xle1, twist0=0.0, tw
     return m
 
 
+def discretize_ndivs(NDIVS, length=1.0):
+    """Node positions 0..length of the NDIVS sections [(fraction, ncells,
+    expansion, central), ...] of GeometricTools' discretisation, as
+    simplewing's ``span_NDIVS`` and ``rfl_NDIVS`` give them
+    (src/FLOWPanel_utils.jl:110-125): each section covers ``fraction`` of the
+    length with ``ncells`` cells whose lengths grow linearly from the first to
+    the last by the factor ``expansion`` (the lofted swept wing of
+    examples/sweptwing.jl pins this: 15 cells at expansion 10 grow by equal
+    steps from 1 to 10); ``central`` mirrors the growth about the section's
+    middle (cells grow from both ends towards it by ``expansion``)."""
+    pts = [0.0]
+    x0 = 0.0
+    tot = sum(float(f) for f, *_ in NDIVS)
+    for frac, n, r, central in NDIVS:
+        L = length * float(frac) / tot
+        n = int(n)
+        if central and n > 1:
+            h = n // 2
+            w = _ramp(h, r) if h > 0 else np.zeros(0)
+            mid = [1.0 * r] if n % 2 else []
+            w = np.concatenate([w, mid, w[::-1]])
+        else:
+            w = _ramp(n, r)
+        w = w / w.sum() * L
+        pts.extend((x0 + np.cumsum(w)).tolist())
+        x0 += L
+    out = np.asarray(pts)
+    out[-1] = length
+    return out
+
+
+def _ramp(n, r):
+    """n cell weights growing linearly from 1 to r."""
+    if n == 1:
+        return np.ones(1)
+    return 1.0 + (float(r) - 1.0) * np.arange(n) / (n - 1)
+
+
+def simplewing(section, b, ar, tr=1.0, lambda_=0.0, gamma=0.0, span_NDIVS=((1.0, 35, 20.0, True),),
+               b_low=-1.0, b_up=1.0, name="wing", CPoffset=0.0, kind="vortexring"):
+    """The lofted wing of simplewing (src/FLOWPanel_utils.jl:68-150): tip chord
+    b/ar, root chord (b/ar)/tr, leading edge swept by ``lambda_`` and raised
+    by ``gamma`` (degrees), chord and leading edge linear in |semi-span
+    position| s (s = 0 at the root, 1 at the tips), stations at s in
+    [b_low, b_up] from ``span_NDIVS`` (discretize_ndivs, first cell at
+    b_low), untwisted.
+
+    ``section`` (K, 2) is the re-discretised airfoil on a unit chord as a
+    closed loop of K distinct points, x/c and z/c, starting at the trailing
+    edge along the lower surface (the layout of the reference's lofted
+    meshes). Nodes: station-major, K per station; triangles: per span strip,
+    per loop edge k, (a, b, c) and (c, d, a) with a = (j, k), b = (j, k+1),
+    c = (j+1, k+1), d = (j+1, k) -- the split of the reference's triangulated
+    loft (GridTriangleSurface with dimsplit = 1). Shedding rows as
+    generate_loft_liftbody sets them (src/FLOWPanel_abstractliftingbody.jl:
+    85-100): per span strip j, pi = the first triangle of the loop's last
+    quad, pj = the second triangle of its first quad, local nodes (3, 2) of
+    each (1-based), i.e. 0-based rows (2K-2 + 2Kj, 2, 1, 1 + 2Kj, 2, 1)."""
+    sec = np.asarray(section, float)
+    K = sec.shape[0]
+    semispan = b / 2
+    c_tip = b / ar
+    c_root = c_tip / tr
+    t = discretize_ndivs(span_NDIVS)
+    s = b_low + (b_up - b_low) * t
+    a = np.abs(s)
+    chord = c_root + (c_tip - c_root) * a
+    xle = a * semispan * np.tan(np.deg2rad(lambda_))
+    zle = a * semispan * np.tan(np.deg2rad(gamma))
+    nst = len(s)
+    nodes = np.zeros((nst, K, 3))
+    nodes[:, :, 0] = xle[:, None] + chord[:, None] * sec[None, :, 0]
+    nodes[:, :, 1] = (s * semispan)[:, None]
+    nodes[:, :, 2] = zle[:, None] + chord[:, None] * sec[None, :, 1]
+    pn = []
+    for j in range(nst - 1):
+        for k in range(K):
+            a_, b_ = j * K + k, j * K + (k + 1) % K
+            c_, d_ = (j + 1) * K + (k + 1) % K, (j + 1) * K + k
+            pn += [a_, b_, c_, c_, d_, a_]
+    npan = len(pn) // 3
+    sh = np.asarray([(2 * K - 2 + 2 * K * j, 2, 1, 1 + 2 * K * j, 2, 1) for j in range(nst - 1)], np.int32)
+    m = Mesh(nodes.reshape(-1, 3), np.arange(0, 3 * npan + 1, 3, dtype=np.int32), np.asarray(pn, np.int32), sh)
+    m.bodies = [Body(name, kind, npan, len(sh), CPoffset)]
+    return m
+
+
 def swept_wing(naca="0012", n_chord=100, n_span=120, chord=1.0, b=5.0, sweep=45.0, taper=1.0,
                twist_root=0.0, twist_tip=0.0):
     """Swept wing as a MultiBody of two halves lofted from the root outwards on
