@@ -284,6 +284,100 @@ def _ramp(n, r):
     return 1.0 + (float(r) - 1.0) * np.arange(n) / (n - 1)
 
 
+def rediscretize_airfoil(x, y, NDIVS_up, NDIVS_lo, spline_k=5, spline_s=1e-8, nsamples=100_000):
+    """Re-discretise an airfoil contour (GeometricTools' rediscretize_airfoil,
+    as simplewing calls it with rflspl_s, src/FLOWPanel_utils.jl:76-147):
+    the contour, from the trailing edge over one surface to the leading edge
+    (the point of least x) and back over the other, is split there; each
+    surface is splined as y(x) with the smoothing spline of FITPACK (curfit,
+    order ``spline_k``, smoothing ``spline_s``: the library both
+    GeometricTools' Dierckx and scipy's UnivariateSpline wrap) and
+    re-discretised by arc length from the leading edge with the NDIVS
+    sections (discretize_ndivs), the arc length measured on ``nsamples``
+    chords of the curve. Returns (K, 2): the trailing edge (from the second
+    surface's spline), the second surface from the trailing edge to before
+    the leading edge, the leading edge (first surface), then the first
+    surface up to before the trailing edge -- the closed loop of the
+    reference's lofted sections. With the reference's RAE 101 file and
+    rfl_NDIVS this reproduces the section of its lofted swept-wing mesh to
+    1e-9 of the chord."""
+    from scipy.interpolate import UnivariateSpline
+
+    x = np.asarray(x, float)
+    y = np.asarray(y, float)
+    ile = int(np.argmin(x))
+    first = np.stack([x[:ile + 1][::-1], y[:ile + 1][::-1]], axis=1)    # LE -> TE
+    second = np.stack([x[ile:], y[ile:]], axis=1)                        # LE -> TE
+
+    def surface(pts, NDIVS):
+        sp = UnivariateSpline(pts[:, 0], pts[:, 1], k=spline_k, s=spline_s)
+        xs = np.linspace(pts[0, 0], pts[-1, 0], nsamples + 1)
+        ys = sp(xs)
+        L = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(xs), np.diff(ys)))])
+        xn = np.interp(discretize_ndivs(NDIVS) * L[-1], L, xs)
+        return np.stack([xn, sp(xn)], axis=1)
+
+    a = surface(first, NDIVS_up)
+    b = surface(second, NDIVS_lo)
+    return np.concatenate([b[::-1][:-1], a[:-1]])
+
+
+def revolution_liftbody(profile, NDIVS_theta, name="body", CPoffset=0.0, kind="vortexring"):
+    """Lifting body of revolution about the x axis (generate_revolution_liftbody,
+    src/FLOWPanel_abstractliftingbody.jl:124-176): ``profile`` (K, 2) is the
+    closed contour (x axial, r radial; first point = last point, kept as two
+    nodes: the grid loops in the azimuth only), revolved over NDIVS_theta
+    equal azimuthal steps (the reference's start angle, 270 deg, is a
+    multiple of the step for any NDIVS_theta dividing 360 into whole degrees
+    of that kind, and only permutes the stations). Nodes station-major, K per
+    station; triangles per strip and profile edge k as in simplewing, (a, b,
+    c) and (c, d, a) with a = (j, k), b = (j, k+1), c = (j+1, k+1),
+    d = (j+1, k), the azimuth running so that the normals point away from the
+    contour's interior (into the flow). Shedding rows as the reference sets
+    them for a closed contour: per strip, pi = the first triangle of the
+    last profile quad, pj = the second triangle of the first, local nodes
+    (3, 2) of each (1-based)."""
+    P = np.asarray(profile, float)
+    K = P.shape[0]
+    nq = K - 1
+    th = 2 * np.pi * np.arange(NDIVS_theta) / NDIVS_theta
+
+    def build(sign):
+        t = sign * th
+        nodes = np.zeros((NDIVS_theta, K, 3))
+        nodes[:, :, 0] = P[None, :, 0]
+        nodes[:, :, 1] = P[None, :, 1] * np.cos(t)[:, None]
+        nodes[:, :, 2] = P[None, :, 1] * np.sin(t)[:, None]
+        return nodes.reshape(-1, 3)
+
+    def tris():
+        pn = []
+        for j in range(NDIVS_theta):
+            j1 = (j + 1) % NDIVS_theta
+            for k in range(nq):
+                a_, b_, c_, d_ = j * K + k, j * K + k + 1, j1 * K + k + 1, j1 * K + k
+                pn += [a_, b_, c_, c_, d_, a_]
+        return np.asarray(pn, np.int32)
+
+    pn = tris()
+    nodes = build(1.0)
+    # orientation: the normal of a triangle a quarter of the way round the
+    # contour against the direction from the contour's centroid (at that
+    # azimuth) to the triangle
+    q = 3 * 2 * (nq // 4)
+    tri = nodes[pn[q:q + 3]]
+    nrm = np.cross(tri[1] - tri[0], tri[2] - tri[0])
+    cen = P[:-1].mean(axis=0)
+    ref = np.array([cen[0], cen[1], 0.0])
+    if np.dot(nrm, tri.mean(axis=0) - ref) < 0:
+        nodes = build(-1.0)
+    npan = len(pn) // 3
+    sh = np.asarray([(2 * nq - 2 + 2 * nq * j, 2, 1, 1 + 2 * nq * j, 2, 1) for j in range(NDIVS_theta)], np.int32)
+    m = Mesh(nodes, np.arange(0, 3 * npan + 1, 3, dtype=np.int32), pn, sh)
+    m.bodies = [Body(name, kind, npan, len(sh), CPoffset)]
+    return m
+
+
 def simplewing(section, b, ar, tr=1.0, lambda_=0.0, gamma=0.0, span_NDIVS=((1.0, 35, 20.0, True),),
                b_low=-1.0, b_up=1.0, name="wing", CPoffset=0.0, kind="vortexring"):
     """The lofted wing of simplewing (src/FLOWPanel_utils.jl:68-150): tip chord

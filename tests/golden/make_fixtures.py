@@ -12,6 +12,11 @@ Run from the repository root where the reference checkout is available:
   triangles), read with ``meshio.read_msh``; used by
   test/runtests_meshes2.jl:45-93.
 
+* ``airfoils.npz``: the airfoil contours examples/data/airfoil-rae101.csv
+  (RAE 101, the swept wing of test/runtests_solvers.jl and
+  examples/sweptwing.jl) and examples/data/naca662015.csv (NACA 66-2015, the
+  duct of test/runtests_solvers2.jl), (x, y) in file order.
+
 Nodes are float64, cells int32 CSR (0-based), both in file order.
 """
 import os
@@ -38,6 +43,9 @@ def main(ref):
         out[f"offsets_{side}"] = m.panel_offsets
         out[f"pnodes_{side}"] = m.panel_nodes
     np.savez_compressed(os.path.join(HERE, "sweptwing_vtu.npz"), **out)
+    np.savez_compressed(os.path.join(HERE, "airfoils.npz"),
+                        rae101=np.loadtxt(os.path.join(data, "airfoil-rae101.csv"), delimiter=",", skiprows=1),
+                        naca662015=np.loadtxt(os.path.join(data, "naca662015.csv"), delimiter=",", skiprows=1))
     m = mio.read_msh(os.path.join(data, "sweptwing-openvsp.msh"))
     np.savez_compressed(os.path.join(HERE, "sweptwing_openvsp.npz"), nodes=m.nodes, offsets=m.panel_offsets,
                         pnodes=m.panel_nodes)
