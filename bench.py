@@ -476,8 +476,17 @@ def run_ours(args, rank, ws, dist):
     tc_launches, tc_ms, tc_flops, tc_elems = ktime["mixed"]
     tc_tflops = tc_flops / (tc_ms * 1e-3) / 1e12 if tc_ms > 0 else 0.0
     peak_tc, peak_src = measured_peak("bf16_tflops", 1590.0)
+    peak_hbm, hbm_src = measured_peak("hbm_gbs", 6650.0)
     per_elem = profile_traffic("k_tc_gemm_sub")   # DRAM bytes per updated C element, from ncu
     traffic = per_elem * tc_elems / tc_launches if (per_elem and tc_launches) else None
+    # with K = 128 the update does 2 x 128 flops per C element against 8 bytes
+    # of C read-modify-write (32 flop/B), under the 3xTF32 ridge point
+    # (bf16 peak / 2 / 3 over HBM, ~43 flop/B): HBM is the bound that applies
+    tc_gbs = 8.0 * tc_elems / (tc_ms * 1e-3) / 1e9 if tc_ms > 0 else 0.0
+    # the critical path: the panel chain on stream 0, led by the diagonal
+    # block (one CTA, dependent elimination steps)
+    diag = next((k for k in timeline["kernels"] if k["stream"] == 0 and k["kernel"] == "diagonal block"), None)
+    peak32 = cap.measure_fma_peak(device, False)
     # FP64 pipe roofline of the assembly: ops pinned by the oracle's operation
     # counter (248 per quad-ring interaction, 290 per horseshoe) / device time
     peak64 = cap.measure_fma_peak(device, True)
@@ -522,12 +531,27 @@ def run_ours(args, rank, ws, dist):
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 3 * 8 * N,
                     "d2h_bytes_per_step": 8 * N},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor", "kernel": "k_tc_gemm_sub (tcgen05 3xTF32 trailing update)",
-                         "achieved": tc_tflops, "peak": peak_tc, "unit": "TFLOP/s",
-                         "frac": tc_tflops / peak_tc, "traffic": traffic,
-                         "launches": tc_launches, "ms_total": tc_ms,
-                         "peak_source": peak_src + " (dense BF16; the TF32 pipe is half of it, and 3xTF32 "
-                                        "issues 3 tensor MMAs per algorithmic flop)"},
+            "roofline": {"bound": "hbm", "kernel": "k_tc_gemm_sub (tcgen05 3xTF32 trailing update, K = 128)",
+                         "achieved": tc_gbs, "peak": peak_hbm, "unit": "GB/s", "frac": tc_gbs / peak_hbm,
+                         "traffic": traffic, "launches": tc_launches, "ms_total": tc_ms,
+                         "algorithmic_bytes": "8 B per updated C element (FP32 read + write; the operand "
+                                              "panels add under 3 %)",
+                         "peak_source": hbm_src,
+                         "tensor_view": {"achieved_tflops": tc_tflops, "bf16_peak_tflops": peak_tc,
+                                         "frac_of_bf16": tc_tflops / peak_tc,
+                                         "frac_of_3xtf32_ceiling": tc_tflops / (peak_tc / 6.0),
+                                         "note": "2 m n k algorithmic flops; TF32 runs at half the BF16 "
+                                                 "rate and 3xTF32 issues 3 MMAs per flop"}},
+            "critical_path_roofline": None if diag is None else {
+                "bound": "latency", "kernel": "k_pdiag (128 x 128 diagonal block, one CTA)",
+                "avg_us_in_place": diag["avg_us"], "launches": diag["launches"],
+                "achieved_gflops": (2.0 / 3.0) * 128 ** 3 / (diag["avg_us"] * 1e-6) / 1e9,
+                "peak_gflops_one_sm": peak32 * 1e3 / 148.0,
+                "frac": (2.0 / 3.0) * 128 ** 3 / (diag["avg_us"] * 1e-6) / 1e9 / (peak32 * 1e3 / 148.0),
+                "chain_ms": timeline["stream0_busy_ms"], "span_ms": timeline["span_ms"],
+                "peak_source": "measured FP32 FMA throughput (fp_measure_fma_peak) / 148 SMs",
+                "note": "2/3 128^3 flops per launch on one SM: the kernel is a chain of dependent steps, "
+                        "its frac says how far from compute-bound it is"},
             "assembly_roofline": {"bound": "fp64 pipe", "kernel": "k_asm_ring+k_asm_wake",
                                   "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                                   "frac": achieved / peak64,
