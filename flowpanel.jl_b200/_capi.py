@@ -31,7 +31,8 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls",
            "fp_ugradmu", "fp_ugradmu_ex", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads",
            "fp_set_tuning")
-FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH = 0, 1, 2, 3
+FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH, FP_TUNE_TC_SMEM = 0, 1, 2, 3, 4
+FP_TUNE_FP64_DMMA = 5
 
 
 class SolveOpts(C.Structure):
@@ -382,7 +383,7 @@ class Context:
         return tags, streams, t0, t1
 
     def set_tuning(self, knob, value):
-        """fp_set_tuning: FP_TUNE_TC_STAGES (2 or 3), FP_TUNE_LU_OVERLAP (0 or 1)."""
+        """fp_set_tuning: one of the FP_TUNE_* knobs (include/flowpanel_b200.h)."""
         self._chk(self._L.fp_set_tuning(self.h, int(knob), int(value)))
 
     def kernel_timing(self, enable=True):

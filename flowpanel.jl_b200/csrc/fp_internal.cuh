@@ -139,6 +139,8 @@ struct fp_ctx {
   bool use_tc = true;           // tcgen05 3xTF32 trailing update for the FP32 factors
   int tc_stages = 2;            // ring depth of that update in the static-order LU (fp_set_tuning)
   int tc_tiles = 0;             // static-order LU: output tiles per CTA of the multi-tile update, 0 = one-tile kernel
+  int tc_smem = 0;              // static-order LU: shared memory reserved by each one-tile update CTA (0 = its own)
+  bool fp64_dmma = true;        // FP64 LU: trailing update on the FP64 tensor path (mma.sync .f64) instead of SIMT
   bool lu_overlap = true;       // static-order LU: trailing update on the second stream (fp_set_tuning)
   // The static-order FP32 factorisation replayed as a CUDA graph (both streams,
   // the diagonal-block inverses included): captured on the second call with
@@ -269,6 +271,8 @@ int num_sms();
 
 // Raises a kernel's dynamic shared-memory limit once per device. Thread-safe:
 // a repeated call from a racing thread only sets the same value again.
+constexpr int kTcSmemMax = 232448;   // the opt-in shared memory of one CTA on sm_100
+
 struct SmemAttr {
   std::atomic<unsigned long long> done{0};
   template <class K>

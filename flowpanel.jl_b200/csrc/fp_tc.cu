@@ -565,7 +565,7 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
   // the reduce-add needs a 16-byte aligned C and column pitch
   if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(lda * 4)) & 15) != 0) return false;
   static SmemAttr attr;
-  if (attr.ensure(tc::k_tc_gemm_sub<3>, tc::smem_bytes<3>()) != cudaSuccess) return false;
+  if (attr.ensure(tc::k_tc_gemm_sub<3>, kTcSmemMax) != cudaSuccess) return false;
   const int slot = c->tc_slot;
   if (ensure_tc_scratch(c, slot, std::max<int64_t>(m, nn)) != FP_OK) return false;
   const int ldk = (int)round_up(kk, 32);
@@ -609,8 +609,8 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
        15) != 0)
     return false;
   static SmemAttr attr2, attr3, attrm;
-  if (attr2.ensure(tc::k_tc_gemm_sub<2>, tc::smem_bytes<2>()) != cudaSuccess) return false;
-  if (attr3.ensure(tc::k_tc_gemm_sub<3>, tc::smem_bytes<3>()) != cudaSuccess) return false;
+  if (attr2.ensure(tc::k_tc_gemm_sub<2>, kTcSmemMax) != cudaSuccess) return false;
+  if (attr3.ensure(tc::k_tc_gemm_sub<3>, kTcSmemMax) != cudaSuccess) return false;
   if (attrm.ensure(tc::k_tc_gemm_multi<false>, tc::mt::smem<false>()) != cudaSuccess) return false;
   const bool multi = c->tc_tiles > 0;
   CUtensorMap mAh, mAl, mBh, mBl, mC;
@@ -627,11 +627,11 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
     tc::k_tc_gemm_multi<false><<<ctas, tc::mt::THREADS, tc::mt::smem<false>(), c->stream>>>(
         mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->tc_tiles, c->d_status);
   } else if (c->tc_stages == 2)
-    tc::k_tc_gemm_sub<2><<<grid, tc::THREADS, tc::smem_bytes<2>(), c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m,
-                                                                              (int)nn, kk, c->d_status);
+    tc::k_tc_gemm_sub<2><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status);
   else
-    tc::k_tc_gemm_sub<3><<<grid, tc::THREADS, tc::smem_bytes<3>(), c->stream>>>(mAh, mAl, mBh, mBl, mC, (int)m,
-                                                                              (int)nn, kk, c->d_status);
+    tc::k_tc_gemm_sub<3><<<grid, tc::THREADS, std::max(tc::smem_bytes<3>(), c->tc_smem), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;

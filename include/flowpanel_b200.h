@@ -395,11 +395,20 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       before (same sizes, buffers and knobs) replays as one CUDA
  *                       graph; 0 (default): direct launches, which measured faster
  *                       on the 12k wing (14.8 against 16.4 ms: the captured kernels
- *                       lose the panel stream's priority) */
+ *                       lose the panel stream's priority)
+ *   FP_TUNE_TC_SMEM     bytes of shared memory each CTA of that LU's one-tile
+ *                       tensor-core update reserves (0, the default: its ring
+ *                       and barriers only; at most 232448): fewer update CTAs
+ *                       an SM, more room for the panel kernels beside them
+ *   FP_TUNE_FP64_DMMA   1 (default): the FP64 LU's trailing update runs on the FP64
+ *                       tensor path (mma.sync .f64), 16.9 TF/s on the 12k wing;
+ *                       0: the SIMT FP64 kernel, 15.0 TF/s (same results) */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
 #define FP_TUNE_GRAPH 3
+#define FP_TUNE_TC_SMEM 4
+#define FP_TUNE_FP64_DMMA 5
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels

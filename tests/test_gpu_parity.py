@@ -79,6 +79,30 @@ def test_wing_solve_matches_oracle(fp, O, ctx, precision):
         assert st.max_abs_L > 0
 
 
+@pytest.mark.parametrize("nc,ns", [(40, 48), (60, 90)])
+def test_fp64_lu_dmma_update_matches_oracle(fp, O, nc, ns):
+    """FP_TUNE_FP64_DMMA = 1: the FP64 LU's trailing update on the FP64 tensor
+    path (mma.sync .f64) gives the oracle's strengths to 1e-10, and the SIMT
+    update's to 1e-12 (1,920 and 5,400 panels: several 256-column panels with
+    partial tiles at the edges)."""
+    w, body, normals, cps, D, U = _wing_setup(fp, nc, ns)
+    xs = []
+    for dmma in (1, 0):
+        c = fp._capi.Context(0)
+        try:
+            c.set_tuning(fp._capi.FP_TUNE_FP64_DMMA, dmma)
+            c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+            c.set_wake(w.shedding, D, D)
+            x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "fp64"))
+            xs.append(x)
+        finally:
+            c.close()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(xs[0] - xr) / np.linalg.norm(xr) < 1e-10
+    assert np.linalg.norm(xs[0] - xs[1]) / np.linalg.norm(xs[1]) < 1e-12
+
+
 def test_multi_rhs_sweep(fp, O, ctx):
     """Angle-of-attack sweep as many right-hand sides on one factorisation (fixed wake)."""
     w, body, normals, cps, D, U = _wing_setup(fp, 20, 24)
