@@ -490,6 +490,7 @@ def run_ours(args, rank, ws, dist):
     # FP64 pipe roofline of the assembly: ops pinned by the oracle's operation
     # counter (248 per quad-ring interaction, 290 per horseshoe) / device time
     peak64 = cap.measure_fma_peak(device, True)
+    peak_dmma = cap.measure_fma_peak(device, True, tensor=True)
     ops = 248.0 * N * N + 290.0 * 2 * w.nsheddings * N
     achieved = ops / (stg_d[0] * 1e-3) / 1e12
     d_launches, d_ms, d_flops, _ = ktime["fp64"]
@@ -556,10 +557,13 @@ def run_ours(args, rank, ws, dist):
                                   "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                                   "frac": achieved / peak64,
                                   "peak_source": "measured FP64 FMA throughput (fp_measure_fma_peak)"},
-            "fp64_trailing_update": {"kernel": "k_gemm_sub_dmma (FP64 tensor path, mma.sync .f64)",
+            "fp64_trailing_update": {"kernel": "k_gemm_sub_dmma<1024,4,2> (FP64 tensor path, mma.sync .f64)",
                                      "launches": d_launches, "ms_total": d_ms,
                                      "tflops": d_flops / (d_ms * 1e-3) / 1e12 if d_ms else 0,
-                                     "frac_of_fp64_fma_peak": (d_flops / (d_ms * 1e-3) / 1e12 / peak64) if d_ms else 0},
+                                     "frac_of_fp64_fma_peak": (d_flops / (d_ms * 1e-3) / 1e12 / peak64) if d_ms else 0,
+                                     "fp64_tensor_peak_tflops": peak_dmma,
+                                     "frac_of_fp64_tensor_peak": (d_flops / (d_ms * 1e-3) / 1e12 / peak_dmma)
+                                     if d_ms else 0},
             "mixed_factor_timeline": timeline,
             "cusolver_getrf": cusolver,
             "sphere_config1": sphere,

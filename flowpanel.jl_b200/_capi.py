@@ -407,10 +407,11 @@ class Context:
         return ms.value, n.value
 
 
-def measure_fma_peak(device=0, fp64=True):
-    """Sustained FMA throughput (TFLOP/s) of the FP64 or FP32 pipe."""
+def measure_fma_peak(device=0, fp64=True, tensor=False):
+    """Sustained FMA throughput (TFLOP/s) of the FP64 or FP32 pipe, or with
+    ``tensor`` of the FP64 tensor path (mma.sync m8n8k4 .f64)."""
     t = C.c_double()
-    rc = lib().fp_measure_fma_peak(int(device), 1 if fp64 else 0, C.byref(t))
+    rc = lib().fp_measure_fma_peak(int(device), 2 if tensor else (1 if fp64 else 0), C.byref(t))
     if rc:
         raise FlowPanelError(rc, "fp_measure_fma_peak failed")
     return t.value

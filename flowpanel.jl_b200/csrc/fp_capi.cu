@@ -781,7 +781,8 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       c->use_graph = value != 0;
       return FP_OK;
     case FP_TUNE_FP64_DMMA:
-      c->fp64_dmma = value != 0;
+      if (value < 0 || value > 3) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..3");
+      c->fp64_dmma = value;
       return FP_OK;
     case FP_TUNE_TC_SMEM:
       if (value < 0 || value > kTcSmemMax)

@@ -140,7 +140,7 @@ struct fp_ctx {
   int tc_stages = 2;            // ring depth of that update in the static-order LU (fp_set_tuning)
   int tc_tiles = 0;             // static-order LU: output tiles per CTA of the multi-tile update, 0 = one-tile kernel
   int tc_smem = 0;              // static-order LU: shared memory reserved by each one-tile update CTA (0 = its own)
-  bool fp64_dmma = true;        // FP64 LU: trailing update on the FP64 tensor path (mma.sync .f64) instead of SIMT
+  int fp64_dmma = 3;            // FP64 LU update: 0 SIMT; FP64 tensor path with 8 (1), 16 (2) or 32 (3) warps
   bool lu_overlap = true;       // static-order LU: trailing update on the second stream (fp_set_tuning)
   // The static-order FP32 factorisation replayed as a CUDA graph (both streams,
   // the diagonal-block inverses included): captured on the second call with

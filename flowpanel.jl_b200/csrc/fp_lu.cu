@@ -931,17 +931,18 @@ k_gemm_sub_f64(const double* __restrict__ Am, const double* __restrict__ Bm, dou
 }
 
 // The same FP64 update on the FP64 tensor path (mma.sync m8n8k4 .f64, the
-// DMMA instruction; tcgen05 has no FP64 kind): 128 x 128 CTA tiles, 8 warps
-// as 2 (rows) x 4 (columns) of 64 x 32 warp tiles, each 8 x 4 fragments of
-// 8 x 8 with the accumulators in registers; 16-deep K slices through a
-// 3-stage cp.async ring. Shared-memory pitches keep the fragment loads free
-// of bank conflicts: A slices [k][row] with 136-double rows (the 4 k rows a
-// fragment reads start 64 bytes apart in the bank space), B slices
-// [col][k] with 20-double rows (8 columns a fragment reads cover all banks).
+// DMMA instruction; tcgen05 has no FP64 kind): 128 x 128 CTA tiles, NT/32
+// warps, each a (8 MF) x (8 NF) warp tile of MF x NF fragments of 8 x 8 with
+// the accumulators in registers (256 threads: 2 x 4 warps of 64 x 32; 512
+// threads: 4 x 4 warps of 32 x 32); 16-deep K slices through a 3-stage
+// cp.async ring. Shared-memory pitches keep the fragment loads free of bank
+// conflicts: A slices [k][row] with 136-double rows (the 4 k rows a fragment
+// reads start 64 bytes apart in the bank space), B slices [col][k] with
+// 20-double rows (the 8 columns a fragment reads cover all banks).
 // Fragments (PTX ISA, mma m8n8k4 .f64): lane = 4 g + t; A(8x4, row) element
 // (g, t); B(4x8, col) element (t, g); C(8x8) elements (g, 2t) and (g, 2t+1).
 namespace dm {
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, NT = 256;
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3;
 constexpr int AP = BM + 8, BP = BK + 4;
 __host__ __device__ constexpr size_t stage_doubles() { return (size_t)BK * AP + (size_t)BN * BP; }
 constexpr size_t smem() { return STAGES * stage_doubles() * sizeof(double); }
@@ -953,18 +954,21 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(dm::NT, 1)
+template <int NT, int MF, int NF>
+__global__ void __launch_bounds__(NT, 1)
 k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, double* __restrict__ Cm, int64_t lda,
                 int64_t m, int64_t nn, int kk) {
   using namespace dm;
+  constexpr int WARPS_M = BM / (8 * MF);
+  static_assert(WARPS_M * (BN / (8 * NF)) * 32 == NT, "the warp tiles cover the CTA tile");
   extern __shared__ __align__(16) unsigned char gsm[];
   double* const ring = reinterpret_cast<double*>(gsm);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int wm = (warp & 1) * 64, wn = (warp >> 1) * 32;
+  const int wm = (warp % WARPS_M) * 8 * MF, wn = (warp / WARPS_M) * 8 * NF;
   const int64_t i0 = (int64_t)blockIdx.x * BM, j0 = (int64_t)blockIdx.y * BN;
   const int nk = (kk + BK - 1) / BK;
-  // one K slice into stage s: 1024 16-byte pieces of A and 1024 of B, 4 + 4 per thread
+  // one K slice into stage s: 1024 16-byte pieces of A and 1024 of B
   auto issue = [&](int kb, int s) {
     double* As = ring + (size_t)s * stage_doubles();
     double* Bs = As + BK * AP;
@@ -994,11 +998,11 @@ k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, do
     if (s < nk) issue(s, s);
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
-  double acc[8][4][2];
+  double acc[MF][NF][2];
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+  for (int a = 0; a < MF; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int b = 0; b < NF; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 #pragma unroll 1
   for (int kb = 0; kb < nk; ++kb) {
     asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");
@@ -1009,26 +1013,26 @@ k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, do
     const double* Bs = As + BK * AP;
 #pragma unroll
     for (int k4 = 0; k4 < BK; k4 += 4) {
-      double a[8], b[4];
+      double a[MF], b[NF];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi) a[mi] = As[(k4 + t) * AP + wm + mi * 8 + g];
+      for (int mi = 0; mi < MF; ++mi) a[mi] = As[(k4 + t) * AP + wm + mi * 8 + g];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) b[ni] = Bs[(wn + ni * 8 + g) * BP + k4 + t];
+      for (int ni = 0; ni < NF; ++ni) b[ni] = Bs[(wn + ni * 8 + g) * BP + k4 + t];
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi)
+      for (int mi = 0; mi < MF; ++mi)
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
+        for (int ni = 0; ni < NF; ++ni) dmma(acc[mi][ni][0], acc[mi][ni][1], a[mi], b[ni]);
     }
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
 #pragma unroll
-  for (int ni = 0; ni < 4; ++ni)
+  for (int ni = 0; ni < NF; ++ni)
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const int64_t gj = j0 + wn + ni * 8 + 2 * t + e;
       if (gj >= nn) continue;
 #pragma unroll
-      for (int mi = 0; mi < 8; ++mi) {
+      for (int mi = 0; mi < MF; ++mi) {
         const int64_t gi = i0 + wm + mi * 8 + g;
         if (gi < m) Cm[gj * lda + gi] -= acc[mi][ni][e];
       }
@@ -1051,11 +1055,20 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
     const int slot = kt_begin(c);
     TraceScope tr(c, TR_GEMM_SIMT);
     if (mis == 0 && c->fp64_dmma) {
-      static SmemAttr attr;
-      FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub_dmma, (int)dm::smem()));
+      static SmemAttr attr8, attr16, attr32;
+      FP_CUDA_TRY(c->err, attr8.ensure(k_gemm_sub_dmma<256, 8, 4>, (int)dm::smem()));
+      FP_CUDA_TRY(c->err, attr16.ensure(k_gemm_sub_dmma<512, 4, 4>, (int)dm::smem()));
+      FP_CUDA_TRY(c->err, attr32.ensure(k_gemm_sub_dmma<1024, 4, 2>, (int)dm::smem()));
       dim3 g((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + dm::BN - 1) / dm::BN));
-      k_gemm_sub_dmma<<<g, dm::NT, dm::smem(), c->stream>>>((const double*)Am, (const double*)Bm, (double*)Cm, lda, m,
-                                                            nn, kk);
+      if (c->fp64_dmma == 3)
+        k_gemm_sub_dmma<1024, 4, 2><<<g, 1024, dm::smem(), c->stream>>>((const double*)Am, (const double*)Bm,
+                                                                         (double*)Cm, lda, m, nn, kk);
+      else if (c->fp64_dmma == 2)
+        k_gemm_sub_dmma<512, 4, 4><<<g, 512, dm::smem(), c->stream>>>((const double*)Am, (const double*)Bm,
+                                                                       (double*)Cm, lda, m, nn, kk);
+      else
+        k_gemm_sub_dmma<256, 8, 4><<<g, 256, dm::smem(), c->stream>>>((const double*)Am, (const double*)Bm,
+                                                                       (double*)Cm, lda, m, nn, kk);
     } else if (mis == 0) {
       static SmemAttr attr;
       FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub_f64, (int)d64::smem()));

@@ -19,6 +19,27 @@ __global__ void __launch_bounds__(256) k_fma_peak(T* out, int iters, T a, T b) {
   if (s == T(-1.2345)) out[0] = s;   // keep the chain alive
 }
 
+// FP64 tensor path: 8 independent m8n8k4 .f64 MMAs per step and warp,
+// operands and accumulators in registers
+__global__ void __launch_bounds__(256) k_dmma_peak(double* out, int iters, double a, double b) {
+  double c[8][2];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) c[q][0] = c[q][1] = threadIdx.x + q;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(c[q][0]), "+d"(c[q][1])
+                     : "d"(a), "d"(b));
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) s += c[q][0] + c[q][1];
+  if (s == -1.2345) out[0] = s;   // keep the chain alive
+}
+
 }  // namespace fpb
 
 extern "C" int fp_measure_fma_peak(int device, int fp64, double* tflops) {
@@ -36,7 +57,8 @@ extern "C" int fp_measure_fma_peak(int device, int fp64, double* tflops) {
   float best = 1e30f;
   for (int rep = 0; rep < 4; ++rep) {
     cudaEventRecord(e0);
-    if (fp64) k_fma_peak<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+    if (fp64 == 2) k_dmma_peak<<<blocks, threads>>>((double*)out, iters / 4, 1e-3, 1e-3);
+    else if (fp64) k_fma_peak<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
     else k_fma_peak<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
@@ -48,7 +70,9 @@ extern "C" int fp_measure_fma_peak(int device, int fp64, double* tflops) {
   cudaEventDestroy(e1);
   cudaFree(out);
   if (cudaGetLastError() != cudaSuccess) return FP_ECUDA;
-  const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  // FMA: 8 x 16 per thread and iteration; MMA: 8 x 16 MMAs of 8 x 8 x 4 per warp and iteration
+  const double flops = fp64 == 2 ? 2.0 * 256 * 8 * 16 * (double)(iters / 4) * blocks * (threads / 32)
+                                 : 2.0 * 8 * 16 * (double)iters * blocks * threads;
   *tflops = flops / (best * 1e-3) / 1e12;
   return FP_OK;
 }

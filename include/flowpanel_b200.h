@@ -377,8 +377,9 @@ int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
 #define FP_STAGE_POST 6      /* fp_ugradmu / fp_surface_loads */
 
 /* Measurement utility (no counterpart in the reference): sustained FMA
- * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, in
- * TFLOP/s, the denominator of the compute-bound kernels' roofline. */
+ * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, or of
+ * its FP64 tensor path (fp64 = 2: mma.sync m8n8k4 .f64), in TFLOP/s, the
+ * denominator of the compute-bound kernels' roofline. */
 int fp_measure_fma_peak(int device, int fp64, double* tflops);
 
 /* Tuning knobs of a context (no counterpart in the reference; the defaults are
@@ -400,9 +401,10 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       tensor-core update reserves (0, the default: its ring
  *                       and barriers only; at most 232448): fewer update CTAs
  *                       an SM, more room for the panel kernels beside them
- *   FP_TUNE_FP64_DMMA   1 (default): the FP64 LU's trailing update runs on the FP64
- *                       tensor path (mma.sync .f64), 16.9 TF/s on the 12k wing;
- *                       0: the SIMT FP64 kernel, 15.0 TF/s (same results) */
+ *   FP_TUNE_FP64_DMMA   the FP64 LU's trailing update: 0 the SIMT FP64 kernel
+ *                       (15.0 TF/s on the 12k wing); 1, 2, 3 the FP64 tensor
+ *                       path (mma.sync .f64) with 8, 16 or 32 warps a CTA (17.0,
+ *                       19.2, 19.7 TF/s; 3 is the default); same results */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
