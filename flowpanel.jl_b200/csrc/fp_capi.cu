@@ -474,6 +474,7 @@ static int factor_static_graph(fp_ctx* c, bool bf16) {
   std::vector<uintptr_t> key = {(uintptr_t)c->N, (uintptr_t)c->ld, (uintptr_t)c->d_G32, (uintptr_t)c->d_ipiv,
                                 (uintptr_t)c->d_cert, (uintptr_t)c->d_status, (uintptr_t)c->d_minv,
                                 (uintptr_t)bf16, (uintptr_t)c->tc_stages, (uintptr_t)c->tc_tiles, (uintptr_t)c->tc_smem,
+                                (uintptr_t)c->tc_split, (uintptr_t)c->tc_red,
                                 (uintptr_t)c->lu_overlap, (uintptr_t)c->use_tc};
   for (int s = 0; s < 2; ++s)
     for (int i = 0; i < 4; ++i) key.push_back((uintptr_t)c->d_tc[s][i]);
@@ -783,6 +784,13 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
     case FP_TUNE_FP64_DMMA:
       if (value < 0 || value > 3) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..3");
       c->fp64_dmma = value;
+      return FP_OK;
+    case FP_TUNE_TC_RED:
+      c->tc_red = value != 0;
+      return FP_OK;
+    case FP_TUNE_TC_SPLIT:
+      if (value < 0 || value > 3) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_SPLIT is 0..3");
+      c->tc_split = value;
       return FP_OK;
     case FP_TUNE_TC_SMEM:
       if (value < 0 || value > kTcSmemMax)

@@ -140,6 +140,8 @@ struct fp_ctx {
   int tc_stages = 2;            // ring depth of that update in the static-order LU (fp_set_tuning)
   int tc_tiles = 0;             // static-order LU: output tiles per CTA of the multi-tile update, 0 = one-tile kernel
   int tc_smem = 0;              // static-order LU: shared memory reserved by each one-tile update CTA (0 = its own)
+  int tc_split = 0;             // static-order LU: 0 pre-split operands; 1..3 split in shared memory (3, 4, 6 x stages)
+  bool tc_red = true;           // static-order LU: the update's epilogue adds to C by red.global instead of TMA
   int fp64_dmma = 3;            // FP64 LU update: 0 SIMT; FP64 tensor path with 8 (1), 16 (2) or 32 (3) warps
   bool lu_overlap = true;       // static-order LU: trailing update on the second stream (fp_set_tuning)
   // The static-order FP32 factorisation replayed as a CUDA graph (both streams,
@@ -238,6 +240,10 @@ bool tc_gemm_sub_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_
 // with ldk floats per row (Ah, Al: m rows; Bh, Bl: nn columns); C column-major (ldc).
 bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const float* Bh, const float* Bl, int ldk,
                           float* C, int64_t ldc, int64_t m, int64_t nn, int kk);
+// C -= A B from unsplit FP32 K-major operands (Ax: m rows, Bx: nn columns,
+// ldk floats a row); the 3xTF32 split is done in shared memory
+bool tc_gemm_sub_xsplit(fp_ctx* c, const float* Ax, const float* Bx, int ldk, float* C, int64_t ldc, int64_t m,
+                        int64_t nn, int kk);
 // C -= A B on the SIMT pipe (FP32), all three blocks of one matrix (lda)
 int gemm_sub_simt_f32(fp_ctx* c, const float* A, const float* B, float* C, int64_t lda, int64_t m, int64_t nn,
                       int kk);

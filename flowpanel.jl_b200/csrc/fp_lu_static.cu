@@ -478,10 +478,12 @@ k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, cons
       __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(Ah) + o);
       d[0] = __floats2bfloat162_rn(v.x, v.y);
       d[1] = __floats2bfloat162_rn(v.z, v.w);
-    } else {
+    } else if (Al) {
       const float4 h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
       *reinterpret_cast<float4*>(&Ah[o]) = h;
       *reinterpret_cast<float4*>(&Al[o]) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+    } else {   // unsplit: the update splits in shared memory
+      *reinterpret_cast<float4*>(&Ah[o]) = v;
     }
     lmax = fmaxf(lmax, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
   }
@@ -587,12 +589,14 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
       __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(Bh) + o);
       d[0] = __floats2bfloat162_rn(v[0], v[1]);
       d[1] = __floats2bfloat162_rn(v[2], v[3]);
-    } else {
+    } else if (Bl) {
       float h[4], lo[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) { h[i] = tf32_rna(v[i]); lo[i] = v[i] - h[i]; }
       *reinterpret_cast<float4*>(&Bh[o]) = make_float4(h[0], h[1], h[2], h[3]);
       *reinterpret_cast<float4*>(&Bl[o]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    } else {   // unsplit: the update splits in shared memory
+      *reinterpret_cast<float4*>(&Bh[o]) = make_float4(v[0], v[1], v[2], v[3]);
     }
   }
 }
@@ -624,6 +628,9 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   FP_CUDA_TRY(c->err, attr_urb.ensure(k_u12<32, 2, true>, (int)CfgR::smem()));
   if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
   if (int rc = ensure_tc_scratch(c, 1, n)) return rc;
+  // the tensor-core update splits the operands in shared memory: L21 and U12
+  // are written unsplit (the FP32 form; the BF16 form has no lo part)
+  const bool xsplit = !bf16 && c->tc_split > 0 && c->use_tc;
   st::k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(ipiv, n);
   ++c->nlaunch;
   float* const dinv_base = reinterpret_cast<float*>(c->d_minv);
@@ -641,6 +648,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     if (bf16) {
       const __nv_bfloat16* bh = reinterpret_cast<const __nv_bfloat16*>(s[2]) + boff * PW;
       if (c->use_tc && tc_gemm_sub_bf16(c, s[0], bh, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
+    } else if (xsplit) {
+      if (c->use_tc && tc_gemm_sub_xsplit(c, s[0], s[2] + boff * PW, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
     } else if (c->use_tc && tc_gemm_sub_presplit(c, s[0], s[1], s[2] + boff * PW, s[3] + boff * PW, PW, at(kend, cb),
                                                  lda, m, nn, kk)) {
       return FP_OK;
@@ -664,7 +673,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       TraceScope tr(c, TR_L21);
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
       if (bf16) k_l21<true><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
-      else k_l21<false><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+      else k_l21<false><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], xsplit ? nullptr : s[1], cert);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
@@ -678,7 +687,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         if (bf16)
           k_u12<8, 1, true><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else
-          k_u12<8, 1, false><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+          k_u12<8, 1, false><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
+                                                                              xsplit ? nullptr : s[3]);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
@@ -697,8 +707,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           if (bf16)
             k_u12<32, 2, true><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh, nullptr);
           else
-            k_u12<32, 2, false><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh,
-                                                                            s[3] + (knext - kend) * PW);
+            k_u12<32, 2, false><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(
+                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
           ++c->nlaunch;
           FP_CUDA_TRY(c->err, cudaGetLastError());
         }

@@ -118,11 +118,24 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
                : "memory");
 }
 
-template <int STAGES>
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  return __uint_as_float(h);
+}
+
+// RED: the epilogue adds -D to C with red.global.add.f32 straight from the
+// registers (lane = row, 128-byte coalesced per column; Cp / ldc address C)
+// instead of staging it for a TMA reduce-add.
+template <int STAGES, bool RED = false>
 __global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
-              const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status) {
+              const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status,
+              float* __restrict__ Cp = nullptr, int64_t ldc = 0) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -196,7 +209,207 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
   // epilogue: every warp waits for the accumulator, stages -D for its 32 rows
   // column by column ([column][row], 32 rows = 128 B per column) in the ring,
   // whose operands the MMAs have all consumed, and adds it to C with TMA
-  const bool ok = mbar_wait(done, 0);
+  // warp-uniform: the epilogue's tcgen05.ld is a .sync.aligned warp instruction
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok && RED) {
+    const int64_t row = (int64_t)m0 + warp * 32 + lane;
+    float* cp = Cp + (int64_t)n0 * ldc + row;
+#pragma unroll 1
+    for (int cc = 0; cc < BN; cc += 8) {
+      uint32_t r[8];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                   : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                   : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < m) {
+        const int nc = n - (n0 + cc);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (j < nc) asm volatile("red.global.add.f32 [%0], %1;" ::"l"(cp), "f"(-__uint_as_float(r[j])) : "memory");
+          cp += ldc;
+        }
+      } else {
+        cp += 8 * ldc;
+      }
+    }
+  } else if (ok) {
+    float* stg = reinterpret_cast<float*>(smem) + warp * 32 * BN;
+#pragma unroll 1
+    for (int cc = 0; cc < BN; cc += 32) {
+      uint32_t r[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stg[(cc + j) * 32 + lane] = -__uint_as_float(r[j]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0 && m0 + warp * 32 < m) {
+      tma_reduce_add_2d(&tmC, stg, m0 + warp * 32, n0);
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      // the CTA may leave once the copy has read the staging buffer; its adds complete in L2
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
+  } else if (threadIdx.x == 0) {
+    atomicOr(status, (int)DEV_TIMEOUT);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// The same one-tile update from unsplit FP32 operands (K-major x copies of
+// the L21 panel and of the U12 rows): the split into hi = rna_tf32(x) and
+// lo = x - hi is done in shared memory, so a K block moves 16 KB by TMA
+// instead of 32 KB and more K blocks are in flight for the same shared
+// memory (XS stages of x, LB buffers of lo). 4 warps:
+//   warp 0 / lane 0   TMA producer: x of A and B into stage kb % XS;
+//   warps 2..3        converters: wait for the stage, write hi over x and lo
+//                     into buffer kb % LB (once the MMAs that read its last
+//                     contents are done), make the writes visible to the
+//                     tensor core (fence.proxy.async), one arrival;
+//   warp 1 / lane 0   MMA issuer: 3 x 2 tcgen05.mma (K = 8) per K block into
+//                     the 128-column TMEM accumulator; one commit frees the x
+//                     stage, one the lo buffer;
+//   all four warps    epilogue as k_tc_gemm_sub (the drained stages and lo
+//                     buffers, at least 64 KB, hold the staging).
+// Bounded waits as k_tc_gemm_sub.
+namespace xs {
+constexpr int XBYTES = TILE_A + TILE_B;   // one K block of x (A then B)
+constexpr int CT = 64;                    // converter threads
+template <int XS, int LB> constexpr int smem_bytes() { return (XS + LB) * XBYTES + 1024 + 256; }
+}  // namespace xs
+
+template <int XS, int LB>
+__global__ void __launch_bounds__(THREADS)
+k_tc_gemm_sub_xs(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                 const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status) {
+  using namespace xs;
+  static_assert((XS + LB) * XBYTES >= 4 * 32 * BN * 4, "the drained stages hold the epilogue's staging");
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint8_t* lo_base = smem + XS * XBYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + (XS + LB) * XBYTES);
+  uint64_t* xempty = full + XS;
+  uint64_t* cvt = xempty + XS;
+  uint64_t* loempty = cvt + LB;
+  uint64_t* done = loempty + LB;
+  uint64_t* drain = done + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  volatile int* cvt_fail = abort_flag + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int nk = (K + BK - 1) / BK;
+
+  if (threadIdx.x == 0) {
+    *cvt_fail = 0;
+    for (int q = 0; q < XS; ++q) { mbar_init(&full[q], 1); mbar_init(&xempty[q], 1); }
+    for (int q = 0; q < LB; ++q) { mbar_init(&cvt[q], 1); mbar_init(&loempty[q], 1); }
+    mbar_init(done, 1);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {   // producer
+      int issued = 0;
+      for (int kb = 0; kb < nk; ++kb) {
+        const int st = kb % XS;
+        if (kb >= XS && !mbar_wait(&xempty[st], ((kb / XS) - 1) & 1)) { *abort_flag = 1; break; }
+        if (*(volatile int*)abort_flag) break;
+        mbar_expect_tx(&full[st], XBYTES);
+        uint8_t* base = smem + st * XBYTES;
+        tma_load_2d(base, &tmA, kb * BK, m0, &full[st]);
+        tma_load_2d(base + TILE_A, &tmB, kb * BK, n0, &full[st]);
+        issued = kb + 1;
+      }
+      if (*(volatile int*)abort_flag)   // drain the copies this CTA issued before leaving
+        for (int kb = (issued > XS ? issued - XS : 0); kb < issued; ++kb) mbar_wait(&full[kb % XS], (kb / XS) & 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {   // MMA issuer
+      int issued = 0;
+      bool ok = true;
+      for (int kb = 0; kb < nk; ++kb) {
+        const int st = kb % XS, b = kb % LB;
+        if (!mbar_wait(&cvt[b], (kb / LB) & 1)) { ok = false; *abort_flag = 1; break; }
+        if (*(volatile int*)abort_flag) { ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t xb = smem_u32(smem + st * XBYTES), lb = smem_u32(lo_base + b * XBYTES);
+        const uint64_t dAh = sdesc(xb), dBh = sdesc(xb + TILE_A);
+        const uint64_t dAl = sdesc(lb), dBl = sdesc(lb + TILE_A);
+#pragma unroll
+        for (int kk = 0; kk < BK / 8; ++kk) {
+          const uint64_t off = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+          umma_tf32(tmem, dAh + off, dBl + off, (kb | kk) != 0 ? 1u : 0u);
+          umma_tf32(tmem, dAl + off, dBh + off, 1u);
+          umma_tf32(tmem, dAh + off, dBh + off, 1u);
+        }
+        umma_commit(&xempty[st]);
+        umma_commit(&loempty[b]);
+        issued = kb + 1;
+      }
+      if (ok) umma_commit(done);
+      else if (issued > 0) {   // MMAs still in flight must finish before TMEM is freed
+        umma_commit(drain);
+        mbar_wait(drain, 0);
+      }
+    }
+  } else {   // converters
+    // every converter thread reaches both named barriers of every K block:
+    // failures are written before the first, read between the two, so the
+    // 64 threads leave the loop together
+    const int ct = threadIdx.x - 64;
+    for (int kb = 0; kb < nk; ++kb) {
+      const int st = kb % XS, b = kb % LB;
+      bool ok = mbar_wait(&full[st], (kb / XS) & 1);
+      if (ok && kb >= LB) ok = mbar_wait(&loempty[b], ((kb / LB) - 1) & 1);
+      if (!ok) { *cvt_fail = 1; *(volatile int*)abort_flag = 1; }
+      asm volatile("bar.sync 1, %0;" ::"n"(CT) : "memory");
+      const int stop = *cvt_fail;
+      asm volatile("bar.sync 1, %0;" ::"n"(CT) : "memory");
+      if (stop) break;
+      float4* x = reinterpret_cast<float4*>(smem + st * XBYTES);
+      float4* lo = reinterpret_cast<float4*>(lo_base + b * XBYTES);
+#pragma unroll 4
+      for (int q = ct; q < XBYTES / 16; q += CT) {
+        const float4 v = x[q];
+        const float4 h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
+        x[q] = h;
+        lo[q] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync 1, %0;" ::"n"(CT) : "memory");
+      if (ct == 0) mbar_arrive(&cvt[b]);
+    }
+  }
+  __syncwarp();
+  // warp-uniform: the epilogue's tcgen05.ld is a .sync.aligned warp instruction
+  const bool ok = __all_sync(0xffffffffu, !*(volatile int*)abort_flag && mbar_wait(done, 0));
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
     float* stg = reinterpret_cast<float*>(smem) + warp * 32 * BN;
@@ -221,7 +434,6 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
     if (lane == 0 && m0 + warp * 32 < m) {
       tma_reduce_add_2d(&tmC, stg, m0 + warp * 32, n0);
       asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-      // the CTA may leave once the copy has read the staging buffer; its adds complete in L2
       asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
     }
   } else if (threadIdx.x == 0) {
@@ -277,16 +489,13 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
       : "memory");
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
-template <bool BF16>
+template <bool BF16, bool RED = false>
 __global__ void __launch_bounds__(mt::THREADS, 1)
 k_tc_gemm_multi(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
                 const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
                 const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int tiles_per_cta,
-                int* __restrict__ status) {
+                int* __restrict__ status, float* __restrict__ Cp = nullptr, int64_t ldc = 0) {
   using namespace mt;
   constexpr int SB = stage_bytes<BF16>(), KB = kblock<BF16>();
   extern __shared__ uint8_t smem_raw[];
@@ -407,8 +616,37 @@ k_tc_gemm_multi(const __grid_constant__ CUtensorMap tmAh, const __grid_constant_
       const int b = u & 1;
       int m0, n0;
       tile_mn(t, m0, n0);
-      if (!mbar_wait(&accf[b], (u >> 1) & 1)) { ok = false; break; }
+      // warp-uniform: tcgen05.ld is a .sync.aligned warp instruction
+      if (!__all_sync(0xffffffffu, mbar_wait(&accf[b], (u >> 1) & 1))) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (RED) {   // -D added to C with red.global straight from the registers (lane = row)
+        const int64_t row = (int64_t)m0 + q * 32 + lane;
+        float* cp = Cp + (int64_t)n0 * ldc + row;
+#pragma unroll 1
+        for (int cc = 0; cc < BN; cc += 8) {
+          uint32_t r[8];
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + cc);
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                         "=r"(r[7])
+                       : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (row < m) {
+            const int nc = n - (n0 + cc);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              if (j < nc) asm volatile("red.global.add.f32 [%0], %1;" ::"l"(cp), "f"(-__uint_as_float(r[j])) : "memory");
+              cp += ldc;
+            }
+          } else {
+            cp += 8 * ldc;
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acce[b]);
+        continue;
+      }
 #pragma unroll 1
       for (int cc = 0; cc < BN; cc += 32) {
         uint32_t r[32];
@@ -453,11 +691,6 @@ k_tc_gemm_multi(const __grid_constant__ CUtensorMap tmAh, const __grid_constant_
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(mt::TMEM_COLS) : "memory");
 }
 
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-  return __uint_as_float(h);
-}
 
 // L21 panel (m x K, column-major, lda) -> K-major copies Ah, Al (m x ldk, row-major).
 __global__ void k_split_A(const float* __restrict__ A, int64_t lda, int m, int K, int ldk,
@@ -608,9 +841,11 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
         reinterpret_cast<uintptr_t>(Al) | reinterpret_cast<uintptr_t>(Bh) | reinterpret_cast<uintptr_t>(Bl)) &
        15) != 0)
     return false;
-  static SmemAttr attr2, attr3, attrm;
+  static SmemAttr attr2, attr3, attrm, attr2r, attrmr;
+  if (attrmr.ensure(tc::k_tc_gemm_multi<false, true>, tc::mt::smem<false>()) != cudaSuccess) return false;
   if (attr2.ensure(tc::k_tc_gemm_sub<2>, kTcSmemMax) != cudaSuccess) return false;
   if (attr3.ensure(tc::k_tc_gemm_sub<3>, kTcSmemMax) != cudaSuccess) return false;
+  if (attr2r.ensure(tc::k_tc_gemm_sub<2, true>, kTcSmemMax) != cudaSuccess) return false;
   if (attrm.ensure(tc::k_tc_gemm_multi<false>, tc::mt::smem<false>()) != cudaSuccess) return false;
   const bool multi = c->tc_tiles > 0;
   CUtensorMap mAh, mAl, mBh, mBl, mC;
@@ -624,14 +859,56 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
   if (multi) {
     const int tiles = (int)(grid.x * grid.y);
     const unsigned ctas = (unsigned)((tiles + c->tc_tiles - 1) / c->tc_tiles);
-    tc::k_tc_gemm_multi<false><<<ctas, tc::mt::THREADS, tc::mt::smem<false>(), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->tc_tiles, c->d_status);
-  } else if (c->tc_stages == 2)
+    if (c->tc_red)
+      tc::k_tc_gemm_multi<false, true><<<ctas, tc::mt::THREADS, tc::mt::smem<false>(), c->stream>>>(
+          mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->tc_tiles, c->d_status, C, ldc);
+    else
+      tc::k_tc_gemm_multi<false><<<ctas, tc::mt::THREADS, tc::mt::smem<false>(), c->stream>>>(
+          mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->tc_tiles, c->d_status);
+  } else if (c->tc_red)
+    tc::k_tc_gemm_sub<2, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+  else if (c->tc_stages == 2)
     tc::k_tc_gemm_sub<2><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
         mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status);
   else
     tc::k_tc_gemm_sub<3><<<grid, tc::THREADS, std::max(tc::smem_bytes<3>(), c->tc_smem), c->stream>>>(
         mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status);
+  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
+  ++c->nlaunch;
+  return cudaGetLastError() == cudaSuccess;
+}
+
+// C -= A B from unsplit FP32 operands (K-major, ldk floats a row), the split
+// done in shared memory by k_tc_gemm_sub_xs (x stages by c->tc_split: 1 -> 3,
+// 2 -> 4, 3 -> 6; one lo buffer).
+bool tc_gemm_sub_xsplit(fp_ctx* c, const float* Ax, const float* Bx, int ldk, float* C, int64_t ldc, int64_t m,
+                        int64_t nn, int kk) {
+  if (kk <= 0 || kk > ldk || m <= 0 || nn <= 0 || (ldk & 3) != 0) return false;
+  if (!tc::encode_fn()) return false;
+  if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(ldc * 4) | reinterpret_cast<uintptr_t>(Ax) |
+        reinterpret_cast<uintptr_t>(Bx)) & 15) != 0)
+    return false;
+  static SmemAttr a3, a4, a6;
+  if (a3.ensure(tc::k_tc_gemm_sub_xs<3, 1>, kTcSmemMax) != cudaSuccess) return false;
+  if (a4.ensure(tc::k_tc_gemm_sub_xs<4, 1>, kTcSmemMax) != cudaSuccess) return false;
+  if (a6.ensure(tc::k_tc_gemm_sub_xs<6, 1>, kTcSmemMax) != cudaSuccess) return false;
+  CUtensorMap mA, mB, mC;
+  if (!tc::make_map(&mA, Ax, kk, m, ldk, tc::BM) || !tc::make_map(&mB, Bx, kk, nn, ldk, tc::BN) ||
+      !tc::make_map_c(&mC, C, m, nn, ldc, tc::BN))
+    return false;
+  dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
+  const int ev = kt_begin(c);
+  TraceScope tr(c, TR_GEMM_TC);
+  if (c->tc_split >= 3)
+    tc::k_tc_gemm_sub_xs<6, 1><<<grid, tc::THREADS, std::max(tc::xs::smem_bytes<6, 1>(), c->tc_smem), c->stream>>>(
+        mA, mB, mC, (int)m, (int)nn, kk, c->d_status);
+  else if (c->tc_split == 2)
+    tc::k_tc_gemm_sub_xs<4, 1><<<grid, tc::THREADS, std::max(tc::xs::smem_bytes<4, 1>(), c->tc_smem), c->stream>>>(
+        mA, mB, mC, (int)m, (int)nn, kk, c->d_status);
+  else
+    tc::k_tc_gemm_sub_xs<3, 1><<<grid, tc::THREADS, std::max(tc::xs::smem_bytes<3, 1>(), c->tc_smem), c->stream>>>(
+        mA, mB, mC, (int)m, (int)nn, kk, c->d_status);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;

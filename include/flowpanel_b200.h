@@ -404,13 +404,24 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *   FP_TUNE_FP64_DMMA   the FP64 LU's trailing update: 0 the SIMT FP64 kernel
  *                       (15.0 TF/s on the 12k wing); 1, 2, 3 the FP64 tensor
  *                       path (mma.sync .f64) with 8, 16 or 32 warps a CTA (17.0,
- *                       19.2, 19.7 TF/s; 3 is the default); same results */
+ *                       19.2, 19.7 TF/s; 3 is the default); same results
+ *   FP_TUNE_TC_SPLIT    the static-order LU's tensor-core update: 0 reads
+ *                       operands split into TF32 hi / lo by the panel kernels
+ *                       (32 KB a K block); 1, 2, 3: reads the unsplit FP32
+ *                       operands (16 KB a K block) and splits them in shared
+ *                       memory, with 3, 4 or 6 K blocks in flight a CTA
+ *   FP_TUNE_TC_RED      1 (default): that update's epilogue adds to C with
+ *                       red.global from the registers (factorisation 14.6 ms on
+ *                       the 12k wing); 0: stages -D in shared memory for a TMA
+ *                       reduce-add (15.1 ms) */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
 #define FP_TUNE_GRAPH 3
 #define FP_TUNE_TC_SMEM 4
 #define FP_TUNE_FP64_DMMA 5
+#define FP_TUNE_TC_SPLIT 6
+#define FP_TUNE_TC_RED 7
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels

@@ -44,6 +44,40 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
 
 
+@pytest.mark.parametrize("nc,ns", [(8, 4), (12, 8), (20, 24), (40, 48), (60, 80), (50, 30)])
+@pytest.mark.parametrize("knob,value", [("FP_TUNE_TC_SPLIT", 1), ("FP_TUNE_TC_SPLIT", 2), ("FP_TUNE_TC_SPLIT", 3),
+                                        ("FP_TUNE_TC_RED", 0), ("FP_TUNE_TC_TILES", 2), ("FP_TUNE_TC_TILES", 4)])
+def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
+    """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
+    1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
+    shared memory; FP_TUNE_TC_RED 0 adds the product to C by a TMA
+    reduce-add instead of red.global; FP_TUNE_TC_TILES runs the multi-tile
+    kernel (double-buffered accumulator, red.global epilogue). The factors are as accurate as the default's (refinement
+    in a handful of steps, the oracle's solution to 1e-10), for one partial
+    panel up to many panels with a partial last one (1,500 panels: a last K
+    block of 92)."""
+    w = fp.meshes.swept_wing("0012", nc, ns)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(4.2)
+    V = np.array([np.cos(a), 0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    c = fp._capi.Context(0)
+    try:
+        c.set_tuning(getattr(fp._capi, knob), value)
+        c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+        c.set_wake(w.shedding, D, D)
+        x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
+    finally:
+        c.close()
+    assert st.used_gmres == 0 and st.ir_iters <= 5, st.asdict()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+
+
 @pytest.mark.parametrize("nc,ns", [(20, 24), (60, 80)])
 def test_bf16_form_reaches_fp64_solution(fp, O, ctx, nc, ns):
     """FP_PREC_BF16: the factorisation starts from the BF16-rounded AIC and its
