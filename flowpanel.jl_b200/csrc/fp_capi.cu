@@ -104,6 +104,8 @@ int time_end(fp_ctx* c, double* ms) {
 }
 
 void free_matrices(fp_ctx* c) {
+  if (c->stream_bg) cudaStreamSynchronize(c->stream_bg);   // a background pass may still write G
+  c->g64_pending = false;
   dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
   dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_mbox); dfree(c->d_part);
   dfree(c->d_dinv128_64); dfree(c->d_dinv128_32); dfree(c->d_mprev64); dfree(c->d_mprev32);
@@ -153,6 +155,9 @@ int fp_ctx_create(int device, fp_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream_bg, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_g64, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_asm, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_panel, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_rest, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
@@ -171,6 +176,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
+  if (c->stream_bg) cudaStreamSynchronize(c->stream_bg);
   free_matrices(c);
   post_free(c);
   dfree(c->d_panels); dfree(c->d_src); dfree(c->d_tgt); dfree(c->d_wake);
@@ -181,6 +187,9 @@ int fp_ctx_destroy(fp_ctx* c) {
   for (cudaEvent_t e : c->trace.pool) cudaEventDestroy(e);
   if (c->ev_panel) cudaEventDestroy(c->ev_panel);
   if (c->ev_rest) cudaEventDestroy(c->ev_rest);
+  if (c->ev_g64) cudaEventDestroy(c->ev_g64);
+  if (c->ev_asm) cudaEventDestroy(c->ev_asm);
+  if (c->stream_bg) cudaStreamDestroy(c->stream_bg);
   if (c->stream2) cudaStreamDestroy(c->stream2);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -196,6 +205,11 @@ int fp_set_geometry(fp_ctx* c, const double* nodes, int64_t nnodes, const int32_
   cudaSetDevice(c->device);
   if (!nodes || !offsets || !pnodes || nnodes <= 0 || npanels <= 0)
     return c->err.set(FP_EINVAL, "fp_set_geometry: empty mesh or null pointer");
+  // a background assembly pass may still read the panels it may free
+  if (c->g64_pending) {
+    FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream_bg));
+    c->g64_pending = false;
+  }
   if (offsets[0] != 0) return c->err.set(FP_EINVAL, "fp_set_geometry: panel_offsets[0] must be 0");
   for (int64_t p = 0; p < npanels; ++p) {
     const int nn = offsets[p + 1] - offsets[p];
@@ -311,6 +325,11 @@ int fp_set_wake(fp_ctx* c, const int32_t* shedding, int64_t nsh, const double* D
   if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_set_wake: call fp_set_geometry first");
   if (nsh < 0 || (nsh > 0 && (!shedding || !Das || !Dbs)))
     return c->err.set(FP_EINVAL, "fp_set_wake: bad arguments");
+  // a background assembly pass may still read the wake records it may free
+  if (c->g64_pending) {
+    FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream_bg));
+    c->g64_pending = false;
+  }
   const double tol = 2 * 2.220446049250313e-16;
   std::vector<WakeRec> w(nsh);
   std::vector<int> touched(c->N, 0);
@@ -378,6 +397,8 @@ int fp_assemble(fp_ctx* c, int element, double kerneloffset, double kernelcutoff
   if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_MIXED_GEPP &&
       precision != FP_PREC_BF16)
     return c->err.set(FP_EINVAL, "fp_assemble: unknown precision");
+  // the previous assembly's background pass must be done before G is written again
+  if (int rc = sync_g64(c)) return rc;
   const size_t elems = (size_t)c->ld * c->capN;   // for the largest body the buffers hold
   if (!c->d_G) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_G, elems * sizeof(double)));
@@ -392,9 +413,21 @@ int fp_assemble(fp_ctx* c, int element, double kerneloffset, double kernelcutoff
   c->kern_offset = kerneloffset;
   c->kern_cutoff = kernelcutoff;
   if (time_begin(c)) return FP_ECUDA;
-  int rc = element == FP_ELEMENT_VORTEXRING ? launch_assemble_ring(c, kerneloffset, kernelcutoff, w32)
-                                            : launch_assemble_source(c, kerneloffset, w32);
-  if (rc) return rc;
+  int rc;
+  if (element == FP_ELEMENT_VORTEXRING && w32 && c->asm32) {
+    // the FP32 AIC on the critical path; the FP64 AIC (read only by the
+    // refinement residuals) on the background stream under the factorisation
+    if ((rc = launch_assemble_ring32(c, kerneloffset, kernelcutoff))) return rc;
+    FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_asm, c->stream));
+    FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream_bg, c->ev_asm, 0));
+    if ((rc = launch_assemble_ring(c, kerneloffset, kernelcutoff, false, c->stream_bg))) return rc;
+    FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_g64, c->stream_bg));
+    c->g64_pending = true;
+  } else {
+    rc = element == FP_ELEMENT_VORTEXRING ? launch_assemble_ring(c, kerneloffset, kernelcutoff, w32)
+                                          : launch_assemble_source(c, kerneloffset, w32);
+    if (rc) return rc;
+  }
   if (time_end(c, &c->ms_assemble)) return FP_ECUDA;
   c->kms[FP_STAGE_ASSEMBLE] = c->ms_assemble;
   c->klaunch[FP_STAGE_ASSEMBLE] = (element == FP_ELEMENT_VORTEXRING && c->nsh > 0) ? 2 : 1;
@@ -408,6 +441,7 @@ int fp_get_aic(fp_ctx* c, double* G) {
   if (check_ctx(c)) return FP_EINVAL;
   cudaSetDevice(c->device);
   if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_get_aic: nothing assembled");
+  if (int rc = sync_g64(c)) return rc;
   FP_CUDA_TRY(c->err, cudaMemcpy2DAsync(G, c->N * sizeof(double), c->d_G, c->ld * sizeof(double),
                                         c->N * sizeof(double), c->N, cudaMemcpyDeviceToHost, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
@@ -521,6 +555,10 @@ int fp_factor(fp_ctx* c, int precision) {
       precision != FP_PREC_BF16)
     return c->err.set(FP_EINVAL, "fp_factor: unknown precision");
   if (int rc = alloc_factor_buffers(c, precision)) return rc;
+  // every factorisation but the FP32 ones of an FP32-assembled AIC reads G
+  if (precision == FP_PREC_FP64 || precision == FP_PREC_BF16 ||
+      (c->assembled_prec != FP_PREC_MIXED && c->assembled_prec != FP_PREC_MIXED_GEPP))
+    if (int rc = sync_g64(c)) return rc;
   if (time_begin(c)) return FP_ECUDA;
   int rc;
   double ms_static = 0;
@@ -550,6 +588,7 @@ int fp_factor(fp_ctx* c, int precision) {
       if (st & DEV_ZERO_PIVOT) {
         FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream));
         if (time_begin(c)) return FP_ECUDA;
+        if ((rc = sync_g64(c))) return rc;
         if ((rc = convert_f64_f32(c, c->d_G, c->d_G32, c->N, c->N, c->ld, c->ld))) return rc;
         pivoted = true;
       } else {
@@ -705,6 +744,7 @@ int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stat
   c->last.used_gmres = 0;
   int rc;
   if (time_begin(c)) return FP_ECUDA;
+  if ((rc = sync_g64(c))) return rc;   // the residuals read the FP64 AIC
   if (o.solver == FP_SOLVER_GMRES) {
     int it = 0;
     double rr = 0;
@@ -784,6 +824,9 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
     case FP_TUNE_FP64_DMMA:
       if (value < 0 || value > 3) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..3");
       c->fp64_dmma = value;
+      return FP_OK;
+    case FP_TUNE_ASM32:
+      c->asm32 = value != 0;
       return FP_OK;
     case FP_TUNE_TC_RED:
       c->tc_red = value != 0;
@@ -876,6 +919,7 @@ int fp_solve_ls(fp_ctx* c, double kerneloffset, double kernelcutoff, const doubl
   if (check_ctx(c)) return FP_EINVAL;
   cudaSetDevice(c->device);
   if (!c->has_geometry) return c->err.set(FP_ESTATE, "fp_solve_ls: no geometry");
+  if (int rc = sync_g64(c)) return rc;
   if (!Uinfs || !x || npres < 0 || npres >= c->N || (npres > 0 && (!el_index || !el_value)))
     return c->err.set(FP_EINVAL, "fp_solve_ls: bad arguments");
   // prescribed elements sorted by index (src/FLOWPanel_liftingbody.jl:399)
@@ -1028,6 +1072,7 @@ int fp_adjoint_solve(fp_ctx* c, const double* ybar, int64_t k, double* lambda) {
   if (c->factored < 0) return c->err.set(FP_ESTATE, "fp_adjoint_solve: no factors (call fp_factor)");
   const int64_t n = c->N, ld = c->ld;
   int rc;
+  if ((rc = sync_g64(c))) return rc;   // the adjoint's residuals read the FP64 AIC
   if ((rc = ensure_adjoint(c, k))) return rc;
   FP_CUDA_TRY(c->err, cudaMemcpy2DAsync(c->d_ab, ld * sizeof(double), ybar, n * sizeof(double), n * sizeof(double), k,
                                         cudaMemcpyHostToDevice, c->stream));

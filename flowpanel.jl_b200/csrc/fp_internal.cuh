@@ -157,6 +157,11 @@ struct fp_ctx {
   size_t tc_cap[2] = {0, 0};
   int tc_slot = 0;                      // scratch set of the current launches
   cudaStream_t stream2 = nullptr;       // second stream of the look-ahead factorisation
+  cudaStream_t stream_bg = nullptr;     // lowest priority: the FP64 AIC pass under the FP32 factorisation
+  cudaEvent_t ev_g64 = nullptr;         // that pass done (stream_bg -> stream)
+  cudaEvent_t ev_asm = nullptr;         // assembly inputs ready (stream -> stream_bg)
+  bool g64_pending = false;             // the FP64 AIC is still being written on stream_bg
+  bool asm32 = false;                   // mixed forms: FP32 AIC pass first, FP64 pass in the background
   cudaEvent_t ev_panel = nullptr;       // panel factored (stream -> stream2)
   cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)
 
@@ -190,7 +195,9 @@ struct fp_ctx {
 namespace fpb {
 
 // assembly (fp_assembly.cu)
-int launch_assemble_ring(fp_ctx* c, double offset, double cutoff, bool write32);
+int launch_assemble_ring(fp_ctx* c, double offset, double cutoff, bool write32, cudaStream_t s = nullptr);
+// the FP32 AIC (G32) alone, the ring in panel-local FP32 coordinates
+int launch_assemble_ring32(fp_ctx* c, double offset, double cutoff);
 int launch_assemble_source(fp_ctx* c, double offset, bool write32);
 int launch_rhs(fp_ctx* c, const double* d_U, int64_t k);
 
@@ -278,6 +285,10 @@ int num_sms();
 // Raises a kernel's dynamic shared-memory limit once per device. Thread-safe:
 // a repeated call from a racing thread only sets the same value again.
 constexpr int kTcSmemMax = 232448;   // the opt-in shared memory of one CTA on sm_100
+
+// Orders the context's stream after the background FP64 assembly pass, once;
+// every reader of the FP64 AIC (or writer of a new one) calls it first.
+inline int sync_g64(fp_ctx* c);
 
 struct SmemAttr {
   std::atomic<unsigned long long> done{0};
@@ -385,4 +396,11 @@ inline void tr_collect(fp_ctx* c) {
   t.used = 0;
   t.base = -1;
 }
+inline int sync_g64(fp_ctx* c) {
+  if (!c->g64_pending) return FP_OK;
+  c->g64_pending = false;
+  FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_g64, 0));
+  return FP_OK;
+}
+
 }  // namespace fpb

@@ -413,7 +413,14 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *   FP_TUNE_TC_RED      1 (default): that update's epilogue adds to C with
  *                       red.global from the registers (factorisation 14.6 ms on
  *                       the 12k wing); 0: stages -D in shared memory for a TMA
- *                       reduce-add (15.1 ms) */
+ *                       reduce-add (15.1 ms)
+ *   FP_TUNE_ASM32       1: fp_assemble for the FP32 factorisations writes the
+ *                       FP32 AIC in panel-local FP32 coordinates on the
+ *                       critical path (1.53 ms on the 12k wing) and the FP64
+ *                       AIC (read only by the refinement) on a background
+ *                       stream under the factorisation, which that pass slows
+ *                       by 2.2 ms; 0 (default): one FP64 pass writes both
+ *                       (2.49 ms) */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -422,6 +429,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_FP64_DMMA 5
 #define FP_TUNE_TC_SPLIT 6
 #define FP_TUNE_TC_RED 7
+#define FP_TUNE_ASM32 8
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels
