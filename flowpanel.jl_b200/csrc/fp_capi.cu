@@ -157,6 +157,7 @@ int fp_ctx_create(int device, fp_ctx** out) {
       cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream_bg, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_g64, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_diag, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_asm, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_panel, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_rest, cudaEventDisableTiming) != cudaSuccess ||
@@ -188,6 +189,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->ev_panel) cudaEventDestroy(c->ev_panel);
   if (c->ev_rest) cudaEventDestroy(c->ev_rest);
   if (c->ev_g64) cudaEventDestroy(c->ev_g64);
+  if (c->ev_diag) cudaEventDestroy(c->ev_diag);
   if (c->ev_asm) cudaEventDestroy(c->ev_asm);
   if (c->stream_bg) cudaStreamDestroy(c->stream_bg);
   if (c->stream2) cudaStreamDestroy(c->stream2);

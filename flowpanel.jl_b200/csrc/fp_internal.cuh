@@ -163,6 +163,7 @@ struct fp_ctx {
   bool g64_pending = false;             // the FP64 AIC is still being written on stream_bg
   bool asm32 = false;                   // mixed forms: FP32 AIC pass first, FP64 pass in the background
   cudaEvent_t ev_panel = nullptr;       // panel factored (stream -> stream2)
+  cudaEvent_t ev_diag = nullptr;        // static-order LU: diagonal block factored (stream -> stream2)
   cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)
 
   // surface post-processing (fp_post.cu). The mesh topology of a triangular

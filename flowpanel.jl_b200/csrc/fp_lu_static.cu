@@ -669,6 +669,9 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
+    // the columns beyond the next panel need only the diagonal block's
+    // inverses for their U12: the second stream starts them beside k_l21
+    FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_diag, c->stream));
     if (kend < n) {
       TraceScope tr(c, TR_L21);
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
@@ -712,13 +715,15 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           ++c->nlaunch;
           FP_CUDA_TRY(c->err, cudaGetLastError());
         }
+        // the update reads L21 (the panel stream's k_l21)
+        if (c->lu_overlap) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
         if (int rc = update(slot, kend, K0, knext, n, knext - kend)) return rc;
       }
       return FP_OK;
     };
     if (c->lu_overlap) {
       OnStream2 on2(c);
-      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
+      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_diag, 0));
       if (int rc = rest()) return rc;
       FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
     } else {
