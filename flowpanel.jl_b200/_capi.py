@@ -30,7 +30,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_uind_vjp", "fp_kernel_timing", "fp_kernel_timing_read", "fp_batch_create",
            "fp_batch_destroy", "fp_batch_last_error", "fp_batch_solve", "fp_trace", "fp_trace_read", "fp_phi", "fp_solve_ls",
            "fp_ugradmu", "fp_ugradmu_ex", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads",
-           "fp_set_tuning")
+           "fp_set_tuning", "fp_autotune")
 FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH, FP_TUNE_TC_SMEM = 0, 1, 2, 3, 4
 FP_TUNE_FP64_DMMA, FP_TUNE_TC_SPLIT, FP_TUNE_TC_RED, FP_TUNE_ASM32 = 5, 6, 7, 8
 
@@ -90,6 +90,7 @@ def lib():
         L.fp_set_rhs.argtypes = [vp, _dp, C.c_int64]
         L.fp_factor.argtypes = [vp, C.c_int]
         L.fp_set_tuning.argtypes = [vp, C.c_int, C.c_int]
+        L.fp_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int)]
         L.fp_solve.argtypes = [vp, _dp, C.c_int64, C.POINTER(SolveOpts), C.POINTER(Stats)]
         L.fp_solve_body.argtypes = [vp, C.c_int, C.c_double, C.c_double, _dp, C.c_int64,
                                     C.POINTER(SolveOpts), _dp, C.POINTER(Stats)]
@@ -381,6 +382,13 @@ class Context:
         self._chk(self._L.fp_trace_read(self.h, k, _i(tags), _i(streams), t0.ctypes.data_as(C.POINTER(C.c_float)),
                                         t1.ctypes.data_as(C.POINTER(C.c_float)), C.byref(n)))
         return tags, streams, t0, t1
+
+    def autotune(self, precision, reps=2):
+        """fp_autotune: pick the fastest factorisation knobs for the assembled
+        AIC (cached per size and precision); returns the 9 knob values."""
+        out = (C.c_int * 9)()
+        self._chk(self._L.fp_autotune(self.h, int(precision), int(reps), out))
+        return list(out)
 
     def set_tuning(self, knob, value):
         """fp_set_tuning: one of the FP_TUNE_* knobs (include/flowpanel_b200.h)."""

@@ -233,10 +233,13 @@ class B200Solver:
         + FP64 refinement) | "mixed_gepp" (FP32 factors pivoted as the FP64
         form + FP64 refinement) | "bf16" (BF16 tensor-core operands, GMRES-IR
         with FP64 residuals; the largest meshes)
+    autotune: before the first LU solve of each problem size, time the
+        factorisation's knob settings on the assembled AIC (fp_autotune) and
+        keep the fastest for this solver
     """
 
     def __init__(self, method="ludiv", precision="fp64", device=0, ir_tol=1e-12, ir_maxiter=10,
-                 gmres_memory=50, atol=None, rtol=None, itmax=0):
+                 gmres_memory=50, atol=None, rtol=None, itmax=0, autotune=False):
         if method not in ("ludiv", "backslash", "gmres"):
             raise ValueError(f"unknown method {method}")
         if precision not in ("fp64", "mixed", "mixed_gepp", "bf16"):
@@ -248,6 +251,8 @@ class B200Solver:
         self.ctx = _capi.Context(device)
         self.stats = None
         self._geom_of = None
+        self.autotune = autotune
+        self.tuned = {}   # (N, precision) -> knob values chosen by fp_autotune
 
     def load(self, body: AbstractBody, normals=None, CPs=None):
         m = body.mesh
@@ -304,6 +309,13 @@ def solve(body: AbstractBody, Uinfs, Das=None, Dbs=None, solver: Optional[B200So
         pres = calc_elprescribe(body) if elprescribe is None else list(elprescribe)
         x, st = solver.ctx.solve_ls(Uinfs, pres, body.kerneloffset, body.kernelcutoff)
     else:
+        if solver.autotune and solver.method != "gmres" and solver.precision in ("fp64", "mixed", "bf16"):
+            key = (body.ncells, solver.precision)
+            if key not in solver.tuned:
+                prec = {"fp64": _capi.FP_PREC_FP64, "mixed": _capi.FP_PREC_MIXED, "bf16": _capi.FP_PREC_BF16}
+                solver.ctx.assemble(body.element, body.kerneloffset, body.kernelcutoff,
+                                    _capi.FP_PREC_MIXED if solver.precision == "mixed" else _capi.FP_PREC_FP64)
+                solver.tuned[key] = solver.ctx.autotune(prec[solver.precision])
         x, st = solver.ctx.solve_body(body.element, Uinfs, body.kerneloffset, body.kernelcutoff, solver.opts)
     solver.stats = st.asdict()
     body.strength = np.array(x, dtype=np.float64)

@@ -806,6 +806,67 @@ int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stat
   return FP_OK;
 }
 
+// The knob values of one configuration, in FP_TUNE_* order.
+static std::vector<int> current_knobs(const fp_ctx* c) {
+  return {c->tc_stages, c->lu_overlap ? 1 : 0, c->tc_tiles, c->use_graph ? 1 : 0, c->tc_smem, c->fp64_dmma,
+          c->tc_split, c->tc_red ? 1 : 0, c->asm32 ? 1 : 0};
+}
+
+int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
+  if (check_ctx(c)) return FP_EINVAL;
+  FP_CUDA_TRY(c->err, cudaSetDevice(c->device));
+  if (precision != FP_PREC_FP64 && precision != FP_PREC_MIXED && precision != FP_PREC_BF16)
+    return c->err.set(FP_EINVAL, "fp_autotune: precision must be FP_PREC_FP64, FP_PREC_MIXED or FP_PREC_BF16");
+  reps = std::max(1, std::min(reps, 16));
+  const uint64_t key = ((uint64_t)c->N << 8) | (uint64_t)precision;
+  auto hit = c->tuned.find(key);
+  if (hit == c->tuned.end()) {
+    if (c->assembled < 0) return c->err.set(FP_ESTATE, "fp_autotune: assemble first");
+    if (precision == FP_PREC_MIXED && c->assembled_prec != FP_PREC_MIXED && c->assembled_prec != FP_PREC_MIXED_GEPP)
+      return c->err.set(FP_ESTATE, "fp_autotune: FP_PREC_MIXED needs an AIC assembled for it");
+    // candidates: (knob, value) settings over the defaults; each is timed by
+    // its median factorisation (device time) on the assembled AIC
+    std::vector<std::vector<std::pair<int, int>>> cand;
+    if (precision == FP_PREC_FP64) {
+      for (int v : {3, 2, 1, 0}) cand.push_back({{FP_TUNE_FP64_DMMA, v}});
+    } else {
+      for (int red : {1, 0})
+        for (int stages : {2, 3})
+          for (int tiles : {0, 4}) {
+            if (tiles && stages == 3) continue;   // the multi-tile kernel has its own ring
+            cand.push_back({{FP_TUNE_TC_RED, red}, {FP_TUNE_TC_STAGES, stages}, {FP_TUNE_TC_TILES, tiles}});
+          }
+    }
+    const std::vector<int> saved = current_knobs(c);
+    const int element = c->assembled, aprec = c->assembled_prec;
+    const double off = c->kern_offset, cut = c->kern_cutoff;
+    double best = 1e300;
+    std::vector<int> best_knobs = saved;
+    for (const auto& cfg : cand) {
+      for (int k = 0; k < (int)saved.size(); ++k) fp_set_tuning(c, k, saved[k]);
+      for (const auto& kv : cfg) fp_set_tuning(c, kv.first, kv.second);
+      std::vector<double> ms;
+      for (int r = 0; r < reps + 1; ++r) {   // the first run warms the kernels up
+        // the FP32 factorisations work in place on the FP32 AIC: assemble it again
+        if (precision != FP_PREC_FP64 && precision != FP_PREC_BF16)
+          if (int rc = fp_assemble(c, element, off, cut, aprec)) return rc;
+        if (int rc = fp_factor(c, precision)) return rc;
+        if (r > 0) ms.push_back(c->ms_factor);
+      }
+      std::sort(ms.begin(), ms.end());
+      const double med = ms[ms.size() / 2];
+      if (med < best) { best = med; best_knobs = current_knobs(c); }
+    }
+    hit = c->tuned.emplace(key, best_knobs).first;
+    // leave the context assembled, not factored
+    if (int rc = fp_assemble(c, element, off, cut, aprec)) return rc;
+  }
+  for (int k = 0; k < (int)hit->second.size(); ++k) fp_set_tuning(c, k, hit->second[k]);
+  if (knobs_out)
+    for (int k = 0; k < (int)hit->second.size(); ++k) knobs_out[k] = hit->second[k];
+  return FP_OK;
+}
+
 int fp_set_tuning(fp_ctx* c, int knob, int value) {
   if (check_ctx(c)) return FP_EINVAL;
   switch (knob) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -162,6 +163,7 @@ struct fp_ctx {
   cudaEvent_t ev_asm = nullptr;         // assembly inputs ready (stream -> stream_bg)
   bool g64_pending = false;             // the FP64 AIC is still being written on stream_bg
   bool asm32 = false;                   // mixed forms: FP32 AIC pass first, FP64 pass in the background
+  std::map<uint64_t, std::vector<int>> tuned;   // fp_autotune: (N, precision) -> knob values
   cudaEvent_t ev_panel = nullptr;       // panel factored (stream -> stream2)
   cudaEvent_t ev_diag = nullptr;        // static-order LU: diagonal block factored (stream -> stream2)
   cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)

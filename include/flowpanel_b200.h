@@ -432,6 +432,16 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_ASM32 8
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
+/* Autotuner (no counterpart in the reference): times the factorisation of the
+ * assembled AIC under candidate knob settings (FP_PREC_FP64: the FP64 update
+ * variants of FP_TUNE_FP64_DMMA; FP_PREC_MIXED / FP_PREC_BF16: the tensor-core
+ * update's epilogue, ring depth and tile kernel), reps timed runs each after
+ * one warm-up, and keeps the fastest for this context. The choice is cached
+ * per (N, precision): a later call for the same size only applies it. The
+ * context is left assembled (FP32 trials re-assemble), not factored; knobs
+ * (may be NULL) receives the 9 knob values in FP_TUNE_* order. */
+int fp_autotune(fp_ctx* ctx, int precision, int reps, int* knobs);
+
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels
  * this context has launched since it was created. */
 int fp_kernel_launches(fp_ctx* ctx, int64_t* count);

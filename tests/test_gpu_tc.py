@@ -102,3 +102,33 @@ def test_bf16_form_reaches_fp64_solution(fp, O, ctx, nc, ns):
     Gr = O.assemble_vortexring(w, cps, normals, D, D)
     xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_autotune_keeps_results(fp, O, precision):
+    """fp_autotune through B200Solver(autotune=True): the knobs chosen for the
+    size are cached (a second solve does not tune again) and the solution is
+    the oracle's to 1e-10."""
+    w = fp.meshes.swept_wing("0012", 40, 48)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(4.2)
+    V = np.array([np.cos(a), 0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    solver = fp.B200Solver(method="ludiv", precision=precision, autotune=True)
+    try:
+        fp.solve(body, U, D, D, solver=solver)
+        key = (w.npanels, precision)
+        assert key in solver.tuned and len(solver.tuned[key]) == 9
+        knobs = list(solver.tuned[key])
+        fp.solve(body, U, D, D, solver=solver)
+        assert solver.tuned[key] == knobs
+        again = solver.ctx.autotune(fp._capi.FP_PREC_MIXED if precision == "mixed" else fp._capi.FP_PREC_FP64)
+        assert again == knobs   # cached per size: applied, not re-timed
+    finally:
+        solver.close()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(body.strength - xr) / np.linalg.norm(xr) < 1e-10
