@@ -32,7 +32,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_ugradmu", "fp_ugradmu_ex", "fp_calcfield_cp", "fp_calcfield_f", "fp_calcfield_lds", "fp_surface_loads",
            "fp_set_tuning", "fp_autotune")
 FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH, FP_TUNE_TC_SMEM = 0, 1, 2, 3, 4
-FP_TUNE_FP64_DMMA, FP_TUNE_TC_SPLIT, FP_TUNE_TC_RED, FP_TUNE_ASM32 = 5, 6, 7, 8
+FP_TUNE_FP64_DMMA, FP_TUNE_TC_SPLIT, FP_TUNE_TC_RED, FP_TUNE_ASM32, FP_TUNE_TC_NARROW = 5, 6, 7, 8, 9
 
 
 class SolveOpts(C.Structure):
@@ -385,8 +385,8 @@ class Context:
 
     def autotune(self, precision, reps=2):
         """fp_autotune: pick the fastest factorisation knobs for the assembled
-        AIC (cached per size and precision); returns the 9 knob values."""
-        out = (C.c_int * 9)()
+        AIC (cached per size and precision); returns the 10 knob values."""
+        out = (C.c_int * 10)()
         self._chk(self._L.fp_autotune(self.h, int(precision), int(reps), out))
         return list(out)
 

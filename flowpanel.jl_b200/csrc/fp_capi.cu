@@ -510,7 +510,7 @@ static int factor_static_graph(fp_ctx* c, bool bf16) {
   std::vector<uintptr_t> key = {(uintptr_t)c->N, (uintptr_t)c->ld, (uintptr_t)c->d_G32, (uintptr_t)c->d_ipiv,
                                 (uintptr_t)c->d_cert, (uintptr_t)c->d_status, (uintptr_t)c->d_minv,
                                 (uintptr_t)bf16, (uintptr_t)c->tc_stages, (uintptr_t)c->tc_tiles, (uintptr_t)c->tc_smem,
-                                (uintptr_t)c->tc_split, (uintptr_t)c->tc_red,
+                                (uintptr_t)c->tc_split, (uintptr_t)c->tc_red, (uintptr_t)c->tc_narrow_stages,
                                 (uintptr_t)c->lu_overlap, (uintptr_t)c->use_tc};
   for (int s = 0; s < 2; ++s)
     for (int i = 0; i < 4; ++i) key.push_back((uintptr_t)c->d_tc[s][i]);
@@ -809,7 +809,7 @@ int fp_solve(fp_ctx* c, double* x, int64_t k, const fp_solve_opts* opts, fp_stat
 // The knob values of one configuration, in FP_TUNE_* order.
 static std::vector<int> current_knobs(const fp_ctx* c) {
   return {c->tc_stages, c->lu_overlap ? 1 : 0, c->tc_tiles, c->use_graph ? 1 : 0, c->tc_smem, c->fp64_dmma,
-          c->tc_split, c->tc_red ? 1 : 0, c->asm32 ? 1 : 0};
+          c->tc_split, c->tc_red ? 1 : 0, c->asm32 ? 1 : 0, c->tc_narrow_stages};
 }
 
 int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
@@ -834,7 +834,11 @@ int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
         for (int stages : {2, 3})
           for (int tiles : {0, 4}) {
             if (tiles && stages == 3) continue;   // the multi-tile kernel has its own ring
-            cand.push_back({{FP_TUNE_TC_RED, red}, {FP_TUNE_TC_STAGES, stages}, {FP_TUNE_TC_TILES, tiles}});
+            for (int narrow : {6, 0}) {
+              if (narrow && !red) continue;   // the deep narrow ring is a red.global kernel
+              cand.push_back({{FP_TUNE_TC_RED, red}, {FP_TUNE_TC_STAGES, stages}, {FP_TUNE_TC_TILES, tiles},
+                              {FP_TUNE_TC_NARROW, narrow}});
+            }
           }
     }
     const std::vector<int> saved = current_knobs(c);
@@ -887,6 +891,10 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
     case FP_TUNE_FP64_DMMA:
       if (value < 0 || value > 3) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..3");
       c->fp64_dmma = value;
+      return FP_OK;
+    case FP_TUNE_TC_NARROW:
+      if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");
+      c->tc_narrow_stages = value;
       return FP_OK;
     case FP_TUNE_ASM32:
       c->asm32 = value != 0;

@@ -841,8 +841,9 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
         reinterpret_cast<uintptr_t>(Al) | reinterpret_cast<uintptr_t>(Bh) | reinterpret_cast<uintptr_t>(Bl)) &
        15) != 0)
     return false;
-  static SmemAttr attr2, attr3, attrm, attr2r, attr3r, attrmr;
+  static SmemAttr attr2, attr3, attrm, attr2r, attr3r, attr6r, attrmr;
   if (attr3r.ensure(tc::k_tc_gemm_sub<3, true>, kTcSmemMax) != cudaSuccess) return false;
+  if (attr6r.ensure(tc::k_tc_gemm_sub<6, true>, kTcSmemMax) != cudaSuccess) return false;
   if (attrmr.ensure(tc::k_tc_gemm_multi<false, true>, tc::mt::smem<false>()) != cudaSuccess) return false;
   if (attr2.ensure(tc::k_tc_gemm_sub<2>, kTcSmemMax) != cudaSuccess) return false;
   if (attr3.ensure(tc::k_tc_gemm_sub<3>, kTcSmemMax) != cudaSuccess) return false;
@@ -866,7 +867,13 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
     else
       tc::k_tc_gemm_multi<false><<<ctas, tc::mt::THREADS, tc::mt::smem<false>(), c->stream>>>(
           mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->tc_tiles, c->d_status);
-  } else if (c->tc_red && c->tc_stages == 3)
+  } else if (c->tc_red && c->tc_narrow_stages == 6 && grid.y == 1 && (int)grid.x <= num_sms())
+    // one column of tiles (the next panel's update, on the factorisation's
+    // critical path): at most one CTA an SM, so a 6-stage ring costs no
+    // occupancy and puts 6 of the 8 K blocks in flight at once
+    tc::k_tc_gemm_sub<6, true><<<grid, tc::THREADS, tc::smem_bytes<6>(), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+  else if (c->tc_red && c->tc_stages == 3)
     tc::k_tc_gemm_sub<3, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<3>(), c->tc_smem), c->stream>>>(
         mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
   else if (c->tc_red)

@@ -420,7 +420,10 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       AIC (read only by the refinement) on a background
  *                       stream under the factorisation, which that pass slows
  *                       by 2.2 ms; 0 (default): one FP64 pass writes both
- *                       (2.49 ms) */
+ *                       (2.49 ms)
+ *   FP_TUNE_TC_NARROW   6 (default): the update of one column of tiles (the next
+ *                       panel's columns, on the critical path) uses a 6-stage
+ *                       ring; 0: the same ring as the other updates */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -430,6 +433,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_TC_SPLIT 6
 #define FP_TUNE_TC_RED 7
 #define FP_TUNE_ASM32 8
+#define FP_TUNE_TC_NARROW 9
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the
@@ -439,7 +443,7 @@ int fp_set_tuning(fp_ctx* ctx, int knob, int value);
  * one warm-up, and keeps the fastest for this context. The choice is cached
  * per (N, precision): a later call for the same size only applies it. The
  * context is left assembled (FP32 trials re-assemble), not factored; knobs
- * (may be NULL) receives the 9 knob values in FP_TUNE_* order. */
+ * (may be NULL) receives the 10 knob values in FP_TUNE_* order. */
 int fp_autotune(fp_ctx* ctx, int precision, int reps, int* knobs);
 
 /* Measurement utility (no counterpart in the reference): number of CUDA kernels

@@ -47,7 +47,7 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
 @pytest.mark.parametrize("nc,ns", [(8, 4), (12, 8), (20, 24), (40, 48), (60, 80), (50, 30)])
 @pytest.mark.parametrize("knob,value", [("FP_TUNE_TC_SPLIT", 1), ("FP_TUNE_TC_SPLIT", 2), ("FP_TUNE_TC_SPLIT", 3),
                                         ("FP_TUNE_TC_RED", 0), ("FP_TUNE_TC_TILES", 2), ("FP_TUNE_TC_TILES", 4),
-                                        ("FP_TUNE_ASM32", 1)])
+                                        ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0)])
 def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
     1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
@@ -121,7 +121,7 @@ def test_autotune_keeps_results(fp, O, precision):
     try:
         fp.solve(body, U, D, D, solver=solver)
         key = (w.npanels, precision)
-        assert key in solver.tuned and len(solver.tuned[key]) == 9
+        assert key in solver.tuned and len(solver.tuned[key]) == 10
         knobs = list(solver.tuned[key])
         fp.solve(body, U, D, D, solver=solver)
         assert solver.tuned[key] == knobs
