@@ -403,8 +403,9 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       an SM, more room for the panel kernels beside them
  *   FP_TUNE_FP64_DMMA   the FP64 LU's trailing update: 0 the SIMT FP64 kernel
  *                       (15.0 TF/s on the 12k wing); 1, 2, 3 the FP64 tensor
- *                       path (mma.sync .f64) with 8, 16 or 32 warps a CTA (17.0,
- *                       19.2, 19.7 TF/s; 3 is the default); same results
+ *                       path (mma.sync .f64) with 8, 16 or 32 warps a CTA and
+ *                       16-deep K slices (17.0, 19.2, 19.7 TF/s); 4 (default):
+ *                       32 warps, 32-deep K slices (20.8 TF/s); same results
  *   FP_TUNE_TC_SPLIT    the static-order LU's tensor-core update: 0 reads
  *                       operands split into TF32 hi / lo by the panel kernels
  *                       (32 KB a K block); 1, 2, 3: reads the unsplit FP32
