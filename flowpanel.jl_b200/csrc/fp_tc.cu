@@ -127,25 +127,42 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(h);
 }
 
+// kind::f16 instruction descriptor: D f32, A/B bf16 (1), both K-major, N >> 3, M >> 4
+constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                                ((uint32_t)(BM >> 4) << 24);
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(IDESC_BF16), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
 // RED: the epilogue adds -D to C with red.global.add.f32 straight from the
 // registers (lane = row, 128-byte coalesced per column; Cp / ldc address C)
 // instead of staging it for a TMA reduce-add.
-template <int STAGES, bool RED = false>
+// BF16: BF16 operands (tmAh, tmBh only; kind::f16, one MMA per 16-deep
+// step, 32-deep K blocks of 64-byte rows: 16 KB a stage).
+template <int STAGES, bool RED = false, bool BF16 = false>
 __global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
               const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status,
               float* __restrict__ Cp = nullptr, int64_t ldc = 0) {
+  constexpr int SB = BF16 ? 2 * TILE_A : STAGE_BYTES;   // bytes a stage
+  constexpr int KB = BF16 ? 32 : BK;                    // K elements a stage
+  static_assert(RED || STAGES * SB >= 4 * 32 * BN * 4, "the drained ring holds the epilogue's staging");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * SB);
   uint64_t* empty = full + STAGES;
   uint64_t* done = empty + STAGES;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int nk = (K + BK - 1) / BK;
+  const int nk = (K + KB - 1) / KB;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
@@ -171,12 +188,17 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
       const int s = kb % STAGES;
       if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1)) { *abort_flag = 1; break; }
       if (*(volatile int*)abort_flag) break;
-      mbar_expect_tx(&full[s], STAGE_BYTES);
-      uint8_t* base = smem + s * STAGE_BYTES;
-      tma_load_2d(base, &tmAh, kb * BK, m0, &full[s]);
-      tma_load_2d(base + TILE_A, &tmAl, kb * BK, m0, &full[s]);
-      tma_load_2d(base + 2 * TILE_A, &tmBh, kb * BK, n0, &full[s]);
-      tma_load_2d(base + 2 * TILE_A + TILE_B, &tmBl, kb * BK, n0, &full[s]);
+      mbar_expect_tx(&full[s], SB);
+      uint8_t* base = smem + s * SB;
+      if (BF16) {
+        tma_load_2d(base, &tmAh, kb * KB, m0, &full[s]);
+        tma_load_2d(base + TILE_A, &tmBh, kb * KB, n0, &full[s]);
+      } else {
+        tma_load_2d(base, &tmAh, kb * BK, m0, &full[s]);
+        tma_load_2d(base + TILE_A, &tmAl, kb * BK, m0, &full[s]);
+        tma_load_2d(base + 2 * TILE_A, &tmBh, kb * BK, n0, &full[s]);
+        tma_load_2d(base + 2 * TILE_A + TILE_B, &tmBl, kb * BK, n0, &full[s]);
+      }
       ++issued;
     }
     if (*(volatile int*)abort_flag) {
@@ -191,15 +213,24 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
       const int s = kb % STAGES;
       if (!mbar_wait(&full[s], (kb / STAGES) & 1)) { ok = false; *abort_flag = 1; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
-      const uint64_t dAh = sdesc(base), dAl = sdesc(base + TILE_A);
-      const uint64_t dBh = sdesc(base + 2 * TILE_A), dBl = sdesc(base + 2 * TILE_A + TILE_B);
+      const uint32_t base = smem_u32(smem + s * SB);
+      if (BF16) {
+        const uint64_t dA = sdesc(base), dB = sdesc(base + TILE_A);
 #pragma unroll
-      for (int kk = 0; kk < BK / 8; ++kk) {
-        const uint64_t off = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
-        umma_tf32(tmem, dAh + off, dBl + off, (kb | kk) != 0 ? 1u : 0u);
-        umma_tf32(tmem, dAl + off, dBh + off, 1u);
-        umma_tf32(tmem, dAh + off, dBh + off, 1u);
+        for (int kk = 0; kk < 2; ++kk) {   // 16 bf16 = 32 bytes along K per MMA
+          const uint64_t off = (uint64_t)((kk * 32) >> 4);
+          umma_bf16(tmem, dA + off, dB + off, (kb | kk) != 0 ? 1u : 0u);
+        }
+      } else {
+        const uint64_t dAh = sdesc(base), dAl = sdesc(base + TILE_A);
+        const uint64_t dBh = sdesc(base + 2 * TILE_A), dBl = sdesc(base + 2 * TILE_A + TILE_B);
+#pragma unroll
+        for (int kk = 0; kk < BK / 8; ++kk) {
+          const uint64_t off = (uint64_t)((kk * 32) >> 4);   // 8 tf32 = 32 bytes along K
+          umma_tf32(tmem, dAh + off, dBl + off, (kb | kk) != 0 ? 1u : 0u);
+          umma_tf32(tmem, dAl + off, dBh + off, 1u);
+          umma_tf32(tmem, dAh + off, dBh + off, 1u);
+        }
       }
       umma_commit(&empty[s]);
     }
@@ -475,19 +506,8 @@ template <bool BF16> __host__ __device__ constexpr int stage_bytes() { return BF
 template <bool BF16> __host__ __device__ constexpr int kblock() { return BF16 ? 32 : BK; }
 template <bool BF16> __host__ __device__ constexpr int smem() { return STAGES * stage_bytes<BF16>() + 4 * 2 * STG_BYTES + 1024 + 256; }
 constexpr uint32_t TMEM_COLS = 2 * BN;
-// kind::f16 instruction descriptor: D f32, A/B bf16 (1), both K-major, N >> 3, M >> 4
-constexpr uint32_t IDESC_BF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                                ((uint32_t)(BM >> 4) << 24);
 }  // namespace mt
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(mt::IDESC_BF16), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-      : "memory");
-}
 
 
 template <bool BF16, bool RED = false>
@@ -934,8 +954,9 @@ bool tc_gemm_sub_bf16(fp_ctx* c, const void* Ah, const void* Bh, int ldk, float*
   if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(ldc * 4) | reinterpret_cast<uintptr_t>(Ah) |
         reinterpret_cast<uintptr_t>(Bh)) & 15) != 0)
     return false;
-  static SmemAttr attr;
+  static SmemAttr attr, attr1;
   if (attr.ensure(tc::k_tc_gemm_multi<true>, tc::mt::smem<true>()) != cudaSuccess) return false;
+  if (attr1.ensure(tc::k_tc_gemm_sub<4, true, true>, kTcSmemMax) != cudaSuccess) return false;
   auto map16 = [&](CUtensorMap* tm, const void* base, int64_t rows) {
     cuuint64_t dims[2] = {(cuuint64_t)kk, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)ldk * 2};
@@ -948,11 +969,19 @@ bool tc_gemm_sub_bf16(fp_ctx* c, const void* Ah, const void* Bh, int ldk, float*
   CUtensorMap mA, mB, mC;
   if (!map16(&mA, Ah, m) || !map16(&mB, Bh, nn) || !tc::make_map_c(&mC, C, m, nn, ldc, 32)) return false;
   const int tiles = (int)(((m + tc::BM - 1) / tc::BM) * ((nn + tc::BN - 1) / tc::BN));
-  const int tpc = c->tc_tiles > 0 ? c->tc_tiles : 4;
   const int ev = kt_begin(c);
   TraceScope tr(c, TR_GEMM_TC);
-  tc::k_tc_gemm_multi<true><<<(unsigned)((tiles + tpc - 1) / tpc), tc::mt::THREADS, tc::mt::smem<true>(), c->stream>>>(
-      mA, mA, mB, mB, mC, (int)m, (int)nn, kk, tpc, c->d_status);
+  if (c->tc_red && c->tc_tiles == 0) {
+    // one tile a CTA, 4-stage ring of 16 KB stages, red.global epilogue
+    dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
+    constexpr int sb = 4 * 2 * tc::TILE_A + 1024 + 256;
+    tc::k_tc_gemm_sub<4, true, true><<<grid, tc::THREADS, std::max(sb, c->tc_smem), c->stream>>>(
+        mA, mA, mB, mB, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+  } else {
+    const int tpc = c->tc_tiles > 0 ? c->tc_tiles : 4;
+    tc::k_tc_gemm_multi<true><<<(unsigned)((tiles + tpc - 1) / tpc), tc::mt::THREADS, tc::mt::smem<true>(),
+                                c->stream>>>(mA, mA, mB, mB, mC, (int)m, (int)nn, kk, tpc, c->d_status);
+  }
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;
