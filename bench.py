@@ -562,7 +562,7 @@ def run_ours(args, rank, ws, dist):
                                   "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                                   "frac": achieved / peak64,
                                   "peak_source": "measured FP64 FMA throughput (fp_measure_fma_peak)"},
-            "fp64_trailing_update": {"kernel": "k_gemm_sub_dmma<1024,4,2,32,3> (FP64 tensor path, mma.sync .f64)",
+            "fp64_trailing_update": {"kernel": "k_gemm_sub_dmma<512,4,2,32,2,64,2> (FP64 tensor path, mma.sync .f64, 128 x 64 tiles)",
                                      "launches": d_launches, "ms_total": d_ms,
                                      "tflops": d_flops / (d_ms * 1e-3) / 1e12 if d_ms else 0,
                                      "frac_of_fp64_fma_peak": (d_flops / (d_ms * 1e-3) / 1e12 / peak64) if d_ms else 0,

@@ -828,7 +828,7 @@ int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
     // its median factorisation (device time) on the assembled AIC
     std::vector<std::vector<std::pair<int, int>>> cand;
     if (precision == FP_PREC_FP64) {
-      for (int v : {3, 4, 2, 1, 0}) cand.push_back({{FP_TUNE_FP64_DMMA, v}});
+      for (int v : {6, 5, 4, 3, 0}) cand.push_back({{FP_TUNE_FP64_DMMA, v}});
     } else {
       for (int red : {1, 0})
         for (int stages : {2, 3})
@@ -889,7 +889,7 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       c->use_graph = value != 0;
       return FP_OK;
     case FP_TUNE_FP64_DMMA:
-      if (value < 0 || value > 4) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..4");
+      if (value < 0 || value > 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..6");
       c->fp64_dmma = value;
       return FP_OK;
     case FP_TUNE_TC_NARROW:

@@ -144,7 +144,7 @@ struct fp_ctx {
   int tc_split = 0;             // static-order LU: 0 pre-split operands; 1..3 split in shared memory (3, 4, 6 x stages)
   bool tc_red = true;           // static-order LU: the update's epilogue adds to C by red.global instead of TMA
   int tc_narrow_stages = 6;     // ring depth of the update of one column of tiles (6, or 0: as the others)
-  int fp64_dmma = 4;            // FP64 LU update: 0 SIMT; FP64 tensor path with 8 (1), 16 (2), 32 (3) warps, 32 + 32-deep K (4)
+  int fp64_dmma = 6;            // FP64 LU update: 0 SIMT; FP64 tensor path, variants 1..6 (fp_set_tuning)
   bool lu_overlap = true;       // static-order LU: trailing update on the second stream (fp_set_tuning)
   // The static-order FP32 factorisation replayed as a CUDA graph (both streams,
   // the diagonal-block inverses included): captured on the second call with

@@ -942,10 +942,14 @@ k_gemm_sub_f64(const double* __restrict__ Am, const double* __restrict__ Bm, dou
 // Fragments (PTX ISA, mma m8n8k4 .f64): lane = 4 g + t; A(8x4, row) element
 // (g, t); B(4x8, col) element (t, g); C(8x8) elements (g, 2t) and (g, 2t+1).
 namespace dm {
-constexpr int BM = 128, BN = 128, AP = BM + 8;
+constexpr int BM = 128, AP = BM + 8;
 template <int BK> __host__ __device__ constexpr int bp() { return BK + 4; }
-template <int BK> __host__ __device__ constexpr size_t stage_doubles() { return (size_t)BK * AP + (size_t)BN * bp<BK>(); }
-template <int BK, int STAGES> constexpr size_t smem() { return STAGES * stage_doubles<BK>() * sizeof(double); }
+template <int BK, int BN = 128> __host__ __device__ constexpr size_t stage_doubles() {
+  return (size_t)BK * AP + (size_t)BN * bp<BK>();
+}
+template <int BK, int STAGES, int BN = 128> constexpr size_t smem() {
+  return STAGES * stage_doubles<BK, BN>() * sizeof(double);
+}
 }  // namespace dm
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
@@ -954,8 +958,8 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int NT, int MF, int NF, int BK = 16, int STAGES = 3>
-__global__ void __launch_bounds__(NT, 1)
+template <int NT, int MF, int NF, int BK = 16, int STAGES = 3, int BN = 128, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB)
 k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, double* __restrict__ Cm, int64_t lda,
                 int64_t m, int64_t nn, int kk) {
   using namespace dm;
@@ -971,7 +975,7 @@ k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, do
   const int nk = (kk + BK - 1) / BK;
   // one K slice into stage s: 1024 16-byte pieces of A and 1024 of B
   auto issue = [&](int kb, int s) {
-    double* As = ring + (size_t)s * stage_doubles<BK>();
+    double* As = ring + (size_t)s * stage_doubles<BK, BN>();
     double* Bs = As + BK * AP;
     const int k0 = kb * BK;
 #pragma unroll
@@ -1010,7 +1014,7 @@ k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, do
     __syncthreads();   // slice kb has landed for every thread; slot (kb - 1) % STAGES is free
     if (kb + STAGES - 1 < nk) issue(kb + STAGES - 1, (kb + STAGES - 1) % STAGES);
     asm volatile("cp.async.commit_group;" ::: "memory");
-    const double* As = ring + (size_t)(kb % STAGES) * stage_doubles<BK>();
+    const double* As = ring + (size_t)(kb % STAGES) * stage_doubles<BK, BN>();
     const double* Bs = As + BK * AP;
 #pragma unroll
     for (int k4 = 0; k4 < BK; k4 += 4) {
@@ -1056,17 +1060,27 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
     const int slot = kt_begin(c);
     TraceScope tr(c, TR_GEMM_SIMT);
     if (mis == 0 && c->fp64_dmma) {
-      static SmemAttr attr8, attr16, attr32, attr32k;
+      static SmemAttr attr8, attr16, attr32, attr32k, attr2c, attr2k;
       constexpr int sm16 = (int)dm::smem<16, 3>(), sm32 = (int)dm::smem<32, 3>();
       FP_CUDA_TRY(c->err, attr8.ensure(k_gemm_sub_dmma<256, 8, 4>, sm16));
       FP_CUDA_TRY(c->err, attr16.ensure(k_gemm_sub_dmma<512, 4, 4>, sm16));
       FP_CUDA_TRY(c->err, attr32.ensure(k_gemm_sub_dmma<1024, 4, 2>, sm16));
       FP_CUDA_TRY(c->err, attr32k.ensure(k_gemm_sub_dmma<1024, 4, 2, 32, 3>, sm32));
-      dim3 g((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + dm::BN - 1) / dm::BN));
+      constexpr int sm64 = (int)dm::smem<16, 3, 64>();
+      FP_CUDA_TRY(c->err, attr2c.ensure(k_gemm_sub_dmma<512, 4, 2, 16, 3, 64, 2>, sm64));
+      constexpr int sm64k = (int)dm::smem<32, 2, 64>();
+      FP_CUDA_TRY(c->err, attr2k.ensure(k_gemm_sub_dmma<512, 4, 2, 32, 2, 64, 2>, sm64k));
+      dim3 g((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + 127) / 128));
       const double* Ad = (const double*)Am;
       const double* Bd = (const double*)Bm;
       double* Cd = (double*)Cm;
-      if (c->fp64_dmma == 4)
+      if (c->fp64_dmma == 6) {   // 128 x 64 tiles, two CTAs an SM, 32-deep K slices in 2 stages
+        dim3 g2((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + 63) / 64));
+        k_gemm_sub_dmma<512, 4, 2, 32, 2, 64, 2><<<g2, 512, sm64k, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+      } else if (c->fp64_dmma == 5) {   // 128 x 64 tiles, two CTAs an SM
+        dim3 g2((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + 63) / 64));
+        k_gemm_sub_dmma<512, 4, 2, 16, 3, 64, 2><<<g2, 512, sm64, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+      } else if (c->fp64_dmma == 4)
         k_gemm_sub_dmma<1024, 4, 2, 32, 3><<<g, 1024, sm32, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
       else if (c->fp64_dmma == 3)
         k_gemm_sub_dmma<1024, 4, 2><<<g, 1024, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);

@@ -402,10 +402,14 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       and barriers only; at most 232448): fewer update CTAs
  *                       an SM, more room for the panel kernels beside them
  *   FP_TUNE_FP64_DMMA   the FP64 LU's trailing update: 0 the SIMT FP64 kernel
- *                       (15.0 TF/s on the 12k wing); 1, 2, 3 the FP64 tensor
- *                       path (mma.sync .f64) with 8, 16 or 32 warps a CTA and
- *                       16-deep K slices (17.0, 19.2, 19.7 TF/s); 4 (default):
- *                       32 warps, 32-deep K slices (20.8 TF/s); same results
+ *                       (15.0 TF/s on the 12k wing); the FP64 tensor path
+ *                       (mma.sync .f64) on 128 x 128 tiles, one CTA an SM:
+ *                       1, 2, 3 with 8, 16 or 32 warps and 16-deep K slices
+ *                       (17.0, 19.2, 19.7 TF/s), 4 with 32 warps and 32-deep
+ *                       slices (20.8); on 128 x 64 tiles, two CTAs of 16 warps
+ *                       an SM: 5 with 16-deep slices in 3 stages (22.4), 6
+ *                       (default) with 32-deep slices in 2 stages (23.1);
+ *                       all give the same results
  *   FP_TUNE_TC_SPLIT    the static-order LU's tensor-core update: 0 reads
  *                       operands split into TF32 hi / lo by the panel kernels
  *                       (32 KB a K block); 1, 2, 3: reads the unsplit FP32

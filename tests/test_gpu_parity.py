@@ -80,11 +80,11 @@ def test_wing_solve_matches_oracle(fp, O, ctx, precision):
 
 
 @pytest.mark.parametrize("nc,ns", [(40, 48), (60, 90)])
-@pytest.mark.parametrize("mode", [1, 2, 3, 4])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4, 5, 6])
 def test_fp64_lu_dmma_update_matches_oracle(fp, O, nc, ns, mode):
-    """FP_TUNE_FP64_DMMA = 1..4: the FP64 LU's trailing update on the FP64
-    tensor path (mma.sync .f64; 8, 16 or 32 warps a CTA, 16- or 32-deep K
-    slices) gives the oracle's
+    """FP_TUNE_FP64_DMMA = 1..6: the FP64 LU's trailing update on the FP64
+    tensor path (mma.sync .f64; 128 x 128 tiles with 8, 16 or 32 warps a CTA,
+    128 x 64 tiles two CTAs an SM; 16- or 32-deep K slices) gives the oracle's
     strengths to 1e-10, and the SIMT update's to 1e-12 (1,920 and 5,400
     panels: several 256-column panels with partial tiles at the edges)."""
     w, body, normals, cps, D, U = _wing_setup(fp, nc, ns)
