@@ -237,6 +237,70 @@ def cusolver_reference(n, reps=3):
     return out
 
 
+def least_squares_timing(fp, device, reps=3):
+    """Least squares of a watertight lifting body (RigidWakeBody{VortexRing, 2},
+    the reference's duct: NACA 66-2015 ring wing re-discretised with 10 cells a
+    section per surface and revolved in 60 and in 120 azimuthal steps, 7,200 and
+    14,400 triangles): device ms of fp_solve_ls (assembly, then the prescribed
+    strength folded into the right-hand side, the FP64 Gram matrix of the
+    reduced AIC, its LU and the solve), median of reps; the Gram product's
+    share and rate (N^3 flops for the symmetric N x N product)."""
+    cap = fp._capi
+    c = np.load(os.path.join(ROOT, "tests", "golden", "airfoils.npz"))["naca662015"]
+    nd = [(0.25, 10, 10.0, False), (0.50, 10, 1.0, True), (0.25, 10, 0.1, False)]
+    S = fp.meshes.rediscretize_airfoil(c[:, 0], c[:, 1], nd, nd)
+    S = np.concatenate([S, S[:1]])
+    d, ar = 2 * 0.835, 0.6
+    P = S * d * ar
+    P[:, 1] += d / 2
+    a = np.deg2rad(5.0)
+    V = np.array([np.cos(a), 0.0, np.sin(a)])
+    out = {"config": "duct (test/runtests_solvers2.jl), NACA 66-2015 ring wing, least squares, FP64", "cases": []}
+    for ntheta in (60, 120):
+        m = fp.meshes.revolution_liftbody(P, ntheta, name="duct", CPoffset=1e-14)
+        body = fp.RigidWakeBody(m, watertight=True, CPoffset=1e-14, characteristiclength=lambda *x: d * ar)
+        normals = fp.calc_normals(body)
+        cps = fp.calc_controlpoints(body, normals)
+        ctx = cap.Context(device)
+        ctx.set_geometry(m.nodes, m.panel_offsets, m.panel_nodes, cps, normals)
+        D = np.tile(V, (m.nsheddings, 1))
+        ctx.set_wake(m.shedding, D, D)
+        U = np.tile(V, (m.npanels, 1))
+        ms = []
+        for r in range(reps + 1):
+            x, st = ctx.solve_ls(U, [(0, 0.0)])
+            if r > 0:
+                ms.append(st.ms_assemble + st.ms_factor)
+        ctx.close()
+        n = m.npanels
+        out["cases"].append({"n_panels": n, "ms": float(np.median(ms)),
+                             "gram_gflop": float(n) ** 3 / 1e9})
+    return out
+
+
+def potential_timing(fp, device, nprobes=100_000, reps=3):
+    """Potential of the solved 12k wing (doublet panels and the wake's
+    semi-infinite doublets, fp_phi) at nprobes points uniform in a box around
+    it: device ms of the kernel (FP_STAGE_PHI), median of reps."""
+    cap = fp._capi
+    w, body, normals, cps, V, D, U = wing_problem(fp)
+    ctx = cap.Context(device)
+    ctx.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+    ctx.set_wake(w.shedding, D, D)
+    x, _ = ctx.solve_body(cap.FP_ELEMENT_VORTEXRING, U, opts=cap.make_opts("ludiv", "fp64"))
+    rng = np.random.default_rng(3)
+    lo, hi = w.nodes.min(axis=0) - 0.5, w.nodes.max(axis=0) + 0.5
+    T = lo + (hi - lo) * rng.random((nprobes, 3))
+    ms = []
+    for r in range(reps + 1):
+        ctx.phi(cap.FP_ELEMENT_VORTEXRING, x, T)
+        if r > 0:
+            ms.append(ctx.last_kernel_ms(cap.FP_STAGE_PHI)[0])
+    ctx.close()
+    return {"config": f"12k wing doublets + wake, {nprobes} probes in its bounding box + 0.5 m, FP64",
+            "ms": float(np.median(ms)), "probes_per_s": nprobes / (float(np.median(ms)) * 1e-3)}
+
+
 def sphere_timing(fp, device, reps=5):
     """Config 1: the 1,800-panel source sphere (30 x 60 cells, pole rows as
     triangles), FP64 assembly + LU + solve through fp_solve_body, device ms."""
@@ -465,6 +529,9 @@ def run_ours(args, rank, ws, dist):
     ctx.set_rhs(U)
     # config 1: the 1,800-panel source sphere
     sphere = sphere_timing(fp, device)
+    # the least-squares solve of watertight bodies and the potential field
+    lsq = least_squares_timing(fp, device)
+    pot = potential_timing(fp, device)
     # cuSOLVER getrf of the same size, for comparison with the hand-written LUs
     try:
         cusolver = cusolver_reference(N)
@@ -572,6 +639,8 @@ def run_ours(args, rank, ws, dist):
             "mixed_factor_timeline": timeline,
             "cusolver_getrf": cusolver,
             "sphere_config1": sphere,
+            "least_squares_f2": lsq,
+            "potential_f3": pot,
             "aoa_sweep_config3a": aoa,
             "batched_wings": batched,
             "surface_loads": post,

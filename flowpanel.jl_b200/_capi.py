@@ -19,7 +19,7 @@ FP_ELEMENT_SOURCE, FP_ELEMENT_VORTEXRING, FP_ELEMENT_SOURCE_DOUBLET = 0, 1, 2
 FP_PREC_FP64, FP_PREC_MIXED, FP_PREC_MIXED_GEPP, FP_PREC_BF16 = 0, 1, 2, 3
 _PRECISIONS = {"fp64": FP_PREC_FP64, "mixed": FP_PREC_MIXED, "mixed_gepp": FP_PREC_MIXED_GEPP, "bf16": FP_PREC_BF16}
 FP_SOLVER_LU, FP_SOLVER_GMRES = 0, 1
-FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP, FP_STAGE_POST = range(7)
+FP_STAGE_ASSEMBLE, FP_STAGE_FACTOR, FP_STAGE_SOLVE, FP_STAGE_UIND, FP_STAGE_ADJOINT, FP_STAGE_VJP, FP_STAGE_POST, FP_STAGE_PHI = range(8)
 FP_UGRADMU_COMBINED, FP_UGRADMU_CELL, FP_UGRADMU_NODE = 0, 1, 2
 
 # every symbol the header declares

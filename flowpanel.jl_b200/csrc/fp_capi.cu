@@ -1063,7 +1063,12 @@ int fp_phi(fp_ctx* c, int element, const double* strengths, const double* target
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(dout, out, m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   const double* sigma = element == FP_ELEMENT_VORTEXRING ? nullptr : ds;
   const double* mu = element == FP_ELEMENT_SOURCE ? nullptr : (element == FP_ELEMENT_SOURCE_DOUBLET ? ds + c->N : ds);
+  double ms = 0;
+  if (time_begin(c)) return FP_ECUDA;
   if (int rc = launch_phi(c, sigma, mu, dt, m, dout, wake)) return rc;
+  if (time_end(c, &ms)) return FP_ECUDA;
+  c->kms[FP_STAGE_PHI] = ms;
+  c->klaunch[FP_STAGE_PHI] = 1;
   FP_CUDA_TRY(c->err, cudaMemcpyAsync(out, dout, m * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamSynchronize(c->stream));
   return FP_OK;
@@ -1381,7 +1386,7 @@ int fp_kernel_launches(fp_ctx* c, int64_t* count) {
 }
 
 int fp_last_kernel_ms(fp_ctx* c, int stage, double* ms, int* launches) {
-  if (check_ctx(c) || stage < 0 || stage > FP_STAGE_POST) return FP_EINVAL;
+  if (check_ctx(c) || stage < 0 || stage > FP_STAGE_PHI) return FP_EINVAL;
   if (ms) *ms = c->kms[stage];
   if (launches) *launches = c->klaunch[stage];
   return FP_OK;

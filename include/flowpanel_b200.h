@@ -375,6 +375,7 @@ int fp_last_kernel_ms(fp_ctx* ctx, int stage, double* ms, int* launches);
 #define FP_STAGE_ADJOINT 4   /* fp_adjoint_solve */
 #define FP_STAGE_VJP 5       /* fp_assembly_vjp / fp_uind_vjp */
 #define FP_STAGE_POST 6      /* fp_ugradmu / fp_surface_loads */
+#define FP_STAGE_PHI 7       /* fp_phi */
 
 /* Measurement utility (no counterpart in the reference): sustained FMA
  * throughput of the FP64 (fp64 = 1) or FP32 (fp64 = 0) pipe of a device, or of
