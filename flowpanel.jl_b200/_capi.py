@@ -33,6 +33,7 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
            "fp_set_tuning", "fp_autotune")
 FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH, FP_TUNE_TC_SMEM = 0, 1, 2, 3, 4
 FP_TUNE_FP64_DMMA, FP_TUNE_TC_SPLIT, FP_TUNE_TC_RED, FP_TUNE_ASM32, FP_TUNE_TC_NARROW = 5, 6, 7, 8, 9
+FP_TUNE_TRS2 = 10
 
 
 class SolveOpts(C.Structure):

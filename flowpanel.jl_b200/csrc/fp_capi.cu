@@ -109,6 +109,8 @@ void free_matrices(fp_ctx* c) {
   dfree(c->d_G); dfree(c->d_LU); dfree(c->d_G32); dfree(c->d_ipiv);
   dfree(c->d_dinv64); dfree(c->d_dinv32); dfree(c->d_flags); dfree(c->d_mbox); dfree(c->d_part);
   dfree(c->d_dinv128_64); dfree(c->d_dinv128_32); dfree(c->d_mprev64); dfree(c->d_mprev32);
+  dfree(c->d_mq32); dfree(c->d_ms32); dfree(c->d_zbox);
+  c->trs2_ready = false;
   if (c->d_minv) { cudaFree(c->d_minv); c->d_minv = nullptr; }
   dfree(c->d_rhs); dfree(c->d_x); dfree(c->d_r); dfree(c->d_w32); dfree(c->d_norms);
   dfree(c->d_V); dfree(c->d_h);
@@ -477,6 +479,11 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
     FP_CUDA_TRY(c->err, cudaMalloc(&c->d_mbox, words * sizeof(unsigned long long)));
     FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_mbox, 0, words * sizeof(unsigned long long), c->stream));
   }
+  if (!c->d_zbox) {
+    const size_t words = (size_t)((N + 127) / 128) * 128;
+    FP_CUDA_TRY(c->err, cudaMalloc(&c->d_zbox, words * sizeof(unsigned long long)));
+    FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_zbox, 0, words * sizeof(unsigned long long), c->stream));
+  }
   if (!c->d_part) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_part, (size_t)kGemvSplitHost * 4 * N * sizeof(double)));
   if (!c->d_minv) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_minv, kMinvBytes + (size_t)2 * kPanelSlots * kLuNB * sizeof(int)));
   if (precision == FP_PREC_FP64) {
@@ -493,6 +500,8 @@ static int alloc_factor_buffers(fp_ctx* c, int precision) {
       FP_CUDA_TRY(c->err, cudaMalloc(&c->d_dinv128_32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
     if (!c->d_mprev32)
       FP_CUDA_TRY(c->err, cudaMalloc(&c->d_mprev32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
+    if (!c->d_mq32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_mq32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
+    if (!c->d_ms32) FP_CUDA_TRY(c->err, cudaMalloc(&c->d_ms32, ((N + 127) / 128) * 2 * 128 * 128 * sizeof(float)));
   }
   return FP_OK;
 }
@@ -891,6 +900,10 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
     case FP_TUNE_FP64_DMMA:
       if (value < 0 || value > 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_FP64_DMMA is 0..6");
       c->fp64_dmma = value;
+      return FP_OK;
+    case FP_TUNE_TRS2:
+      c->trs_skip2 = value != 0;
+      if (!c->trs_skip2) c->trs2_ready = false;
       return FP_OK;
     case FP_TUNE_TC_NARROW:
       if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");

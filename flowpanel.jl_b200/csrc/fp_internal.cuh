@@ -99,6 +99,11 @@ struct fp_ctx {
   float* d_dinv128_32 = nullptr;        // inverses of the 128-row diagonal blocks (FP32 factors)
   double* d_mprev64 = nullptr;          // inv(D_bb) T(b, p) of each 128-row block's predecessor, per sweep (FP64)
   float* d_mprev32 = nullptr;           // the same for the FP32 factors
+  float* d_mq32 = nullptr;              // two-block sweep chain: R_b = Q_b - P_b P_{b-1} per block and sweep (FP32)
+  float* d_ms32 = nullptr;              // S_b = P_b Q_{b-1}
+  unsigned long long* d_zbox = nullptr; // the sweeps' second mailbox: z_b words (epoch, value)
+  bool trs_skip2 = false;               // FP32 sweeps: the two-block chain (FP_TUNE_TRS2)
+  bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)
   double* d_norms = nullptr;            // column norms (2 x cap_rhs)

@@ -1489,11 +1489,22 @@ __device__ __forceinline__ void load_tile4x16(const T* __restrict__ src, int64_t
   }
 }
 
-template <class T, bool LOWER>
+// SKIP2 (FP32 sweeps): the chain of dependent blocks runs two blocks at a
+// time. With P_b = inv(D_bb) T(b, b-1) (Mprev), Q_b = inv(D_bb) T(b, b-2)
+// (sweep order), z_b = inv(D_bb)(b_b - sum over s <= b-3 of T(b, s) y_s):
+//   y_b = z_b - P_b z_{b-1} + S_b y_{b-3} - R_b y_{b-2},
+//   R_b = Q_b - P_b P_{b-1} (Mq), S_b = P_b Q_{b-1} (Ms), formed once per
+// factorisation (k_mprev with distance 2, k_mprod). Block b publishes z_b to
+// the second mailbox zbox as soon as it has it; only R_b y_{b-2} waits for a
+// block's immediate chain, so the chain has n/256 steps instead of n/128.
+template <class T, bool LOWER, bool SKIP2 = false>
 __global__ void __launch_bounds__(kTrs1Threads)
 k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Dinv128, const T* __restrict__ Mprev,
        T* __restrict__ B, unsigned int* __restrict__ flags, unsigned int* __restrict__ ticket,
-       int* __restrict__ status, unsigned long long* __restrict__ mbox, unsigned epoch) {
+       int* __restrict__ status, unsigned long long* __restrict__ mbox, unsigned epoch,
+       const T* __restrict__ Mq = nullptr, const T* __restrict__ Ms = nullptr,
+       unsigned long long* __restrict__ zbox = nullptr) {
+  static_assert(!SKIP2 || sizeof(T) == 4, "the two-block chain is for the FP32 sweeps");
   extern __shared__ __align__(16) unsigned char tsm[];
   T (*Ds)[SB + 1] = reinterpret_cast<T (*)[SB + 1]>(tsm);                    // Ds[l][r] = inv(D)(r, l)
   T (*red)[SB] = reinterpret_cast<T (*)[SB]>(tsm + (size_t)SB * (SB + 1) * sizeof(T));   // per phase
@@ -1520,10 +1531,11 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
     T sum[4] = {T(0), T(0), T(0), T(0)};
     int64_t ready = 0;   // dependencies known complete (this warp)
     if constexpr (sizeof(T) == 4) {
-      // every earlier block but the predecessor, its values from its mailbox:
-      // lanes 0..15 poll the words of columns ph + 8 lane (spinning first,
-      // then backing off), the warp shares them by shuffles
-      for (int64_t s = 0; s + 1 < tk; ++s) {
+      // every earlier block but the predecessor (but the last two with
+      // SKIP2), its values from its mailbox: lanes 0..15 poll the words of
+      // columns ph + 8 lane (spinning first, then backing off), the warp
+      // shares them by shuffles
+      for (int64_t s = 0; s + (SKIP2 ? 2 : 1) < tk; ++s) {
         const int64_t cb = LOWER ? s : nblk - 1 - s;
         const int64_t c0 = cb * SB;
         const int cn = (int)imin64(SB, n - c0);
@@ -1601,7 +1613,55 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
       __syncthreads();
       if (h == 0) xfin[r] = s0 + xpart[r];
     }
-    if (tk > 0) {   // x_b = x' - Mprev_b y_p, on the chain
+    if constexpr (SKIP2) {
+      // z_b for the next block in sweep order; then
+      // y_b = z_b - (P_b z_{b-1} - S_b y_{b-3} + R_b y_{b-2}), the R_b term last
+      if (h == 0 && r < nb)
+        st_relaxed_u64(&zbox[k0 + r], ((unsigned long long)epoch << 32) | __float_as_uint(xfin[r]));
+      T s2[4] = {T(0), T(0), T(0), T(0)};
+      // s2 += sign M v over this thread's 4 rows x 16 columns, v the 128 words
+      // of block vb in box (lanes 0..15 poll columns ph + 8 lane)
+      auto add_mv = [&](const T* Mt, int64_t vb, const unsigned long long* box, T sign) {
+        const int64_t v0 = vb * SB;
+        const int nv = (int)imin64(SB, n - v0);
+        T mt[16][4];
+        load_tile4x16<T>(Mt, SB, rg, ph, nb, nv, mt);
+        float yl = 0.f;
+        const int col = ph + 8 * lane;
+        if (lane < 16 && col < nv) {
+          int spins = 0;
+          for (;;) {
+            const unsigned long long w = ld_relaxed_u64(&box[v0 + col]);
+            if ((unsigned)(w >> 32) == epoch) { yl = __uint_as_float((unsigned)w); break; }
+            if (++spins > kSpinLimit) { atomicOr(status, (int)DEV_TIMEOUT); stop_s = 1; break; }
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const T yv = sign * __shfl_sync(0xffffffffu, yl, i);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) s2[j] += mt[i][j] * yv;
+        }
+      };
+      const int64_t dir = LOWER ? -1 : 1;
+      const int64_t tile = (b * 2 + (LOWER ? 0 : 1)) * SB * SB;
+      if (tk >= 1) add_mv(Mprev + tile, b + dir, zbox, T(1));
+      if (tk >= 3) add_mv(Ms + tile, b + 3 * dir, mbox, T(-1));
+      if (tk >= 2) add_mv(Mq + tile, b + 2 * dir, mbox, T(1));   // on the chain
+#pragma unroll
+      for (int j = 0; j < 4; ++j) red[ph][4 * rg + j] = s2[j];
+      __syncthreads();
+      if (stop_s) return;
+      if (h == 0 && r < nb) {
+        T s0 = T(0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s0 += red[q][r];
+        const T xv = xfin[r] - s0;
+        st_relaxed_u64(&mbox[k0 + r], ((unsigned long long)epoch << 32) | __float_as_uint(xv));
+        B[k0 + r] = xv;
+      }
+    } else if (tk > 0) {   // x_b = x' - Mprev_b y_p, on the chain
       // the predecessor's tile Mprev_b, loaded before the wait
       const int64_t pb = LOWER ? b - 1 : b + 1;
       const int np = (int)imin64(SB, n - pb * SB);
@@ -1680,15 +1740,16 @@ k_trs1(const T* __restrict__ A, int64_t lda, int64_t n, const T* __restrict__ Di
 // columns). blockIdx.y: 0 forward, 1 backward.
 template <class T>
 __global__ void __launch_bounds__(256)
-k_mprev(const T* __restrict__ LU, int64_t lda, int64_t n, const T* __restrict__ Dinv128, T* __restrict__ Mprev) {
+k_mprev(const T* __restrict__ LU, int64_t lda, int64_t n, const T* __restrict__ Dinv128, T* __restrict__ Mprev,
+        int dist = 1) {
   constexpr int KC = sizeof(T) == 4 ? 32 : 16;
   __shared__ __align__(16) T Dsh[KC][SB + 4];   // Dsh[l][r] = inv(D)(r, l0 + l)
   __shared__ __align__(16) T Tsh[KC][SB + 4];   // Tsh[l][c] = T(l0 + l, c)
   const int64_t nblk = (n + SB - 1) / SB;
   const int64_t b = blockIdx.x;
   const bool lower = blockIdx.y == 0;
-  const int64_t p = lower ? b - 1 : b + 1;
-  if (p < 0 || p >= nblk) return;   // the sweep's first block has no predecessor
+  const int64_t p = lower ? b - dist : b + dist;
+  if (p < 0 || p >= nblk) return;   // the sweep's first blocks have no such predecessor
   const int64_t k0 = b * SB, p0 = p * SB;
   const int nb = (int)imin64(SB, n - k0), np = (int)imin64(SB, n - p0);
   const T* Di = Dinv128 + b * 2 * SB * SB + (lower ? 0 : SB * SB);
@@ -1724,6 +1785,66 @@ k_mprev(const T* __restrict__ LU, int64_t lda, int64_t n, const T* __restrict__ 
   for (int j = 0; j < 8; ++j)
 #pragma unroll
     for (int i = 0; i < 8; ++i) out[(c0 + j) * SB + r0 + i] = acc[i][j];
+}
+
+// The products of the two-block sweep chain, per 128-row block b and sweep
+// (sweep order: p1, p2 = the blocks one and two before b):
+//   job 0: Ms_b = P_b Q_{p1}            (b at sweep position >= 3)
+//   job 1: Mq_b = Q_b - P_b P_{p1}       (b at sweep position >= 2, in place)
+// P = Mprev, Q = Mq as k_mprev left it (distance 2); SB x SB column-major
+// tiles whose columns beyond a partial block are zero. Job 0 runs before
+// job 1 (it reads Q_{p1}).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_mprod(const T* __restrict__ P, T* __restrict__ Q, T* __restrict__ S, int64_t n, int job) {
+  constexpr int KC = sizeof(T) == 4 ? 32 : 16;
+  __shared__ __align__(16) T Ysh[KC][SB + 4];   // Ysh[l][r] = P_b(r, l0 + l)
+  __shared__ __align__(16) T Zsh[KC][SB + 4];   // Zsh[l][c] = Z(l0 + l, c)
+  const int64_t nblk = (n + SB - 1) / SB;
+  const int64_t b = blockIdx.x;
+  const bool lower = blockIdx.y == 0;
+  const int64_t tk = lower ? b : nblk - 1 - b;
+  if (tk < (job == 0 ? 3 : 2)) return;
+  const int64_t p1 = lower ? b - 1 : b + 1;
+  const int64_t tb = (b * 2 + (lower ? 0 : 1)) * SB * SB, tp = (p1 * 2 + (lower ? 0 : 1)) * SB * SB;
+  const T* Y = P + tb;
+  const T* Z = job == 0 ? Q + tp : P + tp;
+  T* out = job == 0 ? S + tb : Q + tb;
+  const int tid = threadIdx.x;
+  const int r0 = 8 * (tid & 15), c0 = 8 * (tid >> 4);
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+  for (int l0 = 0; l0 < SB; l0 += KC) {
+    __syncthreads();
+    for (int e = tid; e < KC * SB; e += 256) {
+      const int r = e % SB, l = e / SB;
+      Ysh[l][r] = Y[(l0 + l) * SB + r];
+      const int ll = e % KC, c = e / KC;
+      Zsh[ll][c] = Z[c * SB + l0 + ll];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int l = 0; l < KC; ++l) {
+      T x[8], y[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) { x[i] = Ysh[l][r0 + i]; y[i] = Zsh[l][c0 + i]; }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] += x[i] * y[j];
+    }
+  }
+  __syncthreads();   // job 1 overwrites Q_b, which no other block of this launch reads
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int64_t o = (int64_t)(c0 + j) * SB + r0 + i;
+      out[o] = job == 0 ? acc[i][j] : out[o] - acc[i][j];
+    }
 }
 
 // Inverses of the 128-row diagonal blocks from those of the 64-row blocks:
@@ -1817,6 +1938,16 @@ static int run_trs1(fp_ctx* c, const T* A, int64_t n, int64_t lda, const T* Dinv
   FP_CUDA_TRY(c->err, cudaMemsetAsync(c->d_flags, 0, (nblk + 1) * sizeof(unsigned int), c->stream));
   const unsigned grid = (unsigned)std::min<int64_t>(nblk, 2 * num_sms());
   if (++c->trs_epoch == 0) ++c->trs_epoch;   // epoch 0 marks words never written
+  if constexpr (sizeof(T) == 4) {
+    if (c->trs_skip2 && c->trs2_ready) {
+      k_trs1<float, LOWER, true><<<grid, kTrs1Threads, trs1_smem<T>(), c->stream>>>(
+          A, lda, n, Dinv128, Mprev, B, c->d_flags, c->d_flags + nblk, c->d_status, c->d_mbox, c->trs_epoch,
+          c->d_mq32, c->d_ms32, c->d_zbox);
+      ++c->nlaunch;
+      FP_CUDA_TRY(c->err, cudaGetLastError());
+      return FP_OK;
+    }
+  }
   k_trs1<T, LOWER><<<grid, kTrs1Threads, trs1_smem<T>(), c->stream>>>(A, lda, n, Dinv128, Mprev, B, c->d_flags,
                                                                       c->d_flags + nblk, c->d_status, c->d_mbox,
                                                                       c->trs_epoch);
@@ -1890,6 +2021,11 @@ int lu_solve(fp_ctx* c, const T* LU, int64_t n, int64_t lda, const int32_t* ipiv
     static SmemAttr attr_lo, attr_up;
     FP_CUDA_TRY(c->err, attr_lo.ensure(k_trs1<T, true>, (int)trs1_smem<T>()));
     FP_CUDA_TRY(c->err, attr_up.ensure(k_trs1<T, false>, (int)trs1_smem<T>()));
+    if constexpr (sizeof(T) == 4) {
+      static SmemAttr attr_lo2, attr_up2;
+      FP_CUDA_TRY(c->err, attr_lo2.ensure(k_trs1<float, true, true>, (int)trs1_smem<T>()));
+      FP_CUDA_TRY(c->err, attr_up2.ensure(k_trs1<float, false, true>, (int)trs1_smem<T>()));
+    }
     if (int rc = run_trs1<T, true>(c, LU, n, lda, D128, Mp, B)) return rc;
     return run_trs1<T, false>(c, LU, n, lda, D128, Mp, B);
   }
@@ -1917,9 +2053,23 @@ int lu_diag_inverses(fp_ctx* c, const T* LU, int64_t n, int64_t lda) {
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   T* Mp = reinterpret_cast<T*>(sizeof(T) == 8 ? (void*)c->d_mprev64 : (void*)c->d_mprev32);
-  k_mprev<T><<<dim3((unsigned)((n + SB - 1) / SB), 2), 256, 0, c->stream>>>(LU, lda, n, D128, Mp);
+  const dim3 gm((unsigned)((n + SB - 1) / SB), 2);
+  k_mprev<T><<<gm, 256, 0, c->stream>>>(LU, lda, n, D128, Mp);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
+  if constexpr (sizeof(T) == 4) {
+    // the two-block chain of the FP32 sweeps: Q (distance 2), then S = P Q_p1,
+    // then R = Q - P P_p1 in place of Q
+    c->trs2_ready = false;
+    if (c->trs_skip2 && c->d_mq32 && c->d_ms32 && c->d_zbox) {
+      k_mprev<float><<<gm, 256, 0, c->stream>>>(LU, lda, n, D128, c->d_mq32, 2);
+      k_mprod<float><<<gm, 256, 0, c->stream>>>(c->d_mprev32, c->d_mq32, c->d_ms32, n, 0);
+      k_mprod<float><<<gm, 256, 0, c->stream>>>(c->d_mprev32, c->d_mq32, c->d_ms32, n, 1);
+      c->nlaunch += 3;
+      FP_CUDA_TRY(c->err, cudaGetLastError());
+      c->trs2_ready = true;
+    }
+  }
   return FP_OK;
 }
 

@@ -429,7 +429,15 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       (2.49 ms)
  *   FP_TUNE_TC_NARROW   6 (default): the update of one column of tiles (the next
  *                       panel's columns, on the critical path) uses a 6-stage
- *                       ring; 0: the same ring as the other updates */
+ *                       ring; 0: the same ring as the other updates
+ *   FP_TUNE_TRS2        1: the FP32 triangular sweeps of the refinement run their
+ *                       chain of dependent 128-row blocks two blocks a step
+ *                       (products formed once per factorisation); 0 (default):
+ *                       one block a step, which measured faster on the 12k wing
+ *                       (solve stage 2.38 against 2.51 ms: the two-step form
+ *                       also needs the block three back, which arrives just
+ *                       before the block two back). Takes effect at the next
+ *                       fp_factor */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -440,6 +448,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_TC_RED 7
 #define FP_TUNE_ASM32 8
 #define FP_TUNE_TC_NARROW 9
+#define FP_TUNE_TRS2 10
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

@@ -47,7 +47,7 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
 @pytest.mark.parametrize("nc,ns", [(8, 4), (12, 8), (20, 24), (40, 48), (60, 80), (50, 30)])
 @pytest.mark.parametrize("knob,value", [("FP_TUNE_TC_SPLIT", 1), ("FP_TUNE_TC_SPLIT", 2), ("FP_TUNE_TC_SPLIT", 3),
                                         ("FP_TUNE_TC_RED", 0), ("FP_TUNE_TC_TILES", 2), ("FP_TUNE_TC_TILES", 4),
-                                        ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0)])
+                                        ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0), ("FP_TUNE_TRS2", 1)])
 def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
     1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
@@ -55,7 +55,8 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     reduce-add instead of red.global; FP_TUNE_TC_TILES runs the multi-tile
     kernel (double-buffered accumulator, red.global epilogue); FP_TUNE_ASM32
     assembles the FP32 AIC in panel-local FP32 coordinates and the FP64 AIC
-    on a background stream. The factors are as accurate as the default's (refinement
+    on a background stream; FP_TUNE_TRS2 1 runs the FP32 sweeps' chain two
+    blocks a step. The factors are as accurate as the default's (refinement
     in a handful of steps, the oracle's solution to 1e-10), for one partial
     panel up to many panels with a partial last one (1,500 panels: a last K
     block of 92)."""
