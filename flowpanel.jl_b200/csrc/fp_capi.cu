@@ -853,6 +853,12 @@ int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
     const std::vector<int> saved = current_knobs(c);
     const int element = c->assembled, aprec = c->assembled_prec;
     const double off = c->kern_offset, cut = c->kern_cutoff;
+    // on an error the caller's knobs come back before the status is returned
+    auto fail = [&](int rc) {
+      const std::string msg = c->err.msg;
+      for (int k = 0; k < (int)saved.size(); ++k) fp_set_tuning(c, k, saved[k]);
+      return c->err.set(rc, msg);
+    };
     double best = 1e300;
     std::vector<int> best_knobs = saved;
     for (const auto& cfg : cand) {
@@ -862,8 +868,8 @@ int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
       for (int r = 0; r < reps + 1; ++r) {   // the first run warms the kernels up
         // the FP32 factorisations work in place on the FP32 AIC: assemble it again
         if (precision != FP_PREC_FP64 && precision != FP_PREC_BF16)
-          if (int rc = fp_assemble(c, element, off, cut, aprec)) return rc;
-        if (int rc = fp_factor(c, precision)) return rc;
+          if (int rc = fp_assemble(c, element, off, cut, aprec)) return fail(rc);
+        if (int rc = fp_factor(c, precision)) return fail(rc);
         if (r > 0) ms.push_back(c->ms_factor);
       }
       std::sort(ms.begin(), ms.end());
@@ -872,7 +878,7 @@ int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
     }
     hit = c->tuned.emplace(key, best_knobs).first;
     // leave the context assembled, not factored
-    if (int rc = fp_assemble(c, element, off, cut, aprec)) return rc;
+    if (int rc = fp_assemble(c, element, off, cut, aprec)) return fail(rc);
   }
   for (int k = 0; k < (int)hit->second.size(); ++k) fp_set_tuning(c, k, hit->second[k]);
   if (knobs_out)
