@@ -185,7 +185,7 @@ def surface_loads_timing(fp, reps=5):
 
 
 TRACE_TAGS = {0: "diagonal block", 1: "L21 (rows below)", 2: "U12 (next panel)", 3: "U12 (columns beyond)",
-              4: "tcgen05 update", 5: "split A", 6: "split B", 7: "SIMT update"}
+              4: "tcgen05 update", 5: "split A", 6: "split B", 7: "SIMT update", 8: "panel inverses"}
 
 
 def factor_timeline(ctx, cap, prec):

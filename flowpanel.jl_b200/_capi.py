@@ -34,6 +34,8 @@ EXPORTS = ("fp_ctx_create", "fp_ctx_destroy", "fp_last_error", "fp_device_count"
 FP_TUNE_TC_STAGES, FP_TUNE_LU_OVERLAP, FP_TUNE_TC_TILES, FP_TUNE_GRAPH, FP_TUNE_TC_SMEM = 0, 1, 2, 3, 4
 FP_TUNE_FP64_DMMA, FP_TUNE_TC_SPLIT, FP_TUNE_TC_RED, FP_TUNE_ASM32, FP_TUNE_TC_NARROW = 5, 6, 7, 8, 9
 FP_TUNE_TRS2 = 10
+FP_TUNE_PANEL_GEMM = 11
+FP_TUNE_TC_BF16X3 = 12
 
 
 class SolveOpts(C.Structure):

@@ -911,6 +911,13 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       c->trs_skip2 = value != 0;
       if (!c->trs_skip2) c->trs2_ready = false;
       return FP_OK;
+    case FP_TUNE_PANEL_GEMM:
+      if (value < 0 || value > 2) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_PANEL_GEMM is 0..2");
+      c->panel_gemm = value;
+      return FP_OK;
+    case FP_TUNE_TC_BF16X3:
+      c->tc_x3 = value != 0;
+      return FP_OK;
     case FP_TUNE_TC_NARROW:
       if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");
       c->tc_narrow_stages = value;

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <string>
@@ -103,6 +104,8 @@ struct fp_ctx {
   float* d_ms32 = nullptr;              // S_b = P_b Q_{b-1}
   unsigned long long* d_zbox = nullptr; // the sweeps' second mailbox: z_b words (epoch, value)
   bool trs_skip2 = false;               // FP32 sweeps: the two-block chain (FP_TUNE_TRS2)
+  int panel_gemm = 0;                   // static-order LU: 1 full panel inverses, GEMM-form L21 / U12; 2: with k_pdiag2 (FP_TUNE_PANEL_GEMM)
+  bool tc_x3 = false;                   // mixed form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)
@@ -234,7 +237,10 @@ int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, doub
 constexpr int kLuNB = 64;        // block size of the factorisation and the solves
 constexpr int kOuterPanel = 256;  // columns per outer panel of the factorisation
 constexpr int kPanelSlots = kOuterPanel / kLuNB;   // blocks per outer panel
-constexpr size_t kMinvBytes = (size_t)2 * kPanelSlots * kLuNB * kLuNB * sizeof(double);   // two sets
+// two sets of the pivoted LU's block inverses, or two panel slots of the
+// static-order LU (its 32 x 32 inverses and the full 128 x 128 inverses)
+constexpr size_t kMinvBytes = std::max((size_t)2 * kPanelSlots * kLuNB * kLuNB * sizeof(double),
+                                       (size_t)2 * (8 * 32 * 32 + 2 * 128 * 128) * sizeof(float));
 // split-operand scratch of the tensor-core update for scratch set `slot` (fp_tc.cu)
 int ensure_tc_scratch(fp_ctx* c, int slot, int64_t rows_max);
 constexpr int kGemvSplitHost = 16;
@@ -246,6 +252,8 @@ constexpr int kStaticPanel = 128;
 int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert, bool bf16 = false);
 bool tc_gemm_sub_bf16(fp_ctx* c, const void* Ah, const void* Bh, int ldk, float* C, int64_t ldc, int64_t m,
                       int64_t nn, int kk);
+bool tc_gemm_sub_bf16x3(fp_ctx* c, const void* Ah, const void* Al, const void* Bh, const void* Bl, int ldk, float* C,
+                        int64_t ldc, int64_t m, int64_t nn, int kk);
 // b = FP32 copy of the FP64 a rounded to BF16 values
 int convert_f64_bf16(fp_ctx* c, const double* a, float* b, int64_t n, int64_t k, int64_t lda, int64_t ldb);
 // FP32 trailing update on tensor cores (fp_tc.cu); returns false if the
@@ -367,7 +375,7 @@ inline void kt_collect(fp_ctx* c) {
 
 // Trace: tr_event records one event on the current stream and returns its
 // slot (-1 when tracing is off); TraceScope brackets one launch.
-enum TraceTag { TR_DIAG = 0, TR_L21 /* k_blk */, TR_U12 /* k_pfix */, TR_STRIP, TR_GEMM_TC, TR_SPLIT_A, TR_SPLIT_B, TR_GEMM_SIMT };
+enum TraceTag { TR_DIAG = 0, TR_L21 /* k_blk */, TR_U12 /* k_pfix */, TR_STRIP, TR_GEMM_TC, TR_SPLIT_A, TR_SPLIT_B, TR_GEMM_SIMT, TR_PINV };
 inline int tr_event(fp_ctx* c) {
   Trace& t = c->trace;
   if (!t.on) return -1;

@@ -90,34 +90,71 @@ __device__ __forceinline__ void piece(int q, int& r, int& c) {
     r = (q % R4) * 4;
   }
 }
+// A block in flight: fetch() issues all of a thread's 16-byte loads, put()
+// stores them to shared memory, so that a kernel can issue the loads of all
+// its blocks before the first store (one round trip to L2 / HBM, not one a
+// block).
+template <int NT, int ROWS, int COLS>
+struct Staged {
+  static constexpr int R4 = ROWS / 4, NV = R4 * COLS, PER = (NV + NT - 1) / NT;
+  float4 v[PER];
+  template <class Pad>
+  __device__ __forceinline__ void fetch(const float* __restrict__ g, int64_t ld, int rows, int cols, Pad pad, int tid) {
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int q = tid + u * NT;
+      int r, c;
+      piece<ROWS, COLS>(q, r, c);
+      if (q < NV && c < cols && r + 4 <= rows) {
+        v[u] = __ldcg(reinterpret_cast<const float4*>(g + (int64_t)c * ld + r));
+      } else if (q < NV) {
+        float t[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) t[i] = (c < cols && r + i < rows) ? __ldcg(g + (int64_t)c * ld + r + i) : pad(r + i, c);
+        v[u] = make_float4(t[0], t[1], t[2], t[3]);
+      }
+    }
+  }
+  template <class S>
+  __device__ __forceinline__ void put(S s, int tid) const {
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int q = tid + u * NT;
+      if (q < NV) {
+        int r, c;
+        piece<ROWS, COLS>(q, r, c);
+        s(r, c, v[u].x); s(r + 1, c, v[u].y); s(r + 2, c, v[u].z); s(r + 3, c, v[u].w);
+      }
+    }
+  }
+};
+// The four IB x IB inverses of one kind (which = 0: L, 1: U) of a panel's
+// dinv into dst (inverse t's row r at dst[t * IB + r]) by asynchronous
+// 16-byte copies (cp.async: no registers, all in flight at once); the caller
+// waits with cp_async_wait_all() before its __syncthreads.
+template <int NT, int P>
+__device__ __forceinline__ void copy_inv_async(float (*dst)[P], const float* __restrict__ dinv, int which, int tid) {
+  constexpr int NV = NIB * IB * IB / 4;
+  static_assert(P % 4 == 0, "16-byte rows");
+#pragma unroll
+  for (int u = 0; u < (NV + NT - 1) / NT; ++u) {
+    const int e = tid + u * NT;
+    if (e < NV) {
+      const int t = e / (IB * IB / 4), r = (e / (IB / 4)) % IB, c = (e % (IB / 4)) * 4;
+      const uint32_t d = (uint32_t)__cvta_generic_to_shared(&dst[t * IB + r][c]);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(&dinv[dinv_off(t, which) + r * IB + c])
+                   : "memory");
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 template <int NT, int ROWS, int COLS, class S, class Pad>
 __device__ __forceinline__ void load_block(const float* __restrict__ g, int64_t ld, int rows, int cols, S s, Pad pad,
                                            int tid) {
-  constexpr int R4 = ROWS / 4, NV = R4 * COLS, PER = (NV + NT - 1) / NT;
-  float4 v[PER];
-#pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int q = tid + u * NT;
-    int r, c;
-    piece<ROWS, COLS>(q, r, c);
-    if (q < NV && c < cols && r + 4 <= rows) {
-      v[u] = __ldcg(reinterpret_cast<const float4*>(g + (int64_t)c * ld + r));
-    } else if (q < NV) {
-      float t[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) t[i] = (c < cols && r + i < rows) ? __ldcg(g + (int64_t)c * ld + r + i) : pad(r + i, c);
-      v[u] = make_float4(t[0], t[1], t[2], t[3]);
-    }
-  }
-#pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int q = tid + u * NT;
-    if (q < NV) {
-      int r, c;
-      piece<ROWS, COLS>(q, r, c);
-      s(r, c, v[u].x); s(r + 1, c, v[u].y); s(r + 2, c, v[u].z); s(r + 3, c, v[u].w);
-    }
-  }
+  Staged<NT, ROWS, COLS> b;
+  b.fetch(g, ld, rows, cols, pad, tid);
+  b.put(s, tid);
 }
 template <int NT, int ROWS, int COLS, class S>
 __device__ __forceinline__ void store_block(float* __restrict__ g, int64_t ld, int rows, int cols, S s, int tid) {
@@ -414,16 +451,16 @@ k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, cons
   const int tid = threadIdx.x;
   const int64_t row0 = r0 + (int64_t)blockIdx.x * L21_ROWS;
   const int rows = (int)imin64(L21_ROWS, n - row0);
-  load_block<L21_THREADS, L21_ROWS, PW>(
-      A + k * lda + row0, lda, rows, PW, [&](int r, int c, float v) { X[r][c] = v; }, [](int, int) { return 0.f; },
-      tid);
-  load_block<L21_THREADS, PW - IB, PW - IB>(
-      A + (k + IB) * lda + k, lda, PW - IB, PW - IB, [&](int r, int c, float v) { Ub[r][c] = v; },
-      [](int, int) { return 0.f; }, tid);
-  for (int e = tid; e < NIB * IB * IB / 4; e += L21_THREADS) {
-    const int t = e / (IB * IB / 4), r = (e / (IB / 4)) % IB, c = (e % (IB / 4)) * 4;
-    *reinterpret_cast<float4*>(&Ut[t * IB + r][c]) =
-        __ldcg(reinterpret_cast<const float4*>(&dinv[dinv_off(t, 1) + r * IB + c]));
+  {   // all loads in flight before the first store
+    const auto zero = [](int, int) { return 0.f; };
+    Staged<L21_THREADS, L21_ROWS, PW> xs;
+    Staged<L21_THREADS, PW - IB, PW - IB> us;
+    copy_inv_async<L21_THREADS>(Ut, dinv, 1, tid);
+    xs.fetch(A + k * lda + row0, lda, rows, PW, zero, tid);
+    us.fetch(A + (k + IB) * lda + k, lda, PW - IB, PW - IB, zero, tid);
+    xs.put([&](int r, int c, float v) { X[r][c] = v; }, tid);
+    us.put([&](int r, int c, float v) { Ub[r][c] = v; }, tid);
+    cp_async_wait_all();
   }
   __syncthreads();
   const int rg = tid & 15, cg = tid >> 4;   // 16 row pairs x 8 column quads = 32 x 32
@@ -526,16 +563,16 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
   const int tid = threadIdx.x;
   const int64_t col0 = c0 + (int64_t)blockIdx.x * CW;
   const int cols = (int)imin64(CW, c1 - col0);
-  load_block<T, PW, CW>(
-      A + col0 * lda + k, lda, PW, cols, [&](int r, int c, float v) { Z[r][c] = v; }, [](int, int) { return 0.f; },
-      tid);
-  load_block<T, PW - IB, PW - IB>(
-      A + k * lda + k + IB, lda, PW - IB, PW - IB, [&](int r, int s, float v) { Lb[r][s] = v; },
-      [](int, int) { return 0.f; }, tid);
-  for (int e = tid; e < NIB * IB * IB / 4; e += T) {
-    const int t = e / (IB * IB / 4), r = (e / (IB / 4)) % IB, c = (e % (IB / 4)) * 4;
-    *reinterpret_cast<float4*>(&Lt[t * IB + r][c]) =
-        __ldcg(reinterpret_cast<const float4*>(&dinv[dinv_off(t, 0) + r * IB + c]));
+  {   // all loads in flight before the first store
+    const auto zero = [](int, int) { return 0.f; };
+    Staged<T, PW, CW> zs;
+    Staged<T, PW - IB, PW - IB> ls;
+    copy_inv_async<T>(Lt, dinv, 0, tid);
+    zs.fetch(A + col0 * lda + k, lda, PW, cols, zero, tid);
+    ls.fetch(A + k * lda + k + IB, lda, PW - IB, PW - IB, zero, tid);
+    zs.put([&](int r, int c, float v) { Z[r][c] = v; }, tid);
+    ls.put([&](int r, int s, float v) { Lb[r][s] = v; }, tid);
+    cp_async_wait_all();
   }
   __syncthreads();
   constexpr int CQ = CW / 4;
@@ -601,6 +638,444 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
   }
 }
 
+// ---------------------------------------------------------------------------
+// The GEMM form of K6 / K2 (FP_TUNE_PANEL_GEMM 1, 2). K1b k_pinv forms the
+// full inverses of the diagonal block's factors once a panel; L21 = A21 inv(U)
+// and U12 = inv(L) A12 are then one triangular product each: one K loop a
+// thread, no dependent steps and no barriers between them.
+//
+// Per panel slot of the scratch, after dinv: inv(L)^T (PW x PW; row s holds
+// column s of inv(L)) and inv(U) (PW x PW, row-major), both written whole
+// (zeros outside the triangle).
+constexpr int kInvFloats = PW * PW;
+constexpr int kSlotFloats = kDinvFloats + 2 * kInvFloats;
+constexpr int kLinvtOff = kDinvFloats, kUinvOff = kDinvFloats + kInvFloats;
+constexpr int GP = PW + 4;   // pitch of 128-float rows in shared memory (16-byte rows, 4 banks apart)
+constexpr int DP = IB + 4;   // pitch of 32-float rows
+
+// One 16-byte asynchronous copy global -> shared; bytes < 16 copies that many
+// and zero-fills the rest (bytes = 0: no global read).
+__device__ __forceinline__ void cp16(void* sdst, const float* gsrc, int bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+// PW x PW floats, row-major at g with pitch PW, into dst (pitch GP)
+template <int NT>
+__device__ __forceinline__ void copy_square_async(float (*dst)[GP], const float* __restrict__ g, int tid) {
+#pragma unroll
+  for (int u = 0; u < PW * PW / 4 / NT; ++u) {
+    const int e = tid + u * NT, r = e / (PW / 4), c = (e % (PW / 4)) * 4;
+    cp16(&dst[r][c], g + (size_t)r * PW + c, 16);
+  }
+}
+
+// K1 with FP_TUNE_PANEL_GEMM 2: the diagonal block by right-looking
+// elimination, one pivot a step. 256 threads, each holding an 8 x 8 tile of
+// the block in registers (warp w: rows 32 (w >> 1) .. +32, columns
+// 64 (w & 1) .. +64). Before step kk the owners of column kk and row kk have
+// posted them to a double-buffered shared array (column entries below the
+// pivot, row entries right of it, zeros elsewhere; the pivot apart); after one
+// __syncthreads every warp whose region reaches the trailing block applies the
+// rank-1 update A(i, j) -= A(i, kk) / A(kk, kk) A(kk, j). The columns below
+// the pivots keep their unscaled values until the end, when they are divided
+// by the pivots (L). Little code and one barrier a pivot; the inverses of L
+// and U come from k_pinv<true>.
+constexpr int PD2_THREADS = 256;
+__global__ void __launch_bounds__(PD2_THREADS, 1)
+k_pdiag2(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ cert, int* __restrict__ status) {
+  __shared__ __align__(16) float colb[2][PW];
+  __shared__ __align__(16) float rowb[2][PW];
+  __shared__ __align__(16) float pivs[PW];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = 32 * (warp >> 1) + 8 * (lane >> 3), c0 = 64 * (warp & 1) + 8 * (lane & 7);
+  const int rw1 = 32 * (warp >> 1) + 31, cw1 = 64 * (warp & 1) + 63;   // last row / column of the warp's region
+  const int nb = (int)imin64(PW, n - k);
+  float t[8][8];
+  {
+    float4 v[8][2];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int c = c0 + b;
+      if (c < nb && r0 + 8 <= nb) {
+        const float4* p = reinterpret_cast<const float4*>(A + (k + c) * lda + k + r0);
+        v[b][0] = __ldcg(p);
+        v[b][1] = __ldcg(p + 1);
+      } else {
+        float s[8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+          s[a] = (c < nb && r0 + a < nb) ? __ldcg(A + (k + c) * lda + k + r0 + a) : (r0 + a == c ? 1.f : 0.f);
+        v[b][0] = make_float4(s[0], s[1], s[2], s[3]);
+        v[b][1] = make_float4(s[4], s[5], s[6], s[7]);
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      t[0][b] = v[b][0].x; t[1][b] = v[b][0].y; t[2][b] = v[b][0].z; t[3][b] = v[b][0].w;
+      t[4][b] = v[b][1].x; t[5][b] = v[b][1].y; t[6][b] = v[b][1].z; t[7][b] = v[b][1].w;
+    }
+  }
+  // the owners of column kk and row kk post them for step kk (buffer kk & 1)
+  const auto post = [&](int kk) {
+    float* const cb = colb[kk & 1];
+    float* const rb = rowb[kk & 1];
+    const int bc = kk - c0, ar = kk - r0;
+    switch (bc) {   // column kk of this tile: a static column in each case
+#define FP_PD2_COL(B)                                                        \
+  case B:                                                                    \
+    _Pragma("unroll") for (int a = 0; a < 8; ++a) {                          \
+      cb[r0 + a] = (r0 + a > kk) ? t[a][B] : 0.f;                            \
+      if (r0 + a == kk) pivs[kk] = t[a][B];                                  \
+    }                                                                        \
+    break;
+      FP_PD2_COL(0) FP_PD2_COL(1) FP_PD2_COL(2) FP_PD2_COL(3) FP_PD2_COL(4) FP_PD2_COL(5) FP_PD2_COL(6) FP_PD2_COL(7)
+#undef FP_PD2_COL
+      default: break;
+    }
+    switch (ar) {   // row kk of this tile
+#define FP_PD2_ROW(R)                                                                          \
+  case R:                                                                                      \
+    _Pragma("unroll") for (int b = 0; b < 8; ++b) rb[c0 + b] = (c0 + b > kk) ? t[R][b] : 0.f; \
+    break;
+      FP_PD2_ROW(0) FP_PD2_ROW(1) FP_PD2_ROW(2) FP_PD2_ROW(3) FP_PD2_ROW(4) FP_PD2_ROW(5) FP_PD2_ROW(6) FP_PD2_ROW(7)
+#undef FP_PD2_ROW
+      default: break;
+    }
+  };
+  post(0);
+  __syncthreads();
+#pragma unroll 1
+  for (int kk = 0; kk < PW - 1; ++kk) {
+    if (rw1 > kk && cw1 > kk) {   // warp-uniform: the region reaches the trailing block
+      const float rp = rcp_fast(pivs[kk]);
+      const float4* cp = reinterpret_cast<const float4*>(&colb[kk & 1][r0]);
+      const float4* rq = reinterpret_cast<const float4*>(&rowb[kk & 1][c0]);
+      const float4 l0 = cp[0], l1 = cp[1], u0 = rq[0], u1 = rq[1];
+      const float l[8] = {l0.x * rp, l0.y * rp, l0.z * rp, l0.w * rp, l1.x * rp, l1.y * rp, l1.z * rp, l1.w * rp};
+      const float u[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) t[a][b] = fmaf(-l[a], u[b], t[a][b]);
+    }
+    post(kk + 1);
+    __syncthreads();
+  }
+  // L below the diagonal: the column values over their pivots
+  float lmax = 0.f;
+  {
+    const float4 p0 = *reinterpret_cast<const float4*>(&pivs[c0]), p1 = *reinterpret_cast<const float4*>(&pivs[c0 + 4]);
+    const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const float rp = rcp_fast(pv[b]);
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+        if (r0 + a > c0 + b) {
+          t[a][b] *= rp;
+          lmax = fmaxf(lmax, fabsf(t[a][b]));
+        }
+    }
+  }
+  if (tid < nb) {
+    const float p = pivs[tid];
+    if (!(fabsf(p) > 0.f && fabsf(p) <= FLT_MAX)) atomicOr(status, (int)DEV_ZERO_PIVOT);
+  }
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const int c = c0 + b;
+    if (c >= nb) continue;
+    float* const g = A + (k + c) * lda + k + r0;
+    if (r0 + 8 <= nb) {
+      reinterpret_cast<float4*>(g)[0] = make_float4(t[0][b], t[1][b], t[2][b], t[3][b]);
+      reinterpret_cast<float4*>(g)[1] = make_float4(t[4][b], t[5][b], t[6][b], t[7][b]);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+        if (r0 + a < nb) g[a] = t[a][b];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
+  if (lane == 0) atomic_max_pos(cert, lmax);
+}
+
+// The IB x IB diagonal-block inverses from the staged factored block G
+// (G[p][q] = column p, row q): lane c forms column c, of inv(L_ii) by
+// substitution down column m of L (unit diagonal), of inv(U_ii) up column m of
+// U; both read contiguous columns. dst[r][c] = the inverse's (r, c).
+__device__ __forceinline__ void inv_block_lower(const float (*G)[GP], int ib, int lane, float (*dst)[DP]) {
+  float y[IB];
+#pragma unroll
+  for (int r = 0; r < IB; ++r) y[r] = (r == lane) ? 1.f : 0.f;
+#pragma unroll
+  for (int m = 0; m < IB - 1; ++m) {   // y(r) -= L(r, m) y(m), r > m
+#pragma unroll
+    for (int g = 0; g < IB / 4; ++g) {
+      if (4 * g + 3 <= m) continue;
+      const float4 q = *reinterpret_cast<const float4*>(&G[ib + m][ib + 4 * g]);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * g + e > m) y[4 * g + e] = fmaf(-qv[e], y[m], y[4 * g + e]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < IB; ++r) dst[r][lane] = y[r];
+}
+__device__ __forceinline__ void inv_block_upper(const float (*G)[GP], int ib, int lane, float (*dst)[DP]) {
+  float x[IB];
+#pragma unroll
+  for (int r = 0; r < IB; ++r) x[r] = (r == lane) ? 1.f : 0.f;
+#pragma unroll
+  for (int m = IB - 1; m >= 0; --m) {   // x(m) /= U(m, m); x(r) -= U(r, m) x(m), r < m
+    x[m] *= rcp_fast(G[ib + m][ib + m]);
+#pragma unroll
+    for (int g = 0; g < IB / 4; ++g) {
+      if (4 * g >= m) continue;
+      const float4 q = *reinterpret_cast<const float4*>(&G[ib + m][ib + 4 * g]);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4 * g + e < m) x[4 * g + e] = fmaf(-qv[e], x[m], x[4 * g + e]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < IB; ++r) dst[r][lane] = x[r];
+}
+
+// K1b: 2 NIB CTAs. CTA b < NIB forms block column j = b of inv(L), CTA
+// b >= NIB block column j = b - NIB of inv(U^T) = inv(U)^T; both are the
+// inverse of a lower-triangular M from its diagonal-block inverses D_i:
+//   X_jj = D_j,   X_ij = -D_i sum_{m=j}^{i-1} M_im X_mj   (i = j+1 .. NIB-1),
+// with M = L, D_i = inv(L_ii), or M = U^T, D_i = inv(U_ii)^T. Block (i, j) of
+// X goes to out[IB j + c][IB i + r] = X_ij(r, c): out is inv(L)^T for L and
+// inv(U) for U. Launched only for full panels (rows below exist).
+// The factored block is staged whole: G[p][q] = column p, row q of it.
+// OWN_D: the D_i are formed here from the staged block (after k_pdiag2, which
+// keeps no inverses); else they are read from the slot's dinv (k_pdiag).
+constexpr int PI_THREADS = 256;
+constexpr size_t pinv_smem() {
+  return ((size_t)PW * GP + (size_t)NIB * IB * DP + (size_t)PW * DP + (size_t)IB * DP) * sizeof(float);
+}
+template <bool OWN_D>
+__global__ void __launch_bounds__(PI_THREADS)
+k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ slot) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float (*G)[GP] = reinterpret_cast<float (*)[GP]>(smem);
+  float (*Ds)[DP] = reinterpret_cast<float (*)[DP]>(smem + (size_t)PW * GP * sizeof(float));
+  float (*Xs)[DP] = Ds + NIB * IB;   // block column j of X, rows 0 .. PW - 1 (those below IB j used)
+  float (*Ts)[DP] = Xs + PW;
+  const int tid = threadIdx.x;
+  const bool upper = blockIdx.x >= NIB;
+  const int j = upper ? blockIdx.x - NIB : blockIdx.x;
+#pragma unroll
+  for (int u = 0; u < PW * PW / 4 / PI_THREADS; ++u) {
+    const int e = tid + u * PI_THREADS, p = e / (PW / 4), q = (e % (PW / 4)) * 4;
+    cp16(&G[p][q], A + (k + p) * lda + k + q, 16);
+  }
+  if (!OWN_D) copy_inv_async<PI_THREADS>(Ds, slot, upper ? 1 : 0, tid);
+  cp_async_wait_all();
+  __syncthreads();
+  if (OWN_D) {
+    const int warp = tid >> 5, lane = tid & 31, i = j + warp;
+    if (i < NIB) {
+      if (upper) inv_block_upper(G, IB * i, lane, Ds + IB * i);
+      else inv_block_lower(G, IB * i, lane, Ds + IB * i);
+    }
+    __syncthreads();
+  }
+  // M(r, m) and D_i(r, m) of the triangle being inverted
+  const auto Mx = [&](int r, int m) { return upper ? G[r][m] : G[m][r]; };
+  const auto Dx = [&](int i, int r, int m) { return upper ? Ds[i * IB + m][r] : Ds[i * IB + r][m]; };
+  const int r = tid >> 3, c = (tid & 7) * 4;   // this thread's 1 x 4 piece of a 32 x 32 block
+#pragma unroll
+  for (int e = 0; e < 4; ++e) Xs[IB * j + r][c + e] = Dx(j, r, c + e);
+  __syncthreads();
+#pragma unroll 1
+  for (int i = j + 1; i < NIB; ++i) {
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+    for (int m = IB * j; m < IB * i; ++m) {
+      const float a = Mx(IB * i + r, m);
+      const float4 x = *reinterpret_cast<const float4*>(&Xs[m][c]);
+      t[0] = fmaf(a, x.x, t[0]); t[1] = fmaf(a, x.y, t[1]); t[2] = fmaf(a, x.z, t[2]); t[3] = fmaf(a, x.w, t[3]);
+    }
+    *reinterpret_cast<float4*>(&Ts[r][c]) = make_float4(t[0], t[1], t[2], t[3]);
+    __syncthreads();
+    float y[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
+    for (int m = 0; m < IB; ++m) {
+      const float d = Dx(i, r, m);
+      const float4 x = *reinterpret_cast<const float4*>(&Ts[m][c]);
+      y[0] = fmaf(d, x.x, y[0]); y[1] = fmaf(d, x.y, y[1]); y[2] = fmaf(d, x.z, y[2]); y[3] = fmaf(d, x.w, y[3]);
+    }
+    *reinterpret_cast<float4*>(&Xs[IB * i + r][c]) = make_float4(-y[0], -y[1], -y[2], -y[3]);
+    __syncthreads();
+  }
+  // out[IB j + cc][q] = X(q, cc) for q >= IB j, 0 above
+  float* const out = slot + (upper ? kUinvOff : kLinvtOff);
+#pragma unroll
+  for (int u = 0; u < IB * PW / 4 / PI_THREADS; ++u) {
+    const int e = tid + u * PI_THREADS, cc = e / (PW / 4), q = (e % (PW / 4)) * 4;
+    float v[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) v[h] = (q + h >= IB * j) ? Xs[q + h][cc] : 0.f;
+    *reinterpret_cast<float4*>(out + (size_t)(IB * j + cc) * PW + q) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// The split of four consecutive K values of a K-major operand at o (element
+// offset), by split mode SM: kSplitTf32 TF32 hi / lo (unsplit FP32 when lo is
+// null), kSplitBf16 BF16, kSplitBf16x2 BF16 hi / lo (lo = the BF16 rounding of
+// the remainder).
+constexpr int kSplitTf32 = 0, kSplitBf16 = 1, kSplitBf16x2 = 2;
+template <int SM>
+__device__ __forceinline__ void put_split(float* __restrict__ hi, float* __restrict__ lo, int64_t o, const float v[4]) {
+  if (SM == kSplitBf16) {
+    __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
+    d[0] = __floats2bfloat162_rn(v[0], v[1]);
+    d[1] = __floats2bfloat162_rn(v[2], v[3]);
+  } else if (SM == kSplitBf16x2) {
+    __nv_bfloat162* dh = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
+    __nv_bfloat162* dl = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(lo) + o);
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * p], v[2 * p + 1]);
+      dh[p] = h;
+      dl[p] = __floats2bfloat162_rn(v[2 * p] - __low2float(h), v[2 * p + 1] - __high2float(h));
+    }
+  } else if (lo) {
+    float h[4], l[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { h[i] = tf32_rna(v[i]); l[i] = v[i] - h[i]; }
+    *reinterpret_cast<float4*>(hi + o) = make_float4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<float4*>(lo + o) = make_float4(l[0], l[1], l[2], l[3]);
+  } else {
+    *reinterpret_cast<float4*>(hi + o) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// K6g: L21 = A21 inv(U) for the rows [r0 + 32 b, +32) below the panel at k.
+// 8 warps, warp w owns the columns [16 w, +16) (inv(U) is upper triangular:
+// its K loop stops at 16 w + 16), a 4 x 4 piece a lane. Writes L21 in place
+// and its split (K-major, as k_l21), max|L21| into cert.
+constexpr int L21G_THREADS = 256;
+constexpr size_t l21g_smem() { return ((size_t)PW * DP + (size_t)PW * GP) * sizeof(float); }
+template <int SM>
+__global__ void __launch_bounds__(L21G_THREADS)
+k_l21g(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, const float* __restrict__ slot,
+       float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float (*XT)[DP] = reinterpret_cast<float (*)[DP]>(smem);   // XT[s][r] = A21(r, s)
+  float (*Us)[GP] = reinterpret_cast<float (*)[GP]>(smem + (size_t)PW * DP * sizeof(float));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t row0 = r0 + (int64_t)blockIdx.x * L21_ROWS;
+  const int rows = (int)imin64(L21_ROWS, n - row0);
+#pragma unroll
+  for (int u = 0; u < PW * L21_ROWS / 4 / L21G_THREADS; ++u) {
+    const int e = tid + u * L21G_THREADS, s = e / (L21_ROWS / 4), q = (e % (L21_ROWS / 4)) * 4;
+    const int bytes = 4 * max(0, min(4, rows - q));
+    const float* col = A + (k + s) * lda;
+    cp16(&XT[s][q], bytes ? col + row0 + q : col, bytes);
+  }
+  copy_square_async<L21G_THREADS>(Us, slot + kUinvOff, tid);
+  cp_async_wait_all();
+  __syncthreads();
+  const int cq = lane & 3, rq = lane >> 2;
+  const int cb = 16 * warp + 4 * cq, rb = 4 * rq;
+  float acc[4][4] = {};
+  const int send = 16 * warp + 16;
+#pragma unroll 4
+  for (int s = 0; s < send; ++s) {
+    const float4 x = *reinterpret_cast<const float4*>(&XT[s][rb]);
+    const float4 u = *reinterpret_cast<const float4*>(&Us[s][cb]);
+    const float xv[4] = {x.x, x.y, x.z, x.w}, uv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(xv[a], uv[b], acc[a][b]);
+  }
+  float lmax = 0.f;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {   // L21 in place: column k + cb + b, rows row0 + rb ..
+    float* const g = A + (k + cb + b) * lda + row0 + rb;
+    if (rb + 4 <= rows) {
+      *reinterpret_cast<float4*>(g) = make_float4(acc[0][b], acc[1][b], acc[2][b], acc[3][b]);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (rb + a < rows) g[a] = acc[a][b];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {   // the split: row (row0 - r0 + rb + a), K values cb .. cb + 3
+    if (rb + a < rows) {
+      put_split<SM>(Ah, Al, (row0 - r0 + rb + a) * (int64_t)PW + cb, acc[a]);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) lmax = fmaxf(lmax, fabsf(acc[a][b]));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
+  if (lane == 0) atomic_max_pos(cert, lmax);
+}
+
+// K2g: U12 = inv(L) A12 for the panel's rows [k, k + PW) and the columns
+// [c0 + CW b, +CW) of [c0, c1). A 4 x 4 piece a lane; a warp's piece is
+// WR = 512 / CW rows x CW columns, and its K loop stops at its last row
+// (inv(L) is lower triangular). Writes U12 in place and its split (K-major:
+// column j - c0 holds its PW values), as k_u12.
+template <int CW>
+struct U12gCfg {
+  static constexpr int THREADS = 8 * CW;
+  static constexpr int WR = 512 / CW;
+  static constexpr int ZP = CW + 4;
+  static constexpr size_t smem() { return ((size_t)PW * GP + (size_t)PW * ZP) * sizeof(float); }
+};
+template <int CW, int SM>
+__global__ void __launch_bounds__(U12gCfg<CW>::THREADS)
+k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, const float* __restrict__ slot,
+       float* __restrict__ Bh, float* __restrict__ Bl) {
+  typedef U12gCfg<CW> Cfg;
+  constexpr int T = Cfg::THREADS, ZP = Cfg::ZP, CQ = CW / 4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  float (*LT)[GP] = reinterpret_cast<float (*)[GP]>(smem);   // LT[s][i] = inv(L)(i, s)
+  float (*Z)[ZP] = reinterpret_cast<float (*)[ZP]>(smem + (size_t)PW * GP * sizeof(float));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t col0 = c0 + (int64_t)blockIdx.x * CW;
+  const int cols = (int)imin64(CW, c1 - col0);
+  copy_square_async<T>(LT, slot + kLinvtOff, tid);
+  {
+    Staged<T, PW, CW> zs;
+    zs.fetch(A + col0 * lda + k, lda, PW, cols, [](int, int) { return 0.f; }, tid);
+    zs.put([&](int r, int c, float v) { Z[r][c] = v; }, tid);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int cq = lane % CQ, rq = lane / CQ;
+  const int ib = Cfg::WR * warp + 4 * rq, cb = 4 * cq;
+  float acc[4][4] = {};
+  const int send = Cfg::WR * (warp + 1);
+#pragma unroll 4
+  for (int s = 0; s < send; ++s) {
+    const float4 l = *reinterpret_cast<const float4*>(&LT[s][ib]);
+    const float4 z = *reinterpret_cast<const float4*>(&Z[s][cb]);
+    const float lv[4] = {l.x, l.y, l.z, l.w}, zv[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(lv[a], zv[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    if (cb + b >= cols) break;
+    const float v[4] = {acc[0][b], acc[1][b], acc[2][b], acc[3][b]};
+    *reinterpret_cast<float4*>(A + (col0 + cb + b) * lda + k + ib) = make_float4(v[0], v[1], v[2], v[3]);
+    put_split<SM>(Bh, Bl, (col0 - c0 + cb + b) * (int64_t)PW + ib, v);
+  }
+}
+
 __global__ void k_iota(int32_t* __restrict__ ipiv, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) ipiv[i] = (int32_t)i;
@@ -614,17 +1089,37 @@ __global__ void k_iota(int32_t* __restrict__ ipiv, int64_t n) {
 // it) in the tensor-core scratch set of that parity.
 int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv, float* cert, bool bf16) {
   using namespace st;
-  static_assert((size_t)2 * kDinvFloats * sizeof(float) <= kMinvBytes, "inverse slots fit the panel scratch");
+  static_assert((size_t)2 * kSlotFloats * sizeof(float) <= kMinvBytes, "inverse slots fit the panel scratch");
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
-  typedef U12Cfg<8, 1> CfgN;    // the next panel's columns: many small CTAs
+  typedef U12Cfg<16, 1> CfgN;   // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
   static SmemAttr attr_d, attr_l, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
+  static SmemAttr attr_pi, attr_pi2, attr_lg[3], attr_ugn[3], attr_ugr[3];
+  const bool pg = c->panel_gemm > 0;
+  const bool pd2 = c->panel_gemm == 2;   // the diagonal block by k_pdiag2
+  typedef U12gCfg<16> GCfgN;
+  typedef U12gCfg<32> GCfgR;
+  if (pg) {
+    FP_CUDA_TRY(c->err, attr_pi.ensure(k_pinv<false>, (int)pinv_smem()));
+    FP_CUDA_TRY(c->err, attr_pi2.ensure(k_pinv<true>, (int)pinv_smem()));
+    FP_CUDA_TRY(c->err, attr_lg[0].ensure(k_l21g<kSplitTf32>, (int)l21g_smem()));
+    FP_CUDA_TRY(c->err, attr_lg[1].ensure(k_l21g<kSplitBf16>, (int)l21g_smem()));
+    FP_CUDA_TRY(c->err, attr_lg[2].ensure(k_l21g<kSplitBf16x2>, (int)l21g_smem()));
+    FP_CUDA_TRY(c->err, attr_ugn[0].ensure(k_u12g<16, kSplitTf32>, (int)GCfgN::smem()));
+    FP_CUDA_TRY(c->err, attr_ugn[1].ensure(k_u12g<16, kSplitBf16>, (int)GCfgN::smem()));
+    FP_CUDA_TRY(c->err, attr_ugn[2].ensure(k_u12g<16, kSplitBf16x2>, (int)GCfgN::smem()));
+    FP_CUDA_TRY(c->err, attr_ugr[0].ensure(k_u12g<32, kSplitTf32>, (int)GCfgR::smem()));
+    FP_CUDA_TRY(c->err, attr_ugr[1].ensure(k_u12g<32, kSplitBf16>, (int)GCfgR::smem()));
+    FP_CUDA_TRY(c->err, attr_ugr[2].ensure(k_u12g<32, kSplitBf16x2>, (int)GCfgR::smem()));
+  }
+  // the FP32 form's update from BF16 pairs (needs the GEMM-form panel kernels)
+  const bool x3 = !bf16 && pg && c->tc_x3 && c->use_tc;
   FP_CUDA_TRY(c->err, attr_d.ensure(k_pdiag, (int)pdiag_smem()));
   FP_CUDA_TRY(c->err, attr_l.ensure(k_l21<false>, (int)l21_smem()));
-  FP_CUDA_TRY(c->err, attr_un.ensure(k_u12<8, 1, false>, (int)CfgN::smem()));
+  FP_CUDA_TRY(c->err, attr_un.ensure(k_u12<16, 1, false>, (int)CfgN::smem()));
   FP_CUDA_TRY(c->err, attr_ur.ensure(k_u12<32, 2, false>, (int)CfgR::smem()));
   FP_CUDA_TRY(c->err, attr_lb.ensure(k_l21<true>, (int)l21_smem()));
-  FP_CUDA_TRY(c->err, attr_unb.ensure(k_u12<8, 1, true>, (int)CfgN::smem()));
+  FP_CUDA_TRY(c->err, attr_unb.ensure(k_u12<16, 1, true>, (int)CfgN::smem()));
   FP_CUDA_TRY(c->err, attr_urb.ensure(k_u12<32, 2, true>, (int)CfgR::smem()));
   if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
   if (int rc = ensure_tc_scratch(c, 1, n)) return rc;
@@ -648,6 +1143,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     if (bf16) {
       const __nv_bfloat16* bh = reinterpret_cast<const __nv_bfloat16*>(s[2]) + boff * PW;
       if (c->use_tc && tc_gemm_sub_bf16(c, s[0], bh, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
+    } else if (x3) {
+      const __nv_bfloat16* bh = reinterpret_cast<const __nv_bfloat16*>(s[2]) + boff * PW;
+      const __nv_bfloat16* bl = reinterpret_cast<const __nv_bfloat16*>(s[3]) + boff * PW;
+      if (tc_gemm_sub_bf16x3(c, s[0], s[1], bh, bl, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
     } else if (xsplit) {
       if (c->use_tc && tc_gemm_sub_xsplit(c, s[0], s[2] + boff * PW, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
     } else if (c->use_tc && tc_gemm_sub_presplit(c, s[0], s[1], s[2] + boff * PW, s[3] + boff * PW, PW, at(kend, cb),
@@ -661,11 +1160,19 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     const int64_t kend = std::min<int64_t>(K0 + PW, n);
     const int64_t knext = std::min<int64_t>(kend + PW, n);
     const int slot = (int)((K0 / PW) & 1);
-    float* const dinv = dinv_base + (size_t)slot * kDinvFloats;
+    float* const dinv = dinv_base + (size_t)slot * kSlotFloats;   // then inv(L)^T, inv(U) (GEMM form)
     float* const* s = c->d_tc[slot];
     {
       TraceScope tr(c, TR_DIAG);
-      k_pdiag<<<1, kDiagThreads, pdiag_smem(), c->stream>>>(A, lda, n, K0, dinv, cert, c->d_status);
+      if (pd2) k_pdiag2<<<1, PD2_THREADS, 0, c->stream>>>(A, lda, n, K0, cert, c->d_status);
+      else k_pdiag<<<1, kDiagThreads, pdiag_smem(), c->stream>>>(A, lda, n, K0, dinv, cert, c->d_status);
+      ++c->nlaunch;
+      FP_CUDA_TRY(c->err, cudaGetLastError());
+    }
+    if (pg && kend < n) {   // the full inverses (a full panel: rows below exist)
+      TraceScope tr(c, TR_PINV);
+      if (pd2) k_pinv<true><<<2 * NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
+      else k_pinv<false><<<2 * NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
@@ -675,8 +1182,16 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     if (kend < n) {
       TraceScope tr(c, TR_L21);
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
-      if (bf16) k_l21<true><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
-      else k_l21<false><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], xsplit ? nullptr : s[1], cert);
+      float* const al = bf16 ? s[1] : (xsplit ? nullptr : s[1]);
+      if (pg) {
+        if (bf16) k_l21g<kSplitBf16><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+        else if (x3) k_l21g<kSplitBf16x2><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+        else k_l21g<kSplitTf32><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+      } else if (bf16) {
+        k_l21<true><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+      } else {
+        k_l21<false><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+      }
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
@@ -686,11 +1201,18 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
       {
         TraceScope tr(c, TR_U12);
-        const unsigned g = (unsigned)((knext - kend + 7) / 8);
-        if (bf16)
-          k_u12<8, 1, true><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+        const unsigned g = (unsigned)((knext - kend + 15) / 16);
+        if (pg && bf16)
+          k_u12g<16, kSplitBf16><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+        else if (x3)
+          k_u12g<16, kSplitBf16x2><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+        else if (pg)
+          k_u12g<16, kSplitTf32><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
+                                                                                     xsplit ? nullptr : s[3]);
+        else if (bf16)
+          k_u12<16, 1, true><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else
-          k_u12<8, 1, false><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
+          k_u12<16, 1, false><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
                                                                               xsplit ? nullptr : s[3]);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -705,9 +1227,19 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           TraceScope tr(c, TR_STRIP);
           const unsigned g = (unsigned)((n - knext + 31) / 32);
           // the B operand of the columns beyond starts (knext - kend) columns in (bf16 or float elements)
-          float* bh = bf16 ? reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(s[2]) + (knext - kend) * PW)
-                           : s[2] + (knext - kend) * PW;
-          if (bf16)
+          const auto b16 = [&](float* p) {
+            return reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(p) + (knext - kend) * PW);
+          };
+          float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
+          if (pg && bf16)
+            k_u12g<32, kSplitBf16><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh, nullptr);
+          else if (x3)
+            k_u12g<32, kSplitBf16x2><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh,
+                                                                                        b16(s[3]));
+          else if (pg)
+            k_u12g<32, kSplitTf32><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(
+                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
+          else if (bf16)
             k_u12<32, 2, true><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh, nullptr);
           else
             k_u12<32, 2, false><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(

@@ -144,13 +144,17 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint6
 // instead of staging it for a TMA reduce-add.
 // BF16: BF16 operands (tmAh, tmBh only; kind::f16, one MMA per 16-deep
 // step, 32-deep K blocks of 64-byte rows: 16 KB a stage).
-template <int STAGES, bool RED = false, bool BF16 = false>
+// X3 (with BF16): each operand as a BF16 pair hi + lo, C -= Ah Bl + Al Bh +
+// Ah Bh (three kind::f16 MMAs per 16-deep step, 32 KB a stage): half the
+// operand bytes and MMA time of 3xTF32 a K element, 16-bit operand splits.
+template <int STAGES, bool RED = false, bool BF16 = false, bool X3 = false>
 __global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
               const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status,
               float* __restrict__ Cp = nullptr, int64_t ldc = 0) {
-  constexpr int SB = BF16 ? 2 * TILE_A : STAGE_BYTES;   // bytes a stage
+  constexpr int SB = BF16 ? (X3 ? 4 : 2) * TILE_A : STAGE_BYTES;   // bytes a stage
+  static_assert(!X3 || BF16, "X3 splits BF16 operands");
   constexpr int KB = BF16 ? 32 : BK;                    // K elements a stage
   static_assert(RED || STAGES * SB >= 4 * 32 * BN * 4, "the drained ring holds the epilogue's staging");
   extern __shared__ uint8_t smem_raw[];
@@ -190,7 +194,12 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
       if (*(volatile int*)abort_flag) break;
       mbar_expect_tx(&full[s], SB);
       uint8_t* base = smem + s * SB;
-      if (BF16) {
+      if (BF16 && X3) {
+        tma_load_2d(base, &tmAh, kb * KB, m0, &full[s]);
+        tma_load_2d(base + TILE_A, &tmAl, kb * KB, m0, &full[s]);
+        tma_load_2d(base + 2 * TILE_A, &tmBh, kb * KB, n0, &full[s]);
+        tma_load_2d(base + 3 * TILE_A, &tmBl, kb * KB, n0, &full[s]);
+      } else if (BF16) {
         tma_load_2d(base, &tmAh, kb * KB, m0, &full[s]);
         tma_load_2d(base + TILE_A, &tmBh, kb * KB, n0, &full[s]);
       } else {
@@ -214,7 +223,17 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
       if (!mbar_wait(&full[s], (kb / STAGES) & 1)) { ok = false; *abort_flag = 1; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t base = smem_u32(smem + s * SB);
-      if (BF16) {
+      if (BF16 && X3) {
+        const uint64_t dAh = sdesc(base), dAl = sdesc(base + TILE_A);
+        const uint64_t dBh = sdesc(base + 2 * TILE_A), dBl = sdesc(base + 3 * TILE_A);
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {   // 16 bf16 = 32 bytes along K per MMA
+          const uint64_t off = (uint64_t)((kk * 32) >> 4);
+          umma_bf16(tmem, dAh + off, dBl + off, (kb | kk) != 0 ? 1u : 0u);
+          umma_bf16(tmem, dAl + off, dBh + off, 1u);
+          umma_bf16(tmem, dAh + off, dBh + off, 1u);
+        }
+      } else if (BF16) {
         const uint64_t dA = sdesc(base), dB = sdesc(base + TILE_A);
 #pragma unroll
         for (int kk = 0; kk < 2; ++kk) {   // 16 bf16 = 32 bytes along K per MMA
@@ -940,6 +959,48 @@ bool tc_gemm_sub_xsplit(fp_ctx* c, const float* Ax, const float* Bx, int ldk, fl
   else
     tc::k_tc_gemm_sub_xs<3, 1><<<grid, tc::THREADS, std::max(tc::xs::smem_bytes<3, 1>(), c->tc_smem), c->stream>>>(
         mA, mB, mC, (int)m, (int)nn, kk, c->d_status);
+  kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
+  ++c->nlaunch;
+  return cudaGetLastError() == cudaSuccess;
+}
+
+// C -= A B from BF16 pairs (Ah + Al: m rows, Bh + Bl: nn columns, K-major
+// with ldk bf16 elements a row; kk <= ldk): three kind::f16 MMAs a 16-deep
+// step, red.global epilogue; the update of one column of tiles (at most one
+// CTA an SM) uses a 6-stage ring, the others 2 stages (two CTAs an SM).
+bool tc_gemm_sub_bf16x3(fp_ctx* c, const void* Ah, const void* Al, const void* Bh, const void* Bl, int ldk, float* C,
+                        int64_t ldc, int64_t m, int64_t nn, int kk) {
+  if (kk <= 0 || kk > ldk || m <= 0 || nn <= 0 || (ldk & 7) != 0) return false;
+  if (!tc::encode_fn()) return false;
+  if (((reinterpret_cast<uintptr_t>(C) | (uintptr_t)(ldc * 4) | reinterpret_cast<uintptr_t>(Ah) |
+        reinterpret_cast<uintptr_t>(Al) | reinterpret_cast<uintptr_t>(Bh) | reinterpret_cast<uintptr_t>(Bl)) &
+       15) != 0)
+    return false;
+  static SmemAttr a2, a6;
+  if (a2.ensure(tc::k_tc_gemm_sub<2, true, true, true>, kTcSmemMax) != cudaSuccess) return false;
+  if (a6.ensure(tc::k_tc_gemm_sub<6, true, true, true>, kTcSmemMax) != cudaSuccess) return false;
+  auto map16 = [&](CUtensorMap* tm, const void* base, int64_t rows) {
+    cuuint64_t dims[2] = {(cuuint64_t)kk, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ldk * 2};
+    cuuint32_t box[2] = {32u, (cuuint32_t)tc::BM};
+    cuuint32_t es[2] = {1, 1};
+    return tc::encode_fn()(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  CUtensorMap mAh, mAl, mBh, mBl, mC;
+  if (!map16(&mAh, Ah, m) || !map16(&mAl, Al, m) || !map16(&mBh, Bh, nn) || !map16(&mBl, Bl, nn) ||
+      !tc::make_map_c(&mC, C, m, nn, ldc, 32))
+    return false;
+  dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
+  const int ev = kt_begin(c);
+  TraceScope tr(c, TR_GEMM_TC);
+  if (c->tc_narrow_stages == 6 && grid.y == 1 && (int)grid.x <= num_sms())
+    tc::k_tc_gemm_sub<6, true, true, true><<<grid, tc::THREADS, tc::smem_bytes<6>(), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+  else
+    tc::k_tc_gemm_sub<2, true, true, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;

@@ -359,7 +359,7 @@ int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* fl
  * launches on both of its streams; fp_trace_read returns, for the last
  * factorisation, each launch's kernel tag (0 diagonal block, 1 block update,
  * 2 panel fix-up, 3 column strip, 4 tensor-core update, 5/6 operand splits,
- * 7 SIMT update),
+ * 7 SIMT update, 8 full inverses of the diagonal block's factors),
  * its stream (0 the panel stream, 1 the trailing-update stream) and its start
  * and end in ms from the start of the factorisation; count = launches. */
 int fp_trace(fp_ctx* ctx, int enable);
@@ -437,7 +437,19 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       (solve stage 2.38 against 2.51 ms: the two-step form
  *                       also needs the block three back, which arrives just
  *                       before the block two back). Takes effect at the next
- *                       fp_factor */
+ *                       fp_factor
+ *   FP_TUNE_PANEL_GEMM  1: the static-order LU forms the full 128 x 128
+ *                       inverses of each diagonal block's L and U (one small
+ *                       kernel) and computes L21 and U12 as one triangular
+ *                       product each; 2: the same, with the diagonal block
+ *                       factored by right-looking elimination (one pivot a
+ *                       step, register tiles); 0 (default): block substitution
+ *                       with the 32 x 32 diagonal-block inverses
+ *   FP_TUNE_TC_BF16X3   1: the FP32 form's trailing update multiplies BF16 pairs
+ *                       (each operand as hi + lo, C -= Ah Bl + Al Bh + Ah Bh:
+ *                       three kind::f16 MMAs, half the operand bytes of the
+ *                       3xTF32 default, 16-bit operand splits that the FP64
+ *                       refinement absorbs); needs FP_TUNE_PANEL_GEMM 1 or 2 */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -449,6 +461,8 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_ASM32 8
 #define FP_TUNE_TC_NARROW 9
 #define FP_TUNE_TRS2 10
+#define FP_TUNE_PANEL_GEMM 11
+#define FP_TUNE_TC_BF16X3 12
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

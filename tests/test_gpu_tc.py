@@ -47,7 +47,8 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
 @pytest.mark.parametrize("nc,ns", [(8, 4), (12, 8), (20, 24), (40, 48), (60, 80), (50, 30)])
 @pytest.mark.parametrize("knob,value", [("FP_TUNE_TC_SPLIT", 1), ("FP_TUNE_TC_SPLIT", 2), ("FP_TUNE_TC_SPLIT", 3),
                                         ("FP_TUNE_TC_RED", 0), ("FP_TUNE_TC_TILES", 2), ("FP_TUNE_TC_TILES", 4),
-                                        ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0), ("FP_TUNE_TRS2", 1)])
+                                        ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0), ("FP_TUNE_TRS2", 1),
+                                        ("FP_TUNE_PANEL_GEMM", 0), ("FP_TUNE_PANEL_GEMM", 1), ("FP_TUNE_PANEL_GEMM", 2)])
 def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
     1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
@@ -56,7 +57,9 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     kernel (double-buffered accumulator, red.global epilogue); FP_TUNE_ASM32
     assembles the FP32 AIC in panel-local FP32 coordinates and the FP64 AIC
     on a background stream; FP_TUNE_TRS2 1 runs the FP32 sweeps' chain two
-    blocks a step. The factors are as accurate as the default's (refinement
+    blocks a step; FP_TUNE_PANEL_GEMM 0 forms L21 and U12 by block
+    substitution, 1 as products with the full panel inverses, 2 also factors
+    the diagonal block one pivot a step (k_pdiag2). The factors are as accurate as the default's (refinement
     in a handful of steps, the oracle's solution to 1e-10), for one partial
     panel up to many panels with a partial last one (1,500 panels: a last K
     block of 92)."""
@@ -77,6 +80,37 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     finally:
         c.close()
     assert st.used_gmres == 0 and st.ir_iters <= 5, st.asdict()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+
+
+@pytest.mark.parametrize("nc,ns", [(12, 8), (20, 24), (60, 80), (50, 30)])
+@pytest.mark.parametrize("panel", [1, 2])
+def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel):
+    """FP_TUNE_TC_BF16X3 1: the mixed form's trailing update multiplies BF16
+    pairs (hi + lo, three MMAs) instead of TF32 pairs; the factors carry 16-bit
+    operand splits, and the FP64 refinement (GMRES-IR behind it) still reaches
+    the oracle's solution to 1e-10, from one partial panel to many panels with
+    a partial last one."""
+    w = fp.meshes.swept_wing("0012", nc, ns)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(4.2)
+    V = np.array([np.cos(a), 0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    c = fp._capi.Context(0)
+    try:
+        c.set_tuning(fp._capi.FP_TUNE_PANEL_GEMM, panel)
+        c.set_tuning(fp._capi.FP_TUNE_TC_BF16X3, 1)
+        c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+        c.set_wake(w.shedding, D, D)
+        x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
+    finally:
+        c.close()
+    assert st.rel_residual < 1e-11, st.asdict()
     Gr = O.assemble_vortexring(w, cps, normals, D, D)
     xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
