@@ -838,6 +838,9 @@ int fp_autotune(fp_ctx* c, int precision, int reps, int* knobs_out) {
     std::vector<std::vector<std::pair<int, int>>> cand;
     if (precision == FP_PREC_FP64) {
       for (int v : {6, 5, 4, 3, 0}) cand.push_back({{FP_TUNE_FP64_DMMA, v}});
+    } else if (precision == FP_PREC_MIXED && c->tc_x3 && c->panel_gemm > 0) {
+      // the BF16-pair update has one epilogue and ring; only the narrow ring varies
+      for (int narrow : {6, 0}) cand.push_back({{FP_TUNE_TC_NARROW, narrow}});
     } else {
       for (int red : {1, 0})
         for (int stages : {2, 3})

@@ -104,8 +104,8 @@ struct fp_ctx {
   float* d_ms32 = nullptr;              // S_b = P_b Q_{b-1}
   unsigned long long* d_zbox = nullptr; // the sweeps' second mailbox: z_b words (epoch, value)
   bool trs_skip2 = false;               // FP32 sweeps: the two-block chain (FP_TUNE_TRS2)
-  int panel_gemm = 0;                   // static-order LU: 1 full panel inverses, GEMM-form L21 / U12; 2: with k_pdiag2 (FP_TUNE_PANEL_GEMM)
-  bool tc_x3 = false;                   // mixed form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
+  int panel_gemm = 1;                   // static-order FP32 LU: 1 full panel inverses, GEMM-form L21 / U12; 2: with k_pdiag2 (FP_TUNE_PANEL_GEMM)
+  bool tc_x3 = true;                    // FP32 form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)

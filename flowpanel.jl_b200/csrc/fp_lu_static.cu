@@ -927,16 +927,11 @@ k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ 
 
 // The split of four consecutive K values of a K-major operand at o (element
 // offset), by split mode SM: kSplitTf32 TF32 hi / lo (unsplit FP32 when lo is
-// null), kSplitBf16 BF16, kSplitBf16x2 BF16 hi / lo (lo = the BF16 rounding of
-// the remainder).
-constexpr int kSplitTf32 = 0, kSplitBf16 = 1, kSplitBf16x2 = 2;
+// null), kSplitBf16x2 BF16 hi / lo (lo = the BF16 rounding of the remainder).
+constexpr int kSplitTf32 = 0, kSplitBf16x2 = 2;
 template <int SM>
 __device__ __forceinline__ void put_split(float* __restrict__ hi, float* __restrict__ lo, int64_t o, const float v[4]) {
-  if (SM == kSplitBf16) {
-    __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
-    d[0] = __floats2bfloat162_rn(v[0], v[1]);
-    d[1] = __floats2bfloat162_rn(v[2], v[3]);
-  } else if (SM == kSplitBf16x2) {
+  if (SM == kSplitBf16x2) {
     __nv_bfloat162* dh = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
     __nv_bfloat162* dl = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(lo) + o);
 #pragma unroll
@@ -1094,23 +1089,22 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   typedef U12Cfg<16, 1> CfgN;   // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
   static SmemAttr attr_d, attr_l, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
-  static SmemAttr attr_pi, attr_pi2, attr_lg[3], attr_ugn[3], attr_ugr[3];
-  const bool pg = c->panel_gemm > 0;
-  const bool pd2 = c->panel_gemm == 2;   // the diagonal block by k_pdiag2
+  static SmemAttr attr_pi, attr_pi2, attr_lg[2], attr_ugn[2], attr_ugr[2];
+  // the GEMM form of the panel kernels, for the FP32 form (the BF16 form keeps
+  // block substitution: with BF16 updates its GMRES-IR needed more iterations)
+  const bool pg = c->panel_gemm > 0 && !bf16;
+  const bool pd2 = pg && c->panel_gemm == 2;   // the diagonal block by k_pdiag2
   typedef U12gCfg<16> GCfgN;
   typedef U12gCfg<32> GCfgR;
   if (pg) {
     FP_CUDA_TRY(c->err, attr_pi.ensure(k_pinv<false>, (int)pinv_smem()));
     FP_CUDA_TRY(c->err, attr_pi2.ensure(k_pinv<true>, (int)pinv_smem()));
     FP_CUDA_TRY(c->err, attr_lg[0].ensure(k_l21g<kSplitTf32>, (int)l21g_smem()));
-    FP_CUDA_TRY(c->err, attr_lg[1].ensure(k_l21g<kSplitBf16>, (int)l21g_smem()));
-    FP_CUDA_TRY(c->err, attr_lg[2].ensure(k_l21g<kSplitBf16x2>, (int)l21g_smem()));
+    FP_CUDA_TRY(c->err, attr_lg[1].ensure(k_l21g<kSplitBf16x2>, (int)l21g_smem()));
     FP_CUDA_TRY(c->err, attr_ugn[0].ensure(k_u12g<16, kSplitTf32>, (int)GCfgN::smem()));
-    FP_CUDA_TRY(c->err, attr_ugn[1].ensure(k_u12g<16, kSplitBf16>, (int)GCfgN::smem()));
-    FP_CUDA_TRY(c->err, attr_ugn[2].ensure(k_u12g<16, kSplitBf16x2>, (int)GCfgN::smem()));
+    FP_CUDA_TRY(c->err, attr_ugn[1].ensure(k_u12g<16, kSplitBf16x2>, (int)GCfgN::smem()));
     FP_CUDA_TRY(c->err, attr_ugr[0].ensure(k_u12g<32, kSplitTf32>, (int)GCfgR::smem()));
-    FP_CUDA_TRY(c->err, attr_ugr[1].ensure(k_u12g<32, kSplitBf16>, (int)GCfgR::smem()));
-    FP_CUDA_TRY(c->err, attr_ugr[2].ensure(k_u12g<32, kSplitBf16x2>, (int)GCfgR::smem()));
+    FP_CUDA_TRY(c->err, attr_ugr[1].ensure(k_u12g<32, kSplitBf16x2>, (int)GCfgR::smem()));
   }
   // the FP32 form's update from BF16 pairs (needs the GEMM-form panel kernels)
   const bool x3 = !bf16 && pg && c->tc_x3 && c->use_tc;
@@ -1184,8 +1178,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
       float* const al = bf16 ? s[1] : (xsplit ? nullptr : s[1]);
       if (pg) {
-        if (bf16) k_l21g<kSplitBf16><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
-        else if (x3) k_l21g<kSplitBf16x2><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+        if (x3) k_l21g<kSplitBf16x2><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
         else k_l21g<kSplitTf32><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
       } else if (bf16) {
         k_l21<true><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
@@ -1202,9 +1195,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       {
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
-        if (pg && bf16)
-          k_u12g<16, kSplitBf16><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
-        else if (x3)
+        if (x3)
           k_u12g<16, kSplitBf16x2><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else if (pg)
           k_u12g<16, kSplitTf32><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
@@ -1231,9 +1222,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
             return reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(p) + (knext - kend) * PW);
           };
           float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
-          if (pg && bf16)
-            k_u12g<32, kSplitBf16><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh, nullptr);
-          else if (x3)
+          if (x3)
             k_u12g<32, kSplitBf16x2><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh,
                                                                                         b16(s[3]));
           else if (pg)

@@ -438,18 +438,22 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       also needs the block three back, which arrives just
  *                       before the block two back). Takes effect at the next
  *                       fp_factor
- *   FP_TUNE_PANEL_GEMM  1: the static-order LU forms the full 128 x 128
- *                       inverses of each diagonal block's L and U (one small
- *                       kernel) and computes L21 and U12 as one triangular
- *                       product each; 2: the same, with the diagonal block
- *                       factored by right-looking elimination (one pivot a
- *                       step, register tiles); 0 (default): block substitution
- *                       with the 32 x 32 diagonal-block inverses
- *   FP_TUNE_TC_BF16X3   1: the FP32 form's trailing update multiplies BF16 pairs
- *                       (each operand as hi + lo, C -= Ah Bl + Al Bh + Ah Bh:
- *                       three kind::f16 MMAs, half the operand bytes of the
- *                       3xTF32 default, 16-bit operand splits that the FP64
- *                       refinement absorbs); needs FP_TUNE_PANEL_GEMM 1 or 2 */
+ *   FP_TUNE_PANEL_GEMM  the static-order LU of the FP32 form: 1 (default) forms
+ *                       the full 128 x 128 inverses of each diagonal block's L
+ *                       and U (one small kernel) and computes L21 and U12 as
+ *                       one triangular product each (factorisation 13.66 ->
+ *                       13.3 ms on the 12k wing with the 3xTF32 update); 2: the
+ *                       same with the diagonal block factored one pivot a step
+ *                       (k_pdiag2; 15.7 ms); 0: block substitution with the
+ *                       32 x 32 diagonal-block inverses. The BF16 form always
+ *                       uses block substitution
+ *   FP_TUNE_TC_BF16X3   1 (default): the FP32 form's trailing update multiplies
+ *                       BF16 pairs (each operand as hi + lo, C -= Ah Bl + Al Bh +
+ *                       Ah Bh: three kind::f16 MMAs, half the operand bytes of
+ *                       3xTF32; the 16-bit operand splits leave the refinement
+ *                       at 4 steps on the 12k wing: factorisation 13.3 ->
+ *                       12.1 ms); 0: 3xTF32 (TF32 pairs). Needs
+ *                       FP_TUNE_PANEL_GEMM 1 or 2 */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -468,7 +472,8 @@ int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 /* Autotuner (no counterpart in the reference): times the factorisation of the
  * assembled AIC under candidate knob settings (FP_PREC_FP64: the FP64 update
  * variants of FP_TUNE_FP64_DMMA; FP_PREC_MIXED / FP_PREC_BF16: the tensor-core
- * update's epilogue, ring depth and tile kernel), reps timed runs each after
+ * update's epilogue, ring depth and tile kernel, or with the BF16-pair update
+ * of FP_TUNE_TC_BF16X3 the ring of the next panel's update only), reps timed runs each after
  * one warm-up, and keeps the fastest for this context. The choice is cached
  * per (N, precision): a later call for the same size only applies it. The
  * context is left assembled (FP32 trials re-assemble), not factored; knobs

@@ -73,6 +73,9 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     U = np.tile(V, (w.npanels, 1))
     c = fp._capi.Context(0)
     try:
+        # the TF32-pair update, whose variants these are (the BF16-pair default
+        # has its own test below)
+        c.set_tuning(fp._capi.FP_TUNE_TC_BF16X3, 0)
         c.set_tuning(getattr(fp._capi, knob), value)
         c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
         c.set_wake(w.shedding, D, D)
