@@ -197,8 +197,10 @@ def factor_timeline(ctx, cap, prec):
     ctx.trace(False)
     tags, streams, t0, t1 = ctx.trace_read()
     out = {"span_ms": float(t1.max() - t0.min()) if len(t0) else 0.0, "kernels": []}
-    for s in (0, 1):
+    for s in (0, 1, 2):
         sel = streams == s
+        if s == 2 and not sel.any():
+            continue
         out[f"stream{s}_busy_ms"] = float(np.sum(t1[sel] - t0[sel]))
         for tg in sorted(set(tags[sel].tolist())):
             m = sel & (tags == tg)
@@ -552,8 +554,9 @@ def run_ours(args, rank, ws, dist):
     per_elem = profile_traffic("k_tc_gemm_sub")   # DRAM bytes per updated C element, from ncu
     traffic = per_elem * tc_elems / tc_launches if (per_elem and tc_launches) else None
     # with K = 128 the update does 2 x 128 flops per C element against 8 bytes
-    # of C read-modify-write (32 flop/B), under the 3xTF32 ridge point
-    # (bf16 peak / 2 / 3 over HBM, ~43 flop/B): HBM is the bound that applies
+    # of C read-modify-write (32 flop/B), under the ridge point of its BF16
+    # pairs (bf16 peak / 3 MMAs a flop over HBM, ~86 flop/B): HBM is the bound
+    # that applies
     tc_gbs = 8.0 * tc_elems / (tc_ms * 1e-3) / 1e9 if tc_ms > 0 else 0.0
     # the critical path: the panel chain on stream 0, led by the diagonal
     # block (one CTA, dependent elimination steps)
@@ -604,7 +607,8 @@ def run_ours(args, rank, ws, dist):
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 3 * 8 * N,
                     "d2h_bytes_per_step": 8 * N},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_tc_gemm_sub (tcgen05 3xTF32 trailing update, K = 128)",
+            "roofline": {"bound": "hbm", "kernel": "k_tc_gemm_sub<2,RED,BF16,X3> (tcgen05 trailing update from BF16 "
+                                                   "hi/lo pairs, three kind::f16 MMAs a 16-deep step, K = 128)",
                          "achieved": tc_gbs, "peak": peak_hbm, "unit": "GB/s", "frac": tc_gbs / peak_hbm,
                          "traffic": traffic, "launches": tc_launches, "ms_total": tc_ms,
                          "algorithmic_bytes": "8 B per updated C element (FP32 read + write; the operand "
@@ -612,9 +616,9 @@ def run_ours(args, rank, ws, dist):
                          "peak_source": hbm_src,
                          "tensor_view": {"achieved_tflops": tc_tflops, "bf16_peak_tflops": peak_tc,
                                          "frac_of_bf16": tc_tflops / peak_tc,
-                                         "frac_of_3xtf32_ceiling": tc_tflops / (peak_tc / 6.0),
-                                         "note": "2 m n k algorithmic flops; TF32 runs at half the BF16 "
-                                                 "rate and 3xTF32 issues 3 MMAs per flop"}},
+                                         "frac_of_bf16_pair_ceiling": tc_tflops / (peak_tc / 3.0),
+                                         "note": "2 m n k algorithmic flops; the BF16-pair update issues "
+                                                 "3 BF16 MMAs per flop"}},
             "critical_path_roofline": None if diag is None else {
                 "bound": "latency", "kernel": "k_pdiag (128 x 128 diagonal block, one CTA)",
                 "avg_us_in_place": diag["avg_us"], "launches": diag["launches"],

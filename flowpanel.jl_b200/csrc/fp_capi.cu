@@ -157,6 +157,8 @@ int fp_ctx_create(int device, fp_ctx** out) {
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_pinv, cudaEventDisableTiming) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream_bg, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_g64, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_diag, cudaEventDisableTiming) != cudaSuccess ||
@@ -179,6 +181,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
+  if (c->stream3) cudaStreamSynchronize(c->stream3);
   if (c->stream_bg) cudaStreamSynchronize(c->stream_bg);
   free_matrices(c);
   post_free(c);
@@ -193,6 +196,8 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->ev_g64) cudaEventDestroy(c->ev_g64);
   if (c->ev_diag) cudaEventDestroy(c->ev_diag);
   if (c->ev_asm) cudaEventDestroy(c->ev_asm);
+  if (c->ev_pinv) cudaEventDestroy(c->ev_pinv);
+  if (c->stream3) cudaStreamDestroy(c->stream3);
   if (c->stream_bg) cudaStreamDestroy(c->stream_bg);
   if (c->stream2) cudaStreamDestroy(c->stream2);
   if (c->stream) cudaStreamDestroy(c->stream);

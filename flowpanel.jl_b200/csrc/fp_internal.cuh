@@ -104,7 +104,7 @@ struct fp_ctx {
   float* d_ms32 = nullptr;              // S_b = P_b Q_{b-1}
   unsigned long long* d_zbox = nullptr; // the sweeps' second mailbox: z_b words (epoch, value)
   bool trs_skip2 = false;               // FP32 sweeps: the two-block chain (FP_TUNE_TRS2)
-  int panel_gemm = 1;                   // static-order FP32 LU: 1 full panel inverses, GEMM-form L21 / U12; 2: with k_pdiag2 (FP_TUNE_PANEL_GEMM)
+  int panel_gemm = 2;                   // static-order FP32 LU: 1 both panel inverses, GEMM-form L21 / U12; 2: inv(L) only, beside k_l21 (FP_TUNE_PANEL_GEMM)
   bool tc_x3 = true;                    // FP32 form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
@@ -167,6 +167,7 @@ struct fp_ctx {
   size_t tc_cap[2] = {0, 0};
   int tc_slot = 0;                      // scratch set of the current launches
   cudaStream_t stream2 = nullptr;       // second stream of the look-ahead factorisation
+  cudaStream_t stream3 = nullptr;       // third stream (high priority): the static-order LU's inv(L) beside k_l21
   cudaStream_t stream_bg = nullptr;     // lowest priority: the FP64 AIC pass under the FP32 factorisation
   cudaEvent_t ev_g64 = nullptr;         // that pass done (stream_bg -> stream)
   cudaEvent_t ev_asm = nullptr;         // assembly inputs ready (stream -> stream_bg)
@@ -176,6 +177,7 @@ struct fp_ctx {
   cudaEvent_t ev_panel = nullptr;       // panel factored (stream -> stream2)
   cudaEvent_t ev_diag = nullptr;        // static-order LU: diagonal block factored (stream -> stream2)
   cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)
+  cudaEvent_t ev_pinv = nullptr;        // static-order LU: inv(L) formed (stream3 -> stream, stream2)
 
   // surface post-processing (fp_post.cu). The mesh topology of a triangular
   // body is built on first use after fp_set_geometry, the Kutta-average
@@ -321,6 +323,14 @@ struct SmemAttr {
   }
 };
 
+// Routes the launches of a section to stream s (tensor-core scratch unchanged).
+struct OnStream {
+  fp_ctx* c;
+  cudaStream_t s0;
+  OnStream(fp_ctx* c_, cudaStream_t s) : c(c_), s0(c_->stream) { c->stream = s; }
+  ~OnStream() { c->stream = s0; }
+};
+
 // Routes the launches of a section to stream2 and its tensor-core scratch.
 struct OnStream2 {
   fp_ctx* c;
@@ -396,7 +406,7 @@ struct TraceScope {
     if (s < 0) return;
     const int e = tr_event(c);
     if (e < 0) return;
-    c->trace.recs.push_back(TraceRec{tag, c->stream == c->stream2 ? 1 : 0, s});
+    c->trace.recs.push_back(TraceRec{tag, c->stream == c->stream2 ? 1 : (c->stream == c->stream3 ? 2 : 0), s});
   }
 };
 inline void tr_collect(fp_ctx* c) {

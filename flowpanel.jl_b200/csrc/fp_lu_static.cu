@@ -420,6 +420,37 @@ k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restr
   if (lane == 0) atomic_max_pos(cert, lmax);
 }
 
+// The split of four consecutive K values of a K-major operand at o (element
+// offset), by split mode SM: kSplitTf32 TF32 hi / lo (unsplit FP32 when lo is
+// null), kSplitBf16 BF16 (the BF16 form; no lo), kSplitBf16x2 BF16 hi / lo
+// (lo = the BF16 rounding of the remainder).
+constexpr int kSplitTf32 = 0, kSplitBf16 = 1, kSplitBf16x2 = 2;
+template <int SM>
+__device__ __forceinline__ void put_split(float* __restrict__ hi, float* __restrict__ lo, int64_t o, const float v[4]) {
+  if (SM == kSplitBf16) {
+    __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
+    d[0] = __floats2bfloat162_rn(v[0], v[1]);
+    d[1] = __floats2bfloat162_rn(v[2], v[3]);
+  } else if (SM == kSplitBf16x2) {
+    __nv_bfloat162* dh = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
+    __nv_bfloat162* dl = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(lo) + o);
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * p], v[2 * p + 1]);
+      dh[p] = h;
+      dl[p] = __floats2bfloat162_rn(v[2 * p] - __low2float(h), v[2 * p + 1] - __high2float(h));
+    }
+  } else if (lo) {
+    float h[4], l[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { h[i] = tf32_rna(v[i]); l[i] = v[i] - h[i]; }
+    *reinterpret_cast<float4*>(hi + o) = make_float4(h[0], h[1], h[2], h[3]);
+    *reinterpret_cast<float4*>(lo + o) = make_float4(l[0], l[1], l[2], l[3]);
+  } else {
+    *reinterpret_cast<float4*>(hi + o) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // K6: L21 = A21 U^-1 for the rows [r0 + 32 b, +32) below the panel at k, by
 // block substitution over the four inner column blocks t:
@@ -438,7 +469,7 @@ constexpr size_t l21_smem() {
          (size_t)NIB * IB * UP * sizeof(float);
 }
 
-template <bool BF16>
+template <int SM>
 __global__ void __launch_bounds__(L21_THREADS)
 k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, const float* __restrict__ dinv,
       float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
@@ -510,18 +541,8 @@ k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, cons
   for (int e = tid; e < rows * C4; e += L21_THREADS) {   // K-major split: 16-byte stores along each row
     const int r = e / C4, c = (e % C4) * 4;
     const float4 v = *reinterpret_cast<const float4*>(&X[r][c]);
-    const int64_t o = (row0 - r0 + r) * (int64_t)PW + c;
-    if (BF16) {   // the operand in BF16 (element offsets in a bf16 array)
-      __nv_bfloat162* d = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(Ah) + o);
-      d[0] = __floats2bfloat162_rn(v.x, v.y);
-      d[1] = __floats2bfloat162_rn(v.z, v.w);
-    } else if (Al) {
-      const float4 h = make_float4(tf32_rna(v.x), tf32_rna(v.y), tf32_rna(v.z), tf32_rna(v.w));
-      *reinterpret_cast<float4*>(&Ah[o]) = h;
-      *reinterpret_cast<float4*>(&Al[o]) = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
-    } else {   // unsplit: the update splits in shared memory
-      *reinterpret_cast<float4*>(&Ah[o]) = v;
-    }
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+    put_split<SM>(Ah, Al, (row0 - r0 + r) * (int64_t)PW + c, vv);
     lmax = fmaxf(lmax, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
   }
 #pragma unroll
@@ -669,196 +690,19 @@ __device__ __forceinline__ void copy_square_async(float (*dst)[GP], const float*
   }
 }
 
-// K1 with FP_TUNE_PANEL_GEMM 2: the diagonal block by right-looking
-// elimination, one pivot a step. 256 threads, each holding an 8 x 8 tile of
-// the block in registers (warp w: rows 32 (w >> 1) .. +32, columns
-// 64 (w & 1) .. +64). Before step kk the owners of column kk and row kk have
-// posted them to a double-buffered shared array (column entries below the
-// pivot, row entries right of it, zeros elsewhere; the pivot apart); after one
-// __syncthreads every warp whose region reaches the trailing block applies the
-// rank-1 update A(i, j) -= A(i, kk) / A(kk, kk) A(kk, j). The columns below
-// the pivots keep their unscaled values until the end, when they are divided
-// by the pivots (L). Little code and one barrier a pivot; the inverses of L
-// and U come from k_pinv<true>.
-constexpr int PD2_THREADS = 256;
-__global__ void __launch_bounds__(PD2_THREADS, 1)
-k_pdiag2(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ cert, int* __restrict__ status) {
-  __shared__ __align__(16) float colb[2][PW];
-  __shared__ __align__(16) float rowb[2][PW];
-  __shared__ __align__(16) float pivs[PW];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int r0 = 32 * (warp >> 1) + 8 * (lane >> 3), c0 = 64 * (warp & 1) + 8 * (lane & 7);
-  const int rw1 = 32 * (warp >> 1) + 31, cw1 = 64 * (warp & 1) + 63;   // last row / column of the warp's region
-  const int nb = (int)imin64(PW, n - k);
-  float t[8][8];
-  {
-    float4 v[8][2];
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int c = c0 + b;
-      if (c < nb && r0 + 8 <= nb) {
-        const float4* p = reinterpret_cast<const float4*>(A + (k + c) * lda + k + r0);
-        v[b][0] = __ldcg(p);
-        v[b][1] = __ldcg(p + 1);
-      } else {
-        float s[8];
-#pragma unroll
-        for (int a = 0; a < 8; ++a)
-          s[a] = (c < nb && r0 + a < nb) ? __ldcg(A + (k + c) * lda + k + r0 + a) : (r0 + a == c ? 1.f : 0.f);
-        v[b][0] = make_float4(s[0], s[1], s[2], s[3]);
-        v[b][1] = make_float4(s[4], s[5], s[6], s[7]);
-      }
-    }
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      t[0][b] = v[b][0].x; t[1][b] = v[b][0].y; t[2][b] = v[b][0].z; t[3][b] = v[b][0].w;
-      t[4][b] = v[b][1].x; t[5][b] = v[b][1].y; t[6][b] = v[b][1].z; t[7][b] = v[b][1].w;
-    }
-  }
-  // the owners of column kk and row kk post them for step kk (buffer kk & 1)
-  const auto post = [&](int kk) {
-    float* const cb = colb[kk & 1];
-    float* const rb = rowb[kk & 1];
-    const int bc = kk - c0, ar = kk - r0;
-    switch (bc) {   // column kk of this tile: a static column in each case
-#define FP_PD2_COL(B)                                                        \
-  case B:                                                                    \
-    _Pragma("unroll") for (int a = 0; a < 8; ++a) {                          \
-      cb[r0 + a] = (r0 + a > kk) ? t[a][B] : 0.f;                            \
-      if (r0 + a == kk) pivs[kk] = t[a][B];                                  \
-    }                                                                        \
-    break;
-      FP_PD2_COL(0) FP_PD2_COL(1) FP_PD2_COL(2) FP_PD2_COL(3) FP_PD2_COL(4) FP_PD2_COL(5) FP_PD2_COL(6) FP_PD2_COL(7)
-#undef FP_PD2_COL
-      default: break;
-    }
-    switch (ar) {   // row kk of this tile
-#define FP_PD2_ROW(R)                                                                          \
-  case R:                                                                                      \
-    _Pragma("unroll") for (int b = 0; b < 8; ++b) rb[c0 + b] = (c0 + b > kk) ? t[R][b] : 0.f; \
-    break;
-      FP_PD2_ROW(0) FP_PD2_ROW(1) FP_PD2_ROW(2) FP_PD2_ROW(3) FP_PD2_ROW(4) FP_PD2_ROW(5) FP_PD2_ROW(6) FP_PD2_ROW(7)
-#undef FP_PD2_ROW
-      default: break;
-    }
-  };
-  post(0);
-  __syncthreads();
-#pragma unroll 1
-  for (int kk = 0; kk < PW - 1; ++kk) {
-    if (rw1 > kk && cw1 > kk) {   // warp-uniform: the region reaches the trailing block
-      const float rp = rcp_fast(pivs[kk]);
-      const float4* cp = reinterpret_cast<const float4*>(&colb[kk & 1][r0]);
-      const float4* rq = reinterpret_cast<const float4*>(&rowb[kk & 1][c0]);
-      const float4 l0 = cp[0], l1 = cp[1], u0 = rq[0], u1 = rq[1];
-      const float l[8] = {l0.x * rp, l0.y * rp, l0.z * rp, l0.w * rp, l1.x * rp, l1.y * rp, l1.z * rp, l1.w * rp};
-      const float u[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-#pragma unroll
-        for (int b = 0; b < 8; ++b) t[a][b] = fmaf(-l[a], u[b], t[a][b]);
-    }
-    post(kk + 1);
-    __syncthreads();
-  }
-  // L below the diagonal: the column values over their pivots
-  float lmax = 0.f;
-  {
-    const float4 p0 = *reinterpret_cast<const float4*>(&pivs[c0]), p1 = *reinterpret_cast<const float4*>(&pivs[c0 + 4]);
-    const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const float rp = rcp_fast(pv[b]);
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-        if (r0 + a > c0 + b) {
-          t[a][b] *= rp;
-          lmax = fmaxf(lmax, fabsf(t[a][b]));
-        }
-    }
-  }
-  if (tid < nb) {
-    const float p = pivs[tid];
-    if (!(fabsf(p) > 0.f && fabsf(p) <= FLT_MAX)) atomicOr(status, (int)DEV_ZERO_PIVOT);
-  }
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    const int c = c0 + b;
-    if (c >= nb) continue;
-    float* const g = A + (k + c) * lda + k + r0;
-    if (r0 + 8 <= nb) {
-      reinterpret_cast<float4*>(g)[0] = make_float4(t[0][b], t[1][b], t[2][b], t[3][b]);
-      reinterpret_cast<float4*>(g)[1] = make_float4(t[4][b], t[5][b], t[6][b], t[7][b]);
-    } else {
-#pragma unroll
-      for (int a = 0; a < 8; ++a)
-        if (r0 + a < nb) g[a] = t[a][b];
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
-  if (lane == 0) atomic_max_pos(cert, lmax);
-}
-
-// The IB x IB diagonal-block inverses from the staged factored block G
-// (G[p][q] = column p, row q): lane c forms column c, of inv(L_ii) by
-// substitution down column m of L (unit diagonal), of inv(U_ii) up column m of
-// U; both read contiguous columns. dst[r][c] = the inverse's (r, c).
-__device__ __forceinline__ void inv_block_lower(const float (*G)[GP], int ib, int lane, float (*dst)[DP]) {
-  float y[IB];
-#pragma unroll
-  for (int r = 0; r < IB; ++r) y[r] = (r == lane) ? 1.f : 0.f;
-#pragma unroll
-  for (int m = 0; m < IB - 1; ++m) {   // y(r) -= L(r, m) y(m), r > m
-#pragma unroll
-    for (int g = 0; g < IB / 4; ++g) {
-      if (4 * g + 3 <= m) continue;
-      const float4 q = *reinterpret_cast<const float4*>(&G[ib + m][ib + 4 * g]);
-      const float qv[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (4 * g + e > m) y[4 * g + e] = fmaf(-qv[e], y[m], y[4 * g + e]);
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < IB; ++r) dst[r][lane] = y[r];
-}
-__device__ __forceinline__ void inv_block_upper(const float (*G)[GP], int ib, int lane, float (*dst)[DP]) {
-  float x[IB];
-#pragma unroll
-  for (int r = 0; r < IB; ++r) x[r] = (r == lane) ? 1.f : 0.f;
-#pragma unroll
-  for (int m = IB - 1; m >= 0; --m) {   // x(m) /= U(m, m); x(r) -= U(r, m) x(m), r < m
-    x[m] *= rcp_fast(G[ib + m][ib + m]);
-#pragma unroll
-    for (int g = 0; g < IB / 4; ++g) {
-      if (4 * g >= m) continue;
-      const float4 q = *reinterpret_cast<const float4*>(&G[ib + m][ib + 4 * g]);
-      const float qv[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (4 * g + e < m) x[4 * g + e] = fmaf(-qv[e], x[m], x[4 * g + e]);
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < IB; ++r) dst[r][lane] = x[r];
-}
-
 // K1b: 2 NIB CTAs. CTA b < NIB forms block column j = b of inv(L), CTA
 // b >= NIB block column j = b - NIB of inv(U^T) = inv(U)^T; both are the
 // inverse of a lower-triangular M from its diagonal-block inverses D_i:
 //   X_jj = D_j,   X_ij = -D_i sum_{m=j}^{i-1} M_im X_mj   (i = j+1 .. NIB-1),
 // with M = L, D_i = inv(L_ii), or M = U^T, D_i = inv(U_ii)^T. Block (i, j) of
 // X goes to out[IB j + c][IB i + r] = X_ij(r, c): out is inv(L)^T for L and
-// inv(U) for U. Launched only for full panels (rows below exist).
-// The factored block is staged whole: G[p][q] = column p, row q of it.
-// OWN_D: the D_i are formed here from the staged block (after k_pdiag2, which
-// keeps no inverses); else they are read from the slot's dinv (k_pdiag).
+// inv(U) for U. Launched only for full panels (rows below exist); a grid of
+// NIB CTAs forms inv(L) alone. The factored block is staged whole:
+// G[p][q] = column p, row q of it; the D_i come from the slot's dinv (k_pdiag).
 constexpr int PI_THREADS = 256;
 constexpr size_t pinv_smem() {
   return ((size_t)PW * GP + (size_t)NIB * IB * DP + (size_t)PW * DP + (size_t)IB * DP) * sizeof(float);
 }
-template <bool OWN_D>
 __global__ void __launch_bounds__(PI_THREADS)
 k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ slot) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -874,17 +718,9 @@ k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ 
     const int e = tid + u * PI_THREADS, p = e / (PW / 4), q = (e % (PW / 4)) * 4;
     cp16(&G[p][q], A + (k + p) * lda + k + q, 16);
   }
-  if (!OWN_D) copy_inv_async<PI_THREADS>(Ds, slot, upper ? 1 : 0, tid);
+  copy_inv_async<PI_THREADS>(Ds, slot, upper ? 1 : 0, tid);
   cp_async_wait_all();
   __syncthreads();
-  if (OWN_D) {
-    const int warp = tid >> 5, lane = tid & 31, i = j + warp;
-    if (i < NIB) {
-      if (upper) inv_block_upper(G, IB * i, lane, Ds + IB * i);
-      else inv_block_lower(G, IB * i, lane, Ds + IB * i);
-    }
-    __syncthreads();
-  }
   // M(r, m) and D_i(r, m) of the triangle being inverted
   const auto Mx = [&](int r, int m) { return upper ? G[r][m] : G[m][r]; };
   const auto Dx = [&](int i, int r, int m) { return upper ? Ds[i * IB + m][r] : Ds[i * IB + r][m]; };
@@ -922,32 +758,6 @@ k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ 
 #pragma unroll
     for (int h = 0; h < 4; ++h) v[h] = (q + h >= IB * j) ? Xs[q + h][cc] : 0.f;
     *reinterpret_cast<float4*>(out + (size_t)(IB * j + cc) * PW + q) = make_float4(v[0], v[1], v[2], v[3]);
-  }
-}
-
-// The split of four consecutive K values of a K-major operand at o (element
-// offset), by split mode SM: kSplitTf32 TF32 hi / lo (unsplit FP32 when lo is
-// null), kSplitBf16x2 BF16 hi / lo (lo = the BF16 rounding of the remainder).
-constexpr int kSplitTf32 = 0, kSplitBf16x2 = 2;
-template <int SM>
-__device__ __forceinline__ void put_split(float* __restrict__ hi, float* __restrict__ lo, int64_t o, const float v[4]) {
-  if (SM == kSplitBf16x2) {
-    __nv_bfloat162* dh = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(hi) + o);
-    __nv_bfloat162* dl = reinterpret_cast<__nv_bfloat162*>(reinterpret_cast<__nv_bfloat16*>(lo) + o);
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * p], v[2 * p + 1]);
-      dh[p] = h;
-      dl[p] = __floats2bfloat162_rn(v[2 * p] - __low2float(h), v[2 * p + 1] - __high2float(h));
-    }
-  } else if (lo) {
-    float h[4], l[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) { h[i] = tf32_rna(v[i]); l[i] = v[i] - h[i]; }
-    *reinterpret_cast<float4*>(hi + o) = make_float4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<float4*>(lo + o) = make_float4(l[0], l[1], l[2], l[3]);
-  } else {
-    *reinterpret_cast<float4*>(hi + o) = make_float4(v[0], v[1], v[2], v[3]);
   }
 }
 
@@ -1088,17 +898,19 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
   typedef U12Cfg<16, 1> CfgN;   // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
-  static SmemAttr attr_d, attr_l, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
-  static SmemAttr attr_pi, attr_pi2, attr_lg[2], attr_ugn[2], attr_ugr[2];
+  static SmemAttr attr_d, attr_l, attr_lx, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
+  static SmemAttr attr_pi, attr_lg[2], attr_ugn[2], attr_ugr[2];
   // the GEMM form of the panel kernels, for the FP32 form (the BF16 form keeps
   // block substitution: with BF16 updates its GMRES-IR needed more iterations)
-  const bool pg = c->panel_gemm > 0 && !bf16;
-  const bool pd2 = pg && c->panel_gemm == 2;   // the diagonal block by k_pdiag2
+  const bool pg = c->panel_gemm > 0 && !bf16;   // U12 = inv(L) A12
+  // 2: L21 by block substitution on the panel stream, inv(L) alone on the
+  // third stream beside it; 1: both inverses on the panel stream, L21 = A21 inv(U)
+  const bool lside = pg && c->panel_gemm == 2;
+  const bool lg = pg && !lside;
   typedef U12gCfg<16> GCfgN;
   typedef U12gCfg<32> GCfgR;
   if (pg) {
-    FP_CUDA_TRY(c->err, attr_pi.ensure(k_pinv<false>, (int)pinv_smem()));
-    FP_CUDA_TRY(c->err, attr_pi2.ensure(k_pinv<true>, (int)pinv_smem()));
+    FP_CUDA_TRY(c->err, attr_pi.ensure(k_pinv, (int)pinv_smem()));
     FP_CUDA_TRY(c->err, attr_lg[0].ensure(k_l21g<kSplitTf32>, (int)l21g_smem()));
     FP_CUDA_TRY(c->err, attr_lg[1].ensure(k_l21g<kSplitBf16x2>, (int)l21g_smem()));
     FP_CUDA_TRY(c->err, attr_ugn[0].ensure(k_u12g<16, kSplitTf32>, (int)GCfgN::smem()));
@@ -1109,10 +921,11 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   // the FP32 form's update from BF16 pairs (needs the GEMM-form panel kernels)
   const bool x3 = !bf16 && pg && c->tc_x3 && c->use_tc;
   FP_CUDA_TRY(c->err, attr_d.ensure(k_pdiag, (int)pdiag_smem()));
-  FP_CUDA_TRY(c->err, attr_l.ensure(k_l21<false>, (int)l21_smem()));
+  FP_CUDA_TRY(c->err, attr_l.ensure(k_l21<kSplitTf32>, (int)l21_smem()));
+  FP_CUDA_TRY(c->err, attr_lx.ensure(k_l21<kSplitBf16x2>, (int)l21_smem()));
   FP_CUDA_TRY(c->err, attr_un.ensure(k_u12<16, 1, false>, (int)CfgN::smem()));
   FP_CUDA_TRY(c->err, attr_ur.ensure(k_u12<32, 2, false>, (int)CfgR::smem()));
-  FP_CUDA_TRY(c->err, attr_lb.ensure(k_l21<true>, (int)l21_smem()));
+  FP_CUDA_TRY(c->err, attr_lb.ensure(k_l21<kSplitBf16>, (int)l21_smem()));
   FP_CUDA_TRY(c->err, attr_unb.ensure(k_u12<16, 1, true>, (int)CfgN::smem()));
   FP_CUDA_TRY(c->err, attr_urb.ensure(k_u12<32, 2, true>, (int)CfgR::smem()));
   if (int rc = ensure_tc_scratch(c, 0, n)) return rc;
@@ -1158,32 +971,43 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     float* const* s = c->d_tc[slot];
     {
       TraceScope tr(c, TR_DIAG);
-      if (pd2) k_pdiag2<<<1, PD2_THREADS, 0, c->stream>>>(A, lda, n, K0, cert, c->d_status);
-      else k_pdiag<<<1, kDiagThreads, pdiag_smem(), c->stream>>>(A, lda, n, K0, dinv, cert, c->d_status);
+      k_pdiag<<<1, kDiagThreads, pdiag_smem(), c->stream>>>(A, lda, n, K0, dinv, cert, c->d_status);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
-    if (pg && kend < n) {   // the full inverses (a full panel: rows below exist)
+    if (lg && kend < n) {   // the full inverses (a full panel: rows below exist)
       TraceScope tr(c, TR_PINV);
-      if (pd2) k_pinv<true><<<2 * NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
-      else k_pinv<false><<<2 * NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
+      k_pinv<<<2 * NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
     // the columns beyond the next panel need only the diagonal block's
     // inverses for their U12: the second stream starts them beside k_l21
     FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_diag, c->stream));
+    if (lside && kend < n) {   // inv(L) (the first NIB CTAs of k_pinv) on the third stream, beside k_l21
+      OnStream on3(c, c->stream3);
+      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_diag, 0));
+      {
+        TraceScope tr(c, TR_PINV);
+        k_pinv<<<NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      }
+      FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_pinv, c->stream));
+    }
     if (kend < n) {
       TraceScope tr(c, TR_L21);
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
       float* const al = bf16 ? s[1] : (xsplit ? nullptr : s[1]);
-      if (pg) {
+      if (lg) {
         if (x3) k_l21g<kSplitBf16x2><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
         else k_l21g<kSplitTf32><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
       } else if (bf16) {
-        k_l21<true><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+        k_l21<kSplitBf16><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+      } else if (x3) {
+        k_l21<kSplitBf16x2><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
       } else {
-        k_l21<false><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+        k_l21<kSplitTf32><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
       }
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1192,6 +1016,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     if (knext > kend) {
       // the next panel's columns: after the previous panel's trailing update
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
+      if (lside && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));
       {
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
@@ -1214,6 +1039,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     // after the panel's own work on the same stream
     auto rest = [&]() -> int {
       if (n > knext) {
+        if (lside) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));   // inv(L)
         {
           TraceScope tr(c, TR_STRIP);
           const unsigned g = (unsigned)((n - knext + 31) / 32);

@@ -360,7 +360,8 @@ int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* fl
  * factorisation, each launch's kernel tag (0 diagonal block, 1 block update,
  * 2 panel fix-up, 3 column strip, 4 tensor-core update, 5/6 operand splits,
  * 7 SIMT update, 8 full inverses of the diagonal block's factors),
- * its stream (0 the panel stream, 1 the trailing-update stream) and its start
+ * its stream (0 the panel stream, 1 the trailing-update stream, 2 the third
+ * stream of FP_TUNE_PANEL_GEMM 2) and its start
  * and end in ms from the start of the factorisation; count = launches. */
 int fp_trace(fp_ctx* ctx, int enable);
 int fp_trace_read(fp_ctx* ctx, int64_t cap, int* tags, int* streams, float* t0, float* t1, int64_t* count);
@@ -438,15 +439,19 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       also needs the block three back, which arrives just
  *                       before the block two back). Takes effect at the next
  *                       fp_factor
- *   FP_TUNE_PANEL_GEMM  the static-order LU of the FP32 form: 1 (default) forms
- *                       the full 128 x 128 inverses of each diagonal block's L
- *                       and U (one small kernel) and computes L21 and U12 as
- *                       one triangular product each (factorisation 13.66 ->
- *                       13.3 ms on the 12k wing with the 3xTF32 update); 2: the
- *                       same with the diagonal block factored one pivot a step
- *                       (k_pdiag2; 15.7 ms); 0: block substitution with the
- *                       32 x 32 diagonal-block inverses. The BF16 form always
- *                       uses block substitution
+ *   FP_TUNE_PANEL_GEMM  the static-order LU of the FP32 form: 2 (default) forms
+ *                       the full 128 x 128 inverse of each diagonal block's L on
+ *                       a third stream beside k_l21 (L21 by block substitution)
+ *                       and U12 = inv(L) A12 as one triangular product; 1 forms
+ *                       both full inverses on the panel stream and L21 =
+ *                       A21 inv(U) as a product too; 0: block substitution
+ *                       with the 32 x 32 diagonal-block inverses for both.
+ *                       12k wing with the BF16-pair update: 11.7 / 12.1 /
+ *                       13.1 ms of factorisation for 2 / 1 / 0 (a diagonal
+ *                       block factored one pivot a step, with register tiles
+ *                       and one barrier a pivot, measured 82 us a panel against
+ *                       43 us and was dropped). The BF16 form always uses block
+ *                       substitution
  *   FP_TUNE_TC_BF16X3   1 (default): the FP32 form's trailing update multiplies
  *                       BF16 pairs (each operand as hi + lo, C -= Ah Bl + Al Bh +
  *                       Ah Bh: three kind::f16 MMAs, half the operand bytes of

@@ -58,8 +58,8 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     assembles the FP32 AIC in panel-local FP32 coordinates and the FP64 AIC
     on a background stream; FP_TUNE_TRS2 1 runs the FP32 sweeps' chain two
     blocks a step; FP_TUNE_PANEL_GEMM 0 forms L21 and U12 by block
-    substitution, 1 as products with the full panel inverses, 2 also factors
-    the diagonal block one pivot a step (k_pdiag2). The factors are as accurate as the default's (refinement
+    substitution, 1 as products with the full panel inverses, 2 forms L21 by
+    substitution and inv(L) on a third stream, U12 as a product. The factors are as accurate as the default's (refinement
     in a handful of steps, the oracle's solution to 1e-10), for one partial
     panel up to many panels with a partial last one (1,500 panels: a last K
     block of 92)."""
