@@ -36,6 +36,7 @@ FP_TUNE_FP64_DMMA, FP_TUNE_TC_SPLIT, FP_TUNE_TC_RED, FP_TUNE_ASM32, FP_TUNE_TC_N
 FP_TUNE_TRS2 = 10
 FP_TUNE_PANEL_GEMM = 11
 FP_TUNE_TC_BF16X3 = 12
+FP_TUNE_TC_PREFETCH = 13
 
 
 class SolveOpts(C.Structure):

@@ -106,6 +106,7 @@ struct fp_ctx {
   bool trs_skip2 = false;               // FP32 sweeps: the two-block chain (FP_TUNE_TRS2)
   int panel_gemm = 2;                   // static-order FP32 LU: 1 both panel inverses, GEMM-form L21 / U12; 2: inv(L) only, beside k_l21 (FP_TUNE_PANEL_GEMM)
   bool tc_x3 = true;                    // FP32 form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
+  int tc_prefetch = 1;                  // red.global updates: idle warps prefetch the C tile into L2 (FP_TUNE_TC_PREFETCH)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)

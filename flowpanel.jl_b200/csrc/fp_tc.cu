@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(THREADS, 2)
 k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ CUtensorMap tmAl,
               const __grid_constant__ CUtensorMap tmBh, const __grid_constant__ CUtensorMap tmBl,
               const __grid_constant__ CUtensorMap tmC, int m, int n, int K, int* __restrict__ status,
-              float* __restrict__ Cp = nullptr, int64_t ldc = 0) {
+              float* __restrict__ Cp = nullptr, int64_t ldc = 0, int pf = 0) {
   constexpr int SB = BF16 ? (X3 ? 4 : 2) * TILE_A : STAGE_BYTES;   // bytes a stage
   static_assert(!X3 || BF16, "X3 splits BF16 operands");
   constexpr int KB = BF16 ? 32 : BK;                    // K elements a stage
@@ -185,6 +185,16 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
+  if (RED && pf && warp >= 2) {
+    // warps 2 and 3 only wait for the accumulator during the main loop:
+    // meanwhile they bring the CTA's C tile into L2 (one bulk prefetch of up
+    // to 512 bytes a column), so that the epilogue's reductions find it there
+    const uint32_t bytes = (uint32_t)(min(BM, m - m0) * 4) & ~15u;
+    if (bytes)
+      for (int cc = threadIdx.x - 64; cc < BN && n0 + cc < n; cc += 64)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Cp + (int64_t)(n0 + cc) * ldc + m0), "r"(bytes)
+                     : "memory");
+  }
   if (warp == 0 && lane == 0) {
     // producer
     int issued = 0;
@@ -911,13 +921,13 @@ bool tc_gemm_sub_presplit(fp_ctx* c, const float* Ah, const float* Al, const flo
     // critical path): at most one CTA an SM, so a 6-stage ring costs no
     // occupancy and puts 6 of the 8 K blocks in flight at once
     tc::k_tc_gemm_sub<6, true><<<grid, tc::THREADS, tc::smem_bytes<6>(), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   else if (c->tc_red && c->tc_stages == 3)
     tc::k_tc_gemm_sub<3, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<3>(), c->tc_smem), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   else if (c->tc_red)
     tc::k_tc_gemm_sub<2, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   else if (c->tc_stages == 2)
     tc::k_tc_gemm_sub<2><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
         mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status);
@@ -997,10 +1007,10 @@ bool tc_gemm_sub_bf16x3(fp_ctx* c, const void* Ah, const void* Al, const void* B
   TraceScope tr(c, TR_GEMM_TC);
   if (c->tc_narrow_stages == 6 && grid.y == 1 && (int)grid.x <= num_sms())
     tc::k_tc_gemm_sub<6, true, true, true><<<grid, tc::THREADS, tc::smem_bytes<6>(), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   else
     tc::k_tc_gemm_sub<2, true, true, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;

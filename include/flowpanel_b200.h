@@ -458,7 +458,13 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       3xTF32; the 16-bit operand splits leave the refinement
  *                       at 4 steps on the 12k wing: factorisation 13.3 ->
  *                       12.1 ms); 0: 3xTF32 (TF32 pairs). Needs
- *                       FP_TUNE_PANEL_GEMM 1 or 2 */
+ *                       FP_TUNE_PANEL_GEMM 1 or 2
+ *   FP_TUNE_TC_PREFETCH 1 (default): in the tensor-core updates with the
+ *                       red.global epilogue, the two warps that wait for the
+ *                       accumulator prefetch the CTA's C tile into L2 during
+ *                       the main loop (12k wing: update 93 -> 84 us a panel,
+ *                       factorisation 11.85 -> 11.10 ms); 0: the reductions
+ *                       fetch C */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -472,6 +478,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_TRS2 10
 #define FP_TUNE_PANEL_GEMM 11
 #define FP_TUNE_TC_BF16X3 12
+#define FP_TUNE_TC_PREFETCH 13
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

@@ -48,7 +48,8 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
 @pytest.mark.parametrize("knob,value", [("FP_TUNE_TC_SPLIT", 1), ("FP_TUNE_TC_SPLIT", 2), ("FP_TUNE_TC_SPLIT", 3),
                                         ("FP_TUNE_TC_RED", 0), ("FP_TUNE_TC_TILES", 2), ("FP_TUNE_TC_TILES", 4),
                                         ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0), ("FP_TUNE_TRS2", 1),
-                                        ("FP_TUNE_PANEL_GEMM", 0), ("FP_TUNE_PANEL_GEMM", 1), ("FP_TUNE_PANEL_GEMM", 2)])
+                                        ("FP_TUNE_PANEL_GEMM", 0), ("FP_TUNE_PANEL_GEMM", 1), ("FP_TUNE_PANEL_GEMM", 2),
+                                        ("FP_TUNE_TC_PREFETCH", 1)])
 def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
     1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
@@ -59,7 +60,8 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     on a background stream; FP_TUNE_TRS2 1 runs the FP32 sweeps' chain two
     blocks a step; FP_TUNE_PANEL_GEMM 0 forms L21 and U12 by block
     substitution, 1 as products with the full panel inverses, 2 forms L21 by
-    substitution and inv(L) on a third stream, U12 as a product. The factors are as accurate as the default's (refinement
+    substitution and inv(L) on a third stream, U12 as a product;
+    FP_TUNE_TC_PREFETCH 1 prefetches each CTA's C tile into L2. The factors are as accurate as the default's (refinement
     in a handful of steps, the oracle's solution to 1e-10), for one partial
     panel up to many panels with a partial last one (1,500 panels: a last K
     block of 92)."""
@@ -89,8 +91,8 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
 
 
 @pytest.mark.parametrize("nc,ns", [(12, 8), (20, 24), (60, 80), (50, 30)])
-@pytest.mark.parametrize("panel", [1, 2])
-def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel):
+@pytest.mark.parametrize("panel,prefetch", [(1, 0), (2, 0), (2, 1)])
+def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch):
     """FP_TUNE_TC_BF16X3 1: the mixed form's trailing update multiplies BF16
     pairs (hi + lo, three MMAs) instead of TF32 pairs; the factors carry 16-bit
     operand splits, and the FP64 refinement (GMRES-IR behind it) still reaches
@@ -108,6 +110,7 @@ def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel):
     try:
         c.set_tuning(fp._capi.FP_TUNE_PANEL_GEMM, panel)
         c.set_tuning(fp._capi.FP_TUNE_TC_BF16X3, 1)
+        c.set_tuning(fp._capi.FP_TUNE_TC_PREFETCH, prefetch)
         c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
         c.set_wake(w.shedding, D, D)
         x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
