@@ -961,7 +961,7 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 template <int NT, int MF, int NF, int BK = 16, int STAGES = 3, int BN = 128, int MINB = 1>
 __global__ void __launch_bounds__(NT, MINB)
 k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, double* __restrict__ Cm, int64_t lda,
-                int64_t m, int64_t nn, int kk) {
+                int64_t m, int64_t nn, int kk, int pf) {
   using namespace dm;
   constexpr int BP = bp<BK>();
   constexpr int WARPS_M = BM / (8 * MF);
@@ -973,6 +973,13 @@ k_gemm_sub_dmma(const double* __restrict__ Am, const double* __restrict__ Bm, do
   const int wm = (warp % WARPS_M) * 8 * MF, wn = (warp / WARPS_M) * 8 * NF;
   const int64_t i0 = (int64_t)blockIdx.x * BM, j0 = (int64_t)blockIdx.y * BN;
   const int nk = (kk + BK - 1) / BK;
+  if (pf && tid < BN && j0 + tid < nn) {
+    // the epilogue reads the C tile once: bring it into L2 (one bulk prefetch
+    // of up to BM doubles a column) while the K loop runs
+    const uint32_t bytes = (uint32_t)(imin64(BM, m - i0) * 8) & ~15u;
+    if (bytes)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Cm + (j0 + tid) * lda + i0), "r"(bytes) : "memory");
+  }
   // one K slice into stage s: 1024 16-byte pieces of A and 1024 of B
   auto issue = [&](int kb, int s) {
     double* As = ring + (size_t)s * stage_doubles<BK, BN>();
@@ -1076,18 +1083,18 @@ static int gemm_sub(fp_ctx* c, const T* Am, const T* Bm, T* Cm, int64_t lda, int
       double* Cd = (double*)Cm;
       if (c->fp64_dmma == 6) {   // 128 x 64 tiles, two CTAs an SM, 32-deep K slices in 2 stages
         dim3 g2((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + 63) / 64));
-        k_gemm_sub_dmma<512, 4, 2, 32, 2, 64, 2><<<g2, 512, sm64k, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+        k_gemm_sub_dmma<512, 4, 2, 32, 2, 64, 2><<<g2, 512, sm64k, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk, c->tc_prefetch);
       } else if (c->fp64_dmma == 5) {   // 128 x 64 tiles, two CTAs an SM
         dim3 g2((unsigned)((m + dm::BM - 1) / dm::BM), (unsigned)((nn + 63) / 64));
-        k_gemm_sub_dmma<512, 4, 2, 16, 3, 64, 2><<<g2, 512, sm64, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+        k_gemm_sub_dmma<512, 4, 2, 16, 3, 64, 2><<<g2, 512, sm64, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk, c->tc_prefetch);
       } else if (c->fp64_dmma == 4)
-        k_gemm_sub_dmma<1024, 4, 2, 32, 3><<<g, 1024, sm32, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+        k_gemm_sub_dmma<1024, 4, 2, 32, 3><<<g, 1024, sm32, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk, c->tc_prefetch);
       else if (c->fp64_dmma == 3)
-        k_gemm_sub_dmma<1024, 4, 2><<<g, 1024, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+        k_gemm_sub_dmma<1024, 4, 2><<<g, 1024, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk, c->tc_prefetch);
       else if (c->fp64_dmma == 2)
-        k_gemm_sub_dmma<512, 4, 4><<<g, 512, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+        k_gemm_sub_dmma<512, 4, 4><<<g, 512, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk, c->tc_prefetch);
       else
-        k_gemm_sub_dmma<256, 8, 4><<<g, 256, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk);
+        k_gemm_sub_dmma<256, 8, 4><<<g, 256, sm16, c->stream>>>(Ad, Bd, Cd, lda, m, nn, kk, c->tc_prefetch);
     } else if (mis == 0) {
       static SmemAttr attr;
       FP_CUDA_TRY(c->err, attr.ensure(k_gemm_sub_f64, (int)d64::smem()));

@@ -1047,7 +1047,7 @@ bool tc_gemm_sub_bf16(fp_ctx* c, const void* Ah, const void* Bh, int ldk, float*
     dim3 grid((unsigned)((m + tc::BM - 1) / tc::BM), (unsigned)((nn + tc::BN - 1) / tc::BN));
     constexpr int sb = 4 * 2 * tc::TILE_A + 1024 + 256;
     tc::k_tc_gemm_sub<4, true, true><<<grid, tc::THREADS, std::max(sb, c->tc_smem), c->stream>>>(
-        mA, mA, mB, mB, mC, (int)m, (int)nn, kk, c->d_status, C, ldc);
+        mA, mA, mB, mB, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   } else {
     const int tpc = c->tc_tiles > 0 ? c->tc_tiles : 4;
     tc::k_tc_gemm_multi<true><<<(unsigned)((tiles + tpc - 1) / tpc), tc::mt::THREADS, tc::mt::smem<true>(),

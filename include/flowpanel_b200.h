@@ -463,8 +463,9 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       red.global epilogue, the two warps that wait for the
  *                       accumulator prefetch the CTA's C tile into L2 during
  *                       the main loop (12k wing: update 93 -> 84 us a panel,
- *                       factorisation 11.85 -> 11.10 ms); 0: the reductions
- *                       fetch C */
+ *                       factorisation 11.85 -> 11.10 ms); the FP64 LU's
+ *                       tensor-path update prefetches its C tile at the start
+ *                       the same way; 0: the epilogues fetch C */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
