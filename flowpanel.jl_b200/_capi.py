@@ -37,6 +37,7 @@ FP_TUNE_TRS2 = 10
 FP_TUNE_PANEL_GEMM = 11
 FP_TUNE_TC_BF16X3 = 12
 FP_TUNE_TC_PREFETCH = 13
+FP_TUNE_PDL = 14
 
 
 class SolveOpts(C.Structure):

@@ -39,6 +39,11 @@ struct ErrorSink {
     }                                                                                \
   } while (0)
 
+// Programmatic dependent launch: hold this grid until the grids it depends
+// on have completed and their memory is visible (a no-op for a grid launched
+// without the programmatic attribute).
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 

@@ -107,6 +107,7 @@ struct fp_ctx {
   int panel_gemm = 2;                   // static-order FP32 LU: 1 both panel inverses, GEMM-form L21 / U12; 2: inv(L) only, beside k_l21 (FP_TUNE_PANEL_GEMM)
   bool tc_x3 = true;                    // FP32 form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
   int tc_prefetch = 1;                  // red.global updates: idle warps prefetch the C tile into L2 (FP_TUNE_TC_PREFETCH)
+  bool pdl = true;                      // static-order LU: programmatic dependent launch of its kernels (FP_TUNE_PDL)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)
@@ -323,6 +324,27 @@ struct SmemAttr {
     return e;
   }
 };
+
+// Launches kernel on stream s, with programmatic dependent launch when pdl:
+// the launch may begin before the stream's previous kernel has finished, and
+// the kernel's griddep_wait() holds it until that kernel's results are
+// visible. Only kernels that call griddep_wait() before reading what their
+// predecessors wrote may be launched with pdl.
+template <class... KArgs, class... Args>
+inline cudaError_t launch_k(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? at : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Routes the launches of a section to stream s (tensor-core scratch unchanged).
 struct OnStream {

@@ -385,6 +385,7 @@ __device__ __forceinline__ void update_tiles(float (*As)[SP], const float (*LT)[
 __global__ void __launch_bounds__(kDiagThreads, 1)
 k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ dinv,
         float* __restrict__ cert, int* __restrict__ status) {
+  griddep_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   float (*As)[SP] = reinterpret_cast<float (*)[SP]>(smem);
   float (*LT)[SP] = reinterpret_cast<float (*)[SP]>(smem + (size_t)PW * SP * sizeof(float));
@@ -473,6 +474,7 @@ template <int SM>
 __global__ void __launch_bounds__(L21_THREADS)
 k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, const float* __restrict__ dinv,
       float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
+  griddep_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   float (*X)[XP] = reinterpret_cast<float (*)[XP]>(smem);
   // Ub[s][c - IB] = U(s, c) for s < 96, c >= 32 (entries below the diagonal blocks are not read)
@@ -573,6 +575,7 @@ template <int CW, int RT, bool BF16>
 __global__ void __launch_bounds__(U12Cfg<CW, RT>::THREADS)
 k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, const float* __restrict__ dinv,
       float* __restrict__ Bh, float* __restrict__ Bl) {
+  griddep_wait();
   typedef U12Cfg<CW, RT> Cfg;
   constexpr int T = Cfg::THREADS, ZP = Cfg::ZP, LP = Cfg::LP;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -705,6 +708,7 @@ constexpr size_t pinv_smem() {
 }
 __global__ void __launch_bounds__(PI_THREADS)
 k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ slot) {
+  griddep_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   float (*G)[GP] = reinterpret_cast<float (*)[GP]>(smem);
   float (*Ds)[DP] = reinterpret_cast<float (*)[DP]>(smem + (size_t)PW * GP * sizeof(float));
@@ -771,6 +775,7 @@ template <int SM>
 __global__ void __launch_bounds__(L21G_THREADS)
 k_l21g(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, const float* __restrict__ slot,
        float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
+  griddep_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   float (*XT)[DP] = reinterpret_cast<float (*)[DP]>(smem);   // XT[s][r] = A21(r, s)
   float (*Us)[GP] = reinterpret_cast<float (*)[GP]>(smem + (size_t)PW * DP * sizeof(float));
@@ -842,6 +847,7 @@ template <int CW, int SM>
 __global__ void __launch_bounds__(U12gCfg<CW>::THREADS)
 k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, const float* __restrict__ slot,
        float* __restrict__ Bh, float* __restrict__ Bl) {
+  griddep_wait();
   typedef U12gCfg<CW> Cfg;
   constexpr int T = Cfg::THREADS, ZP = Cfg::ZP, CQ = CW / 4;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -971,13 +977,13 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     float* const* s = c->d_tc[slot];
     {
       TraceScope tr(c, TR_DIAG);
-      k_pdiag<<<1, kDiagThreads, pdiag_smem(), c->stream>>>(A, lda, n, K0, dinv, cert, c->d_status);
+      launch_k(c->pdl, k_pdiag, 1, kDiagThreads, pdiag_smem(), c->stream, A, lda, n, K0, dinv, cert, c->d_status);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
     if (lg && kend < n) {   // the full inverses (a full panel: rows below exist)
       TraceScope tr(c, TR_PINV);
-      k_pinv<<<2 * NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
+      launch_k(c->pdl, k_pinv, 2 * NIB, PI_THREADS, pinv_smem(), c->stream, A, lda, K0, dinv);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
@@ -989,7 +995,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_diag, 0));
       {
         TraceScope tr(c, TR_PINV);
-        k_pinv<<<NIB, PI_THREADS, pinv_smem(), c->stream>>>(A, lda, K0, dinv);
+        launch_k(c->pdl, k_pinv, NIB, PI_THREADS, pinv_smem(), c->stream, A, lda, K0, dinv);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
@@ -1000,14 +1006,14 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
       float* const al = bf16 ? s[1] : (xsplit ? nullptr : s[1]);
       if (lg) {
-        if (x3) k_l21g<kSplitBf16x2><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
-        else k_l21g<kSplitTf32><<<g, L21G_THREADS, l21g_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+        if (x3) launch_k(c->pdl, k_l21g<kSplitBf16x2>, g, L21G_THREADS, l21g_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+        else launch_k(c->pdl, k_l21g<kSplitTf32>, g, L21G_THREADS, l21g_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
       } else if (bf16) {
-        k_l21<kSplitBf16><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+        launch_k(c->pdl, k_l21<kSplitBf16>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
       } else if (x3) {
-        k_l21<kSplitBf16x2><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+        launch_k(c->pdl, k_l21<kSplitBf16x2>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], s[1], cert);
       } else {
-        k_l21<kSplitTf32><<<g, L21_THREADS, l21_smem(), c->stream>>>(A, lda, n, K0, kend, dinv, s[0], al, cert);
+        launch_k(c->pdl, k_l21<kSplitTf32>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
       }
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1021,14 +1027,14 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
         if (x3)
-          k_u12g<16, kSplitBf16x2><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+          launch_k(c->pdl, k_u12g<16, kSplitBf16x2>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else if (pg)
-          k_u12g<16, kSplitTf32><<<g, GCfgN::THREADS, GCfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
+          launch_k(c->pdl, k_u12g<16, kSplitTf32>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2],
                                                                                      xsplit ? nullptr : s[3]);
         else if (bf16)
-          k_u12<16, 1, true><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2], s[3]);
+          launch_k(c->pdl, k_u12<16, 1, true>, g, CfgN::THREADS, CfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else
-          k_u12<16, 1, false><<<g, CfgN::THREADS, CfgN::smem(), c->stream>>>(A, lda, K0, kend, knext, dinv, s[2],
+          launch_k(c->pdl, k_u12<16, 1, false>, g, CfgN::THREADS, CfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2],
                                                                               xsplit ? nullptr : s[3]);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1049,15 +1055,15 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           };
           float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
           if (x3)
-            k_u12g<32, kSplitBf16x2><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh,
+            launch_k(c->pdl, k_u12g<32, kSplitBf16x2>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh,
                                                                                         b16(s[3]));
           else if (pg)
-            k_u12g<32, kSplitTf32><<<g, GCfgR::THREADS, GCfgR::smem(), c->stream>>>(
+            launch_k(c->pdl, k_u12g<32, kSplitTf32>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, 
                 A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
           else if (bf16)
-            k_u12<32, 2, true><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(A, lda, K0, knext, n, dinv, bh, nullptr);
+            launch_k(c->pdl, k_u12<32, 2, true>, g, CfgR::THREADS, CfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh, nullptr);
           else
-            k_u12<32, 2, false><<<g, CfgR::THREADS, CfgR::smem(), c->stream>>>(
+            launch_k(c->pdl, k_u12<32, 2, false>, g, CfgR::THREADS, CfgR::smem(), c->stream, 
                 A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
           ++c->nlaunch;
           FP_CUDA_TRY(c->err, cudaGetLastError());

@@ -195,6 +195,7 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(Cp + (int64_t)(n0 + cc) * ldc + m0), "r"(bytes)
                      : "memory");
   }
+  griddep_wait();   // the operands and C come from the stream's earlier kernels
   if (warp == 0 && lane == 0) {
     // producer
     int issued = 0;
@@ -1006,11 +1007,12 @@ bool tc_gemm_sub_bf16x3(fp_ctx* c, const void* Ah, const void* Al, const void* B
   const int ev = kt_begin(c);
   TraceScope tr(c, TR_GEMM_TC);
   if (c->tc_narrow_stages == 6 && grid.y == 1 && (int)grid.x <= num_sms())
-    tc::k_tc_gemm_sub<6, true, true, true><<<grid, tc::THREADS, tc::smem_bytes<6>(), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
+    launch_k(c->pdl, tc::k_tc_gemm_sub<6, true, true, true>, grid, dim3(tc::THREADS), tc::smem_bytes<6>(), c->stream,
+             mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
   else
-    tc::k_tc_gemm_sub<2, true, true, true><<<grid, tc::THREADS, std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream>>>(
-        mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk, c->d_status, C, ldc, c->tc_prefetch);
+    launch_k(c->pdl, tc::k_tc_gemm_sub<2, true, true, true>, grid, dim3(tc::THREADS),
+             std::max(tc::smem_bytes<2>(), c->tc_smem), c->stream, mAh, mAl, mBh, mBl, mC, (int)m, (int)nn, kk,
+             c->d_status, C, ldc, c->tc_prefetch);
   kt_end(c, ev, 2.0 * (double)m * (double)nn * (double)kk, (double)m * (double)nn);
   ++c->nlaunch;
   return cudaGetLastError() == cudaSuccess;

@@ -465,7 +465,12 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       the main loop (12k wing: update 93 -> 84 us a panel,
  *                       factorisation 11.85 -> 11.10 ms); the FP64 LU's
  *                       tensor-path update prefetches its C tile at the start
- *                       the same way; 0: the epilogues fetch C */
+ *                       the same way; 0: the epilogues fetch C
+ *   FP_TUNE_PDL         1 (default): the static-order LU's kernels (and its
+ *                       BF16-pair updates) are launched with programmatic
+ *                       dependent launch, so that a kernel's launch overlaps
+ *                       the end of its stream's previous kernel (12k wing:
+ *                       factorisation 11.12 -> 10.79 ms); 0: plain launches */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -480,6 +485,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_PANEL_GEMM 11
 #define FP_TUNE_TC_BF16X3 12
 #define FP_TUNE_TC_PREFETCH 13
+#define FP_TUNE_PDL 14
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the
