@@ -43,6 +43,9 @@ struct ErrorSink {
 // on have completed and their memory is visible (a no-op for a grid launched
 // without the programmatic attribute).
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the stream's next grid (launched with the programmatic attribute) begin
+// its launch: that grid still waits in griddep_wait() for this one to finish.
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 inline int64_t round_up(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
 __host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }

@@ -414,6 +414,7 @@ k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restr
     __syncthreads();
   }
   __syncthreads();
+  griddep_launch();
   // write the factors back (16-byte stores down the columns)
   store_block<kDiagThreads, PW, PW>(A + k * lda + k, lda, nb, nb, [&](int r, int c) { return As[r][c]; }, tid);
 #pragma unroll
@@ -536,6 +537,7 @@ k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, cons
       for (int j = 0; j < 4; ++j) X[2 * rg + i][c0 + 4 * cg + j] = l[i][j];
     __syncthreads();
   }
+  griddep_launch();
   store_block<L21_THREADS, L21_ROWS, PW>(A + k * lda + row0, lda, rows, PW, [&](int r, int c) { return X[r][c]; },
                                         tid);
   float lmax = 0.f;
@@ -640,6 +642,7 @@ k_u12(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, con
       for (int j = 0; j < 4; ++j) Z[t0 + RT * rq + i][4 * cq + j] = u[i][j];
     __syncthreads();
   }
+  griddep_launch();
   store_block<T, PW, CW>(A + col0 * lda + k, lda, PW, cols, [&](int r, int c) { return Z[r][c]; }, tid);
   constexpr int R4 = PW / 4;
   for (int e = tid; e < cols * R4; e += T) {   // the split, K-major: column j - c0 holds its PW values
@@ -753,6 +756,7 @@ k_pinv(const float* __restrict__ A, int64_t lda, int64_t k, float* __restrict__ 
     *reinterpret_cast<float4*>(&Xs[IB * i + r][c]) = make_float4(-y[0], -y[1], -y[2], -y[3]);
     __syncthreads();
   }
+  griddep_launch();
   // out[IB j + cc][q] = X(q, cc) for q >= IB j, 0 above
   float* const out = slot + (upper ? kUinvOff : kLinvtOff);
 #pragma unroll
@@ -806,6 +810,7 @@ k_l21g(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, con
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(xv[a], uv[b], acc[a][b]);
   }
+  griddep_launch();
   float lmax = 0.f;
 #pragma unroll
   for (int b = 0; b < 4; ++b) {   // L21 in place: column k + cb + b, rows row0 + rb ..
@@ -878,6 +883,7 @@ k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, co
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(lv[a], zv[b], acc[a][b]);
   }
+  griddep_launch();
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     if (cb + b >= cols) break;

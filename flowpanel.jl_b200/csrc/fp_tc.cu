@@ -273,6 +273,7 @@ k_tc_gemm_sub(const __grid_constant__ CUtensorMap tmAh, const __grid_constant__ 
   // warp-uniform: the epilogue's tcgen05.ld is a .sync.aligned warp instruction
   const bool ok = __all_sync(0xffffffffu, mbar_wait(done, 0));
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  griddep_launch();
   if (ok && RED) {
     const int64_t row = (int64_t)m0 + warp * 32 + lane;
     float* cp = Cp + (int64_t)n0 * ldc + row;
