@@ -38,6 +38,7 @@ FP_TUNE_PANEL_GEMM = 11
 FP_TUNE_TC_BF16X3 = 12
 FP_TUNE_TC_PREFETCH = 13
 FP_TUNE_PDL = 14
+FP_TUNE_LU_SPLIT = 15
 
 
 class SolveOpts(C.Structure):

@@ -159,6 +159,9 @@ int fp_ctx_create(int device, fp_ctx** out) {
       cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_pinv, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_u12n, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_tcr, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_l21t, cudaEventDisableTiming) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream_bg, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_g64, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_diag, cudaEventDisableTiming) != cudaSuccess ||
@@ -197,6 +200,9 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->ev_diag) cudaEventDestroy(c->ev_diag);
   if (c->ev_asm) cudaEventDestroy(c->ev_asm);
   if (c->ev_pinv) cudaEventDestroy(c->ev_pinv);
+  if (c->ev_u12n) cudaEventDestroy(c->ev_u12n);
+  if (c->ev_tcr) cudaEventDestroy(c->ev_tcr);
+  if (c->ev_l21t) cudaEventDestroy(c->ev_l21t);
   if (c->stream3) cudaStreamDestroy(c->stream3);
   if (c->stream_bg) cudaStreamDestroy(c->stream_bg);
   if (c->stream2) cudaStreamDestroy(c->stream2);
@@ -931,6 +937,9 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       return FP_OK;
     case FP_TUNE_PDL:
       c->pdl = value != 0;
+      return FP_OK;
+    case FP_TUNE_LU_SPLIT:
+      c->lu_split = value != 0;
       return FP_OK;
     case FP_TUNE_TC_NARROW:
       if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");

@@ -107,6 +107,7 @@ struct fp_ctx {
   int panel_gemm = 2;                   // static-order FP32 LU: 1 both panel inverses, GEMM-form L21 / U12; 2: inv(L) only, beside k_l21 (FP_TUNE_PANEL_GEMM)
   bool tc_x3 = true;                    // FP32 form: the update from BF16 pairs, three MMAs (FP_TUNE_TC_BF16X3)
   int tc_prefetch = 1;                  // red.global updates: idle warps prefetch the C tile into L2 (FP_TUNE_TC_PREFETCH)
+  bool lu_split = true;                 // static-order LU: split panel chain (FP_TUNE_LU_SPLIT)
   bool pdl = true;                      // static-order LU: programmatic dependent launch of its kernels (FP_TUNE_PDL)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
@@ -180,6 +181,9 @@ struct fp_ctx {
   cudaEvent_t ev_diag = nullptr;        // static-order LU: diagonal block factored (stream -> stream2)
   cudaEvent_t ev_rest = nullptr;        // trailing update done (stream2 -> stream)
   cudaEvent_t ev_pinv = nullptr;        // static-order LU: inv(L) formed (stream3 -> stream, stream2)
+  cudaEvent_t ev_u12n = nullptr;        // split panel chain: the next panel's U12 formed (stream -> stream3)
+  cudaEvent_t ev_tcr = nullptr;         // split panel chain: the rows below the next panel updated (stream3 -> stream)
+  cudaEvent_t ev_l21t = nullptr;        // split panel chain: L21 of the rows below the next panel (stream3 -> stream2)
 
   // surface post-processing (fp_post.cu). The mesh topology of a triangular
   // body is built on first use after fp_set_geometry, the Kutta-average

@@ -454,7 +454,8 @@ __device__ __forceinline__ void put_split(float* __restrict__ hi, float* __restr
 }
 
 // ---------------------------------------------------------------------------
-// K6: L21 = A21 U^-1 for the rows [r0 + 32 b, +32) below the panel at k, by
+// K6: L21 = A21 U^-1 for the rows [rbeg + 32 b, +32) (rows [r0, n) below the
+// panel at k, the split operand indexed from r0) by
 // block substitution over the four inner column blocks t:
 //   Y_t = A21_t - sum_{s < t} L_s U(s, t),   L_t = Y_t inv(U_tt).
 // The row block, the panel's U above the diagonal blocks and the four
@@ -473,7 +474,7 @@ constexpr size_t l21_smem() {
 
 template <int SM>
 __global__ void __launch_bounds__(L21_THREADS)
-k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, const float* __restrict__ dinv,
+k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, int64_t rbeg, const float* __restrict__ dinv,
       float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
   griddep_wait();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -483,7 +484,7 @@ k_l21(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, cons
   float (*Ut)[UP] = reinterpret_cast<float (*)[UP]>(reinterpret_cast<unsigned char*>(Ub) +
                                                      (size_t)(PW - IB) * UBP * sizeof(float));   // inv(U_tt), 4 x 32 rows
   const int tid = threadIdx.x;
-  const int64_t row0 = r0 + (int64_t)blockIdx.x * L21_ROWS;
+  const int64_t row0 = rbeg + (int64_t)blockIdx.x * L21_ROWS;   // rows [rbeg, n); the split is indexed from r0
   const int rows = (int)imin64(L21_ROWS, n - row0);
   {   // all loads in flight before the first store
     const auto zero = [](int, int) { return 0.f; };
@@ -954,27 +955,35 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream2, c->ev_rest, 0));
   // C -= L21 U12 on the rows [kend, n) and columns [cb, ce): tensor cores from
   // the split operands, or the SIMT kernel on the factors in place
-  auto update = [&](int slot, int64_t kend, int64_t K0, int64_t cb, int64_t ce, int64_t boff) -> int {
-    const int64_t m = n - kend, nn = ce - cb;
+  // (rows [kend + roff, kend + roff + mrows), mrows < 0: to n; roff rows into the L21 operand)
+  auto update = [&](int slot, int64_t kend, int64_t K0, int64_t cb, int64_t ce, int64_t boff, int64_t roff = 0,
+                    int64_t mrows = -1) -> int {
+    const int64_t r0 = kend + roff;
+    const int64_t m = mrows < 0 ? n - r0 : std::min<int64_t>(mrows, n - r0), nn = ce - cb;
     if (m <= 0 || nn <= 0) return FP_OK;
     float* const* s = c->d_tc[slot];
     const int kk = (int)std::min<int64_t>(PW, n - K0);
+    const int64_t ao = roff * PW;   // the L21 operand's rows are PW elements apart (bf16 or float)
     if (bf16) {
+      const __nv_bfloat16* ah = reinterpret_cast<const __nv_bfloat16*>(s[0]) + ao;
       const __nv_bfloat16* bh = reinterpret_cast<const __nv_bfloat16*>(s[2]) + boff * PW;
-      if (c->use_tc && tc_gemm_sub_bf16(c, s[0], bh, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
+      if (c->use_tc && tc_gemm_sub_bf16(c, ah, bh, PW, at(r0, cb), lda, m, nn, kk)) return FP_OK;
     } else if (x3) {
+      const __nv_bfloat16* ah = reinterpret_cast<const __nv_bfloat16*>(s[0]) + ao;
+      const __nv_bfloat16* al = reinterpret_cast<const __nv_bfloat16*>(s[1]) + ao;
       const __nv_bfloat16* bh = reinterpret_cast<const __nv_bfloat16*>(s[2]) + boff * PW;
       const __nv_bfloat16* bl = reinterpret_cast<const __nv_bfloat16*>(s[3]) + boff * PW;
-      if (tc_gemm_sub_bf16x3(c, s[0], s[1], bh, bl, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
+      if (tc_gemm_sub_bf16x3(c, ah, al, bh, bl, PW, at(r0, cb), lda, m, nn, kk)) return FP_OK;
     } else if (xsplit) {
-      if (c->use_tc && tc_gemm_sub_xsplit(c, s[0], s[2] + boff * PW, PW, at(kend, cb), lda, m, nn, kk)) return FP_OK;
-    } else if (c->use_tc && tc_gemm_sub_presplit(c, s[0], s[1], s[2] + boff * PW, s[3] + boff * PW, PW, at(kend, cb),
-                                                 lda, m, nn, kk)) {
+      if (c->use_tc && tc_gemm_sub_xsplit(c, s[0] + ao, s[2] + boff * PW, PW, at(r0, cb), lda, m, nn, kk)) return FP_OK;
+    } else if (c->use_tc && tc_gemm_sub_presplit(c, s[0] + ao, s[1] + ao, s[2] + boff * PW, s[3] + boff * PW, PW,
+                                                 at(r0, cb), lda, m, nn, kk)) {
       return FP_OK;
     }
     FP_CUDA_TRY(c->err, cudaGetLastError());
-    return gemm_sub_simt_f32(c, at(kend, K0), at(K0, cb), at(kend, cb), lda, m, nn, (int)std::min<int64_t>(PW, n - K0));
+    return gemm_sub_simt_f32(c, at(r0, K0), at(K0, cb), at(r0, cb), lda, m, nn, (int)std::min<int64_t>(PW, n - K0));
   };
+  bool prev_split = false;   // the previous panel's rows below the next one were left to the third stream
   for (int64_t K0 = 0; K0 < n; K0 += PW) {
     const int64_t kend = std::min<int64_t>(K0 + PW, n);
     const int64_t knext = std::min<int64_t>(kend + PW, n);
@@ -1007,7 +1016,41 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       }
       FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_pinv, c->stream));
     }
-    if (kend < n) {
+    // split: the panel stream keeps only what the next diagonal block needs
+    // (L21 and the next-panel update of the next panel's 128 rows); the
+    // third stream does the rows below, beside the next k_pdiag
+    const bool sp = c->lu_split && lside && c->lu_overlap && kend + PW < n;
+    // the rows below this panel's diagonal block were last updated on the third stream
+    if (prev_split && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_tcr, 0));
+    if (sp) {
+      float* const al = s[1];
+      {
+        TraceScope tr(c, TR_L21);
+        const int64_t he = kend + PW;   // the next panel's rows
+        if (x3)
+          launch_k(c->pdl, k_l21<kSplitBf16x2>, (unsigned)(PW / L21_ROWS), L21_THREADS, l21_smem(), c->stream, A, lda,
+                   he, K0, kend, kend, dinv, s[0], s[1], cert);
+        else
+          launch_k(c->pdl, k_l21<kSplitTf32>, (unsigned)(PW / L21_ROWS), L21_THREADS, l21_smem(), c->stream, A, lda, he,
+                   K0, kend, kend, dinv, s[0], xsplit ? nullptr : al, cert);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      }
+      OnStream on3(c, c->stream3);
+      {
+        TraceScope tr(c, TR_L21);
+        const unsigned g = (unsigned)((n - kend - PW + L21_ROWS - 1) / L21_ROWS);
+        if (x3)
+          launch_k(c->pdl, k_l21<kSplitBf16x2>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend + PW,
+                   dinv, s[0], s[1], cert);
+        else
+          launch_k(c->pdl, k_l21<kSplitTf32>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend + PW, dinv,
+                   s[0], xsplit ? nullptr : al, cert);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      }
+      FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_l21t, c->stream));
+    } else if (kend < n) {
       TraceScope tr(c, TR_L21);
       const unsigned g = (unsigned)((n - kend + L21_ROWS - 1) / L21_ROWS);
       float* const al = bf16 ? s[1] : (xsplit ? nullptr : s[1]);
@@ -1015,11 +1058,11 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         if (x3) launch_k(c->pdl, k_l21g<kSplitBf16x2>, g, L21G_THREADS, l21g_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], s[1], cert);
         else launch_k(c->pdl, k_l21g<kSplitTf32>, g, L21G_THREADS, l21g_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
       } else if (bf16) {
-        launch_k(c->pdl, k_l21<kSplitBf16>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
+        launch_k(c->pdl, k_l21<kSplitBf16>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], al, cert);
       } else if (x3) {
-        launch_k(c->pdl, k_l21<kSplitBf16x2>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], s[1], cert);
+        launch_k(c->pdl, k_l21<kSplitBf16x2>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], s[1], cert);
       } else {
-        launch_k(c->pdl, k_l21<kSplitTf32>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
+        launch_k(c->pdl, k_l21<kSplitTf32>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], al, cert);
       }
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1045,8 +1088,18 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
-      if (int rc = update(slot, kend, K0, kend, knext, 0)) return rc;
+      if (sp) {
+        FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_u12n, c->stream));
+        if (int rc = update(slot, kend, K0, kend, knext, 0, 0, PW)) return rc;   // the next diagonal block's rows
+        OnStream on3(c, c->stream3);
+        FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_u12n, 0));
+        if (int rc = update(slot, kend, K0, kend, knext, 0, PW)) return rc;      // the rows below
+        FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_tcr, c->stream));
+      } else if (int rc = update(slot, kend, K0, kend, knext, 0)) {
+        return rc;
+      }
     }
+    prev_split = sp;
     // the columns beyond the next panel: on the second stream (look-ahead), or
     // after the panel's own work on the same stream
     auto rest = [&]() -> int {
@@ -1074,8 +1127,9 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           ++c->nlaunch;
           FP_CUDA_TRY(c->err, cudaGetLastError());
         }
-        // the update reads L21 (the panel stream's k_l21)
+        // the update reads L21 (the panel stream's k_l21, and the third stream's when split)
         if (c->lu_overlap) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
+        if (sp) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_l21t, 0));
         if (int rc = update(slot, kend, K0, knext, n, knext - kend)) return rc;
       }
       return FP_OK;

@@ -470,7 +470,15 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       BF16-pair updates) are launched with programmatic
  *                       dependent launch, so that a kernel's launch overlaps
  *                       the end of its stream's previous kernel (12k wing:
- *                       factorisation 11.12 -> 10.79 ms); 0: plain launches */
+ *                       factorisation 11.12 -> 10.79 ms); 0: plain launches
+ *   FP_TUNE_LU_SPLIT    1: the panel stream of the static-order LU keeps only
+ *                       what the next diagonal block needs (L21 of the next
+ *                       panel's rows and the update of its diagonal tile); the
+ *                       third stream does L21 of the rows below and the rest of
+ *                       the next panel's column beside the next k_pdiag (with
+ *                       FP_TUNE_PANEL_GEMM 2; default 1: 12k wing
+ *                       factorisation 10.85 -> 10.68 ms); 0: both on the panel
+ *                       stream */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -486,6 +494,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_TC_BF16X3 12
 #define FP_TUNE_TC_PREFETCH 13
 #define FP_TUNE_PDL 14
+#define FP_TUNE_LU_SPLIT 15
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the
