@@ -39,6 +39,7 @@ FP_TUNE_TC_BF16X3 = 12
 FP_TUNE_TC_PREFETCH = 13
 FP_TUNE_PDL = 14
 FP_TUNE_LU_SPLIT = 15
+FP_TUNE_LU_FUSE = 16
 
 
 class SolveOpts(C.Structure):

@@ -842,6 +842,11 @@ k_l21g(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, con
 // WR = 512 / CW rows x CW columns, and its K loop stops at its last row
 // (inv(L) is lower triangular). Writes U12 in place and its split (K-major:
 // column j - c0 holds its PW values), as k_u12.
+// DIAG (the split panel chain): then also the next diagonal tile's update,
+// A(kd + r, j) -= sum_s L21(kd + r, k + s) U12(k + s, j) for r < PW and the
+// CTA's columns j, in FP32 on the FMA pipe: U12 from the registers through
+// shared memory, the 128 x 128 block of L21 (written before this launch)
+// staged where inv(L) was.
 template <int CW>
 struct U12gCfg {
   static constexpr int THREADS = 8 * CW;
@@ -849,10 +854,10 @@ struct U12gCfg {
   static constexpr int ZP = CW + 4;
   static constexpr size_t smem() { return ((size_t)PW * GP + (size_t)PW * ZP) * sizeof(float); }
 };
-template <int CW, int SM>
+template <int CW, int SM, bool DIAG = false>
 __global__ void __launch_bounds__(U12gCfg<CW>::THREADS)
 k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, const float* __restrict__ slot,
-       float* __restrict__ Bh, float* __restrict__ Bl) {
+       float* __restrict__ Bh, float* __restrict__ Bl, int64_t kd) {
   griddep_wait();
   typedef U12gCfg<CW> Cfg;
   constexpr int T = Cfg::THREADS, ZP = Cfg::ZP, CQ = CW / 4;
@@ -892,6 +897,39 @@ k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, co
     *reinterpret_cast<float4*>(A + (col0 + cb + b) * lda + k + ib) = make_float4(v[0], v[1], v[2], v[3]);
     put_split<SM>(Bh, Bl, (col0 - c0 + cb + b) * (int64_t)PW + ib, v);
   }
+  if constexpr (DIAG) {
+    __syncthreads();   // every warp is done with inv(L) and the A12 block
+#pragma unroll
+    for (int u = 0; u < PW * PW / 4 / T; ++u) {   // LT[s][r] = L21(kd + r, k + s)
+      const int e = tid + u * T, sc = e / (PW / 4), q = (e % (PW / 4)) * 4;
+      cp16(&LT[sc][q], A + (k + sc) * lda + kd + q, 16);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) Z[ib + a][cb + b] = acc[a][b];
+    cp_async_wait_all();
+    __syncthreads();
+    float upd[4][4] = {};
+#pragma unroll 4
+    for (int s = 0; s < PW; ++s) {
+      const float4 l = *reinterpret_cast<const float4*>(&LT[s][ib]);
+      const float4 z = *reinterpret_cast<const float4*>(&Z[s][cb]);
+      const float lv[4] = {l.x, l.y, l.z, l.w}, zv[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) upd[a][b] = fmaf(lv[a], zv[b], upd[a][b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      if (cb + b >= cols) break;
+      float4* const g = reinterpret_cast<float4*>(A + (col0 + cb + b) * lda + kd + ib);
+      float4 v = *g;
+      v.x -= upd[0][b]; v.y -= upd[1][b]; v.z -= upd[2][b]; v.w -= upd[3][b];
+      *g = v;
+    }
+  }
 }
 
 __global__ void k_iota(int32_t* __restrict__ ipiv, int64_t n) {
@@ -912,7 +950,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   typedef U12Cfg<16, 1> CfgN;   // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
   static SmemAttr attr_d, attr_l, attr_lx, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
-  static SmemAttr attr_pi, attr_lg[2], attr_ugn[2], attr_ugr[2];
+  static SmemAttr attr_pi, attr_lg[2], attr_ugn[2], attr_ugr[2], attr_ugd[2];
   // the GEMM form of the panel kernels, for the FP32 form (the BF16 form keeps
   // block substitution: with BF16 updates its GMRES-IR needed more iterations)
   const bool pg = c->panel_gemm > 0 && !bf16;   // U12 = inv(L) A12
@@ -928,6 +966,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     FP_CUDA_TRY(c->err, attr_lg[1].ensure(k_l21g<kSplitBf16x2>, (int)l21g_smem()));
     FP_CUDA_TRY(c->err, attr_ugn[0].ensure(k_u12g<16, kSplitTf32>, (int)GCfgN::smem()));
     FP_CUDA_TRY(c->err, attr_ugn[1].ensure(k_u12g<16, kSplitBf16x2>, (int)GCfgN::smem()));
+    FP_CUDA_TRY(c->err, attr_ugd[0].ensure(k_u12g<16, kSplitTf32, true>, (int)GCfgN::smem()));
+    FP_CUDA_TRY(c->err, attr_ugd[1].ensure(k_u12g<16, kSplitBf16x2, true>, (int)GCfgN::smem()));
     FP_CUDA_TRY(c->err, attr_ugr[0].ensure(k_u12g<32, kSplitTf32>, (int)GCfgR::smem()));
     FP_CUDA_TRY(c->err, attr_ugr[1].ensure(k_u12g<32, kSplitBf16x2>, (int)GCfgR::smem()));
   }
@@ -1072,14 +1112,28 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       // the next panel's columns: after the previous panel's trailing update
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
       if (lside && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));
-      {
+      // split: U12 of the next panel's columns and the update of its diagonal
+      // tile in one launch (k_u12g<16, ., true>)
+      const bool fused = sp && c->lu_fuse;
+      if (fused) {
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
         if (x3)
-          launch_k(c->pdl, k_u12g<16, kSplitBf16x2>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3]);
+          launch_k(c->pdl, k_u12g<16, kSplitBf16x2, true>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend,
+                   knext, dinv, s[2], s[3], kend);
+        else
+          launch_k(c->pdl, k_u12g<16, kSplitTf32, true>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend,
+                   knext, dinv, s[2], xsplit ? nullptr : s[3], kend);
+        ++c->nlaunch;
+        FP_CUDA_TRY(c->err, cudaGetLastError());
+      } else {
+        TraceScope tr(c, TR_U12);
+        const unsigned g = (unsigned)((knext - kend + 15) / 16);
+        if (x3)
+          launch_k(c->pdl, k_u12g<16, kSplitBf16x2>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3], (int64_t)0);
         else if (pg)
           launch_k(c->pdl, k_u12g<16, kSplitTf32>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2],
-                                                                                     xsplit ? nullptr : s[3]);
+                                                                                     xsplit ? nullptr : s[3], (int64_t)0);
         else if (bf16)
           launch_k(c->pdl, k_u12<16, 1, true>, g, CfgN::THREADS, CfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else
@@ -1090,7 +1144,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       }
       if (sp) {
         FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_u12n, c->stream));
-        if (int rc = update(slot, kend, K0, kend, knext, 0, 0, PW)) return rc;   // the next diagonal block's rows
+        if (!fused)
+          if (int rc = update(slot, kend, K0, kend, knext, 0, 0, PW)) return rc;   // the next diagonal block's rows
         OnStream on3(c, c->stream3);
         FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_u12n, 0));
         if (int rc = update(slot, kend, K0, kend, knext, 0, PW)) return rc;      // the rows below
@@ -1115,10 +1170,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
           if (x3)
             launch_k(c->pdl, k_u12g<32, kSplitBf16x2>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh,
-                                                                                        b16(s[3]));
+                                                                                        b16(s[3]), (int64_t)0);
           else if (pg)
             launch_k(c->pdl, k_u12g<32, kSplitTf32>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, 
-                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
+                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW, (int64_t)0);
           else if (bf16)
             launch_k(c->pdl, k_u12<32, 2, true>, g, CfgR::THREADS, CfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh, nullptr);
           else

@@ -478,7 +478,11 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       the next panel's column beside the next k_pdiag (with
  *                       FP_TUNE_PANEL_GEMM 2; default 1: 12k wing
  *                       factorisation 10.85 -> 10.68 ms); 0: both on the panel
- *                       stream */
+ *                       stream
+ *   FP_TUNE_LU_FUSE     1: with the split chain, U12 of the next panel's
+ *                       columns and the update of its diagonal tile (FP32, on
+ *                       the FMA pipe) are one kernel; 0 (default): the tile is
+ *                       updated by a tensor-core launch */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -495,6 +499,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_TC_PREFETCH 13
 #define FP_TUNE_PDL 14
 #define FP_TUNE_LU_SPLIT 15
+#define FP_TUNE_LU_FUSE 16
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

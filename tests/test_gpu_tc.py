@@ -49,7 +49,8 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
                                         ("FP_TUNE_TC_RED", 0), ("FP_TUNE_TC_TILES", 2), ("FP_TUNE_TC_TILES", 4),
                                         ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0), ("FP_TUNE_TRS2", 1),
                                         ("FP_TUNE_PANEL_GEMM", 0), ("FP_TUNE_PANEL_GEMM", 1), ("FP_TUNE_PANEL_GEMM", 2),
-                                        ("FP_TUNE_TC_PREFETCH", 1), ("FP_TUNE_PDL", 1), ("FP_TUNE_LU_SPLIT", 1)])
+                                        ("FP_TUNE_TC_PREFETCH", 1), ("FP_TUNE_PDL", 1), ("FP_TUNE_LU_SPLIT", 0),
+                                        ("FP_TUNE_LU_FUSE", 1)])
 def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
     1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
@@ -62,8 +63,9 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     substitution, 1 as products with the full panel inverses, 2 forms L21 by
     substitution and inv(L) on a third stream, U12 as a product;
     FP_TUNE_TC_PREFETCH 1 prefetches each CTA's C tile into L2; FP_TUNE_PDL 1
-    launches the kernels with programmatic dependent launch; FP_TUNE_LU_SPLIT 1
-    leaves the rows below the next panel to the third stream. The factors are as accurate as the default's (refinement
+    launches the kernels with programmatic dependent launch; FP_TUNE_LU_SPLIT 0
+    keeps the rows below the next panel on the panel stream; FP_TUNE_LU_FUSE 1
+    updates the next diagonal tile inside the U12 kernel. The factors are as accurate as the default's (refinement
     in a handful of steps, the oracle's solution to 1e-10), for one partial
     panel up to many panels with a partial last one (1,500 panels: a last K
     block of 92)."""
@@ -93,8 +95,9 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
 
 
 @pytest.mark.parametrize("nc,ns", [(12, 8), (20, 24), (60, 80), (50, 30)])
-@pytest.mark.parametrize("panel,prefetch,pdl,split", [(1, 0, 0, 0), (2, 0, 0, 0), (2, 1, 0, 0), (2, 1, 1, 0), (2, 1, 1, 1)])
-def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, pdl, split):
+@pytest.mark.parametrize("panel,prefetch,pdl,split,fuse", [(1, 0, 0, 0, 0), (2, 0, 0, 0, 0), (2, 1, 0, 0, 0),
+                                                           (2, 1, 1, 0, 0), (2, 1, 1, 1, 0), (2, 1, 1, 1, 1)])
+def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, pdl, split, fuse):
     """FP_TUNE_TC_BF16X3 1: the mixed form's trailing update multiplies BF16
     pairs (hi + lo, three MMAs) instead of TF32 pairs; the factors carry 16-bit
     operand splits, and the FP64 refinement (GMRES-IR behind it) still reaches
@@ -115,6 +118,7 @@ def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, 
         c.set_tuning(fp._capi.FP_TUNE_TC_PREFETCH, prefetch)
         c.set_tuning(fp._capi.FP_TUNE_PDL, pdl)
         c.set_tuning(fp._capi.FP_TUNE_LU_SPLIT, split)
+        c.set_tuning(fp._capi.FP_TUNE_LU_FUSE, fuse)
         c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
         c.set_wake(w.shedding, D, D)
         x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
