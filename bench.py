@@ -710,7 +710,19 @@ def wingbody_measure(fp, device, steps=3, warmup=1, cpu=True, nprobes=1_000_000)
     ns64 = min(20000, M)
     U64 = ctx.uind(VR, gamma, probes[:ns64], np.tile(V, (ns64, 1)), cap.FP_PREC_FP64)
     f64_ms_per_probe = ctx.last_kernel_ms(cap.FP_STAGE_UIND)[0] / ns64
-    # the FP64 form on the same body, for the errors of the mixed form
+    # the BF16 form (BF16-rounded AIC, BF16 tensor-core update, GMRES-IR with
+    # FP64 residuals to 1e-10) on the same body, beside the mixed form
+    opts16 = cap.make_opts("ludiv", "bf16", ir_tol=1e-10)
+    stg16 = np.zeros(3)
+    for i in range(1 + steps):
+        ctx.assemble(VR, 1e-8, 1e-14, cap.FP_PREC_BF16)
+        ctx.factor(cap.FP_PREC_BF16)
+        st16 = ctx.solve_device(1, opts16)
+        if i > 0:
+            stg16 += [st16.ms_assemble, st16.ms_factor, st16.ms_solve]
+    stg16 /= steps
+    gamma16, st16 = ctx.solve(1, opts16)
+    # the FP64 form on the same body, for the errors of both reduced forms
     x64, st64 = ctx.solve_body(VR, U, opts=cap.make_opts("ludiv", "fp64"))
     fms = float(np.mean(field_ms))
     nquad = int(np.sum(np.diff(m.panel_offsets) == 4))
@@ -736,6 +748,13 @@ def wingbody_measure(fp, device, steps=3, warmup=1, cpu=True, nprobes=1_000_000)
            "refinement": {"ir_iters": st.ir_iters, "used_gmres": st.used_gmres, "gmres_iters": st.gmres_iters,
                           "rel_residual": st.rel_residual},
            "fp64_form_ms": {"assemble": st64.ms_assemble, "factor": st64.ms_factor, "solve": st64.ms_solve},
+           "bf16_form": {"form": "BF16-rounded AIC, BF16 tensor-core update (kind::f16) with FP32 accumulation, "
+                                 "static row order, GMRES-IR with FP64 residuals on the FP64 AIC to 1e-10",
+                         "solve_ms": {"assemble": stg16[0], "factor": stg16[1], "solve": stg16[2],
+                                      "total": float(stg16.sum())},
+                         "refinement": {"ir_iters": st16.ir_iters, "used_gmres": st16.used_gmres,
+                                        "gmres_iters": st16.gmres_iters, "rel_residual": st16.rel_residual},
+                         "strength_rel_vs_fp64": float(np.linalg.norm(gamma16 - x64) / np.linalg.norm(x64))},
            "errors_vs_fp64": {"strength_rel": float(np.linalg.norm(gamma - x64) / np.linalg.norm(x64)),
                               "Cp_max_abs": float(np.abs(Cpb - Cpd).max()), "CL": CLb, "CL_fp64": CLd,
                               "abs_dCL": abs(CLb - CLd), "CD": CDb, "CD_fp64": CDd, "abs_dCD": abs(CDb - CDd)},
