@@ -40,6 +40,7 @@ FP_TUNE_TC_PREFETCH = 13
 FP_TUNE_PDL = 14
 FP_TUNE_LU_SPLIT = 15
 FP_TUNE_LU_FUSE = 16
+FP_TUNE_U12_WIDE = 17
 
 
 class SolveOpts(C.Structure):

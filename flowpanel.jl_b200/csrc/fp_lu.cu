@@ -2291,34 +2291,8 @@ __global__ void k_colnorm2(const double* __restrict__ a, int64_t n, int64_t lda,
     out[q] = t;
   }
 }
-// Squared norms of k columns: chunks of the column reduced by many CTAs
-// (one CTA a column took 10.7 us at n = 12k), summed with atomicAdd.
-__global__ void k_colnorm2_part(const double* __restrict__ a, int64_t n, int64_t lda, double* __restrict__ out) {
-  const double* col = a + (int64_t)blockIdx.y * lda;
-  double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double v = col[i];
-    s = fma(v, v, s);
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  __shared__ double red[8];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < 8; ++w) t += red[w];
-    atomicAdd(&out[blockIdx.y], t);
-  }
-}
 int colnorm2(fp_ctx* c, const double* a, int64_t n, int64_t lda, int64_t k, double* d_out) {
-  if (n <= 4096) {
-    k_colnorm2<<<(unsigned)k, 256, 0, c->stream>>>(a, n, lda, d_out);
-  } else {
-    FP_CUDA_TRY(c->err, cudaMemsetAsync(d_out, 0, (size_t)k * sizeof(double), c->stream));
-    const unsigned chunks = (unsigned)std::min<int64_t>(64, (n + 2047) / 2048);
-    k_colnorm2_part<<<dim3(chunks, (unsigned)k), 256, 0, c->stream>>>(a, n, lda, d_out);
-  }
+  k_colnorm2<<<(unsigned)k, 256, 0, c->stream>>>(a, n, lda, d_out);
   ++c->nlaunch;
   FP_CUDA_TRY(c->err, cudaGetLastError());
   return FP_OK;

@@ -950,7 +950,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   typedef U12Cfg<16, 1> CfgN;   // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
   static SmemAttr attr_d, attr_l, attr_lx, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
-  static SmemAttr attr_pi, attr_lg[2], attr_ugn[2], attr_ugr[2], attr_ugd[2];
+  static SmemAttr attr_pi, attr_lg[2], attr_ugn[2], attr_ugr[2], attr_ugd[2], attr_ugw[2];
   // the GEMM form of the panel kernels, for the FP32 form (the BF16 form keeps
   // block substitution: with BF16 updates its GMRES-IR needed more iterations)
   const bool pg = c->panel_gemm > 0 && !bf16;   // U12 = inv(L) A12
@@ -960,6 +960,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   const bool lg = pg && !lside;
   typedef U12gCfg<16> GCfgN;
   typedef U12gCfg<32> GCfgR;
+  typedef U12gCfg<64> GCfgW;   // FP_TUNE_U12_WIDE: 64 columns a CTA for the columns beyond
   if (pg) {
     FP_CUDA_TRY(c->err, attr_pi.ensure(k_pinv, (int)pinv_smem()));
     FP_CUDA_TRY(c->err, attr_lg[0].ensure(k_l21g<kSplitTf32>, (int)l21g_smem()));
@@ -970,6 +971,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     FP_CUDA_TRY(c->err, attr_ugd[1].ensure(k_u12g<16, kSplitBf16x2, true>, (int)GCfgN::smem()));
     FP_CUDA_TRY(c->err, attr_ugr[0].ensure(k_u12g<32, kSplitTf32>, (int)GCfgR::smem()));
     FP_CUDA_TRY(c->err, attr_ugr[1].ensure(k_u12g<32, kSplitBf16x2>, (int)GCfgR::smem()));
+    FP_CUDA_TRY(c->err, attr_ugw[0].ensure(k_u12g<64, kSplitTf32>, (int)GCfgW::smem()));
+    FP_CUDA_TRY(c->err, attr_ugw[1].ensure(k_u12g<64, kSplitBf16x2>, (int)GCfgW::smem()));
   }
   // the FP32 form's update from BF16 pairs (needs the GEMM-form panel kernels)
   const bool x3 = !bf16 && pg && c->tc_x3 && c->use_tc;
@@ -1168,7 +1171,11 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
             return reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(p) + (knext - kend) * PW);
           };
           float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
-          if (x3)
+          const unsigned gw = (unsigned)((n - knext + 63) / 64);
+          if (x3 && c->u12_wide)
+            launch_k(c->pdl, k_u12g<64, kSplitBf16x2>, gw, GCfgW::THREADS, GCfgW::smem(), c->stream, A, lda, K0, knext, n,
+                     dinv, bh, b16(s[3]), (int64_t)0);
+          else if (x3)
             launch_k(c->pdl, k_u12g<32, kSplitBf16x2>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh,
                                                                                         b16(s[3]), (int64_t)0);
           else if (pg)

@@ -482,7 +482,10 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *   FP_TUNE_LU_FUSE     1: with the split chain, U12 of the next panel's
  *                       columns and the update of its diagonal tile (FP32, on
  *                       the FMA pipe) are one kernel; 0 (default): the tile is
- *                       updated by a tensor-core launch */
+ *                       updated by a tensor-core launch
+ *   FP_TUNE_U12_WIDE    1: U12 of the columns beyond the next panel (BF16-pair
+ *                       update) with 64 columns a CTA of 512 threads; 0
+ *                       (default): 32 columns a CTA of 256 threads */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -500,6 +503,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_PDL 14
 #define FP_TUNE_LU_SPLIT 15
 #define FP_TUNE_LU_FUSE 16
+#define FP_TUNE_U12_WIDE 17
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the
