@@ -697,6 +697,120 @@ __device__ __forceinline__ void copy_square_async(float (*dst)[GP], const float*
   }
 }
 
+// K6 with asynchronous staging (FP_TUNE_L21_ASYNC): the same substitution as
+// k_l21, but the row block and U are kept column-major in shared memory, as
+// they lie in global memory, so that every staging copy is a cp.async (all
+// of a CTA's loads in flight at once, no registers): XT[c][r] = A21(r, c),
+// UbT[c][s] = U(s, IB + c). Thread tile: rows 2 rg, 2 rg + 1 x 4 columns.
+constexpr int XTP = L21_ROWS + 4;   // pitch of XT (32 rows)
+constexpr int UTP = PW - IB + 4;    // pitch of UbT (96 rows)
+constexpr size_t l21a_smem() {
+  return ((size_t)PW * XTP + (size_t)(PW - IB) * UTP + (size_t)NIB * IB * UP) * sizeof(float);
+}
+template <int SM>
+__global__ void __launch_bounds__(L21_THREADS)
+k_l21a(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, int64_t r0, int64_t rbeg,
+       const float* __restrict__ dinv, float* __restrict__ Ah, float* __restrict__ Al, float* __restrict__ cert) {
+  griddep_wait();
+  extern __shared__ __align__(16) unsigned char smem[];
+  float (*XT)[XTP] = reinterpret_cast<float (*)[XTP]>(smem);
+  float (*UbT)[UTP] = reinterpret_cast<float (*)[UTP]>(smem + (size_t)PW * XTP * sizeof(float));
+  float (*Ut)[UP] = reinterpret_cast<float (*)[UP]>(reinterpret_cast<unsigned char*>(UbT) +
+                                                     (size_t)(PW - IB) * UTP * sizeof(float));
+  const int tid = threadIdx.x;
+  const int64_t row0 = rbeg + (int64_t)blockIdx.x * L21_ROWS;
+  const int rows = (int)imin64(L21_ROWS, n - row0);
+#pragma unroll
+  for (int u = 0; u < PW * (L21_ROWS / 4) / L21_THREADS; ++u) {   // XT: 128 columns x 8 chunks of 4 rows
+    const int e = tid + u * L21_THREADS, c = e / (L21_ROWS / 4), q = (e % (L21_ROWS / 4)) * 4;
+    const int bytes = 4 * max(0, min(4, rows - q));
+    const float* col = A + (k + c) * lda;
+    cp16(&XT[c][q], bytes ? col + row0 + q : col, bytes);
+  }
+#pragma unroll
+  for (int u = 0; u < (PW - IB) * ((PW - IB) / 4) / L21_THREADS; ++u) {   // UbT: 96 columns x 24 chunks
+    const int e = tid + u * L21_THREADS, c = e / ((PW - IB) / 4), q = (e % ((PW - IB) / 4)) * 4;
+    cp16(&UbT[c][q], A + (k + IB + c) * lda + k + q, 16);
+  }
+  copy_inv_async<L21_THREADS>(Ut, dinv, 1, tid);
+  cp_async_wait_all();
+  __syncthreads();
+  const int rg = tid & 15, cg = tid >> 4;   // 16 row pairs x 8 column quads = 32 x 32
+#pragma unroll 1
+  for (int t = 0; t < NIB; ++t) {
+    const int c0 = t * IB;
+    float y[2][4] = {};
+#pragma unroll 2
+    for (int s = 0; s < c0; s += 4) {   // sum_s L_s U(s, t): XT's columns < c0 hold L
+      float4 uq[4];   // U(s .. s+3, c0 + 4 cg + j)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) uq[j] = *reinterpret_cast<const float4*>(&UbT[c0 - IB + 4 * cg + j][s]);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const float2 x = *reinterpret_cast<const float2*>(&XT[s + d][2 * rg]);
+        const float uv[4] = {(&uq[0].x)[d], (&uq[1].x)[d], (&uq[2].x)[d], (&uq[3].x)[d]};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          y[0][j] = fmaf(x.x, uv[j], y[0][j]);
+          y[1][j] = fmaf(x.y, uv[j], y[1][j]);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {   // own entries of block t: nothing else reads them yet
+      float2* p = reinterpret_cast<float2*>(&XT[c0 + 4 * cg + j][2 * rg]);
+      float2 v = *p;
+      v.x -= y[0][j]; v.y -= y[1][j];
+      *p = v;
+    }
+    __syncthreads();
+    float l[2][4] = {};
+#pragma unroll 4
+    for (int s = 0; s < IB; ++s) {   // L_t = Y_t inv(U_tt)
+      const float4 q = *reinterpret_cast<const float4*>(&Ut[t * IB + s][4 * cg]);
+      const float2 x = *reinterpret_cast<const float2*>(&XT[c0 + s][2 * rg]);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        l[0][j] = fmaf(x.x, qv[j], l[0][j]);
+        l[1][j] = fmaf(x.y, qv[j], l[1][j]);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      *reinterpret_cast<float2*>(&XT[c0 + 4 * cg + j][2 * rg]) = make_float2(l[0][j], l[1][j]);
+    __syncthreads();
+  }
+  griddep_launch();
+  // L21 in place (column-major, as staged) and its split (K-major rows)
+#pragma unroll
+  for (int u = 0; u < PW * (L21_ROWS / 4) / L21_THREADS; ++u) {
+    const int e = tid + u * L21_THREADS, c = e / (L21_ROWS / 4), q = (e % (L21_ROWS / 4)) * 4;
+    float* const g = A + (k + c) * lda + row0 + q;
+    const float4 v = *reinterpret_cast<const float4*>(&XT[c][q]);
+    if (q + 4 <= rows) {
+      *reinterpret_cast<float4*>(g) = v;
+    } else {
+      const float vv[4] = {v.x, v.y, v.z, v.w};
+      for (int i = 0; i < 4; ++i)
+        if (q + i < rows) g[i] = vv[i];
+    }
+  }
+  float lmax = 0.f;
+  constexpr int C4 = PW / 4;
+  for (int e = tid; e < L21_ROWS * C4; e += L21_THREADS) {   // lanes over rows: conflict-free column reads
+    const int r = e % L21_ROWS, c = (e / L21_ROWS) * 4;
+    if (r >= rows) continue;
+    const float v[4] = {XT[c][r], XT[c + 1][r], XT[c + 2][r], XT[c + 3][r]};
+    put_split<SM>(Ah, Al, (row0 - r0 + r) * (int64_t)PW + c, v);
+    lmax = fmaxf(lmax, fmaxf(fmaxf(fabsf(v[0]), fabsf(v[1])), fmaxf(fabsf(v[2]), fabsf(v[3]))));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
+  if ((tid & 31) == 0) atomic_max_pos(cert, lmax);
+}
+
 // K1b: 2 NIB CTAs. CTA b < NIB forms block column j = b of inv(L), CTA
 // b >= NIB block column j = b - NIB of inv(U^T) = inv(U)^T; both are the
 // inverse of a lower-triangular M from its diagonal-block inverses D_i:
@@ -949,7 +1063,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   FP_CUDA_TRY(c->err, cudaMemsetAsync(cert, 0, sizeof(float), c->stream));
   typedef U12Cfg<16, 1> CfgN;   // the next panel's columns: many small CTAs
   typedef U12Cfg<32, 2> CfgR;   // the columns beyond
-  static SmemAttr attr_d, attr_l, attr_lx, attr_un, attr_ur, attr_lb, attr_unb, attr_urb;
+  static SmemAttr attr_d, attr_l, attr_lx, attr_un, attr_ur, attr_lb, attr_unb, attr_urb, attr_la[3];
+  FP_CUDA_TRY(c->err, attr_la[0].ensure(k_l21a<kSplitTf32>, (int)l21a_smem()));
+  FP_CUDA_TRY(c->err, attr_la[1].ensure(k_l21a<kSplitBf16x2>, (int)l21a_smem()));
+  FP_CUDA_TRY(c->err, attr_la[2].ensure(k_l21a<kSplitBf16>, (int)l21a_smem()));
   static SmemAttr attr_pi, attr_lg[2], attr_ugn[2], attr_ugr[2], attr_ugd[2], attr_ugw[2];
   // the GEMM form of the panel kernels, for the FP32 form (the BF16 form keeps
   // block substitution: with BF16 updates its GMRES-IR needed more iterations)
@@ -1071,10 +1188,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         TraceScope tr(c, TR_L21);
         const int64_t he = kend + PW;   // the next panel's rows
         if (x3)
-          launch_k(c->pdl, k_l21<kSplitBf16x2>, (unsigned)(PW / L21_ROWS), L21_THREADS, l21_smem(), c->stream, A, lda,
+          launch_k(c->pdl, c->l21_async ? k_l21a<kSplitBf16x2> : k_l21<kSplitBf16x2>, (unsigned)(PW / L21_ROWS), L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda,
                    he, K0, kend, kend, dinv, s[0], s[1], cert);
         else
-          launch_k(c->pdl, k_l21<kSplitTf32>, (unsigned)(PW / L21_ROWS), L21_THREADS, l21_smem(), c->stream, A, lda, he,
+          launch_k(c->pdl, c->l21_async ? k_l21a<kSplitTf32> : k_l21<kSplitTf32>, (unsigned)(PW / L21_ROWS), L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda, he,
                    K0, kend, kend, dinv, s[0], xsplit ? nullptr : al, cert);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1084,10 +1201,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         TraceScope tr(c, TR_L21);
         const unsigned g = (unsigned)((n - kend - PW + L21_ROWS - 1) / L21_ROWS);
         if (x3)
-          launch_k(c->pdl, k_l21<kSplitBf16x2>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend + PW,
+          launch_k(c->pdl, c->l21_async ? k_l21a<kSplitBf16x2> : k_l21<kSplitBf16x2>, g, L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda, n, K0, kend, kend + PW,
                    dinv, s[0], s[1], cert);
         else
-          launch_k(c->pdl, k_l21<kSplitTf32>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend + PW, dinv,
+          launch_k(c->pdl, c->l21_async ? k_l21a<kSplitTf32> : k_l21<kSplitTf32>, g, L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda, n, K0, kend, kend + PW, dinv,
                    s[0], xsplit ? nullptr : al, cert);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
@@ -1101,11 +1218,11 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         if (x3) launch_k(c->pdl, k_l21g<kSplitBf16x2>, g, L21G_THREADS, l21g_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], s[1], cert);
         else launch_k(c->pdl, k_l21g<kSplitTf32>, g, L21G_THREADS, l21g_smem(), c->stream, A, lda, n, K0, kend, dinv, s[0], al, cert);
       } else if (bf16) {
-        launch_k(c->pdl, k_l21<kSplitBf16>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], al, cert);
+        launch_k(c->pdl, c->l21_async ? k_l21a<kSplitBf16> : k_l21<kSplitBf16>, g, L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], al, cert);
       } else if (x3) {
-        launch_k(c->pdl, k_l21<kSplitBf16x2>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], s[1], cert);
+        launch_k(c->pdl, c->l21_async ? k_l21a<kSplitBf16x2> : k_l21<kSplitBf16x2>, g, L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], s[1], cert);
       } else {
-        launch_k(c->pdl, k_l21<kSplitTf32>, g, L21_THREADS, l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], al, cert);
+        launch_k(c->pdl, c->l21_async ? k_l21a<kSplitTf32> : k_l21<kSplitTf32>, g, L21_THREADS, c->l21_async ? l21a_smem() : l21_smem(), c->stream, A, lda, n, K0, kend, kend, dinv, s[0], al, cert);
       }
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());

@@ -484,8 +484,13 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       the FMA pipe) are one kernel; 0 (default): the tile is
  *                       updated by a tensor-core launch
  *   FP_TUNE_U12_WIDE    1: U12 of the columns beyond the next panel (BF16-pair
- *                       update) with 64 columns a CTA of 512 threads; 0
- *                       (default): 32 columns a CTA of 256 threads */
+ *                       update) with 64 columns a CTA of 512 threads (12k
+ *                       wing: 10.81 against 10.80 ms); 0 (default): 32
+ *                       columns a CTA of 256 threads
+ *   FP_TUNE_L21_ASYNC   1 (default): the static-order LU's L21 by a kernel that
+ *                       keeps the row block and U column-major in shared memory,
+ *                       staged by cp.async (12k wing: factorisation 10.81 ->
+ *                       10.52 ms); 0: row-major staging through registers */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -504,6 +509,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_LU_SPLIT 15
 #define FP_TUNE_LU_FUSE 16
 #define FP_TUNE_U12_WIDE 17
+#define FP_TUNE_L21_ASYNC 18
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the
