@@ -950,6 +950,9 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
     case FP_TUNE_L21_ASYNC:
       c->l21_async = value != 0;
       return FP_OK;
+    case FP_TUNE_U12_ASYNC:
+      c->u12_async = value != 0;
+      return FP_OK;
     case FP_TUNE_TC_NARROW:
       if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");
       c->tc_narrow_stages = value;

@@ -109,6 +109,7 @@ struct fp_ctx {
   int tc_prefetch = 1;                  // red.global updates: idle warps prefetch the C tile into L2 (FP_TUNE_TC_PREFETCH)
   bool lu_split = true;                 // static-order LU: split panel chain (FP_TUNE_LU_SPLIT)
   bool l21_async = true;                // static-order LU: k_l21 with asynchronous column-major staging (FP_TUNE_L21_ASYNC)
+  bool u12_async = false;               // static-order LU: k_u12g stages A12 column-major by cp.async (FP_TUNE_U12_ASYNC)
   bool u12_wide = false;                // static-order LU: U12 of the columns beyond, 64 columns a CTA (FP_TUNE_U12_WIDE)
   bool lu_fuse = false;                 // split chain: U12 and the diagonal tile's update in one kernel (FP_TUNE_LU_FUSE)
   bool pdl = true;                      // static-order LU: programmatic dependent launch of its kernels (FP_TUNE_PDL)

@@ -966,12 +966,16 @@ struct U12gCfg {
   static constexpr int THREADS = 8 * CW;
   static constexpr int WR = 512 / CW;
   static constexpr int ZP = CW + 4;
-  static constexpr size_t smem() { return ((size_t)PW * GP + (size_t)PW * ZP) * sizeof(float); }
+  // the A12 block row-major (Z[s][c], through registers) or column-major
+  // (ZT[c][s], by cp.async: FP_TUNE_U12_ASYNC), whichever is larger
+  static constexpr size_t smem() {
+    return ((size_t)PW * GP + std::max((size_t)PW * ZP, (size_t)CW * GP)) * sizeof(float);
+  }
 };
 template <int CW, int SM, bool DIAG = false>
 __global__ void __launch_bounds__(U12gCfg<CW>::THREADS)
 k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, const float* __restrict__ slot,
-       float* __restrict__ Bh, float* __restrict__ Bl, int64_t kd) {
+       float* __restrict__ Bh, float* __restrict__ Bl, int64_t kd, int zasync) {
   griddep_wait();
   typedef U12gCfg<CW> Cfg;
   constexpr int T = Cfg::THREADS, ZP = Cfg::ZP, CQ = CW / 4;
@@ -981,8 +985,16 @@ k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, co
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t col0 = c0 + (int64_t)blockIdx.x * CW;
   const int cols = (int)imin64(CW, c1 - col0);
+  float (*ZT)[GP] = reinterpret_cast<float (*)[GP]>(Z);   // async staging: ZT[c][s] = A12(s, c)
   copy_square_async<T>(LT, slot + kLinvtOff, tid);
-  {
+  if (zasync) {
+#pragma unroll
+    for (int u = 0; u < CW * (PW / 4) / T; ++u) {   // column c of the block: PW contiguous floats
+      const int e = tid + u * T, c = e / (PW / 4), q = (e % (PW / 4)) * 4;
+      const float* col = A + (col0 + c) * lda + k;
+      cp16(&ZT[c][q], c < cols ? col + q : A + col0 * lda + k, c < cols ? 16 : 0);
+    }
+  } else {
     Staged<T, PW, CW> zs;
     zs.fetch(A + col0 * lda + k, lda, PW, cols, [](int, int) { return 0.f; }, tid);
     zs.put([&](int r, int c, float v) { Z[r][c] = v; }, tid);
@@ -993,15 +1005,34 @@ k_u12g(float* __restrict__ A, int64_t lda, int64_t k, int64_t c0, int64_t c1, co
   const int ib = Cfg::WR * warp + 4 * rq, cb = 4 * cq;
   float acc[4][4] = {};
   const int send = Cfg::WR * (warp + 1);
+  if (zasync) {
+#pragma unroll 2
+    for (int s = 0; s < send; s += 4) {   // 4 K values a step: inv(L) rows and A12 columns as float4
+      float4 zq[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) zq[b] = *reinterpret_cast<const float4*>(&ZT[cb + b][s]);
+#pragma unroll
+      for (int d = 0; d < 4; ++d) {
+        const float4 l = *reinterpret_cast<const float4*>(&LT[s + d][ib]);
+        const float lv[4] = {l.x, l.y, l.z, l.w};
+        const float zv[4] = {(&zq[0].x)[d], (&zq[1].x)[d], (&zq[2].x)[d], (&zq[3].x)[d]};
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(lv[a], zv[b], acc[a][b]);
+      }
+    }
+  } else {
 #pragma unroll 4
-  for (int s = 0; s < send; ++s) {
-    const float4 l = *reinterpret_cast<const float4*>(&LT[s][ib]);
-    const float4 z = *reinterpret_cast<const float4*>(&Z[s][cb]);
-    const float lv[4] = {l.x, l.y, l.z, l.w}, zv[4] = {z.x, z.y, z.z, z.w};
+    for (int s = 0; s < send; ++s) {
+      const float4 l = *reinterpret_cast<const float4*>(&LT[s][ib]);
+      const float4 z = *reinterpret_cast<const float4*>(&Z[s][cb]);
+      const float lv[4] = {l.x, l.y, l.z, l.w}, zv[4] = {z.x, z.y, z.z, z.w};
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(lv[a], zv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(lv[a], zv[b], acc[a][b]);
+    }
   }
   griddep_launch();
 #pragma unroll
@@ -1240,20 +1271,20 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
         if (x3)
           launch_k(c->pdl, k_u12g<16, kSplitBf16x2, true>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend,
-                   knext, dinv, s[2], s[3], kend);
+                   knext, dinv, s[2], s[3], kend, (int)c->u12_async);
         else
           launch_k(c->pdl, k_u12g<16, kSplitTf32, true>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend,
-                   knext, dinv, s[2], xsplit ? nullptr : s[3], kend);
+                   knext, dinv, s[2], xsplit ? nullptr : s[3], kend, (int)c->u12_async);
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       } else {
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
         if (x3)
-          launch_k(c->pdl, k_u12g<16, kSplitBf16x2>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3], (int64_t)0);
+          launch_k(c->pdl, k_u12g<16, kSplitBf16x2>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3], (int64_t)0, (int)c->u12_async);
         else if (pg)
           launch_k(c->pdl, k_u12g<16, kSplitTf32>, g, GCfgN::THREADS, GCfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2],
-                                                                                     xsplit ? nullptr : s[3], (int64_t)0);
+                                                                                     xsplit ? nullptr : s[3], (int64_t)0, (int)c->u12_async);
         else if (bf16)
           launch_k(c->pdl, k_u12<16, 1, true>, g, CfgN::THREADS, CfgN::smem(), c->stream, A, lda, K0, kend, knext, dinv, s[2], s[3]);
         else
@@ -1291,13 +1322,13 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
           const unsigned gw = (unsigned)((n - knext + 63) / 64);
           if (x3 && c->u12_wide)
             launch_k(c->pdl, k_u12g<64, kSplitBf16x2>, gw, GCfgW::THREADS, GCfgW::smem(), c->stream, A, lda, K0, knext, n,
-                     dinv, bh, b16(s[3]), (int64_t)0);
+                     dinv, bh, b16(s[3]), (int64_t)0, (int)c->u12_async);
           else if (x3)
             launch_k(c->pdl, k_u12g<32, kSplitBf16x2>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh,
-                                                                                        b16(s[3]), (int64_t)0);
+                                                                                        b16(s[3]), (int64_t)0, (int)c->u12_async);
           else if (pg)
             launch_k(c->pdl, k_u12g<32, kSplitTf32>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, 
-                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW, (int64_t)0);
+                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW, (int64_t)0, (int)c->u12_async);
           else if (bf16)
             launch_k(c->pdl, k_u12<32, 2, true>, g, CfgR::THREADS, CfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh, nullptr);
           else

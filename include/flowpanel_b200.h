@@ -490,7 +490,10 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *   FP_TUNE_L21_ASYNC   1 (default): the static-order LU's L21 by a kernel that
  *                       keeps the row block and U column-major in shared memory,
  *                       staged by cp.async (12k wing: factorisation 10.81 ->
- *                       10.52 ms); 0: row-major staging through registers */
+ *                       10.52 ms); 0: row-major staging through registers
+ *   FP_TUNE_U12_ASYNC   1: the GEMM-form U12 kernel stages its A12 block
+ *                       column-major by cp.async (K loop over 4 values a step);
+ *                       0 (default): row-major through registers */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -510,6 +513,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_LU_FUSE 16
 #define FP_TUNE_U12_WIDE 17
 #define FP_TUNE_L21_ASYNC 18
+#define FP_TUNE_U12_ASYNC 19
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

@@ -95,10 +95,12 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
 
 
 @pytest.mark.parametrize("nc,ns", [(12, 8), (20, 24), (60, 80), (50, 30)])
-@pytest.mark.parametrize("panel,prefetch,pdl,split,fuse,wide,l21a",
-                         [(1, 0, 0, 0, 0, 0, 0), (2, 0, 0, 0, 0, 0, 0), (2, 1, 0, 0, 0, 0, 0), (2, 1, 1, 0, 0, 0, 0),
-                          (2, 1, 1, 1, 0, 0, 0), (2, 1, 1, 1, 1, 0, 0), (2, 1, 1, 1, 0, 1, 0), (2, 1, 1, 1, 0, 0, 1)])
-def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, pdl, split, fuse, wide, l21a):
+@pytest.mark.parametrize("panel,prefetch,pdl,split,fuse,wide,l21a,u12a",
+                         [(1, 0, 0, 0, 0, 0, 0, 0), (2, 0, 0, 0, 0, 0, 0, 0), (2, 1, 0, 0, 0, 0, 0, 0),
+                          (2, 1, 1, 0, 0, 0, 0, 0), (2, 1, 1, 1, 0, 0, 0, 0), (2, 1, 1, 1, 1, 0, 0, 0),
+                          (2, 1, 1, 1, 0, 1, 0, 0), (2, 1, 1, 1, 0, 0, 1, 0), (2, 1, 1, 1, 0, 0, 1, 1),
+                          (2, 1, 1, 1, 1, 1, 1, 1)])
+def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, pdl, split, fuse, wide, l21a, u12a):
     """FP_TUNE_TC_BF16X3 1: the mixed form's trailing update multiplies BF16
     pairs (hi + lo, three MMAs) instead of TF32 pairs; the factors carry 16-bit
     operand splits, and the FP64 refinement (GMRES-IR behind it) still reaches
@@ -122,6 +124,7 @@ def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, 
         c.set_tuning(fp._capi.FP_TUNE_LU_FUSE, fuse)
         c.set_tuning(fp._capi.FP_TUNE_U12_WIDE, wide)
         c.set_tuning(fp._capi.FP_TUNE_L21_ASYNC, l21a)
+        c.set_tuning(fp._capi.FP_TUNE_U12_ASYNC, u12a)
         c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
         c.set_wake(w.shedding, D, D)
         x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
