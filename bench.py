@@ -197,9 +197,9 @@ def factor_timeline(ctx, cap, prec):
     ctx.trace(False)
     tags, streams, t0, t1 = ctx.trace_read()
     out = {"span_ms": float(t1.max() - t0.min()) if len(t0) else 0.0, "kernels": []}
-    for s in (0, 1, 2):
+    for s in (0, 1, 2, 3):
         sel = streams == s
-        if s == 2 and not sel.any():
+        if s >= 2 and not sel.any():
             continue
         out[f"stream{s}_busy_ms"] = float(np.sum(t1[sel] - t0[sel]))
         for tg in sorted(set(tags[sel].tolist())):

@@ -43,6 +43,7 @@ FP_TUNE_LU_FUSE = 16
 FP_TUNE_U12_WIDE = 17
 FP_TUNE_L21_ASYNC = 18
 FP_TUNE_U12_ASYNC = 19
+FP_TUNE_REST_SPLIT = 20
 
 
 class SolveOpts(C.Structure):

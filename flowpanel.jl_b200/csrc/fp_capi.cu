@@ -158,6 +158,9 @@ int fp_ctx_create(int device, fp_ctx** out) {
       cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->stream3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->stream4, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_top, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_u12r, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_pinv, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_u12n, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_tcr, cudaEventDisableTiming) != cudaSuccess ||
@@ -185,6 +188,7 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
   if (c->stream3) cudaStreamSynchronize(c->stream3);
+  if (c->stream4) cudaStreamSynchronize(c->stream4);
   if (c->stream_bg) cudaStreamSynchronize(c->stream_bg);
   free_matrices(c);
   post_free(c);
@@ -203,6 +207,9 @@ int fp_ctx_destroy(fp_ctx* c) {
   if (c->ev_u12n) cudaEventDestroy(c->ev_u12n);
   if (c->ev_tcr) cudaEventDestroy(c->ev_tcr);
   if (c->ev_l21t) cudaEventDestroy(c->ev_l21t);
+  if (c->ev_top) cudaEventDestroy(c->ev_top);
+  if (c->ev_u12r) cudaEventDestroy(c->ev_u12r);
+  if (c->stream4) cudaStreamDestroy(c->stream4);
   if (c->stream3) cudaStreamDestroy(c->stream3);
   if (c->stream_bg) cudaStreamDestroy(c->stream_bg);
   if (c->stream2) cudaStreamDestroy(c->stream2);
@@ -952,6 +959,9 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       return FP_OK;
     case FP_TUNE_U12_ASYNC:
       c->u12_async = value != 0;
+      return FP_OK;
+    case FP_TUNE_REST_SPLIT:
+      c->rest_split = value != 0;
       return FP_OK;
     case FP_TUNE_TC_NARROW:
       if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");

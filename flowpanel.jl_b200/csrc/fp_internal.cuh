@@ -112,6 +112,7 @@ struct fp_ctx {
   bool u12_async = false;               // static-order LU: k_u12g stages A12 column-major by cp.async (FP_TUNE_U12_ASYNC)
   bool u12_wide = false;                // static-order LU: U12 of the columns beyond, 64 columns a CTA (FP_TUNE_U12_WIDE)
   bool lu_fuse = false;                 // split chain: U12 and the diagonal tile's update in one kernel (FP_TUNE_LU_FUSE)
+  bool rest_split = false;              // split chain: the trailing update in two row ranges, U12 of the columns beyond on stream4 (FP_TUNE_REST_SPLIT)
   bool pdl = true;                      // static-order LU: programmatic dependent launch of its kernels (FP_TUNE_PDL)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
@@ -175,6 +176,7 @@ struct fp_ctx {
   int tc_slot = 0;                      // scratch set of the current launches
   cudaStream_t stream2 = nullptr;       // second stream of the look-ahead factorisation
   cudaStream_t stream3 = nullptr;       // third stream (high priority): the static-order LU's inv(L) beside k_l21
+  cudaStream_t stream4 = nullptr;       // fourth stream (high priority): U12 of the columns beyond, beside the trailing update
   cudaStream_t stream_bg = nullptr;     // lowest priority: the FP64 AIC pass under the FP32 factorisation
   cudaEvent_t ev_g64 = nullptr;         // that pass done (stream_bg -> stream)
   cudaEvent_t ev_asm = nullptr;         // assembly inputs ready (stream -> stream_bg)
@@ -188,6 +190,8 @@ struct fp_ctx {
   cudaEvent_t ev_u12n = nullptr;        // split panel chain: the next panel's U12 formed (stream -> stream3)
   cudaEvent_t ev_tcr = nullptr;         // split panel chain: the rows below the next panel updated (stream3 -> stream)
   cudaEvent_t ev_l21t = nullptr;        // split panel chain: L21 of the rows below the next panel (stream3 -> stream2)
+  cudaEvent_t ev_top = nullptr;         // trailing update of the next panel's rows done (stream2 -> stream, stream4)
+  cudaEvent_t ev_u12r = nullptr;        // U12 of the columns beyond formed (stream4 -> stream2)
 
   // surface post-processing (fp_post.cu). The mesh topology of a triangular
   // body is built on first use after fp_set_geometry, the Kutta-average
@@ -437,7 +441,7 @@ struct TraceScope {
     if (s < 0) return;
     const int e = tr_event(c);
     if (e < 0) return;
-    c->trace.recs.push_back(TraceRec{tag, c->stream == c->stream2 ? 1 : (c->stream == c->stream3 ? 2 : 0), s});
+    c->trace.recs.push_back(TraceRec{tag, c->stream == c->stream2 ? 1 : (c->stream == c->stream3 ? 2 : (c->stream == c->stream4 ? 3 : 0)), s});
   }
 };
 inline void tr_collect(fp_ctx* c) {

@@ -1143,6 +1143,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   auto at = [&](int64_t r, int64_t col) { return A + col * lda + r; };
   c->trace.base = tr_event(c);
   FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
+  if (c->rest_split) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
   FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream2, c->ev_rest, 0));
   // C -= L21 U12 on the rows [kend, n) and columns [cb, ce): tensor cores from
   // the split operands, or the SIMT kernel on the factors in place
@@ -1211,6 +1212,12 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     // (L21 and the next-panel update of the next panel's 128 rows); the
     // third stream does the rows below, beside the next k_pdiag
     const bool sp = c->lu_split && lside && c->lu_overlap && kend + PW < n;
+    // rest split: the trailing update of the columns beyond runs as the next
+    // panel's rows (T), then the rows below (B); the next panel's U12 kernels
+    // read only T's rows, so they wait for T (ev_top) and U12 of the columns
+    // beyond runs on the fourth stream beside B; what reads B's rows waits
+    // for ev_rest
+    const bool rs = sp && c->rest_split;
     // the rows below this panel's diagonal block were last updated on the third stream
     if (prev_split && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_tcr, 0));
     if (sp) {
@@ -1260,12 +1267,14 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     }
     FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_panel, c->stream));
     if (knext > kend) {
-      // the next panel's columns: after the previous panel's trailing update
-      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
-      if (lside && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));
       // split: U12 of the next panel's columns and the update of its diagonal
       // tile in one launch (k_u12g<16, ., true>)
       const bool fused = sp && c->lu_fuse;
+      // the next panel's columns: after the previous panel's trailing update
+      // (rest split: its rows of this panel, unless the launch also updates
+      // the diagonal tile below them)
+      FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->rest_split && !fused ? c->ev_top : c->ev_rest, 0));
+      if (lside && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));
       if (fused) {
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
@@ -1295,14 +1304,18 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       }
       if (sp) {
         FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_u12n, c->stream));
-        if (!fused)
+        if (!fused) {
+          if (c->rest_split) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
           if (int rc = update(slot, kend, K0, kend, knext, 0, 0, PW)) return rc;   // the next diagonal block's rows
+        }
         OnStream on3(c, c->stream3);
         FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_u12n, 0));
+        if (c->rest_split) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
         if (int rc = update(slot, kend, K0, kend, knext, 0, PW)) return rc;      // the rows below
         FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_tcr, c->stream));
-      } else if (int rc = update(slot, kend, K0, kend, knext, 0)) {
-        return rc;
+      } else {
+        if (c->rest_split) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
+        if (int rc = update(slot, kend, K0, kend, knext, 0)) return rc;
       }
     }
     prev_split = sp;
@@ -1310,35 +1323,48 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     // after the panel's own work on the same stream
     auto rest = [&]() -> int {
       if (n > knext) {
-        if (lside) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));   // inv(L)
-        {
-          TraceScope tr(c, TR_STRIP);
-          const unsigned g = (unsigned)((n - knext + 31) / 32);
-          // the B operand of the columns beyond starts (knext - kend) columns in (bf16 or float elements)
-          const auto b16 = [&](float* p) {
-            return reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(p) + (knext - kend) * PW);
-          };
-          float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
-          const unsigned gw = (unsigned)((n - knext + 63) / 64);
-          if (x3 && c->u12_wide)
-            launch_k(c->pdl, k_u12g<64, kSplitBf16x2>, gw, GCfgW::THREADS, GCfgW::smem(), c->stream, A, lda, K0, knext, n,
-                     dinv, bh, b16(s[3]), (int64_t)0, (int)c->u12_async);
-          else if (x3)
-            launch_k(c->pdl, k_u12g<32, kSplitBf16x2>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh,
-                                                                                        b16(s[3]), (int64_t)0, (int)c->u12_async);
-          else if (pg)
-            launch_k(c->pdl, k_u12g<32, kSplitTf32>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, 
-                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW, (int64_t)0, (int)c->u12_async);
-          else if (bf16)
-            launch_k(c->pdl, k_u12<32, 2, true>, g, CfgR::THREADS, CfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh, nullptr);
-          else
-            launch_k(c->pdl, k_u12<32, 2, false>, g, CfgR::THREADS, CfgR::smem(), c->stream, 
-                A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
-          ++c->nlaunch;
-          FP_CUDA_TRY(c->err, cudaGetLastError());
+        {   // rest split: U12 of the columns beyond on the fourth stream, after T of the previous panel
+          OnStream on4(c, rs ? c->stream4 : c->stream);
+          if (rs) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_top, 0));
+          if (lside) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));   // inv(L)
+          {
+            TraceScope tr(c, TR_STRIP);
+            const unsigned g = (unsigned)((n - knext + 31) / 32);
+            // the B operand of the columns beyond starts (knext - kend) columns in (bf16 or float elements)
+            const auto b16 = [&](float* p) {
+              return reinterpret_cast<float*>(reinterpret_cast<__nv_bfloat16*>(p) + (knext - kend) * PW);
+            };
+            float* bh = (bf16 || x3) ? b16(s[2]) : s[2] + (knext - kend) * PW;
+            const unsigned gw = (unsigned)((n - knext + 63) / 64);
+            if (x3 && c->u12_wide)
+              launch_k(c->pdl, k_u12g<64, kSplitBf16x2>, gw, GCfgW::THREADS, GCfgW::smem(), c->stream, A, lda, K0, knext, n,
+                       dinv, bh, b16(s[3]), (int64_t)0, (int)c->u12_async);
+            else if (x3)
+              launch_k(c->pdl, k_u12g<32, kSplitBf16x2>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh,
+                                                                                          b16(s[3]), (int64_t)0, (int)c->u12_async);
+            else if (pg)
+              launch_k(c->pdl, k_u12g<32, kSplitTf32>, g, GCfgR::THREADS, GCfgR::smem(), c->stream, 
+                  A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW, (int64_t)0, (int)c->u12_async);
+            else if (bf16)
+              launch_k(c->pdl, k_u12<32, 2, true>, g, CfgR::THREADS, CfgR::smem(), c->stream, A, lda, K0, knext, n, dinv, bh, nullptr);
+            else
+              launch_k(c->pdl, k_u12<32, 2, false>, g, CfgR::THREADS, CfgR::smem(), c->stream, 
+                  A, lda, K0, knext, n, dinv, bh, xsplit ? nullptr : s[3] + (knext - kend) * PW);
+            ++c->nlaunch;
+            FP_CUDA_TRY(c->err, cudaGetLastError());
+          }
+          if (rs) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_u12r, c->stream));
         }
+        if (rs) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_u12r, 0));
         // the update reads L21 (the panel stream's k_l21, and the third stream's when split)
         if (c->lu_overlap) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
+        if (rs) {
+          if (int rc = update(slot, kend, K0, knext, n, knext - kend, 0, PW)) return rc;   // T: the next panel's rows
+          FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
+          FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_l21t, 0));
+          if (int rc = update(slot, kend, K0, knext, n, knext - kend, PW)) return rc;      // B: the rows below
+          return FP_OK;
+        }
         if (sp) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_l21t, 0));
         if (int rc = update(slot, kend, K0, knext, n, knext - kend)) return rc;
       }
@@ -1348,9 +1374,11 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       OnStream2 on2(c);
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_diag, 0));
       if (int rc = rest()) return rc;
+      if (c->rest_split && !rs) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
       FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
     } else {
       if (int rc = rest()) return rc;
+      if (c->rest_split) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
       FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_rest, c->stream));
     }
   }

@@ -356,12 +356,13 @@ int fp_kernel_timing_read(fp_ctx* ctx, int64_t* launches, double* ms, double* fl
 
 /* Timeline of the next factorisations (no counterpart in the reference): with
  * enable != 0, every fp_factor records CUDA events around each of its kernel
- * launches on both of its streams; fp_trace_read returns, for the last
+ * launches on all of its streams; fp_trace_read returns, for the last
  * factorisation, each launch's kernel tag (0 diagonal block, 1 block update,
  * 2 panel fix-up, 3 column strip, 4 tensor-core update, 5/6 operand splits,
  * 7 SIMT update, 8 full inverses of the diagonal block's factors),
  * its stream (0 the panel stream, 1 the trailing-update stream, 2 the third
- * stream of FP_TUNE_PANEL_GEMM 2) and its start
+ * stream of FP_TUNE_PANEL_GEMM 2, 3 the fourth stream of
+ * FP_TUNE_REST_SPLIT) and its start
  * and end in ms from the start of the factorisation; count = launches. */
 int fp_trace(fp_ctx* ctx, int enable);
 int fp_trace_read(fp_ctx* ctx, int64_t cap, int* tags, int* streams, float* t0, float* t1, int64_t* count);
@@ -493,7 +494,13 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       10.52 ms); 0: row-major staging through registers
  *   FP_TUNE_U12_ASYNC   1: the GEMM-form U12 kernel stages its A12 block
  *                       column-major by cp.async (K loop over 4 values a step);
- *                       0 (default): row-major through registers */
+ *                       0 (default): row-major through registers
+ *   FP_TUNE_REST_SPLIT  split panel chain: 1: the trailing update of the
+ *                       columns beyond the next panel runs as two launches,
+ *                       the next panel's 128 rows first, then the rows below;
+ *                       the next panel's U12 kernels wait for the first only,
+ *                       and U12 of the columns beyond runs on a fourth stream
+ *                       beside the second; 0 (default): one launch */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -514,6 +521,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_U12_WIDE 17
 #define FP_TUNE_L21_ASYNC 18
 #define FP_TUNE_U12_ASYNC 19
+#define FP_TUNE_REST_SPLIT 20
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

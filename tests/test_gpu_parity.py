@@ -233,7 +233,7 @@ def test_factor_trace(fp, ctx):
     tags, streams, t0, t1 = ctx.trace_read()
     assert len(tags) > 10
     assert set(np.unique(tags)) <= set(range(9)) and {0, 1, 2, 3, 8} <= set(np.unique(tags))   # 8: the panel inverses
-    assert {0, 1} <= set(np.unique(streams)) <= {0, 1, 2}
+    assert {0, 1} <= set(np.unique(streams)) <= {0, 1, 2, 3}
     assert np.all(t1 >= t0) and np.all(t0 >= 0)
     for s in (0, 1):
         o = np.argsort(t0[streams == s])
