@@ -41,3 +41,21 @@ def test_no_device_is_a_clean_error(fp):
         pytest.skip("a device is present")
     with pytest.raises(fp._capi.FlowPanelError):
         fp._capi.Context(0)
+
+
+def test_binding_constants_match_header(fp):
+    """Every integer #define of include/flowpanel_b200.h that the Python binding
+    also defines has the same value there, and every fp_set_tuning knob
+    (FP_TUNE_*) is defined in the binding."""
+    src = open(os.path.join(ROOT, "include", "flowpanel_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    defs = {k: int(v) for k, v in re.findall(r"^\s*#define\s+(FP_\w+)\s+(-?\d+)\s*$", src, flags=re.M)}
+    assert any(k.startswith("FP_TUNE_") for k in defs)
+    cap = fp._capi
+    for k, v in defs.items():
+        if k.startswith("FP_TUNE_"):
+            assert hasattr(cap, k), k
+        if hasattr(cap, k):
+            assert getattr(cap, k) == v, (k, getattr(cap, k), v)
+    knobs = sorted(v for k, v in defs.items() if k.startswith("FP_TUNE_"))
+    assert knobs == list(range(len(knobs)))   # knob numbers are dense from 0
