@@ -23,6 +23,7 @@ k_asm_ring(const PanelRec* __restrict__ panels, int64_t n, const double* __restr
            int64_t ld, double offset, double cutoff2, double offset2, double* __restrict__ G,
            float* __restrict__ G32) {
   __shared__ PanelRec sp[kAsmPanels];
+  __shared__ int quads;   // every panel of the tile has 4 nodes
   const int64_t j0 = (int64_t)blockIdx.y * kAsmPanels;
   const int npt = (int)imin64(kAsmPanels, n - j0);
   {
@@ -30,11 +31,39 @@ k_asm_ring(const PanelRec* __restrict__ panels, int64_t n, const double* __restr
     double* dst = reinterpret_cast<double*>(sp);
     for (int q = threadIdx.x; q < npt * 16; q += kAsmThreads) dst[q] = src[q];
   }
+  if (threadIdx.x < 32) {
+    const bool q4 = threadIdx.x >= npt || (int)panels[j0 + threadIdx.x].nn == 4;
+    const unsigned all = __all_sync(0xffffffffu, q4);
+    if (threadIdx.x == 0) quads = (int)all;
+  }
   __syncthreads();
   const int64_t i = (int64_t)blockIdx.x * kAsmThreads + threadIdx.x;
   if (i >= n) return;
   const double X = tgt[i], Y = tgt[n + i], Z = tgt[2 * n + i];
   const double n1 = tgt[3 * n + i], n2 = tgt[4 * n + i], n3 = tgt[5 * n + i];
+  if (quads) {
+    // two panels a step, no per-panel branch on the node count: the two
+    // entries' sqrt / reciprocal chains are independent and interleave
+    int jj = 0;
+    for (; jj + 1 < npt; jj += 2) {
+      const double g0 = ring_dot_n<double, 4>(sp[jj].p, X, Y, Z, n1, n2, n3, offset, cutoff2, offset2);
+      const double g1 = ring_dot_n<double, 4>(sp[jj + 1].p, X, Y, Z, n1, n2, n3, offset, cutoff2, offset2);
+      const int64_t idx = (j0 + jj) * ld + i;
+      G[idx] = g0;
+      G[idx + ld] = g1;
+      if (W32) {
+        G32[idx] = (float)g0;
+        G32[idx + ld] = (float)g1;
+      }
+    }
+    if (jj < npt) {
+      const double g = ring_dot_n<double, 4>(sp[jj].p, X, Y, Z, n1, n2, n3, offset, cutoff2, offset2);
+      const int64_t idx = (j0 + jj) * ld + i;
+      G[idx] = g;
+      if (W32) G32[idx] = (float)g;
+    }
+    return;
+  }
   for (int jj = 0; jj < npt; ++jj) {
     const PanelRec& P = sp[jj];
     const double g = ring_dot<double>(P.p, (int)P.nn, X, Y, Z, n1, n2, n3, offset, cutoff2, offset2);
