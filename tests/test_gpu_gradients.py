@@ -140,3 +140,37 @@ def test_gradient_matches_central_differences(fp, setup):
     assert abs(ga - fd) <= 2e-6 * max(abs(fd), 1.0), (ga, fd)
     # a lifting wing: dCL/dAoA is positive and of thin-wing magnitude
     assert 1.0 < ga < 2 * np.pi
+
+
+@pytest.fixture(scope="module")
+def setup12k(fp):
+    import torch
+    A = fp.adjoint
+    w = fp.meshes.swept_wing("0012", 100, 120, CHORD, SPAN, SWEEP, 1.0)   # the 12,000-panel wing
+    g = A._Geom(w)
+    phi, xqc, zqc = A.twist_basis(w.nodes, 13)
+    solver = fp.B200Solver("ludiv", "fp64")
+    yield dict(torch=torch, A=A, w=w, g=g, phi=phi, xqc=xqc, zqc=zqc, solver=solver)
+    solver.close()
+
+
+def test_gradient_matches_central_differences_12k(fp, setup12k):
+    """Config 4 at its own size: dCL with respect to every vertex coordinate
+    of the 12,000-panel wing by the adjoint, against central finite
+    differences of the GPU primal (FP64, h = 1e-6) on 50 random unit
+    directions."""
+    S = setup12k
+    assert S["w"].npanels == 12000
+    CL0, gn, gt, ga = _gradients(S, 0)
+    assert np.all(np.isfinite(gn)) and 0.1 < CL0 < 0.5
+    rng = np.random.default_rng(12)
+    h = 1e-6
+    scale = np.abs(gn).max()
+    errs = []
+    for _ in range(50):
+        vn = rng.standard_normal(S["w"].nodes.shape)
+        vn /= np.linalg.norm(vn)
+        fd = (_primal(S, vn, np.zeros(13), 0.0, h, 0) - _primal(S, -vn, np.zeros(13), 0.0, h, 0)) / (2 * h)
+        adj = float(np.sum(gn * vn))
+        errs.append(abs(adj - fd) / max(abs(fd), scale))
+    assert max(errs) <= 2e-6, max(errs)
