@@ -155,7 +155,7 @@ def setup12k(fp):
 
 
 def test_gradient_matches_central_differences_12k(fp, setup12k):
-    """Config 4 at its own size: dCL with respect to every vertex coordinate
+    """The gradient at full size: dCL with respect to every vertex coordinate
     of the 12,000-panel wing by the adjoint, against central finite
     differences of the GPU primal (FP64, h = 1e-6) on 50 random unit
     directions."""
