@@ -961,7 +961,8 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       c->u12_async = value != 0;
       return FP_OK;
     case FP_TUNE_REST_SPLIT:
-      c->rest_split = value != 0;
+      if (value < 0 || value > 2) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_REST_SPLIT is 0, 1 or 2");
+      c->rest_split = value;
       return FP_OK;
     case FP_TUNE_TC_NARROW:
       if (value != 0 && value != 6) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_TC_NARROW is 0 or 6");

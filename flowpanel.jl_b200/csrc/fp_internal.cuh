@@ -112,7 +112,7 @@ struct fp_ctx {
   bool u12_async = false;               // static-order LU: k_u12g stages A12 column-major by cp.async (FP_TUNE_U12_ASYNC)
   bool u12_wide = false;                // static-order LU: U12 of the columns beyond, 64 columns a CTA (FP_TUNE_U12_WIDE)
   bool lu_fuse = false;                 // split chain: U12 and the diagonal tile's update in one kernel (FP_TUNE_LU_FUSE)
-  bool rest_split = false;              // split chain: the trailing update in two row ranges, U12 of the columns beyond on stream4 (FP_TUNE_REST_SPLIT)
+  int rest_split = 0;                   // split chain: the trailing update in two row ranges, U12 of the columns beyond on stream4 (FP_TUNE_REST_SPLIT; 2: the first range on stream4 too)
   bool pdl = true;                      // static-order LU: programmatic dependent launch of its kernels (FP_TUNE_PDL)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums

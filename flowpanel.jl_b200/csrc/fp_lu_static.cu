@@ -1218,6 +1218,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     // beyond runs on the fourth stream beside B; what reads B's rows waits
     // for ev_rest
     const bool rs = sp && c->rest_split;
+    // 2: T on the fourth stream after U12 of the columns beyond, so that B
+    // starts as soon as that U12 is done; T waits for B of the previous
+    // panel (the same rows), which keeps the additions to a row in order
+    const bool rs2 = rs && c->rest_split == 2;
     // the rows below this panel's diagonal block were last updated on the third stream
     if (prev_split && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_tcr, 0));
     if (sp) {
@@ -1354,13 +1358,21 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
             FP_CUDA_TRY(c->err, cudaGetLastError());
           }
           if (rs) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_u12r, c->stream));
+          if (rs2) {
+            FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));   // L21 of these rows
+            FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));    // B of the previous panel
+            if (int rc = update(slot, kend, K0, knext, n, knext - kend, 0, PW)) return rc;   // T
+            FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
+          }
         }
         if (rs) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_u12r, 0));
         // the update reads L21 (the panel stream's k_l21, and the third stream's when split)
         if (c->lu_overlap) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));
         if (rs) {
-          if (int rc = update(slot, kend, K0, knext, n, knext - kend, 0, PW)) return rc;   // T: the next panel's rows
-          FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
+          if (!rs2) {
+            if (int rc = update(slot, kend, K0, knext, n, knext - kend, 0, PW)) return rc;   // T: the next panel's rows
+            FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_top, c->stream));
+          }
           FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_l21t, 0));
           if (int rc = update(slot, kend, K0, knext, n, knext - kend, PW)) return rc;      // B: the rows below
           return FP_OK;

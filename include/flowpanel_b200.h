@@ -500,7 +500,10 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       the next panel's 128 rows first, then the rows below;
  *                       the next panel's U12 kernels wait for the first only,
  *                       and U12 of the columns beyond runs on a fourth stream
- *                       beside the second; 0 (default): one launch */
+ *                       beside the second; 2: the same with the first range
+ *                       on the fourth stream after that U12, so that the
+ *                       second starts as soon as the U12 is done; 0
+ *                       (default): one launch */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2

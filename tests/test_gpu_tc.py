@@ -50,7 +50,8 @@ def test_mixed_lu_refines_in_few_steps(fp, O, ctx, nc, ns, precision):
                                         ("FP_TUNE_ASM32", 1), ("FP_TUNE_TC_NARROW", 0), ("FP_TUNE_TRS2", 1),
                                         ("FP_TUNE_PANEL_GEMM", 0), ("FP_TUNE_PANEL_GEMM", 1), ("FP_TUNE_PANEL_GEMM", 2),
                                         ("FP_TUNE_TC_PREFETCH", 1), ("FP_TUNE_PDL", 1), ("FP_TUNE_LU_SPLIT", 0),
-                                        ("FP_TUNE_LU_FUSE", 1), ("FP_TUNE_REST_SPLIT", 1)])
+                                        ("FP_TUNE_LU_FUSE", 1), ("FP_TUNE_REST_SPLIT", 1),
+                                        ("FP_TUNE_REST_SPLIT", 2)])
 def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     """The static-order LU's tensor-core update variants: FP_TUNE_TC_SPLIT
     1..3 reads unsplit FP32 operands and splits them into TF32 hi / lo in
@@ -66,7 +67,8 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
     launches the kernels with programmatic dependent launch; FP_TUNE_LU_SPLIT 0
     keeps the rows below the next panel on the panel stream; FP_TUNE_LU_FUSE 1
     updates the next diagonal tile inside the U12 kernel; FP_TUNE_REST_SPLIT 1
-    runs the trailing update as the next panel's rows, then the rows below. The factors are as accurate as the default's (refinement
+    runs the trailing update as the next panel's rows, then the rows below
+    (2: the first range on the fourth stream). The factors are as accurate as the default's (refinement
     in a handful of steps, the oracle's solution to 1e-10), for one partial
     panel up to many panels with a partial last one (1,500 panels: a last K
     block of 92)."""
@@ -101,7 +103,8 @@ def test_static_lu_update_variants(fp, O, nc, ns, knob, value):
                           (2, 1, 1, 0, 0, 0, 0, 0, 0), (2, 1, 1, 1, 0, 0, 0, 0, 0), (2, 1, 1, 1, 1, 0, 0, 0, 0),
                           (2, 1, 1, 1, 0, 1, 0, 0, 0), (2, 1, 1, 1, 0, 0, 1, 0, 0), (2, 1, 1, 1, 0, 0, 1, 1, 0),
                           (2, 1, 1, 1, 1, 1, 1, 1, 0), (2, 1, 1, 1, 0, 0, 1, 0, 1), (2, 1, 1, 1, 1, 0, 1, 0, 1),
-                          (2, 1, 1, 0, 0, 0, 1, 0, 1), (1, 1, 1, 1, 0, 0, 1, 0, 1)])
+                          (2, 1, 1, 0, 0, 0, 1, 0, 1), (1, 1, 1, 1, 0, 0, 1, 0, 1), (2, 1, 1, 1, 0, 0, 1, 0, 2),
+                          (2, 1, 1, 1, 1, 0, 1, 0, 2)])
 def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, pdl, split, fuse, wide, l21a, u12a,
                                                 rsplit):
     """FP_TUNE_TC_BF16X3 1: the mixed form's trailing update multiplies BF16
