@@ -44,6 +44,7 @@ FP_TUNE_U12_WIDE = 17
 FP_TUNE_L21_ASYNC = 18
 FP_TUNE_U12_ASYNC = 19
 FP_TUNE_REST_SPLIT = 20
+FP_TUNE_PDIAG_LINV = 21
 
 
 class SolveOpts(C.Structure):

@@ -538,7 +538,11 @@ static int factor_static_graph(fp_ctx* c, bool bf16) {
                                 (uintptr_t)c->d_cert, (uintptr_t)c->d_status, (uintptr_t)c->d_minv,
                                 (uintptr_t)bf16, (uintptr_t)c->tc_stages, (uintptr_t)c->tc_tiles, (uintptr_t)c->tc_smem,
                                 (uintptr_t)c->tc_split, (uintptr_t)c->tc_red, (uintptr_t)c->tc_narrow_stages,
-                                (uintptr_t)c->lu_overlap, (uintptr_t)c->use_tc};
+                                (uintptr_t)c->lu_overlap, (uintptr_t)c->use_tc, (uintptr_t)c->panel_gemm,
+                                (uintptr_t)c->tc_x3, (uintptr_t)c->tc_prefetch, (uintptr_t)c->lu_split,
+                                (uintptr_t)c->lu_fuse, (uintptr_t)c->u12_wide, (uintptr_t)c->l21_async,
+                                (uintptr_t)c->u12_async, (uintptr_t)c->pdl, (uintptr_t)c->rest_split,
+                                (uintptr_t)c->pdiag_linv};
   for (int s = 0; s < 2; ++s)
     for (int i = 0; i < 4; ++i) key.push_back((uintptr_t)c->d_tc[s][i]);
   key.push_back((uintptr_t)c->d_dinv32);
@@ -959,6 +963,9 @@ int fp_set_tuning(fp_ctx* c, int knob, int value) {
       return FP_OK;
     case FP_TUNE_U12_ASYNC:
       c->u12_async = value != 0;
+      return FP_OK;
+    case FP_TUNE_PDIAG_LINV:
+      c->pdiag_linv = value != 0;
       return FP_OK;
     case FP_TUNE_REST_SPLIT:
       if (value < 0 || value > 2) return c->err.set(FP_EINVAL, "fp_set_tuning: FP_TUNE_REST_SPLIT is 0, 1 or 2");

@@ -114,6 +114,7 @@ struct fp_ctx {
   bool lu_fuse = false;                 // split chain: U12 and the diagonal tile's update in one kernel (FP_TUNE_LU_FUSE)
   int rest_split = 0;                   // split chain: the trailing update in two row ranges, U12 of the columns beyond on stream4 (FP_TUNE_REST_SPLIT; 2: the first range on stream4 too)
   bool pdl = true;                      // static-order LU: programmatic dependent launch of its kernels (FP_TUNE_PDL)
+  bool pdiag_linv = false;              // static-order LU: k_pdiag forms the full inv(L), no k_pinv (FP_TUNE_PDIAG_LINV)
   bool trs2_ready = false;              // R and S formed for the current FP32 factors
   double* d_part = nullptr;             // GEMV partial sums
   void* d_minv = nullptr;               // per block of a panel: M' = inv(L11) P11 (NB x NB, FP64 size), then the row order (NB ints)

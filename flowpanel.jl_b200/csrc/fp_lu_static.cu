@@ -191,10 +191,11 @@ __device__ __forceinline__ void store_block(float* __restrict__ g, int64_t ld, i
 //   (c) all warps update the rest of the block; the next diagonal block's
 //       tiles come first, so that warp 0 eliminates it while warps 1..7
 //       update the rest.
-constexpr size_t pdiag_smem() {
+constexpr size_t pdiag_smem(bool linv = false) {
   return (size_t)PW * SP * sizeof(float)        // As
          + (size_t)IB * SP * sizeof(float)      // LT: the inner block's L columns, transposed
-         + (size_t)2 * IB * sizeof(float);      // pivot row, two buffers
+         + (size_t)2 * IB * sizeof(float)       // pivot row, two buffers
+         + (linv ? (size_t)PW * (IB + 4) * sizeof(float) : 0);   // Dl: the four inv(L_kk) (full inv(L) only)
 }
 
 // Warp 0: the IB x IB block at (k0, k0) of As factored in place. Lane i
@@ -244,7 +245,8 @@ __device__ __forceinline__ void eliminate(float (*As)[SP], float* pbuf, int k0, 
 // Warp 0: inv(U_kk) -> dinv[.., 1]; warp 1: inv(L_kk) -> dinv[.., 0]; lane c
 // forms column c by substitution in registers (constant loop bounds, so the
 // loops unroll and the column stays in registers), four partial sums.
-__device__ __forceinline__ void invert(const float (*As)[SP], float* __restrict__ dinv, int kb, int warp, int lane) {
+__device__ __forceinline__ void invert(const float (*As)[SP], float* __restrict__ dinv, int kb, int warp, int lane,
+                                       float (*Dl)[IB + 4]) {
   const int k0 = kb * IB;
   if (warp == 0) {
     float x[IB];
@@ -282,6 +284,9 @@ __device__ __forceinline__ void invert(const float (*As)[SP], float* __restrict_
     }
 #pragma unroll
     for (int i = 0; i < IB; ++i) dinv[dinv_off(kb, 0) + i * IB + lane] = y[i];
+    if (Dl != nullptr)
+#pragma unroll
+      for (int i = 0; i < IB; ++i) Dl[kb * IB + i][lane] = y[i];
   }
 }
 
@@ -382,14 +387,69 @@ __device__ __forceinline__ void update_tiles(float (*As)[SP], const float (*LT)[
   }
 }
 
+// The full inv(L) of the factored block in As (with linvt, in place of a
+// separate k_pinv launch), by block rows: X_ii = D_i = inv(L_ii) (kept in Dl
+// by invert), X_ij = -D_i sum_{m=j}^{i-1} L_im X_mj for j < i. As is free
+// once the factors are stored: row block i of it still holds L when X_i. is
+// formed (the sums T_ij go to LT), the rows above already hold X. Written as
+// k_pinv writes it: linvt[c * PW + q] = inv(L)(q, c) for q in or below the
+// block row of c, 0 above.
+__device__ __forceinline__ void full_linv(float (*As)[SP], float (*LT)[SP], const float (*Dl)[IB + 4],
+                                          float* __restrict__ linvt, int tid) {
+  __syncthreads();   // every thread has read As for the store
+  for (int e = tid; e < NIB * IB * IB; e += kDiagThreads) {   // X_ii = D_i
+    const int b = e / (IB * IB), r = (e / IB) % IB, c = e % IB;
+    As[b * IB + r][b * IB + c] = Dl[b * IB + r][c];
+  }
+  __syncthreads();
+  const int r = tid >> 3, c4 = (tid & 7) * 4;   // a 1 x 4 piece of a 32 x 32 block
+#pragma unroll 1
+  for (int i = 1; i < NIB; ++i) {
+#pragma unroll 1
+    for (int j = 0; j < i; ++j) {   // T_ij = sum_m L(i IB + r, m) X(m, j IB + c4 ..)
+      float t[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+      for (int m = j * IB; m < i * IB; ++m) {
+        const float a = As[i * IB + r][m];
+        const float4 x = *reinterpret_cast<const float4*>(&As[m][j * IB + c4]);
+        t[0] = fmaf(a, x.x, t[0]); t[1] = fmaf(a, x.y, t[1]); t[2] = fmaf(a, x.z, t[2]); t[3] = fmaf(a, x.w, t[3]);
+      }
+      *reinterpret_cast<float4*>(&LT[r][j * IB + c4]) = make_float4(t[0], t[1], t[2], t[3]);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int j = 0; j < i; ++j) {   // X_ij = -D_i T_ij
+      float y[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
+      for (int q = 0; q < IB; ++q) {
+        const float d = Dl[i * IB + r][q];
+        const float4 x = *reinterpret_cast<const float4*>(&LT[q][j * IB + c4]);
+        y[0] = fmaf(d, x.x, y[0]); y[1] = fmaf(d, x.y, y[1]); y[2] = fmaf(d, x.z, y[2]); y[3] = fmaf(d, x.w, y[3]);
+      }
+      *reinterpret_cast<float4*>(&As[i * IB + r][j * IB + c4]) = make_float4(-y[0], -y[1], -y[2], -y[3]);
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < PW * PW / 4; e += kDiagThreads) {   // lanes over q: coalesced stores
+    const int q = e % PW, c0 = (e / PW) * 4;
+    const bool below = q / IB >= c0 / IB;   // the four columns share a block column
+    const float4 v = below ? *reinterpret_cast<const float4*>(&As[q][c0]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    linvt[(size_t)(c0 + 0) * PW + q] = v.x;
+    linvt[(size_t)(c0 + 1) * PW + q] = v.y;
+    linvt[(size_t)(c0 + 2) * PW + q] = v.z;
+    linvt[(size_t)(c0 + 3) * PW + q] = v.w;
+  }
+}
+
 __global__ void __launch_bounds__(kDiagThreads, 1)
 k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restrict__ dinv,
-        float* __restrict__ cert, int* __restrict__ status) {
+        float* __restrict__ cert, int* __restrict__ status, float* __restrict__ linvt) {
   griddep_wait();
   extern __shared__ __align__(16) unsigned char smem[];
   float (*As)[SP] = reinterpret_cast<float (*)[SP]>(smem);
   float (*LT)[SP] = reinterpret_cast<float (*)[SP]>(smem + (size_t)PW * SP * sizeof(float));
   float* pbuf = reinterpret_cast<float*>(LT + IB);
+  float (*Dl)[IB + 4] = linvt != nullptr ? reinterpret_cast<float (*)[IB + 4]>(pbuf + 2 * IB) : nullptr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nb = (int)imin64(PW, n - k);
   load_block<kDiagThreads, PW, PW>(
@@ -402,7 +462,7 @@ k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restr
 #pragma unroll 1
   for (int kb = 0; kb < NIB; ++kb) {
     const int k0 = kb * IB, R = PW - k0 - IB;   // R rows (and columns) after the inner block
-    if (warp < 2) invert(As, dinv, kb, warp, lane);
+    if (warp < 2) invert(As, dinv, kb, warp, lane, Dl);
     else if (tid - 64 < 2 * R) substitute(As, LT, k0, R, tid - 64, lmax);
     if (R == 0) break;
     __syncthreads();
@@ -420,6 +480,7 @@ k_pdiag(float* __restrict__ A, int64_t lda, int64_t n, int64_t k, float* __restr
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(FULL, lmax, o));
   if (lane == 0) atomic_max_pos(cert, lmax);
+  if (linvt != nullptr && nb == PW) full_linv(As, LT, Dl, linvt, tid);
 }
 
 // The split of four consecutive K values of a K-major operand at o (element
@@ -1105,6 +1166,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   // 2: L21 by block substitution on the panel stream, inv(L) alone on the
   // third stream beside it; 1: both inverses on the panel stream, L21 = A21 inv(U)
   const bool lside = pg && c->panel_gemm == 2;
+  // FP_TUNE_PDIAG_LINV: k_pdiag forms the full inv(L) too (no k_pinv), and
+  // with the split chain L21 of the next panel's rows moves to the third
+  // stream, beside U12 of the next panel's columns on the panel stream
+  const bool dl = lside && c->pdiag_linv;
   const bool lg = pg && !lside;
   typedef U12gCfg<16> GCfgN;
   typedef U12gCfg<32> GCfgR;
@@ -1124,7 +1189,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
   }
   // the FP32 form's update from BF16 pairs (needs the GEMM-form panel kernels)
   const bool x3 = !bf16 && pg && c->tc_x3 && c->use_tc;
-  FP_CUDA_TRY(c->err, attr_d.ensure(k_pdiag, (int)pdiag_smem()));
+  FP_CUDA_TRY(c->err, attr_d.ensure(k_pdiag, (int)pdiag_smem(true)));
   FP_CUDA_TRY(c->err, attr_l.ensure(k_l21<kSplitTf32>, (int)l21_smem()));
   FP_CUDA_TRY(c->err, attr_lx.ensure(k_l21<kSplitBf16x2>, (int)l21_smem()));
   FP_CUDA_TRY(c->err, attr_un.ensure(k_u12<16, 1, false>, (int)CfgN::smem()));
@@ -1184,7 +1249,9 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     float* const* s = c->d_tc[slot];
     {
       TraceScope tr(c, TR_DIAG);
-      launch_k(c->pdl, k_pdiag, 1, kDiagThreads, pdiag_smem(), c->stream, A, lda, n, K0, dinv, cert, c->d_status);
+      float* const linvt = (dl && kend < n) ? dinv + kLinvtOff : nullptr;
+      launch_k(c->pdl, k_pdiag, 1, kDiagThreads, pdiag_smem(linvt != nullptr), c->stream, A, lda, n, K0, dinv, cert,
+               c->d_status, linvt);
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
@@ -1197,7 +1264,8 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     // the columns beyond the next panel need only the diagonal block's
     // inverses for their U12: the second stream starts them beside k_l21
     FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_diag, c->stream));
-    if (lside && kend < n) {   // inv(L) (the first NIB CTAs of k_pinv) on the third stream, beside k_l21
+    if (dl && kend < n) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_pinv, c->stream));   // inv(L) came with k_pdiag
+    if (lside && !dl && kend < n) {   // inv(L) (the first NIB CTAs of k_pinv) on the third stream, beside k_l21
       OnStream on3(c, c->stream3);
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_diag, 0));
       {
@@ -1226,6 +1294,10 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
     if (prev_split && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_tcr, 0));
     if (sp) {
       float* const al = s[1];
+      // with the full inv(L) from k_pdiag both L21 launches run on the third
+      // stream, the next panel's rows first
+      OnStream on3h(c, dl ? c->stream3 : c->stream);
+      if (dl) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_diag, 0));
       {
         TraceScope tr(c, TR_L21);
         const int64_t he = kend + PW;   // the next panel's rows
@@ -1238,6 +1310,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         ++c->nlaunch;
         FP_CUDA_TRY(c->err, cudaGetLastError());
       }
+      if (dl) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_panel, c->stream));
       OnStream on3(c, c->stream3);
       {
         TraceScope tr(c, TR_L21);
@@ -1269,7 +1342,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       ++c->nlaunch;
       FP_CUDA_TRY(c->err, cudaGetLastError());
     }
-    FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_panel, c->stream));
+    if (!(dl && sp)) FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_panel, c->stream));
     if (knext > kend) {
       // split: U12 of the next panel's columns and the update of its diagonal
       // tile in one launch (k_u12g<16, ., true>)
@@ -1280,6 +1353,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
       FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->rest_split && !fused ? c->ev_top : c->ev_rest, 0));
       if (lside && kend < n) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_pinv, 0));
       if (fused) {
+        if (dl) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));   // L21 of the next panel's rows
         TraceScope tr(c, TR_U12);
         const unsigned g = (unsigned)((knext - kend + 15) / 16);
         if (x3)
@@ -1310,6 +1384,7 @@ int lu_factor_static(fp_ctx* c, float* A, int64_t n, int64_t lda, int32_t* ipiv,
         FP_CUDA_TRY(c->err, cudaEventRecord(c->ev_u12n, c->stream));
         if (!fused) {
           if (c->rest_split) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_rest, 0));
+          if (dl) FP_CUDA_TRY(c->err, cudaStreamWaitEvent(c->stream, c->ev_panel, 0));   // L21 of these rows
           if (int rc = update(slot, kend, K0, kend, knext, 0, 0, PW)) return rc;   // the next diagonal block's rows
         }
         OnStream on3(c, c->stream3);

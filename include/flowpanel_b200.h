@@ -503,7 +503,13 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
  *                       beside the second; 2: the same with the first range
  *                       on the fourth stream after that U12, so that the
  *                       second starts as soon as the U12 is done; 0
- *                       (default): one launch */
+ *                       (default): one launch
+ *   FP_TUNE_PDIAG_LINV  1: the diagonal-block kernel also forms the full
+ *                       inverse of the block's L (no separate inverse
+ *                       launch), and with the split chain L21 of the next
+ *                       panel's rows runs on the third stream beside U12 of
+ *                       the next panel's columns; 0 (default): a separate
+ *                       launch on the third stream */
 #define FP_TUNE_TC_STAGES 0
 #define FP_TUNE_LU_OVERLAP 1
 #define FP_TUNE_TC_TILES 2
@@ -525,6 +531,7 @@ int fp_measure_fma_peak(int device, int fp64, double* tflops);
 #define FP_TUNE_L21_ASYNC 18
 #define FP_TUNE_U12_ASYNC 19
 #define FP_TUNE_REST_SPLIT 20
+#define FP_TUNE_PDIAG_LINV 21
 int fp_set_tuning(fp_ctx* ctx, int knob, int value);
 
 /* Autotuner (no counterpart in the reference): times the factorisation of the

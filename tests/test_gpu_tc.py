@@ -143,6 +143,40 @@ def test_bf16_pair_update_reaches_fp64_solution(fp, O, nc, ns, panel, prefetch, 
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
 
 
+@pytest.mark.parametrize("nc,ns", [(12, 8), (20, 24), (60, 80), (50, 30)])
+@pytest.mark.parametrize("split,fuse,rsplit,x3", [(1, 0, 0, 1), (1, 1, 0, 1), (1, 0, 2, 1), (0, 0, 0, 1), (1, 0, 0, 0)])
+def test_pdiag_full_inverse(fp, O, nc, ns, split, fuse, rsplit, x3):
+    """FP_TUNE_PDIAG_LINV 1: the diagonal-block kernel forms the full inv(L)
+    (no separate inverse launch) and L21 of the next panel's rows runs on the
+    third stream; the mixed solve still reaches the oracle's solution to
+    1e-10 with the split chain on or off, the fused U12 kernel, the trailing
+    update in two row ranges, and either operand form."""
+    w = fp.meshes.swept_wing("0012", nc, ns)
+    body = fp.RigidWakeBody(w)
+    normals = fp.calc_normals(body)
+    cps = fp.calc_controlpoints(body, normals)
+    a = np.deg2rad(4.2)
+    V = np.array([np.cos(a), 0, np.sin(a)])
+    D = np.tile(V, (w.nsheddings, 1))
+    U = np.tile(V, (w.npanels, 1))
+    c = fp._capi.Context(0)
+    try:
+        c.set_tuning(fp._capi.FP_TUNE_PDIAG_LINV, 1)
+        c.set_tuning(fp._capi.FP_TUNE_TC_BF16X3, x3)
+        c.set_tuning(fp._capi.FP_TUNE_LU_SPLIT, split)
+        c.set_tuning(fp._capi.FP_TUNE_LU_FUSE, fuse)
+        c.set_tuning(fp._capi.FP_TUNE_REST_SPLIT, rsplit)
+        c.set_geometry(w.nodes, w.panel_offsets, w.panel_nodes, cps, normals)
+        c.set_wake(w.shedding, D, D)
+        x, st = c.solve_body(fp._capi.FP_ELEMENT_VORTEXRING, U, opts=fp._capi.make_opts("ludiv", "mixed"))
+    finally:
+        c.close()
+    assert st.used_gmres == 0 and st.ir_iters <= 5 and st.rel_residual < 1e-11, st.asdict()
+    Gr = O.assemble_vortexring(w, cps, normals, D, D)
+    xr = O.solve_ludiv(Gr, O.rhs_noflowthrough(U, normals))
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-10
+
+
 @pytest.mark.parametrize("nc,ns", [(20, 24), (60, 80)])
 def test_bf16_form_reaches_fp64_solution(fp, O, ctx, nc, ns):
     """FP_PREC_BF16: the factorisation starts from the BF16-rounded AIC and its
